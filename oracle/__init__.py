@@ -1,0 +1,408 @@
+"""CPU oracles for the dense depthmap path.  TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+and reference legs import this package, and only as the checker or as the
+timed CPU baseline.  The product (``opensfm_b200``) never imports it.
+
+Three oracles:
+
+``port``
+    ``depthmap_oracle.c``: this project's plain-C restatement of the
+    reference's legacy path (``opensfm/src/lib/dense/src/depthmap.cc``):
+    brute force, PatchMatch (raster schedule, seeded RNG), plane scoring,
+    median post-process, cleaner, pruner.
+``ref``
+    The reference's own ``depthmap.cc`` compiled unmodified against the
+    project's OpenCV shim (``oracle/Makefile`` -> ``oracle/_ref/``), driven
+    through ``ref_capi.cc``.  Present wherever ``/root/reference`` was
+    available when ``make`` ran; ``ref_available()`` says whether it is.
+``ncc_fp64``
+    A numpy float64 restatement of ``ComputePlaneImageScore``
+    (``depthmap.cc:441-487``), the yardstick for NCC error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libdepthmap_ref.so")
+REF_DENSE = "/root/reference/opensfm/src/lib/dense"
+
+_port = None
+_ref = None
+
+_d = ctypes.POINTER(ctypes.c_double)
+_f = ctypes.POINTER(ctypes.c_float)
+_u8 = ctypes.POINTER(ctypes.c_uint8)
+_i32 = ctypes.POINTER(ctypes.c_int32)
+
+
+def build(with_ref: bool = True) -> None:
+    """Builds the C restatement, and the compiled reference if its sources exist."""
+    subprocess.check_call(["make", "-s", "-C", HERE, os.path.join(HERE, "_build", "liboracle.so")])
+    if with_ref and os.path.isdir(REF_DENSE):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_DENSE={REF_DENSE}"])
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def _P(a, t):
+    return a.ctypes.data_as(t)
+
+
+def port():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_LIB):
+            build(with_ref=False)
+        L = ctypes.CDLL(PORT_LIB)
+        L.or_compute.argtypes = [ctypes.c_int, ctypes.c_int, _d, _d, _d, _u8, _u8, ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint64,
+                                 _f, _f, _f, _i32]
+        L.or_score_planes.argtypes = [ctypes.c_int, _d, _d, _d, _u8, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, _f, _f, _i32]
+        L.or_median5.argtypes = [_f, _f, ctypes.c_int, ctypes.c_int]
+        L.or_clean.argtypes = [ctypes.c_int, _d, _d, _d, _f, ctypes.c_int, ctypes.c_int,
+                               ctypes.c_float, ctypes.c_int, _f]
+        L.or_prune.argtypes = [ctypes.c_int, _d, _d, _d, _f, _f, _u8, _u8, ctypes.c_int,
+                               ctypes.c_int, ctypes.c_float, _f, _f, _u8, _u8, ctypes.c_long]
+        L.or_prune.restype = ctypes.c_long
+        L.or_inv3.argtypes = [_d, _d]
+        L.or_patch_variance.argtypes = [_u8, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int]
+        L.or_patch_variance.restype = ctypes.c_float
+        _port = L
+    return _port
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise FileNotFoundError("compiled reference oracle not built: " + REF_LIB)
+        L = ctypes.CDLL(REF_LIB)
+        L.ref_est_new.restype = ctypes.c_void_p
+        L.ref_est_free.argtypes = [ctypes.c_void_p]
+        L.ref_est_add_view.argtypes = [ctypes.c_void_p, _d, _d, _d, _u8, _u8, ctypes.c_int,
+                                       ctypes.c_int]
+        L.ref_est_set_depth_range.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_int]
+        L.ref_est_set_patchmatch_iterations.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_est_set_patch_size.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_est_set_min_patch_sd.argtypes = [ctypes.c_void_p, ctypes.c_float]
+        L.ref_est_compute.argtypes = [ctypes.c_void_p, ctypes.c_int, _f, _f, _f, _i32]
+        L.ref_est_score_planes.argtypes = [ctypes.c_void_p, _f, _f, _i32]
+        L.ref_est_plane_image_score.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _f,
+                                                ctypes.c_int]
+        L.ref_est_plane_image_score.restype = ctypes.c_float
+        L.ref_patch_variance.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.ref_patch_variance.restype = ctypes.c_float
+        L.ref_median5.argtypes = [_f, _f, ctypes.c_int, ctypes.c_int]
+        L.ref_inv3.argtypes = [_d, _d]
+        L.ref_srand.argtypes = [ctypes.c_uint]
+        L.ref_cleaner_new.restype = ctypes.c_void_p
+        L.ref_cleaner_free.argtypes = [ctypes.c_void_p]
+        L.ref_cleaner_set_same_depth_threshold.argtypes = [ctypes.c_void_p, ctypes.c_float]
+        L.ref_cleaner_set_min_consistent_views.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_cleaner_add_view.argtypes = [ctypes.c_void_p, _d, _d, _d, _f, ctypes.c_int,
+                                           ctypes.c_int]
+        L.ref_cleaner_clean.argtypes = [ctypes.c_void_p, _f, ctypes.c_int, ctypes.c_int]
+        L.ref_pruner_new.restype = ctypes.c_void_p
+        L.ref_pruner_free.argtypes = [ctypes.c_void_p]
+        L.ref_pruner_set_same_depth_threshold.argtypes = [ctypes.c_void_p, ctypes.c_float]
+        L.ref_pruner_add_view.argtypes = [ctypes.c_void_p, _d, _d, _d, _f, _f, _u8, _u8,
+                                          ctypes.c_int, ctypes.c_int]
+        L.ref_pruner_prune.argtypes = [ctypes.c_void_p]
+        L.ref_pruner_prune.restype = ctypes.c_long
+        L.ref_pruner_fetch.argtypes = [ctypes.c_void_p, _f, _f, _u8, _u8]
+        _ref = L
+    return _ref
+
+
+# --------------------------------------------------------------------------
+# Views: every oracle entry takes lists of K, R, t (float64) and images.
+
+def _stack_cams(Ks, Rs, ts):
+    K = np.ascontiguousarray(np.stack([np.asarray(k, np.float64).reshape(9) for k in Ks]))
+    R = np.ascontiguousarray(np.stack([np.asarray(r, np.float64).reshape(9) for r in Rs]))
+    t = np.ascontiguousarray(np.stack([np.asarray(x, np.float64).reshape(3) for x in ts]))
+    return K, R, t
+
+
+def port_compute(mode: int, Ks, Rs, ts, images, masks, patch_size=7, min_depth=1.0,
+                 max_depth=10.0, num_planes=50, iterations=3, min_patch_sd=1.0, seed=1):
+    """mode 0 brute force, 1 PatchMatch, 2 PatchMatch (sample)."""
+    K, R, t = _stack_cams(Ks, Rs, ts)
+    im = np.ascontiguousarray(np.stack(images).astype(np.uint8))
+    mk = np.ascontiguousarray(np.stack(masks).astype(np.uint8))
+    n, H, W = im.shape
+    depth = np.zeros((H, W), np.float32)
+    plane = np.zeros((H, W, 3), np.float32)
+    score = np.zeros((H, W), np.float32)
+    nghbr = np.zeros((H, W), np.int32)
+    port().or_compute(mode, n, _P(K, _d), _P(R, _d), _P(t, _d), _P(im, _u8), _P(mk, _u8), W, H,
+                      patch_size, min_depth, max_depth, num_planes, iterations, min_patch_sd,
+                      seed, _P(depth, _f), _P(plane, _f), _P(score, _f), _P(nghbr, _i32))
+    return depth, plane, score, nghbr
+
+
+def port_score_planes(Ks, Rs, ts, images, planes, patch_size=7):
+    K, R, t = _stack_cams(Ks, Rs, ts)
+    im = np.ascontiguousarray(np.stack(images).astype(np.uint8))
+    n, H, W = im.shape
+    pl = np.ascontiguousarray(planes, np.float32)
+    score = np.zeros((H, W), np.float32)
+    nghbr = np.zeros((H, W), np.int32)
+    port().or_score_planes(n, _P(K, _d), _P(R, _d), _P(t, _d), _P(im, _u8), W, H, patch_size,
+                           _P(pl, _f), _P(score, _f), _P(nghbr, _i32))
+    return score, nghbr
+
+
+def port_median5(depth):
+    d = np.ascontiguousarray(depth, np.float32)
+    out = np.empty_like(d)
+    port().or_median5(_P(d, _f), _P(out, _f), d.shape[1], d.shape[0])
+    return out
+
+
+def port_clean(Ks, Rs, ts, depths, threshold=0.01, min_views=2):
+    K, R, t = _stack_cams(Ks, Rs, ts)
+    d = np.ascontiguousarray(np.stack(depths).astype(np.float32))
+    n, H, W = d.shape
+    out = np.zeros((H, W), np.float32)
+    port().or_clean(n, _P(K, _d), _P(R, _d), _P(t, _d), _P(d, _f), W, H, threshold, min_views,
+                    _P(out, _f))
+    return out
+
+
+def port_prune(Ks, Rs, ts, depths, planes, colors, labels, threshold=0.01):
+    K, R, t = _stack_cams(Ks, Rs, ts)
+    d = np.ascontiguousarray(np.stack(depths).astype(np.float32))
+    p = np.ascontiguousarray(np.stack(planes).astype(np.float32))
+    c = np.ascontiguousarray(np.stack(colors).astype(np.uint8))
+    lb = np.ascontiguousarray(np.stack(labels).astype(np.uint8))
+    n, H, W = d.shape
+    cap = H * W
+    pts = np.zeros((cap, 3), np.float32)
+    nrm = np.zeros((cap, 3), np.float32)
+    col = np.zeros((cap, 3), np.uint8)
+    lab = np.zeros((cap,), np.uint8)
+    cnt = port().or_prune(n, _P(K, _d), _P(R, _d), _P(t, _d), _P(d, _f), _P(p, _f), _P(c, _u8),
+                          _P(lb, _u8), W, H, threshold, _P(pts, _f), _P(nrm, _f), _P(col, _u8),
+                          _P(lab, _u8), cap)
+    return pts[:cnt].copy(), nrm[:cnt].copy(), col[:cnt].copy(), lab[:cnt].copy()
+
+
+# --------------------------------------------------------------------------
+# The compiled reference, through the same argument conventions.
+
+class RefEstimator:
+    """The reference's dense::DepthmapEstimator (compiled), pydense-style."""
+
+    def __init__(self):
+        self.L = ref()
+        self.h = self.L.ref_est_new()
+        self.shape = None
+        self._keep = []
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.ref_est_free(self.h)
+            self.h = None
+
+    def add_view(self, K, R, t, image, mask):
+        K = np.ascontiguousarray(K, np.float64)
+        R = np.ascontiguousarray(R, np.float64)
+        t = np.ascontiguousarray(t, np.float64)
+        im = np.ascontiguousarray(image, np.uint8)
+        mk = np.ascontiguousarray(mask, np.uint8)
+        self._keep += [K, R, t]
+        if self.shape is None:
+            self.shape = im.shape
+        self.L.ref_est_add_view(self.h, _P(K, _d), _P(R, _d), _P(t, _d), _P(im, _u8),
+                                _P(mk, _u8), im.shape[1], im.shape[0])
+
+    def set_depth_range(self, mn, mx, n):
+        self.L.ref_est_set_depth_range(self.h, mn, mx, n)
+
+    def set_patchmatch_iterations(self, n):
+        self.L.ref_est_set_patchmatch_iterations(self.h, n)
+
+    def set_patch_size(self, n):
+        self.L.ref_est_set_patch_size(self.h, n)
+
+    def set_min_patch_sd(self, sd):
+        self.L.ref_est_set_min_patch_sd(self.h, sd)
+
+    def _compute(self, mode):
+        H, W = self.shape
+        depth = np.zeros((H, W), np.float32)
+        plane = np.zeros((H, W, 3), np.float32)
+        score = np.zeros((H, W), np.float32)
+        nghbr = np.zeros((H, W), np.int32)
+        self.L.ref_est_compute(self.h, mode, _P(depth, _f), _P(plane, _f), _P(score, _f),
+                               _P(nghbr, _i32))
+        return [depth, plane, score, nghbr]
+
+    def compute_brute_force(self):
+        return self._compute(0)
+
+    def compute_patch_match(self):
+        return self._compute(1)
+
+    def compute_patch_match_sample(self):
+        return self._compute(2)
+
+    def score_planes(self, planes):
+        H, W = self.shape
+        pl = np.ascontiguousarray(planes, np.float32)
+        score = np.zeros((H, W), np.float32)
+        nghbr = np.zeros((H, W), np.int32)
+        self.L.ref_est_score_planes(self.h, _P(pl, _f), _P(score, _f), _P(nghbr, _i32))
+        return score, nghbr
+
+
+def ref_clean(Ks, Rs, ts, depths, threshold=0.01, min_views=2):
+    L = ref()
+    h = L.ref_cleaner_new()
+    keep = []
+    try:
+        L.ref_cleaner_set_same_depth_threshold(h, threshold)
+        L.ref_cleaner_set_min_consistent_views(h, min_views)
+        for K, R, t, d in zip(Ks, Rs, ts, depths):
+            K = np.ascontiguousarray(K, np.float64)
+            R = np.ascontiguousarray(R, np.float64)
+            t = np.ascontiguousarray(t, np.float64)
+            d = np.ascontiguousarray(d, np.float32)
+            keep += [K, R, t, d]
+            L.ref_cleaner_add_view(h, _P(K, _d), _P(R, _d), _P(t, _d), _P(d, _f), d.shape[1],
+                                   d.shape[0])
+        H, W = depths[0].shape
+        out = np.zeros((H, W), np.float32)
+        L.ref_cleaner_clean(h, _P(out, _f), W, H)
+        return out
+    finally:
+        L.ref_cleaner_free(h)
+
+
+def ref_prune(Ks, Rs, ts, depths, planes, colors, labels, threshold=0.01):
+    L = ref()
+    h = L.ref_pruner_new()
+    keep = []
+    try:
+        L.ref_pruner_set_same_depth_threshold(h, threshold)
+        for K, R, t, d, p, c, lb in zip(Ks, Rs, ts, depths, planes, colors, labels):
+            arrs = [np.ascontiguousarray(K, np.float64), np.ascontiguousarray(R, np.float64),
+                    np.ascontiguousarray(t, np.float64), np.ascontiguousarray(d, np.float32),
+                    np.ascontiguousarray(p, np.float32), np.ascontiguousarray(c, np.uint8),
+                    np.ascontiguousarray(lb, np.uint8)]
+            keep += arrs
+            L.ref_pruner_add_view(h, _P(arrs[0], _d), _P(arrs[1], _d), _P(arrs[2], _d),
+                                  _P(arrs[3], _f), _P(arrs[4], _f), _P(arrs[5], _u8),
+                                  _P(arrs[6], _u8), d.shape[1], d.shape[0])
+        n = L.ref_pruner_prune(h)
+        pts = np.zeros((n, 3), np.float32)
+        nrm = np.zeros((n, 3), np.float32)
+        col = np.zeros((n, 3), np.uint8)
+        lab = np.zeros((n,), np.uint8)
+        if n:
+            L.ref_pruner_fetch(h, _P(pts, _f), _P(nrm, _f), _P(col, _u8), _P(lab, _u8))
+        return pts, nrm, col, lab
+    finally:
+        L.ref_pruner_free(h)
+
+
+def ref_median5(depth):
+    d = np.ascontiguousarray(depth, np.float32)
+    out = np.empty_like(d)
+    ref().ref_median5(_P(d, _f), _P(out, _f), d.shape[1], d.shape[0])
+    return out
+
+
+# --------------------------------------------------------------------------
+# float64 NCC restatement (depthmap.cc:441-487), vectorised over pixels.
+
+def ncc_fp64(Ks, Rs, ts, images, planes, patch_size=7, pixels=None):
+    """Per-pixel max-over-views NCC in float64 for the given planes.
+
+    Returns (score (H, W) float64, nghbr (H, W) int32); the homography, the
+    affine warp, bilinear sampling, bilateral weights and the moments are all
+    float64.  ``pixels``: optional boolean mask restricting the work.
+    """
+    K = [np.asarray(k, np.float64) for k in Ks]
+    R = [np.asarray(r, np.float64) for r in Rs]
+    t = [np.asarray(x, np.float64).reshape(3) for x in ts]
+    imgs = [np.asarray(im, np.float64) for im in images]
+    H, W = imgs[0].shape
+    hpz = (patch_size - 1) // 2
+    ii, jj = np.mgrid[0:H, 0:W]
+    interior = (ii >= hpz) & (ii < H - hpz) & (jj >= hpz) & (jj < W - hpz)
+    if pixels is not None:
+        interior &= pixels
+    pi, pj = ii[interior].astype(np.float64), jj[interior].astype(np.float64)
+    v = np.asarray(planes, np.float64)[interior]  # (P, 3)
+    K1inv = np.linalg.inv(K[0])
+    best = np.full(pi.shape, -1.0)
+    bestn = np.zeros(pi.shape, np.int32)
+    ref = imgs[0]
+    c = ref[pi.astype(int), pj.astype(int)]
+    for o in range(1, len(imgs)):
+        Q = R[o] @ R[0].T
+        a = Q @ t[0] - t[o]
+        # H = K2 (Q + a v^T) K1inv, per pixel.
+        M = Q[None] + a[None, :, None] * v[:, None, :]
+        Hm = K[o][None] @ M @ K1inv[None]
+        u = Hm[:, 0, 0] * pj + Hm[:, 0, 1] * pi + Hm[:, 0, 2]
+        vv = Hm[:, 1, 0] * pj + Hm[:, 1, 1] * pi + Hm[:, 1, 2]
+        w = Hm[:, 2, 0] * pj + Hm[:, 2, 1] * pi + Hm[:, 2, 2]
+        ok = w != 0
+        w = np.where(ok, w, 1.0)
+        dxx = (Hm[:, 0, 0] * w - Hm[:, 2, 0] * u) / (w * w)
+        dxy = (Hm[:, 1, 0] * w - Hm[:, 2, 0] * vv) / (w * w)
+        dyx = (Hm[:, 0, 1] * w - Hm[:, 2, 1] * u) / (w * w)
+        dyy = (Hm[:, 1, 1] * w - Hm[:, 2, 1] * vv) / (w * w)
+        x0, y0 = u / w, vv / w
+        sx = sy = sxx = syy = sxy = sw = 0.0
+        img = imgs[o]
+        for dy in range(-hpz, hpz + 1):
+            for dx in range(-hpz, hpz + 1):
+                x1 = ref[pi.astype(int) + dy, pj.astype(int) + dx]
+                x2 = x0 + dxx * dx + dyx * dy
+                y2 = y0 + dxy * dx + dyy * dy
+                inside = (x2 >= 0) & (x2 < W - 1) & (y2 >= 0) & (y2 < H - 1)
+                xs = np.where(inside, x2, 0.0)
+                ys = np.where(inside, y2, 0.0)
+                ix, iy = np.floor(xs).astype(int), np.floor(ys).astype(int)
+                fx, fy = xs - ix, ys - iy
+                s = ((1 - fy) * ((1 - fx) * img[iy, ix] + fx * img[iy, ix + 1]) +
+                     fy * ((1 - fx) * img[iy + 1, ix] + fx * img[iy + 1, ix + 1]))
+                y = np.where(inside, s, 0.0)
+                wt = np.exp(-(x1 - c) ** 2 / (2 * 50.0 ** 2) - (dx * dx + dy * dy) / (2 * 25.0))
+                sx = sx + wt * x1
+                sy = sy + wt * y
+                sxx = sxx + wt * x1 * x1
+                syy = syy + wt * y * y
+                sxy = sxy + wt * x1 * y
+                sw = sw + wt
+        mx, my = sx / sw, sy / sw
+        vx = sxx / sw - mx * mx
+        vy = syy / sw - my * my
+        ncc = np.where((vx < 0.1) | (vy < 0.1) | ~ok, -1.0,
+                       (sxy / sw - mx * my) / np.sqrt(np.maximum(vx * vy, 1e-300)))
+        upd = ncc > best
+        best = np.where(upd, ncc, best)
+        bestn = np.where(upd, o, bestn)
+    score = np.zeros((H, W))
+    nghbr = np.zeros((H, W), np.int32)
+    score[interior] = best
+    nghbr[interior] = bestn
+    return score, nghbr
