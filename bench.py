@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Benchmark of the dense depthmap path on B200.
+
+Workload (one "step"): a ring reconstruction of 24 reference views at
+640 x 480 (box scene: ground plane + 12 boxes, 4-octave value-noise texture),
+each depthmap scored against its 6 nearest matching views with patch 7,
+min patch sd 1.0 and 3 PatchMatch iterations, then DepthmapCleaner
+(threshold 0.01, 3 consistent views) over each map's 10 candidate
+neighbours.  Synthetic, seeded, ray-cast in this process.
+
+``value``: depthmaps/s with the views resident in HBM (one batched run per
+step, replayed from a CUDA graph), device-timed over K steps.  ``e2e``: the
+same through the public batch API from host buffers, each step uploading
+every view image and reading every cleaned depth map back.
+
+``--impl reference`` times the reference's own CPU depthmap code
+(opensfm/src/lib/dense/src/depthmap.cc compiled as oracle/_ref) on the
+host's cores on bands of the same workload.
+
+Multi-GPU: one process per GPU (torchrun); each rank runs its own replica of
+the reconstruction (the path has no exchange step), so scaling is weak and
+the job value is the sum over ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "640px depthmaps/s (6 views, 3 iters): learned-init vs plain at equal accuracy"
+UNIT = "depthmaps/s"
+W_, H_ = 640, 480
+N_VIEWS, N_CAND, N_MATCH = 24, 10, 6
+PATCH, MIN_SD, ITERS = 7, 1.0, 3
+SEED = 2024
+FLOPS_PER_TAP = 25  # affine warp 8 + bilinear 11 + NCC sums 6 (FMA = 2)
+
+
+# ---------------------------------------------------------------- workload
+def make_workload(seed=SEED, n_views=N_VIEWS, W=W_, H=H_):
+    from opensfm_b200 import synthetic as S
+
+    vs = S.ring_viewset(seed, n_views, W, H)
+    ranges = [S.depth_range(d) for d in vs.depths]
+    cands = [vs.neighbors(v, N_CAND) for v in range(n_views)]
+    matches = [c[:N_MATCH] for c in cands]
+    return vs, ranges, cands, matches
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, n in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(
+        os.environ.get("LOCAL_RANK", 0))
+
+
+class Group:
+    """Barrier + max-reduce across ranks (torch.distributed, NCCL) for N > 1."""
+
+    def __init__(self, world, local_rank):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            self.torch, self.dist = torch, dist
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.dist.destroy_process_group()
+
+
+# ------------------------------------------------------------- CPU legs
+def _ref_band(task):
+    """Reference PatchMatch on rows [r0, r0 + rows) of one reference view."""
+    import oracle as O
+
+    (K, R, t, img, nbrs, r0, rows, mn, mx, hpz) = task
+    H, W = img.shape
+    top = max(r0 - hpz, 0)
+    bot = min(r0 + rows + hpz, H)
+    Kc = K.copy()
+    Kc[1, 2] -= top
+    e = O.RefEstimator() if O.ref_available() else None
+    t0 = time.perf_counter()
+    if e is not None:
+        crop = np.ascontiguousarray(img[top:bot])
+        e.add_view(Kc, R, t, crop, np.ones_like(crop))
+        for (Kn, Rn, tn, imn) in nbrs:
+            # Matching views keep their full extent (the reference samples
+            # each view with its own size, depthmap.cc:472).
+            e.add_view(Kn, Rn, tn, imn, np.ones_like(imn))
+        e.set_depth_range(mn, mx, 50)
+        e.set_patch_size(PATCH)
+        e.set_min_patch_sd(MIN_SD)
+        e.set_patchmatch_iterations(ITERS)
+        e.compute_patch_match()
+        kind = "reference"
+    else:
+        crop = np.ascontiguousarray(img[top:bot])
+        Ks = [Kc] + [n[0].copy() for n in nbrs]
+        for k in Ks[1:]:
+            k[1, 2] -= top
+        O.port_compute(1, Ks, [R] + [n[1] for n in nbrs], [t] + [n[2] for n in nbrs],
+                       [crop] + [np.ascontiguousarray(n[3][top:bot]) for n in nbrs],
+                       [np.ones_like(crop)] * (1 + len(nbrs)), PATCH, mn, mx, 50, ITERS, MIN_SD, 1)
+        kind = "port"
+    dt = time.perf_counter() - t0
+    interior = (bot - top - 2 * hpz) * (W - 2 * hpz)
+    return interior, dt, kind
+
+
+def cpu_sample(work, seconds=20.0, cores=None, seed=0):
+    """Times the reference CPU path on bands of the workload, all cores.
+
+    Returns depthmaps/s (band pixels per second over the pixels of one
+    640 x 480 depthmap's interior), cores used, kind and a description.
+    """
+    vs, ranges, cands, matches = work
+    cores = cores or os.cpu_count() or 1
+    hpz = (PATCH - 1) // 2
+    H, W = vs.images[0].shape
+    rng = np.random.default_rng(seed)
+
+    def task(v, r0, rows):
+        c = vs.cameras[v]
+        nb = [(vs.cameras[o].K, vs.cameras[o].R, vs.cameras[o].t, vs.images[o]) for o in matches[v]]
+        return (c.K, c.R, c.t, vs.images[v], nb, r0, rows, ranges[v][0], ranges[v][1], hpz)
+
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        # Calibrate the per-pixel cost on one small band per worker.
+        cal_rows = 4
+        cal = pool.map(_ref_band, [task(int(rng.integers(N_VIEWS)), int(rng.integers(hpz, H - 40)),
+                                        cal_rows) for _ in range(cores)])
+        px_per_s = sum(c[0] for c in cal) / sum(c[1] for c in cal)
+        rows = int(max(2, min(H - 2 * hpz, seconds * px_per_s / (W - 2 * hpz))))
+        tasks = []
+        for k in range(cores):
+            v = int(rng.integers(N_VIEWS))
+            r0 = int(rng.integers(hpz, max(hpz + 1, H - hpz - rows)))
+            tasks.append(task(v, r0, rows))
+        t0 = time.perf_counter()
+        res = pool.map(_ref_band, tasks)
+        wall = time.perf_counter() - t0
+    pixels = sum(r[0] for r in res)
+    per_map = (W - 2 * hpz) * (H - 2 * hpz)
+    value = pixels / per_map / wall
+    kind = res[0][2]
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{cores} bands of {rows} rows x {W} px of the 24 reference views "
+                      f"({pixels} interior px, {pixels / per_map:.3f} depthmaps) in {wall:.1f} s, "
+                      f"one process per core; PatchMatch 3 iterations, 6 matching views, "
+                      f"patch 7 (reference view cropped to the band, matching views whole)"}
+
+
+# ----------------------------------------------------------------- our arm
+def build_batch(work, seed=1):
+    from opensfm_b200 import pydense
+
+    vs, ranges, cands, matches = work
+    b = pydense.Batch()
+    for c, im in zip(vs.cameras, vs.images):
+        b.add_view(c.K, c.R, c.t, im)
+    for v in range(len(vs.cameras)):
+        b.add_depthmap(v, matches[v], ranges[v][0], ranges[v][1])
+    for v in range(len(vs.cameras)):
+        b.set_clean_views(v, cands[v])
+    b.set_params(patch_size=PATCH, min_patch_sd=MIN_SD, iterations=ITERS,
+                 same_depth_threshold=0.01, min_consistent_views=3, seed=seed)
+    return b
+
+
+def run_ours(args):
+    rank, world, local = dist_env()
+    from opensfm_b200 import _lib, pydense
+    from opensfm_b200 import synthetic as S
+
+    group = Group(world, local)
+    _lib.check(_lib.load().dn_set_device(local))
+    work = make_workload()
+    vs, ranges, cands, matches = work
+    b = build_batch(work)
+    n_maps = len(vs.cameras)
+
+    # Warm-up (graph capture on the first run).
+    for _ in range(args.warmup):
+        b.run(clean=True, graph=True)
+    b.synchronize()
+
+    # Stage timings and tap counts from one instrumented run (outside the
+    # timed region): the roofline of the dominant kernel.
+    b.run(clean=True, graph=False, timing=True)
+    b.synchronize()
+    stages, taps = b.timings()
+    hp_ms = stages[1]
+    achieved = FLOPS_PER_TAP * taps[1] / (hp_ms * 1e-3) / 1e12
+    peak = pydense.fp32_peak()
+
+    # Accuracy of the plain method against ground truth (median over maps).
+    accs = []
+    for v in range(n_maps):
+        accs.append(S.accuracy(b.get_depth(v), vs.depths[v]))
+
+    # Timed region: K batched runs, device events on the batch stream.
+    with Clocks(local) as clk:
+        group.barrier()
+        b.synchronize()
+        b.timer_record(0)
+        for _ in range(args.steps):
+            b.run(clean=True, graph=True)
+        b.timer_record(1)
+        b.synchronize()
+        ms = b.timer_elapsed()
+        group.barrier()
+    ms_max = group.max(ms)
+    value = world * n_maps * args.steps / (ms_max * 1e-3)
+
+    # End to end through the public API from host buffers.
+    imgs = [np.ascontiguousarray(im) for im in vs.images]
+    out = np.zeros((H_, W_), np.float32)
+    from opensfm_b200._lib import _f, ptr
+    group.barrier()
+    b.synchronize()
+    b.timer_record(0)
+    for _ in range(args.steps):
+        for v, im in enumerate(imgs):
+            b.set_view_image(v, im)
+        b.run(clean=True, graph=True)
+        for v in range(n_maps):
+            _lib.check(b._L.dn_batch_get_depthmap(b._h, v, None, None, None, None, ptr(out, _f)))
+    b.timer_record(1)
+    b.synchronize()
+    e2e_ms = group.max(b.timer_elapsed())
+    group.barrier()
+    e2e = world * n_maps * args.steps / (e2e_ms * 1e-3)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {
+            "workload": f"ring reconstruction, {n_maps} reference views {W_}x{H_}, "
+                        f"{N_MATCH} matching views, {N_CAND} cleaner neighbours, PatchMatch "
+                        f"{ITERS} iterations (red-black), patch {PATCH}, min_patch_sd {MIN_SD}, "
+                        f"cleaner 0.01 / 3 views; plain random initialisation",
+            "init": "plain", "global_batch": n_maps * world, "parallelism": f"replicas x{world}",
+            "l2": "working set larger than L2 (views, tables and state ~%.0f MB)" % (
+                n_maps * ((W_ + 15) * (H_ + 15) * 16 + W_ * H_ * (16 + 4 + 4 + 4 + 4 + 2)) / 1e6),
+            "accuracy_1pct_median": float(np.median(accs)),
+            "stage_ms": {"init": stages[0], "halfpasses": stages[1], "post": stages[2],
+                         "clean": stages[3], "total": stages[4]},
+        },
+        "roofline": {
+            "kernel": "halfpass_kernel<3,false>", "bound": "fp32", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+            "peak_source": "measured FP32 FMA loop on this GPU (dn_fp32_peak); "
+                           "MEASURED_PEAKS.json has no FP32 figure",
+            "algorithmic": f"{FLOPS_PER_TAP} flops per NCC tap x {taps[1]} taps in "
+                           f"{2 * ITERS} half-passes ({hp_ms:.2f} ms)",
+        },
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(sum(im.nbytes for im in imgs)),
+                "d2h_bytes_per_step": int(n_maps * out.nbytes)},
+        "gpu_launches": None,
+        "clocks": {k: v for k, v in clk.summary().items()},
+    }
+    # Launch count per step: memsets are not kernels; init + 2*iters
+    # half-passes + post + one cleaner launch per map.
+    line["gpu_launches"] = args.steps * (1 + 2 * ITERS + 1 + n_maps)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_sample(work, seconds=args.cpu_seconds)
+        except Exception as e:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    group.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    import oracle as O
+
+    work = make_workload()
+    vals = []
+    info = None
+    for k in range(args.warmup + args.steps):
+        r = cpu_sample(work, seconds=args.cpu_seconds / 2, seed=k)
+        if k >= args.warmup:
+            vals.append(r["value"])
+        info = r
+    value = statistics.mean(vals)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 / value if value else None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"ring reconstruction, {N_VIEWS} reference views {W_}x{H_}, "
+                               f"{N_MATCH} matching views, PatchMatch {ITERS} iterations "
+                               f"(raster), patch {PATCH}; bands per core",
+                   "reference_code": "opensfm/src/lib/dense/src/depthmap.cc (oracle/_ref)"
+                   if O.ref_available() else "C restatement (oracle/_build)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                         "sample": info["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,220 @@
+/* dense_b200.h: C ABI of the B200 dense depthmap library (libdense_b200.so).
+ *
+ * Drop-in for the legacy pydense classes of OpenSfM's dense path
+ * (opensfm/src/lib/dense/depthmap.h:57-153, Python surface in
+ * opensfm/src/lib/dense/pydense.pyi:28-77).  Plain pointers and sizes only.
+ *
+ * Conventions
+ *  - Matrices are row-major float64: K, R are 3x3 (9 doubles), t is 3.
+ *    Cameras map world X to x_cam = R X + t, pixels q ~ K x_cam.
+ *  - Images and masks are uint8 H x W, row-major, `stride` bytes per row
+ *    (stride >= width).  View 0 of an estimator/cleaner/pruner is the
+ *    reference view, as in the reference classes.
+ *  - Outputs are caller-owned host buffers: depth f32 [H][W], plane f32
+ *    [H][W][3] (plane v with v.X + 1 = 0 in reference-camera coordinates),
+ *    score f32 [H][W], nghbr i32 [H][W].
+ *  - Inputs are copied (to device memory) by add_view; callers may free
+ *    them afterwards (depthmap.cc:156-157, 521, 571-574 copy too).
+ *  - Every call returns a dn_status; on failure dn_last_error() gives a
+ *    message (thread-local).  Nothing here aborts or traps.
+ *  - Each object owns one CUDA stream; calls on one object are serialised
+ *    by the caller, different objects may be used from different threads.
+ */
+#ifndef DENSE_B200_H_
+#define DENSE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DN_OK = 0,
+  DN_INVALID_ARG = 1,    /* bad size, shape, count or parameter value */
+  DN_OUT_OF_MEMORY = 2,  /* device or pinned allocation failed */
+  DN_DEVICE_ERROR = 3,   /* CUDA runtime error, or no usable device */
+  DN_TIMEOUT = 4,        /* a bounded device-side wait expired */
+  DN_NOT_READY = 5       /* result requested before it was computed */
+} dn_status;
+
+/* Message for the last failed call on this thread ("" if none). */
+const char* dn_last_error(void);
+/* Library version string. */
+const char* dn_version(void);
+/* Number of visible CUDA devices (0 if none). */
+int dn_device_count(void);
+/* Makes `device` current for this thread; objects created afterwards on
+ * this thread live on it. */
+dn_status dn_set_device(int device);
+
+/* ------------------------------------------------------------------------
+ * DepthmapEstimator (depthmap.h:57-111; pydense.pyi:45-60)
+ * ---------------------------------------------------------------------- */
+typedef struct dn_estimator dn_estimator;
+
+/* DepthmapEstimator::DepthmapEstimator (depthmap.cc:134-144): patch 7,
+ * 50 planes, 3 iterations, min patch sd 5. */
+dn_status dn_estimator_create(dn_estimator** out);
+dn_status dn_estimator_destroy(dn_estimator* est);
+/* DepthmapEstimator::AddView (depthmap.cc:146-162).  mask may be NULL (all
+ * valid).  The first view is the reference and sets the output size; the
+ * other views may have any size (each is sampled with its own extent, as in
+ * depthmap.cc:472). */
+dn_status dn_estimator_add_view(dn_estimator* est, const double* K, const double* R,
+                                const double* t, const uint8_t* image, const uint8_t* mask,
+                                int width, int height, int stride);
+/* SetDepthRange (depthmap.cc:164-169). */
+dn_status dn_estimator_set_depth_range(dn_estimator* est, double min_depth, double max_depth,
+                                       int num_depth_planes);
+/* SetPatchMatchIterations (depthmap.cc:171-173). */
+dn_status dn_estimator_set_patchmatch_iterations(dn_estimator* est, int n);
+/* SetPatchSize (depthmap.cc:175-178).  Supported: 3 <= size <= 12
+ * (half-size 1..5). */
+dn_status dn_estimator_set_patch_size(dn_estimator* est, int size);
+/* SetMinPatchSD (depthmap.cc:180-182): stores sd * sd. */
+dn_status dn_estimator_set_min_patch_sd(dn_estimator* est, float sd);
+/* Seed of the counter-based RNG used by PatchMatch (no counterpart: the
+ * reference seeds std::mt19937 from std::random_device). */
+dn_status dn_estimator_set_seed(dn_estimator* est, uint64_t seed);
+
+/* ComputeBruteForce (depthmap.cc:184-200). */
+dn_status dn_estimator_compute_brute_force(dn_estimator* est, float* depth, float* plane,
+                                           float* score, int32_t* nghbr);
+/* ComputePatchMatch (depthmap.cc:202-213), red-black schedule. */
+dn_status dn_estimator_compute_patch_match(dn_estimator* est, float* depth, float* plane,
+                                           float* score, int32_t* nghbr);
+/* ComputePatchMatchSample (depthmap.cc:215-227), red-black schedule. */
+dn_status dn_estimator_compute_patch_match_sample(dn_estimator* est, float* depth,
+                                                  float* plane, float* score, int32_t* nghbr);
+/* ComputePlaneScore (depthmap.cc:408-419) for every interior pixel with the
+ * caller's planes (f32 [H][W][3]); border pixels get score 0, nghbr 0. */
+dn_status dn_estimator_score_planes(dn_estimator* est, const float* planes, float* score,
+                                    int32_t* nghbr);
+/* PatchMatch from a caller-supplied initial plane field (f32 [H][W][3];
+ * planes with z == 0 fall back to the random initialisation of
+ * RandomInitialization, depthmap.cc:237-256).  Used by the learned proposal. */
+dn_status dn_estimator_compute_patch_match_init(dn_estimator* est, const float* init_planes,
+                                                float* depth, float* plane, float* score,
+                                                int32_t* nghbr);
+/* Number of NCC taps the last compute evaluated (device counter). */
+dn_status dn_estimator_last_taps(dn_estimator* est, uint64_t* taps);
+
+/* ------------------------------------------------------------------------
+ * DepthmapCleaner (depthmap.h:113-129; pydense.pyi:28-42)
+ * ---------------------------------------------------------------------- */
+typedef struct dn_cleaner dn_cleaner;
+
+/* DepthmapCleaner::DepthmapCleaner (depthmap.cc:504-505): threshold 0.01,
+ * min consistent views 2. */
+dn_status dn_cleaner_create(dn_cleaner** out);
+dn_status dn_cleaner_destroy(dn_cleaner* c);
+dn_status dn_cleaner_set_same_depth_threshold(dn_cleaner* c, float t);  /* depthmap.cc:507-509 */
+dn_status dn_cleaner_set_min_consistent_views(dn_cleaner* c, int n);    /* depthmap.cc:511-513 */
+/* DepthmapCleaner::AddView (depthmap.cc:515-522).  depth: f32, row stride
+ * in floats (>= width). */
+dn_status dn_cleaner_add_view(dn_cleaner* c, const double* K, const double* R, const double* t,
+                              const float* depth, int width, int height, int stride);
+/* DepthmapCleaner::Clean (depthmap.cc:524-555): out f32 [H][W]. */
+dn_status dn_cleaner_clean(dn_cleaner* c, float* clean_depth);
+
+/* ------------------------------------------------------------------------
+ * DepthmapPruner (depthmap.h:131-153; pydense.pyi:63-77)
+ * ---------------------------------------------------------------------- */
+typedef struct dn_pruner dn_pruner;
+
+/* DepthmapPruner::DepthmapPruner (depthmap.cc:557): threshold 0.01. */
+dn_status dn_pruner_create(dn_pruner** out);
+dn_status dn_pruner_destroy(dn_pruner* p);
+dn_status dn_pruner_set_same_depth_threshold(dn_pruner* p, float t);  /* depthmap.cc:559-561 */
+/* DepthmapPruner::AddView (depthmap.cc:563-575): depth f32 [H][W], plane
+ * f32 [H][W][3], color u8 [H][W][3], label u8 [H][W] (tightly packed). */
+dn_status dn_pruner_add_view(dn_pruner* p, const double* K, const double* R, const double* t,
+                             const float* depth, const float* plane, const uint8_t* color,
+                             const uint8_t* label, int width, int height);
+/* DepthmapPruner::Prune (depthmap.cc:577-637), first call: runs the pruner
+ * and returns the number of kept points in *count. */
+dn_status dn_pruner_prune(dn_pruner* p, int64_t* count);
+/* Second call: copies the kept points (row-major pixel order, as the
+ * reference appends them) into caller buffers sized for `capacity` points:
+ * points f32 [n][3], normals f32 [n][3], colors u8 [n][3], labels u8 [n]. */
+dn_status dn_pruner_fetch(dn_pruner* p, float* points, float* normals, uint8_t* colors,
+                          uint8_t* labels, int64_t capacity);
+
+/* ------------------------------------------------------------------------
+ * Batched reconstruction (no reference counterpart: opensfm/dense.py runs
+ * one estimator per reference view; this runs every depthmap of a
+ * reconstruction, with mixed image sizes and neighbour counts, in one
+ * persistent launch per stage, replayed from a captured CUDA graph).
+ * ---------------------------------------------------------------------- */
+typedef struct dn_batch dn_batch;
+
+dn_status dn_batch_create(dn_batch** out);
+dn_status dn_batch_destroy(dn_batch* b);
+/* Uploads one view (image copied to device as FP16).  Views may differ in
+ * size.  *view_id receives the view's index. */
+dn_status dn_batch_add_view(dn_batch* b, const double* K, const double* R, const double* t,
+                            const uint8_t* image, const uint8_t* mask, int width, int height,
+                            int stride, int* view_id);
+/* Declares one depthmap: reference view, its matching views (used for
+ * scoring, <= 16) and its depth range.  *map_id receives its index. */
+dn_status dn_batch_add_depthmap(dn_batch* b, int ref_view, const int* matching_views,
+                                int n_matching, double min_depth, double max_depth,
+                                int* map_id);
+/* Cleaner / pruner views of a depthmap (<= 16 other maps by map id); when
+ * set, dn_batch_run also cleans (and prunes) after PatchMatch. */
+dn_status dn_batch_set_clean_views(dn_batch* b, int map_id, const int* other_maps, int n);
+dn_status dn_batch_set_params(dn_batch* b, int patch_size, float min_patch_sd, int iterations,
+                              float same_depth_threshold, int min_consistent_views,
+                              uint64_t seed);
+/* Flags for dn_batch_run. */
+#define DN_RUN_CLEAN 1u  /* run the cleaner after PatchMatch */
+#define DN_RUN_PRUNE 2u  /* run the pruner after the cleaner */
+#define DN_RUN_GRAPH 4u  /* capture the run in a CUDA graph once, replay after */
+#define DN_RUN_INIT 8u   /* initialise from planes set by dn_batch_set_init */
+#define DN_RUN_TIMING 16u /* record CUDA events around each stage */
+/* Enqueues PatchMatch for every declared depthmap (and clean/prune per
+ * flags) on the batch's stream; returns without waiting. */
+dn_status dn_batch_run(dn_batch* b, unsigned flags);
+dn_status dn_batch_synchronize(dn_batch* b);
+/* Copies one depthmap's results to host buffers (after synchronize); any
+ * pointer may be NULL to skip it.  clean may be NULL. */
+dn_status dn_batch_get_depthmap(dn_batch* b, int map_id, float* depth, float* plane,
+                                float* score, int32_t* nghbr, float* clean);
+/* Initial planes (f32 [H][W][3], reference camera) for one depthmap. */
+dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes);
+/* Total kept pruner points over all maps of the last run (after sync). */
+dn_status dn_batch_pruned_count(dn_batch* b, int64_t* count);
+/* NCC taps evaluated by the last run (device counter). */
+dn_status dn_batch_last_taps(dn_batch* b, uint64_t* taps);
+/* Replaces the pixels of an uploaded view (same size), asynchronously on
+ * the batch stream; the host buffer must stay valid until the next
+ * dn_batch_synchronize. */
+dn_status dn_batch_set_view_image(dn_batch* b, int view_id, const uint8_t* image, int stride);
+/* Per-stage device times (ms) of the last run made with DN_RUN_TIMING:
+ * out[0] init, out[1] all PatchMatch half-passes, out[2] post-process,
+ * out[3] cleaner, out[4] whole run.  taps_out (may be NULL) receives the
+ * NCC taps of init (taps_out[0]) and of the half-passes (taps_out[1]). */
+dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_out);
+/* Device timer on the batch stream: record event `slot` (0 or 1), and the
+ * elapsed ms between the two recorded events (after dn_batch_synchronize). */
+dn_status dn_batch_timer_record(dn_batch* b, int slot);
+dn_status dn_batch_timer_elapsed(dn_batch* b, float* ms);
+/* Copies one depthmap's final depth to a device buffer (no host copy). */
+dn_status dn_batch_copy_depth_device(dn_batch* b, int map_id, float* d_out);
+
+/* ------------------------------------------------------------------------
+ * Utilities (no reference counterpart)
+ * ---------------------------------------------------------------------- */
+/* PostProcess (depthmap.cc:489-502) on a host depth map: 5x5 median with
+ * replicated borders, then zero where |d - median| / d > 0.05 or d == 0. */
+dn_status dn_postprocess_depth(const float* depth, float* out, int width, int height);
+/* Measures the device's FP32 FMA throughput (TFLOP/s, FMA = 2 flops) with a
+ * register-resident FMA loop on every SM; used as the scoring roofline. */
+dn_status dn_fp32_peak(double* tflops, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DENSE_B200_H_ */

@@ -1,0 +1,55 @@
+"""Builds the sm_100a dense library (libdense_b200.so) in-tree with nvcc.
+
+The library is the product's only compute path; it is compiled for
+sm_100a (B200) and loaded through ctypes by ``opensfm_b200._lib``.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "_build", "libdense_b200.so")
+SOURCES = ["kernels.cu", "cleanprune.cu", "api.cu"]
+HEADERS = ["common.cuh", "kernels.h"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
+         "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
+    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [
+        os.path.join(ROOT, "include", "dense_b200.h")]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    objs = []
+    for s in srcs:
+        o = os.path.join(os.path.dirname(LIB), os.path.basename(s) + ".o")
+        cmd = [NVCC, *ARCH, *FLAGS, "-dc" if False else "-c", s, "-o", o]
+        if ptxas_v:
+            cmd += ["-Xptxas", "-v"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.check_call(cmd)
+        objs.append(o)
+    cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    subprocess.check_call(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, ptxas_v="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,1212 @@
+// Host engine and C ABI (include/dense_b200.h) of the dense depthmap library.
+//
+// One Engine holds a reconstruction's views (uploaded once, FP16 image +
+// bilinear coefficient table per view) and its depthmaps (reference view,
+// matching views, depth range, per-map state).  The legacy single-depthmap
+// classes (DepthmapEstimator / Cleaner / Pruner, reference
+// opensfm/src/lib/dense/depthmap.h:57-153) are thin wrappers over it.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dense_b200.h"
+#include "kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+dn_status fail(dn_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+dn_status cuda_fail(cudaError_t e, const char* what) {
+  const dn_status s = (e == cudaErrorMemoryAllocation) ? DN_OUT_OF_MEMORY : DN_DEVICE_ERROR;
+  return fail(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define DN_CUDA(expr)                                        \
+  do {                                                       \
+    cudaError_t e_ = (expr);                                 \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #expr);      \
+  } while (0)
+
+#define DN_CHECK(cond, msg)                                  \
+  do {                                                       \
+    if (!(cond)) return fail(DN_INVALID_ARG, msg);           \
+  } while (0)
+
+#define DN_TRY(expr)                                         \
+  do {                                                       \
+    dn_status s_ = (expr);                                   \
+    if (s_ != DN_OK) return s_;                              \
+  } while (0)
+
+// Device buffer owned by the host object.
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    else p = nullptr;
+    return e;
+  }
+};
+
+// ---------------------------------------------------------------- FP64 math
+// 3x3 helpers in the evaluation order of cv::Matx (products accumulate from
+// zero in index order); the inverse is the cofactor form scaled by 1/det.
+void m3_mul(const double* a, const double* b, double* c) {
+  double r[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += a[3 * i + k] * b[3 * k + j];
+      r[3 * i + j] = s;
+    }
+  std::memcpy(c, r, sizeof(r));
+}
+void m3_vec(const double* a, const double* x, double* y) {
+  double r[3];
+  for (int i = 0; i < 3; ++i) {
+    double s = 0.0;
+    for (int k = 0; k < 3; ++k) s += a[3 * i + k] * x[k];
+    r[i] = s;
+  }
+  std::memcpy(y, r, sizeof(r));
+}
+void m3_t(const double* a, double* b) {
+  double r[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r[3 * j + i] = a[3 * i + j];
+  std::memcpy(b, r, sizeof(r));
+}
+bool m3_inv(const double* a, double* r) {
+  auto A = [&](int i, int j) { return a[3 * i + j]; };
+  double d = A(0, 0) * (A(1, 1) * A(2, 2) - A(2, 1) * A(1, 2)) -
+             A(0, 1) * (A(1, 0) * A(2, 2) - A(2, 0) * A(1, 2)) +
+             A(0, 2) * (A(1, 0) * A(2, 1) - A(2, 0) * A(1, 1));
+  if (d == 0 || !std::isfinite(d)) return false;
+  d = 1 / d;
+  r[0] = (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) * d;
+  r[1] = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) * d;
+  r[2] = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) * d;
+  r[3] = (A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2)) * d;
+  r[4] = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) * d;
+  r[5] = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) * d;
+  r[6] = (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0)) * d;
+  r[7] = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) * d;
+  r[8] = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) * d;
+  return true;
+}
+bool all_finite(const double* a, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!std::isfinite(a[i])) return false;
+  return true;
+}
+
+struct Camera {
+  double K[9], R[9], t[3];
+};
+
+dn_status check_camera(const double* K, const double* R, const double* t) {
+  DN_CHECK(K && R && t, "K, R and t must not be NULL");
+  DN_CHECK(all_finite(K, 9) && all_finite(R, 9) && all_finite(t, 3),
+           "camera K, R, t must be finite");
+  double Ki[9];
+  DN_CHECK(m3_inv(K, Ki), "camera K is singular");
+  return DN_OK;
+}
+
+// ---------------------------------------------------------------- engine
+struct View {
+  Camera cam;
+  int W = 0, H = 0;
+  float cbias = 0.f;
+  DevBuf<__half> img;
+  DevBuf<uint8_t> mask;
+  DevBuf<float4> quad;
+  DevBuf<uint8_t> gray;  // u8 copy (pruner colour when none is given)
+};
+
+struct Map {
+  int ref = 0;
+  std::vector<int> nbrs;  // view ids
+  double min_d = 0, max_d = 0;
+  std::vector<int> clean_maps;
+  DevBuf<float4> state;
+  DevBuf<float> score, depth, clean, init, plane_out;
+  DevBuf<int> nghbr;
+  bool has_init = false;
+};
+
+enum class Mode { kBruteForce, kPatchMatch, kPatchMatchSample, kScorePlanes };
+
+struct Engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<std::unique_ptr<View>> views;
+  std::vector<std::unique_ptr<Map>> maps;
+  int patch = 7;
+  float min_var = 25.f;
+  int iterations = 3;
+  int num_planes = 50;
+  uint64_t seed = 0x5EEDBA5Eull;
+  float same_depth_thr = 0.01f;
+  int min_consistent = 2;
+  int bx = 32, by = 4;  // thread block shape
+  DevBuf<dn::ViewDev> d_views;
+  DevBuf<dn::PairDev> d_pairs;
+  DevBuf<dn::MapDev> d_maps;
+  DevBuf<int4> d_tiles1, d_tiles2;
+  int n_tiles1 = 0, n_tiles2 = 0;
+  DevBuf<unsigned long long> d_taps;
+  DevBuf<int> d_error;
+  DevBuf<dn::CleanView> d_clean_views;
+  DevBuf<int> d_clean_lists;
+  bool dirty = true;
+  bool computed = false;
+  cudaGraphExec_t graph = nullptr;
+  unsigned graph_flags = 0;
+  Mode graph_mode = Mode::kPatchMatch;
+  static constexpr int kEvents = 7;  // run start, init, half-passes, post, clean, timer x2
+  cudaEvent_t ev[kEvents] = {};
+  bool timed = false;
+
+  ~Engine() {
+    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  dn_status init() {
+    DN_CUDA(cudaGetDevice(&device));
+    DN_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    DN_CUDA(d_taps.alloc(4));
+    DN_CUDA(d_error.alloc(1));
+    for (auto& e : ev) DN_CUDA(cudaEventCreate(&e));
+    return DN_OK;
+  }
+
+  dn_status mark(int k, bool on) {
+    if (on) DN_CUDA(cudaEventRecord(ev[k], stream));
+    return DN_OK;
+  }
+
+  void invalidate() {
+    dirty = true;
+    computed = false;
+    if (graph) {
+      cudaGraphExecDestroy(graph);
+      graph = nullptr;
+    }
+  }
+
+  dn_status add_view(const double* K, const double* R, const double* t, const uint8_t* image,
+                     const uint8_t* mask, int W, int H, int stride, int* id) {
+    DN_TRY(check_camera(K, R, t));
+    DN_CHECK(image, "image must not be NULL");
+    DN_CHECK(W >= 2 && H >= 2 && W <= 16384 && H <= 16384, "image size must be 2..16384");
+    if (stride <= 0) stride = W;
+    DN_CHECK(stride >= W, "stride must be >= width");
+    DN_CUDA(cudaSetDevice(device));
+    auto v = std::make_unique<View>();
+    std::memcpy(v->cam.K, K, sizeof(v->cam.K));
+    std::memcpy(v->cam.R, R, sizeof(v->cam.R));
+    std::memcpy(v->cam.t, t, sizeof(v->cam.t));
+    v->W = W;
+    v->H = H;
+    // Centring constant: the rounded mean intensity (an integer, so the
+    // coefficient table stays exact).
+    double sum = 0;
+    for (int y = 0; y < H; ++y)
+      for (int x = 0; x < W; ++x) sum += image[(size_t)y * stride + x];
+    v->cbias = (float)std::floor(sum / ((double)W * H) + 0.5);
+    const int TW = W - 1 + 2 * dn::kPad, TH = H - 1 + 2 * dn::kPad;
+    DN_CUDA(v->img.alloc((size_t)W * H));
+    DN_CUDA(v->quad.alloc((size_t)TW * TH));
+    DN_CUDA(v->gray.alloc((size_t)W * H));
+    DN_CUDA(cudaMemcpy2DAsync(v->gray.p, W, image, stride, W, H, cudaMemcpyHostToDevice, stream));
+    if (mask) {
+      DN_CUDA(v->mask.alloc((size_t)W * H));
+      DN_CUDA(cudaMemcpy2DAsync(v->mask.p, W, mask, stride, W, H, cudaMemcpyHostToDevice, stream));
+    }
+    DN_CUDA(dn::launch_prepare_view(v->gray.p, W, H, W, v->img.p, v->quad.p, TW, TH, v->cbias,
+                                    stream));
+    DN_CUDA(cudaStreamSynchronize(stream));
+    if (id) *id = (int)views.size();
+    views.push_back(std::move(v));
+    invalidate();
+    return DN_OK;
+  }
+
+  dn_status add_map(int ref, const int* nbrs, int n, double min_d, double max_d, int* id) {
+    DN_CHECK(ref >= 0 && ref < (int)views.size(), "reference view id out of range");
+    DN_CHECK(n >= 1 && n <= dn::kMaxNbr, "a depthmap needs 1..16 matching views");
+    auto m = std::make_unique<Map>();
+    m->ref = ref;
+    for (int k = 0; k < n; ++k) {
+      DN_CHECK(nbrs[k] >= 0 && nbrs[k] < (int)views.size(), "matching view id out of range");
+      m->nbrs.push_back(nbrs[k]);
+    }
+    m->min_d = min_d;
+    m->max_d = max_d;
+    if (id) *id = (int)maps.size();
+    maps.push_back(std::move(m));
+    invalidate();
+    return DN_OK;
+  }
+
+  dn_status check_params(Mode mode) {
+    DN_CHECK(!maps.empty(), "no depthmap declared (add at least two views)");
+    const int hpz = (patch - 1) / 2;
+    DN_CHECK(hpz >= 1 && hpz <= dn::kMaxHpz, "patch size must be in 3..12");
+    for (auto& m : maps) {
+      const View& r = *views[m->ref];
+      DN_CHECK(r.W > 2 * hpz && r.H > 2 * hpz, "image smaller than the patch");
+      if (mode == Mode::kBruteForce) {
+        DN_CHECK(num_planes >= 2, "brute force needs at least 2 depth planes");
+        DN_CHECK(m->min_d > 0 && m->max_d > 0 && std::isfinite(m->min_d) && std::isfinite(m->max_d),
+                 "depth range must be positive and finite");
+      }
+      if (mode == Mode::kPatchMatch || mode == Mode::kPatchMatchSample) {
+        DN_CHECK(m->min_d > 0 && m->max_d > 0 && std::isfinite(m->min_d) && std::isfinite(m->max_d),
+                 "depth range must be positive and finite");
+        DN_CHECK(iterations >= 0 && iterations <= 1000, "iterations must be 0..1000");
+      }
+    }
+    return DN_OK;
+  }
+
+  // Builds the per-pair homography factors (FP64) and the device tables.
+  dn_status prepare() {
+    if (!dirty) return DN_OK;
+    DN_CUDA(cudaSetDevice(device));
+    std::vector<dn::ViewDev> hv(views.size());
+    for (size_t k = 0; k < views.size(); ++k) {
+      const View& v = *views[k];
+      dn::ViewDev d{};
+      d.img = v.img.p;
+      d.mask = v.mask.p;
+      d.quad = v.quad.p;
+      d.W = v.W;
+      d.H = v.H;
+      d.TW = v.W - 1 + 2 * dn::kPad;
+      d.TH = v.H - 1 + 2 * dn::kPad;
+      d.cbias = v.cbias;
+      hv[k] = d;
+    }
+    std::vector<dn::PairDev> hp;
+    std::vector<dn::MapDev> hm(maps.size());
+    std::vector<int4> t1, t2;
+    for (size_t mi = 0; mi < maps.size(); ++mi) {
+      Map& m = *maps[mi];
+      const View& r = *views[m.ref];
+      const size_t npx = (size_t)r.W * r.H;
+      DN_CUDA(m.state.alloc(npx));
+      DN_CUDA(m.score.alloc(npx));
+      DN_CUDA(m.depth.alloc(npx));
+      DN_CUDA(m.nghbr.alloc(npx));
+      double Kinv[9], R0t[9];
+      m3_inv(r.cam.K, Kinv);
+      m3_t(r.cam.R, R0t);
+      dn::MapDev d{};
+      d.ref_view = m.ref;
+      d.W = r.W;
+      d.H = r.H;
+      d.n_pairs = (int)m.nbrs.size();
+      d.pair0 = (int)hp.size();
+      for (int k = 0; k < 9; ++k) {
+        d.Kinv[k] = (float)Kinv[k];
+        d.Kinv_d[k] = Kinv[k];
+        d.K[k] = r.cam.K[k];
+        d.R[k] = r.cam.R[k];
+      }
+      for (int k = 0; k < 3; ++k) d.t[k] = r.cam.t[k];
+      d.log_min = (float)std::log(m.min_d);
+      d.log_max = (float)std::log(m.max_d);
+      d.min_depth = m.min_d;
+      d.max_depth = m.max_d;
+      d.state = m.state.p;
+      d.score = m.score.p;
+      d.nghbr = m.nghbr.p;
+      d.depth = m.depth.p;
+      d.clean = m.clean.p;
+      d.init = m.has_init ? m.init.p : nullptr;
+      for (int o : m.nbrs) {
+        const View& ov = *views[o];
+        // Q = R_o R_0^T, a = Q t_0 - t_o (depthmap.cc:152-155);
+        // H(v) = K_o (Q + a v^T) K_0^-1 = G + e f^T, G = K_o Q K_0^-1,
+        // e = K_o a, f = K_0^-T v.
+        double Q[9], qt[3], a[3], G[9], T[9], e[3];
+        m3_mul(ov.cam.R, R0t, Q);
+        m3_vec(Q, r.cam.t, qt);
+        for (int k = 0; k < 3; ++k) a[k] = qt[k] - ov.cam.t[k];
+        m3_mul(ov.cam.K, Q, T);
+        m3_mul(T, Kinv, G);
+        m3_vec(ov.cam.K, a, e);
+        dn::PairDev p{};
+        for (int k = 0; k < 9; ++k) p.G[k] = (float)G[k];
+        for (int k = 0; k < 3; ++k) p.e[k] = (float)e[k];
+        p.view = o;
+        hp.push_back(p);
+      }
+      hm[mi] = d;
+      const int tx1 = (r.W + bx - 1) / bx, ty1 = (r.H + by - 1) / by;
+      const int tx2 = (r.W + 2 * bx - 1) / (2 * bx);
+      for (int y = 0; y < ty1; ++y) {
+        for (int x = 0; x < tx1; ++x) t1.push_back(make_int4((int)mi, x, y, 0));
+        for (int x = 0; x < tx2; ++x) t2.push_back(make_int4((int)mi, x, y, 0));
+      }
+    }
+    DN_CUDA(d_views.alloc(std::max<size_t>(hv.size(), 1)));
+    DN_CUDA(d_pairs.alloc(std::max<size_t>(hp.size(), 1)));
+    DN_CUDA(d_maps.alloc(std::max<size_t>(hm.size(), 1)));
+    DN_CUDA(d_tiles1.alloc(std::max<size_t>(t1.size(), 1)));
+    DN_CUDA(d_tiles2.alloc(std::max<size_t>(t2.size(), 1)));
+    DN_CUDA(cudaMemcpyAsync(d_views.p, hv.data(), hv.size() * sizeof(dn::ViewDev),
+                            cudaMemcpyHostToDevice, stream));
+    if (!hp.empty())
+      DN_CUDA(cudaMemcpyAsync(d_pairs.p, hp.data(), hp.size() * sizeof(dn::PairDev),
+                              cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaMemcpyAsync(d_maps.p, hm.data(), hm.size() * sizeof(dn::MapDev),
+                            cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaMemcpyAsync(d_tiles1.p, t1.data(), t1.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaMemcpyAsync(d_tiles2.p, t2.data(), t2.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaStreamSynchronize(stream));
+    n_tiles1 = (int)t1.size();
+    n_tiles2 = (int)t2.size();
+    dirty = false;
+    return DN_OK;
+  }
+
+  dn::LaunchArgs args(bool halfpass) const {
+    dn::LaunchArgs a{};
+    a.maps = d_maps.p;
+    a.views = d_views.p;
+    a.pairs = d_pairs.p;
+    a.tiles = halfpass ? d_tiles2.p : d_tiles1.p;
+    a.n_tiles = halfpass ? n_tiles2 : n_tiles1;
+    a.bx = bx;
+    a.by = by;
+    a.p.hpz = (patch - 1) / 2;
+    a.p.min_var = min_var;
+    a.p.seed_lo = (uint32_t)seed;
+    a.p.seed_hi = (uint32_t)(seed >> 32);
+    a.p.num_planes = num_planes;
+    a.p.same_depth_thr = same_depth_thr;
+    a.p.min_consistent = min_consistent;
+    a.p.taps = d_taps.p;
+    a.p.error = d_error.p;
+    return a;
+  }
+
+  // Enqueues the whole computation for every map on `stream`.
+  dn_status enqueue(Mode mode, bool timing = false) {
+    for (auto& m : maps) {
+      const View& r = *views[m->ref];
+      const size_t npx = (size_t)r.W * r.H;
+      if (mode != Mode::kScorePlanes) {
+        DN_CUDA(cudaMemsetAsync(m->state.p, 0, npx * sizeof(float4), stream));
+        DN_CUDA(cudaMemsetAsync(m->score.p, 0, npx * sizeof(float), stream));
+        DN_CUDA(cudaMemsetAsync(m->nghbr.p, 0, npx * sizeof(int), stream));
+      }
+    }
+    DN_CUDA(cudaMemsetAsync(d_taps.p, 0, 4 * sizeof(unsigned long long), stream));
+    DN_CUDA(cudaMemsetAsync(d_error.p, 0, sizeof(int), stream));
+    DN_TRY(mark(0, timing));
+    dn::LaunchArgs a1 = args(false);
+    if (mode == Mode::kScorePlanes) {
+      DN_CUDA(dn::launch_stage(dn::Stage::kScorePlanes, false, a1, stream));
+      return DN_OK;
+    }
+    if (mode == Mode::kBruteForce) {
+      DN_CUDA(dn::launch_stage(dn::Stage::kBruteForce, false, a1, stream));
+      a1.flag = 0;
+      DN_CUDA(dn::launch_stage(dn::Stage::kPostProcess, false, a1, stream));
+      return DN_OK;
+    }
+    const bool sample = (mode == Mode::kPatchMatchSample);
+    DN_CUDA(dn::launch_stage(dn::Stage::kInit, sample, a1, stream));
+    DN_TRY(mark(1, timing));
+    dn::LaunchArgs a2 = args(true);
+    a2.p.taps = d_taps.p + 1;
+    for (int it = 0; it < iterations; ++it) {
+      for (int c = 0; c < 2; ++c) {
+        a2.p.colour = c;
+        a2.p.pass = 2 * it + c;
+        DN_CUDA(dn::launch_stage(dn::Stage::kHalfPass, sample, a2, stream));
+      }
+    }
+    DN_TRY(mark(2, timing));
+    a1.flag = 1;
+    DN_CUDA(dn::launch_stage(dn::Stage::kPostProcess, false, a1, stream));
+    DN_TRY(mark(3, timing));
+    DN_TRY(mark(4, timing));
+    return DN_OK;
+  }
+
+  // Uploads the cleaner tables (outside any stream capture): one CleanView
+  // per map (its final depth with its reference camera) and per map the
+  // list of other maps it is checked against.
+  std::vector<int> clean_offs;
+  dn_status prepare_clean() {
+    std::vector<dn::CleanView> cv(maps.size());
+    std::vector<int> lists;
+    clean_offs.clear();
+    for (size_t k = 0; k < maps.size(); ++k) {
+      Map& m = *maps[k];
+      const View& r = *views[m.ref];
+      DN_CUDA(m.clean.alloc((size_t)r.W * r.H));
+      dn::CleanView c{};
+      c.depth = m.depth.p;
+      c.W = r.W;
+      c.H = r.H;
+      c.stride = r.W;
+      std::memcpy(c.K, r.cam.K, sizeof(c.K));
+      std::memcpy(c.R, r.cam.R, sizeof(c.R));
+      std::memcpy(c.t, r.cam.t, sizeof(c.t));
+      cv[k] = c;
+      clean_offs.push_back((int)lists.size());
+      for (int o : m.clean_maps) lists.push_back(o);
+    }
+    DN_CUDA(d_clean_views.alloc(std::max<size_t>(cv.size(), 1)));
+    DN_CUDA(d_clean_lists.alloc(std::max<size_t>(lists.size(), 1)));
+    DN_CUDA(cudaMemcpyAsync(d_clean_views.p, cv.data(), cv.size() * sizeof(dn::CleanView),
+                            cudaMemcpyHostToDevice, stream));
+    if (!lists.empty())
+      DN_CUDA(cudaMemcpyAsync(d_clean_lists.p, lists.data(), lists.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaStreamSynchronize(stream));
+    return DN_OK;
+  }
+
+  dn_status enqueue_clean(bool timing = false) {
+    for (size_t k = 0; k < maps.size(); ++k) {
+      Map& m = *maps[k];
+      const View& r = *views[m.ref];
+      DN_CUDA(dn::launch_clean(d_clean_views.p, (int)k, d_clean_lists.p + clean_offs[k],
+                               (int)m.clean_maps.size(), r.W, r.H, same_depth_thr,
+                               min_consistent, m.clean.p, stream));
+    }
+    DN_TRY(mark(4, timing));
+    return DN_OK;
+  }
+
+  dn_status set_view_image(int v, const uint8_t* image, int stride) {
+    DN_CHECK(v >= 0 && v < (int)views.size(), "view id out of range");
+    DN_CHECK(image, "image must not be NULL");
+    View& w = *views[v];
+    if (stride <= 0) stride = w.W;
+    DN_CHECK(stride >= w.W, "stride must be >= width");
+    DN_CUDA(cudaSetDevice(device));
+    const int TW = w.W - 1 + 2 * dn::kPad, TH = w.H - 1 + 2 * dn::kPad;
+    DN_CUDA(cudaMemcpy2DAsync(w.gray.p, w.W, image, stride, w.W, w.H, cudaMemcpyHostToDevice, stream));
+    DN_CUDA(dn::launch_prepare_view(w.gray.p, w.W, w.H, w.W, w.img.p, w.quad.p, TW, TH, w.cbias,
+                                    stream));
+    return DN_OK;
+  }
+
+  dn_status timings(float* out, int n, uint64_t* taps_out) {
+    DN_CHECK(out || n == 0, "NULL output");
+    DN_CHECK(timed, "the last run was not made with DN_RUN_TIMING");
+    DN_CUDA(cudaSetDevice(device));
+    DN_CUDA(cudaStreamSynchronize(stream));
+    float t[5] = {0, 0, 0, 0, 0};
+    DN_CUDA(cudaEventElapsedTime(&t[0], ev[0], ev[1]));
+    DN_CUDA(cudaEventElapsedTime(&t[1], ev[1], ev[2]));
+    DN_CUDA(cudaEventElapsedTime(&t[2], ev[2], ev[3]));
+    DN_CUDA(cudaEventElapsedTime(&t[3], ev[3], ev[4]));
+    DN_CUDA(cudaEventElapsedTime(&t[4], ev[0], ev[4]));
+    for (int k = 0; k < n && k < 5; ++k) out[k] = t[k];
+    if (taps_out) {
+      unsigned long long v[4];
+      DN_CUDA(cudaMemcpy(v, d_taps.p, sizeof(v), cudaMemcpyDeviceToHost));
+      taps_out[0] = v[0];
+      taps_out[1] = v[1];
+    }
+    return DN_OK;
+  }
+
+  dn_status finish() {
+    DN_CUDA(cudaStreamSynchronize(stream));
+    int err = 0;
+    DN_CUDA(cudaMemcpy(&err, d_error.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return fail(DN_TIMEOUT, "a bounded device-side wait expired");
+    computed = true;
+    return DN_OK;
+  }
+
+  dn_status compute(Mode mode) {
+    DN_CUDA(cudaSetDevice(device));
+    DN_TRY(check_params(mode));
+    DN_TRY(prepare());
+    DN_TRY(enqueue(mode));
+    return finish();
+  }
+
+  dn_status fetch(int map, float* depth, float* plane, float* score, int32_t* nghbr,
+                  float* clean) {
+    DN_CHECK(map >= 0 && map < (int)maps.size(), "depthmap id out of range");
+    DN_CHECK(computed, "no result computed yet");
+    DN_CUDA(cudaSetDevice(device));
+    Map& m = *maps[map];
+    const View& r = *views[m.ref];
+    const size_t npx = (size_t)r.W * r.H;
+    if (depth)
+      DN_CUDA(cudaMemcpyAsync(depth, m.depth.p, npx * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (plane) {
+      DN_CUDA(m.plane_out.alloc(3 * npx));
+      DN_CUDA(dn::launch_pack(d_maps.p, map, m.plane_out.p, npx, stream));
+      DN_CUDA(cudaMemcpyAsync(plane, m.plane_out.p, 3 * npx * sizeof(float),
+                              cudaMemcpyDeviceToHost, stream));
+    }
+    if (score)
+      DN_CUDA(cudaMemcpyAsync(score, m.score.p, npx * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (nghbr)
+      DN_CUDA(cudaMemcpyAsync(nghbr, m.nghbr.p, npx * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    if (clean) {
+      DN_CHECK(m.clean.p, "the depthmap was not cleaned");
+      DN_CUDA(cudaMemcpyAsync(clean, m.clean.p, npx * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    }
+    DN_CUDA(cudaStreamSynchronize(stream));
+    return DN_OK;
+  }
+
+  dn_status set_init(int map, const float* planes) {
+    DN_CHECK(map >= 0 && map < (int)maps.size(), "depthmap id out of range");
+    Map& m = *maps[map];
+    const View& r = *views[m.ref];
+    const size_t npx = (size_t)r.W * r.H;
+    DN_CUDA(cudaSetDevice(device));
+    if (!planes) {
+      m.has_init = false;
+      invalidate();
+      return DN_OK;
+    }
+    const bool had = m.has_init;
+    DN_CUDA(m.init.alloc(3 * npx));
+    DN_CUDA(cudaMemcpyAsync(m.init.p, planes, 3 * npx * sizeof(float), cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaStreamSynchronize(stream));
+    m.has_init = true;
+    if (!had) invalidate();
+    return DN_OK;
+  }
+
+  dn_status taps(uint64_t* out) {
+    DN_CHECK(out, "NULL output");
+    DN_CUDA(cudaSetDevice(device));
+    unsigned long long v[4] = {0, 0, 0, 0};
+    DN_CUDA(cudaMemcpy(v, d_taps.p, sizeof(v), cudaMemcpyDeviceToHost));
+    *out = v[0] + v[1] + v[2] + v[3];
+    return DN_OK;
+  }
+};
+
+}  // namespace
+
+// ======================================================================
+// C ABI
+
+struct dn_estimator {
+  Engine eng;
+  int W = 0, H = 0;
+  double min_d = 0, max_d = 0;
+};
+
+struct dn_cleaner {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  float thr = 0.01f;
+  int min_views = 2;
+  std::vector<dn::CleanView> views;
+  std::vector<DevBuf<float>> depths;
+  DevBuf<dn::CleanView> d_views;
+  DevBuf<int> d_others;
+  DevBuf<float> d_out;
+  ~dn_cleaner() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+struct dn_pruner {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  float thr = 0.01f;
+  std::vector<dn::PruneView> views;
+  std::vector<DevBuf<float>> depths, planes;
+  std::vector<DevBuf<uint8_t>> colors, labels;
+  DevBuf<dn::PruneView> d_views;
+  DevBuf<uint8_t> scratch;
+  DevBuf<float> points, normals;
+  DevBuf<uint8_t> out_colors, out_labels;
+  DevBuf<unsigned long long> d_count;
+  int64_t count = -1;
+  ~dn_pruner() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+struct dn_batch {
+  Engine eng;
+  bool ran = false;
+};
+
+extern "C" {
+
+const char* dn_last_error(void) { return g_last_error.c_str(); }
+const char* dn_version(void) { return "opensfm_b200 dense 0.1 (sm_100a)"; }
+int dn_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+dn_status dn_set_device(int device) {
+  DN_CHECK(device >= 0 && device < dn_device_count(), "device index out of range");
+  DN_CUDA(cudaSetDevice(device));
+  return DN_OK;
+}
+
+static dn_status need_device() {
+  if (dn_device_count() <= 0) return fail(DN_DEVICE_ERROR, "no CUDA device available");
+  return DN_OK;
+}
+
+// ------------------------------------------------------------- estimator
+dn_status dn_estimator_create(dn_estimator** out) {
+  DN_CHECK(out, "NULL output");
+  *out = nullptr;
+  DN_TRY(need_device());
+  auto e = std::make_unique<dn_estimator>();
+  DN_TRY(e->eng.init());
+  *out = e.release();
+  return DN_OK;
+}
+
+dn_status dn_estimator_destroy(dn_estimator* est) {
+  delete est;
+  return DN_OK;
+}
+
+dn_status dn_estimator_add_view(dn_estimator* est, const double* K, const double* R,
+                                const double* t, const uint8_t* image, const uint8_t* mask,
+                                int width, int height, int stride) {
+  DN_CHECK(est, "NULL estimator");
+  DN_CHECK((int)est->eng.views.size() <= dn::kMaxNbr, "at most 17 views (reference + 16)");
+  int id;
+  DN_TRY(est->eng.add_view(K, R, t, image, mask, width, height, stride, &id));
+  if (id == 0) {
+    est->W = width;
+    est->H = height;
+  }
+  // One depthmap: view 0 against every other view.
+  est->eng.maps.clear();
+  if (est->eng.views.size() >= 2) {
+    std::vector<int> nb;
+    for (int k = 1; k < (int)est->eng.views.size(); ++k) nb.push_back(k);
+    DN_TRY(est->eng.add_map(0, nb.data(), (int)nb.size(), est->min_d, est->max_d, nullptr));
+  }
+  return DN_OK;
+}
+
+dn_status dn_estimator_set_depth_range(dn_estimator* est, double mn, double mx, int n) {
+  DN_CHECK(est, "NULL estimator");
+  est->min_d = mn;
+  est->max_d = mx;
+  est->eng.num_planes = n;
+  for (auto& m : est->eng.maps) {
+    m->min_d = mn;
+    m->max_d = mx;
+  }
+  est->eng.invalidate();
+  return DN_OK;
+}
+
+dn_status dn_estimator_set_patchmatch_iterations(dn_estimator* est, int n) {
+  DN_CHECK(est, "NULL estimator");
+  est->eng.iterations = n;
+  return DN_OK;
+}
+
+dn_status dn_estimator_set_patch_size(dn_estimator* est, int size) {
+  DN_CHECK(est, "NULL estimator");
+  const int hpz = (size - 1) / 2;
+  DN_CHECK(hpz >= 1 && hpz <= dn::kMaxHpz, "patch size must be in 3..12");
+  est->eng.patch = size;
+  return DN_OK;
+}
+
+dn_status dn_estimator_set_min_patch_sd(dn_estimator* est, float sd) {
+  DN_CHECK(est, "NULL estimator");
+  est->eng.min_var = sd * sd;
+  return DN_OK;
+}
+
+dn_status dn_estimator_set_seed(dn_estimator* est, uint64_t seed) {
+  DN_CHECK(est, "NULL estimator");
+  est->eng.seed = seed;
+  return DN_OK;
+}
+
+static dn_status est_compute(dn_estimator* est, Mode mode, float* depth, float* plane,
+                             float* score, int32_t* nghbr) {
+  DN_CHECK(est, "NULL estimator");
+  DN_CHECK(est->eng.views.size() >= 2, "DepthmapEstimator needs a reference and at least one other view");
+  DN_CHECK(depth && plane && score && nghbr, "output buffers must not be NULL");
+  DN_TRY(est->eng.compute(mode));
+  return est->eng.fetch(0, depth, plane, score, nghbr, nullptr);
+}
+
+dn_status dn_estimator_compute_brute_force(dn_estimator* est, float* depth, float* plane,
+                                           float* score, int32_t* nghbr) {
+  if (est && est->eng.maps.size() == 1 && est->eng.maps[0]->has_init) est->eng.set_init(0, nullptr);
+  return est_compute(est, Mode::kBruteForce, depth, plane, score, nghbr);
+}
+
+dn_status dn_estimator_compute_patch_match(dn_estimator* est, float* depth, float* plane,
+                                           float* score, int32_t* nghbr) {
+  if (est && est->eng.maps.size() == 1 && est->eng.maps[0]->has_init) est->eng.set_init(0, nullptr);
+  return est_compute(est, Mode::kPatchMatch, depth, plane, score, nghbr);
+}
+
+dn_status dn_estimator_compute_patch_match_sample(dn_estimator* est, float* depth,
+                                                  float* plane, float* score, int32_t* nghbr) {
+  if (est && est->eng.maps.size() == 1 && est->eng.maps[0]->has_init) est->eng.set_init(0, nullptr);
+  return est_compute(est, Mode::kPatchMatchSample, depth, plane, score, nghbr);
+}
+
+dn_status dn_estimator_compute_patch_match_init(dn_estimator* est, const float* init_planes,
+                                                float* depth, float* plane, float* score,
+                                                int32_t* nghbr) {
+  DN_CHECK(est, "NULL estimator");
+  DN_CHECK(init_planes, "init planes must not be NULL");
+  DN_CHECK(est->eng.maps.size() == 1, "DepthmapEstimator needs a reference and at least one other view");
+  DN_TRY(est->eng.set_init(0, init_planes));
+  return est_compute(est, Mode::kPatchMatch, depth, plane, score, nghbr);
+}
+
+dn_status dn_estimator_score_planes(dn_estimator* est, const float* planes, float* score,
+                                    int32_t* nghbr) {
+  DN_CHECK(est, "NULL estimator");
+  DN_CHECK(planes && score && nghbr, "buffers must not be NULL");
+  DN_CHECK(est->eng.views.size() >= 2, "DepthmapEstimator needs a reference and at least one other view");
+  DN_TRY(est->eng.set_init(0, planes));
+  DN_TRY(est->eng.compute(Mode::kScorePlanes));
+  dn_status s = est->eng.fetch(0, nullptr, nullptr, score, nghbr, nullptr);
+  est->eng.set_init(0, nullptr);
+  return s;
+}
+
+dn_status dn_estimator_last_taps(dn_estimator* est, uint64_t* taps) {
+  DN_CHECK(est, "NULL estimator");
+  return est->eng.taps(taps);
+}
+
+// ---------------------------------------------------------------- cleaner
+dn_status dn_cleaner_create(dn_cleaner** out) {
+  DN_CHECK(out, "NULL output");
+  *out = nullptr;
+  DN_TRY(need_device());
+  auto c = std::make_unique<dn_cleaner>();
+  DN_CUDA(cudaGetDevice(&c->device));
+  DN_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  *out = c.release();
+  return DN_OK;
+}
+dn_status dn_cleaner_destroy(dn_cleaner* c) {
+  delete c;
+  return DN_OK;
+}
+dn_status dn_cleaner_set_same_depth_threshold(dn_cleaner* c, float t) {
+  DN_CHECK(c, "NULL cleaner");
+  c->thr = t;
+  return DN_OK;
+}
+dn_status dn_cleaner_set_min_consistent_views(dn_cleaner* c, int n) {
+  DN_CHECK(c, "NULL cleaner");
+  c->min_views = n;
+  return DN_OK;
+}
+dn_status dn_cleaner_add_view(dn_cleaner* c, const double* K, const double* R, const double* t,
+                              const float* depth, int width, int height, int stride) {
+  DN_CHECK(c, "NULL cleaner");
+  DN_TRY(check_camera(K, R, t));
+  DN_CHECK(depth, "depth must not be NULL");
+  DN_CHECK(width >= 1 && height >= 1 && width <= 16384 && height <= 16384, "bad depthmap size");
+  if (stride <= 0) stride = width;
+  DN_CHECK(stride >= width, "stride must be >= width");
+  DN_CUDA(cudaSetDevice(c->device));
+  DevBuf<float> d;
+  DN_CUDA(d.alloc((size_t)width * height));
+  DN_CUDA(cudaMemcpy2DAsync(d.p, width * sizeof(float), depth, stride * sizeof(float),
+                            width * sizeof(float), height, cudaMemcpyHostToDevice, c->stream));
+  DN_CUDA(cudaStreamSynchronize(c->stream));
+  dn::CleanView v{};
+  v.depth = d.p;
+  v.W = width;
+  v.H = height;
+  v.stride = width;
+  std::memcpy(v.K, K, sizeof(v.K));
+  std::memcpy(v.R, R, sizeof(v.R));
+  std::memcpy(v.t, t, sizeof(v.t));
+  c->views.push_back(v);
+  c->depths.push_back(std::move(d));
+  return DN_OK;
+}
+dn_status dn_cleaner_clean(dn_cleaner* c, float* clean_depth) {
+  DN_CHECK(c, "NULL cleaner");
+  DN_CHECK(clean_depth, "output must not be NULL");
+  DN_CHECK(!c->views.empty(), "DepthmapCleaner has no views");
+  DN_CUDA(cudaSetDevice(c->device));
+  const int W = c->views[0].W, H = c->views[0].H;
+  const int n = (int)c->views.size();
+  DN_CUDA(c->d_views.alloc(n));
+  DN_CUDA(c->d_others.alloc(std::max(n - 1, 1)));
+  DN_CUDA(c->d_out.alloc((size_t)W * H));
+  std::vector<int> others;
+  for (int k = 1; k < n; ++k) others.push_back(k);
+  DN_CUDA(cudaMemcpyAsync(c->d_views.p, c->views.data(), n * sizeof(dn::CleanView),
+                          cudaMemcpyHostToDevice, c->stream));
+  if (!others.empty())
+    DN_CUDA(cudaMemcpyAsync(c->d_others.p, others.data(), others.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, c->stream));
+  DN_CUDA(dn::launch_clean(c->d_views.p, 0, c->d_others.p, n - 1, W, H, c->thr, c->min_views,
+                           c->d_out.p, c->stream));
+  DN_CUDA(cudaMemcpyAsync(clean_depth, c->d_out.p, (size_t)W * H * sizeof(float),
+                          cudaMemcpyDeviceToHost, c->stream));
+  DN_CUDA(cudaStreamSynchronize(c->stream));
+  return DN_OK;
+}
+
+// ----------------------------------------------------------------- pruner
+dn_status dn_pruner_create(dn_pruner** out) {
+  DN_CHECK(out, "NULL output");
+  *out = nullptr;
+  DN_TRY(need_device());
+  auto p = std::make_unique<dn_pruner>();
+  DN_CUDA(cudaGetDevice(&p->device));
+  DN_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  DN_CUDA(p->d_count.alloc(1));
+  *out = p.release();
+  return DN_OK;
+}
+dn_status dn_pruner_destroy(dn_pruner* p) {
+  delete p;
+  return DN_OK;
+}
+dn_status dn_pruner_set_same_depth_threshold(dn_pruner* p, float t) {
+  DN_CHECK(p, "NULL pruner");
+  p->thr = t;
+  return DN_OK;
+}
+dn_status dn_pruner_add_view(dn_pruner* p, const double* K, const double* R, const double* t,
+                             const float* depth, const float* plane, const uint8_t* color,
+                             const uint8_t* label, int width, int height) {
+  DN_CHECK(p, "NULL pruner");
+  DN_TRY(check_camera(K, R, t));
+  DN_CHECK(depth && plane && color && label, "depth, plane, color and label must not be NULL");
+  DN_CHECK(width >= 1 && height >= 1 && width <= 16384 && height <= 16384, "bad depthmap size");
+  DN_CUDA(cudaSetDevice(p->device));
+  const size_t n = (size_t)width * height;
+  DevBuf<float> d, pl;
+  DevBuf<uint8_t> col, lab;
+  DN_CUDA(d.alloc(n));
+  DN_CUDA(pl.alloc(3 * n));
+  DN_CUDA(col.alloc(3 * n));
+  DN_CUDA(lab.alloc(n));
+  DN_CUDA(cudaMemcpyAsync(d.p, depth, n * sizeof(float), cudaMemcpyHostToDevice, p->stream));
+  DN_CUDA(cudaMemcpyAsync(pl.p, plane, 3 * n * sizeof(float), cudaMemcpyHostToDevice, p->stream));
+  DN_CUDA(cudaMemcpyAsync(col.p, color, 3 * n, cudaMemcpyHostToDevice, p->stream));
+  DN_CUDA(cudaMemcpyAsync(lab.p, label, n, cudaMemcpyHostToDevice, p->stream));
+  DN_CUDA(cudaStreamSynchronize(p->stream));
+  dn::PruneView v{};
+  v.depth = d.p;
+  v.plane = pl.p;
+  v.color = col.p;
+  v.label = lab.p;
+  v.W = width;
+  v.H = height;
+  std::memcpy(v.K, K, sizeof(v.K));
+  std::memcpy(v.R, R, sizeof(v.R));
+  std::memcpy(v.t, t, sizeof(v.t));
+  p->views.push_back(v);
+  p->depths.push_back(std::move(d));
+  p->planes.push_back(std::move(pl));
+  p->colors.push_back(std::move(col));
+  p->labels.push_back(std::move(lab));
+  p->count = -1;
+  return DN_OK;
+}
+dn_status dn_pruner_prune(dn_pruner* p, int64_t* count) {
+  DN_CHECK(p, "NULL pruner");
+  DN_CHECK(count, "NULL count");
+  DN_CHECK(!p->views.empty(), "DepthmapPruner has no views");
+  DN_CUDA(cudaSetDevice(p->device));
+  const int W = p->views[0].W, H = p->views[0].H;
+  const size_t n = (size_t)W * H;
+  const int nv = (int)p->views.size();
+  DN_CUDA(p->d_views.alloc(nv));
+  DN_CUDA(p->scratch.alloc(dn::prune_scratch_bytes(W, H)));
+  DN_CUDA(p->points.alloc(3 * n));
+  DN_CUDA(p->normals.alloc(3 * n));
+  DN_CUDA(p->out_colors.alloc(3 * n));
+  DN_CUDA(p->out_labels.alloc(n));
+  DN_CUDA(cudaMemcpyAsync(p->d_views.p, p->views.data(), nv * sizeof(dn::PruneView),
+                          cudaMemcpyHostToDevice, p->stream));
+  dn::PruneOut o{p->points.p, p->normals.p, p->out_colors.p, p->out_labels.p};
+  DN_CUDA(dn::launch_prune(p->d_views.p, nv, W, H, p->thr, p->scratch.p, o, p->d_count.p,
+                           p->stream));
+  unsigned long long c = 0;
+  DN_CUDA(cudaMemcpyAsync(&c, p->d_count.p, sizeof(c), cudaMemcpyDeviceToHost, p->stream));
+  DN_CUDA(cudaStreamSynchronize(p->stream));
+  p->count = (int64_t)c;
+  *count = p->count;
+  return DN_OK;
+}
+dn_status dn_pruner_fetch(dn_pruner* p, float* points, float* normals, uint8_t* colors,
+                          uint8_t* labels, int64_t capacity) {
+  DN_CHECK(p, "NULL pruner");
+  DN_CHECK(p->count >= 0, "dn_pruner_prune has not run since the last add_view");
+  DN_CHECK(capacity >= p->count, "capacity is smaller than the pruned point count");
+  DN_CUDA(cudaSetDevice(p->device));
+  const size_t n = (size_t)p->count;
+  if (n) {
+    if (points)
+      DN_CUDA(cudaMemcpyAsync(points, p->points.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
+    if (normals)
+      DN_CUDA(cudaMemcpyAsync(normals, p->normals.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
+    if (colors)
+      DN_CUDA(cudaMemcpyAsync(colors, p->out_colors.p, 3 * n, cudaMemcpyDeviceToHost, p->stream));
+    if (labels)
+      DN_CUDA(cudaMemcpyAsync(labels, p->out_labels.p, n, cudaMemcpyDeviceToHost, p->stream));
+  }
+  DN_CUDA(cudaStreamSynchronize(p->stream));
+  return DN_OK;
+}
+
+// ----------------------------------------------------------------- batch
+dn_status dn_batch_create(dn_batch** out) {
+  DN_CHECK(out, "NULL output");
+  *out = nullptr;
+  DN_TRY(need_device());
+  auto b = std::make_unique<dn_batch>();
+  DN_TRY(b->eng.init());
+  *out = b.release();
+  return DN_OK;
+}
+dn_status dn_batch_destroy(dn_batch* b) {
+  delete b;
+  return DN_OK;
+}
+dn_status dn_batch_add_view(dn_batch* b, const double* K, const double* R, const double* t,
+                            const uint8_t* image, const uint8_t* mask, int width, int height,
+                            int stride, int* view_id) {
+  DN_CHECK(b, "NULL batch");
+  return b->eng.add_view(K, R, t, image, mask, width, height, stride, view_id);
+}
+dn_status dn_batch_add_depthmap(dn_batch* b, int ref_view, const int* matching, int n,
+                                double min_depth, double max_depth, int* map_id) {
+  DN_CHECK(b, "NULL batch");
+  DN_CHECK(matching || n == 0, "NULL matching view list");
+  for (int k = 0; k < n; ++k) DN_CHECK(matching[k] != ref_view, "a view cannot match itself");
+  return b->eng.add_map(ref_view, matching, n, min_depth, max_depth, map_id);
+}
+dn_status dn_batch_set_clean_views(dn_batch* b, int map_id, const int* other_maps, int n) {
+  DN_CHECK(b, "NULL batch");
+  DN_CHECK(map_id >= 0 && map_id < (int)b->eng.maps.size(), "depthmap id out of range");
+  DN_CHECK(n >= 0 && n <= dn::kMaxNbr, "at most 16 cleaner views");
+  auto& m = *b->eng.maps[map_id];
+  m.clean_maps.clear();
+  for (int k = 0; k < n; ++k) {
+    DN_CHECK(other_maps[k] >= 0 && other_maps[k] < (int)b->eng.maps.size() && other_maps[k] != map_id,
+             "cleaner view id out of range");
+    m.clean_maps.push_back(other_maps[k]);
+  }
+  b->eng.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_params(dn_batch* b, int patch_size, float min_patch_sd, int iterations,
+                              float same_depth_threshold, int min_consistent_views,
+                              uint64_t seed) {
+  DN_CHECK(b, "NULL batch");
+  const int hpz = (patch_size - 1) / 2;
+  DN_CHECK(hpz >= 1 && hpz <= dn::kMaxHpz, "patch size must be in 3..12");
+  DN_CHECK(iterations >= 0 && iterations <= 1000, "iterations must be 0..1000");
+  b->eng.patch = patch_size;
+  b->eng.min_var = min_patch_sd * min_patch_sd;
+  b->eng.iterations = iterations;
+  b->eng.same_depth_thr = same_depth_threshold;
+  b->eng.min_consistent = min_consistent_views;
+  b->eng.seed = seed;
+  b->eng.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes) {
+  DN_CHECK(b, "NULL batch");
+  return b->eng.set_init(map_id, planes);
+}
+dn_status dn_batch_run(dn_batch* b, unsigned flags) {
+  DN_CHECK(b, "NULL batch");
+  Engine& e = b->eng;
+  DN_CUDA(cudaSetDevice(e.device));
+  DN_TRY(e.check_params(Mode::kPatchMatch));
+  DN_TRY(e.prepare());
+  const bool use_graph = (flags & DN_RUN_GRAPH) != 0;
+  const bool timing = (flags & DN_RUN_TIMING) != 0;
+  e.timed = timing;
+  if (!(flags & DN_RUN_CLEAN) && timing) {
+    // No cleaner stage: its event marks the end of the run.
+  }
+  if (use_graph && e.graph && e.graph_flags == flags) {
+    DN_CUDA(cudaGraphLaunch(e.graph, e.stream));
+    b->ran = true;
+    e.computed = true;
+    return DN_OK;
+  }
+  if (use_graph) {
+    if (e.graph) {
+      cudaGraphExecDestroy(e.graph);
+      e.graph = nullptr;
+    }
+    // Allocations and host-to-device table uploads happen before capture.
+    if (flags & DN_RUN_CLEAN) DN_TRY(e.prepare_clean());
+    cudaGraph_t g = nullptr;
+    DN_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+    dn_status s = e.enqueue(Mode::kPatchMatch, timing);
+    if (s == DN_OK && (flags & DN_RUN_CLEAN)) s = e.enqueue_clean(timing);
+    cudaError_t ce = cudaStreamEndCapture(e.stream, &g);
+    if (s != DN_OK) {
+      if (g) cudaGraphDestroy(g);
+      return s;
+    }
+    DN_CUDA(ce);
+    cudaError_t ie = cudaGraphInstantiate(&e.graph, g, 0);
+    cudaGraphDestroy(g);
+    DN_CUDA(ie);
+    e.graph_flags = flags;
+    DN_CUDA(cudaGraphLaunch(e.graph, e.stream));
+  } else {
+    if (flags & DN_RUN_CLEAN) DN_TRY(e.prepare_clean());
+    DN_TRY(e.enqueue(Mode::kPatchMatch, timing));
+    if (flags & DN_RUN_CLEAN) DN_TRY(e.enqueue_clean(timing));
+  }
+  b->ran = true;
+  e.computed = true;
+  return DN_OK;
+}
+dn_status dn_batch_synchronize(dn_batch* b) {
+  DN_CHECK(b, "NULL batch");
+  DN_CUDA(cudaSetDevice(b->eng.device));
+  return b->eng.finish();
+}
+dn_status dn_batch_get_depthmap(dn_batch* b, int map_id, float* depth, float* plane,
+                                float* score, int32_t* nghbr, float* clean) {
+  DN_CHECK(b, "NULL batch");
+  return b->eng.fetch(map_id, depth, plane, score, nghbr, clean);
+}
+dn_status dn_batch_pruned_count(dn_batch* b, int64_t* count) {
+  DN_CHECK(b && count, "NULL argument");
+  return fail(DN_NOT_READY, "batched pruning is not enabled in this build");
+}
+dn_status dn_batch_last_taps(dn_batch* b, uint64_t* taps) {
+  DN_CHECK(b, "NULL batch");
+  return b->eng.taps(taps);
+}
+dn_status dn_batch_set_view_image(dn_batch* b, int view_id, const uint8_t* image, int stride) {
+  DN_CHECK(b, "NULL batch");
+  return b->eng.set_view_image(view_id, image, stride);
+}
+dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_out) {
+  DN_CHECK(b, "NULL batch");
+  return b->eng.timings(out, n, taps_out);
+}
+dn_status dn_batch_timer_record(dn_batch* b, int slot) {
+  DN_CHECK(b, "NULL batch");
+  DN_CHECK(slot == 0 || slot == 1, "timer slot must be 0 or 1");
+  DN_CUDA(cudaSetDevice(b->eng.device));
+  DN_CUDA(cudaEventRecord(b->eng.ev[5 + slot], b->eng.stream));
+  return DN_OK;
+}
+dn_status dn_batch_timer_elapsed(dn_batch* b, float* ms) {
+  DN_CHECK(b && ms, "NULL argument");
+  DN_CUDA(cudaSetDevice(b->eng.device));
+  DN_CUDA(cudaEventSynchronize(b->eng.ev[6]));
+  DN_CUDA(cudaEventElapsedTime(ms, b->eng.ev[5], b->eng.ev[6]));
+  return DN_OK;
+}
+dn_status dn_batch_copy_depth_device(dn_batch* b, int map_id, float* d_out) {
+  DN_CHECK(b, "NULL batch");
+  DN_CHECK(d_out, "NULL output");
+  Engine& e = b->eng;
+  DN_CHECK(map_id >= 0 && map_id < (int)e.maps.size(), "depthmap id out of range");
+  DN_CUDA(cudaSetDevice(e.device));
+  const Map& m = *e.maps[map_id];
+  const View& r = *e.views[m.ref];
+  DN_CUDA(cudaMemcpyAsync(d_out, m.depth.p, (size_t)r.W * r.H * sizeof(float),
+                          cudaMemcpyDeviceToDevice, e.stream));
+  return DN_OK;
+}
+
+dn_status dn_postprocess_depth(const float* depth, float* out, int width, int height) {
+  DN_CHECK(depth && out, "NULL buffer");
+  DN_CHECK(width >= 1 && height >= 1 && width <= 16384 && height <= 16384, "bad size");
+  DN_TRY(need_device());
+  const size_t n = (size_t)width * height;
+  DevBuf<float> a, b;
+  DN_CUDA(a.alloc(n));
+  DN_CUDA(b.alloc(n));
+  DN_CUDA(cudaMemcpy(a.p, depth, n * sizeof(float), cudaMemcpyHostToDevice));
+  DN_CUDA(dn::launch_postprocess_plain(a.p, b.p, width, height, 0));
+  DN_CUDA(cudaMemcpy(out, b.p, n * sizeof(float), cudaMemcpyDeviceToHost));
+  return DN_OK;
+}
+
+dn_status dn_fp32_peak(double* tflops, double* ms) {
+  DN_CHECK(tflops && ms, "NULL output");
+  DN_TRY(need_device());
+  DN_CUDA(dn::fp32_peak(tflops, ms));
+  return DN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,582 @@
+// sm_100a kernels of the dense depthmap path: coefficient tables, random /
+// given-plane initialisation, brute-force plane sweep, plane scoring,
+// red-black PatchMatch half-passes, median post-process and packing.
+//
+// Every kernel works on a batch: blockIdx.x indexes a tile list of
+// (map, tile_x, tile_y) built on the host, so one launch covers every
+// depthmap of a reconstruction whatever their sizes.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace dn {
+
+// Resident 128-thread blocks per SM each estimator kernel is compiled for:
+// the per-tap weights live in registers, (2 HPZ + 1)^2 x 2 of them.
+template <int HPZ>
+constexpr int kMinBlocks = HPZ <= 2 ? 4 : (HPZ == 3 ? 3 : 2);
+
+// ----------------------------------------------------------------------
+// Per-view preparation.
+
+__global__ void u8_to_half_kernel(const uint8_t* __restrict__ src, int W, int H, int stride,
+                                  __half* __restrict__ dst) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x < W && y < H) dst[(size_t)y * W + x] = __ushort2half_rn(src[(size_t)y * stride + x]);
+}
+
+// Bilinear coefficient table.  Entry (ix, iy), ix in [-P, W-2+P], holds the
+// bilinear interpolant of the 2x2 block at (ix, iy) as a polynomial in
+// f1 = 1 + fx, g1 = 1 + fy:  y - cbias = e0 + f1 e1 + g1 (e2 + f1 e3).
+// Blocks that reach outside [0, W-1) x [0, H-1) hold the constant -cbias,
+// i.e. the reference's zero sample (LinearInterpolation, depthmap.cc:16-18).
+// All coefficients are small integers, exact in FP32.
+__global__ void build_quad_kernel(const __half* __restrict__ img, int W, int H, float cbias,
+                                  float4* __restrict__ quad, int TW, int TH) {
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x, ty = blockIdx.y;
+  if (tx >= TW || ty >= TH) return;
+  const int ix = tx - kPad, iy = ty - kPad;
+  float4 q = make_float4(-cbias, 0.f, 0.f, 0.f);
+  if (ix >= 0 && ix <= W - 2 && iy >= 0 && iy <= H - 2) {
+    const float q00 = __half2float(img[(size_t)iy * W + ix]);
+    const float q01 = __half2float(img[(size_t)iy * W + ix + 1]);
+    const float q10 = __half2float(img[(size_t)(iy + 1) * W + ix]);
+    const float q11 = __half2float(img[(size_t)(iy + 1) * W + ix + 1]);
+    const float d1 = q01 - q00, d2 = q10 - q00, d3 = q11 - q10 - q01 + q00;
+    q = make_float4(q00 - d1 - d2 + d3 - cbias, d1 - d3, d2 - d3, d3);
+  }
+  quad[(size_t)ty * TW + tx] = q;
+}
+
+// ----------------------------------------------------------------------
+// Shared-memory staging of the reference tile plus a patch-radius halo.
+
+template <int HPZ>
+__device__ inline void stage_tile(float* tile, int pitch, int rows, const __half* img, int W,
+                                  int H, int y0, int x0) {
+  const int n = pitch * rows;
+  for (int k = threadIdx.y * blockDim.x + threadIdx.x; k < n; k += blockDim.x * blockDim.y) {
+    const int r = k / pitch, c = k - r * pitch;
+    int y = y0 - HPZ + r, x = x0 - HPZ + c;
+    y = min(max(y, 0), H - 1);
+    x = min(max(x, 0), W - 1);
+    tile[k] = __half2float(img[(size_t)y * W + x]);
+  }
+}
+
+__device__ inline void flush_taps(unsigned taps, unsigned long long* counter) {
+  __shared__ unsigned long long block_taps;
+  if (threadIdx.x == 0 && threadIdx.y == 0) block_taps = 0;
+  __syncthreads();
+  if (taps) atomicAdd(&block_taps, (unsigned long long)taps);
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0 && block_taps && counter)
+    atomicAdd(counter, block_taps);
+}
+
+// Variance (depthmap.cc:32-44) of the patch around the tile pixel (ly, lx),
+// in the reference's float order.
+template <int HPZ>
+__device__ inline float patch_variance(const float* tile, int pitch, int ly, int lx) {
+  constexpr int N = (2 * HPZ + 1) * (2 * HPZ + 1);
+  float sum = 0.f;
+#pragma unroll
+  for (int u = -HPZ; u <= HPZ; ++u)
+#pragma unroll
+    for (int v = -HPZ; v <= HPZ; ++v) sum = __fadd_rn(sum, tile[(ly + u) * pitch + lx + v]);
+  const float mean = __fdiv_rn(sum, (float)N);
+  float s2 = 0.f;
+#pragma unroll
+  for (int u = -HPZ; u <= HPZ; ++u)
+#pragma unroll
+    for (int v = -HPZ; v <= HPZ; ++v) {
+      const float d = __fsub_rn(tile[(ly + u) * pitch + lx + v], mean);
+      s2 = __fadd_rn(s2, __fmul_rn(d, d));
+    }
+  return __fdiv_rn(s2, (float)N);
+}
+
+// ----------------------------------------------------------------------
+// Initialisation: RandomInitialization + ComputeIgnoreMask
+// (depthmap.cc:237-269), or a given plane field (learned proposal).
+
+template <int HPZ, bool SAMPLE>
+__global__ void __launch_bounds__(128, kMinBlocks<HPZ>)
+init_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+            const PairDev* __restrict__ pairs, const int4* __restrict__ tiles, RunParams p) {
+  extern __shared__ float tile[];
+  const int4 tl = tiles[blockIdx.x];
+  const MapDev& m = maps[tl.x];
+  const ViewDev& rv = views[m.ref_view];
+  const int W = m.W, H = m.H;
+  const int x0 = tl.y * blockDim.x, y0 = tl.z * blockDim.y;
+  const int pitch = blockDim.x + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
+  __syncthreads();
+  const int i = y0 + threadIdx.y, j = x0 + threadIdx.x;
+  unsigned taps = 0;
+  if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) {
+    const size_t pix = (size_t)i * W + j;
+    const int ly = threadIdx.y + HPZ, lx = threadIdx.x + HPZ;
+    const bool masked = rv.mask && rv.mask[pix] == 0;
+    const bool low = patch_variance<HPZ>(tile, pitch, ly, lx) < p.min_var;
+    float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
+    float sc = 0.f;
+    int nb = 0;
+    if (!masked && !low) {
+      const uint4 r = philox4x32_10(make_uint4((uint32_t)pix, (uint32_t)tl.x, 0xFFFFFFFFu, 0u),
+                                    p.seed_lo, p.seed_hi);
+      float3 v;
+      float depth;
+      bool given = false;
+      if (m.init) {
+        v = make_float3(m.init[3 * pix], m.init[3 * pix + 1], m.init[3 * pix + 2]);
+        given = v.z != 0.0f;
+        if (given) depth = depth_of_plane(j, i, m.Kinv_d, v);
+      }
+      if (!given) {
+        // UniformRand(log min, log max) then exp; normal (U(-1,1), U(-1,1), -1).
+        depth = expf(fmaf(m.log_max - m.log_min, u01(r.x), m.log_min));
+        const float3 n = make_float3(fmaf(2.f, u01(r.y), -1.f), fmaf(2.f, u01(r.z), -1.f), -1.f);
+        v = plane_from_depth_normal((float)j, (float)i, m.Kinv_d, depth, n);
+      }
+      RefPatch<HPZ> rp;
+      ref_patch_from_tile<HPZ>(rp, tile, pitch, ly, lx);
+      const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
+      if (SAMPLE) {
+        nb = 1 + (int)(r.w % (uint32_t)m.n_pairs);
+        const PairDev& pr = pairs[m.pair0 + nb - 1];
+        sc = ncc_view<HPZ>(rp, views[pr.view], pr, h, (float)j, (float)i, taps);
+      } else {
+        sc = ncc_max<HPZ>(rp, views, pairs + m.pair0, m.n_pairs, h, (float)j, (float)i, nb, taps);
+      }
+      st = make_float4(v.x, v.y, v.z, depth);
+    }
+    m.state[pix] = st;
+    m.score[pix] = sc;
+    m.nghbr[pix] = nb;
+  }
+  flush_taps(taps, p.taps);
+}
+
+// ----------------------------------------------------------------------
+// Brute-force sweep (ComputeBruteForce, depthmap.cc:184-200): P fronto-
+// parallel planes uniform in inverse depth; a plane replaces the current
+// one only if its score is strictly higher (the result starts at score 0).
+
+template <int HPZ>
+__global__ void __launch_bounds__(128, kMinBlocks<HPZ>)
+brute_force_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+                   const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
+                   RunParams p) {
+  extern __shared__ float tile[];
+  const int4 tl = tiles[blockIdx.x];
+  const MapDev& m = maps[tl.x];
+  const ViewDev& rv = views[m.ref_view];
+  const int W = m.W, H = m.H;
+  const int x0 = tl.y * blockDim.x, y0 = tl.z * blockDim.y;
+  const int pitch = blockDim.x + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
+  __syncthreads();
+  const int i = y0 + threadIdx.y, j = x0 + threadIdx.x;
+  unsigned taps = 0;
+  if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) {
+    const size_t pix = (size_t)i * W + j;
+    RefPatch<HPZ> rp;
+    ref_patch_from_tile<HPZ>(rp, tile, pitch, threadIdx.y + HPZ, threadIdx.x + HPZ);
+    float best = 0.f, bestd = 0.f;
+    int bestn = 0;
+    float3 bestv = make_float3(0.f, 0.f, 0.f);
+    const double a = __ddiv_rn(1.0, m.min_depth);
+    const double span = __dsub_rn(__ddiv_rn(1.0, m.max_depth), a);
+    const double den = (double)(p.num_planes - 1);
+    for (int d = 0; d < p.num_planes; ++d) {
+      const float depth =
+          (float)__ddiv_rn(1.0, __dadd_rn(a, __ddiv_rn(__dmul_rn((double)d, span), den)));
+      const float3 v =
+          plane_from_depth_normal((float)j, (float)i, m.Kinv_d, depth, make_float3(0.f, 0.f, -1.f));
+      const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
+      int nb;
+      const float s = ncc_max<HPZ>(rp, views, pairs + m.pair0, m.n_pairs, h, (float)j, (float)i,
+                                   nb, taps);
+      if (s > best) {
+        best = s;
+        bestn = nb;
+        bestv = v;
+        bestd = depth_of_plane(j, i, m.Kinv_d, v);
+      }
+    }
+    m.state[pix] = make_float4(bestv.x, bestv.y, bestv.z, bestd);
+    m.score[pix] = best;
+    m.nghbr[pix] = bestn;
+  }
+  flush_taps(taps, p.taps);
+}
+
+// ----------------------------------------------------------------------
+// ComputePlaneScore for given planes (m.init) on every interior pixel.
+
+template <int HPZ>
+__global__ void __launch_bounds__(128, kMinBlocks<HPZ>)
+score_planes_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+                    const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
+                    RunParams p) {
+  extern __shared__ float tile[];
+  const int4 tl = tiles[blockIdx.x];
+  const MapDev& m = maps[tl.x];
+  const ViewDev& rv = views[m.ref_view];
+  const int W = m.W, H = m.H;
+  const int x0 = tl.y * blockDim.x, y0 = tl.z * blockDim.y;
+  const int pitch = blockDim.x + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
+  __syncthreads();
+  const int i = y0 + threadIdx.y, j = x0 + threadIdx.x;
+  unsigned taps = 0;
+  if (i < H && j < W) {
+    const size_t pix = (size_t)i * W + j;
+    float sc = 0.f;
+    int nb = 0;
+    if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) {
+      RefPatch<HPZ> rp;
+      ref_patch_from_tile<HPZ>(rp, tile, pitch, threadIdx.y + HPZ, threadIdx.x + HPZ);
+      const float3 v = make_float3(m.init[3 * pix], m.init[3 * pix + 1], m.init[3 * pix + 2]);
+      const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
+      sc = ncc_max<HPZ>(rp, views, pairs + m.pair0, m.n_pairs, h, (float)j, (float)i, nb, taps);
+    }
+    m.score[pix] = sc;
+    m.nghbr[pix] = nb;
+  }
+  flush_taps(taps, p.taps);
+}
+
+// ----------------------------------------------------------------------
+// Red-black PatchMatch half-pass.  Pixels of colour `p.colour`
+// ((i + j) % 2 == colour) are updated from the opposite colour, which this
+// pass does not write, so there is no race.  Candidates per pixel
+// (PatchMatchUpdatePixel, depthmap.cc:305-374, widened for red-black):
+//   - the planes of the 4 adjacent pixels (up, left, down, right);
+//   - per direction, the plane of the best-scoring pixel among distances
+//     3, 5, ..., 23 (all of the opposite colour), which carries good planes
+//     across many pixels per pass the way the reference's raster sweep does;
+//   - 6 random refinements of the current plane with the reference's
+//     schedule (depth x exp(0.02 N), normal slope + 0.5 N; ranges x0.3, x0.8).
+// A candidate whose plane equals the current plane bit for bit is skipped:
+// its score at this pixel is the current score.
+
+template <int HPZ, bool SAMPLE>
+__global__ void __launch_bounds__(128, kMinBlocks<HPZ>)
+halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+                const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
+                RunParams p) {
+  extern __shared__ float tile[];
+  const int4 tl = tiles[blockIdx.x];
+  const MapDev& m = maps[tl.x];
+  const ViewDev& rv = views[m.ref_view];
+  const int W = m.W, H = m.H;
+  const int x0 = tl.y * (2 * blockDim.x), y0 = tl.z * blockDim.y;
+  const int pitch = 2 * blockDim.x + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
+  __syncthreads();
+  const int i = y0 + threadIdx.y;
+  const int j = x0 + 2 * threadIdx.x + ((i + p.colour) & 1);
+  unsigned taps = 0;
+  const size_t pix = (size_t)i * W + j;
+  float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) st = m.state[pix];
+  if (st.w != 0.0f) {
+    RefPatch<HPZ> rp;
+    ref_patch_from_tile<HPZ>(rp, tile, pitch, threadIdx.y + HPZ, (j - x0) + HPZ);
+    const float fj = (float)j, fi = (float)i;
+    float cur = m.score[pix];
+    int curn = m.nghbr[pix];
+    float3 cv = make_float3(st.x, st.y, st.z);
+    float cd = st.w;
+    const PairDev* mp = pairs + m.pair0;
+
+    auto try_plane = [&](float3 v, int view) {
+      if (same_plane(v, cv)) return;
+      const Hyp h = make_hyp(m.Kinv, v, fj, fi);
+      float s;
+      int nb;
+      if (SAMPLE) {
+        nb = view;
+        if (nb < 1 || nb > m.n_pairs) return;
+        const PairDev& pr = mp[nb - 1];
+        s = ncc_view<HPZ>(rp, views[pr.view], pr, h, fj, fi, taps);
+      } else {
+        s = ncc_max<HPZ>(rp, views, mp, m.n_pairs, h, fj, fi, nb, taps);
+      }
+      if (s > cur) {
+        cur = s;
+        curn = nb;
+        cv = v;
+        cd = depth_of_plane(j, i, m.Kinv_d, v);
+      }
+    };
+
+    const int di[4] = {-1, 0, 1, 0}, dj[4] = {0, -1, 0, 1};
+#pragma unroll 1
+    for (int d = 0; d < 4; ++d) {
+      const int qi = i + di[d], qj = j + dj[d];
+      const size_t q = (size_t)qi * W + qj;
+      const float4 sq = m.state[q];
+      if (sq.w != 0.0f) try_plane(make_float3(sq.x, sq.y, sq.z), SAMPLE ? m.nghbr[q] : 0);
+    }
+#pragma unroll 1
+    for (int d = 0; d < 4; ++d) {
+      float bs = -3.0f;
+      long bq = -1;
+      for (int k = 0; k < kFarSamples; ++k) {
+        const int dist = kFarStart + 2 * k;
+        const int qi = i + di[d] * dist, qj = j + dj[d] * dist;
+        if (qi < 0 || qi >= H || qj < 0 || qj >= W) break;
+        const size_t q = (size_t)qi * W + qj;
+        const float sq = m.score[q];
+        if (sq > bs && m.state[q].w != 0.0f) {
+          bs = sq;
+          bq = (long)q;
+        }
+      }
+      if (bq >= 0) {
+        const float4 sq = m.state[bq];
+        try_plane(make_float3(sq.x, sq.y, sq.z), SAMPLE ? m.nghbr[bq] : 0);
+      }
+    }
+    // Refinement draws: 18 normals from 5 Philox blocks.
+    uint32_t rnd[20];
+#pragma unroll
+    for (int b = 0; b < 5; ++b) {
+      const uint4 r = philox4x32_10(make_uint4((uint32_t)pix, (uint32_t)tl.x, (uint32_t)p.pass,
+                                               (uint32_t)b), p.seed_lo, p.seed_hi);
+      rnd[4 * b] = r.x;
+      rnd[4 * b + 1] = r.y;
+      rnd[4 * b + 2] = r.z;
+      rnd[4 * b + 3] = r.w;
+    }
+    float z[18];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float2 g = normal2(rnd[2 * k], rnd[2 * k + 1]);
+      z[2 * k] = g.x;
+      z[2 * k + 1] = g.y;
+    }
+    const int refn = curn;
+    float depth_range = 0.02f, normal_range = 0.5f;
+#pragma unroll 1
+    for (int k = 0; k < 6; ++k) {
+      if (cv.z == 0.0f) continue;
+      const float depth = cd * expf(depth_range * z[3 * k]);
+      const float3 n = make_float3(-cv.x / cv.z + normal_range * z[3 * k + 1],
+                                   -cv.y / cv.z + normal_range * z[3 * k + 2], -1.0f);
+      const float3 v = plane_from_depth_normal(fj, fi, m.Kinv_d, depth, n);
+      try_plane(v, refn);
+      depth_range *= 0.3f;
+      normal_range *= 0.8f;
+    }
+    if (SAMPLE && m.n_pairs >= 2) {
+      // A random other matching view for the current plane.
+      int other = 1 + (int)(rnd[18] % (uint32_t)(m.n_pairs - 1));
+      if (other >= curn) other += 1;
+      const Hyp h = make_hyp(m.Kinv, cv, fj, fi);
+      const PairDev& pr = mp[other - 1];
+      const float s = ncc_view<HPZ>(rp, views[pr.view], pr, h, fj, fi, taps);
+      if (s > cur) {
+        cur = s;
+        curn = other;
+      }
+    }
+    m.state[pix] = make_float4(cv.x, cv.y, cv.z, cd);
+    m.score[pix] = cur;
+    m.nghbr[pix] = curn;
+  }
+  flush_taps(taps, p.taps);
+}
+
+// ----------------------------------------------------------------------
+// PostProcess (depthmap.cc:489-502): 5x5 median of the depth (replicated
+// border, as cv::medianBlur does for float input); a pixel keeps its depth
+// only if it is non-zero and within 5 % of the median.
+
+__device__ inline void cswap(float& a, float& b) {
+  const float lo = fminf(a, b), hi = fmaxf(a, b);
+  a = lo;
+  b = hi;
+}
+
+// Median of the 5x5 window around (i, j) of a row-major depth image read
+// through `at(y, x)`, with replicated borders.
+template <typename At>
+__device__ inline float median5(At at, int i, int j, int W, int H) {
+  float v[25];
+#pragma unroll
+  for (int a = 0; a < 5; ++a)
+#pragma unroll
+    for (int b = 0; b < 5; ++b) {
+      const int y = min(max(i + a - 2, 0), H - 1), x = min(max(j + b - 2, 0), W - 1);
+      v[5 * a + b] = at(y, x);
+    }
+  // Odd-even transposition sort of 25 values (25 rounds).
+#pragma unroll
+  for (int r = 0; r < 25; ++r)
+#pragma unroll
+    for (int k = (r & 1); k + 1 < 25; k += 2) cswap(v[k], v[k + 1]);
+  return v[12];
+}
+
+__device__ inline float post_value(float d, float med) {
+  const bool zero = (d == 0.0f) || ((double)__fdiv_rn(fabsf(__fsub_rn(d, med)), d) > 0.05);
+  return zero ? 0.0f : d;
+}
+
+__global__ void postprocess_kernel(const MapDev* __restrict__ maps, const int4* __restrict__ tiles,
+                                   int apply) {
+  const int4 tl = tiles[blockIdx.x];
+  const MapDev& m = maps[tl.x];
+  const int W = m.W, H = m.H;
+  const int i = tl.z * blockDim.y + threadIdx.y, j = tl.y * blockDim.x + threadIdx.x;
+  if (i >= H || j >= W) return;
+  const size_t pix = (size_t)i * W + j;
+  const float d = m.state[pix].w;
+  if (!apply) {
+    m.depth[pix] = d;
+    return;
+  }
+  const float4* st = m.state;
+  const float med = median5([&](int y, int x) { return st[(size_t)y * W + x].w; }, i, j, W, H);
+  m.depth[pix] = post_value(d, med);
+}
+
+__global__ void postprocess_plain_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                         int W, int H) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= H || j >= W) return;
+  const float med = median5([&](int y, int x) { return in[(size_t)y * W + x]; }, i, j, W, H);
+  out[(size_t)i * W + j] = post_value(in[(size_t)i * W + j], med);
+}
+
+// Register-resident FMA loop: 8 independent chains per thread.
+__global__ void fp32_peak_kernel(float* out, int iters, float a, float b) {
+  float x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3f + k;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = fmaf(x[k], a, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == 1234.5f) out[0] = s;  // keeps the loop alive
+}
+
+// Interleaves the state into the reference's output layout.
+__global__ void pack_kernel(const MapDev* __restrict__ maps, int map, float* __restrict__ plane) {
+  const MapDev& m = maps[map];
+  const size_t n = (size_t)m.W * m.H;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const float4 s = m.state[k];
+    plane[3 * k] = s.x;
+    plane[3 * k + 1] = s.y;
+    plane[3 * k + 2] = s.z;
+  }
+}
+
+// ----------------------------------------------------------------------
+// Host-side launchers.
+
+template <int HPZ>
+static cudaError_t launch_hpz(Stage stage, bool sample, const LaunchArgs& a, cudaStream_t s) {
+  const dim3 blk(a.bx, a.by);
+  if (stage == Stage::kHalfPass) {
+    const size_t smem = sizeof(float) * (2 * a.bx + 2 * HPZ) * (a.by + 2 * HPZ);
+    if (sample)
+      halfpass_kernel<HPZ, true><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+    else
+      halfpass_kernel<HPZ, false><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+    return cudaGetLastError();
+  }
+  const size_t smem = sizeof(float) * (a.bx + 2 * HPZ) * (a.by + 2 * HPZ);
+  switch (stage) {
+    case Stage::kInit:
+      if (sample)
+        init_kernel<HPZ, true><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+      else
+        init_kernel<HPZ, false><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+      break;
+    case Stage::kBruteForce:
+      brute_force_kernel<HPZ><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+      break;
+    case Stage::kScorePlanes:
+      score_planes_kernel<HPZ><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStream_t s) {
+  if (a.n_tiles == 0) return cudaSuccess;
+  if (stage == Stage::kPostProcess) {
+    postprocess_kernel<<<a.n_tiles, dim3(a.bx, a.by), 0, s>>>(a.maps, a.tiles, a.flag);
+    return cudaGetLastError();
+  }
+  switch (a.p.hpz) {
+    case 1: return launch_hpz<1>(stage, sample, a, s);
+    case 2: return launch_hpz<2>(stage, sample, a, s);
+    case 3: return launch_hpz<3>(stage, sample, a, s);
+    case 4: return launch_hpz<4>(stage, sample, a, s);
+    case 5: return launch_hpz<5>(stage, sample, a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, __half* d_img,
+                                float4* d_quad, int TW, int TH, float cbias, cudaStream_t s) {
+  u8_to_half_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(d_u8, W, H, stride, d_img);
+  build_quad_kernel<<<dim3((TW + 255) / 256, TH), 256, 0, s>>>(d_img, W, H, cbias, d_quad, TW, TH);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_postprocess_plain(const float* in, float* out, int W, int H, cudaStream_t s) {
+  postprocess_plain_kernel<<<dim3((W + 31) / 32, (H + 7) / 8), dim3(32, 8), 0, s>>>(in, out, W, H);
+  return cudaGetLastError();
+}
+
+cudaError_t fp32_peak(double* tflops, double* ms) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  float* out = nullptr;
+  cudaError_t e = cudaMalloc(&out, sizeof(float));
+  if (e != cudaSuccess) return e;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  fp32_peak_kernel<<<blocks, threads>>>(out, 64, 0.999f, 1e-3f);  // warm-up
+  cudaEventRecord(e0);
+  fp32_peak_kernel<<<blocks, threads>>>(out, iters, 0.999f, 1e-3f);
+  cudaEventRecord(e1);
+  e = cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (e != cudaSuccess) return e;
+  const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  *ms = t;
+  *tflops = flops / (t * 1e-3) / 1e12;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const MapDev* maps, int map, float* plane, size_t n, cudaStream_t s) {
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+  pack_kernel<<<blocks, 256, 0, s>>>(maps, map, plane);
+  return cudaGetLastError();
+}
+
+}  // namespace dn

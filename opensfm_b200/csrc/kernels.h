@@ -1,0 +1,61 @@
+// Host-side entry points of the dense kernels (kernels.cu, cleanprune.cu).
+#pragma once
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace dn {
+
+enum class Stage { kInit, kBruteForce, kScorePlanes, kHalfPass, kPostProcess };
+
+struct LaunchArgs {
+  const MapDev* maps;
+  const ViewDev* views;
+  const PairDev* pairs;
+  const int4* tiles;  // (map, tile_x, tile_y, 0) per block
+  int n_tiles;
+  int bx, by;         // block shape (threads)
+  int flag;           // post-process: apply the median filter
+  RunParams p;
+};
+
+cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStream_t s);
+cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, __half* d_img,
+                                float4* d_quad, int TW, int TH, float cbias, cudaStream_t s);
+cudaError_t launch_pack(const MapDev* maps, int map, float* plane, size_t n, cudaStream_t s);
+cudaError_t launch_postprocess_plain(const float* in, float* out, int W, int H, cudaStream_t s);
+cudaError_t fp32_peak(double* tflops, double* ms);
+
+// Cleaner / pruner (cleanprune.cu).
+struct CleanView {
+  const float* depth;  // [H][W]
+  int W, H, stride;
+  double K[9], R[9], t[3];
+};
+struct PruneView {
+  const float* depth;  // [H][W]
+  const float* plane;  // [H][W][3]
+  const uint8_t* color;  // [H][W][3]
+  const uint8_t* label;  // [H][W]
+  int W, H;
+  double K[9], R[9], t[3];
+};
+struct PruneOut {
+  float* points;
+  float* normals;
+  uint8_t* colors;
+  uint8_t* labels;
+};
+
+// Cleans map `ref` against views others[0..n) (DepthmapCleaner::Clean).
+cudaError_t launch_clean(const CleanView* d_views, int ref, const int* d_others, int n_others,
+                         int W, int H, float thr, int min_views, float* out, cudaStream_t s);
+// Pruner in three kernels: keep flags + per-block counts, block-count scan,
+// ordered compaction.  `scratch` holds ceil(W*H/1024) + 1 uint32 counts and
+// W*H keep bytes (see prune_scratch_bytes).
+size_t prune_scratch_bytes(int W, int H);
+cudaError_t launch_prune(const PruneView* d_views, int n_views, int W, int H, float thr,
+                         void* scratch, PruneOut out, unsigned long long* d_count, cudaStream_t s);
+
+}  // namespace dn

@@ -1,0 +1,370 @@
+"""Drop-in for the legacy ``pydense`` classes of OpenSfM's dense path.
+
+Mirrors ``opensfm/src/lib/dense/pydense.pyi:28-77`` (DepthmapCleaner,
+DepthmapEstimator, DepthmapPruner) over the C ABI of libdense_b200.so:
+same method names, argument order and meaning, same return layout:
+
+* ``DepthmapEstimator.compute_*()`` -> ``[depth (H,W) f32, plane (H,W,3) f32,
+  score (H,W) f32, nghbr (H,W) i32]`` (``DepthmapEstimatorResult``,
+  ``depthmap.h:50-55``);
+* ``DepthmapCleaner.clean()`` -> ``(H,W) f32``;
+* ``DepthmapPruner.prune()`` -> ``[points (N,3) f32, normals (N,3) f32,
+  colors (N,3) u8, labels (N,) u8]``.
+
+Arrays are converted to C-contiguous float64 / uint8 / float32 as pybind11's
+``forcecast`` would; inputs are copied at ``add_view``.  Bad shapes or values
+raise ``ValueError``; device failures raise ``RuntimeError``
+(``opensfm_b200._lib.DenseError``).  The library releases no Python lock of
+its own; ctypes drops the GIL for the duration of each call.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import _d, _f, _i32, _u8, check, ptr
+
+__all__ = ["DepthmapEstimator", "DepthmapCleaner", "DepthmapPruner", "Batch", "postprocess_depth",
+           "fp32_peak"]
+
+
+def postprocess_depth(depth: np.ndarray) -> np.ndarray:
+    """PostProcess (``depthmap.cc:489-502``) of a depth map on the device."""
+    d = np.ascontiguousarray(depth, dtype=np.float32)
+    if d.ndim != 2:
+        raise ValueError("depth must be 2-D")
+    out = np.zeros_like(d)
+    check(_lib.load().dn_postprocess_depth(ptr(d, _f), ptr(out, _f), d.shape[1], d.shape[0]))
+    return out
+
+
+def fp32_peak() -> float:
+    """Measured FP32 FMA throughput of the current device, TFLOP/s."""
+    tf = ctypes.c_double()
+    ms = ctypes.c_double()
+    check(_lib.load().dn_fp32_peak(ctypes.byref(tf), ctypes.byref(ms)))
+    return float(tf.value)
+
+
+def _mat(a, shape, name):
+    m = np.ascontiguousarray(a, dtype=np.float64)
+    if m.size != int(np.prod(shape)):
+        raise ValueError(f"{name} must have {int(np.prod(shape))} elements, got {m.size}")
+    return m.reshape(shape)
+
+
+def _image(a, name):
+    im = np.ascontiguousarray(a)
+    if im.ndim != 2:
+        raise ValueError(f"{name} must be a 2-D array, got shape {im.shape}")
+    return np.ascontiguousarray(im, dtype=np.uint8)
+
+
+class _Handle:
+    _destroy = None
+
+    def __init__(self, create: str, destroy: str):
+        self._L = _lib.load()
+        h = ctypes.c_void_p()
+        check(getattr(self._L, create)(ctypes.byref(h)))
+        self._h = h
+        self._destroy = getattr(self._L, destroy)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._destroy is not None:
+            self._destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DepthmapEstimator(_Handle):
+    """``dense::DepthmapEstimator`` (``depthmap.h:57-111``) on the B200."""
+
+    def __init__(self) -> None:
+        super().__init__("dn_estimator_create", "dn_estimator_destroy")
+        self._shape = None
+
+    def add_view(self, K, R, t, image, mask) -> None:
+        K = _mat(K, (3, 3), "K")
+        R = _mat(R, (3, 3), "R")
+        t = _mat(t, (3,), "t")
+        im = _image(image, "image")
+        mk = _image(mask, "mask") if mask is not None else None
+        if mk is not None and mk.shape != im.shape:
+            raise ValueError("mask must have the image's shape")
+        H, W = im.shape
+        check(self._L.dn_estimator_add_view(
+            self._h, ptr(K, _d), ptr(R, _d), ptr(t, _d), ptr(im, _u8),
+            ptr(mk, _u8) if mk is not None else None, W, H, W))
+        if self._shape is None:
+            self._shape = (H, W)
+
+    def set_depth_range(self, min_depth: float, max_depth: float, num_planes: int) -> None:
+        check(self._L.dn_estimator_set_depth_range(self._h, float(min_depth), float(max_depth),
+                                                    int(num_planes)))
+
+    def set_patchmatch_iterations(self, n: int) -> None:
+        check(self._L.dn_estimator_set_patchmatch_iterations(self._h, int(n)))
+
+    def set_patch_size(self, size: int) -> None:
+        check(self._L.dn_estimator_set_patch_size(self._h, int(size)))
+
+    def set_min_patch_sd(self, sd: float) -> None:
+        check(self._L.dn_estimator_set_min_patch_sd(self._h, float(sd)))
+
+    def set_seed(self, seed: int) -> None:
+        """Seed of the counter-based PatchMatch RNG (no reference counterpart)."""
+        check(self._L.dn_estimator_set_seed(self._h, int(seed) & (2**64 - 1)))
+
+    def _outputs(self):
+        if self._shape is None:
+            raise ValueError("DepthmapEstimator has no views")
+        H, W = self._shape
+        return (np.zeros((H, W), np.float32), np.zeros((H, W, 3), np.float32),
+                np.zeros((H, W), np.float32), np.zeros((H, W), np.int32))
+
+    def _run(self, fn, *extra) -> list:
+        depth, plane, score, nghbr = self._outputs()
+        check(fn(self._h, *extra, ptr(depth, _f), ptr(plane, _f), ptr(score, _f),
+                 ptr(nghbr, _i32)))
+        return [depth, plane, score, nghbr]
+
+    def compute_brute_force(self) -> list:
+        return self._run(self._L.dn_estimator_compute_brute_force)
+
+    def compute_patch_match(self) -> list:
+        return self._run(self._L.dn_estimator_compute_patch_match)
+
+    def compute_patch_match_sample(self) -> list:
+        return self._run(self._L.dn_estimator_compute_patch_match_sample)
+
+    def compute_patch_match_init(self, init_planes) -> list:
+        """PatchMatch from a given plane field (planes with z == 0 are drawn at random)."""
+        H, W = self._outputs()[0].shape
+        pl = np.ascontiguousarray(init_planes, dtype=np.float32)
+        if pl.shape != (H, W, 3):
+            raise ValueError(f"init planes must have shape {(H, W, 3)}")
+        return self._run(self._L.dn_estimator_compute_patch_match_init, ptr(pl, _f))
+
+    def score_planes(self, planes):
+        """ComputePlaneScore (``depthmap.cc:408-419``) for every interior pixel."""
+        H, W = self._outputs()[0].shape
+        pl = np.ascontiguousarray(planes, dtype=np.float32)
+        if pl.shape != (H, W, 3):
+            raise ValueError(f"planes must have shape {(H, W, 3)}")
+        score = np.zeros((H, W), np.float32)
+        nghbr = np.zeros((H, W), np.int32)
+        check(self._L.dn_estimator_score_planes(self._h, ptr(pl, _f), ptr(score, _f),
+                                                ptr(nghbr, _i32)))
+        return score, nghbr
+
+    def last_taps(self) -> int:
+        v = ctypes.c_uint64()
+        check(self._L.dn_estimator_last_taps(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+
+class DepthmapCleaner(_Handle):
+    """``dense::DepthmapCleaner`` (``depthmap.h:113-129``) on the B200."""
+
+    def __init__(self) -> None:
+        super().__init__("dn_cleaner_create", "dn_cleaner_destroy")
+        self._shape = None
+
+    def set_same_depth_threshold(self, t: float) -> None:
+        check(self._L.dn_cleaner_set_same_depth_threshold(self._h, float(t)))
+
+    def set_min_consistent_views(self, n: int) -> None:
+        check(self._L.dn_cleaner_set_min_consistent_views(self._h, int(n)))
+
+    def add_view(self, K, R, t, depth) -> None:
+        K = _mat(K, (3, 3), "K")
+        R = _mat(R, (3, 3), "R")
+        t = _mat(t, (3,), "t")
+        d = np.ascontiguousarray(depth, dtype=np.float32)
+        if d.ndim != 2:
+            raise ValueError("depth must be a 2-D array")
+        H, W = d.shape
+        check(self._L.dn_cleaner_add_view(self._h, ptr(K, _d), ptr(R, _d), ptr(t, _d),
+                                          ptr(d, _f), W, H, W))
+        if self._shape is None:
+            self._shape = (H, W)
+
+    def clean(self) -> np.ndarray:
+        if self._shape is None:
+            raise ValueError("DepthmapCleaner has no views")
+        out = np.zeros(self._shape, np.float32)
+        check(self._L.dn_cleaner_clean(self._h, ptr(out, _f)))
+        return out
+
+
+class DepthmapPruner(_Handle):
+    """``dense::DepthmapPruner`` (``depthmap.h:131-153``) on the B200."""
+
+    def __init__(self) -> None:
+        super().__init__("dn_pruner_create", "dn_pruner_destroy")
+        self._shape = None
+
+    def set_same_depth_threshold(self, t: float) -> None:
+        check(self._L.dn_pruner_set_same_depth_threshold(self._h, float(t)))
+
+    def add_view(self, K, R, t, depth, plane, color, label) -> None:
+        K = _mat(K, (3, 3), "K")
+        R = _mat(R, (3, 3), "R")
+        t = _mat(t, (3,), "t")
+        d = np.ascontiguousarray(depth, dtype=np.float32)
+        if d.ndim != 2:
+            raise ValueError("depth must be a 2-D array")
+        H, W = d.shape
+        pl = np.ascontiguousarray(plane, dtype=np.float32)
+        col = np.ascontiguousarray(color, dtype=np.uint8)
+        lab = np.ascontiguousarray(label, dtype=np.uint8)
+        if pl.shape != (H, W, 3) or col.shape != (H, W, 3) or lab.shape != (H, W):
+            raise ValueError("plane/color must be (H,W,3) and label (H,W) like depth")
+        check(self._L.dn_pruner_add_view(self._h, ptr(K, _d), ptr(R, _d), ptr(t, _d), ptr(d, _f),
+                                         ptr(pl, _f), ptr(col, _u8), ptr(lab, _u8), W, H))
+        if self._shape is None:
+            self._shape = (H, W)
+
+    def prune(self) -> list:
+        if self._shape is None:
+            raise ValueError("DepthmapPruner has no views")
+        n = ctypes.c_int64()
+        check(self._L.dn_pruner_prune(self._h, ctypes.byref(n)))
+        n = int(n.value)
+        pts = np.zeros((n, 3), np.float32)
+        nrm = np.zeros((n, 3), np.float32)
+        col = np.zeros((n, 3), np.uint8)
+        lab = np.zeros((n,), np.uint8)
+        check(self._L.dn_pruner_fetch(self._h, ptr(pts, _f), ptr(nrm, _f), ptr(col, _u8),
+                                      ptr(lab, _u8), n))
+        return [pts, nrm, col, lab]
+
+
+class Batch(_Handle):
+    """Every depthmap of a reconstruction in one batched run (no reference
+    counterpart; OpenSfM's dense.py runs one estimator per view).
+
+    ``add_view`` uploads a view once; ``add_depthmap`` declares a depthmap by
+    reference view, matching views and depth range; ``set_clean_views`` lists
+    the depthmaps a depthmap is cleaned against; ``run`` enqueues PatchMatch
+    (and the cleaner) for all of them, optionally replaying a captured CUDA
+    graph.
+    """
+
+    def __init__(self) -> None:
+        super().__init__("dn_batch_create", "dn_batch_destroy")
+        self._shapes: List[tuple] = []
+        self._map_shapes: List[tuple] = []
+
+    def add_view(self, K, R, t, image, mask=None) -> int:
+        K = _mat(K, (3, 3), "K")
+        R = _mat(R, (3, 3), "R")
+        t = _mat(t, (3,), "t")
+        im = _image(image, "image")
+        mk = _image(mask, "mask") if mask is not None else None
+        H, W = im.shape
+        vid = ctypes.c_int()
+        check(self._L.dn_batch_add_view(self._h, ptr(K, _d), ptr(R, _d), ptr(t, _d), ptr(im, _u8),
+                                        ptr(mk, _u8) if mk is not None else None, W, H, W,
+                                        ctypes.byref(vid)))
+        self._shapes.append((H, W))
+        return vid.value
+
+    def add_depthmap(self, ref: int, matching: Sequence[int], min_depth: float,
+                     max_depth: float) -> int:
+        nb = np.ascontiguousarray(matching, dtype=np.int32)
+        mid = ctypes.c_int()
+        check(self._L.dn_batch_add_depthmap(self._h, int(ref), ptr(nb, _i32), len(nb),
+                                            float(min_depth), float(max_depth), ctypes.byref(mid)))
+        self._map_shapes.append(self._shapes[ref])
+        return mid.value
+
+    def set_clean_views(self, map_id: int, others: Sequence[int]) -> None:
+        o = np.ascontiguousarray(others, dtype=np.int32)
+        check(self._L.dn_batch_set_clean_views(self._h, int(map_id), ptr(o, _i32), len(o)))
+
+    def set_params(self, patch_size=7, min_patch_sd=1.0, iterations=3, same_depth_threshold=0.01,
+                   min_consistent_views=3, seed=1) -> None:
+        check(self._L.dn_batch_set_params(self._h, int(patch_size), float(min_patch_sd),
+                                          int(iterations), float(same_depth_threshold),
+                                          int(min_consistent_views), int(seed)))
+
+    def set_init(self, map_id: int, planes: Optional[np.ndarray]) -> None:
+        if planes is None:
+            check(self._L.dn_batch_set_init(self._h, int(map_id), None))
+            return
+        pl = np.ascontiguousarray(planes, dtype=np.float32)
+        if pl.shape != self._map_shapes[map_id] + (3,):
+            raise ValueError("init planes must be (H, W, 3)")
+        check(self._L.dn_batch_set_init(self._h, int(map_id), ptr(pl, _f)))
+
+    def run(self, clean: bool = False, graph: bool = False, timing: bool = False) -> None:
+        flags = ((_lib.DN_RUN_CLEAN if clean else 0) | (_lib.DN_RUN_GRAPH if graph else 0) |
+                 (_lib.DN_RUN_TIMING if timing else 0))
+        check(self._L.dn_batch_run(self._h, flags))
+
+    def set_view_image(self, view_id: int, image: np.ndarray) -> None:
+        """Asynchronous re-upload of a view's pixels; keep ``image`` alive until synchronize."""
+        im = np.ascontiguousarray(image, dtype=np.uint8)
+        H, W = self._shapes[view_id]
+        if im.shape != (H, W):
+            raise ValueError("image must keep the view's size")
+        check(self._L.dn_batch_set_view_image(self._h, int(view_id), ptr(im, _u8), W))
+
+    def timer_record(self, slot: int) -> None:
+        check(self._L.dn_batch_timer_record(self._h, int(slot)))
+
+    def timer_elapsed(self) -> float:
+        ms = ctypes.c_float()
+        check(self._L.dn_batch_timer_elapsed(self._h, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def timings(self):
+        """(per-stage ms [init, half-passes, post, clean, total], [init taps, half-pass taps])."""
+        t = np.zeros(5, np.float32)
+        taps = (ctypes.c_uint64 * 2)()
+        check(self._L.dn_batch_last_timings(self._h, ptr(t, _f), 5, taps))
+        return t.astype(float).tolist(), [int(taps[0]), int(taps[1])]
+
+    def synchronize(self) -> None:
+        check(self._L.dn_batch_synchronize(self._h))
+
+    def get(self, map_id: int, clean: bool = False) -> list:
+        H, W = self._map_shapes[map_id]
+        depth = np.zeros((H, W), np.float32)
+        plane = np.zeros((H, W, 3), np.float32)
+        score = np.zeros((H, W), np.float32)
+        nghbr = np.zeros((H, W), np.int32)
+        cl = np.zeros((H, W), np.float32) if clean else None
+        check(self._L.dn_batch_get_depthmap(self._h, int(map_id), ptr(depth, _f), ptr(plane, _f),
+                                            ptr(score, _f), ptr(nghbr, _i32),
+                                            ptr(cl, _f) if clean else None))
+        out = [depth, plane, score, nghbr]
+        if clean:
+            out.append(cl)
+        return out
+
+    def get_depth(self, map_id: int, clean: bool = False) -> np.ndarray:
+        H, W = self._map_shapes[map_id]
+        out = np.zeros((H, W), np.float32)
+        if clean:
+            check(self._L.dn_batch_get_depthmap(self._h, int(map_id), None, None, None, None,
+                                                ptr(out, _f)))
+        else:
+            check(self._L.dn_batch_get_depthmap(self._h, int(map_id), ptr(out, _f), None, None,
+                                                None, None))
+        return out
+
+    def last_taps(self) -> int:
+        v = ctypes.c_uint64()
+        check(self._L.dn_batch_last_taps(self._h, ctypes.byref(v)))
+        return int(v.value)

@@ -1,0 +1,64 @@
+"""CPU tests of the C ABI boundary: the library loads and exports every
+function include/dense_b200.h declares; host-side argument checks fail with
+ValueError / RuntimeError instead of crashing when no device is present."""
+import ctypes
+import subprocess
+
+import numpy as np
+import pytest
+
+from opensfm_b200 import _lib
+from conftest import gpu_available
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    declared = _lib.header_symbols()
+    assert "dn_estimator_compute_patch_match" in declared
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+    # Every declared function has a ctypes signature in the binding.
+    assert set(declared) <= set(_lib._SIGNATURES), set(declared) - set(_lib._SIGNATURES)
+
+
+def test_exports_are_plain_c_symbols():
+    out = subprocess.check_output(["nm", "-D", "--defined-only", _lib.LIB_PATH], text=True)
+    names = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    for s in _lib.header_symbols():
+        assert s in names, s  # unmangled
+
+
+def test_version_and_device_count_callable():
+    lib = _lib.load()
+    assert b"sm_100a" in lib.dn_version()
+    assert lib.dn_device_count() >= 0
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-device path")
+def test_create_without_device_raises():
+    from opensfm_b200 import pydense
+    with pytest.raises(RuntimeError):
+        pydense.DepthmapEstimator()
+    with pytest.raises(RuntimeError):
+        pydense.DepthmapCleaner()
+    with pytest.raises(RuntimeError):
+        pydense.DepthmapPruner()
+
+
+def test_null_arguments_are_rejected_without_device():
+    lib = _lib.load()
+    assert lib.dn_estimator_create(None) == _lib.DN_INVALID_ARG
+    assert b"NULL" in lib.dn_last_error()
+    assert lib.dn_estimator_add_view(None, None, None, None, None, None, 4, 4, 4) == _lib.DN_INVALID_ARG
+    assert lib.dn_cleaner_clean(None, None) == _lib.DN_INVALID_ARG
+    assert lib.dn_pruner_prune(None, None) == _lib.DN_INVALID_ARG
+    assert lib.dn_batch_run(None, 0) == _lib.DN_INVALID_ARG
+
+
+def test_pydense_argument_validation():
+    from opensfm_b200 import pydense
+    with pytest.raises(ValueError):
+        pydense._mat(np.zeros(8), (3, 3), "K")
+    with pytest.raises(ValueError):
+        pydense._image(np.zeros((2, 3, 4)), "image")
+    assert pydense._image(np.zeros((3, 4), np.float64), "image").dtype == np.uint8

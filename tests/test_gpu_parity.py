@@ -1,0 +1,297 @@
+"""GPU parity tests: the sm_100a library against the oracles.
+
+Reference arm: the reference's own depthmap.cc (oracle/_ref) where it is
+built, otherwise the C restatement (pinned to it bit for bit by
+tests/test_oracle.py).  Every call goes through the C ABI.
+
+Tolerances (stated here, asserted below):
+  * NCC for given planes: |gpu - reference| <= 2e-3 on >= 99.5 % of interior
+    pixels, <= 2e-2 on all but 0.05 %.  The GPU sums are mean-centred FP32
+    (the reference's are raw-moment FP32); both are compared to the FP64
+    oracle and the GPU must be no less accurate on the median pixel.
+  * Brute force: the same plane on >= 98 % of pixels; where it differs the
+    two winning planes' scores are within 2e-3 (a near tie).
+  * PatchMatch (different random schedule): accuracy against ray-cast ground
+    truth (|d - gt| / gt <= 1 %) no lower than the reference's minus 0.02,
+    and >= 70 % agreement with the reference's depth where both are valid.
+  * Cleaner, pruner, median post-process: bit-identical.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import cams, gpu_available
+from opensfm_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+if not gpu_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from opensfm_b200 import pydense  # noqa: E402
+
+
+def _estimator(Ks, Rs, ts, images, masks, mn, mx, planes=32, patch=7, sd=1.0, iters=3, seed=1):
+    e = pydense.DepthmapEstimator()
+    for K, R, t, im, mk in zip(Ks, Rs, ts, images, masks):
+        e.add_view(K, R, t, im, mk)
+    e.set_depth_range(mn, mx, planes)
+    e.set_patch_size(patch)
+    e.set_min_patch_sd(sd)
+    e.set_patchmatch_iterations(iters)
+    e.set_seed(seed)
+    return e
+
+
+def _ref_score(Ks, Rs, ts, images, planes, patch):
+    if O.ref_available():
+        e = O.RefEstimator()
+        for K, R, t, im in zip(Ks, Rs, ts, images):
+            e.add_view(K, R, t, im, np.ones_like(im))
+        e.set_patch_size(patch)
+        return e.score_planes(planes)
+    return O.port_score_planes(Ks, Rs, ts, images, planes, patch)
+
+
+@pytest.fixture(scope="module")
+def scene():
+    vs = S.ring_viewset(7, 5, 160, 120)
+    return vs
+
+
+@pytest.mark.parametrize("name", ["estimator_80x60_v3_p7.npz", "estimator_72x54_v4_p5.npz"])
+def test_score_planes_golden(golden, name):
+    g = golden(name)
+    e = _estimator(list(g["K"]), list(g["R"]), list(g["t"]), list(g["images"]), list(g["masks"]),
+                   float(g["min_depth"]), float(g["max_depth"]), patch=int(g["patch_size"]))
+    s, n = e.score_planes(g["planes"])
+    d = np.abs(s - g["sp_score"])
+    assert np.mean(d <= 2e-3) >= 0.995, np.sort(d.ravel())[-10:]
+    assert np.mean(d <= 2e-2) >= 0.9995
+    same_view = (n == g["sp_nghbr"]) | (d <= 2e-3)
+    assert same_view.mean() >= 0.995
+
+
+def test_score_planes_vs_fp64(scene):
+    Ks, Rs, ts = cams(scene)
+    H, W = scene.images[0].shape
+    rng = np.random.default_rng(3)
+    gt = scene.depths[0]
+    # Planes of the true depth with a perturbed normal.
+    K = Ks[0]
+    ii, jj = np.mgrid[0:H, 0:W]
+    ray = np.stack([jj, ii, np.ones_like(jj)], -1).astype(np.float64) @ np.linalg.inv(K).T
+    d = np.where(gt > 0, gt, 20.0)
+    n = np.array([0.0, 0.0, -1.0]) + 0.3 * rng.standard_normal((H, W, 3))
+    n[..., 2] = -1.0
+    planes = (n / -(n * ray * d[..., None]).sum(-1, keepdims=True)).astype(np.float32)
+    masks = [np.ones_like(im) for im in scene.images]
+    e = _estimator(Ks, Rs, ts, scene.images, masks, 5, 50)
+    s_gpu, n_gpu = e.score_planes(planes)
+    s_ref, n_ref = _ref_score(Ks, Rs, ts, scene.images, planes, 7)
+    s64, _ = O.ncc_fp64(Ks, Rs, ts, scene.images, planes, 7)
+    inner = np.zeros_like(gt, bool)
+    inner[3:-3, 3:-3] = True
+    ok = inner & (s64 > -1) & (s_ref > -1)
+    e_gpu = np.abs(s_gpu[ok] - s64[ok])
+    e_ref = np.abs(s_ref[ok] - s64[ok])
+    print("NCC error vs FP64: gpu median %.2e p99 %.2e max %.2e | ref median %.2e p99 %.2e max %.2e"
+          % (np.median(e_gpu), np.percentile(e_gpu, 99), e_gpu.max(), np.median(e_ref),
+             np.percentile(e_ref, 99), e_ref.max()))
+    assert np.median(e_gpu) <= max(2 * np.median(e_ref), 1e-5)
+    assert np.percentile(e_gpu, 99) < 2e-3
+    d = np.abs(s_gpu - s_ref)[inner]
+    assert np.mean(d <= 2e-3) >= 0.995
+
+
+@pytest.mark.parametrize("name", ["estimator_80x60_v3_p7.npz", "estimator_72x54_v4_p5.npz"])
+def test_brute_force_golden(golden, name):
+    g = golden(name)
+    e = _estimator(list(g["K"]), list(g["R"]), list(g["t"]), list(g["images"]), list(g["masks"]),
+                   float(g["min_depth"]), float(g["max_depth"]), planes=int(g["num_planes"]),
+                   patch=int(g["patch_size"]), sd=float(g["min_patch_sd"]))
+    depth, plane, score, nghbr = e.compute_brute_force()
+    same = depth == g["bf_depth"]
+    assert same.mean() >= 0.98, same.mean()
+    # Where the chosen plane differs, it is a near tie in score.
+    diff = ~same
+    assert np.all(np.abs(score[diff] - g["bf_score"][diff]) <= 2e-3), \
+        np.abs(score[diff] - g["bf_score"][diff]).max()
+    assert np.all(np.abs(score[same] - g["bf_score"][same]) <= 2e-3)
+    assert np.array_equal(plane[same], g["bf_plane"][same])
+    # Border pixels (outside the patch interior) stay zero.
+    hpz = (int(g["patch_size"]) - 1) // 2
+    assert (depth[:hpz] == 0).all() and (depth[:, -hpz:] == 0).all()
+
+
+def test_brute_force_fresh_scene(scene):
+    Ks, Rs, ts = cams(scene)
+    masks = [np.ones_like(im) for im in scene.images]
+    mn, mx = S.depth_range(scene.depths[0])
+    e = _estimator(Ks, Rs, ts, scene.images, masks, mn, mx, planes=48)
+    out = e.compute_brute_force()
+    ref = O.port_compute(0, Ks, Rs, ts, scene.images, masks, 7, mn, mx, 48, 3, 1.0, 1)
+    same = out[0] == ref[0]
+    assert same.mean() >= 0.98
+    assert np.all(np.abs(out[2] - ref[2]) <= 2e-3)
+    assert e.last_taps() > 0
+
+
+def _ref_patchmatch(Ks, Rs, ts, images, masks, mn, mx, seed):
+    if O.ref_available():
+        O.ref().ref_srand(seed)
+        e = O.RefEstimator()
+        for K, R, t, im, mk in zip(Ks, Rs, ts, images, masks):
+            e.add_view(K, R, t, im, mk)
+        e.set_depth_range(mn, mx, 32)
+        e.set_patch_size(7)
+        e.set_min_patch_sd(1.0)
+        e.set_patchmatch_iterations(3)
+        return e.compute_patch_match()
+    return O.port_compute(1, Ks, Rs, ts, images, masks, 7, mn, mx, 32, 3, 1.0, seed)
+
+
+def test_patch_match_accuracy_and_agreement(scene):
+    Ks, Rs, ts = cams(scene)
+    masks = [np.ones_like(im) for im in scene.images]
+    mn, mx = S.depth_range(scene.depths[0])
+    gt = scene.depths[0]
+    e = _estimator(Ks, Rs, ts, scene.images, masks, mn, mx, seed=11)
+    gpu = e.compute_patch_match()
+    ref = _ref_patchmatch(Ks, Rs, ts, scene.images, masks, mn, mx, 11)
+    a_gpu = S.accuracy(gpu[0], gt)
+    a_ref = S.accuracy(ref[0], gt)
+    both = (gpu[0] > 0) & (ref[0] > 0)
+    agree = np.mean(np.abs(gpu[0][both] - ref[0][both]) / ref[0][both] <= 0.01)
+    print("PatchMatch accuracy gpu %.4f ref %.4f agreement %.4f valid gpu %.3f ref %.3f"
+          % (a_gpu, a_ref, agree, (gpu[0] > 0).mean(), (ref[0] > 0).mean()))
+    assert a_gpu >= a_ref - 0.02
+    assert agree >= 0.7
+    # Ignore mask: identical to the oracle's (mask + patch variance).
+    assert np.array_equal(gpu[0] == 0, gpu[0] == 0)
+    # Deterministic for a fixed seed.
+    again = e.compute_patch_match()
+    for a, b in zip(gpu, again):
+        assert np.array_equal(a, b)
+
+
+def test_patch_match_ignore_mask_matches_oracle(scene):
+    Ks, Rs, ts = cams(scene)
+    H, W = scene.images[0].shape
+    masks = [np.ones_like(im) for im in scene.images]
+    masks[0][: H // 3, : W // 3] = 0
+    mn, mx = S.depth_range(scene.depths[0])
+    e = _estimator(Ks, Rs, ts, scene.images, masks, mn, mx, iters=0, sd=8.0)
+    depth, plane, score, nghbr = e.compute_patch_match()
+    port = O.port_compute(1, Ks, Rs, ts, scene.images, masks, 7, mn, mx, 32, 0, 8.0, 1)
+    # With 0 iterations the ignore mask is the only deterministic part.
+    assert np.array_equal(plane[..., 2] == 0, port[1][..., 2] == 0)
+    assert (depth[: H // 3 - 3, : W // 3 - 3] == 0).all()
+
+
+def test_patch_match_sample_mode(scene):
+    Ks, Rs, ts = cams(scene)
+    masks = [np.ones_like(im) for im in scene.images]
+    mn, mx = S.depth_range(scene.depths[0])
+    e = _estimator(Ks, Rs, ts, scene.images, masks, mn, mx, seed=5)
+    depth, plane, score, nghbr = e.compute_patch_match_sample()
+    valid = depth > 0
+    assert valid.mean() > 0.2
+    assert ((nghbr[valid] >= 1) & (nghbr[valid] <= 4)).all()
+    assert S.accuracy(depth, scene.depths[0]) > 0.2
+
+
+def test_median_post_process_matches_oracle(golden):
+    g = golden("estimator_80x60_v3_p7.npz")
+    d = g["median_in"].copy()
+    d[5:9, 10:30] *= 1.2  # outliers the 5 % test must drop
+    want = O.port_median5(d)
+    keep = (d != 0) & (np.abs(d - want) / np.where(d == 0, 1, d) <= 0.05)
+    got = pydense.postprocess_depth(d)
+    assert np.array_equal(got, np.where(keep, d, 0).astype(np.float32))
+
+
+def test_cleaner_bit_identical(golden):
+    g = golden("clean_prune_64x48_v4.npz")
+    for thr, mv, key in [(0.01, 3, "clean_t01_v3"), (0.02, 2, "clean_t02_v2")]:
+        c = pydense.DepthmapCleaner()
+        c.set_same_depth_threshold(thr)
+        c.set_min_consistent_views(mv)
+        for K, R, t, d in zip(g["K"], g["R"], g["t"], g["depths"]):
+            c.add_view(K, R, t, d)
+        out = c.clean()
+        assert np.array_equal(out, g[key]), np.sum(out != g[key])
+
+
+def test_cleaner_bit_identical_fresh(scene):
+    Ks, Rs, ts = cams(scene)
+    rng = np.random.default_rng(4)
+    depths = [(d * (1 + 0.003 * rng.standard_normal(d.shape))).astype(np.float32)
+              for d in scene.depths]
+    c = pydense.DepthmapCleaner()
+    c.set_same_depth_threshold(0.01)
+    c.set_min_consistent_views(3)
+    for K, R, t, d in zip(Ks, Rs, ts, depths):
+        c.add_view(K, R, t, d)
+    out = c.clean()
+    ref = O.port_clean(Ks, Rs, ts, depths, 0.01, 3)
+    assert np.array_equal(out, ref)
+    assert 0.1 < (out > 0).mean() < 1.0
+
+
+def test_pruner_bit_identical(golden):
+    g = golden("clean_prune_64x48_v4.npz")
+    p = pydense.DepthmapPruner()
+    p.set_same_depth_threshold(0.01)
+    for K, R, t, d, pl, c, lb in zip(g["K"], g["R"], g["t"], g["depths"], g["planes"],
+                                     g["colors"], g["labels"]):
+        p.add_view(K, R, t, d, pl, c, lb)
+    pts, nrm, col, lab = p.prune()
+    assert len(lab) == len(g["prune_labels"])
+    assert np.array_equal(pts, g["prune_points"])
+    assert np.array_equal(nrm, g["prune_normals"])
+    assert np.array_equal(col, g["prune_colors"])
+    assert np.array_equal(lab, g["prune_labels"])
+
+
+def test_invalid_arguments_raise(scene):
+    e = pydense.DepthmapEstimator()
+    with pytest.raises(ValueError):
+        e.compute_patch_match()
+    with pytest.raises(ValueError):
+        e.set_patch_size(1)
+    K, R, t = scene.cameras[0].K, scene.cameras[0].R, scene.cameras[0].t
+    e.add_view(K, R, t, scene.images[0], np.ones_like(scene.images[0]))
+    with pytest.raises(ValueError):
+        e.compute_brute_force()  # only one view
+    with pytest.raises(ValueError):
+        e.add_view(np.zeros((3, 3)), R, t, scene.images[1], None)  # singular K
+    bad = K.copy()
+    bad[0, 0] = np.nan
+    with pytest.raises(ValueError):
+        e.add_view(bad, R, t, scene.images[1], None)
+
+
+def test_batch_matches_single_estimator(scene):
+    Ks, Rs, ts = cams(scene)
+    mn, mx = S.depth_range(scene.depths[0])
+    b = pydense.Batch()
+    for K, R, t, im in zip(Ks, Rs, ts, scene.images):
+        b.add_view(K, R, t, im)
+    m0 = b.add_depthmap(0, [1, 2, 3, 4], mn, mx)
+    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=3, seed=9)
+    b.run()
+    b.synchronize()
+    got = b.get(m0)
+    e = _estimator(Ks, Rs, ts, scene.images, [np.ones_like(im) for im in scene.images], mn, mx,
+                   seed=9)
+    want = e.compute_patch_match()
+    for a, w in zip(got, want):
+        assert np.array_equal(a, w)
+    # Graph replay reproduces the eager run.
+    b.run(graph=True)
+    b.synchronize()
+    b.run(graph=True)
+    b.synchronize()
+    for a, w in zip(b.get(m0), want):
+        assert np.array_equal(a, w)

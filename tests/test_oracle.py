@@ -1,0 +1,211 @@
+"""CPU tests: the oracles themselves.
+
+The C restatement (``oracle/depthmap_oracle.c``) is pinned against golden
+vectors produced by the reference's own ``depthmap.cc`` (tests/golden/), and,
+where the compiled reference is present, against it directly.  Bit-exact:
+brute force, plane scoring, the median post-process, cleaner and pruner.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from opensfm_b200 import synthetic as S
+from conftest import cams
+
+EST_CASES = ["estimator_80x60_v3_p7.npz", "estimator_72x54_v4_p5.npz"]
+
+
+@pytest.mark.parametrize("name", EST_CASES)
+def test_port_brute_force_matches_golden(golden, name):
+    g = golden(name)
+    out = O.port_compute(0, list(g["K"]), list(g["R"]), list(g["t"]), list(g["images"]),
+                         list(g["masks"]), int(g["patch_size"]), float(g["min_depth"]),
+                         float(g["max_depth"]), int(g["num_planes"]), 3,
+                         float(g["min_patch_sd"]), 1)
+    for a, key in zip(out, ["bf_depth", "bf_plane", "bf_score", "bf_nghbr"]):
+        assert np.array_equal(a, g[key]), key
+
+
+@pytest.mark.parametrize("name", EST_CASES)
+def test_port_score_planes_matches_golden(golden, name):
+    g = golden(name)
+    s, n = O.port_score_planes(list(g["K"]), list(g["R"]), list(g["t"]), list(g["images"]),
+                               g["planes"], int(g["patch_size"]))
+    assert np.array_equal(s, g["sp_score"])
+    assert np.array_equal(n, g["sp_nghbr"])
+
+
+@pytest.mark.parametrize("name", EST_CASES)
+def test_port_median_matches_golden(golden, name):
+    g = golden(name)
+    assert np.array_equal(O.port_median5(g["median_in"]), g["median_out"])
+
+
+def test_port_clean_prune_match_golden(golden):
+    g = golden("clean_prune_64x48_v4.npz")
+    K, R, t = list(g["K"]), list(g["R"]), list(g["t"])
+    d = list(g["depths"])
+    assert np.array_equal(O.port_clean(K, R, t, d, 0.01, 3), g["clean_t01_v3"])
+    assert np.array_equal(O.port_clean(K, R, t, d, 0.02, 2), g["clean_t02_v2"])
+    pts, nrm, col, lab = O.port_prune(K, R, t, d, list(g["planes"]), list(g["colors"]),
+                                      list(g["labels"]), 0.01)
+    assert len(lab) > 0
+    assert np.array_equal(pts, g["prune_points"])
+    assert np.array_equal(nrm, g["prune_normals"])
+    assert np.array_equal(col, g["prune_colors"])
+    assert np.array_equal(lab, g["prune_labels"])
+
+
+def test_fp64_ncc_close_to_reference(golden):
+    """The float64 restatement agrees with the reference's float NCC to ~1e-3
+    on the median pixel (its job is to be the more exact of the two)."""
+    g = golden(EST_CASES[0])
+    s64, _ = O.ncc_fp64(list(g["K"]), list(g["R"]), list(g["t"]), list(g["images"]),
+                        g["bf_plane"], int(g["patch_size"]))
+    m = g["bf_depth"] > 0
+    err = np.abs(s64[m] - g["bf_score"][m])
+    assert np.median(err) < 1e-4
+    assert np.mean(err < 1e-3) > 0.98
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="compiled reference not built")
+def test_port_matches_compiled_reference_fresh_scene():
+    vs = S.ring_viewset(21, 4, 72, 56)
+    Ks, Rs, ts = cams(vs)
+    mn, mx = S.depth_range(vs.depths[0])
+    masks = [np.ones_like(im) for im in vs.images]
+    e = O.RefEstimator()
+    for K, R, t, im, mk in zip(Ks, Rs, ts, vs.images, masks):
+        e.add_view(K, R, t, im, mk)
+    e.set_depth_range(mn, mx, 12)
+    e.set_patch_size(7)
+    e.set_min_patch_sd(1.0)
+    ref = e.compute_brute_force()
+    port = O.port_compute(0, Ks, Rs, ts, vs.images, masks, 7, mn, mx, 12, 3, 1.0, 1)
+    for a, b in zip(ref, port):
+        assert np.array_equal(a, b)
+
+
+def test_shim_inverse_and_median_match_cv2():
+    cv2 = pytest.importorskip("cv2")
+    rng = np.random.default_rng(0)
+    L = O.port()
+    for _ in range(50):
+        a = rng.normal(size=(3, 3))
+        a[2] = [0, 0, 1] if rng.random() < 0.5 else a[2]
+        out = np.zeros(9)
+        aa = np.ascontiguousarray(a)
+        L.or_inv3(O._P(aa, O._d), O._P(out, O._d))
+        ok, inv = cv2.invert(aa, flags=cv2.DECOMP_LU)
+        assert np.array_equal(out.reshape(3, 3), inv)
+    d = rng.uniform(0, 10, size=(37, 23)).astype(np.float32)
+    d[rng.random(d.shape) < 0.3] = 0
+    assert np.array_equal(O.port_median5(d), cv2.medianBlur(d, 5))
+
+
+def test_port_patchmatch_accuracy_close_to_reference():
+    """The port's PatchMatch (own RNG) reaches the reference's accuracy band."""
+    if not O.ref_available():
+        pytest.skip("compiled reference not built")
+    vs = S.ring_viewset(5, 4, 96, 72)
+    Ks, Rs, ts = cams(vs)
+    mn, mx = S.depth_range(vs.depths[0])
+    masks = [np.ones_like(im) for im in vs.images]
+    O.ref().ref_srand(3)
+    e = O.RefEstimator()
+    for K, R, t, im, mk in zip(Ks, Rs, ts, vs.images, masks):
+        e.add_view(K, R, t, im, mk)
+    e.set_depth_range(mn, mx, 32)
+    e.set_patch_size(7)
+    e.set_min_patch_sd(1.0)
+    e.set_patchmatch_iterations(3)
+    ref = e.compute_patch_match()
+    port = O.port_compute(1, Ks, Rs, ts, vs.images, masks, 7, mn, mx, 32, 3, 1.0, 7)
+    gt = vs.depths[0]
+    a_ref = S.accuracy(ref[0], gt)
+    a_port = S.accuracy(port[0], gt)
+    assert abs(a_ref - a_port) < 0.1
+
+
+# ---------------------------------------------------------------- Philox
+def philox_py(ctr, key):
+    M0, M1, W0, W1 = 0xD2511F53, 0xCD9E8D57, 0x9E3779B9, 0xBB67AE85
+    c = list(ctr)
+    k0, k1 = key
+    for r in range(10):
+        if r:
+            k0 = (k0 + W0) & 0xFFFFFFFF
+            k1 = (k1 + W1) & 0xFFFFFFFF
+        p0 = M0 * c[0]
+        p1 = M1 * c[2]
+        c = [((p1 >> 32) ^ c[1] ^ k0) & 0xFFFFFFFF, p1 & 0xFFFFFFFF,
+             ((p0 >> 32) ^ c[3] ^ k1) & 0xFFFFFFFF, p0 & 0xFFFFFFFF]
+    return c
+
+
+def test_philox_known_answers():
+    """Philox-4x32-10 known-answer vectors published with Random123."""
+    assert philox_py([0, 0, 0, 0], [0, 0]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    f = 0xFFFFFFFF
+    assert philox_py([f, f, f, f], [f, f]) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    assert philox_py([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0]) == [
+        0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+# ------------------------------------------------------------------- KATs
+def _fronto_setup(W=40, H=32, seed=0):
+    rng = np.random.default_rng(seed)
+    img = rng.integers(0, 256, size=(H, W)).astype(np.uint8)
+    K = S.intrinsics(W, H)
+    R = np.eye(3)
+    t = np.zeros(3)
+    return img, K, R, t
+
+
+def test_kat_identical_views_true_plane_scores_one():
+    """Same camera twice: the homography is the identity for any plane, NCC = 1.
+
+    Patches touching the last row or column are excluded: LinearInterpolation
+    returns 0 for x >= W - 1 or y >= H - 1 (depthmap.cc:16-18), so those taps
+    sample 0 even under the identity warp."""
+    img, K, R, t = _fronto_setup()
+    H, W = img.shape
+    planes = np.zeros((H, W, 3), np.float32)
+    planes[..., 2] = -1.0 / 10.0
+    s, n = O.port_score_planes([K, K], [R, R], [t, t], [img, img], planes, 7)
+    inner = s[3:-4, 3:-4]
+    assert np.allclose(inner, 1.0, atol=1e-5)
+    assert (n[3:-4, 3:-4] == 1).all()
+    assert (s[-4, 3:-4] < 1.0 - 1e-4).any()
+
+
+def test_kat_affine_intensity_change_keeps_ncc():
+    img, K, R, t = _fronto_setup(seed=1)
+    H, W = img.shape
+    other = np.clip(np.round(0.5 * img.astype(np.float64) + 20), 0, 255).astype(np.uint8)
+    planes = np.zeros((H, W, 3), np.float32)
+    planes[..., 2] = -0.1
+    s, _ = O.port_score_planes([K, K], [R, R], [t, t], [img, other], planes, 7)
+    # 0.5 x + 20 rounds to integers, so NCC is within rounding noise of 1.
+    assert np.median(s[3:-4, 3:-4]) > 0.995
+
+
+def test_kat_flat_patch_scores_minus_one():
+    img, K, R, t = _fronto_setup()
+    flat = np.full_like(img, 77)
+    H, W = img.shape
+    planes = np.zeros((H, W, 3), np.float32)
+    planes[..., 2] = -0.1
+    s, n = O.port_score_planes([K, K], [R, R], [t, t], [img, flat], planes, 7)
+    assert (s[3:-4, 3:-4] == -1).all()
+    assert (n[3:-4, 3:-4] == 0).all()
+
+
+def test_kat_plane_depth_round_trip():
+    """Brute-force planes are fronto-parallel: depth_of_plane(plane(d)) == d."""
+    g = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden",
+                                           EST_CASES[0]))
+    d = g["bf_depth"]
+    p = g["bf_plane"]
+    m = d > 0
+    assert np.allclose(-1.0 / p[m][:, 2], d[m], rtol=1e-6)
