@@ -233,17 +233,18 @@ def cpu_sample(work, seconds=20.0, cores=None, seed=0):
 
 
 # ----------------------------------------------------------------- our arm
-def build_batch(work, seed=1):
+def build_batch(work, seed=1, n_maps=None):
     from opensfm_b200 import pydense
 
     vs, ranges, cands, matches = work
+    n_maps = n_maps or len(vs.cameras)
     b = pydense.Batch()
     for c, im in zip(vs.cameras, vs.images):
         b.add_view(c.K, c.R, c.t, im)
-    for v in range(len(vs.cameras)):
+    for v in range(n_maps):
         b.add_depthmap(v, matches[v], ranges[v][0], ranges[v][1])
-    for v in range(len(vs.cameras)):
-        b.set_clean_views(v, cands[v])
+    for v in range(n_maps):
+        b.set_clean_views(v, [o for o in cands[v] if o < n_maps])
     b.set_params(patch_size=PATCH, min_patch_sd=MIN_SD, iterations=ITERS,
                  same_depth_threshold=0.01, min_consistent_views=3, seed=seed)
     return b
@@ -258,8 +259,11 @@ def run_ours(args):
     _lib.check(_lib.load().dn_set_device(local))
     work = make_workload()
     vs, ranges, cands, matches = work
-    b = build_batch(work)
-    n_maps = len(vs.cameras)
+    n_maps = args.maps or len(vs.cameras)
+    b = build_batch(work, n_maps=n_maps)
+    if args.tuning:
+        bx, by, var = (int(x) for x in args.tuning.split(","))
+        b.set_tuning(bx, by, var)
 
     # Warm-up (graph capture on the first run).
     for _ in range(args.warmup):
@@ -302,7 +306,7 @@ def run_ours(args):
     b.synchronize()
     b.timer_record(0)
     for _ in range(args.steps):
-        for v, im in enumerate(imgs):
+        for v, im in enumerate(imgs[:n_maps]):
             b.set_view_image(v, im)
         b.run(clean=True, graph=True)
         for v in range(n_maps):
@@ -337,7 +341,8 @@ def run_ours(args):
             "algorithmic": f"{FLOPS_PER_TAP} flops per NCC tap x {taps[1]} taps in "
                            f"{2 * ITERS} half-passes ({hp_ms:.2f} ms)",
         },
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(sum(im.nbytes for im in imgs)),
+        "e2e": {"value": e2e, "unit": UNIT,
+                "h2d_bytes_per_step": int(sum(im.nbytes for im in imgs[:n_maps])),
                 "d2h_bytes_per_step": int(n_maps * out.nbytes)},
         "gpu_launches": None,
         "clocks": {k: v for k, v in clk.summary().items()},
@@ -395,6 +400,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tuning", default="", help="bx,by,variant (default: library default)")
+    ap.add_argument("--maps", type=int, default=0,
+                    help="depthmaps per step (default: all 24; smaller for profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -197,6 +197,13 @@ dn_status dn_batch_set_view_image(dn_batch* b, int view_id, const uint8_t* image
  * out[3] cleaner, out[4] whole run.  taps_out (may be NULL) receives the
  * NCC taps of init (taps_out[0]) and of the half-passes (taps_out[1]). */
 dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_out);
+/* Launch tuning (no reference counterpart): thread block shape bx x by
+ * (bx * by <= 128, bx a multiple of 32) and the lanes that share one pixel
+ * in the initialisation and PatchMatch kernels (1, 2 or 4; 2 and 4 apply to
+ * the 7 x 7 patch).  Chosen by opensfm_b200.autotune; scores agree between
+ * settings to float rounding of the sums. */
+dn_status dn_batch_set_tuning(dn_batch* b, int bx, int by, int variant);
+dn_status dn_estimator_set_tuning(dn_estimator* est, int bx, int by, int variant);
 /* Device timer on the batch stream: record event `slot` (0 or 1), and the
  * elapsed ms between the two recorded events (after dn_batch_synchronize). */
 dn_status dn_batch_timer_record(dn_batch* b, int slot);

@@ -84,6 +84,8 @@ _SIGNATURES = {
     "dn_batch_last_timings": ([_vp, _f, _i, ctypes.POINTER(ctypes.c_uint64)], _i),
     "dn_batch_copy_depth_device": ([_vp, _i, _vp], _i),
     "dn_batch_timer_record": ([_vp, _i], _i),
+    "dn_batch_set_tuning": ([_vp, _i, _i, _i], _i),
+    "dn_estimator_set_tuning": ([_vp, _i, _i, _i], _i),
     "dn_batch_timer_elapsed": ([_vp, _f], _i),
     "dn_postprocess_depth": ([_f, _f, _i, _i], _i),
     "dn_fp32_peak": ([ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], _i),

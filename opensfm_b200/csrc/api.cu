@@ -189,11 +189,12 @@ struct Engine {
   float same_depth_thr = 0.01f;
   int min_consistent = 2;
   int bx = 32, by = 4;  // thread block shape
+  int variant = 4;      // lanes per pixel in init / half-passes (1, 2, 4)
   DevBuf<dn::ViewDev> d_views;
   DevBuf<dn::PairDev> d_pairs;
   DevBuf<dn::MapDev> d_maps;
-  DevBuf<int4> d_tiles1, d_tiles2;
-  int n_tiles1 = 0, n_tiles2 = 0;
+  DevBuf<int4> d_tiles1, d_tiles2, d_tiles_init;
+  int n_tiles1 = 0, n_tiles2 = 0, n_tiles_init = 0;
   DevBuf<unsigned long long> d_taps;
   DevBuf<int> d_error;
   DevBuf<dn::CleanView> d_clean_views;
@@ -333,7 +334,8 @@ struct Engine {
     }
     std::vector<dn::PairDev> hp;
     std::vector<dn::MapDev> hm(maps.size());
-    std::vector<int4> t1, t2;
+    std::vector<int4> t1, t2, ti;
+    const int lanes = (patch == 7) ? variant : 1;
     for (size_t mi = 0; mi < maps.size(); ++mi) {
       Map& m = *maps[mi];
       const View& r = *views[m.ref];
@@ -387,11 +389,14 @@ struct Engine {
         hp.push_back(p);
       }
       hm[mi] = d;
+      const int px = bx / lanes;  // pixels per warp row in init / half-passes
       const int tx1 = (r.W + bx - 1) / bx, ty1 = (r.H + by - 1) / by;
-      const int tx2 = (r.W + 2 * bx - 1) / (2 * bx);
+      const int tx2 = (r.W + 2 * px - 1) / (2 * px);
+      const int txi = (r.W + px - 1) / px;
       for (int y = 0; y < ty1; ++y) {
         for (int x = 0; x < tx1; ++x) t1.push_back(make_int4((int)mi, x, y, 0));
         for (int x = 0; x < tx2; ++x) t2.push_back(make_int4((int)mi, x, y, 0));
+        for (int x = 0; x < txi; ++x) ti.push_back(make_int4((int)mi, x, y, 0));
       }
     }
     DN_CUDA(d_views.alloc(std::max<size_t>(hv.size(), 1)));
@@ -399,6 +404,7 @@ struct Engine {
     DN_CUDA(d_maps.alloc(std::max<size_t>(hm.size(), 1)));
     DN_CUDA(d_tiles1.alloc(std::max<size_t>(t1.size(), 1)));
     DN_CUDA(d_tiles2.alloc(std::max<size_t>(t2.size(), 1)));
+    DN_CUDA(d_tiles_init.alloc(std::max<size_t>(ti.size(), 1)));
     DN_CUDA(cudaMemcpyAsync(d_views.p, hv.data(), hv.size() * sizeof(dn::ViewDev),
                             cudaMemcpyHostToDevice, stream));
     if (!hp.empty())
@@ -410,9 +416,12 @@ struct Engine {
                             cudaMemcpyHostToDevice, stream));
     DN_CUDA(cudaMemcpyAsync(d_tiles2.p, t2.data(), t2.size() * sizeof(int4),
                             cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaMemcpyAsync(d_tiles_init.p, ti.data(), ti.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, stream));
     DN_CUDA(cudaStreamSynchronize(stream));
     n_tiles1 = (int)t1.size();
     n_tiles2 = (int)t2.size();
+    n_tiles_init = (int)ti.size();
     dirty = false;
     return DN_OK;
   }
@@ -435,6 +444,7 @@ struct Engine {
     a.p.min_consistent = min_consistent;
     a.p.taps = d_taps.p;
     a.p.error = d_error.p;
+    a.p.variant = variant;
     return a;
   }
 
@@ -464,7 +474,10 @@ struct Engine {
       return DN_OK;
     }
     const bool sample = (mode == Mode::kPatchMatchSample);
-    DN_CUDA(dn::launch_stage(dn::Stage::kInit, sample, a1, stream));
+    dn::LaunchArgs ai = a1;
+    ai.tiles = d_tiles_init.p;
+    ai.n_tiles = n_tiles_init;
+    DN_CUDA(dn::launch_stage(dn::Stage::kInit, sample, ai, stream));
     DN_TRY(mark(1, timing));
     dn::LaunchArgs a2 = args(true);
     a2.p.taps = d_taps.p + 1;
@@ -1160,6 +1173,24 @@ dn_status dn_batch_set_view_image(dn_batch* b, int view_id, const uint8_t* image
 dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_out) {
   DN_CHECK(b, "NULL batch");
   return b->eng.timings(out, n, taps_out);
+}
+static dn_status set_tuning(Engine& e, int bx, int by, int variant) {
+  DN_CHECK(bx >= 32 && bx % 32 == 0 && by >= 1 && bx * by <= 128,
+           "block shape must have bx a multiple of 32 and bx * by <= 128");
+  DN_CHECK(variant == 1 || variant == 2 || variant == 4, "lanes per pixel must be 1, 2 or 4");
+  e.bx = bx;
+  e.by = by;
+  e.variant = variant;
+  e.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_tuning(dn_batch* b, int bx, int by, int variant) {
+  DN_CHECK(b, "NULL batch");
+  return set_tuning(b->eng, bx, by, variant);
+}
+dn_status dn_estimator_set_tuning(dn_estimator* est, int bx, int by, int variant) {
+  DN_CHECK(est, "NULL estimator");
+  return set_tuning(est->eng, bx, by, variant);
 }
 dn_status dn_batch_timer_record(dn_batch* b, int slot) {
   DN_CHECK(b, "NULL batch");

@@ -14,6 +14,9 @@ namespace dn {
 // the per-tap weights live in registers, (2 HPZ + 1)^2 x 2 of them.
 template <int HPZ>
 constexpr int kMinBlocks = HPZ <= 2 ? 4 : (HPZ == 3 ? 3 : 2);
+// With L lanes per pixel each lane keeps 2 x 56 / L weights.
+template <int HPZ, int L>
+constexpr int kMinBlocksL = L == 1 ? kMinBlocks<HPZ> : (L == 2 ? 4 : 6);
 
 // ----------------------------------------------------------------------
 // Per-view preparation.
@@ -99,8 +102,11 @@ __device__ inline float patch_variance(const float* tile, int pitch, int ly, int
 // Initialisation: RandomInitialization + ComputeIgnoreMask
 // (depthmap.cc:237-269), or a given plane field (learned proposal).
 
-template <int HPZ, bool SAMPLE>
-__global__ void __launch_bounds__(128, kMinBlocks<HPZ>)
+// L lanes per pixel (L = 1, or 2 / 4 for the 7 x 7 patch): lane group g of
+// a warp row owns one pixel; every lane of a group computes the same values
+// and lane 0 writes them.
+template <int HPZ, bool SAMPLE, int L>
+__global__ void __launch_bounds__(128, (kMinBlocksL<HPZ, L>))
 init_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
             const PairDev* __restrict__ pairs, const int4* __restrict__ tiles, RunParams p) {
   extern __shared__ float tile[];
@@ -108,15 +114,19 @@ init_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
   const MapDev& m = maps[tl.x];
   const ViewDev& rv = views[m.ref_view];
   const int W = m.W, H = m.H;
-  const int x0 = tl.y * blockDim.x, y0 = tl.z * blockDim.y;
-  const int pitch = blockDim.x + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  const int px = blockDim.x / L;  // pixels per warp row
+  const int x0 = tl.y * px, y0 = tl.z * blockDim.y;
+  const int pitch = px + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
   stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
   __syncthreads();
-  const int i = y0 + threadIdx.y, j = x0 + threadIdx.x;
+  const int g = threadIdx.x / L, lane = threadIdx.x % L;
+  const unsigned mask = (L == 1) ? (1u << (threadIdx.x & 31))
+                                 : (((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1)));
+  const int i = y0 + threadIdx.y, j = x0 + g;
   unsigned taps = 0;
   if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) {
     const size_t pix = (size_t)i * W + j;
-    const int ly = threadIdx.y + HPZ, lx = threadIdx.x + HPZ;
+    const int ly = threadIdx.y + HPZ, lx = g + HPZ;
     const bool masked = rv.mask && rv.mask[pix] == 0;
     const bool low = patch_variance<HPZ>(tile, pitch, ly, lx) < p.min_var;
     float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -139,21 +149,24 @@ init_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
         const float3 n = make_float3(fmaf(2.f, u01(r.y), -1.f), fmaf(2.f, u01(r.z), -1.f), -1.f);
         v = plane_from_depth_normal((float)j, (float)i, m.Kinv_d, depth, n);
       }
-      RefPatch<HPZ> rp;
-      ref_patch_from_tile<HPZ>(rp, tile, pitch, ly, lx);
+      Patch<HPZ, L> pt;
+      pt.build(tile, pitch, ly, lx, lane, mask);
       const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
       if (SAMPLE) {
         nb = 1 + (int)(r.w % (uint32_t)m.n_pairs);
         const PairDev& pr = pairs[m.pair0 + nb - 1];
-        sc = ncc_view<HPZ>(rp, views[pr.view], pr, h, (float)j, (float)i, taps);
+        sc = pt.view(views[pr.view], pr, h, (float)j, (float)i, taps);
       } else {
-        sc = ncc_max<HPZ>(rp, views, pairs + m.pair0, m.n_pairs, h, (float)j, (float)i, nb, taps);
+        sc = patch_max<HPZ, L>(pt, views, pairs + m.pair0, m.n_pairs, h, (float)j, (float)i, nb,
+                               taps);
       }
       st = make_float4(v.x, v.y, v.z, depth);
     }
-    m.state[pix] = st;
-    m.score[pix] = sc;
-    m.nghbr[pix] = nb;
+    if (lane == 0) {
+      m.state[pix] = st;
+      m.score[pix] = sc;
+      m.nghbr[pix] = nb;
+    }
   }
   flush_taps(taps, p.taps);
 }
@@ -262,8 +275,8 @@ score_planes_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__
 // A candidate whose plane equals the current plane bit for bit is skipped:
 // its score at this pixel is the current score.
 
-template <int HPZ, bool SAMPLE>
-__global__ void __launch_bounds__(128, kMinBlocks<HPZ>)
+template <int HPZ, bool SAMPLE, int L>
+__global__ void __launch_bounds__(128, (kMinBlocksL<HPZ, L>))
 halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
                 const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
                 RunParams p) {
@@ -272,19 +285,23 @@ halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ vie
   const MapDev& m = maps[tl.x];
   const ViewDev& rv = views[m.ref_view];
   const int W = m.W, H = m.H;
-  const int x0 = tl.y * (2 * blockDim.x), y0 = tl.z * blockDim.y;
-  const int pitch = 2 * blockDim.x + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  const int px = blockDim.x / L;  // pixels per warp row
+  const int x0 = tl.y * (2 * px), y0 = tl.z * blockDim.y;
+  const int pitch = 2 * px + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
   stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
   __syncthreads();
+  const int g = threadIdx.x / L, lane = threadIdx.x % L;
+  const unsigned mask = (L == 1) ? (1u << (threadIdx.x & 31))
+                                 : (((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1)));
   const int i = y0 + threadIdx.y;
-  const int j = x0 + 2 * threadIdx.x + ((i + p.colour) & 1);
+  const int j = x0 + 2 * g + ((i + p.colour) & 1);
   unsigned taps = 0;
   const size_t pix = (size_t)i * W + j;
   float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
   if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) st = m.state[pix];
   if (st.w != 0.0f) {
-    RefPatch<HPZ> rp;
-    ref_patch_from_tile<HPZ>(rp, tile, pitch, threadIdx.y + HPZ, (j - x0) + HPZ);
+    Patch<HPZ, L> pt;
+    pt.build(tile, pitch, threadIdx.y + HPZ, (j - x0) + HPZ, lane, mask);
     const float fj = (float)j, fi = (float)i;
     float cur = m.score[pix];
     int curn = m.nghbr[pix];
@@ -301,9 +318,9 @@ halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ vie
         nb = view;
         if (nb < 1 || nb > m.n_pairs) return;
         const PairDev& pr = mp[nb - 1];
-        s = ncc_view<HPZ>(rp, views[pr.view], pr, h, fj, fi, taps);
+        s = pt.view(views[pr.view], pr, h, fj, fi, taps);
       } else {
-        s = ncc_max<HPZ>(rp, views, mp, m.n_pairs, h, fj, fi, nb, taps);
+        s = patch_max<HPZ, L>(pt, views, mp, m.n_pairs, h, fj, fi, nb, taps);
       }
       if (s > cur) {
         cur = s;
@@ -313,80 +330,83 @@ halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ vie
       }
     };
 
-    const int di[4] = {-1, 0, 1, 0}, dj[4] = {0, -1, 0, 1};
-#pragma unroll 1
-    for (int d = 0; d < 4; ++d) {
-      const int qi = i + di[d], qj = j + dj[d];
-      const size_t q = (size_t)qi * W + qj;
-      const float4 sq = m.state[q];
-      if (sq.w != 0.0f) try_plane(make_float3(sq.x, sq.y, sq.z), SAMPLE ? m.nghbr[q] : 0);
-    }
-#pragma unroll 1
-    for (int d = 0; d < 4; ++d) {
-      float bs = -3.0f;
-      long bq = -1;
-      for (int k = 0; k < kFarSamples; ++k) {
-        const int dist = kFarStart + 2 * k;
-        const int qi = i + di[d] * dist, qj = j + dj[d] * dist;
-        if (qi < 0 || qi >= H || qj < 0 || qj >= W) break;
-        const size_t q = (size_t)qi * W + qj;
-        const float sq = m.score[q];
-        if (sq > bs && m.state[q].w != 0.0f) {
-          bs = sq;
-          bq = (long)q;
-        }
-      }
-      if (bq >= 0) {
-        const float4 sq = m.state[bq];
-        try_plane(make_float3(sq.x, sq.y, sq.z), SAMPLE ? m.nghbr[bq] : 0);
-      }
-    }
-    // Refinement draws: 18 normals from 5 Philox blocks.
-    uint32_t rnd[20];
-#pragma unroll
-    for (int b = 0; b < 5; ++b) {
-      const uint4 r = philox4x32_10(make_uint4((uint32_t)pix, (uint32_t)tl.x, (uint32_t)p.pass,
-                                               (uint32_t)b), p.seed_lo, p.seed_hi);
-      rnd[4 * b] = r.x;
-      rnd[4 * b + 1] = r.y;
-      rnd[4 * b + 2] = r.z;
-      rnd[4 * b + 3] = r.w;
-    }
-    float z[18];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      const float2 g = normal2(rnd[2 * k], rnd[2 * k + 1]);
-      z[2 * k] = g.x;
-      z[2 * k + 1] = g.y;
-    }
-    const int refn = curn;
+    // One evaluation site for all 14 candidate slots keeps the kernel's code
+    // small and the warp's lanes at the same slot: 0-3 adjacent pixels,
+    // 4-7 far samples, 8-13 refinements.
+    int refn = curn;
     float depth_range = 0.02f, normal_range = 0.5f;
 #pragma unroll 1
-    for (int k = 0; k < 6; ++k) {
-      if (cv.z == 0.0f) continue;
-      const float depth = cd * expf(depth_range * z[3 * k]);
-      const float3 n = make_float3(-cv.x / cv.z + normal_range * z[3 * k + 1],
-                                   -cv.y / cv.z + normal_range * z[3 * k + 2], -1.0f);
-      const float3 v = plane_from_depth_normal(fj, fi, m.Kinv_d, depth, n);
-      try_plane(v, refn);
-      depth_range *= 0.3f;
-      normal_range *= 0.8f;
+    for (int slot = 0; slot < 14; ++slot) {
+      float3 v = make_float3(0.f, 0.f, 0.f);
+      int view = 0;
+      bool valid = false;
+      if (slot < 8) {
+        const int d = slot & 3;
+        const int di = (d == 0) ? -1 : (d == 2 ? 1 : 0);
+        const int dj = (d == 1) ? -1 : (d == 3 ? 1 : 0);
+        long q = -1;
+        if (slot < 4) {
+          q = (long)(i + di) * W + (j + dj);
+        } else {
+          float bs = -3.0f;
+          for (int k = 0; k < kFarSamples; ++k) {
+            const int dist = kFarStart + 2 * k;
+            const int qi = i + di * dist, qj = j + dj * dist;
+            if (qi < 0 || qi >= H || qj < 0 || qj >= W) break;
+            const long qq = (long)qi * W + qj;
+            const float sq = m.score[qq];
+            if (sq > bs && m.state[qq].w != 0.0f) {
+              bs = sq;
+              q = qq;
+            }
+          }
+        }
+        if (q >= 0) {
+          const float4 sq = m.state[q];
+          if (sq.w != 0.0f) {
+            v = make_float3(sq.x, sq.y, sq.z);
+            view = SAMPLE ? m.nghbr[q] : 0;
+            valid = true;
+          }
+        }
+      } else {
+        if (slot == 8) refn = curn;
+        if (cv.z != 0.0f) {
+          const uint4 r = philox4x32_10(
+              make_uint4((uint32_t)pix, (uint32_t)tl.x, (uint32_t)p.pass, (uint32_t)(slot - 8)),
+              p.seed_lo, p.seed_hi);
+          const float2 g0 = normal2(r.x, r.y), g1 = normal2(r.z, r.w);
+          const float depth = cd * expf(depth_range * g0.x);
+          const float3 n = make_float3(-cv.x / cv.z + normal_range * g0.y,
+                                       -cv.y / cv.z + normal_range * g1.x, -1.0f);
+          v = plane_from_depth_normal(fj, fi, m.Kinv_d, depth, n);
+          view = refn;
+          valid = true;
+          depth_range *= 0.3f;
+          normal_range *= 0.8f;
+        }
+      }
+      if (valid) try_plane(v, view);
     }
     if (SAMPLE && m.n_pairs >= 2) {
       // A random other matching view for the current plane.
-      int other = 1 + (int)(rnd[18] % (uint32_t)(m.n_pairs - 1));
+      const uint4 r = philox4x32_10(make_uint4((uint32_t)pix, (uint32_t)tl.x, (uint32_t)p.pass, 6u),
+                                    p.seed_lo, p.seed_hi);
+      int other = 1 + (int)(r.x % (uint32_t)(m.n_pairs - 1));
       if (other >= curn) other += 1;
       const Hyp h = make_hyp(m.Kinv, cv, fj, fi);
       const PairDev& pr = mp[other - 1];
-      const float s = ncc_view<HPZ>(rp, views[pr.view], pr, h, fj, fi, taps);
+      const float s = pt.view(views[pr.view], pr, h, fj, fi, taps);
       if (s > cur) {
         cur = s;
         curn = other;
       }
     }
-    m.state[pix] = make_float4(cv.x, cv.y, cv.z, cd);
-    m.score[pix] = cur;
-    m.nghbr[pix] = curn;
+    if (lane == 0) {
+      m.state[pix] = make_float4(cv.x, cv.y, cv.z, cd);
+      m.score[pix] = cur;
+      m.nghbr[pix] = curn;
+    }
   }
   flush_taps(taps, p.taps);
 }
@@ -486,31 +506,37 @@ __global__ void pack_kernel(const MapDev* __restrict__ maps, int map, float* __r
 // ----------------------------------------------------------------------
 // Host-side launchers.
 
-template <int HPZ>
+template <int HPZ, int L>
 static cudaError_t launch_hpz(Stage stage, bool sample, const LaunchArgs& a, cudaStream_t s) {
   const dim3 blk(a.bx, a.by);
+  const int px = a.bx / L;
   if (stage == Stage::kHalfPass) {
-    const size_t smem = sizeof(float) * (2 * a.bx + 2 * HPZ) * (a.by + 2 * HPZ);
+    const size_t smem = sizeof(float) * (2 * px + 2 * HPZ) * (a.by + 2 * HPZ);
     if (sample)
-      halfpass_kernel<HPZ, true><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+      halfpass_kernel<HPZ, true, L><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
     else
-      halfpass_kernel<HPZ, false><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+      halfpass_kernel<HPZ, false, L><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
     return cudaGetLastError();
   }
-  const size_t smem = sizeof(float) * (a.bx + 2 * HPZ) * (a.by + 2 * HPZ);
   switch (stage) {
-    case Stage::kInit:
+    case Stage::kInit: {
+      const size_t smem = sizeof(float) * (px + 2 * HPZ) * (a.by + 2 * HPZ);
       if (sample)
-        init_kernel<HPZ, true><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+        init_kernel<HPZ, true, L><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
       else
-        init_kernel<HPZ, false><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+        init_kernel<HPZ, false, L><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
       break;
-    case Stage::kBruteForce:
+    }
+    case Stage::kBruteForce: {
+      const size_t smem = sizeof(float) * (a.bx + 2 * HPZ) * (a.by + 2 * HPZ);
       brute_force_kernel<HPZ><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
       break;
-    case Stage::kScorePlanes:
+    }
+    case Stage::kScorePlanes: {
+      const size_t smem = sizeof(float) * (a.bx + 2 * HPZ) * (a.by + 2 * HPZ);
       score_planes_kernel<HPZ><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
       break;
+    }
     default:
       return cudaErrorInvalidValue;
   }
@@ -523,12 +549,19 @@ cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStre
     postprocess_kernel<<<a.n_tiles, dim3(a.bx, a.by), 0, s>>>(a.maps, a.tiles, a.flag);
     return cudaGetLastError();
   }
+  // Lanes per pixel (a.p.variant): 1, 2 or 4 for the 7 x 7 patch (init and
+  // half-passes; brute force and plane scoring use 1); other patch sizes 1.
   switch (a.p.hpz) {
-    case 1: return launch_hpz<1>(stage, sample, a, s);
-    case 2: return launch_hpz<2>(stage, sample, a, s);
-    case 3: return launch_hpz<3>(stage, sample, a, s);
-    case 4: return launch_hpz<4>(stage, sample, a, s);
-    case 5: return launch_hpz<5>(stage, sample, a, s);
+    case 1: return launch_hpz<1, 1>(stage, sample, a, s);
+    case 2: return launch_hpz<2, 1>(stage, sample, a, s);
+    case 3:
+      if (stage == Stage::kInit || stage == Stage::kHalfPass) {
+        if (a.p.variant == 2) return launch_hpz<3, 2>(stage, sample, a, s);
+        if (a.p.variant == 4) return launch_hpz<3, 4>(stage, sample, a, s);
+      }
+      return launch_hpz<3, 1>(stage, sample, a, s);
+    case 4: return launch_hpz<4, 1>(stage, sample, a, s);
+    case 5: return launch_hpz<5, 1>(stage, sample, a, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -331,12 +331,19 @@ def ref_median5(depth):
 # --------------------------------------------------------------------------
 # float64 NCC restatement (depthmap.cc:441-487), vectorised over pixels.
 
-def ncc_fp64(Ks, Rs, ts, images, planes, patch_size=7, pixels=None):
+def ncc_fp64(Ks, Rs, ts, images, planes, patch_size=7, pixels=None, margins=False):
     """Per-pixel max-over-views NCC in float64 for the given planes.
 
     Returns (score (H, W) float64, nghbr (H, W) int32); the homography, the
     affine warp, bilinear sampling, bilateral weights and the moments are all
     float64.  ``pixels``: optional boolean mask restricting the work.
+
+    With ``margins=True`` also returns, per pixel, the distances to the
+    reference's two discontinuities, minimised over views and taps: ``edge``,
+    how close a tap lands to x = 0, x = W-1, y = 0 or y = H-1 (where
+    LinearInterpolation switches to 0, depthmap.cc:16-18), and ``var``, how
+    close var_x or var_y is to the 0.1 cut-off (depthmap.cc:68).  Float
+    implementations legitimately disagree on pixels with tiny margins.
     """
     K = [np.asarray(k, np.float64) for k in Ks]
     R = [np.asarray(r, np.float64) for r in Rs]
@@ -353,6 +360,8 @@ def ncc_fp64(Ks, Rs, ts, images, planes, patch_size=7, pixels=None):
     K1inv = np.linalg.inv(K[0])
     best = np.full(pi.shape, -1.0)
     bestn = np.zeros(pi.shape, np.int32)
+    edge_m = np.full(pi.shape, np.inf)
+    var_m = np.full(pi.shape, np.inf)
     ref = imgs[0]
     c = ref[pi.astype(int), pj.astype(int)]
     for o in range(1, len(imgs)):
@@ -379,6 +388,10 @@ def ncc_fp64(Ks, Rs, ts, images, planes, patch_size=7, pixels=None):
                 x2 = x0 + dxx * dx + dyx * dy
                 y2 = y0 + dxy * dx + dyy * dy
                 inside = (x2 >= 0) & (x2 < W - 1) & (y2 >= 0) & (y2 < H - 1)
+                if margins:
+                    e = np.minimum(np.minimum(np.abs(x2), np.abs(x2 - (W - 1))),
+                                   np.minimum(np.abs(y2), np.abs(y2 - (H - 1))))
+                    edge_m = np.minimum(edge_m, np.where(ok, e, np.inf))
                 xs = np.where(inside, x2, 0.0)
                 ys = np.where(inside, y2, 0.0)
                 ix, iy = np.floor(xs).astype(int), np.floor(ys).astype(int)
@@ -398,6 +411,8 @@ def ncc_fp64(Ks, Rs, ts, images, planes, patch_size=7, pixels=None):
         vy = syy / sw - my * my
         ncc = np.where((vx < 0.1) | (vy < 0.1) | ~ok, -1.0,
                        (sxy / sw - mx * my) / np.sqrt(np.maximum(vx * vy, 1e-300)))
+        if margins:
+            var_m = np.minimum(var_m, np.minimum(np.abs(vx - 0.1), np.abs(vy - 0.1)))
         upd = ncc > best
         best = np.where(upd, ncc, best)
         bestn = np.where(upd, o, bestn)
@@ -405,4 +420,10 @@ def ncc_fp64(Ks, Rs, ts, images, planes, patch_size=7, pixels=None):
     nghbr = np.zeros((H, W), np.int32)
     score[interior] = best
     nghbr[interior] = bestn
+    if margins:
+        em = np.full((H, W), np.inf)
+        vm = np.full((H, W), np.inf)
+        em[interior] = edge_m
+        vm[interior] = var_m
+        return score, nghbr, em, vm
     return score, nghbr
