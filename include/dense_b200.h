@@ -221,6 +221,38 @@ dn_status dn_postprocess_depth(const float* depth, float* out, int width, int he
  * register-resident FMA loop on every SM; used as the scoring roofline. */
 dn_status dn_fp32_peak(double* tflops, double* ms);
 
+/* ------------------------------------------------------------------------
+ * Pruning without device allocation.
+ *
+ * No counterpart in the reference.  DepthmapPruner::Prune for callers that
+ * cannot allocate device memory (their process hands the GPU's memory to its
+ * own pool, or must not allocate once running).  Inputs and outputs are
+ * caller-owned DEVICE buffers; the working memory is a static array compiled
+ * into the library (about 4.3 MB per GPU, held until exit).  Limits: the
+ * reference depthmap (view 0) has at most 4,194,304 pixels, at most 17 views,
+ * and `capacity` (points the output buffers hold) is at least its
+ * width * height.  The number of kept points is written to the device
+ * counter *count.  Work is enqueued on `stream` (a cudaStream_t, NULL for
+ * the default stream) and the call returns without waiting.  All calls share
+ * the static array: calls whose GPU work overlaps race and must be
+ * serialised by the caller.  The first call on a device looks up the array's
+ * address with that device current; make it before any stream capture.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  double K[9], R[9], t[3];  /* host values, as for dn_pruner_add_view */
+  const float* depth;       /* device, [height][width] */
+  const float* plane;       /* device, [height][width][3] */
+  const uint8_t* color;     /* device, [height][width][3] */
+  const uint8_t* label;     /* device, [height][width] */
+  int width, height;
+} dn_prune_view;
+
+dn_status dn_prune_noalloc(const dn_prune_view* views, int n_views, float same_depth_threshold,
+                           float* points, float* normals, uint8_t* colors, uint8_t* labels,
+                           int64_t capacity, unsigned long long* count, void* stream);
+/* Message for the last failed dn_prune_noalloc call on this thread. */
+const char* dn_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -89,7 +89,17 @@ _SIGNATURES = {
     "dn_batch_timer_elapsed": ([_vp, _f], _i),
     "dn_postprocess_depth": ([_f, _f, _i, _i], _i),
     "dn_fp32_peak": ([ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], _i),
+    "dn_prune_noalloc": ([_vp, _i, ctypes.c_float, _vp, _vp, _vp, _vp, ctypes.c_int64, _vp, _vp], _i),
+    "dn_noalloc_last_error": ([], ctypes.c_char_p),
 }
+
+
+class PruneView(ctypes.Structure):
+    """dn_prune_view (include/dense_b200.h): host camera, device buffers."""
+
+    _fields_ = [("K", ctypes.c_double * 9), ("R", ctypes.c_double * 9), ("t", ctypes.c_double * 3),
+                ("depth", ctypes.c_void_p), ("plane", ctypes.c_void_p), ("color", ctypes.c_void_p),
+                ("label", ctypes.c_void_p), ("width", ctypes.c_int), ("height", ctypes.c_int)]
 
 
 def header_symbols() -> List[str]:
