@@ -258,17 +258,19 @@ struct Engine {
     for (int y = 0; y < H; ++y)
       for (int x = 0; x < W; ++x) sum += image[(size_t)y * stride + x];
     v->cbias = (float)std::floor(sum / ((double)W * H) + 0.5);
-    const int TW = W - 1 + 2 * dn::kPad, TH = H - 1 + 2 * dn::kPad;
+    const dn::TableGeom tg = dn::table_geom(W, H);
+    DN_CHECK(W <= 8192 - 2 * dn::kPad, "image wider than the table layout supports (8176)");
     DN_CUDA(v->img.alloc((size_t)W * H));
-    DN_CUDA(v->quad.alloc((size_t)TW * TH));
+    // 64 spare entries after the last row: prefetches may reach past it.
+    DN_CUDA(v->quad.alloc((size_t)tg.TP * tg.TH + 64));
     DN_CUDA(v->gray.alloc((size_t)W * H));
     DN_CUDA(cudaMemcpy2DAsync(v->gray.p, W, image, stride, W, H, cudaMemcpyHostToDevice, stream));
     if (mask) {
       DN_CUDA(v->mask.alloc((size_t)W * H));
       DN_CUDA(cudaMemcpy2DAsync(v->mask.p, W, mask, stride, W, H, cudaMemcpyHostToDevice, stream));
     }
-    DN_CUDA(dn::launch_prepare_view(v->gray.p, W, H, W, v->img.p, v->quad.p, TW, TH, v->cbias,
-                                    stream));
+    DN_CUDA(dn::launch_prepare_view(v->gray.p, W, H, W, v->img.p, v->quad.p, tg.TP, tg.TW, tg.TH,
+                                    v->cbias, stream));
     DN_CUDA(cudaStreamSynchronize(stream));
     if (id) *id = (int)views.size();
     views.push_back(std::move(v));
@@ -322,14 +324,17 @@ struct Engine {
     for (size_t k = 0; k < views.size(); ++k) {
       const View& v = *views[k];
       dn::ViewDev d{};
+      const dn::TableGeom tg = dn::table_geom(v.W, v.H);
       d.img = v.img.p;
       d.mask = v.mask.p;
       d.quad = v.quad.p;
+      d.quad0 = v.quad.p + (size_t)dn::kPad * tg.TP + dn::kPad;
       d.W = v.W;
       d.H = v.H;
-      d.TW = v.W - 1 + 2 * dn::kPad;
-      d.TH = v.H - 1 + 2 * dn::kPad;
+      d.TP = tg.TP;
+      d.TH = tg.TH;
       d.cbias = v.cbias;
+      d.magic = tg.magic;
       hv[k] = d;
     }
     std::vector<dn::PairDev> hp;
@@ -550,10 +555,10 @@ struct Engine {
     if (stride <= 0) stride = w.W;
     DN_CHECK(stride >= w.W, "stride must be >= width");
     DN_CUDA(cudaSetDevice(device));
-    const int TW = w.W - 1 + 2 * dn::kPad, TH = w.H - 1 + 2 * dn::kPad;
+    const dn::TableGeom tg = dn::table_geom(w.W, w.H);
     DN_CUDA(cudaMemcpy2DAsync(w.gray.p, w.W, image, stride, w.W, w.H, cudaMemcpyHostToDevice, stream));
-    DN_CUDA(dn::launch_prepare_view(w.gray.p, w.W, w.H, w.W, w.img.p, w.quad.p, TW, TH, w.cbias,
-                                    stream));
+    DN_CUDA(dn::launch_prepare_view(w.gray.p, w.W, w.H, w.W, w.img.p, w.quad.p, tg.TP, tg.TW, tg.TH,
+                                    w.cbias, stream));
     return DN_OK;
   }
 

@@ -24,13 +24,19 @@ constexpr int kMaxHpz = 5;     // patch half-size supported (patch 3..11)
 constexpr int kFarSamples = 11;  // far propagation samples per direction
 constexpr int kFarStart = 3;     // first far sample distance (then +2)
 
+// Coefficient table rows have a pitch TP = 1024 k - 1 entries (k a power of
+// two).  With the floor trick t = x + M rounded down, M = 2^23 + 2^22 / k,
+// the 32-bit product bits(ty) * TP + bits(tx) equals iy * TP + ix exactly
+// (mod 2^32), so one IMAD turns the two biased floats into the entry index.
 struct ViewDev {
   const __half* img;     // [H][W]
   const uint8_t* mask;   // [H][W] or null (all valid)
-  const float4* quad;    // [TH][TW]
-  int W, H, TW, TH;
+  const float4* quad;    // [TH][TP], entry (ix, iy) at (iy + P) * TP + ix + P
+  const float4* quad0;   // &quad[entry (0, 0)]
+  int W, H, TP, TH;
   float cbias;           // intensity centring constant folded into quad.x
-  int pad_[3];
+  float magic;           // M for this pitch
+  int pad_[2];
 };
 
 struct PairDev {
@@ -68,7 +74,7 @@ struct RunParams {
   int min_consistent;
   unsigned long long* taps;  // NCC tap counter
   int* error;                // device error word
-  int variant;               // NCC walk: 0/1 one view at a time, 2/3 views in lock step
+  int variant;               // lanes per pixel (init and half-passes)
 };
 
 // ------------------------------------------------------------------ RNG
@@ -222,8 +228,8 @@ __device__ inline Hyp make_hyp(const float* Kinv, float3 v, float j, float i) {
 // (ComputePlaneImageScore, depthmap.cc:449-465): centre (X0, Y0) and the
 // Jacobian columns (ax, ay) per dx and (bx, by) per dy, plus how the patch
 // can be sampled: kOutside (every tap outside the image: all samples 0,
-// var_y = 0, NCC = -1), kFast (inside the padded table, fixed-point path),
-// kSlow (float coordinates, clamped), kDegenerate (w == 0: NCC = -1).
+// var_y = 0, NCC = -1), kFast (inside the padded table), kSlow (leaves the
+// padded table: taps clamped), kDegenerate (w == 0: NCC = -1).
 enum WarpMode { kOutside = 0, kFast = 1, kSlow = 2, kDegenerate = 3 };
 struct Warp {
   float X0, Y0, ax, bx, ay, by;
@@ -265,44 +271,31 @@ __device__ inline Warp warp_setup(const ViewDev& vw, const PairDev& pr, const Hy
   }
   const float lo = -(float)kPad + 0.01f;
   const bool fast = (wp.X0 - ex >= lo) && (wp.X0 + ex < Wm1 + (float)kPad - 0.01f) &&
-                    (wp.Y0 - ey >= lo) && (wp.Y0 + ey < Hm1 + (float)kPad - 0.01f) &&
-                    ex < 200.f && ey < 200.f;
+                    (wp.Y0 - ey >= lo) && (wp.Y0 + ey < Hm1 + (float)kPad - 0.01f);
   wp.mode = fast ? kFast : kSlow;
   return wp;
 }
 
-// Fixed-point walk of one view's patch: tap (dx, dy) sits at
-// XS + dx AX + dy BX (9.23 fixed point, relative to floor(X0)), likewise y.
-struct Walk {
-  const float4* base;  // table entry of (floor(X0), floor(Y0))
-  int XS, YS, AX, AY, BX, BY;
-  int TW;
-};
-
-template <int HPZ>
-__device__ inline Walk make_walk(const ViewDev& vw, const Warp& wp) {
-  Walk k;
-  const float fbx = floorf(wp.X0), fby = floorf(wp.Y0);
-  const float sc = 8388608.0f;  // 2^23
-  k.XS = __float2int_rn((wp.X0 - fbx - HPZ * wp.ax - HPZ * wp.bx) * sc);
-  k.YS = __float2int_rn((wp.Y0 - fby - HPZ * wp.ay - HPZ * wp.by) * sc);
-  k.AX = __float2int_rn(wp.ax * sc);
-  k.BX = __float2int_rn(wp.bx * sc);
-  k.AY = __float2int_rn(wp.ay * sc);
-  k.BY = __float2int_rn(wp.by * sc);
-  k.TW = vw.TW;
-  k.base = vw.quad + (size_t)((int)fby + kPad) * vw.TW + ((int)fbx + kPad);
-  return k;
+// Bilinear sample at (x, y) inside the padded table: floor by adding the
+// magic constant rounding down, exact fractions, one IMAD for the entry
+// index, one 16-byte load and three FMAs:  y - cbias = e0 + fx e1 +
+// fy (e2 + fx e3).
+__device__ inline float table_sample(const ViewDev& vw, float x, float y) {
+  const float M = vw.magic;
+  const float tx = __fadd_rd(x, M), ty = __fadd_rd(y, M);
+  const float fx = x - (tx - M), fy = y - (ty - M);
+  const int off = (int)(__float_as_uint(ty) * (unsigned)vw.TP + __float_as_uint(tx));
+  const float4 q = __ldg(vw.quad0 + off);
+  return fmaf(fy, fmaf(fx, q.w, q.z), fmaf(fx, q.y, q.x));
 }
 
-// Sample of the coefficient table at fixed-point (XF, YF): the fraction
-// bits become the float 1 + f directly; one 16-byte load and three FMAs.
-__device__ inline float walk_sample(const Walk& k, int XF, int YF) {
-  const int ix = XF >> 23, iy = YF >> 23;
-  const float f1 = __int_as_float((XF & 0x7FFFFF) | 0x3F800000);
-  const float g1 = __int_as_float((YF & 0x7FFFFF) | 0x3F800000);
-  const float4 q = __ldg(k.base + iy * k.TW + ix);
-  return fmaf(g1, fmaf(f1, q.w, q.z), fmaf(f1, q.y, q.x));
+// Same, clamped: taps outside the padded table read its corner entry, whose
+// sample is the reference's zero.
+__device__ inline float table_sample_clamped(const ViewDev& vw, float x, float y) {
+  const float xlo = -(float)kPad, xhi = (float)(vw.W - 1 + kPad);
+  const float ylo = -(float)kPad, yhi = (float)(vw.H - 1 + kPad);
+  if (x >= xlo && x < xhi && y >= ylo && y < yhi) return table_sample(vw, x, y);
+  return vw.quad[0].x;
 }
 
 template <int HPZ>
@@ -313,62 +306,24 @@ __device__ inline float ncc_finish(const RefPatch<HPZ>& rp, float s1, float s2, 
   return (s3 * rp.inv_sw) * rsqrtf(rp.varx * vary);
 }
 
-// Slow path: float tap coordinates; out-of-table taps read the table's
-// corner entry, whose sample is the reference's zero.
-template <int HPZ>
-__device__ inline float ncc_slow(const RefPatch<HPZ>& rp, const ViewDev& vw, const Warp& wp) {
-  const float Wm1 = (float)(vw.W - 1), Hm1 = (float)(vw.H - 1);
-  const float xlo = -(float)kPad, xhi = Wm1 + (float)kPad;
-  const float ylo = -(float)kPad, yhi = Hm1 + (float)kPad;
-  float s1 = 0.f, s2 = 0.f, s3 = 0.f;
-#pragma unroll
-  for (int dy = -HPZ; dy <= HPZ; ++dy)
-#pragma unroll
-    for (int dx = -HPZ; dx <= HPZ; ++dx) {
-      const float x = fmaf(wp.bx, (float)dy, fmaf(wp.ax, (float)dx, wp.X0));
-      const float yv = fmaf(wp.by, (float)dy, fmaf(wp.ay, (float)dx, wp.Y0));
-      int ix = -kPad, iy = -kPad;
-      float f1 = 1.f, g1 = 1.f;
-      if (x >= xlo && x < xhi && yv >= ylo && yv < yhi) {
-        const float fx = floorf(x), fy = floorf(yv);
-        ix = (int)fx;
-        iy = (int)fy;
-        f1 = 1.0f + (x - fx);
-        g1 = 1.0f + (yv - fy);
-      }
-      const float4 q = __ldg(vw.quad + (size_t)(iy + kPad) * vw.TW + (ix + kPad));
-      const float y = fmaf(g1, fmaf(f1, q.w, q.z), fmaf(f1, q.y, q.x));
-      const int t = (dy + HPZ) * (2 * HPZ + 1) + (dx + HPZ);
-      const float wy = rp.w[t] * y;
-      s1 += wy;
-      s2 = fmaf(wy, y, s2);
-      s3 = fmaf(rp.wx[t], y, s3);
-    }
-  return ncc_finish<HPZ>(rp, s1, s2, s3);
-}
-
 // Bilateral NCC of the reference patch against one matching view under
 // hypothesis h (ComputePlaneImageScore, depthmap.cc:441-478; NCCEstimator,
 // depthmap.cc:46-74).  Same local affine warp of the plane-induced
-// homography, same bilinear sample with zeros outside [0,W-1) x [0,H-1),
+// homography, tap positions X0 + ax dx + bx dy in float as the reference
+// forms them, same bilinear sample with zeros outside [0,W-1) x [0,H-1),
 // same weights.  Sums are mean-centred: x by the patch's weighted mean
 // (hoisted), y by the view's constant cbias (folded into the table).
-template <int HPZ>
-__device__ inline float ncc_view(const RefPatch<HPZ>& rp, const ViewDev& vw, const PairDev& pr,
-                                 const Hyp& h, float j, float i, unsigned& taps) {
-  const Warp wp = warp_setup<HPZ>(vw, pr, h, j, i);
-  if (wp.mode == kOutside || wp.mode == kDegenerate) return -1.0f;
-  taps += RefPatch<HPZ>::N;
-  if (wp.mode == kSlow) return ncc_slow<HPZ>(rp, vw, wp);
-  const Walk k = make_walk<HPZ>(vw, wp);
+template <int HPZ, bool CLAMP>
+__device__ inline float ncc_walk(const RefPatch<HPZ>& rp, const ViewDev& vw, const Warp& wp) {
   float s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
-  for (int dy = 0; dy <= 2 * HPZ; ++dy) {
-    const int xr = k.XS + dy * k.BX, yr = k.YS + dy * k.BY;
+  for (int dy = -HPZ; dy <= HPZ; ++dy) {
+    const float xr = fmaf(wp.bx, (float)dy, wp.X0), yr = fmaf(wp.by, (float)dy, wp.Y0);
 #pragma unroll
-    for (int dx = 0; dx <= 2 * HPZ; ++dx) {
-      const float y = walk_sample(k, xr + dx * k.AX, yr + dx * k.AY);
-      const int t = dy * (2 * HPZ + 1) + dx;
+    for (int dx = -HPZ; dx <= HPZ; ++dx) {
+      const float x = fmaf(wp.ax, (float)dx, xr), yv = fmaf(wp.ay, (float)dx, yr);
+      const float y = CLAMP ? table_sample_clamped(vw, x, yv) : table_sample(vw, x, yv);
+      const int t = (dy + HPZ) * (2 * HPZ + 1) + (dx + HPZ);
       const float wy = rp.w[t] * y;
       s1 += wy;
       s2 = fmaf(wy, y, s2);
@@ -376,6 +331,16 @@ __device__ inline float ncc_view(const RefPatch<HPZ>& rp, const ViewDev& vw, con
     }
   }
   return ncc_finish<HPZ>(rp, s1, s2, s3);
+}
+
+template <int HPZ>
+__device__ inline float ncc_view(const RefPatch<HPZ>& rp, const ViewDev& vw, const PairDev& pr,
+                                 const Hyp& h, float j, float i, unsigned& taps) {
+  const Warp wp = warp_setup<HPZ>(vw, pr, h, j, i);
+  if (wp.mode == kOutside || wp.mode == kDegenerate) return -1.0f;
+  taps += RefPatch<HPZ>::N;
+  if (wp.mode == kSlow) return ncc_walk<HPZ, true>(rp, vw, wp);
+  return ncc_walk<HPZ, false>(rp, vw, wp);
 }
 
 // ComputePlaneScore (depthmap.cc:408-419): max over matching views, the
@@ -403,8 +368,9 @@ __device__ inline float ncc_max(const RefPatch<HPZ>& rp, const ViewDev* views,
 // ... (8 / L columns x 7 rows), the padding column carries weight 0 and
 // samples column 6's position.  Each lane keeps 2 x 56 / L weights instead of
 // 98, so more warps fit on an SM, and lanes l and l + 1 read neighbouring
-// table entries.  The three sums are combined with XOR shuffles inside the
-// lane group; every lane of a group ends with the same score.
+// table entries.  The warp setup of a view is computed by one lane of the
+// group and broadcast; the three sums are combined with XOR shuffles, so
+// every lane of a group ends with the same score.
 template <int L>
 struct CoopPatch {
   static constexpr int C = 8 / L;  // columns per lane
@@ -415,6 +381,7 @@ struct CoopPatch {
   float varx;
   int lane;
   unsigned mask;  // the lane group's bits in the warp
+  int src0;       // warp lane of the group's lane 0
 };
 
 template <int L>
@@ -429,6 +396,7 @@ __device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile,
                                             int lx, int lane, unsigned mask) {
   cp.lane = lane;
   cp.mask = mask;
+  cp.src0 = (threadIdx.x & 31) - lane;
   const float c = tile[ly * pitch + lx];
   const float dcf = 1.0f / 5000.0f;
   const float dxf = 1.0f / 50.0f;
@@ -469,8 +437,33 @@ __device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile,
   cp.varx = sxx * inv_sw;
 }
 
-template <int L>
-__device__ inline float coop_finish(const CoopPatch<L>& cp, float s1, float s2, float s3) {
+// One lane's share of a view's walk, from the group's warp setup.
+template <int L, bool CLAMP>
+__device__ inline float coop_walk(const CoopPatch<L>& cp, const ViewDev& vw, const Warp& wp) {
+  constexpr int C = CoopPatch<L>::C;
+  // Lane's first column dx0 = lane - 3; the padding column (dx = 7, on lane
+  // L - 1) samples dx = 6.
+  const float dx0 = (float)(cp.lane - 3);
+  const float xl = fmaf(wp.ax, dx0, fmaf(wp.bx, -3.0f, wp.X0));
+  const float yl = fmaf(wp.ay, dx0, fmaf(wp.by, -3.0f, wp.Y0));
+  const float last = (float)((C - 1) * L - ((cp.lane == L - 1) ? 1 : 0));
+  float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+  for (int r = 0; r < 7; ++r) {
+    const float xr = fmaf(wp.bx, (float)r, xl), yr = fmaf(wp.by, (float)r, yl);
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      const float cq = (q == C - 1) ? last : (float)(L * q);
+      const float x = q == 0 ? xr : fmaf(wp.ax, cq, xr);
+      const float yv = q == 0 ? yr : fmaf(wp.ay, cq, yr);
+      const float y = CLAMP ? table_sample_clamped(vw, x, yv) : table_sample(vw, x, yv);
+      const int t = r * C + q;
+      const float wy = cp.w[t] * y;
+      s1 += wy;
+      s2 = fmaf(wy, y, s2);
+      s3 = fmaf(cp.wx[t], y, s3);
+    }
+  }
   s1 = group_sum<L>(s1, cp.mask);
   s2 = group_sum<L>(s2, cp.mask);
   s3 = group_sum<L>(s3, cp.mask);
@@ -481,69 +474,60 @@ __device__ inline float coop_finish(const CoopPatch<L>& cp, float s1, float s2, 
 }
 
 template <int L>
+__device__ inline Warp bcast_warp(const Warp& w, unsigned mask, int src) {
+  Warp o;
+  o.X0 = __shfl_sync(mask, w.X0, src);
+  o.Y0 = __shfl_sync(mask, w.Y0, src);
+  o.ax = __shfl_sync(mask, w.ax, src);
+  o.bx = __shfl_sync(mask, w.bx, src);
+  o.ay = __shfl_sync(mask, w.ay, src);
+  o.by = __shfl_sync(mask, w.by, src);
+  o.mode = __shfl_sync(mask, w.mode, src);
+  return o;
+}
+
+template <int L>
+__device__ inline float coop_eval(const CoopPatch<L>& cp, const ViewDev& vw, const Warp& wp,
+                                  unsigned& taps) {
+  if (wp.mode == kOutside || wp.mode == kDegenerate) return -1.0f;
+  if (cp.lane == 0) taps += 49;
+  if (wp.mode == kSlow) return coop_walk<L, true>(cp, vw, wp);
+  return coop_walk<L, false>(cp, vw, wp);
+}
+
+// Single view (sample mode): every lane computes the same setup.
+template <int L>
 __device__ inline float coop_ncc_view(const CoopPatch<L>& cp, const ViewDev& vw,
                                       const PairDev& pr, const Hyp& h, float j, float i,
                                       unsigned& taps) {
-  constexpr int C = CoopPatch<L>::C;
   const Warp wp = warp_setup<3>(vw, pr, h, j, i);
-  if (wp.mode == kOutside || wp.mode == kDegenerate) return -1.0f;
-  if (cp.lane == 0) taps += 49;
-  // The padding column (dx = 7, on lane L - 1) samples dx = 6.
-  const int pad_col = (cp.lane == L - 1) ? 1 : 0;
-  float s1 = 0.f, s2 = 0.f, s3 = 0.f;
-  if (wp.mode == kSlow) {
-    const float Wm1 = (float)(vw.W - 1), Hm1 = (float)(vw.H - 1);
-    const float xlo = -(float)kPad, xhi = Wm1 + (float)kPad;
-    const float ylo = -(float)kPad, yhi = Hm1 + (float)kPad;
-#pragma unroll
-    for (int r = 0; r < 7; ++r)
-#pragma unroll
-      for (int q = 0; q < C; ++q) {
-        const int dx = cp.lane + L * q - ((q == C - 1) ? pad_col : 0) - 3;
-        const int dy = r - 3;
-        const float x = fmaf(wp.bx, (float)dy, fmaf(wp.ax, (float)dx, wp.X0));
-        const float yv = fmaf(wp.by, (float)dy, fmaf(wp.ay, (float)dx, wp.Y0));
-        int ix = -kPad, iy = -kPad;
-        float f1 = 1.f, g1 = 1.f;
-        if (x >= xlo && x < xhi && yv >= ylo && yv < yhi) {
-          const float fx = floorf(x), fy = floorf(yv);
-          ix = (int)fx;
-          iy = (int)fy;
-          f1 = 1.0f + (x - fx);
-          g1 = 1.0f + (yv - fy);
-        }
-        const float4 qd = __ldg(vw.quad + (size_t)(iy + kPad) * vw.TW + (ix + kPad));
-        const float y = fmaf(g1, fmaf(f1, qd.w, qd.z), fmaf(f1, qd.y, qd.x));
-        const int t = r * C + q;
-        const float wy = cp.w[t] * y;
-        s1 += wy;
-        s2 = fmaf(wy, y, s2);
-        s3 = fmaf(cp.wx[t], y, s3);
-      }
-  } else {
-    const Walk k = make_walk<3>(vw, wp);
-    const int xs = k.XS + cp.lane * k.AX, ys = k.YS + cp.lane * k.AY;
-    const int xpad = pad_col * k.AX, ypad = pad_col * k.AY;
-#pragma unroll
-    for (int r = 0; r < 7; ++r) {
-      const int xr = xs + r * k.BX, yr = ys + r * k.BY;
-#pragma unroll
-      for (int q = 0; q < C; ++q) {
-        int XF = xr + (L * q) * k.AX, YF = yr + (L * q) * k.AY;
-        if (q == C - 1) {
-          XF -= xpad;
-          YF -= ypad;
-        }
-        const float y = walk_sample(k, XF, YF);
-        const int t = r * C + q;
-        const float wy = cp.w[t] * y;
-        s1 += wy;
-        s2 = fmaf(wy, y, s2);
-        s3 = fmaf(cp.wx[t], y, s3);
+  return coop_eval<L>(cp, vw, wp, taps);
+}
+
+// Max over views: lane l of the group sets up views l, l + L, ...; each
+// setup is broadcast to the group before the shared walk.
+template <int L>
+__device__ inline float coop_max(const CoopPatch<L>& cp, const ViewDev* views,
+                                 const PairDev* pairs, int n_pairs, const Hyp& h, float j,
+                                 float i, int& best_view, unsigned& taps) {
+  float best = -1.0f;
+  best_view = 0;
+  for (int k0 = 0; k0 < n_pairs; k0 += L) {
+    const int mine = min(k0 + cp.lane, n_pairs - 1);
+    const PairDev& prm = pairs[mine];
+    const Warp own = warp_setup<3>(views[prm.view], prm, h, j, i);
+    const int nv = min(L, n_pairs - k0);
+    for (int v = 0; v < nv; ++v) {
+      const Warp wp = bcast_warp<L>(own, cp.mask, cp.src0 + v);
+      const ViewDev& vw = views[pairs[k0 + v].view];
+      const float s = coop_eval<L>(cp, vw, wp, taps);
+      if (s > best) {
+        best = s;
+        best_view = k0 + v + 1;
       }
     }
   }
-  return coop_finish<L>(cp, s1, s2, s3);
+  return best;
 }
 
 // ------------------------------------------------------------------------
@@ -561,6 +545,10 @@ struct Patch<HPZ, 1> {
                         unsigned& taps) const {
     return ncc_view<HPZ>(rp, vw, pr, h, j, i, taps);
   }
+  __device__ float max(const ViewDev* views, const PairDev* pairs, int n, const Hyp& h, float j,
+                       float i, int& best_view, unsigned& taps) const {
+    return ncc_max<HPZ>(rp, views, pairs, n, h, j, i, best_view, taps);
+  }
 };
 
 template <int L>
@@ -573,6 +561,10 @@ struct CoopIface {
                         unsigned& taps) const {
     return coop_ncc_view<L>(cp, vw, pr, h, j, i, taps);
   }
+  __device__ float max(const ViewDev* views, const PairDev* pairs, int n, const Hyp& h, float j,
+                       float i, int& best_view, unsigned& taps) const {
+    return coop_max<L>(cp, views, pairs, n, h, j, i, best_view, taps);
+  }
 };
 template <>
 struct Patch<3, 2> : CoopIface<2> {};
@@ -583,17 +575,7 @@ template <int HPZ, int L>
 __device__ inline float patch_max(const Patch<HPZ, L>& pt, const ViewDev* views,
                                   const PairDev* pairs, int n_pairs, const Hyp& h, float j,
                                   float i, int& best_view, unsigned& taps) {
-  float best = -1.0f;
-  best_view = 0;
-  for (int k = 0; k < n_pairs; ++k) {
-    const PairDev& pr = pairs[k];
-    const float s = pt.view(views[pr.view], pr, h, j, i, taps);
-    if (s > best) {
-      best = s;
-      best_view = k + 1;
-    }
-  }
-  return best;
+  return pt.max(views, pairs, n_pairs, h, j, i, best_view, taps);
 }
 
 }  // namespace dn

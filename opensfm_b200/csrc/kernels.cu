@@ -16,7 +16,7 @@ template <int HPZ>
 constexpr int kMinBlocks = HPZ <= 2 ? 4 : (HPZ == 3 ? 3 : 2);
 // With L lanes per pixel each lane keeps 2 x 56 / L weights.
 template <int HPZ, int L>
-constexpr int kMinBlocksL = L == 1 ? kMinBlocks<HPZ> : (L == 2 ? 4 : 6);
+constexpr int kMinBlocksL = L == 1 ? kMinBlocks<HPZ> : (L == 2 ? 4 : 5);
 
 // ----------------------------------------------------------------------
 // Per-view preparation.
@@ -28,26 +28,25 @@ __global__ void u8_to_half_kernel(const uint8_t* __restrict__ src, int W, int H,
 }
 
 // Bilinear coefficient table.  Entry (ix, iy), ix in [-P, W-2+P], holds the
-// bilinear interpolant of the 2x2 block at (ix, iy) as a polynomial in
-// f1 = 1 + fx, g1 = 1 + fy:  y - cbias = e0 + f1 e1 + g1 (e2 + f1 e3).
-// Blocks that reach outside [0, W-1) x [0, H-1) hold the constant -cbias,
-// i.e. the reference's zero sample (LinearInterpolation, depthmap.cc:16-18).
-// All coefficients are small integers, exact in FP32.
+// bilinear interpolant of the 2x2 block at (ix, iy) as a polynomial in the
+// fractions:  y - cbias = e0 + fx e1 + fy (e2 + fx e3).  Blocks that reach
+// outside [0, W-1) x [0, H-1) hold the constant -cbias, i.e. the
+// reference's zero sample (LinearInterpolation, depthmap.cc:16-18).  All
+// coefficients are small integers, exact in FP32.  Rows have pitch TP.
 __global__ void build_quad_kernel(const __half* __restrict__ img, int W, int H, float cbias,
-                                  float4* __restrict__ quad, int TW, int TH) {
+                                  float4* __restrict__ quad, int TP, int TW, int TH) {
   const int tx = blockIdx.x * blockDim.x + threadIdx.x, ty = blockIdx.y;
-  if (tx >= TW || ty >= TH) return;
+  if (tx >= TP || ty >= TH) return;
   const int ix = tx - kPad, iy = ty - kPad;
   float4 q = make_float4(-cbias, 0.f, 0.f, 0.f);
-  if (ix >= 0 && ix <= W - 2 && iy >= 0 && iy <= H - 2) {
+  if (tx < TW && ix >= 0 && ix <= W - 2 && iy >= 0 && iy <= H - 2) {
     const float q00 = __half2float(img[(size_t)iy * W + ix]);
     const float q01 = __half2float(img[(size_t)iy * W + ix + 1]);
     const float q10 = __half2float(img[(size_t)(iy + 1) * W + ix]);
     const float q11 = __half2float(img[(size_t)(iy + 1) * W + ix + 1]);
-    const float d1 = q01 - q00, d2 = q10 - q00, d3 = q11 - q10 - q01 + q00;
-    q = make_float4(q00 - d1 - d2 + d3 - cbias, d1 - d3, d2 - d3, d3);
+    q = make_float4(q00 - cbias, q01 - q00, q10 - q00, q11 - q10 - q01 + q00);
   }
-  quad[(size_t)ty * TW + tx] = q;
+  quad[(size_t)ty * TP + tx] = q;
 }
 
 // ----------------------------------------------------------------------
@@ -567,9 +566,11 @@ cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStre
 }
 
 cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, __half* d_img,
-                                float4* d_quad, int TW, int TH, float cbias, cudaStream_t s) {
+                                float4* d_quad, int TP, int TW, int TH, float cbias,
+                                cudaStream_t s) {
   u8_to_half_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(d_u8, W, H, stride, d_img);
-  build_quad_kernel<<<dim3((TW + 255) / 256, TH), 256, 0, s>>>(d_img, W, H, cbias, d_quad, TW, TH);
+  build_quad_kernel<<<dim3((TP + 255) / 256, TH), 256, 0, s>>>(d_img, W, H, cbias, d_quad, TP, TW,
+                                                               TH);
   return cudaGetLastError();
 }
 

@@ -22,7 +22,26 @@ struct LaunchArgs {
 
 cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStream_t s);
 cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, __half* d_img,
-                                float4* d_quad, int TW, int TH, float cbias, cudaStream_t s);
+                                float4* d_quad, int TP, int TW, int TH, float cbias,
+                                cudaStream_t s);
+
+// Table geometry of a W x H view: used width TW = W - 1 + 2P, rows
+// TH = H - 1 + 2P, pitch TP = 1024 k - 1 >= TW (k a power of two) and the
+// floor constant M = 2^23 + 2^22 / k (see ViewDev).
+struct TableGeom {
+  int TW, TH, TP;
+  float magic;
+};
+inline TableGeom table_geom(int W, int H) {
+  TableGeom g;
+  g.TW = W - 1 + 2 * kPad;
+  g.TH = H - 1 + 2 * kPad;
+  int k = 1;
+  while (1024 * k - 1 < g.TW) k *= 2;
+  g.TP = 1024 * k - 1;
+  g.magic = 8388608.0f + 4194304.0f / (float)k;
+  return g;
+}
 cudaError_t launch_pack(const MapDev* maps, int map, float* plane, size_t n, cudaStream_t s);
 cudaError_t launch_postprocess_plain(const float* in, float* out, int W, int H, cudaStream_t s);
 cudaError_t fp32_peak(double* tflops, double* ms);
