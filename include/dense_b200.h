@@ -182,6 +182,14 @@ dn_status dn_batch_synchronize(dn_batch* b);
  * pointer may be NULL to skip it.  clean may be NULL. */
 dn_status dn_batch_get_depthmap(dn_batch* b, int map_id, float* depth, float* plane,
                                 float* score, int32_t* nghbr, float* clean);
+/* PatchMatch schedule: half-passes per run (-1: 2 x iterations), and per
+ * half-pass the candidate sets: the 4 adjacent planes (use_near), the 4 far
+ * planes (use_far), n_refine refinements whose first depth / normal-slope
+ * ranges are depth_range0 / normal_range0, shrinking by 0.3 / 0.8 per step.
+ * Defaults 1, 1, 6, 0.02, 0.5 follow PatchMatchUpdatePixel
+ * (depthmap.cc:305-374). */
+dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int use_far,
+                                int n_refine, float depth_range0, float normal_range0);
 /* Initial planes (f32 [H][W][3], reference camera) for one depthmap. */
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes);
 /* Total kept pruner points over all maps of the last run (after sync). */
@@ -220,6 +228,54 @@ dn_status dn_postprocess_depth(const float* depth, float* out, int width, int he
 /* Measures the device's FP32 FMA throughput (TFLOP/s, FMA = 2 flops) with a
  * register-resident FMA loop on every SM; used as the scoring roofline. */
 dn_status dn_fp32_peak(double* tflops, double* ms);
+
+/* ------------------------------------------------------------------------
+ * Learned initialisation (no reference counterpart: the reference draws the
+ * PatchMatch initialisation at random, depthmap.cc:237-256).  A 6-layer 3x3
+ * convolutional network (32 channels, BF16 activations, FP32 accumulation,
+ * tensor cores) maps per-pixel features (reference intensity + NCC of 8
+ * swept fronto-parallel planes against the 2 nearest matching views) to
+ * (inverse-depth fraction, normal slopes).  Activations are NHWC BF16 device
+ * buffers; `stream` is a cudaStream_t (NULL: default stream); every call
+ * enqueues work and returns.
+ * ---------------------------------------------------------------------- */
+/* Network input features of every depthmap of the batch: feat is a device
+ * BF16 buffer [n_maps][H][W][32] with map stride `map_stride` elements
+ * (>= H * W * 32 of the largest map).  Runs on the batch stream. */
+dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, int n_planes);
+/* Training targets from the last PatchMatch run: target is a device f32
+ * buffer [n_maps][H][W][4] = (inverse-depth fraction, sx, sy, weight), with
+ * weight 1 where the depth is valid and its score >= min_score. */
+dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float min_score);
+/* Initial planes of one depthmap from the network output (device f32
+ * [H][W][4]); the next dn_batch_run with DN_RUN_INIT starts from them. */
+dn_status dn_batch_init_from_output(dn_batch* b, int map_id, const float* out);
+/* y = act(conv3x3(x, w) + bias) over n_pix pixels of images H x W; relu 0/1;
+ * y (BF16) and/or y32 (FP32) may be NULL.  cin 32; cout 32 or 4. */
+dn_status dn_nn_conv3x3_forward(const void* x, const void* w, const float* bias, int64_t n_pix,
+                                int H, int W, int cin, int cout, int relu, void* y, float* y32,
+                                void* stream);
+/* Backward of one layer given dy, the gradient of its pre-activation output
+ * (BF16 [n_pix][cout]): accumulates dw [cout][9 cin] and db [cout] (FP32,
+ * atomic adds) and writes dx (BF16 [n_pix][cin]) multiplied by (x_mask > 0)
+ * when x_mask is given, which makes dx the pre-activation gradient of a
+ * ReLU layer below whose output x_mask is.  dx may be NULL; wt_scratch holds
+ * cin * 9 * 16 * ceil(cout / 16) BF16 values. */
+dn_status dn_nn_conv3x3_backward(const void* dy, const void* x, const void* w,
+                                 const void* x_mask, int64_t n_pix, int H, int W, int cin,
+                                 int cout, void* dx, float* dw, float* db, void* wt_scratch,
+                                 void* stream);
+/* L1 loss of pred (f32 [n_pix][4]) against target ([n_pix][4], last = weight)
+ * with the normal slopes weighted by normal_weight: adds the loss and the
+ * weight total to loss_sum[0] / count[0] and writes dpred (BF16 [n_pix][4]). */
+dn_status dn_nn_l1_loss(const float* pred, const float* target, int64_t n_pix,
+                        float normal_weight, void* dpred, float* loss_sum, float* count,
+                        void* stream);
+/* Adam step on n FP32 parameters with grad / max(count, 1); also writes the
+ * BF16 copy w16 (may be NULL).  bc1 / bc2 are the bias corrections. */
+dn_status dn_nn_adam(float* w, float* m, float* v, const float* grad, int n, const float* count,
+                     float lr, float beta1, float beta2, float eps, float bc1, float bc2,
+                     void* w16, void* stream);
 
 /* ------------------------------------------------------------------------
  * Pruning without device allocation.

@@ -78,6 +78,7 @@ _SIGNATURES = {
     "dn_batch_synchronize": ([_vp], _i),
     "dn_batch_get_depthmap": ([_vp, _i, _f, _f, _f, _i32, _f], _i),
     "dn_batch_set_init": ([_vp, _i, _f], _i),
+    "dn_batch_set_schedule": ([_vp, _i, _i, _i, _i, ctypes.c_float, ctypes.c_float], _i),
     "dn_batch_pruned_count": ([_vp, ctypes.POINTER(ctypes.c_int64)], _i),
     "dn_batch_last_taps": ([_vp, ctypes.POINTER(ctypes.c_uint64)], _i),
     "dn_batch_set_view_image": ([_vp, _i, _u8, _i], _i),
@@ -89,6 +90,15 @@ _SIGNATURES = {
     "dn_batch_timer_elapsed": ([_vp, _f], _i),
     "dn_postprocess_depth": ([_f, _f, _i, _i], _i),
     "dn_fp32_peak": ([ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], _i),
+    "dn_batch_sweep_features": ([_vp, _vp, ctypes.c_int64, _i], _i),
+    "dn_batch_targets": ([_vp, _vp, ctypes.c_int64, ctypes.c_float], _i),
+    "dn_batch_init_from_output": ([_vp, _i, _vp], _i),
+    "dn_nn_conv3x3_forward": ([_vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _i, _vp, _vp, _vp], _i),
+    "dn_nn_conv3x3_backward": ([_vp, _vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _vp, _vp, _vp,
+                                _vp, _vp], _i),
+    "dn_nn_l1_loss": ([_vp, _vp, ctypes.c_int64, ctypes.c_float, _vp, _vp, _vp, _vp], _i),
+    "dn_nn_adam": ([_vp, _vp, _vp, _vp, _i, _vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                    ctypes.c_float, ctypes.c_float, ctypes.c_float, _vp, _vp], _i),
     "dn_prune_noalloc": ([_vp, _i, ctypes.c_float, _vp, _vp, _vp, _vp, ctypes.c_int64, _vp, _vp], _i),
     "dn_noalloc_last_error": ([], ctypes.c_char_p),
 }

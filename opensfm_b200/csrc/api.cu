@@ -16,6 +16,7 @@
 
 #include "dense_b200.h"
 #include "kernels.h"
+#include "learned.h"
 
 namespace {
 
@@ -190,6 +191,9 @@ struct Engine {
   int min_consistent = 2;
   int bx = 32, by = 4;  // thread block shape
   int variant = 4;      // lanes per pixel in init / half-passes (1, 2, 4)
+  int half_passes = -1;  // -1: 2 x iterations
+  int use_near = 1, use_far = 1, n_refine = 6;
+  float depth_range0 = 0.02f, normal_range0 = 0.5f;
   DevBuf<dn::ViewDev> d_views;
   DevBuf<dn::PairDev> d_pairs;
   DevBuf<dn::MapDev> d_maps;
@@ -450,6 +454,11 @@ struct Engine {
     a.p.taps = d_taps.p;
     a.p.error = d_error.p;
     a.p.variant = variant;
+    a.p.use_near = use_near;
+    a.p.use_far = use_far;
+    a.p.n_refine = n_refine;
+    a.p.depth_range0 = depth_range0;
+    a.p.normal_range0 = normal_range0;
     return a;
   }
 
@@ -486,12 +495,11 @@ struct Engine {
     DN_TRY(mark(1, timing));
     dn::LaunchArgs a2 = args(true);
     a2.p.taps = d_taps.p + 1;
-    for (int it = 0; it < iterations; ++it) {
-      for (int c = 0; c < 2; ++c) {
-        a2.p.colour = c;
-        a2.p.pass = 2 * it + c;
-        DN_CUDA(dn::launch_stage(dn::Stage::kHalfPass, sample, a2, stream));
-      }
+    const int hp = half_passes >= 0 ? half_passes : 2 * iterations;
+    for (int k = 0; k < hp; ++k) {
+      a2.p.colour = k & 1;
+      a2.p.pass = k;
+      DN_CUDA(dn::launch_stage(dn::Stage::kHalfPass, sample, a2, stream));
     }
     DN_TRY(mark(2, timing));
     a1.flag = 1;
@@ -1100,6 +1108,22 @@ dn_status dn_batch_set_params(dn_batch* b, int patch_size, float min_patch_sd, i
   b->eng.invalidate();
   return DN_OK;
 }
+dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int use_far,
+                                int n_refine, float depth_range0, float normal_range0) {
+  DN_CHECK(b, "NULL batch");
+  DN_CHECK(half_passes >= -1 && half_passes <= 2000, "half_passes must be -1..2000");
+  DN_CHECK(n_refine >= 0 && n_refine <= 12, "n_refine must be 0..12");
+  DN_CHECK(depth_range0 >= 0.f && normal_range0 >= 0.f, "ranges must be >= 0");
+  Engine& e = b->eng;
+  e.half_passes = half_passes;
+  e.use_near = use_near ? 1 : 0;
+  e.use_far = use_far ? 1 : 0;
+  e.n_refine = n_refine;
+  e.depth_range0 = depth_range0;
+  e.normal_range0 = normal_range0;
+  e.invalidate();
+  return DN_OK;
+}
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes) {
   DN_CHECK(b, "NULL batch");
   return b->eng.set_init(map_id, planes);
@@ -1221,6 +1245,122 @@ dn_status dn_batch_copy_depth_device(dn_batch* b, int map_id, float* d_out) {
   const View& r = *e.views[m.ref];
   DN_CUDA(cudaMemcpyAsync(d_out, m.depth.p, (size_t)r.W * r.H * sizeof(float),
                           cudaMemcpyDeviceToDevice, e.stream));
+  return DN_OK;
+}
+
+dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, int n_planes) {
+  DN_CHECK(b && feat, "NULL argument");
+  DN_CHECK(n_planes >= 1 && n_planes <= 8, "n_planes must be 1..8");
+  Engine& e = b->eng;
+  DN_CUDA(cudaSetDevice(e.device));
+  DN_CHECK(e.patch == 7, "the learned initialisation uses the 7 x 7 patch");
+  for (auto& m : e.maps) {
+    const View& r = *e.views[m->ref];
+    DN_CHECK((int64_t)r.W * r.H * dn::kFeatC <= map_stride, "map_stride too small");
+  }
+  DN_CHECK(e.variant == 4, "the feature sweep runs with 4 lanes per pixel (tuning variant 4)");
+  DN_TRY(e.check_params(Mode::kPatchMatch));
+  DN_TRY(e.prepare());
+  dn::LaunchArgs a = e.args(false);
+  a.tiles = e.d_tiles_init.p;  // 4 lanes per pixel tiling
+  a.n_tiles = e.n_tiles_init;
+  DN_CUDA(dn::launch_sweep(a, static_cast<__nv_bfloat16*>(feat), map_stride, n_planes, e.stream));
+  return DN_OK;
+}
+dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float min_score) {
+  DN_CHECK(b && target, "NULL argument");
+  Engine& e = b->eng;
+  DN_CHECK(e.computed, "no PatchMatch result computed yet");
+  DN_CUDA(cudaSetDevice(e.device));
+  for (size_t k = 0; k < e.maps.size(); ++k) {
+    const Map& m = *e.maps[k];
+    const View& r = *e.views[m.ref];
+    DN_CHECK((int64_t)r.W * r.H * 4 <= map_stride, "map_stride too small");
+    DN_CUDA(dn::launch_planes_to_target(m.state.p, m.score.p, r.W, r.H, e.d_maps.p, (int)k,
+                                        min_score, target + k * map_stride, e.stream));
+  }
+  return DN_OK;
+}
+dn_status dn_batch_init_from_output(dn_batch* b, int map_id, const float* out) {
+  DN_CHECK(b && out, "NULL argument");
+  Engine& e = b->eng;
+  DN_CHECK(map_id >= 0 && map_id < (int)e.maps.size(), "depthmap id out of range");
+  DN_CUDA(cudaSetDevice(e.device));
+  Map& m = *e.maps[map_id];
+  const View& r = *e.views[m.ref];
+  const size_t npx = (size_t)r.W * r.H;
+  if (!m.has_init) {
+    DN_CUDA(m.init.alloc(3 * npx));
+    m.has_init = true;
+    e.invalidate();
+  }
+  DN_TRY(e.prepare());
+  DN_CUDA(dn::launch_output_to_planes(out, r.W, r.H, e.d_maps.p, map_id, m.init.p, e.stream));
+  return DN_OK;
+}
+
+static bool nn_shape_ok(int cin, int cout) { return cin == 32 && (cout == 32 || cout == 4); }
+
+dn_status dn_nn_conv3x3_forward(const void* x, const void* w, const float* bias, int64_t n_pix,
+                                int H, int W, int cin, int cout, int relu, void* y, float* y32,
+                                void* stream) {
+  DN_CHECK(x && w && bias && (y || y32), "NULL argument");
+  DN_CHECK(nn_shape_ok(cin, cout), "supported shapes: cin 32, cout 32 or 4");
+  DN_CHECK(H > 0 && W > 0 && n_pix > 0 && n_pix % ((int64_t)H * W) == 0, "bad n_pix / H / W");
+  dn::ConvArgs c{};
+  c.x = static_cast<const __nv_bfloat16*>(x);
+  c.w = static_cast<const __nv_bfloat16*>(w);
+  c.bias = bias;
+  c.n_pix = n_pix;
+  c.H = H;
+  c.W = W;
+  c.cin = cin;
+  c.cout = cout;
+  c.relu = relu;
+  c.y = static_cast<__nv_bfloat16*>(y);
+  c.y32 = y32;
+  DN_CUDA(dn::conv3x3_forward(c, static_cast<cudaStream_t>(stream)));
+  return DN_OK;
+}
+dn_status dn_nn_conv3x3_backward(const void* dy, const void* x, const void* w,
+                                 const void* x_mask, int64_t n_pix, int H, int W, int cin,
+                                 int cout, void* dx, float* dw, float* db, void* wt_scratch,
+                                 void* stream) {
+  DN_CHECK(dy && x && w && dw && db && wt_scratch, "NULL argument");
+  DN_CHECK(nn_shape_ok(cin, cout), "supported shapes: cin 32, cout 32 or 4");
+  DN_CHECK(H > 0 && W > 0 && n_pix > 0 && n_pix % ((int64_t)H * W) == 0, "bad n_pix / H / W");
+  dn::ConvArgs c{};
+  c.x = static_cast<const __nv_bfloat16*>(x);
+  c.w = static_cast<const __nv_bfloat16*>(w);
+  c.n_pix = n_pix;
+  c.H = H;
+  c.W = W;
+  c.cin = cin;
+  c.cout = cout;
+  c.dy = static_cast<const __nv_bfloat16*>(dy);
+  c.x_mask = static_cast<const __nv_bfloat16*>(x_mask);
+  c.dx = static_cast<__nv_bfloat16*>(dx);
+  c.dw = dw;
+  c.db = db;
+  DN_CUDA(dn::conv3x3_backward(c, static_cast<__nv_bfloat16*>(wt_scratch),
+                               static_cast<cudaStream_t>(stream)));
+  return DN_OK;
+}
+dn_status dn_nn_l1_loss(const float* pred, const float* target, int64_t n_pix,
+                        float normal_weight, void* dpred, float* loss_sum, float* count,
+                        void* stream) {
+  DN_CHECK(pred && target && dpred && loss_sum && count && n_pix > 0, "bad argument");
+  DN_CUDA(dn::launch_l1_loss(pred, target, n_pix, normal_weight,
+                             static_cast<__nv_bfloat16*>(dpred), loss_sum, count,
+                             static_cast<cudaStream_t>(stream)));
+  return DN_OK;
+}
+dn_status dn_nn_adam(float* w, float* m, float* v, const float* grad, int n, const float* count,
+                     float lr, float beta1, float beta2, float eps, float bc1, float bc2,
+                     void* w16, void* stream) {
+  DN_CHECK(w && m && v && grad && count && n > 0, "bad argument");
+  DN_CUDA(dn::launch_adam(w, m, v, grad, n, count, lr, beta1, beta2, eps, bc1, bc2,
+                          static_cast<__nv_bfloat16*>(w16), static_cast<cudaStream_t>(stream)));
   return DN_OK;
 }
 

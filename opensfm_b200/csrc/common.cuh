@@ -75,6 +75,11 @@ struct RunParams {
   unsigned long long* taps;  // NCC tap counter
   int* error;                // device error word
   int variant;               // lanes per pixel (init and half-passes)
+  // PatchMatch candidate schedule (defaults follow PatchMatchUpdatePixel,
+  // depthmap.cc:305-374): adjacent planes, far planes, refinements and the
+  // first refinement's depth / normal-slope ranges.
+  int use_near, use_far, n_refine;
+  float depth_range0, normal_range0;
 };
 
 // ------------------------------------------------------------------ RNG

@@ -333,12 +333,15 @@ halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ vie
     // small and the warp's lanes at the same slot: 0-3 adjacent pixels,
     // 4-7 far samples, 8-13 refinements.
     int refn = curn;
-    float depth_range = 0.02f, normal_range = 0.5f;
+    float depth_range = p.depth_range0, normal_range = p.normal_range0;
+    const int n_slots = 8 + p.n_refine;
 #pragma unroll 1
-    for (int slot = 0; slot < 14; ++slot) {
+    for (int slot = 0; slot < n_slots; ++slot) {
       float3 v = make_float3(0.f, 0.f, 0.f);
       int view = 0;
       bool valid = false;
+      if (slot < 4 && !p.use_near) continue;
+      if (slot >= 4 && slot < 8 && !p.use_far) continue;
       if (slot < 8) {
         const int d = slot & 3;
         const int di = (d == 0) ? -1 : (d == 2 ? 1 : 0);

@@ -1,0 +1,492 @@
+// Learned PatchMatch initialisation (no reference counterpart; the
+// reference initialises at random, depthmap.cc:237-256).
+//
+//  - sweep_features_kernel: network input per pixel, NHWC BF16 with 32
+//    channels: the reference intensity, then the bilateral NCC
+//    (ComputePlaneImageScore) of 8 fronto-parallel planes uniform in inverse
+//    depth against the 2 nearest matching views (16 channels), zeros after.
+//  - conv3x3 forward / backward-data / backward-weight: 3x3 same-padding
+//    convolutions over NHWC BF16 activations as implicit GEMMs on the tensor
+//    cores (mma.sync m16n8k16, BF16 in, FP32 accumulate), bias and ReLU
+//    fused in the epilogues.
+//  - loss / Adam / plane kernels for training and for turning the network's
+//    (inverse depth, normal slopes) into PatchMatch initial planes.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "learned.h"
+
+namespace dn {
+
+// ---------------------------------------------------------------- sweep
+// 4 lanes per pixel (the 7 x 7 cooperative patch of the PatchMatch kernels).
+__global__ void __launch_bounds__(128)
+sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+                      const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
+                      __nv_bfloat16* __restrict__ feat, long long map_stride, int n_planes) {
+  extern __shared__ float tile[];
+  constexpr int HPZ = 3, L = 4;
+  const int4 tl = tiles[blockIdx.x];
+  const MapDev& m = maps[tl.x];
+  const ViewDev& rv = views[m.ref_view];
+  const int W = m.W, H = m.H;
+  const int px = blockDim.x / L;
+  const int x0 = tl.y * px, y0 = tl.z * blockDim.y;
+  const int pitch = px + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  for (int k = threadIdx.y * blockDim.x + threadIdx.x; k < pitch * rows;
+       k += blockDim.x * blockDim.y) {
+    const int r = k / pitch, c = k - r * pitch;
+    const int y = min(max(y0 - HPZ + r, 0), H - 1), x = min(max(x0 - HPZ + c, 0), W - 1);
+    tile[k] = __half2float(rv.img[(size_t)y * W + x]);
+  }
+  __syncthreads();
+  const int g = threadIdx.x / L, lane = threadIdx.x % L;
+  const unsigned mask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
+  const int i = y0 + threadIdx.y, j = x0 + g;
+  if (i >= H || j >= W) return;
+  float f[kFeatC];
+#pragma unroll
+  for (int c = 0; c < kFeatC; ++c) f[c] = 0.f;
+  f[0] = (tile[(threadIdx.y + HPZ) * pitch + g + HPZ] - 128.0f) * (1.0f / 64.0f);
+  if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) {
+    Patch<HPZ, L> pt;
+    pt.build(tile, pitch, threadIdx.y + HPZ, g + HPZ, lane, mask);
+    const double a = 1.0 / m.min_depth, b = 1.0 / m.max_depth;
+    unsigned taps = 0;
+    const int nv = min(2, m.n_pairs);
+    for (int p = 0; p < n_planes && p < 8; ++p) {
+      const float depth = (float)(1.0 / (a + (b - a) * (p + 0.5) / n_planes));
+      const float3 v = plane_from_depth_normal((float)j, (float)i, m.Kinv_d, depth,
+                                               make_float3(0.f, 0.f, -1.f));
+      const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
+      for (int k = 0; k < nv; ++k) {
+        const PairDev& pr = pairs[m.pair0 + k];
+        f[1 + 2 * p + k] = pt.view(views[pr.view], pr, h, (float)j, (float)i, taps);
+      }
+    }
+  }
+  if (lane != 0) return;
+  __nv_bfloat16* out = feat + (long long)tl.x * map_stride + ((size_t)i * W + j) * kFeatC;
+#pragma unroll
+  for (int c = 0; c < kFeatC; c += 2)
+    *reinterpret_cast<__nv_bfloat162*>(out + c) = __floats2bfloat162_rn(f[c], f[c + 1]);
+}
+
+// ------------------------------------------------------------ mma helper
+__device__ inline void mma_bf16(float d[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ inline uint32_t ld_pair(const __nv_bfloat16* p) {
+  return *reinterpret_cast<const uint32_t*>(p);
+}
+__device__ inline uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// Pixel index p of a batch of n images H x W -> (image, y, x); neighbour at
+// offset (dy, dx) or -1 outside the image.
+__device__ inline long long nbr_pixel(long long p, int H, int W, int dy, int dx) {
+  const long long hw = (long long)H * W;
+  const long long img = p / hw;
+  const int r = (int)(p - img * hw);
+  const int y = r / W + dy, x = r % W + dx;
+  if (y < 0 || y >= H || x < 0 || x >= W) return -1;
+  return img * hw + (long long)y * W + x;
+}
+
+// ------------------------------------------------------------ conv forward
+// y[p][co] = b[co] + sum_{tap, ci} x[p + tap][ci] * w[co][tap * CIN + ci];
+// M = pixels (16 per warp), N = COUT (padded to 8s), K = 9 * CIN.
+// Weights ([COUT][9 CIN] BF16, k contiguous) are staged in shared memory.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128)
+conv3x3_fwd_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ w,
+                   const float* __restrict__ bias, long long n_pix, int H, int W, int relu,
+                   __nv_bfloat16* __restrict__ y, float* __restrict__ y32) {
+  constexpr int K = 9 * CIN;
+  constexpr int NT = (COUT + 7) / 8;
+  __shared__ __align__(16) __nv_bfloat16 ws[NT * 8 * K];
+  for (int k = threadIdx.x; k < NT * 8 * K; k += blockDim.x)
+    ws[k] = (k / K) < COUT ? w[k] : __float2bfloat16(0.f);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const long long p0 = ((long long)blockIdx.x * 4 + warp) * 16;
+  if (p0 >= n_pix) return;
+  float acc[NT][4];
+#pragma unroll
+  for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+  const long long pa = p0 + g, pb = p0 + g + 8;
+#pragma unroll 1
+  for (int tap = 0; tap < 9; ++tap) {
+    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+    const long long qa = pa < n_pix ? nbr_pixel(pa, H, W, dy, dx) : -1;
+    const long long qb = pb < n_pix ? nbr_pixel(pb, H, W, dy, dx) : -1;
+#pragma unroll
+    for (int c0 = 0; c0 < CIN; c0 += 16) {
+      const uint32_t a0 = qa >= 0 ? ld_pair(x + qa * CIN + c0 + 2 * t) : 0u;
+      const uint32_t a1 = qb >= 0 ? ld_pair(x + qb * CIN + c0 + 2 * t) : 0u;
+      const uint32_t a2 = qa >= 0 ? ld_pair(x + qa * CIN + c0 + 2 * t + 8) : 0u;
+      const uint32_t a3 = qb >= 0 ? ld_pair(x + qb * CIN + c0 + 2 * t + 8) : 0u;
+      const int kk = tap * CIN + c0 + 2 * t;
+#pragma unroll
+      for (int n = 0; n < NT; ++n) {
+        const __nv_bfloat16* wr = ws + (n * 8 + g) * K + kk;
+        mma_bf16(acc[n], a0, a1, a2, a3, ld_pair(wr), ld_pair(wr + 8));
+      }
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < NT; ++n) {
+    const int co = n * 8 + 2 * t;
+    if (co >= COUT) continue;
+    const float b0 = bias[co], b1 = (co + 1 < COUT) ? bias[co + 1] : 0.f;
+    float v[4] = {acc[n][0] + b0, acc[n][1] + b1, acc[n][2] + b0, acc[n][3] + b1};
+    if (relu)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] = fmaxf(v[k], 0.f);
+    const long long rows[2] = {pa, pb};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long long p = rows[h];
+      if (p >= n_pix) continue;
+      if (y) {
+        if (co + 1 < COUT)
+          *reinterpret_cast<__nv_bfloat162*>(y + p * COUT + co) =
+              __floats2bfloat162_rn(v[2 * h], v[2 * h + 1]);
+        else
+          y[p * COUT + co] = __float2bfloat16(v[2 * h]);
+      }
+      if (y32) {
+        y32[p * COUT + co] = v[2 * h];
+        if (co + 1 < COUT) y32[p * COUT + co + 1] = v[2 * h + 1];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------- conv backward-data
+// dx[p][ci] = mask(x_in[p][ci] > 0) * sum_{tap, co} dy[p - tap][co] *
+// wt[ci][tap * COUT + co], wt the weights transposed to [CIN][9 COUT].
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128)
+conv3x3_bwd_data_kernel(const __nv_bfloat16* __restrict__ dy, const __nv_bfloat16* __restrict__ wt,
+                        const __nv_bfloat16* __restrict__ x_in, long long n_pix, int H, int W,
+                        __nv_bfloat16* __restrict__ dx) {
+  constexpr int COUTP = ((COUT + 15) / 16) * 16;  // K chunks of 16
+  constexpr int K = 9 * COUTP;
+  constexpr int NT = CIN / 8;
+  __shared__ __align__(16) __nv_bfloat16 ws[CIN * K];
+  for (int k = threadIdx.x; k < CIN * K; k += blockDim.x) ws[k] = wt[k];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const long long p0 = ((long long)blockIdx.x * 4 + warp) * 16;
+  if (p0 >= n_pix) return;
+  float acc[NT][4];
+#pragma unroll
+  for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+  const long long pa = p0 + g, pb = p0 + g + 8;
+#pragma unroll 1
+  for (int tap = 0; tap < 9; ++tap) {
+    const int dyy = 1 - tap / 3, dxx = 1 - tap % 3;  // dy at p - (tap offset)
+    const long long qa = pa < n_pix ? nbr_pixel(pa, H, W, dyy, dxx) : -1;
+    const long long qb = pb < n_pix ? nbr_pixel(pb, H, W, dyy, dxx) : -1;
+#pragma unroll
+    for (int c0 = 0; c0 < COUTP; c0 += 16) {
+      auto ld = [&](long long q, int c) -> uint32_t {
+        if (q < 0) return 0u;
+        const __nv_bfloat16 lo = c < COUT ? dy[q * COUT + c] : __float2bfloat16(0.f);
+        const __nv_bfloat16 hi = c + 1 < COUT ? dy[q * COUT + c + 1] : __float2bfloat16(0.f);
+        return pack2(lo, hi);
+      };
+      const uint32_t a0 = ld(qa, c0 + 2 * t), a1 = ld(qb, c0 + 2 * t);
+      const uint32_t a2 = ld(qa, c0 + 2 * t + 8), a3 = ld(qb, c0 + 2 * t + 8);
+      const int kk = tap * COUTP + c0 + 2 * t;
+#pragma unroll
+      for (int n = 0; n < NT; ++n) {
+        const __nv_bfloat16* wr = ws + (n * 8 + g) * K + kk;
+        mma_bf16(acc[n], a0, a1, a2, a3, ld_pair(wr), ld_pair(wr + 8));
+      }
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < NT; ++n) {
+    const int ci = n * 8 + 2 * t;
+    const long long rows[2] = {pa, pb};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long long p = rows[h];
+      if (p >= n_pix) continue;
+      float v0 = acc[n][2 * h], v1 = acc[n][2 * h + 1];
+      if (x_in) {
+        const __nv_bfloat162 xi = *reinterpret_cast<const __nv_bfloat162*>(x_in + p * CIN + ci);
+        if (!(__low2float(xi) > 0.f)) v0 = 0.f;
+        if (!(__high2float(xi) > 0.f)) v1 = 0.f;
+      }
+      *reinterpret_cast<__nv_bfloat162*>(dx + p * CIN + ci) = __floats2bfloat162_rn(v0, v1);
+    }
+  }
+}
+
+// Weights [COUT][9 CIN] -> [CIN][9 COUTP] (COUTP = COUT padded to 16).
+__global__ void transpose_weights_kernel(const __nv_bfloat16* __restrict__ w, int cin, int cout,
+                                         int coutp, __nv_bfloat16* __restrict__ wt) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = cin * 9 * coutp;
+  if (k >= n) return;
+  const int ci = k / (9 * coutp), r = k - ci * 9 * coutp, tap = r / coutp, co = r - tap * coutp;
+  wt[k] = co < cout ? w[(size_t)co * 9 * cin + tap * cin + ci] : __float2bfloat16(0.f);
+}
+
+// ----------------------------------------------------- conv backward-weight
+// dw[co][tap * CIN + ci] += sum_p dy[p][co] * x[p + tap][ci]: M = COUT
+// (tiles of 16), N = 9 CIN (tiles of 8, split over the 4 warps), K = pixels.
+// Each block reduces a chunk of pixels and adds its partial sums atomically.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128)
+conv3x3_bwd_weight_kernel(const __nv_bfloat16* __restrict__ dy, const __nv_bfloat16* __restrict__ x,
+                          long long n_pix, int H, int W, int pix_per_block,
+                          float* __restrict__ dw, float* __restrict__ db) {
+  constexpr int MT = (COUT + 15) / 16;
+  constexpr int NTOT = 9 * CIN / 8;
+  constexpr int NW = (NTOT + 3) / 4;  // n tiles per warp
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  float acc[MT][NW][4];
+#pragma unroll
+  for (int m = 0; m < MT; ++m)
+#pragma unroll
+    for (int n = 0; n < NW; ++n) acc[m][n][0] = acc[m][n][1] = acc[m][n][2] = acc[m][n][3] = 0.f;
+  float bsum[2] = {0.f, 0.f};
+  const long long pbeg = (long long)blockIdx.x * pix_per_block;
+  const long long pend = min(pbeg + pix_per_block, n_pix);
+  auto dyv = [&](long long p, int co) -> __nv_bfloat16 {
+    return (p < pend && co < COUT) ? dy[p * COUT + co] : __float2bfloat16(0.f);
+  };
+#pragma unroll 1
+  for (long long pk = pbeg; pk < pend; pk += 16) {
+    // A fragments: rows co, k = pixels pk + 2t (+1, +8, +9).
+    uint32_t a[MT][4];
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+      const int ca = m * 16 + g, cb = ca + 8;
+      a[m][0] = pack2(dyv(pk + 2 * t, ca), dyv(pk + 2 * t + 1, ca));
+      a[m][1] = pack2(dyv(pk + 2 * t, cb), dyv(pk + 2 * t + 1, cb));
+      a[m][2] = pack2(dyv(pk + 2 * t + 8, ca), dyv(pk + 2 * t + 9, ca));
+      a[m][3] = pack2(dyv(pk + 2 * t + 8, cb), dyv(pk + 2 * t + 9, cb));
+    }
+    if (warp == 0) {
+      // Bias gradient: lanes 0..15 own output channel 2 lanes each... simple
+      // per-lane sums over this 16-pixel step for co = lane, lane + 32.
+      for (int c = lane; c < COUT; c += 32)
+        for (int q = 0; q < 16; ++q) bsum[c / 32] += __bfloat162float(dyv(pk + q, c));
+    }
+#pragma unroll
+    for (int n = 0; n < NW; ++n) {
+      const int nt = warp * NW + n;
+      if (nt >= NTOT) break;
+      const int col = nt * 8 + g;  // (tap, ci)
+      const int tap = col / CIN, ci = col - tap * CIN;
+      const int dyy = tap / 3 - 1, dxx = tap % 3 - 1;
+      auto xv = [&](long long p) -> __nv_bfloat16 {
+        if (p >= pend) return __float2bfloat16(0.f);
+        const long long q = nbr_pixel(p, H, W, dyy, dxx);
+        return q >= 0 ? x[q * CIN + ci] : __float2bfloat16(0.f);
+      };
+      const uint32_t b0 = pack2(xv(pk + 2 * t), xv(pk + 2 * t + 1));
+      const uint32_t b1 = pack2(xv(pk + 2 * t + 8), xv(pk + 2 * t + 9));
+#pragma unroll
+      for (int m = 0; m < MT; ++m) mma_bf16(acc[m][n], a[m][0], a[m][1], a[m][2], a[m][3], b0, b1);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < MT; ++m)
+#pragma unroll
+    for (int n = 0; n < NW; ++n) {
+      const int nt = warp * NW + n;
+      if (nt >= NTOT) break;
+      const int co_a = m * 16 + g, co_b = co_a + 8, col = nt * 8 + 2 * t;
+      if (co_a < COUT) {
+        atomicAdd(dw + (size_t)co_a * 9 * CIN + col, acc[m][n][0]);
+        atomicAdd(dw + (size_t)co_a * 9 * CIN + col + 1, acc[m][n][1]);
+      }
+      if (co_b < COUT) {
+        atomicAdd(dw + (size_t)co_b * 9 * CIN + col, acc[m][n][2]);
+        atomicAdd(dw + (size_t)co_b * 9 * CIN + col + 1, acc[m][n][3]);
+      }
+    }
+  if (warp == 0)
+    for (int c = lane; c < COUT; c += 32) atomicAdd(db + c, bsum[c / 32]);
+}
+
+// ------------------------------------------------------------- loss / Adam
+// Output channels: 0 inverse depth t in [0, 1] over the depth range,
+// 1-2 normal slopes (sx, sy), normal ~ (sx, sy, -1).  L1 loss on pixels with
+// target weight > 0; gradient written as BF16 for the last layer's backward.
+__global__ void l1_loss_kernel(const float* __restrict__ pred, const float* __restrict__ target,
+                               long long n_pix, float normal_weight, __nv_bfloat16* __restrict__ dpred,
+                               float* __restrict__ loss_sum, float* __restrict__ count) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  float l = 0.f, c = 0.f;
+  if (p < n_pix) {
+    const float4 tg = *reinterpret_cast<const float4*>(target + 4 * p);  // t, sx, sy, weight
+    const float wgt = tg.w;
+    float g[4] = {0.f, 0.f, 0.f, 0.f};
+    if (wgt > 0.f) {
+      const float d0 = pred[4 * p] - tg.x, d1 = pred[4 * p + 1] - tg.y, d2 = pred[4 * p + 2] - tg.z;
+      l = wgt * (fabsf(d0) + normal_weight * (fabsf(d1) + fabsf(d2)));
+      c = wgt;
+      g[0] = wgt * copysignf(1.f, d0);
+      g[1] = wgt * normal_weight * copysignf(1.f, d1);
+      g[2] = wgt * normal_weight * copysignf(1.f, d2);
+    }
+    *reinterpret_cast<__nv_bfloat162*>(dpred + 4 * p) = __floats2bfloat162_rn(g[0], g[1]);
+    *reinterpret_cast<__nv_bfloat162*>(dpred + 4 * p + 2) = __floats2bfloat162_rn(g[2], g[3]);
+  }
+  for (int o = 16; o; o >>= 1) {
+    l += __shfl_xor_sync(0xffffffffu, l, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(loss_sum, l);
+    atomicAdd(count, c);
+  }
+}
+
+// Adam on FP32 master weights (grad scaled by 1 / count), BF16 copy out.
+__global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                            const float* __restrict__ grad, int n, const float* __restrict__ count,
+                            float lr, float b1, float b2, float eps, float bc1, float bc2,
+                            __nv_bfloat16* __restrict__ w16) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float c = fmaxf(*count, 1.f);
+  const float gr = grad[k] / c;
+  const float mk = b1 * m[k] + (1.f - b1) * gr;
+  const float vk = b2 * v[k] + (1.f - b2) * gr * gr;
+  m[k] = mk;
+  v[k] = vk;
+  const float nw = w[k] - lr * (mk / bc1) / (sqrtf(vk / bc2) + eps);
+  w[k] = nw;
+  if (w16) w16[k] = __float2bfloat16(nw);
+}
+
+// Network output -> PatchMatch initial planes for one map: depth from the
+// inverse-depth fraction, normal (sx, sy, -1), plane through the back-
+// projected point (PlaneFromDepthAndNormal, depthmap.cc:120-125).
+__global__ void output_to_planes_kernel(const float* __restrict__ out, int W, int H,
+                                        const MapDev* __restrict__ maps, int map,
+                                        float* __restrict__ planes) {
+  const MapDev& m = maps[map];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= W * H) return;
+  const int i = k / W, j = k - i * W;
+  const float t = fminf(fmaxf(out[4 * k], 0.f), 1.f);
+  const double a = 1.0 / m.max_depth, b = 1.0 / m.min_depth;
+  const float depth = (float)(1.0 / (a + (b - a) * (double)t));
+  const float sx = fminf(fmaxf(out[4 * k + 1], -4.f), 4.f);
+  const float sy = fminf(fmaxf(out[4 * k + 2], -4.f), 4.f);
+  const float3 v = plane_from_depth_normal((float)j, (float)i, m.Kinv_d, depth,
+                                           make_float3(sx, sy, -1.f));
+  planes[3 * (size_t)k] = v.x;
+  planes[3 * (size_t)k + 1] = v.y;
+  planes[3 * (size_t)k + 2] = v.z;
+}
+
+// PatchMatch result -> training target (t, sx, sy, weight).
+__global__ void planes_to_target_kernel(const float4* __restrict__ state,
+                                        const float* __restrict__ score, int W, int H,
+                                        const MapDev* __restrict__ maps, int map,
+                                        float min_score, float* __restrict__ target) {
+  const MapDev& m = maps[map];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= W * H) return;
+  const float4 s = state[k];
+  float4 tg = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (s.w > 0.f && s.z != 0.f && score[k] >= min_score) {
+    const double a = 1.0 / m.max_depth, b = 1.0 / m.min_depth;
+    const float t = (float)((1.0 / s.w - a) / (b - a));
+    tg = make_float4(fminf(fmaxf(t, 0.f), 1.f), fminf(fmaxf(-s.x / s.z, -4.f), 4.f),
+                     fminf(fmaxf(-s.y / s.z, -4.f), 4.f), 1.f);
+  }
+  *reinterpret_cast<float4*>(target + 4 * (size_t)k) = tg;
+}
+
+// ------------------------------------------------------------ launchers
+template <int CIN, int COUT>
+static cudaError_t conv_fwd_t(const ConvArgs& c, cudaStream_t s) {
+  const long long blocks = (c.n_pix + 63) / 64;
+  conv3x3_fwd_kernel<CIN, COUT><<<(unsigned)blocks, 128, 0, s>>>(c.x, c.w, c.bias, c.n_pix, c.H, c.W,
+                                                                 c.relu, c.y, c.y32);
+  return cudaGetLastError();
+}
+template <int CIN, int COUT>
+static cudaError_t conv_bwd_t(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaStream_t s) {
+  constexpr int COUTP = ((COUT + 15) / 16) * 16;
+  const long long blocks = (c.n_pix + 63) / 64;
+  if (c.dx) {
+    const int nt = CIN * 9 * COUTP;
+    transpose_weights_kernel<<<(nt + 255) / 256, 256, 0, s>>>(c.w, CIN, COUT, COUTP, wt_scratch);
+    conv3x3_bwd_data_kernel<CIN, COUT><<<(unsigned)blocks, 128, 0, s>>>(c.dy, wt_scratch, c.x_mask,
+                                                                        c.n_pix, c.H, c.W, c.dx);
+  }
+  const int ppb = 1024;
+  const long long wblocks = (c.n_pix + ppb - 1) / ppb;
+  conv3x3_bwd_weight_kernel<CIN, COUT><<<(unsigned)wblocks, 128, 0, s>>>(c.dy, c.x, c.n_pix, c.H, c.W,
+                                                                         ppb, c.dw, c.db);
+  return cudaGetLastError();
+}
+
+cudaError_t conv3x3_forward(const ConvArgs& c, cudaStream_t s) {
+  if (c.cin == 32 && c.cout == 32) return conv_fwd_t<32, 32>(c, s);
+  if (c.cin == 32 && c.cout == 4) return conv_fwd_t<32, 4>(c, s);
+  return cudaErrorInvalidValue;
+}
+cudaError_t conv3x3_backward(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaStream_t s) {
+  if (c.cin == 32 && c.cout == 32) return conv_bwd_t<32, 32>(c, wt_scratch, s);
+  if (c.cin == 32 && c.cout == 4) return conv_bwd_t<32, 4>(c, wt_scratch, s);
+  return cudaErrorInvalidValue;
+}
+cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
+                         int n_planes, cudaStream_t s) {
+  // a.tiles must be the 4-lanes-per-pixel tiling (bx / 4 pixels per row).
+  const size_t smem = sizeof(float) * (a.bx / 4 + 6) * (a.by + 6);
+  sweep_features_kernel<<<a.n_tiles, dim3(a.bx, a.by), smem, s>>>(a.maps, a.views, a.pairs, a.tiles,
+                                                                   feat, map_stride, n_planes);
+  return cudaGetLastError();
+}
+cudaError_t launch_l1_loss(const float* pred, const float* target, long long n_pix,
+                           float normal_weight, __nv_bfloat16* dpred, float* loss_sum, float* count,
+                           cudaStream_t s) {
+  l1_loss_kernel<<<(unsigned)((n_pix + 255) / 256), 256, 0, s>>>(pred, target, n_pix, normal_weight,
+                                                                 dpred, loss_sum, count);
+  return cudaGetLastError();
+}
+cudaError_t launch_adam(float* w, float* m, float* v, const float* grad, int n, const float* count,
+                        float lr, float b1, float b2, float eps, float bc1, float bc2,
+                        __nv_bfloat16* w16, cudaStream_t s) {
+  adam_kernel<<<(n + 255) / 256, 256, 0, s>>>(w, m, v, grad, n, count, lr, b1, b2, eps, bc1, bc2, w16);
+  return cudaGetLastError();
+}
+cudaError_t launch_output_to_planes(const float* out, int W, int H, const MapDev* maps, int map,
+                                    float* planes, cudaStream_t s) {
+  output_to_planes_kernel<<<(W * H + 255) / 256, 256, 0, s>>>(out, W, H, maps, map, planes);
+  return cudaGetLastError();
+}
+cudaError_t launch_planes_to_target(const float4* state, const float* score, int W, int H,
+                                    const MapDev* maps, int map, float min_score, float* target,
+                                    cudaStream_t s) {
+  planes_to_target_kernel<<<(W * H + 255) / 256, 256, 0, s>>>(state, score, W, H, maps, map,
+                                                              min_score, target);
+  return cudaGetLastError();
+}
+
+}  // namespace dn

@@ -1,0 +1,44 @@
+// Host-side entry points of the learned-initialisation kernels (learned.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "kernels.h"
+
+namespace dn {
+
+constexpr int kFeatC = 32;  // network input channels (17 used, zero padded)
+
+struct ConvArgs {
+  const __nv_bfloat16* x;       // input activations [n_pix][cin]
+  const __nv_bfloat16* w;       // weights [cout][9 cin]
+  const float* bias;            // [cout]
+  long long n_pix;              // pixels over the whole batch (images of H x W)
+  int H, W, cin, cout, relu;
+  __nv_bfloat16* y;             // forward output [n_pix][cout] (BF16) or null
+  float* y32;                   // forward output in FP32 or null
+  // backward
+  const __nv_bfloat16* dy;      // gradient of the (post-activation) output
+  const __nv_bfloat16* x_mask;  // input activations for the ReLU mask of dx, or null
+  __nv_bfloat16* dx;            // gradient of the input (null: not needed)
+  float* dw;                    // [cout][9 cin] accumulated (atomic adds)
+  float* db;                    // [cout] accumulated
+};
+
+cudaError_t conv3x3_forward(const ConvArgs& c, cudaStream_t s);
+cudaError_t conv3x3_backward(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaStream_t s);
+cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
+                         int n_planes, cudaStream_t s);
+cudaError_t launch_l1_loss(const float* pred, const float* target, long long n_pix,
+                           float normal_weight, __nv_bfloat16* dpred, float* loss_sum, float* count,
+                           cudaStream_t s);
+cudaError_t launch_adam(float* w, float* m, float* v, const float* grad, int n, const float* count,
+                        float lr, float b1, float b2, float eps, float bc1, float bc2,
+                        __nv_bfloat16* w16, cudaStream_t s);
+cudaError_t launch_output_to_planes(const float* out, int W, int H, const MapDev* maps, int map,
+                                    float* planes, cudaStream_t s);
+cudaError_t launch_planes_to_target(const float4* state, const float* score, int W, int H,
+                                    const MapDev* maps, int map, float min_score, float* target,
+                                    cudaStream_t s);
+
+}  // namespace dn

@@ -1,0 +1,423 @@
+"""Learned PatchMatch initialisation (no reference counterpart).
+
+The reference starts PatchMatch from random planes
+(``RandomInitialization``, ``opensfm/src/lib/dense/src/depthmap.cc:237-256``)
+and spends three raster iterations converging.  Here a small network proposes
+the initial plane of every pixel, so PatchMatch needs fewer iterations for
+the same accuracy; the random initialisation stays as the fallback for any
+pixel without a proposal.
+
+Network: 6 convolutions 3 x 3 (5 x 32 channels + ReLU, then 4 outputs),
+BF16 weights and activations, FP32 accumulation, run by the library's own
+tensor-core kernels (``dn_nn_*`` in ``include/dense_b200.h``).  Input per
+pixel: the reference intensity and the bilateral NCC of 8 swept
+fronto-parallel planes against the 2 nearest matching views
+(``dn_batch_sweep_features``).  Output: the inverse-depth fraction over the
+depth range and the normal slopes (sx, sy), normal ~ (sx, sy, -1).
+
+Training data: plain PatchMatch depthmaps of seeded synthetic scenes (box
+and terrain), computed by this library; targets are the pixels whose score
+is at least ``min_score``.  PyTorch only provides device buffers and a
+stream here; every kernel is the library's.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import time
+from dataclasses import dataclass
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib, pydense
+from . import synthetic as S
+
+FEAT_C = 32
+LAYERS = [(32, 32, 1)] * 5 + [(32, 4, 0)]  # (cin, cout, relu)
+WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
+DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "proposal_net.npz")
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(_torch().cuda.current_stream().cuda_stream)
+
+
+class ProposalNet:
+    """FP32 master weights + Adam state on the device, BF16 copies for the kernels."""
+
+    def __init__(self, seed: int = 0):
+        torch = _torch()
+        g = torch.Generator().manual_seed(seed)
+        self.w32, self.b32, self.w16 = [], [], []
+        for cin, cout, relu in LAYERS:
+            fan_in = 9 * cin
+            std = math.sqrt(2.0 / fan_in) if relu else math.sqrt(1.0 / fan_in)
+            w = torch.randn((cout, 9 * cin), generator=g) * std
+            self.w32.append(w.cuda())
+            self.b32.append(torch.zeros(cout).cuda())
+        self.sync_bf16()
+        self.m = [torch.zeros_like(t) for t in self.w32 + self.b32]
+        self.v = [torch.zeros_like(t) for t in self.w32 + self.b32]
+        self.step = 0
+        self.wt_scratch = torch.empty(32 * 9 * 32, dtype=torch.bfloat16, device="cuda")
+
+    def sync_bf16(self):
+        self.w16 = [w.to(_torch().bfloat16).contiguous() for w in self.w32]
+
+    # ------------------------------------------------------------ state
+    def state_dict(self) -> Dict[str, np.ndarray]:
+        d = {}
+        for k, (w, b) in enumerate(zip(self.w32, self.b32)):
+            d[f"w{k}"] = w.cpu().numpy()
+            d[f"b{k}"] = b.cpu().numpy()
+        d["step"] = np.array(self.step)
+        return d
+
+    def save(self, path: str, **extra):
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        d = self.state_dict()
+        d.update({k: np.asarray(v) for k, v in extra.items()})
+        np.savez(path, **d)
+
+    @classmethod
+    def load(cls, path: str = DEFAULT_WEIGHTS) -> "ProposalNet":
+        torch = _torch()
+        z = np.load(path)
+        net = cls.__new__(cls)
+        net.w32 = [torch.from_numpy(z[f"w{k}"]).cuda() for k in range(len(LAYERS))]
+        net.b32 = [torch.from_numpy(z[f"b{k}"]).cuda() for k in range(len(LAYERS))]
+        net.sync_bf16()
+        net.m = [torch.zeros_like(t) for t in net.w32 + net.b32]
+        net.v = [torch.zeros_like(t) for t in net.w32 + net.b32]
+        net.step = int(z["step"]) if "step" in z else 0
+        net.wt_scratch = torch.empty(32 * 9 * 32, dtype=torch.bfloat16, device="cuda")
+        return net
+
+    # ---------------------------------------------------------- compute
+    def forward(self, feat, n_pix: int, H: int, W: int, keep: bool = False):
+        """feat: BF16 [n_pix * 32].  Returns FP32 output [n_pix, 4] and, with
+        keep, the list of layer inputs for backward."""
+        torch = _torch()
+        L = _lib.load()
+        acts = [feat]
+        x = feat
+        out32 = torch.empty((n_pix, 4), dtype=torch.float32, device="cuda")
+        for k, (cin, cout, relu) in enumerate(LAYERS):
+            last = k == len(LAYERS) - 1
+            y = None if last else torch.empty(n_pix * cout, dtype=torch.bfloat16, device="cuda")
+            _lib.check(L.dn_nn_conv3x3_forward(
+                _ptr(x), _ptr(self.w16[k]), _ptr(self.b32[k]), n_pix, H, W, cin, cout, relu,
+                _ptr(y) if y is not None else None, _ptr(out32) if last else None, _stream()))
+            if not last:
+                x = y
+                acts.append(y)
+        return (out32, acts) if keep else out32
+
+    def backward(self, acts, dpred, n_pix: int, H: int, W: int):
+        """Gradients (FP32, summed over pixels) of every layer's weights and biases."""
+        torch = _torch()
+        L = _lib.load()
+        dws = [torch.zeros_like(w) for w in self.w32]
+        dbs = [torch.zeros_like(b) for b in self.b32]
+        dy = dpred
+        for k in range(len(LAYERS) - 1, -1, -1):
+            cin, cout, relu = LAYERS[k]
+            x = acts[k]
+            need_dx = k > 0
+            dx = torch.empty(n_pix * cin, dtype=torch.bfloat16, device="cuda") if need_dx else None
+            # dx is masked by the ReLU of the layer below (its output x > 0).
+            _lib.check(L.dn_nn_conv3x3_backward(
+                _ptr(dy), _ptr(x), _ptr(self.w16[k]), _ptr(x) if need_dx else None, n_pix, H, W,
+                cin, cout, _ptr(dx) if need_dx else None, _ptr(dws[k]), _ptr(dbs[k]),
+                _ptr(self.wt_scratch), _stream()))
+            dy = dx
+        return dws, dbs
+
+    def adam(self, dws, dbs, count, lr: float, b1=0.9, b2=0.999, eps=1e-8):
+        L = _lib.load()
+        self.step += 1
+        bc1 = 1.0 - b1 ** self.step
+        bc2 = 1.0 - b2 ** self.step
+        params = self.w32 + self.b32
+        grads = dws + dbs
+        w16 = self.w16 + [None] * len(self.b32)
+        for p, g, m, v, h in zip(params, grads, self.m, self.v, w16):
+            _lib.check(L.dn_nn_adam(_ptr(p), _ptr(m), _ptr(v), _ptr(g), p.numel(), _ptr(count), lr,
+                                    b1, b2, eps, bc1, bc2, _ptr(h) if h is not None else None,
+                                    _stream()))
+
+
+# ------------------------------------------------------------------ data
+@dataclass
+class SceneViews:
+    cams: List[S.Camera]
+    images: np.ndarray  # (n, H, W) uint8
+    depths: np.ndarray  # (n, H, W) float32 ground truth
+    ref: int
+    matching: List[int]  # nearest first; the first two are the sweep views
+
+
+def make_scene(seed: int, W: int, H: int, kind: Optional[str] = None, n_match: int = 6) -> SceneViews:
+    """Box scene on a camera ring, or terrain under a nadir grid (by seed parity)."""
+    rng = np.random.default_rng(seed)
+    kind = kind or ("box" if seed % 2 == 0 else "terrain")
+    if kind == "box":
+        scene = S.box_scene(seed)
+        n = n_match + 1
+        cams = S.ring_cameras(n, W, H, step_deg=10.0, start_deg=float(rng.uniform(0, 360)))
+        ref = n // 2
+    else:
+        scene = S.terrain_scene(seed, size=100.0, amp=8.0)
+        grid = S.nadir_cameras(100.0, 60.0, W, H, forward_overlap=0.7, side_overlap=0.6)
+        centres = np.stack([c.center for c in grid])
+        c0 = centres[int(rng.integers(len(grid)))]
+        order = np.argsort(np.linalg.norm(centres - c0, axis=1))[: n_match + 1]
+        cams = [grid[k] for k in order]
+        ref = 0
+    imgs, deps = S.render_gpu(scene, cams)
+    images = imgs.cpu().numpy()
+    depths = deps.cpu().numpy()
+    others = [k for k in range(len(cams)) if k != ref]
+    c_ref = cams[ref].center
+    others.sort(key=lambda k: float(np.linalg.norm(cams[k].center - c_ref)))
+    return SceneViews(cams, images, depths, ref, others[:n_match])
+
+
+def depth_range_of(sv: SceneViews) -> Tuple[float, float]:
+    return S.depth_range(sv.depths[sv.ref])
+
+
+def build_batch(scenes: Sequence[SceneViews], iterations: int = 3, seed: int = 1,
+                patch: int = 7, min_sd: float = 1.0) -> Tuple[pydense.Batch, List[int]]:
+    """One batch holding every scene's views; one depthmap per scene."""
+    b = pydense.Batch()
+    maps = []
+    for sv in scenes:
+        ids = [b.add_view(c.K, c.R, c.t, im) for c, im in zip(sv.cams, sv.images)]
+        mn, mx = depth_range_of(sv)
+        maps.append(b.add_depthmap(ids[sv.ref], [ids[k] for k in sv.matching], mn, mx))
+    b.set_params(patch_size=patch, min_patch_sd=min_sd, iterations=iterations, seed=seed)
+    return b, maps
+
+
+def features(b: pydense.Batch, n_maps: int, H: int, W: int, n_planes: int = 8):
+    torch = _torch()
+    stride = H * W * FEAT_C
+    feat = torch.zeros(n_maps * stride, dtype=torch.bfloat16, device="cuda")
+    _lib.check(b._L.dn_batch_sweep_features(b._h, _ptr(feat), stride, n_planes))
+    b.synchronize()
+    return feat
+
+
+def targets(b: pydense.Batch, n_maps: int, H: int, W: int, min_score: float = 0.5):
+    torch = _torch()
+    stride = H * W * 4
+    tg = torch.zeros(n_maps * stride, dtype=torch.float32, device="cuda")
+    _lib.check(b._L.dn_batch_targets(b._h, _ptr(tg), stride, min_score))
+    b.synchronize()
+    return tg
+
+
+def make_dataset(seeds: Sequence[int], W: int = 320, H: int = 240, chunk: int = 100,
+                 iterations: int = 3, log=None):
+    """Features and plain-PatchMatch targets for every seed (device tensors)."""
+    torch = _torch()
+    feats, tgs = [], []
+    t0 = time.time()
+    for c0 in range(0, len(seeds), chunk):
+        scenes = [make_scene(s, W, H) for s in seeds[c0:c0 + chunk]]
+        b, maps = build_batch(scenes, iterations=iterations, seed=int(seeds[c0]) + 7)
+        b.run()
+        b.synchronize()
+        tgs.append(targets(b, len(maps), H, W))
+        feats.append(features(b, len(maps), H, W))
+        b.close()
+        if log:
+            log(f"dataset {c0 + len(scenes)}/{len(seeds)} scenes, {time.time() - t0:.1f} s")
+    return torch.cat(feats), torch.cat(tgs)
+
+
+# -------------------------------------------------------------- training
+def train(net: ProposalNet, feat, tgt, n_maps: int, H: int, W: int, steps: int = 1500,
+          batch: int = 8, lr: float = 2e-3, normal_weight: float = 0.1, seed: int = 0, log=None):
+    torch = _torch()
+    L = _lib.load()
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    per = H * W
+    n_pix = batch * per
+    loss_acc = torch.zeros(1, dtype=torch.float32, device="cuda")
+    count = torch.zeros(1, dtype=torch.float32, device="cuda")
+    dpred = torch.empty(n_pix * 4, dtype=torch.bfloat16, device="cuda")
+    fv = feat.view(n_maps, per * FEAT_C)
+    tv = tgt.view(n_maps, per * 4)
+    history = []
+    t0 = time.time()
+    for step in range(steps):
+        idx = torch.randint(0, n_maps, (batch,), generator=g).cuda()
+        xb = fv.index_select(0, idx).reshape(-1).contiguous()
+        tb = tv.index_select(0, idx).reshape(-1).contiguous()
+        out, acts = net.forward(xb, n_pix, H, W, keep=True)
+        loss_acc.zero_()
+        count.zero_()
+        _lib.check(L.dn_nn_l1_loss(_ptr(out), _ptr(tb), n_pix, normal_weight, _ptr(dpred),
+                                   _ptr(loss_acc), _ptr(count), _stream()))
+        dws, dbs = net.backward(acts, dpred, n_pix, H, W)
+        cur_lr = lr * 0.5 * (1 + math.cos(math.pi * step / steps))
+        net.adam(dws, dbs, count, cur_lr)
+        if step % 100 == 0 or step == steps - 1:
+            l = float(loss_acc.item() / max(count.item(), 1.0))
+            history.append((step, l))
+            if log:
+                log(f"step {step} loss {l:.4f} lr {cur_lr:.2e} {time.time() - t0:.1f} s")
+    return history
+
+
+# ------------------------------------------------------------- inference
+def propose(net: ProposalNet, b: pydense.Batch, maps: Sequence[int], H: int, W: int):
+    """Runs the sweep and the network for every depthmap of the batch and
+    installs the proposals as the batch's initial planes."""
+    torch = _torch()
+    n = len(maps)
+    feat = features(b, n, H, W)
+    out = net.forward(feat, n * H * W, H, W)
+    torch.cuda.synchronize()
+    for k, m in enumerate(maps):
+        _lib.check(b._L.dn_batch_init_from_output(b._h, int(m), _ptr(out[k * H * W:])))
+    b.synchronize()
+    return out
+
+
+def main(argv=None):
+    """Trains the proposal network: python -m opensfm_b200.learned --scenes 2000."""
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scenes", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args(argv)
+    torch = _torch()
+    log = lambda s: print(s, flush=True)  # noqa: E731
+    seeds = list(range(100000, 100000 + args.scenes))
+    feat, tgt = make_dataset(seeds, log=log)
+    valid = float((tgt.view(-1, 4)[:, 3] > 0).float().mean().item())
+    log(f"target coverage {valid:.3f}")
+    net = ProposalNet(seed=args.seed)
+    hist = train(net, feat, tgt, len(seeds), 240, 320, steps=args.steps, batch=args.batch,
+                 lr=args.lr, log=log)
+    net.save(args.out, history=np.array(hist), scenes=np.array(args.scenes),
+             seeds_start=np.array(seeds[0]))
+    log(f"saved {args.out}")
+
+
+if __name__ == "__main__":
+    main()
+
+
+# ------------------------------------------------------------ evaluation
+# PatchMatch schedules compared by evaluate(): (name, init, half-passes,
+# set_schedule keyword arguments).  "plain" is the reference's random
+# initialisation with its candidate schedule.
+PLAIN_3IT = ("plain-3it", "plain", 6, {})
+SCHEDULES = [
+    ("plain-1it", "plain", 2, {}),
+    ("plain-2it", "plain", 4, {}),
+    PLAIN_3IT,
+    ("learned-0hp", "learned", 0, {}),
+    ("learned-1hp", "learned", 1, {}),
+    ("learned-2hp", "learned", 2, {}),
+    ("learned-4hp", "learned", 4, {}),
+    ("learned-near-2hp", "learned", 2, dict(use_far=False, depth_range0=0.05, normal_range0=0.3)),
+    ("learned-near-3hp", "learned", 3, dict(use_far=False, depth_range0=0.05, normal_range0=0.3)),
+    ("learned-near-4hp", "learned", 4, dict(use_far=False, depth_range0=0.05, normal_range0=0.3)),
+]
+
+
+def evaluate(net: Optional[ProposalNet], seeds: Sequence[int], W: int = 640, H: int = 480,
+             schedules=SCHEDULES, repeats: int = 3, log=None) -> dict:
+    """Plain (random init) vs learned-init PatchMatch on held-out scenes.
+
+    For every schedule: the mean accuracy (|d - gt| / gt <= 1 % over valid
+    ground-truth pixels) and the device time of one batched run over all the
+    scenes; learned settings add the feature sweep and the network time.
+    """
+    torch = _torch()
+    scenes = [make_scene(s, W, H) for s in seeds]
+    b, maps = build_batch(scenes, iterations=3, seed=int(seeds[0]) + 11)
+    gts = [sv.depths[sv.ref] for sv in scenes]
+
+    def acc():
+        return float(np.mean([S.accuracy(b.get_depth(m), gt) for m, gt in zip(maps, gts)]))
+
+    def timed(fn):
+        fn()  # warm-up (and graph capture)
+        b.synchronize()
+        ts = []
+        for _ in range(repeats):
+            b.timer_record(0)
+            fn()
+            b.timer_record(1)
+            b.synchronize()
+            ts.append(b.timer_elapsed())
+        return float(np.median(ts))
+
+    out = {"scenes": len(seeds), "W": W, "H": H, "runs": []}
+    t_sweep = t_net = 0.0
+    if net is not None:
+        stride = H * W * FEAT_C
+        feat = torch.zeros(len(maps) * stride, dtype=torch.bfloat16, device="cuda")
+        _lib.check(b._L.dn_batch_sweep_features(b._h, _ptr(feat), stride, 8))
+        b.synchronize()
+        net.forward(feat, len(maps) * H * W, H, W)
+        torch.cuda.synchronize()
+        b.timer_record(0)
+        _lib.check(b._L.dn_batch_sweep_features(b._h, _ptr(feat), stride, 8))
+        b.timer_record(1)
+        b.synchronize()
+        t_sweep = b.timer_elapsed()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = net.forward(feat, len(maps) * H * W, H, W)
+        e1.record()
+        torch.cuda.synchronize()
+        t_net = e0.elapsed_time(e1)
+        out["proposal_ms"] = {"sweep": t_sweep, "network": t_net}
+    plain_ms = None
+    for name, init, hp, kw in schedules:
+        if init == "learned" and net is None:
+            continue
+        for k, m in enumerate(maps):
+            if init == "learned":
+                _lib.check(b._L.dn_batch_init_from_output(b._h, int(m), _ptr(res[k * H * W:])))
+            else:
+                b.set_init(m, None)
+        b.set_schedule(half_passes=hp, **kw)
+        t = timed(lambda: b.run(graph=True))
+        total = t + (t_sweep + t_net if init == "learned" else 0.0)
+        r = {"name": name, "init": init, "half_passes": hp, "schedule": kw, "accuracy": acc(),
+             "ms_patchmatch": t, "ms": total}
+        if name == PLAIN_3IT[0]:
+            plain_ms = total
+        out["runs"].append(r)
+        if log:
+            log(f"{name:20s} acc {r['accuracy']:.4f} pm {t:7.2f} ms total {total:7.2f} ms")
+    if plain_ms:
+        for r in out["runs"]:
+            r["speedup_vs_plain_3it"] = plain_ms / r["ms"]
+    b.close()
+    return out

@@ -301,6 +301,14 @@ class Batch(_Handle):
                                           int(iterations), float(same_depth_threshold),
                                           int(min_consistent_views), int(seed)))
 
+    def set_schedule(self, half_passes: int = -1, use_near: bool = True, use_far: bool = True,
+                     n_refine: int = 6, depth_range0: float = 0.02,
+                     normal_range0: float = 0.5) -> None:
+        """PatchMatch half-passes and candidate sets (defaults: the reference's schedule)."""
+        check(self._L.dn_batch_set_schedule(self._h, int(half_passes), int(bool(use_near)),
+                                            int(bool(use_far)), int(n_refine), float(depth_range0),
+                                            float(normal_range0)))
+
     def set_init(self, map_id: int, planes: Optional[np.ndarray]) -> None:
         if planes is None:
             check(self._L.dn_batch_set_init(self._h, int(map_id), None))

@@ -46,6 +46,66 @@ def build(force: bool = False) -> str:
     return _LIB_PATH
 
 
+_GPU_SRC = os.path.join(_HERE, "raycast_gpu.cu")
+_GPU_LIB = os.path.join(_HERE, "_build", "libraycast_gpu.so")
+_glib = None
+
+
+def build_gpu(force: bool = False) -> str:
+    """Compiles the CUDA ray caster (sm_100a) next to its source."""
+    if force or not os.path.exists(_GPU_LIB) or (
+        os.path.getmtime(_GPU_LIB) < os.path.getmtime(_GPU_SRC)
+    ):
+        os.makedirs(os.path.dirname(_GPU_LIB), exist_ok=True)
+        subprocess.check_call(["/usr/local/cuda/bin/nvcc", "-gencode",
+                               "arch=compute_100a,code=sm_100a", "-O3", "-Xcompiler", "-fPIC",
+                               "-shared", "-o", _GPU_LIB, _GPU_SRC])
+    return _GPU_LIB
+
+
+def _load_gpu():
+    global _glib
+    if _glib is None:
+        lib = ctypes.CDLL(build_gpu())
+        d = ctypes.c_void_p
+        lib.rcg_render.argtypes = [
+            d, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+            ctypes.c_double, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32, ctypes.c_double,
+            ctypes.c_int, ctypes.c_double, ctypes.c_double, d, ctypes.c_int, ctypes.c_int,
+            ctypes.c_int, ctypes.c_int, d, d, d]
+        lib.rcg_render.restype = ctypes.c_int
+        _glib = lib
+    return _glib
+
+
+def render_gpu(scene: "Scene", cams, supersample: int = 2):
+    """Ray-casts views on the current CUDA device (torch tensors on 'cuda').
+
+    Returns (images uint8 (n, H, W), depths float32 (n, H, W)) as torch CUDA
+    tensors.  All cameras must share one size.
+    """
+    import torch
+
+    lib = _load_gpu()
+    W, H = cams[0].width, cams[0].height
+    n = len(cams)
+    cam = np.concatenate([np.concatenate([c.K.ravel(), c.R.ravel(), c.t.ravel()]) for c in cams])
+    dcam = torch.from_numpy(cam.astype(np.float64)).cuda()
+    boxes = scene.boxes.reshape(-1) if scene.boxes.size else np.zeros(6)
+    dbox = torch.from_numpy(np.ascontiguousarray(boxes, np.float64)).cuda()
+    imgs = torch.empty((n, H, W), dtype=torch.uint8, device="cuda")
+    deps = torch.empty((n, H, W), dtype=torch.float32, device="cuda")
+    st = lib.rcg_render(dbox.data_ptr(), int(scene.boxes.shape[0]), int(scene.ground),
+                        float(scene.ground_half), int(scene.terrain), scene.terrain_amp,
+                        scene.terrain_scale, scene.terrain_seed, scene.terrain_octaves,
+                        scene.tex_seed, scene.tex_freq, scene.tex_octaves, scene.contrast,
+                        scene.sky, dcam.data_ptr(), n, W, H, supersample, imgs.data_ptr(),
+                        deps.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    if st != 0:
+        raise RuntimeError(f"rcg_render failed with CUDA error {st}")
+    return imgs, deps
+
+
 def _load():
     global _lib
     if _lib is None:

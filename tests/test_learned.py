@@ -1,0 +1,164 @@
+"""GPU tests of the learned-initialisation kernels: forward and backward of
+the tensor-core 3x3 convolutions against a float64 PyTorch CPU oracle, the
+loss / Adam kernels, and one training step of the whole network.
+
+Tolerances: activations and weights are BF16 (8 bits of mantissa), sums are
+FP32; results are compared relative to the oracle's largest magnitude:
+single-layer outputs within 1e-2, gradients within 2e-2."""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+pytestmark = pytest.mark.gpu
+
+if not gpu_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+torch = pytest.importorskip("torch")
+
+from opensfm_b200 import _lib, learned  # noqa: E402
+
+
+def _bf(t):
+    return t.to(torch.bfloat16)
+
+
+def _ref_conv(x_nhwc, w, b, relu):
+    """float64 oracle: x (n, H, W, cin), w (cout, 9 cin) with k = tap * cin + ci."""
+    n, H, W, cin = x_nhwc.shape
+    cout = w.shape[0]
+    wt = w.view(cout, 3, 3, cin).permute(0, 3, 1, 2)
+    z = torch.nn.functional.conv2d(x_nhwc.permute(0, 3, 1, 2), wt, b, padding=1)
+    y = torch.relu(z) if relu else z
+    return y.permute(0, 2, 3, 1)
+
+
+def _rel(a, b):
+    return float((a - b).abs().max() / max(b.abs().max(), 1e-12))
+
+
+@pytest.mark.parametrize("cout,relu", [(32, 1), (4, 0)])
+def test_conv_forward_matches_float64(cout, relu):
+    g = torch.Generator().manual_seed(cout)
+    n, H, W, cin = 2, 9, 13, 32
+    x = _bf(torch.randn((n, H, W, cin), generator=g))
+    w = _bf(torch.randn((cout, 9 * cin), generator=g) * 0.1)
+    b = torch.randn(cout, generator=g) * 0.1
+    L = _lib.load()
+    n_pix = n * H * W
+    y32 = torch.empty((n_pix, cout), dtype=torch.float32, device="cuda")
+    y16 = torch.empty((n_pix * cout,), dtype=torch.bfloat16, device="cuda")
+    xd, wd, bd = x.cuda().contiguous(), w.cuda().contiguous(), b.cuda().contiguous()
+    _lib.check(L.dn_nn_conv3x3_forward(learned._ptr(xd), learned._ptr(wd), learned._ptr(bd), n_pix,
+                                       H, W, cin, cout, relu, learned._ptr(y16), learned._ptr(y32),
+                                       None))
+    torch.cuda.synchronize()
+    ref = _ref_conv(x.double(), w.double(), b.double(), relu).reshape(n_pix, cout)
+    assert _rel(y32.cpu().double(), ref) < 1e-4  # FP32 accumulation of BF16 products
+    assert _rel(y16.view(n_pix, cout).cpu().double(), ref) < 1e-2
+
+
+@pytest.mark.parametrize("cout", [32, 4])
+def test_conv_backward_matches_float64(cout):
+    g = torch.Generator().manual_seed(100 + cout)
+    n, H, W, cin = 2, 7, 11, 32
+    x = _bf(torch.relu(torch.randn((n, H, W, cin), generator=g)))  # a ReLU output
+    w = _bf(torch.randn((cout, 9 * cin), generator=g) * 0.1)
+    dz = _bf(torch.randn((n, H, W, cout), generator=g))
+    L = _lib.load()
+    n_pix = n * H * W
+    xd, wd, dzd = x.cuda().contiguous(), w.cuda().contiguous(), dz.cuda().contiguous()
+    dx = torch.empty((n_pix * cin,), dtype=torch.bfloat16, device="cuda")
+    dw = torch.zeros((cout, 9 * cin), dtype=torch.float32, device="cuda")
+    db = torch.zeros((cout,), dtype=torch.float32, device="cuda")
+    scratch = torch.empty(32 * 9 * 32, dtype=torch.bfloat16, device="cuda")
+    P = learned._ptr
+    _lib.check(L.dn_nn_conv3x3_backward(P(dzd), P(xd), P(wd), P(xd), n_pix, H, W, cin, cout, P(dx),
+                                        P(dw), P(db), P(scratch), None))
+    torch.cuda.synchronize()
+    # float64 oracle via autograd: z = conv(x, w); dL/dz = dz.
+    xr = x.double().requires_grad_(True)
+    wr = w.double().requires_grad_(True)
+    br = torch.zeros(cout, dtype=torch.float64, requires_grad=True)
+    z = _ref_conv(xr, wr, br, 0)
+    z.backward(dz.double())
+    want_dx = xr.grad * (x.double() > 0)
+    assert _rel(dw.cpu().double(), wr.grad) < 2e-2
+    assert _rel(db.cpu().double(), br.grad) < 2e-2
+    assert _rel(dx.view(n, H, W, cin).cpu().double(), want_dx) < 2e-2
+
+
+def test_network_gradient_matches_float64():
+    """Whole-network gradient of the L1 loss against float64 autograd on the
+    same BF16-quantised weights and input (intermediate BF16 rounding is the
+    only difference)."""
+    g = torch.Generator().manual_seed(7)
+    n, H, W = 2, 10, 12
+    net = learned.ProposalNet(seed=3)
+    x = _bf(torch.randn((n, H, W, 32), generator=g) * 0.5)
+    n_pix = n * H * W
+    tgt = torch.rand((n_pix, 4), generator=g)
+    tgt[:, 3] = (torch.rand(n_pix, generator=g) > 0.2).float()
+    out, acts = net.forward(x.cuda().reshape(-1).contiguous(), n_pix, H, W, keep=True)
+    L = _lib.load()
+    P = learned._ptr
+    loss = torch.zeros(1, device="cuda")
+    cnt = torch.zeros(1, device="cuda")
+    dpred = torch.empty(n_pix * 4, dtype=torch.bfloat16, device="cuda")
+    tg = tgt.cuda().contiguous()
+    _lib.check(L.dn_nn_l1_loss(P(out), P(tg), n_pix, 0.1, P(dpred), P(loss), P(cnt), None))
+    dws, dbs = net.backward(acts, dpred, n_pix, H, W)
+    torch.cuda.synchronize()
+    # Oracle, rounding to BF16 where the kernels store BF16: each hidden
+    # layer's output, and the gradient flowing into each layer's output.
+    bf = lambda t: t.to(torch.bfloat16).double()  # noqa: E731
+    ws = [w.cpu().to(torch.bfloat16).double().requires_grad_(True) for w in net.w32]
+    bs = [b.cpu().double().requires_grad_(True) for b in net.b32]
+    h = x.double()
+    for k, (cin, cout, relu) in enumerate(learned.LAYERS):
+        h = _ref_conv(h, ws[k], bs[k], relu)
+        if k < len(learned.LAYERS) - 1:
+            h = bf(h)
+            h.register_hook(lambda g: bf(g))
+    pred = h.reshape(n_pix, 4)
+    pred.register_hook(lambda g: bf(g))
+    wgt = tgt[:, 3].double()
+    l = (wgt * ((pred[:, 0] - tgt[:, 0]).abs() + 0.1 * ((pred[:, 1] - tgt[:, 1]).abs() +
+                                                        (pred[:, 2] - tgt[:, 2]).abs()))).sum()
+    l.backward()
+    assert abs(float(loss.item()) - float(l)) / float(l) < 2e-2
+    assert abs(float(cnt.item()) - float(wgt.sum())) < 1e-3
+    for k in range(len(learned.LAYERS)):
+        assert _rel(dws[k].cpu().double(), ws[k].grad) < 2e-2, k
+        assert _rel(dbs[k].cpu().double(), bs[k].grad) < 2e-2, k
+
+
+def test_adam_step_matches_formula():
+    L = _lib.load()
+    P = learned._ptr
+    w = torch.randn(1000, device="cuda")
+    m = torch.zeros_like(w)
+    v = torch.zeros_like(w)
+    grad = torch.randn(1000, device="cuda")
+    cnt = torch.tensor([4.0], device="cuda")
+    w0 = w.clone()
+    w16 = torch.empty(1000, dtype=torch.bfloat16, device="cuda")
+    _lib.check(L.dn_nn_adam(P(w), P(m), P(v), P(grad), 1000, P(cnt), 0.01, 0.9, 0.999, 1e-8,
+                            0.1, 0.001, P(w16), None))
+    torch.cuda.synchronize()
+    gr = grad / 4
+    mk = 0.1 * gr
+    vk = 0.001 * gr * gr
+    want = w0 - 0.01 * (mk / 0.1) / (torch.sqrt(vk / 0.001) + 1e-8)
+    assert torch.allclose(w, want, rtol=1e-5, atol=1e-6)
+    assert torch.equal(w16, w.to(torch.bfloat16))
+
+
+def test_short_training_reduces_loss():
+    """Trains on 16 seeded scenes for 60 steps: the loss must drop."""
+    seeds = list(range(500, 516))
+    feat, tgt = learned.make_dataset(seeds, W=160, H=120, chunk=16)
+    net = learned.ProposalNet(seed=1)
+    hist = learned.train(net, feat, tgt, len(seeds), 120, 160, steps=60, batch=4, lr=3e-3)
+    assert hist[-1][1] < 0.8 * hist[0][1], hist
