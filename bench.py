@@ -5,8 +5,9 @@ Workload (one "step"): a ring reconstruction of 24 reference views at
 640 x 480 (box scene: ground plane + 12 boxes, 4-octave value-noise texture),
 each depthmap scored against its 6 nearest matching views with patch 7,
 min patch sd 1.0 and 3 PatchMatch iterations, then DepthmapCleaner
-(threshold 0.01, 3 consistent views) over each map's 10 candidate
-neighbours.  Synthetic, seeded, ray-cast in this process.
+(threshold 0.01, 3 consistent views) and DepthmapPruner (threshold 0.01)
+over each map's 10 candidate neighbours.  Synthetic, seeded, ray-cast in
+this process.
 
 ``value``: depthmaps/s with the views resident in HBM (one batched run per
 step, replayed from a CUDA graph), device-timed over K steps.  ``e2e``: the
@@ -261,20 +262,38 @@ def run_ours(args):
     vs, ranges, cands, matches = work
     n_maps = args.maps or len(vs.cameras)
     b = build_batch(work, n_maps=n_maps)
+    tuning = None
     if args.tuning:
         bx, by, var = (int(x) for x in args.tuning.split(","))
         b.set_tuning(bx, by, var)
+        tuning = {"choice": [bx, by, var], "source": "--tuning"}
+    else:
+        from opensfm_b200 import autotune
+
+        key = autotune.workload_key([(H_, W_)] * n_maps, [N_MATCH] * n_maps, PATCH)
+        t = autotune.tune(b, key, {"prune": True, "graph": True})
+        tuning = {"choice": list(t["choice"]), "ms": t["ms"], "cached": t["cached"],
+                  "source": "opensfm_b200.autotune"}
 
     # Warm-up (graph capture on the first run).
     for _ in range(args.warmup):
-        b.run(clean=True, graph=True)
+        b.run(prune=True, graph=True)
     b.synchronize()
 
     # Stage timings and tap counts from one instrumented run (outside the
-    # timed region): the roofline of the dominant kernel.
-    b.run(clean=True, graph=False, timing=True)
+    # timed region): the roofline of the dominant kernel.  Stage events need
+    # one launch per stage, so a persistent choice is timed as its per-stage
+    # equivalent (same tiles and lanes; results are identical).
+    choice = tuning["choice"]
+    if choice[2] & 8:
+        b.set_tuning(choice[0], choice[1], choice[2] & 7)
+    b.run(prune=True, graph=False, timing=True)
     b.synchronize()
     stages, taps = b.timings()
+    if choice[2] & 8:
+        b.set_tuning(*choice)
+        b.run(prune=True, graph=True)
+        b.synchronize()
     hp_ms = stages[1]
     achieved = FLOPS_PER_TAP * taps[1] / (hp_ms * 1e-3) / 1e12
     peak = pydense.fp32_peak()
@@ -290,11 +309,12 @@ def run_ours(args):
         b.synchronize()
         b.timer_record(0)
         for _ in range(args.steps):
-            b.run(clean=True, graph=True)
+            b.run(prune=True, graph=True)
         b.timer_record(1)
         b.synchronize()
         ms = b.timer_elapsed()
         group.barrier()
+    pruned = b.pruned_count()
     ms_max = group.max(ms)
     value = world * n_maps * args.steps / (ms_max * 1e-3)
 
@@ -308,7 +328,7 @@ def run_ours(args):
     for _ in range(args.steps):
         for v, im in enumerate(imgs[:n_maps]):
             b.set_view_image(v, im)
-        b.run(clean=True, graph=True)
+        b.run(prune=True, graph=True)
         for v in range(n_maps):
             _lib.check(b._L.dn_batch_get_depthmap(b._h, v, None, None, None, None, ptr(out, _f)))
     b.timer_record(1)
@@ -325,13 +345,15 @@ def run_ours(args):
             "workload": f"ring reconstruction, {n_maps} reference views {W_}x{H_}, "
                         f"{N_MATCH} matching views, {N_CAND} cleaner neighbours, PatchMatch "
                         f"{ITERS} iterations (red-black), patch {PATCH}, min_patch_sd {MIN_SD}, "
-                        f"cleaner 0.01 / 3 views; plain random initialisation",
+                        f"cleaner 0.01 / 3 views, pruner 0.01; plain random initialisation",
+            "pruned_points": pruned,
             "init": "plain", "global_batch": n_maps * world, "parallelism": f"replicas x{world}",
+            "tuning": tuning,
             "l2": "working set larger than L2 (views, tables and state ~%.0f MB)" % (
                 n_maps * ((W_ + 15) * (H_ + 15) * 16 + W_ * H_ * (16 + 4 + 4 + 4 + 4 + 2)) / 1e6),
             "accuracy_1pct_median": float(np.median(accs)),
             "stage_ms": {"init": stages[0], "halfpasses": stages[1], "post": stages[2],
-                         "clean": stages[3], "total": stages[4]},
+                         "clean_and_prune": stages[3], "total": stages[4]},
         },
         "roofline": {
             "kernel": "halfpass_kernel<3,false>", "bound": "fp32", "achieved": achieved,
@@ -348,8 +370,10 @@ def run_ours(args):
         "clocks": {k: v for k, v in clk.summary().items()},
     }
     # Launch count per step: memsets are not kernels; init + 2*iters
-    # half-passes + post + one cleaner launch per map.
-    line["gpu_launches"] = args.steps * (1 + 2 * ITERS + 1 + n_maps)
+    # half-passes + post (or one persistent launch for all three) + one
+    # cleaner launch and three pruner launches per map.
+    pm_launches = 1 if (tuning and tuning["choice"][2] & 8) else (1 + 2 * ITERS + 1)
+    line["gpu_launches"] = args.steps * (pm_launches + 4 * n_maps)
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_sample(work, seconds=args.cpu_seconds)

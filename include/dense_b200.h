@@ -194,6 +194,13 @@ dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int 
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes);
 /* Total kept pruner points over all maps of the last run (after sync). */
 dn_status dn_batch_pruned_count(dn_batch* b, int64_t* count);
+/* One map's pruner output of the last DN_RUN_PRUNE run (after sync): the
+ * cleaned depth and PatchMatch planes of the map and of its cleaner maps go
+ * through DepthmapPruner::Prune (depthmap.cc:577-637), colour = the view's
+ * gray level, label 0.  *count receives the point count; buffers (any may
+ * be NULL) hold `capacity` points. */
+dn_status dn_batch_get_points(dn_batch* b, int map_id, float* points, float* normals,
+                              uint8_t* colors, uint8_t* labels, int64_t capacity, int64_t* count);
 /* NCC taps evaluated by the last run (device counter). */
 dn_status dn_batch_last_taps(dn_batch* b, uint64_t* taps);
 /* Replaces the pixels of an uploaded view (same size), asynchronously on
@@ -206,10 +213,13 @@ dn_status dn_batch_set_view_image(dn_batch* b, int view_id, const uint8_t* image
  * NCC taps of init (taps_out[0]) and of the half-passes (taps_out[1]). */
 dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_out);
 /* Launch tuning (no reference counterpart): thread block shape bx x by
- * (bx * by <= 128, bx a multiple of 32) and the lanes that share one pixel
- * in the initialisation and PatchMatch kernels (1, 2 or 4; 2 and 4 apply to
- * the 7 x 7 patch).  Chosen by opensfm_b200.autotune; scores agree between
- * settings to float rounding of the sums. */
+ * (bx * by <= 128, bx a multiple of 32); variant = the lanes that share one
+ * pixel in the initialisation and PatchMatch kernels (1, 2 or 4; 2 and 4
+ * apply to the 7 x 7 patch), plus 8 to run initialisation, every half-pass
+ * and the post-process of all depthmaps in ONE cooperative persistent
+ * launch (32 x 4 blocks, 7 x 7 patch; tiles taken from atomic counters,
+ * bounded grid barriers between stages).  Chosen by opensfm_b200.autotune;
+ * scores agree between settings to float rounding of the sums. */
 dn_status dn_batch_set_tuning(dn_batch* b, int bx, int by, int variant);
 dn_status dn_estimator_set_tuning(dn_estimator* est, int bx, int by, int variant);
 /* Device timer on the batch stream: record event `slot` (0 or 1), and the

@@ -80,6 +80,8 @@ _SIGNATURES = {
     "dn_batch_set_init": ([_vp, _i, _f], _i),
     "dn_batch_set_schedule": ([_vp, _i, _i, _i, _i, ctypes.c_float, ctypes.c_float], _i),
     "dn_batch_pruned_count": ([_vp, ctypes.POINTER(ctypes.c_int64)], _i),
+    "dn_batch_get_points": ([_vp, _i, _f, _f, _u8, _u8, ctypes.c_int64,
+                             ctypes.POINTER(ctypes.c_int64)], _i),
     "dn_batch_last_taps": ([_vp, ctypes.POINTER(ctypes.c_uint64)], _i),
     "dn_batch_set_view_image": ([_vp, _i, _u8, _i], _i),
     "dn_batch_last_timings": ([_vp, _f, _i, ctypes.POINTER(ctypes.c_uint64)], _i),

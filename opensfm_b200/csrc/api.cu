@@ -173,6 +173,10 @@ struct Map {
   DevBuf<float> score, depth, clean, init, plane_out;
   DevBuf<int> nghbr;
   bool has_init = false;
+  // Pruner (DN_RUN_PRUNE): views (this map first), scratch, outputs.
+  DevBuf<dn::PruneView> prune_views;
+  DevBuf<uint8_t> prune_scratch, prune_colors, prune_labels;
+  DevBuf<float> prune_points, prune_normals;
 };
 
 enum class Mode { kBruteForce, kPatchMatch, kPatchMatchSample, kScorePlanes };
@@ -192,6 +196,8 @@ struct Engine {
   int bx = 32, by = 4;  // thread block shape
   int variant = 4;      // lanes per pixel in init / half-passes (1, 2, 4)
   int half_passes = -1;  // -1: 2 x iterations
+  int persistent = 0;    // one cooperative persistent launch per PatchMatch run
+  DevBuf<unsigned> d_sync;
   int use_near = 1, use_far = 1, n_refine = 6;
   float depth_range0 = 0.02f, normal_range0 = 0.5f;
   DevBuf<dn::ViewDev> d_views;
@@ -431,6 +437,9 @@ struct Engine {
     n_tiles1 = (int)t1.size();
     n_tiles2 = (int)t2.size();
     n_tiles_init = (int)ti.size();
+    // Counters of the persistent launch (allocated here, outside any capture).
+    const int n_half = half_passes >= 0 ? half_passes : 2 * iterations;
+    DN_CUDA(d_sync.alloc(4 + std::max(n_half, 0)));
     dirty = false;
     return DN_OK;
   }
@@ -488,6 +497,28 @@ struct Engine {
       return DN_OK;
     }
     const bool sample = (mode == Mode::kPatchMatchSample);
+    const int hp = half_passes >= 0 ? half_passes : 2 * iterations;
+    if (persistent && !sample && patch == 7) {
+      DN_CHECK(d_sync.p && d_sync.n >= (size_t)(4 + hp), "persistent launch buffers not prepared");
+      DN_CUDA(cudaMemsetAsync(d_sync.p, 0, (4 + hp) * sizeof(unsigned), stream));
+      dn::PersistentArgs pa{};
+      pa.base = a1;
+      pa.tiles_init = d_tiles_init.p;
+      pa.n_init = n_tiles_init;
+      pa.tiles_hp = d_tiles2.p;
+      pa.n_hp = n_tiles2;
+      pa.tiles_post = d_tiles1.p;
+      pa.n_post = n_tiles1;
+      pa.n_half = hp;
+      pa.sync = d_sync.p;
+      pa.base.p.taps = d_taps.p + 1;
+      DN_CUDA(dn::launch_persistent(pa, stream));
+      DN_TRY(mark(1, timing));
+      DN_TRY(mark(2, timing));
+      DN_TRY(mark(3, timing));
+      DN_TRY(mark(4, timing));
+      return DN_OK;
+    }
     dn::LaunchArgs ai = a1;
     ai.tiles = d_tiles_init.p;
     ai.n_tiles = n_tiles_init;
@@ -495,7 +526,6 @@ struct Engine {
     DN_TRY(mark(1, timing));
     dn::LaunchArgs a2 = args(true);
     a2.p.taps = d_taps.p + 1;
-    const int hp = half_passes >= 0 ? half_passes : 2 * iterations;
     for (int k = 0; k < hp; ++k) {
       a2.p.colour = k & 1;
       a2.p.pass = k;
@@ -541,6 +571,59 @@ struct Engine {
       DN_CUDA(cudaMemcpyAsync(d_clean_lists.p, lists.data(), lists.size() * sizeof(int),
                               cudaMemcpyHostToDevice, stream));
     DN_CUDA(cudaStreamSynchronize(stream));
+    return DN_OK;
+  }
+
+  // Pruner tables and buffers (outside any stream capture): per map the
+  // cleaned depth and PatchMatch planes of the map and its cleaner maps.
+  DevBuf<unsigned long long> d_prune_counts;
+  dn_status prepare_prune() {
+    DN_CUDA(d_prune_counts.alloc(std::max<size_t>(maps.size(), 1)));
+    for (size_t k = 0; k < maps.size(); ++k) {
+      Map& m = *maps[k];
+      const View& r = *views[m.ref];
+      const size_t npx = (size_t)r.W * r.H;
+      std::vector<dn::PruneView> pv;
+      std::vector<int> ids = {(int)k};
+      for (int o : m.clean_maps) ids.push_back(o);
+      for (int id : ids) {
+        Map& om = *maps[id];
+        const View& ov = *views[om.ref];
+        dn::PruneView v{};
+        v.depth = om.clean.p;
+        v.plane = reinterpret_cast<const float*>(om.state.p);
+        v.plane_stride = 4;
+        v.color = nullptr;
+        v.label = nullptr;
+        v.gray = ov.gray.p;
+        v.W = ov.W;
+        v.H = ov.H;
+        std::memcpy(v.K, ov.cam.K, sizeof(v.K));
+        std::memcpy(v.R, ov.cam.R, sizeof(v.R));
+        std::memcpy(v.t, ov.cam.t, sizeof(v.t));
+        pv.push_back(v);
+      }
+      DN_CUDA(m.prune_views.alloc(pv.size()));
+      DN_CUDA(m.prune_scratch.alloc(dn::prune_scratch_bytes(r.W, r.H)));
+      DN_CUDA(m.prune_points.alloc(3 * npx));
+      DN_CUDA(m.prune_normals.alloc(3 * npx));
+      DN_CUDA(m.prune_colors.alloc(3 * npx));
+      DN_CUDA(m.prune_labels.alloc(npx));
+      DN_CUDA(cudaMemcpyAsync(m.prune_views.p, pv.data(), pv.size() * sizeof(dn::PruneView),
+                              cudaMemcpyHostToDevice, stream));
+    }
+    DN_CUDA(cudaStreamSynchronize(stream));
+    return DN_OK;
+  }
+  dn_status enqueue_prune() {
+    for (size_t k = 0; k < maps.size(); ++k) {
+      Map& m = *maps[k];
+      const View& r = *views[m.ref];
+      dn::PruneOut o{m.prune_points.p, m.prune_normals.p, m.prune_colors.p, m.prune_labels.p};
+      DN_CUDA(dn::launch_prune(m.prune_views.p, 1 + (int)m.clean_maps.size(), r.W, r.H,
+                               same_depth_thr, m.prune_scratch.p, o, d_prune_counts.p + k, stream));
+    }
+    DN_TRY(mark(4, timed));
     return DN_OK;
   }
 
@@ -792,6 +875,7 @@ dn_status dn_estimator_set_depth_range(dn_estimator* est, double mn, double mx, 
 dn_status dn_estimator_set_patchmatch_iterations(dn_estimator* est, int n) {
   DN_CHECK(est, "NULL estimator");
   est->eng.iterations = n;
+  est->eng.invalidate();
   return DN_OK;
 }
 
@@ -987,6 +1071,7 @@ dn_status dn_pruner_add_view(dn_pruner* p, const double* K, const double* R, con
   DN_CUDA(cudaMemcpyAsync(lab.p, label, n, cudaMemcpyHostToDevice, p->stream));
   DN_CUDA(cudaStreamSynchronize(p->stream));
   dn::PruneView v{};
+  v.plane_stride = 3;
   v.depth = d.p;
   v.plane = pl.p;
   v.color = col.p;
@@ -1134,6 +1219,8 @@ dn_status dn_batch_run(dn_batch* b, unsigned flags) {
   DN_CUDA(cudaSetDevice(e.device));
   DN_TRY(e.check_params(Mode::kPatchMatch));
   DN_TRY(e.prepare());
+  DN_CHECK(!(flags & DN_RUN_PRUNE) || (flags & DN_RUN_CLEAN),
+           "DN_RUN_PRUNE prunes the cleaned depthmaps: add DN_RUN_CLEAN");
   const bool use_graph = (flags & DN_RUN_GRAPH) != 0;
   const bool timing = (flags & DN_RUN_TIMING) != 0;
   e.timed = timing;
@@ -1153,10 +1240,12 @@ dn_status dn_batch_run(dn_batch* b, unsigned flags) {
     }
     // Allocations and host-to-device table uploads happen before capture.
     if (flags & DN_RUN_CLEAN) DN_TRY(e.prepare_clean());
+    if (flags & DN_RUN_PRUNE) DN_TRY(e.prepare_prune());
     cudaGraph_t g = nullptr;
     DN_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
     dn_status s = e.enqueue(Mode::kPatchMatch, timing);
     if (s == DN_OK && (flags & DN_RUN_CLEAN)) s = e.enqueue_clean(timing);
+    if (s == DN_OK && (flags & DN_RUN_PRUNE)) s = e.enqueue_prune();
     cudaError_t ce = cudaStreamEndCapture(e.stream, &g);
     if (s != DN_OK) {
       if (g) cudaGraphDestroy(g);
@@ -1170,8 +1259,10 @@ dn_status dn_batch_run(dn_batch* b, unsigned flags) {
     DN_CUDA(cudaGraphLaunch(e.graph, e.stream));
   } else {
     if (flags & DN_RUN_CLEAN) DN_TRY(e.prepare_clean());
+    if (flags & DN_RUN_PRUNE) DN_TRY(e.prepare_prune());
     DN_TRY(e.enqueue(Mode::kPatchMatch, timing));
     if (flags & DN_RUN_CLEAN) DN_TRY(e.enqueue_clean(timing));
+    if (flags & DN_RUN_PRUNE) DN_TRY(e.enqueue_prune());
   }
   b->ran = true;
   e.computed = true;
@@ -1189,7 +1280,38 @@ dn_status dn_batch_get_depthmap(dn_batch* b, int map_id, float* depth, float* pl
 }
 dn_status dn_batch_pruned_count(dn_batch* b, int64_t* count) {
   DN_CHECK(b && count, "NULL argument");
-  return fail(DN_NOT_READY, "batched pruning is not enabled in this build");
+  Engine& e = b->eng;
+  DN_CHECK(e.d_prune_counts.p, "no pruner run yet (DN_RUN_PRUNE)");
+  DN_CUDA(cudaSetDevice(e.device));
+  std::vector<unsigned long long> c(e.maps.size());
+  DN_CUDA(cudaMemcpy(c.data(), e.d_prune_counts.p, c.size() * sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost));
+  int64_t t = 0;
+  for (auto v : c) t += (int64_t)v;
+  *count = t;
+  return DN_OK;
+}
+dn_status dn_batch_get_points(dn_batch* b, int map_id, float* points, float* normals,
+                              uint8_t* colors, uint8_t* labels, int64_t capacity, int64_t* count) {
+  DN_CHECK(b && count, "NULL argument");
+  Engine& e = b->eng;
+  DN_CHECK(map_id >= 0 && map_id < (int)e.maps.size(), "depthmap id out of range");
+  DN_CHECK(e.d_prune_counts.p, "no pruner run yet (DN_RUN_PRUNE)");
+  DN_CUDA(cudaSetDevice(e.device));
+  unsigned long long c = 0;
+  DN_CUDA(cudaMemcpy(&c, e.d_prune_counts.p + map_id, sizeof(c), cudaMemcpyDeviceToHost));
+  *count = (int64_t)c;
+  if (!points && !normals && !colors && !labels) return DN_OK;
+  DN_CHECK(capacity >= (int64_t)c, "capacity is smaller than the pruned point count");
+  const Map& m = *e.maps[map_id];
+  const size_t n = (size_t)c;
+  if (n) {
+    if (points) DN_CUDA(cudaMemcpy(points, m.prune_points.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (normals) DN_CUDA(cudaMemcpy(normals, m.prune_normals.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (colors) DN_CUDA(cudaMemcpy(colors, m.prune_colors.p, 3 * n, cudaMemcpyDeviceToHost));
+    if (labels) DN_CUDA(cudaMemcpy(labels, m.prune_labels.p, n, cudaMemcpyDeviceToHost));
+  }
+  return DN_OK;
 }
 dn_status dn_batch_last_taps(dn_batch* b, uint64_t* taps) {
   DN_CHECK(b, "NULL batch");
@@ -1206,10 +1328,15 @@ dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_o
 static dn_status set_tuning(Engine& e, int bx, int by, int variant) {
   DN_CHECK(bx >= 32 && bx % 32 == 0 && by >= 1 && bx * by <= 128,
            "block shape must have bx a multiple of 32 and bx * by <= 128");
-  DN_CHECK(variant == 1 || variant == 2 || variant == 4, "lanes per pixel must be 1, 2 or 4");
+  // variant = lanes per pixel (1, 2, 4) + 8 for the persistent launch.
+  const int lanes = variant & 7;
+  DN_CHECK(lanes == 1 || lanes == 2 || lanes == 4, "lanes per pixel must be 1, 2 or 4");
+  DN_CHECK(!(variant & 8) || (bx == 32 && by == 4),
+           "the persistent launch uses 32 x 4 thread blocks");
   e.bx = bx;
   e.by = by;
-  e.variant = variant;
+  e.variant = lanes;
+  e.persistent = (variant & 8) ? 1 : 0;
   e.invalidate();
   return DN_OK;
 }

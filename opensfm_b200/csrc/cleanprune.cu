@@ -169,7 +169,7 @@ __device__ inline bool prune_pixel(const PruneView* __restrict__ views, int n_vi
   const float depth = rv.depth[pix];
   if (depth <= 0.0f) return false;
   float nrm[3];
-  normalize3f(rv.plane + 3 * pix, nrm);
+  normalize3f(rv.plane + (size_t)rv.plane_stride * pix, nrm);
   const float area = (float)__dmul_rn((double)__fdiv_rn(-nrm[2], depth), rv.K[0]);
   backproject_f((double)j, (double)i, (double)depth, Kinv, rv.R, rv.t, pt);
   for (int o = 1; o < n_views; ++o) {
@@ -188,7 +188,7 @@ __device__ inline bool prune_pixel(const PruneView* __restrict__ views, int n_vi
     const float keepf = __fsub_rn(1.0f, thr);
     if ((double)dr > __dmul_rn((double)keepf, rp[2])) {
       float no[3];
-      normalize3f(ov.plane + 3 * q, no);
+      normalize3f(ov.plane + (size_t)ov.plane_stride * q, no);
       if (dr == 0.0f || __dmul_rn((double)__fdiv_rn(-no[2], dr), ov.K[0]) > (double)area)
         return false;
     }
@@ -298,9 +298,9 @@ prune_write_kernel(const PruneView* __restrict__ views, int n_views, float thr,
   for (int a = 0; a < 3; ++a) {
     out.points[3 * (size_t)pos + a] = pt[a];
     out.normals[3 * (size_t)pos + a] = nr[a];
-    out.colors[3 * (size_t)pos + a] = rv.color[3 * k + a];
+    out.colors[3 * (size_t)pos + a] = rv.color ? rv.color[3 * k + a] : rv.gray[k];
   }
-  out.labels[pos] = rv.label[k];
+  out.labels[pos] = rv.label ? rv.label[k] : 0;
 }
 
 size_t prune_scratch_bytes(int W, int H) {

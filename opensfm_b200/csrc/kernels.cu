@@ -105,11 +105,10 @@ __device__ inline float patch_variance(const float* tile, int pitch, int ly, int
 // a warp row owns one pixel; every lane of a group computes the same values
 // and lane 0 writes them.
 template <int HPZ, bool SAMPLE, int L>
-__global__ void __launch_bounds__(128, (kMinBlocksL<HPZ, L>))
-init_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
-            const PairDev* __restrict__ pairs, const int4* __restrict__ tiles, RunParams p) {
+__device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+                                 const PairDev* __restrict__ pairs, const int4 tl,
+                                 const RunParams& p) {
   extern __shared__ float tile[];
-  const int4 tl = tiles[blockIdx.x];
   const MapDev& m = maps[tl.x];
   const ViewDev& rv = views[m.ref_view];
   const int W = m.W, H = m.H;
@@ -168,6 +167,13 @@ init_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
     }
   }
   flush_taps(taps, p.taps);
+}
+
+template <int HPZ, bool SAMPLE, int L>
+__global__ void __launch_bounds__(128, (kMinBlocksL<HPZ, L>))
+init_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+            const PairDev* __restrict__ pairs, const int4* __restrict__ tiles, RunParams p) {
+  init_tile<HPZ, SAMPLE, L>(maps, views, pairs, tiles[blockIdx.x], p);
 }
 
 // ----------------------------------------------------------------------
@@ -275,12 +281,11 @@ score_planes_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__
 // its score at this pixel is the current score.
 
 template <int HPZ, bool SAMPLE, int L>
-__global__ void __launch_bounds__(128, (kMinBlocksL<HPZ, L>))
-halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
-                const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
-                RunParams p) {
+__device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
+                                     const ViewDev* __restrict__ views,
+                                     const PairDev* __restrict__ pairs, const int4 tl,
+                                     const RunParams& p) {
   extern __shared__ float tile[];
-  const int4 tl = tiles[blockIdx.x];
   const MapDev& m = maps[tl.x];
   const ViewDev& rv = views[m.ref_view];
   const int W = m.W, H = m.H;
@@ -413,6 +418,14 @@ halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ vie
   flush_taps(taps, p.taps);
 }
 
+template <int HPZ, bool SAMPLE, int L>
+__global__ void __launch_bounds__(128, (kMinBlocksL<HPZ, L>))
+halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+                const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
+                RunParams p) {
+  halfpass_tile<HPZ, SAMPLE, L>(maps, views, pairs, tiles[blockIdx.x], p);
+}
+
 // ----------------------------------------------------------------------
 // PostProcess (depthmap.cc:489-502): 5x5 median of the depth (replicated
 // border, as cv::medianBlur does for float input); a pixel keeps its depth
@@ -449,9 +462,7 @@ __device__ inline float post_value(float d, float med) {
   return zero ? 0.0f : d;
 }
 
-__global__ void postprocess_kernel(const MapDev* __restrict__ maps, const int4* __restrict__ tiles,
-                                   int apply) {
-  const int4 tl = tiles[blockIdx.x];
+__device__ inline void post_tile(const MapDev* __restrict__ maps, const int4 tl, int apply) {
   const MapDev& m = maps[tl.x];
   const int W = m.W, H = m.H;
   const int i = tl.z * blockDim.y + threadIdx.y, j = tl.y * blockDim.x + threadIdx.x;
@@ -465,6 +476,85 @@ __global__ void postprocess_kernel(const MapDev* __restrict__ maps, const int4* 
   const float4* st = m.state;
   const float med = median5([&](int y, int x) { return st[(size_t)y * W + x].w; }, i, j, W, H);
   m.depth[pix] = post_value(d, med);
+}
+
+__global__ void postprocess_kernel(const MapDev* __restrict__ maps, const int4* __restrict__ tiles,
+                                   int apply) {
+  post_tile(maps, tiles[blockIdx.x], apply);
+}
+
+// ----------------------------------------------------------------------
+// One persistent launch for a whole PatchMatch run over every depthmap of
+// the batch: initialisation, all half-passes and the post-process.  Blocks
+// take tiles of the current stage from an atomic counter (maps of different
+// sizes balance across SMs) and meet at a grid barrier between stages.  The
+// launch is cooperative, so every block is resident and the barrier cannot
+// deadlock; each wait is still bounded, and on expiry the kernel sets the
+// error word and returns (the host reports DN_TIMEOUT).
+// sync: [0] arrivals, [1] generation, [2 + s] tile counter of stage s.
+constexpr long long kBarrierSpins = 1LL << 25;
+
+__device__ inline bool grid_barrier(unsigned* sync, unsigned n_blocks, int* error) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    volatile unsigned* gen = sync + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(sync, 1u);
+    if (arrived == n_blocks - 1) {
+      atomicExch(sync, 0u);
+      __threadfence();
+      atomicAdd(sync + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*gen == g) {
+        if (++spins > kBarrierSpins || *(volatile int*)error) {
+          atomicExch(error, 1);
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+    ok = *(volatile int*)error == 0;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+__device__ inline int next_tile(unsigned* counter) {
+  __shared__ int t;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) t = (int)atomicAdd(counter, 1u);
+  __syncthreads();
+  return t;
+}
+
+template <int HPZ, int L>
+__global__ void __launch_bounds__(128, (kMinBlocksL<HPZ, L>))
+patchmatch_persistent_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+                             const PairDev* __restrict__ pairs,
+                             const int4* __restrict__ tiles_init, int n_init,
+                             const int4* __restrict__ tiles_hp, int n_hp,
+                             const int4* __restrict__ tiles_post, int n_post, int n_half,
+                             RunParams p, unsigned* sync) {
+  const unsigned nb = gridDim.x;
+  for (int t = next_tile(sync + 2); t < n_init; t = next_tile(sync + 2))
+    init_tile<HPZ, false, L>(maps, views, pairs, tiles_init[t], p);
+  if (!grid_barrier(sync, nb, p.error)) return;
+  RunParams q = p;
+  for (int k = 0; k < n_half; ++k) {
+    q.colour = k & 1;
+    q.pass = k;
+    unsigned* ctr = sync + 3 + k;
+    for (int t = next_tile(ctr); t < n_hp; t = next_tile(ctr))
+      halfpass_tile<HPZ, false, L>(maps, views, pairs, tiles_hp[t], q);
+    if (!grid_barrier(sync, nb, p.error)) return;
+  }
+  // The post-process tiles are bx x by pixels of 32 x 4 threads.
+  unsigned* ctr = sync + 3 + n_half;
+  for (int t = next_tile(ctr); t < n_post; t = next_tile(ctr)) post_tile(maps, tiles_post[t], 1);
 }
 
 __global__ void postprocess_plain_kernel(const float* __restrict__ in, float* __restrict__ out,
@@ -564,6 +654,43 @@ cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStre
       return launch_hpz<3, 1>(stage, sample, a, s);
     case 4: return launch_hpz<4, 1>(stage, sample, a, s);
     case 5: return launch_hpz<5, 1>(stage, sample, a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int L>
+static cudaError_t launch_persistent_l(const PersistentArgs& pa, cudaStream_t s) {
+  auto kern = patchmatch_persistent_kernel<3, L>;
+  const LaunchArgs& a = pa.base;
+  const int px = a.bx / L;
+  const size_t smem = sizeof(float) * (2 * px + 6) * (a.by + 6);
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, a.bx * a.by, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(sms * per_sm);
+  cfg.blockDim = dim3(a.bx, a.by);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, a.maps, a.views, a.pairs, pa.tiles_init, pa.n_init,
+                            pa.tiles_hp, pa.n_hp, pa.tiles_post, pa.n_post, pa.n_half, a.p,
+                            pa.sync);
+}
+
+cudaError_t launch_persistent(const PersistentArgs& pa, cudaStream_t s) {
+  if (pa.base.p.hpz != 3) return cudaErrorInvalidValue;
+  switch (pa.base.p.variant) {
+    case 1: return launch_persistent_l<1>(pa, s);
+    case 2: return launch_persistent_l<2>(pa, s);
+    case 4: return launch_persistent_l<4>(pa, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -21,6 +21,21 @@ struct LaunchArgs {
 };
 
 cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStream_t s);
+
+// A whole PatchMatch run (7 x 7 patch, non-sample) in one cooperative
+// persistent launch: init tiles, n_half half-pass stages, post tiles.
+struct PersistentArgs {
+  LaunchArgs base;
+  const int4* tiles_init;
+  int n_init;
+  const int4* tiles_hp;
+  int n_hp;
+  const int4* tiles_post;
+  int n_post;
+  int n_half;
+  unsigned* sync;  // 4 + n_half counters, zeroed before the launch
+};
+cudaError_t launch_persistent(const PersistentArgs& pa, cudaStream_t s);
 cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, __half* d_img,
                                 float4* d_quad, int TP, int TW, int TH, float cbias,
                                 cudaStream_t s);
@@ -53,12 +68,15 @@ struct CleanView {
   double K[9], R[9], t[3];
 };
 struct PruneView {
-  const float* depth;  // [H][W]
-  const float* plane;  // [H][W][3]
-  const uint8_t* color;  // [H][W][3]
-  const uint8_t* label;  // [H][W]
+  const float* depth;    // [H][W]
+  const float* plane;    // [H][W][plane_stride], plane v in the first 3 floats
+  const uint8_t* color;  // [H][W][3], or null: gray replicated to 3 channels
+  const uint8_t* label;  // [H][W], or null: label 0
   int W, H;
   double K[9], R[9], t[3];
+  const uint8_t* gray;   // [H][W] used when color is null
+  int plane_stride;      // floats per pixel in `plane` (3, or 4 for PatchMatch state)
+  int pad_;
 };
 struct PruneOut {
   float* points;

@@ -112,6 +112,7 @@ extern "C" dn_status dn_prune_noalloc(const dn_prune_view* views, int n_views,
     p.label = v.label;
     p.W = v.width;
     p.H = v.height;
+    p.plane_stride = 3;
     for (int i = 0; i < 9; ++i) {
       p.K[i] = v.K[i];
       p.R[i] = v.R[i];

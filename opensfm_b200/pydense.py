@@ -318,10 +318,30 @@ class Batch(_Handle):
             raise ValueError("init planes must be (H, W, 3)")
         check(self._L.dn_batch_set_init(self._h, int(map_id), ptr(pl, _f)))
 
-    def run(self, clean: bool = False, graph: bool = False, timing: bool = False) -> None:
-        flags = ((_lib.DN_RUN_CLEAN if clean else 0) | (_lib.DN_RUN_GRAPH if graph else 0) |
-                 (_lib.DN_RUN_TIMING if timing else 0))
+    def run(self, clean: bool = False, graph: bool = False, timing: bool = False,
+            prune: bool = False) -> None:
+        flags = ((_lib.DN_RUN_CLEAN if clean or prune else 0) | (_lib.DN_RUN_GRAPH if graph else 0) |
+                 (_lib.DN_RUN_TIMING if timing else 0) | (_lib.DN_RUN_PRUNE if prune else 0))
         check(self._L.dn_batch_run(self._h, flags))
+
+    def pruned_count(self) -> int:
+        n = ctypes.c_int64()
+        check(self._L.dn_batch_pruned_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def get_points(self, map_id: int) -> list:
+        """[points (N,3), normals (N,3), colors (N,3) u8, labels (N,) u8] of one map."""
+        n = ctypes.c_int64()
+        check(self._L.dn_batch_get_points(self._h, int(map_id), None, None, None, None, 0,
+                                          ctypes.byref(n)))
+        k = int(n.value)
+        pts = np.zeros((k, 3), np.float32)
+        nrm = np.zeros((k, 3), np.float32)
+        col = np.zeros((k, 3), np.uint8)
+        lab = np.zeros((k,), np.uint8)
+        check(self._L.dn_batch_get_points(self._h, int(map_id), ptr(pts, _f), ptr(nrm, _f),
+                                          ptr(col, _u8), ptr(lab, _u8), k, ctypes.byref(n)))
+        return [pts, nrm, col, lab]
 
     def set_view_image(self, view_id: int, image: np.ndarray) -> None:
         """Asynchronous re-upload of a view's pixels; keep ``image`` alive until synchronize."""

@@ -318,3 +318,67 @@ def test_batch_matches_single_estimator(scene):
     b.synchronize()
     for a, w in zip(b.get(m0), want):
         assert np.array_equal(a, w)
+
+
+def test_batch_clean_and_prune_match_single_objects(scene):
+    """Batched cleaner / pruner (one run for all maps) against the
+    single-object DepthmapCleaner / DepthmapPruner on the same inputs."""
+    Ks, Rs, ts = cams(scene)
+    b = pydense.Batch()
+    for K, R, t, im in zip(Ks, Rs, ts, scene.images):
+        b.add_view(K, R, t, im)
+    n = len(scene.images)
+    for v in range(n):
+        mn, mx = S.depth_range(scene.depths[v])
+        b.add_depthmap(v, [o for o in range(n) if o != v][:3], mn, mx)
+    for v in range(n):
+        b.set_clean_views(v, [o for o in range(n) if o != v])
+    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=2, same_depth_threshold=0.01,
+                 min_consistent_views=2, seed=3)
+    b.run(prune=True)
+    b.synchronize()
+    res = [b.get(v, clean=True) for v in range(n)]
+    for v in (0, 2):
+        others = [o for o in range(n) if o != v]
+        c = pydense.DepthmapCleaner()
+        c.set_same_depth_threshold(0.01)
+        c.set_min_consistent_views(2)
+        for o in [v] + others:
+            c.add_view(Ks[o], Rs[o], ts[o], res[o][0])
+        assert np.array_equal(c.clean(), res[v][4])
+        p = pydense.DepthmapPruner()
+        p.set_same_depth_threshold(0.01)
+        for o in [v] + others:
+            col = np.repeat(scene.images[o][..., None], 3, axis=2)
+            p.add_view(Ks[o], Rs[o], ts[o], res[o][4], res[o][1], col, np.zeros_like(scene.images[o]))
+        want = p.prune()
+        got = b.get_points(v)
+        assert len(got[3]) == len(want[3]) > 0
+        for a, w in zip(got, want):
+            assert np.array_equal(a, w)
+    assert b.pruned_count() >= len(want[3])
+
+
+def test_persistent_launch_matches_per_stage_launches(scene):
+    """One cooperative persistent launch gives the same maps as the
+    per-stage launches (same tiles, same random streams)."""
+    Ks, Rs, ts = cams(scene)
+    b = pydense.Batch()
+    for K, R, t, im in zip(Ks, Rs, ts, scene.images):
+        b.add_view(K, R, t, im)
+    n = len(scene.images)
+    for v in range(n):
+        mn, mx = S.depth_range(scene.depths[v])
+        b.add_depthmap(v, [o for o in range(n) if o != v][:4], mn, mx)
+    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=3, seed=5)
+    results = []
+    for variant in (4, 12, 2, 10):
+        b.set_tuning(32, 4, variant)
+        b.run(graph=(variant >= 8))
+        b.synchronize()
+        results.append([b.get(v) for v in range(n)])
+    for v in range(n):
+        for a, w in zip(results[1][v], results[0][v]):
+            assert np.array_equal(a, w)
+        for a, w in zip(results[3][v], results[2][v]):
+            assert np.array_equal(a, w)
