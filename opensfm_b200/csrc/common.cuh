@@ -368,6 +368,54 @@ __device__ inline float ncc_max(const RefPatch<HPZ>& rp, const ViewDev* views,
 }
 
 // ------------------------------------------------------------------------
+// Packed FP32 pairs: sm_100 executes add / sub / mul / fma on two FP32 values
+// held in a 64-bit register pair with one instruction (.f32x2), each half
+// rounded exactly as the scalar instruction rounds it.  The FP32 pipe does
+// the same work, but the walk below issues about a third fewer instructions,
+// which leaves issue slots for its loads and integer work.
+typedef unsigned long long u64;
+__device__ __forceinline__ u64 pk2(float a, float b) {
+  u64 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float lo2(u64 r) {
+  float a, b;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ float hi2(u64 r) {
+  float a, b;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+  return b;
+}
+__device__ __forceinline__ u64 add2(u64 a, u64 b) {
+  u64 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ u64 add2_rd(u64 a, u64 b) {
+  u64 d;
+  asm("add.rm.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ u64 sub2(u64 a, u64 b) {
+  u64 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ u64 mul2(u64 a, u64 b) {
+  u64 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
+  u64 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// ------------------------------------------------------------------------
 // Cooperative 7 x 7 patch: L lanes (2 or 4, adjacent in the warp) share one
 // pixel.  The patch is padded to 8 columns; lane l owns columns l, l + L,
 // ... (8 / L columns x 7 rows), the padding column carries weight 0 and
@@ -380,8 +428,9 @@ template <int L>
 struct CoopPatch {
   static constexpr int C = 8 / L;  // columns per lane
   static constexpr int S = 7 * C;  // slots per lane
-  float w[S];
-  float wx[S];
+  static constexpr int P = S / 2;  // slot pairs per lane (row r: columns 2m, 2m + 1)
+  u64 w2[P];                       // bilateral weights, packed in column pairs
+  u64 wx2[P];                      // w * (x - mean_x), packed likewise
   float inv_sw;
   float varx;
   int lane;
@@ -399,6 +448,7 @@ __device__ inline float group_sum(float v, unsigned mask) {
 template <int L>
 __device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile, int pitch, int ly,
                                             int lx, int lane, unsigned mask) {
+  constexpr int C = CoopPatch<L>::C;
   cp.lane = lane;
   cp.mask = mask;
   cp.src0 = (threadIdx.x & 31) - lane;
@@ -406,12 +456,12 @@ __device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile,
   const float dcf = 1.0f / 5000.0f;
   const float dxf = 1.0f / 50.0f;
   float sw = 0.f, swx = 0.f;
-  float xs[CoopPatch<L>::S];
+  float ws[CoopPatch<L>::S], xs[CoopPatch<L>::S];
 #pragma unroll
   for (int r = 0; r < 7; ++r)
 #pragma unroll
-    for (int q = 0; q < CoopPatch<L>::C; ++q) {
-      const int t = r * CoopPatch<L>::C + q;
+    for (int q = 0; q < C; ++q) {
+      const int t = r * C + q;
       const int dx = lane + L * q;
       const bool real = dx < 7;
       const int dxx = real ? dx : 6;
@@ -421,7 +471,7 @@ __device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile,
       const float arg = __fsub_rn(__fmul_rn(__fmul_rn(-d, d), dcf),
                                   __fmul_rn((float)(ddx * ddx + ddy * ddy), dxf));
       const float w = real ? expf(arg) : 0.0f;
-      cp.w[t] = w;
+      ws[t] = w;
       xs[t] = x;
       sw += w;
       swx = fmaf(w, x, swx);
@@ -431,44 +481,25 @@ __device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile,
   const float inv_sw = 1.0f / sw;
   const float mx = swx * inv_sw;
   float sxx = 0.f;
+  float wxs[CoopPatch<L>::S];
 #pragma unroll
   for (int t = 0; t < CoopPatch<L>::S; ++t) {
     const float xc = xs[t] - mx;
-    cp.wx[t] = cp.w[t] * xc;
-    sxx = fmaf(cp.wx[t], xc, sxx);
+    wxs[t] = ws[t] * xc;
+    sxx = fmaf(wxs[t], xc, sxx);
+  }
+#pragma unroll
+  for (int k = 0; k < CoopPatch<L>::P; ++k) {
+    cp.w2[k] = pk2(ws[2 * k], ws[2 * k + 1]);
+    cp.wx2[k] = pk2(wxs[2 * k], wxs[2 * k + 1]);
   }
   sxx = group_sum<L>(sxx, mask);
   cp.inv_sw = inv_sw;
   cp.varx = sxx * inv_sw;
 }
 
-// One lane's share of a view's walk, from the group's warp setup.
-template <int L, bool CLAMP>
-__device__ inline float coop_walk(const CoopPatch<L>& cp, const ViewDev& vw, const Warp& wp) {
-  constexpr int C = CoopPatch<L>::C;
-  // Lane's first column dx0 = lane - 3; the padding column (dx = 7, on lane
-  // L - 1) samples dx = 6.
-  const float dx0 = (float)(cp.lane - 3);
-  const float xl = fmaf(wp.ax, dx0, fmaf(wp.bx, -3.0f, wp.X0));
-  const float yl = fmaf(wp.ay, dx0, fmaf(wp.by, -3.0f, wp.Y0));
-  const float last = (float)((C - 1) * L - ((cp.lane == L - 1) ? 1 : 0));
-  float s1 = 0.f, s2 = 0.f, s3 = 0.f;
-#pragma unroll
-  for (int r = 0; r < 7; ++r) {
-    const float xr = fmaf(wp.bx, (float)r, xl), yr = fmaf(wp.by, (float)r, yl);
-#pragma unroll
-    for (int q = 0; q < C; ++q) {
-      const float cq = (q == C - 1) ? last : (float)(L * q);
-      const float x = q == 0 ? xr : fmaf(wp.ax, cq, xr);
-      const float yv = q == 0 ? yr : fmaf(wp.ay, cq, yr);
-      const float y = CLAMP ? table_sample_clamped(vw, x, yv) : table_sample(vw, x, yv);
-      const int t = r * C + q;
-      const float wy = cp.w[t] * y;
-      s1 += wy;
-      s2 = fmaf(wy, y, s2);
-      s3 = fmaf(cp.wx[t], y, s3);
-    }
-  }
+template <int L>
+__device__ inline float coop_finish(const CoopPatch<L>& cp, float s1, float s2, float s3) {
   s1 = group_sum<L>(s1, cp.mask);
   s2 = group_sum<L>(s2, cp.mask);
   s3 = group_sum<L>(s3, cp.mask);
@@ -476,6 +507,97 @@ __device__ inline float coop_walk(const CoopPatch<L>& cp, const ViewDev& vw, con
   const float vary = fmaf(s2, cp.inv_sw, -my * my);
   if (cp.varx < 0.1f || vary < 0.1f) return -1.0f;
   return (s3 * cp.inv_sw) * rsqrtf(cp.varx * vary);
+}
+
+// Column offset (relative to the lane's first column) of the lane's q-th
+// column; the padding column (dx = 7, on lane L - 1) samples dx = 6.
+template <int L>
+__device__ inline float coop_col(int lane, int q) {
+  constexpr int C = CoopPatch<L>::C;
+  return (q == C - 1 && lane == L - 1) ? (float)(L * q - 1) : (float)(L * q);
+}
+
+// One lane's share of a view's walk, from the group's warp setup: taps
+// clamped to the padded table (kSlow), one sample at a time.
+template <int L>
+__device__ inline float coop_walk_clamped(const CoopPatch<L>& cp, const ViewDev& vw,
+                                          const Warp& wp) {
+  constexpr int C = CoopPatch<L>::C;
+  const float dx0 = (float)(cp.lane - 3);
+  const float xl = fmaf(wp.ax, dx0, fmaf(wp.bx, -3.0f, wp.X0));
+  const float yl = fmaf(wp.ay, dx0, fmaf(wp.by, -3.0f, wp.Y0));
+  float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+  for (int r = 0; r < 7; ++r) {
+    const float xr = fmaf(wp.bx, (float)r, xl), yr = fmaf(wp.by, (float)r, yl);
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      const float cq = coop_col<L>(cp.lane, q);
+      const float x = fmaf(wp.ax, cq, xr), yv = fmaf(wp.ay, cq, yr);
+      const float y = table_sample_clamped(vw, x, yv);
+      const int t = r * C + q;
+      const u64 wpair = cp.w2[t >> 1], wxpair = cp.wx2[t >> 1];
+      const float w = (t & 1) ? hi2(wpair) : lo2(wpair);
+      const float wx = (t & 1) ? hi2(wxpair) : lo2(wxpair);
+      const float wy = w * y;
+      s1 += wy;
+      s2 = fmaf(wy, y, s2);
+      s3 = fmaf(wx, y, s3);
+    }
+  }
+  return coop_finish<L>(cp, s1, s2, s3);
+}
+
+// The same walk inside the padded table (kFast), two columns per step on
+// packed FP32 pairs: tap positions, the floor (add rounding down to the
+// magic constant), the fractions and the three weighted sums all run as
+// .f32x2; the entry index and the bilinear polynomial stay scalar.
+template <int L>
+__device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw,
+                                       const Warp& wp) {
+  constexpr int C = CoopPatch<L>::C;
+  constexpr int NP = C / 2;  // column pairs per lane
+  const float dx0 = (float)(cp.lane - 3);
+  const float xl = fmaf(wp.ax, dx0, fmaf(wp.bx, -3.0f, wp.X0));
+  const float yl = fmaf(wp.ay, dx0, fmaf(wp.by, -3.0f, wp.Y0));
+  u64 X[NP], Y[NP];
+#pragma unroll
+  for (int m = 0; m < NP; ++m) {
+    const float c0 = coop_col<L>(cp.lane, 2 * m), c1 = coop_col<L>(cp.lane, 2 * m + 1);
+    X[m] = pk2(fmaf(wp.ax, c0, xl), fmaf(wp.ax, c1, xl));
+    Y[m] = pk2(fmaf(wp.ay, c0, yl), fmaf(wp.ay, c1, yl));
+  }
+  const u64 BX = pk2(wp.bx, wp.bx), BY = pk2(wp.by, wp.by);
+  const u64 MM = pk2(vw.magic, vw.magic);
+  const unsigned TP = (unsigned)vw.TP;
+  const float4* __restrict__ q0 = vw.quad0;
+  u64 S1 = 0ull, S2 = 0ull, S3 = 0ull;  // (+0.0f, +0.0f) pairs
+#pragma unroll
+  for (int r = 0; r < 7; ++r) {
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+      const u64 TX = add2_rd(X[m], MM), TY = add2_rd(Y[m], MM);
+      const u64 FX = sub2(X[m], sub2(TX, MM)), FY = sub2(Y[m], sub2(TY, MM));
+      const unsigned oa = __float_as_uint(lo2(TY)) * TP + __float_as_uint(lo2(TX));
+      const unsigned ob = __float_as_uint(hi2(TY)) * TP + __float_as_uint(hi2(TX));
+      const float4 qa = __ldg(q0 + (int)oa);
+      const float4 qb = __ldg(q0 + (int)ob);
+      const float fxa = lo2(FX), fya = lo2(FY), fxb = hi2(FX), fyb = hi2(FY);
+      const float ya = fmaf(fya, fmaf(fxa, qa.w, qa.z), fmaf(fxa, qa.y, qa.x));
+      const float yb = fmaf(fyb, fmaf(fxb, qb.w, qb.z), fmaf(fxb, qb.y, qb.x));
+      const u64 YY = pk2(ya, yb);
+      const int k = r * NP + m;
+      const u64 WY = mul2(cp.w2[k], YY);
+      S1 = add2(S1, WY);
+      S2 = fma2(WY, YY, S2);
+      S3 = fma2(cp.wx2[k], YY, S3);
+      if (r < 6) {
+        X[m] = add2(X[m], BX);
+        Y[m] = add2(Y[m], BY);
+      }
+    }
+  }
+  return coop_finish<L>(cp, lo2(S1) + hi2(S1), lo2(S2) + hi2(S2), lo2(S3) + hi2(S3));
 }
 
 template <int L>
@@ -496,8 +618,8 @@ __device__ inline float coop_eval(const CoopPatch<L>& cp, const ViewDev& vw, con
                                   unsigned& taps) {
   if (wp.mode == kOutside || wp.mode == kDegenerate) return -1.0f;
   if (cp.lane == 0) taps += 49;
-  if (wp.mode == kSlow) return coop_walk<L, true>(cp, vw, wp);
-  return coop_walk<L, false>(cp, vw, wp);
+  if (wp.mode == kSlow) return coop_walk_clamped<L>(cp, vw, wp);
+  return coop_walk_fast<L>(cp, vw, wp);
 }
 
 // Single view (sample mode): every lane computes the same setup.
