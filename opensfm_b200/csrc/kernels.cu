@@ -65,6 +65,27 @@ __device__ inline void stage_tile(float* tile, int pitch, int rows, const __half
   }
 }
 
+// ----------------------------------------------------------------------
+// The depthmap's matching-view records (pair factors and view tables),
+// copied to shared memory at the start of a tile: every candidate's
+// homography setup and walk reads them there instead of through L1.
+// p[k].view indexes v.
+struct PairViewSm {
+  ViewDev v[kMaxNbr];
+  PairDev p[kMaxNbr];
+};
+
+__device__ inline void stage_pairs(PairViewSm& s, const MapDev& m, const ViewDev* views,
+                                   const PairDev* pairs) {
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  if (t < m.n_pairs) {
+    PairDev pr = pairs[m.pair0 + t];
+    s.v[t] = views[pr.view];
+    pr.view = t;
+    s.p[t] = pr;
+  }
+}
+
 __device__ inline void flush_taps(unsigned taps, unsigned long long* counter) {
   __shared__ unsigned long long block_taps;
   if (threadIdx.x == 0 && threadIdx.y == 0) block_taps = 0;
@@ -115,7 +136,9 @@ __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev*
   const int px = blockDim.x / L;  // pixels per warp row
   const int x0 = tl.y * px, y0 = tl.z * blockDim.y;
   const int pitch = px + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  __shared__ PairViewSm spv;
   stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
+  stage_pairs(spv, m, views, pairs);
   __syncthreads();
   const int g = threadIdx.x / L, lane = threadIdx.x % L;
   const unsigned mask = (L == 1) ? (1u << (threadIdx.x & 31))
@@ -152,11 +175,10 @@ __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev*
       const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
       if (SAMPLE) {
         nb = 1 + (int)(r.w % (uint32_t)m.n_pairs);
-        const PairDev& pr = pairs[m.pair0 + nb - 1];
-        sc = pt.view(views[pr.view], pr, h, (float)j, (float)i, taps);
+        const PairDev& pr = spv.p[nb - 1];
+        sc = pt.view(spv.v[pr.view], pr, h, (float)j, (float)i, taps);
       } else {
-        sc = patch_max<HPZ, L>(pt, views, pairs + m.pair0, m.n_pairs, h, (float)j, (float)i, nb,
-                               taps);
+        sc = patch_max<HPZ, L>(pt, spv.v, spv.p, m.n_pairs, h, (float)j, (float)i, nb, taps);
       }
       st = make_float4(v.x, v.y, v.z, depth);
     }
@@ -193,7 +215,9 @@ brute_force_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ 
   const int W = m.W, H = m.H;
   const int x0 = tl.y * blockDim.x, y0 = tl.z * blockDim.y;
   const int pitch = blockDim.x + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  __shared__ PairViewSm spv;
   stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
+  stage_pairs(spv, m, views, pairs);
   __syncthreads();
   const int i = y0 + threadIdx.y, j = x0 + threadIdx.x;
   unsigned taps = 0;
@@ -214,8 +238,7 @@ brute_force_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ 
           plane_from_depth_normal((float)j, (float)i, m.Kinv_d, depth, make_float3(0.f, 0.f, -1.f));
       const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
       int nb;
-      const float s = ncc_max<HPZ>(rp, views, pairs + m.pair0, m.n_pairs, h, (float)j, (float)i,
-                                   nb, taps);
+      const float s = ncc_max<HPZ>(rp, spv.v, spv.p, m.n_pairs, h, (float)j, (float)i, nb, taps);
       if (s > best) {
         best = s;
         bestn = nb;
@@ -245,7 +268,9 @@ score_planes_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__
   const int W = m.W, H = m.H;
   const int x0 = tl.y * blockDim.x, y0 = tl.z * blockDim.y;
   const int pitch = blockDim.x + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  __shared__ PairViewSm spv;
   stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
+  stage_pairs(spv, m, views, pairs);
   __syncthreads();
   const int i = y0 + threadIdx.y, j = x0 + threadIdx.x;
   unsigned taps = 0;
@@ -258,7 +283,7 @@ score_planes_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__
       ref_patch_from_tile<HPZ>(rp, tile, pitch, threadIdx.y + HPZ, threadIdx.x + HPZ);
       const float3 v = make_float3(m.init[3 * pix], m.init[3 * pix + 1], m.init[3 * pix + 2]);
       const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
-      sc = ncc_max<HPZ>(rp, views, pairs + m.pair0, m.n_pairs, h, (float)j, (float)i, nb, taps);
+      sc = ncc_max<HPZ>(rp, spv.v, spv.p, m.n_pairs, h, (float)j, (float)i, nb, taps);
     }
     m.score[pix] = sc;
     m.nghbr[pix] = nb;
@@ -292,7 +317,9 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
   const int px = blockDim.x / L;  // pixels per warp row
   const int x0 = tl.y * (2 * px), y0 = tl.z * blockDim.y;
   const int pitch = 2 * px + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  __shared__ PairViewSm spv;
   stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
+  stage_pairs(spv, m, views, pairs);
   __syncthreads();
   const int g = threadIdx.x / L, lane = threadIdx.x % L;
   const unsigned mask = (L == 1) ? (1u << (threadIdx.x & 31))
@@ -311,7 +338,8 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
     int curn = m.nghbr[pix];
     float3 cv = make_float3(st.x, st.y, st.z);
     float cd = st.w;
-    const PairDev* mp = pairs + m.pair0;
+    const PairDev* mp = spv.p;
+    const ViewDev* sv = spv.v;
 
     auto try_plane = [&](float3 v, int view) {
       if (same_plane(v, cv)) return;
@@ -322,9 +350,9 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
         nb = view;
         if (nb < 1 || nb > m.n_pairs) return;
         const PairDev& pr = mp[nb - 1];
-        s = pt.view(views[pr.view], pr, h, fj, fi, taps);
+        s = pt.view(sv[pr.view], pr, h, fj, fi, taps);
       } else {
-        s = patch_max<HPZ, L>(pt, views, mp, m.n_pairs, h, fj, fi, nb, taps);
+        s = patch_max<HPZ, L>(pt, sv, mp, m.n_pairs, h, fj, fi, nb, taps);
       }
       if (s > cur) {
         cur = s;
@@ -403,7 +431,7 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
       if (other >= curn) other += 1;
       const Hyp h = make_hyp(m.Kinv, cv, fj, fi);
       const PairDev& pr = mp[other - 1];
-      const float s = pt.view(views[pr.view], pr, h, fj, fi, taps);
+      const float s = pt.view(sv[pr.view], pr, h, fj, fi, taps);
       if (s > cur) {
         cur = s;
         curn = other;
