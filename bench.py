@@ -285,12 +285,12 @@ def run_ours(args):
     # one launch per stage, so a persistent choice is timed as its per-stage
     # equivalent (same tiles and lanes; results are identical).
     choice = tuning["choice"]
-    if choice[2] & 8:
-        b.set_tuning(choice[0], choice[1], choice[2] & 7)
+    if choice[2] & 16:
+        b.set_tuning(choice[0], choice[1], choice[2] & 15)
     b.run(prune=True, graph=False, timing=True)
     b.synchronize()
     stages, taps = b.timings()
-    if choice[2] & 8:
+    if choice[2] & 16:
         b.set_tuning(*choice)
         b.run(prune=True, graph=True)
         b.synchronize()
@@ -372,7 +372,7 @@ def run_ours(args):
     # Launch count per step: memsets are not kernels; init + 2*iters
     # half-passes + post (or one persistent launch for all three) + one
     # cleaner launch and three pruner launches per map.
-    pm_launches = 1 if (tuning and tuning["choice"][2] & 8) else (1 + 2 * ITERS + 1)
+    pm_launches = 1 if (tuning and tuning["choice"][2] & 16) else (1 + 2 * ITERS + 1)
     line["gpu_launches"] = args.steps * (pm_launches + 4 * n_maps)
     if rank == 0 and world == 1 and not args.no_cpu:
         try:

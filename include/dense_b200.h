@@ -214,9 +214,9 @@ dn_status dn_batch_set_view_image(dn_batch* b, int view_id, const uint8_t* image
 dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_out);
 /* Launch tuning (no reference counterpart): thread block shape bx x by
  * (bx * by <= 128, bx a multiple of 32); variant = the lanes that share one
- * pixel in the initialisation and PatchMatch kernels (1, 2 or 4; 2 and 4
- * apply to the 7 x 7 patch), plus 8 to run initialisation, every half-pass
- * and the post-process of all depthmaps in ONE cooperative persistent
+ * pixel in the initialisation and PatchMatch kernels (1, 2, 4 or 8; 2, 4
+ * and 8 apply to the 7 x 7 patch), plus 16 to run initialisation, every
+ * half-pass and the post-process of all depthmaps in ONE cooperative persistent
  * launch (32 x 4 blocks, 7 x 7 patch; tiles taken from atomic counters,
  * bounded grid barriers between stages).  Chosen by opensfm_b200.autotune;
  * scores agree between settings to float rounding of the sums. */

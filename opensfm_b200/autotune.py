@@ -16,9 +16,10 @@ from typing import Dict, List, Sequence, Tuple
 HERE = os.path.dirname(os.path.abspath(__file__))
 CACHE = os.path.join(HERE, "_build", "autotune.json")
 
-# (bx, by, variant): variant = lanes per pixel + 8 for the persistent launch.
+# (bx, by, variant): variant = lanes per pixel (1, 2, 4, 8) + 16 for the
+# persistent launch.
 CANDIDATES: List[Tuple[int, int, int]] = [
-    (32, 4, 4), (32, 4, 12), (64, 2, 4), (32, 2, 4), (32, 4, 2), (32, 4, 10), (32, 4, 1),
+    (32, 4, 4), (32, 4, 20), (32, 4, 8), (64, 2, 4), (32, 2, 4), (32, 4, 2), (32, 4, 1),
 ]
 
 

@@ -194,7 +194,7 @@ struct Engine {
   float same_depth_thr = 0.01f;
   int min_consistent = 2;
   int bx = 32, by = 4;  // thread block shape
-  int variant = 4;      // lanes per pixel in init / half-passes (1, 2, 4)
+  int variant = 4;      // lanes per pixel in init / half-passes (1, 2, 4, 8)
   int half_passes = -1;  // -1: 2 x iterations
   int persistent = 0;    // one cooperative persistent launch per PatchMatch run
   DevBuf<unsigned> d_sync;
@@ -1328,15 +1328,17 @@ dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_o
 static dn_status set_tuning(Engine& e, int bx, int by, int variant) {
   DN_CHECK(bx >= 32 && bx % 32 == 0 && by >= 1 && bx * by <= 128,
            "block shape must have bx a multiple of 32 and bx * by <= 128");
-  // variant = lanes per pixel (1, 2, 4) + 8 for the persistent launch.
-  const int lanes = variant & 7;
-  DN_CHECK(lanes == 1 || lanes == 2 || lanes == 4, "lanes per pixel must be 1, 2 or 4");
-  DN_CHECK(!(variant & 8) || (bx == 32 && by == 4),
+  // variant = lanes per pixel (1, 2, 4, 8) + 16 for the persistent launch.
+  DN_CHECK(variant >= 0 && variant < 32, "variant must be lanes (1, 2, 4, 8) + 16 (persistent)");
+  const int lanes = variant & 15;
+  DN_CHECK(lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8,
+           "lanes per pixel must be 1, 2, 4 or 8");
+  DN_CHECK(!(variant & 16) || (bx == 32 && by == 4),
            "the persistent launch uses 32 x 4 thread blocks");
   e.bx = bx;
   e.by = by;
   e.variant = lanes;
-  e.persistent = (variant & 8) ? 1 : 0;
+  e.persistent = (variant & 16) ? 1 : 0;
   e.invalidate();
   return DN_OK;
 }

@@ -416,21 +416,23 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
 }
 
 // ------------------------------------------------------------------------
-// Cooperative 7 x 7 patch: L lanes (2 or 4, adjacent in the warp) share one
-// pixel.  The patch is padded to 8 columns; lane l owns columns l, l + L,
+// Cooperative 7 x 7 patch: L lanes (2, 4 or 8, adjacent in the warp) share
+// one pixel.  The patch is padded to 8 columns; lane l owns columns l, l + L,
 // ... (8 / L columns x 7 rows), the padding column carries weight 0 and
 // samples column 6's position.  Each lane keeps 2 x 56 / L weights instead of
 // 98, so more warps fit on an SM, and lanes l and l + 1 read neighbouring
-// table entries.  The warp setup of a view is computed by one lane of the
+// table entries (with 8 lanes a group reads a whole patch row at once).  The warp setup of a view is computed by one lane of the
 // group and broadcast; the three sums are combined with XOR shuffles, so
 // every lane of a group ends with the same score.
 template <int L>
 struct CoopPatch {
   static constexpr int C = 8 / L;  // columns per lane
   static constexpr int S = 7 * C;  // slots per lane
-  static constexpr int P = S / 2;  // slot pairs per lane (row r: columns 2m, 2m + 1)
-  u64 w2[P];                       // bilateral weights, packed in column pairs
+  static constexpr int P = S / 2;  // slot pairs per lane: slots 2k, 2k + 1
+  static constexpr bool ODD = (S & 1) != 0;  // one column (L = 8): slot 6 alone
+  u64 w2[P];                       // bilateral weights, packed in slot pairs
   u64 wx2[P];                      // w * (x - mean_x), packed likewise
+  float wt, wxt;                   // the unpaired slot (ODD only)
   float inv_sw;
   float varx;
   int lane;
@@ -493,6 +495,12 @@ __device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile,
     cp.w2[k] = pk2(ws[2 * k], ws[2 * k + 1]);
     cp.wx2[k] = pk2(wxs[2 * k], wxs[2 * k + 1]);
   }
+  if (CoopPatch<L>::ODD) {
+    cp.wt = ws[CoopPatch<L>::S - 1];
+    cp.wxt = wxs[CoopPatch<L>::S - 1];
+  } else {
+    cp.wt = cp.wxt = 0.f;
+  }
   sxx = group_sum<L>(sxx, mask);
   cp.inv_sw = inv_sw;
   cp.varx = sxx * inv_sw;
@@ -536,9 +544,15 @@ __device__ inline float coop_walk_clamped(const CoopPatch<L>& cp, const ViewDev&
       const float x = fmaf(wp.ax, cq, xr), yv = fmaf(wp.ay, cq, yr);
       const float y = table_sample_clamped(vw, x, yv);
       const int t = r * C + q;
-      const u64 wpair = cp.w2[t >> 1], wxpair = cp.wx2[t >> 1];
-      const float w = (t & 1) ? hi2(wpair) : lo2(wpair);
-      const float wx = (t & 1) ? hi2(wxpair) : lo2(wxpair);
+      float w, wx;
+      if (CoopPatch<L>::ODD && t == CoopPatch<L>::S - 1) {
+        w = cp.wt;
+        wx = cp.wxt;
+      } else {
+        const u64 wpair = cp.w2[t >> 1], wxpair = cp.wx2[t >> 1];
+        w = (t & 1) ? hi2(wpair) : lo2(wpair);
+        wx = (t & 1) ? hi2(wxpair) : lo2(wxpair);
+      }
       const float wy = w * y;
       s1 += wy;
       s2 = fmaf(wy, y, s2);
@@ -548,56 +562,89 @@ __device__ inline float coop_walk_clamped(const CoopPatch<L>& cp, const ViewDev&
   return coop_finish<L>(cp, s1, s2, s3);
 }
 
-// The same walk inside the padded table (kFast), two columns per step on
+// Two table samples at the packed positions (X, Y), as table_sample does
+// one: returns the packed samples.
+__device__ __forceinline__ u64 sample_pair(u64 X, u64 Y, u64 MM, unsigned TP,
+                                           const float4* __restrict__ q0) {
+  const u64 TX = add2_rd(X, MM), TY = add2_rd(Y, MM);
+  const u64 FX = sub2(X, sub2(TX, MM)), FY = sub2(Y, sub2(TY, MM));
+  const unsigned oa = __float_as_uint(lo2(TY)) * TP + __float_as_uint(lo2(TX));
+  const unsigned ob = __float_as_uint(hi2(TY)) * TP + __float_as_uint(hi2(TX));
+  const float4 qa = __ldg(q0 + (int)oa);
+  const float4 qb = __ldg(q0 + (int)ob);
+  const float fxa = lo2(FX), fya = lo2(FY), fxb = hi2(FX), fyb = hi2(FY);
+  const float ya = fmaf(fya, fmaf(fxa, qa.w, qa.z), fmaf(fxa, qa.y, qa.x));
+  const float yb = fmaf(fyb, fmaf(fxb, qb.w, qb.z), fmaf(fxb, qb.y, qb.x));
+  return pk2(ya, yb);
+}
+
+// The same walk inside the padded table (kFast), two slots per step on
 // packed FP32 pairs: tap positions, the floor (add rounding down to the
 // magic constant), the fractions and the three weighted sums all run as
-// .f32x2; the entry index and the bilinear polynomial stay scalar.
+// .f32x2; the entry index and the bilinear polynomial stay scalar.  With
+// 2 or 4 lanes a pair is two columns of one row; with 8 lanes (one column
+// per lane) it is two rows, and row 6 is sampled alone.
 template <int L>
 __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw,
                                        const Warp& wp) {
   constexpr int C = CoopPatch<L>::C;
-  constexpr int NP = C / 2;  // column pairs per lane
   const float dx0 = (float)(cp.lane - 3);
   const float xl = fmaf(wp.ax, dx0, fmaf(wp.bx, -3.0f, wp.X0));
   const float yl = fmaf(wp.ay, dx0, fmaf(wp.by, -3.0f, wp.Y0));
-  u64 X[NP], Y[NP];
-#pragma unroll
-  for (int m = 0; m < NP; ++m) {
-    const float c0 = coop_col<L>(cp.lane, 2 * m), c1 = coop_col<L>(cp.lane, 2 * m + 1);
-    X[m] = pk2(fmaf(wp.ax, c0, xl), fmaf(wp.ax, c1, xl));
-    Y[m] = pk2(fmaf(wp.ay, c0, yl), fmaf(wp.ay, c1, yl));
-  }
-  const u64 BX = pk2(wp.bx, wp.bx), BY = pk2(wp.by, wp.by);
   const u64 MM = pk2(vw.magic, vw.magic);
   const unsigned TP = (unsigned)vw.TP;
   const float4* __restrict__ q0 = vw.quad0;
   u64 S1 = 0ull, S2 = 0ull, S3 = 0ull;  // (+0.0f, +0.0f) pairs
+  float t1 = 0.f, t2 = 0.f, t3 = 0.f;   // the unpaired slot
+  if constexpr (C == 1) {
+    const float c0 = coop_col<L>(cp.lane, 0);
+    const float xc = fmaf(wp.ax, c0, xl), yc = fmaf(wp.ay, c0, yl);
+    u64 X = pk2(xc, __fadd_rn(xc, wp.bx)), Y = pk2(yc, __fadd_rn(yc, wp.by));
+    const u64 BX = pk2(2.0f * wp.bx, 2.0f * wp.bx), BY = pk2(2.0f * wp.by, 2.0f * wp.by);
 #pragma unroll
-  for (int r = 0; r < 7; ++r) {
-#pragma unroll
-    for (int m = 0; m < NP; ++m) {
-      const u64 TX = add2_rd(X[m], MM), TY = add2_rd(Y[m], MM);
-      const u64 FX = sub2(X[m], sub2(TX, MM)), FY = sub2(Y[m], sub2(TY, MM));
-      const unsigned oa = __float_as_uint(lo2(TY)) * TP + __float_as_uint(lo2(TX));
-      const unsigned ob = __float_as_uint(hi2(TY)) * TP + __float_as_uint(hi2(TX));
-      const float4 qa = __ldg(q0 + (int)oa);
-      const float4 qb = __ldg(q0 + (int)ob);
-      const float fxa = lo2(FX), fya = lo2(FY), fxb = hi2(FX), fyb = hi2(FY);
-      const float ya = fmaf(fya, fmaf(fxa, qa.w, qa.z), fmaf(fxa, qa.y, qa.x));
-      const float yb = fmaf(fyb, fmaf(fxb, qb.w, qb.z), fmaf(fxb, qb.y, qb.x));
-      const u64 YY = pk2(ya, yb);
-      const int k = r * NP + m;
+    for (int k = 0; k < 3; ++k) {
+      const u64 YY = sample_pair(X, Y, MM, TP, q0);
       const u64 WY = mul2(cp.w2[k], YY);
       S1 = add2(S1, WY);
       S2 = fma2(WY, YY, S2);
       S3 = fma2(cp.wx2[k], YY, S3);
-      if (r < 6) {
-        X[m] = add2(X[m], BX);
-        Y[m] = add2(Y[m], BY);
+      X = add2(X, BX);
+      Y = add2(Y, BY);
+    }
+    const float y6 = table_sample(vw, fmaf(wp.bx, 6.0f, xc), fmaf(wp.by, 6.0f, yc));
+    const float wy = cp.wt * y6;
+    t1 = wy;
+    t2 = wy * y6;
+    t3 = cp.wxt * y6;
+  } else {
+    constexpr int NP = C / 2;  // column pairs per lane
+    u64 X[NP], Y[NP];
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+      const float c0 = coop_col<L>(cp.lane, 2 * m), c1 = coop_col<L>(cp.lane, 2 * m + 1);
+      X[m] = pk2(fmaf(wp.ax, c0, xl), fmaf(wp.ax, c1, xl));
+      Y[m] = pk2(fmaf(wp.ay, c0, yl), fmaf(wp.ay, c1, yl));
+    }
+    const u64 BX = pk2(wp.bx, wp.bx), BY = pk2(wp.by, wp.by);
+#pragma unroll
+    for (int r = 0; r < 7; ++r) {
+#pragma unroll
+      for (int m = 0; m < NP; ++m) {
+        const u64 YY = sample_pair(X[m], Y[m], MM, TP, q0);
+        const int k = r * NP + m;
+        const u64 WY = mul2(cp.w2[k], YY);
+        S1 = add2(S1, WY);
+        S2 = fma2(WY, YY, S2);
+        S3 = fma2(cp.wx2[k], YY, S3);
+        if (r < 6) {
+          X[m] = add2(X[m], BX);
+          Y[m] = add2(Y[m], BY);
+        }
       }
     }
   }
-  return coop_finish<L>(cp, lo2(S1) + hi2(S1), lo2(S2) + hi2(S2), lo2(S3) + hi2(S3));
+  return coop_finish<L>(cp, lo2(S1) + hi2(S1) + t1, lo2(S2) + hi2(S2) + t2,
+                        lo2(S3) + hi2(S3) + t3);
 }
 
 template <int L>
@@ -697,6 +744,8 @@ template <>
 struct Patch<3, 2> : CoopIface<2> {};
 template <>
 struct Patch<3, 4> : CoopIface<4> {};
+template <>
+struct Patch<3, 8> : CoopIface<8> {};
 
 template <int HPZ, int L>
 __device__ inline float patch_max(const Patch<HPZ, L>& pt, const ViewDev* views,

@@ -16,7 +16,7 @@ template <int HPZ>
 constexpr int kMinBlocks = HPZ <= 2 ? 4 : (HPZ == 3 ? 3 : 2);
 // With L lanes per pixel each lane keeps 2 x 56 / L weights.
 template <int HPZ, int L>
-constexpr int kMinBlocksL = L == 1 ? kMinBlocks<HPZ> : (L == 2 ? 4 : 5);
+constexpr int kMinBlocksL = L == 1 ? kMinBlocks<HPZ> : (L == 2 ? 4 : (L == 4 ? 5 : 8));
 
 // ----------------------------------------------------------------------
 // Per-view preparation.
@@ -669,7 +669,7 @@ cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStre
     postprocess_kernel<<<a.n_tiles, dim3(a.bx, a.by), 0, s>>>(a.maps, a.tiles, a.flag);
     return cudaGetLastError();
   }
-  // Lanes per pixel (a.p.variant): 1, 2 or 4 for the 7 x 7 patch (init and
+  // Lanes per pixel (a.p.variant): 1, 2, 4 or 8 for the 7 x 7 patch (init and
   // half-passes; brute force and plane scoring use 1); other patch sizes 1.
   switch (a.p.hpz) {
     case 1: return launch_hpz<1, 1>(stage, sample, a, s);
@@ -678,6 +678,7 @@ cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStre
       if (stage == Stage::kInit || stage == Stage::kHalfPass) {
         if (a.p.variant == 2) return launch_hpz<3, 2>(stage, sample, a, s);
         if (a.p.variant == 4) return launch_hpz<3, 4>(stage, sample, a, s);
+        if (a.p.variant == 8) return launch_hpz<3, 8>(stage, sample, a, s);
       }
       return launch_hpz<3, 1>(stage, sample, a, s);
     case 4: return launch_hpz<4, 1>(stage, sample, a, s);
@@ -719,6 +720,7 @@ cudaError_t launch_persistent(const PersistentArgs& pa, cudaStream_t s) {
     case 1: return launch_persistent_l<1>(pa, s);
     case 2: return launch_persistent_l<2>(pa, s);
     case 4: return launch_persistent_l<4>(pa, s);
+    case 8: return launch_persistent_l<8>(pa, s);
   }
   return cudaErrorInvalidValue;
 }
