@@ -46,6 +46,10 @@ N_VIEWS, N_CAND, N_MATCH = 24, 10, 6
 PATCH, MIN_SD, ITERS = 7, 1.0, 3
 SEED = 2024
 FLOPS_PER_TAP = 25  # affine warp 8 + bilinear 11 + NCC sums 6 (FMA = 2)
+# DRAM bytes (read + write) of one half-pass launch over the 24 maps, from an
+# ncu capture of this workload: the depthmap state read and written once plus
+# the first touch of the coefficient tables; every other gather hits L2.
+HALFPASS_DRAM_BYTES = 283_666_432 + 103_742_464
 
 
 # ---------------------------------------------------------------- workload
@@ -356,8 +360,11 @@ def run_ours(args):
                          "clean_and_prune": stages[3], "total": stages[4]},
         },
         "roofline": {
-            "kernel": "halfpass_kernel<3,false>", "bound": "fp32", "achieved": achieved,
-            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+            "kernel": "halfpass_kernel<3,false,%d>" % (choice[2] & 15), "bound": "fp32",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": HALFPASS_DRAM_BYTES if n_maps == N_VIEWS else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                              "half-pass launch over the 24 maps (4 lanes per pixel)",
             "peak_source": "measured FP32 FMA loop on this GPU (dn_fp32_peak); "
                            "MEASURED_PEAKS.json has no FP32 figure",
             "algorithmic": f"{FLOPS_PER_TAP} flops per NCC tap x {taps[1]} taps in "

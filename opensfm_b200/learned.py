@@ -299,8 +299,11 @@ def propose(net: ProposalNet, b: pydense.Batch, maps: Sequence[int], H: int, W: 
 
 
 def main(argv=None):
-    """Trains the proposal network: python -m opensfm_b200.learned --scenes 2000."""
+    """Trains the proposal network (python -m opensfm_b200.learned --scenes
+    2000), or, with --evaluate, compares learned-init and plain PatchMatch
+    on held-out scenes and prints the result as one JSON line."""
     import argparse
+    import json
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--scenes", type=int, default=2000)
@@ -309,9 +312,20 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--evaluate", action="store_true",
+                    help="evaluate the weights in --out instead of training")
+    ap.add_argument("--eval-seeds", default="900000:900012",
+                    help="held-out scene seeds, start:stop (training uses 100000 and up)")
+    ap.add_argument("--repeats", type=int, default=3)
     args = ap.parse_args(argv)
     torch = _torch()
     log = lambda s: print(s, flush=True)  # noqa: E731
+    if args.evaluate:
+        a, b = (int(x) for x in args.eval_seeds.split(":"))
+        net = ProposalNet.load(args.out)
+        res = evaluate(net, list(range(a, b)), repeats=args.repeats, log=log)
+        print(json.dumps(res), flush=True)
+        return
     seeds = list(range(100000, 100000 + args.scenes))
     feat, tgt = make_dataset(seeds, log=log)
     valid = float((tgt.view(-1, 4)[:, 3] > 0).float().mean().item())
@@ -322,10 +336,6 @@ def main(argv=None):
     net.save(args.out, history=np.array(hist), scenes=np.array(args.scenes),
              seeds_start=np.array(seeds[0]))
     log(f"saved {args.out}")
-
-
-if __name__ == "__main__":
-    main()
 
 
 # ------------------------------------------------------------ evaluation
@@ -421,3 +431,7 @@ def evaluate(net: Optional[ProposalNet], seeds: Sequence[int], W: int = 640, H: 
             r["speedup_vs_plain_3it"] = plain_ms / r["ms"]
     b.close()
     return out
+
+
+if __name__ == "__main__":
+    main()
