@@ -53,13 +53,30 @@ HALFPASS_DRAM_BYTES = 283_666_432 + 103_742_464
 
 
 # ---------------------------------------------------------------- workload
-def make_workload(seed=SEED, n_views=N_VIEWS, W=W_, H=H_):
+WORKLOADS = ("ring24", "mixed-box", "mixed-terrain")
+
+
+def make_workload(seed=SEED, n_views=N_VIEWS, W=W_, H=H_, kind="ring24"):
+    """(views, depth ranges, cleaner neighbours, matching views) per view.
+
+    ring24: the box scene, 24 views 640x480 on a ring, 10 cleaner neighbours
+    and the 6 nearest as matching views.  mixed-box / mixed-terrain: 64 views
+    whose sizes are drawn from 640x480, 480x640, 640x360 and 320x240 by the
+    seed, each with U{4..10} neighbours that serve as matching and cleaner
+    views (rendered by the CUDA ray caster)."""
     from opensfm_b200 import synthetic as S
 
-    vs = S.ring_viewset(seed, n_views, W, H)
+    if kind == "ring24":
+        vs = S.ring_viewset(seed, n_views, W, H)
+        cands = [vs.neighbors(v, N_CAND) for v in range(n_views)]
+        matches = [c[:N_MATCH] for c in cands]
+    else:
+        vs = S.mixed_viewset(seed, 64, kind.split("-")[1], gpu=True)
+        rng = np.random.default_rng(seed + 3)
+        counts = rng.integers(4, 11, size=len(vs.cameras))
+        cands = [vs.neighbors(v, int(k)) for v, k in enumerate(counts)]
+        matches = cands
     ranges = [S.depth_range(d) for d in vs.depths]
-    cands = [vs.neighbors(v, N_CAND) for v in range(n_views)]
-    matches = [c[:N_MATCH] for c in cands]
     return vs, ranges, cands, matches
 
 
@@ -262,9 +279,10 @@ def run_ours(args):
 
     group = Group(world, local)
     _lib.check(_lib.load().dn_set_device(local))
-    work = make_workload()
+    work = make_workload(kind=args.workload)
     vs, ranges, cands, matches = work
     n_maps = args.maps or len(vs.cameras)
+    shapes = [im.shape for im in vs.images]
     b = build_batch(work, n_maps=n_maps)
     tuning = None
     if args.tuning:
@@ -274,7 +292,7 @@ def run_ours(args):
     else:
         from opensfm_b200 import autotune
 
-        key = autotune.workload_key([(H_, W_)] * n_maps, [N_MATCH] * n_maps, PATCH)
+        key = autotune.workload_key(shapes[:n_maps], [len(m) for m in matches[:n_maps]], PATCH)
         t = autotune.tune(b, key, {"prune": True, "graph": True})
         tuning = {"choice": list(t["choice"]), "ms": t["ms"], "cached": t["cached"],
                   "source": "opensfm_b200.autotune"}
@@ -324,7 +342,7 @@ def run_ours(args):
 
     # End to end through the public API from host buffers.
     imgs = [np.ascontiguousarray(im) for im in vs.images]
-    out = np.zeros((H_, W_), np.float32)
+    outs = [np.zeros(sh, np.float32) for sh in shapes[:n_maps]]
     from opensfm_b200._lib import _f, ptr
     group.barrier()
     b.synchronize()
@@ -334,27 +352,44 @@ def run_ours(args):
             b.set_view_image(v, im)
         b.run(prune=True, graph=True)
         for v in range(n_maps):
-            _lib.check(b._L.dn_batch_get_depthmap(b._h, v, None, None, None, None, ptr(out, _f)))
+            _lib.check(b._L.dn_batch_get_depthmap(b._h, v, None, None, None, None,
+                                                  ptr(outs[v], _f)))
     b.timer_record(1)
     b.synchronize()
     e2e_ms = group.max(b.timer_elapsed())
     group.barrier()
     e2e = world * n_maps * args.steps / (e2e_ms * 1e-3)
 
+    ring = args.workload == "ring24"
+    if ring:
+        desc = (f"ring reconstruction, {n_maps} reference views {W_}x{H_}, "
+                f"{N_MATCH} matching views, {N_CAND} cleaner neighbours, PatchMatch "
+                f"{ITERS} iterations (red-black), patch {PATCH}, min_patch_sd {MIN_SD}, "
+                f"cleaner 0.01 / 3 views, pruner 0.01; plain random initialisation")
+    else:
+        sizes = {}
+        for h, w in shapes[:n_maps]:
+            sizes[f"{w}x{h}"] = sizes.get(f"{w}x{h}", 0) + 1
+        desc = (f"{args.workload}: {n_maps} depthmaps of mixed sizes {sizes}, "
+                f"{min(len(m) for m in matches)}-{max(len(m) for m in matches)} matching "
+                f"(and cleaner) views, PatchMatch {ITERS} iterations (red-black), patch "
+                f"{PATCH}, min_patch_sd {MIN_SD}, cleaner 0.01 / 3 views, pruner 0.01; plain "
+                f"random initialisation; {sum(h * w for h, w in shapes[:n_maps]) / 1e6:.2f} "
+                f"Mpx per step")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC if ring else "depthmaps/s (64 mixed-size views, 4-10 matching views, "
+                                      "3 iters, cleaner + pruner)",
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {
-            "workload": f"ring reconstruction, {n_maps} reference views {W_}x{H_}, "
-                        f"{N_MATCH} matching views, {N_CAND} cleaner neighbours, PatchMatch "
-                        f"{ITERS} iterations (red-black), patch {PATCH}, min_patch_sd {MIN_SD}, "
-                        f"cleaner 0.01 / 3 views, pruner 0.01; plain random initialisation",
+            "workload": desc,
             "pruned_points": pruned,
             "init": "plain", "global_batch": n_maps * world, "parallelism": f"replicas x{world}",
             "tuning": tuning,
             "l2": "working set larger than L2 (views, tables and state ~%.0f MB)" % (
-                n_maps * ((W_ + 15) * (H_ + 15) * 16 + W_ * H_ * (16 + 4 + 4 + 4 + 4 + 2)) / 1e6),
+                sum((w + 15) * (h + 15) * 16 + w * h * (16 + 4 + 4 + 4 + 4 + 2)
+                    for h, w in shapes[:n_maps]) / 1e6),
             "accuracy_1pct_median": float(np.median(accs)),
             "stage_ms": {"init": stages[0], "halfpasses": stages[1], "post": stages[2],
                          "clean_and_prune": stages[3], "total": stages[4]},
@@ -362,7 +397,7 @@ def run_ours(args):
         "roofline": {
             "kernel": "halfpass_kernel<3,false,%d>" % (choice[2] & 15), "bound": "fp32",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": HALFPASS_DRAM_BYTES if n_maps == N_VIEWS else None,
+            "traffic": HALFPASS_DRAM_BYTES if (ring and n_maps == N_VIEWS) else None,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                               "half-pass launch over the 24 maps (4 lanes per pixel)",
             "peak_source": "measured FP32 FMA loop on this GPU (dn_fp32_peak); "
@@ -372,7 +407,7 @@ def run_ours(args):
         },
         "e2e": {"value": e2e, "unit": UNIT,
                 "h2d_bytes_per_step": int(sum(im.nbytes for im in imgs[:n_maps])),
-                "d2h_bytes_per_step": int(n_maps * out.nbytes)},
+                "d2h_bytes_per_step": int(sum(o.nbytes for o in outs))},
         "gpu_launches": None,
         "clocks": {k: v for k, v in clk.summary().items()},
     }
@@ -381,7 +416,7 @@ def run_ours(args):
     # cleaner launch and three pruner launches per map.
     pm_launches = 1 if (tuning and tuning["choice"][2] & 16) else (1 + 2 * ITERS + 1)
     line["gpu_launches"] = args.steps * (pm_launches + 4 * n_maps)
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and ring:
         try:
             line["cpu_baseline"] = cpu_sample(work, seconds=args.cpu_seconds)
         except Exception as e:  # noqa: BLE001
@@ -433,7 +468,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tuning", default="", help="bx,by,variant (default: library default)")
     ap.add_argument("--maps", type=int, default=0,
-                    help="depthmaps per step (default: all 24; smaller for profiling)")
+                    help="depthmaps per step (default: all; smaller for profiling)")
+    ap.add_argument("--workload", default="ring24", choices=WORKLOADS,
+                    help="ring24 (640x480, the headline configuration) or 64 mixed-size "
+                         "views of the box or terrain scene")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -303,6 +303,21 @@ __device__ inline float table_sample_clamped(const ViewDev& vw, float x, float y
   return vw.quad[0].x;
 }
 
+// Per-patch centring value for the y sums: the table sample at the floor
+// of the patch centre (the texel value there minus cbias), or, when the
+// patch leaves the padded table, the clamped sample at the centre.  Any
+// finite shift leaves the NCC unchanged in exact arithmetic; one near the
+// patch's own mean keeps var_y free of cancellation in FP32 even where the
+// patch is far from the view's mean intensity (flat sky, bright walls).
+template <bool CLAMP>
+__device__ inline float patch_shift(const ViewDev& vw, const Warp& wp) {
+  if (CLAMP) return table_sample_clamped(vw, wp.X0, wp.Y0);
+  const float M = vw.magic;
+  const float tx = __fadd_rd(wp.X0, M), ty = __fadd_rd(wp.Y0, M);
+  const int off = (int)(__float_as_uint(ty) * (unsigned)vw.TP + __float_as_uint(tx));
+  return __ldg(&vw.quad0[off].x);
+}
+
 template <int HPZ>
 __device__ inline float ncc_finish(const RefPatch<HPZ>& rp, float s1, float s2, float s3) {
   const float my = s1 * rp.inv_sw;
@@ -317,9 +332,10 @@ __device__ inline float ncc_finish(const RefPatch<HPZ>& rp, float s1, float s2, 
 // homography, tap positions X0 + ax dx + bx dy in float as the reference
 // forms them, same bilinear sample with zeros outside [0,W-1) x [0,H-1),
 // same weights.  Sums are mean-centred: x by the patch's weighted mean
-// (hoisted), y by the view's constant cbias (folded into the table).
+// (hoisted), y by a value near the patch's own mean (patch_shift).
 template <int HPZ, bool CLAMP>
 __device__ inline float ncc_walk(const RefPatch<HPZ>& rp, const ViewDev& vw, const Warp& wp) {
+  const float sh = patch_shift<CLAMP>(vw, wp);
   float s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
   for (int dy = -HPZ; dy <= HPZ; ++dy) {
@@ -327,7 +343,8 @@ __device__ inline float ncc_walk(const RefPatch<HPZ>& rp, const ViewDev& vw, con
 #pragma unroll
     for (int dx = -HPZ; dx <= HPZ; ++dx) {
       const float x = fmaf(wp.ax, (float)dx, xr), yv = fmaf(wp.ay, (float)dx, yr);
-      const float y = CLAMP ? table_sample_clamped(vw, x, yv) : table_sample(vw, x, yv);
+      const float y =
+          (CLAMP ? table_sample_clamped(vw, x, yv) : table_sample(vw, x, yv)) - sh;
       const int t = (dy + HPZ) * (2 * HPZ + 1) + (dx + HPZ);
       const float wy = rp.w[t] * y;
       s1 += wy;
@@ -534,6 +551,7 @@ __device__ inline float coop_walk_clamped(const CoopPatch<L>& cp, const ViewDev&
   const float dx0 = (float)(cp.lane - 3);
   const float xl = fmaf(wp.ax, dx0, fmaf(wp.bx, -3.0f, wp.X0));
   const float yl = fmaf(wp.ay, dx0, fmaf(wp.by, -3.0f, wp.Y0));
+  const float sh = patch_shift<true>(vw, wp);
   float s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
   for (int r = 0; r < 7; ++r) {
@@ -542,7 +560,7 @@ __device__ inline float coop_walk_clamped(const CoopPatch<L>& cp, const ViewDev&
     for (int q = 0; q < C; ++q) {
       const float cq = coop_col<L>(cp.lane, q);
       const float x = fmaf(wp.ax, cq, xr), yv = fmaf(wp.ay, cq, yr);
-      const float y = table_sample_clamped(vw, x, yv);
+      const float y = table_sample_clamped(vw, x, yv) - sh;
       const int t = r * C + q;
       float w, wx;
       if (CoopPatch<L>::ODD && t == CoopPatch<L>::S - 1) {
@@ -594,6 +612,8 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
   const u64 MM = pk2(vw.magic, vw.magic);
   const unsigned TP = (unsigned)vw.TP;
   const float4* __restrict__ q0 = vw.quad0;
+  const float sh = patch_shift<false>(vw, wp);
+  const u64 SH = pk2(sh, sh);
   u64 S1 = 0ull, S2 = 0ull, S3 = 0ull;  // (+0.0f, +0.0f) pairs
   float t1 = 0.f, t2 = 0.f, t3 = 0.f;   // the unpaired slot
   if constexpr (C == 1) {
@@ -603,7 +623,7 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
     const u64 BX = pk2(2.0f * wp.bx, 2.0f * wp.bx), BY = pk2(2.0f * wp.by, 2.0f * wp.by);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const u64 YY = sample_pair(X, Y, MM, TP, q0);
+      const u64 YY = sub2(sample_pair(X, Y, MM, TP, q0), SH);
       const u64 WY = mul2(cp.w2[k], YY);
       S1 = add2(S1, WY);
       S2 = fma2(WY, YY, S2);
@@ -611,7 +631,7 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
       X = add2(X, BX);
       Y = add2(Y, BY);
     }
-    const float y6 = table_sample(vw, fmaf(wp.bx, 6.0f, xc), fmaf(wp.by, 6.0f, yc));
+    const float y6 = table_sample(vw, fmaf(wp.bx, 6.0f, xc), fmaf(wp.by, 6.0f, yc)) - sh;
     const float wy = cp.wt * y6;
     t1 = wy;
     t2 = wy * y6;
@@ -630,7 +650,7 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
     for (int r = 0; r < 7; ++r) {
 #pragma unroll
       for (int m = 0; m < NP; ++m) {
-        const u64 YY = sample_pair(X[m], Y[m], MM, TP, q0);
+        const u64 YY = sub2(sample_pair(X[m], Y[m], MM, TP, q0), SH);
         const int k = r * NP + m;
         const u64 WY = mul2(cp.w2[k], YY);
         S1 = add2(S1, WY);

@@ -24,7 +24,7 @@ import os
 import subprocess
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
-from typing import List, Optional, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -322,6 +322,56 @@ def ring_viewset(seed: int, n_views: int, width: int, height: int, step_deg: flo
     imgs, deps = [], []
     for c in cams:
         im, de = render(scene, c, supersample)
+        imgs.append(im)
+        deps.append(de)
+    return ViewSet(scene, cams, imgs, deps)
+
+
+MIXED_SIZES = ((640, 480), (480, 640), (640, 360), (320, 240))
+
+
+def mixed_viewset(seed: int, n_views: int = 64, kind: str = "box",
+                  sizes: Sequence[Tuple[int, int]] = MIXED_SIZES, supersample: int = 2,
+                  scale: float = 1.0, gpu: bool = False,
+                  step_deg: Optional[float] = None) -> ViewSet:
+    """Views of mixed sizes, each drawn uniformly from ``sizes`` (width,
+    height) by the seed, every camera with its own intrinsics.
+
+    kind "box": the box scene seen from a ring of ``n_views`` cameras
+    (radius 15 m, height 6 m), ``step_deg`` apart (default: a full circle).  kind "terrain": a heightfield of amplitude
+    8 m with the feature scale of a 100 x 100 m terrain (the field extends
+    beyond it), seen by nadir cameras at 60 m altitude on a grid with 70 %
+    forward and 60 % side overlap (spacing from the 640 x 480 footprint).
+    ``scale`` shrinks every size (for quick tests); ``gpu`` renders with the
+    CUDA ray caster instead of the CPU one."""
+    rng = np.random.default_rng(seed + 7)
+    pick = rng.integers(len(sizes), size=n_views)
+    dims = [(max(16, int(round(sizes[k][0] * scale))), max(16, int(round(sizes[k][1] * scale))))
+            for k in pick]
+    if kind == "box":
+        scene = box_scene(seed)
+        base = ring_cameras(n_views, 640, 480, step_deg=step_deg or 360.0 / n_views,
+                            start_deg=float(np.random.default_rng(seed + 1).uniform(0, 360)))
+    elif kind == "terrain":
+        scene = terrain_scene(seed, size=100.0, amp=8.0)
+        side = int(np.ceil(np.sqrt(n_views)))
+        K0 = intrinsics(640, 480)
+        fw, fh = 60.0 * 640 / K0[0, 0], 60.0 * 480 / K0[0, 0]
+        span = max((side - 1) * fw * 0.4 + fw, (side - 1) * fh * 0.3 + fh) + 1.0
+        base = nadir_cameras(span, 60.0, 640, 480, forward_overlap=0.7, side_overlap=0.6,
+                             max_views=n_views)
+    else:
+        raise ValueError(f"unknown kind {kind!r}")
+    if len(base) < n_views:
+        raise ValueError(f"only {len(base)} cameras fit the {kind} layout")
+    cams = [Camera(intrinsics(w, h), c.R, c.t, w, h) for c, (w, h) in zip(base, dims)]
+    imgs, deps = [], []
+    for c in cams:
+        if gpu:
+            im, de = render_gpu(scene, [c], supersample)
+            im, de = im[0].cpu().numpy(), de[0].cpu().numpy()
+        else:
+            im, de = render(scene, c, supersample)
         imgs.append(im)
         deps.append(de)
     return ViewSet(scene, cams, imgs, deps)

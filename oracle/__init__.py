@@ -382,15 +382,16 @@ def ncc_fp64(Ks, Rs, ts, images, planes, patch_size=7, pixels=None, margins=Fals
         x0, y0 = u / w, vv / w
         sx = sy = sxx = syy = sxy = sw = 0.0
         img = imgs[o]
+        Ho, Wo = img.shape  # each view is sampled with its own size (depthmap.cc:16)
         for dy in range(-hpz, hpz + 1):
             for dx in range(-hpz, hpz + 1):
                 x1 = ref[pi.astype(int) + dy, pj.astype(int) + dx]
                 x2 = x0 + dxx * dx + dyx * dy
                 y2 = y0 + dxy * dx + dyy * dy
-                inside = (x2 >= 0) & (x2 < W - 1) & (y2 >= 0) & (y2 < H - 1)
+                inside = (x2 >= 0) & (x2 < Wo - 1) & (y2 >= 0) & (y2 < Ho - 1)
                 if margins:
-                    e = np.minimum(np.minimum(np.abs(x2), np.abs(x2 - (W - 1))),
-                                   np.minimum(np.abs(y2), np.abs(y2 - (H - 1))))
+                    e = np.minimum(np.minimum(np.abs(x2), np.abs(x2 - (Wo - 1))),
+                                   np.minimum(np.abs(y2), np.abs(y2 - (Ho - 1))))
                     edge_m = np.minimum(edge_m, np.where(ok, e, np.inf))
                 xs = np.where(inside, x2, 0.0)
                 ys = np.where(inside, y2, 0.0)

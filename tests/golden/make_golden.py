@@ -56,6 +56,39 @@ def estimator_case(seed, W, H, n_views, patch, planes, sd):
     )
 
 
+def estimator_mixed_case(seed, sizes, patch, planes, sd):
+    """Views of different sizes (the reference samples every view with its
+    own rows and cols, depthmap.cc:16): view k is stored as image_k etc."""
+    vs = S.mixed_viewset(seed, len(sizes), "box", sizes=sizes, step_deg=10.0)
+    # mixed_viewset draws the sizes from the seed; pin them to the given order.
+    cams_ = [S.Camera(S.intrinsics(w, h), c.R, c.t, w, h) for c, (w, h) in zip(vs.cameras, sizes)]
+    imgs, deps = [], []
+    for c in cams_:
+        im, de = S.render(vs.scene, c, 2)
+        imgs.append(im)
+        deps.append(de)
+    Ks, Rs, ts = [c.K for c in cams_], [c.R for c in cams_], [c.t for c in cams_]
+    mn, mx = S.depth_range(deps[0])
+    e = O.RefEstimator()
+    for K, R, t, im in zip(Ks, Rs, ts, imgs):
+        e.add_view(K, R, t, im, np.ones_like(im))
+    e.set_depth_range(mn, mx, planes)
+    e.set_patch_size(patch)
+    e.set_min_patch_sd(sd)
+    bf = e.compute_brute_force()
+    rng = np.random.default_rng(seed + 100)
+    rand_planes = (bf[1] * (1 + 0.05 * rng.standard_normal(bf[1].shape))).astype(np.float32)
+    sp_score, sp_nghbr = e.score_planes(rand_planes)
+    out = dict(n_views=len(sizes), min_depth=mn, max_depth=mx, num_planes=planes,
+               patch_size=patch, min_patch_sd=sd, bf_depth=bf[0], bf_plane=bf[1],
+               bf_score=bf[2], bf_nghbr=bf[3], planes=rand_planes, sp_score=sp_score,
+               sp_nghbr=sp_nghbr)
+    for k in range(len(sizes)):
+        out.update({f"K_{k}": Ks[k], f"R_{k}": Rs[k], f"t_{k}": ts[k], f"image_{k}": imgs[k],
+                    f"gt_{k}": deps[k]})
+    return out
+
+
 def clean_prune_case(seed, W, H, n_views):
     vs = S.ring_viewset(seed, n_views, W, H)
     Ks, Rs, ts = cams(vs)
@@ -86,15 +119,24 @@ def clean_prune_case(seed, W, H, n_views):
     )
 
 
+CASES = {
+    "estimator_80x60_v3_p7.npz": lambda: estimator_case(11, 80, 60, 3, 7, 24, 1.0),
+    "estimator_72x54_v4_p5.npz": lambda: estimator_case(12, 72, 54, 4, 5, 16, 2.0),
+    "clean_prune_64x48_v4.npz": lambda: clean_prune_case(13, 64, 48, 4),
+    "estimator_mixed_v4_p7.npz": lambda: estimator_mixed_case(
+        14, [(96, 72), (72, 96), (96, 54), (64, 48)], 7, 24, 1.0),
+}
+
+
 def main():
+    """Writes the fixtures that are missing (all of them with --force)."""
     if not O.ref_available():
         O.build()
-    np.savez_compressed(os.path.join(OUT, "estimator_80x60_v3_p7.npz"),
-                        **estimator_case(11, 80, 60, 3, 7, 24, 1.0))
-    np.savez_compressed(os.path.join(OUT, "estimator_72x54_v4_p5.npz"),
-                        **estimator_case(12, 72, 54, 4, 5, 16, 2.0))
-    np.savez_compressed(os.path.join(OUT, "clean_prune_64x48_v4.npz"),
-                        **clean_prune_case(13, 64, 48, 4))
+    force = "--force" in sys.argv
+    for name, make in CASES.items():
+        path = os.path.join(OUT, name)
+        if force or not os.path.exists(path):
+            np.savez_compressed(path, **make())
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))

@@ -11,10 +11,13 @@ Tolerances (stated here, asserted below):
     oracle and the GPU must be no less accurate on the median pixel.
   * Brute force: the same plane on >= 98 % of pixels; where it differs the
     two winning planes' scores are within 2e-3 (a near tie).  Scores within
-    2e-3 on every pixel whose margins to the reference's discontinuities are
-    at least 1e-3 (a tap 1e-3 px from x = W-1 / y = H-1 / 0, where the
-    reference's bilinear sample jumps to 0, or var within 1e-3 of the 0.1
-    cut-off); such pixels are counted and must stay below 0.5 %.
+    2e-3 on 99.9 % of the pixels whose margins to the reference's
+    discontinuities are at least 1e-3 (a tap 1e-3 px from x = W-1 / y = H-1
+    / 0, where the reference's bilinear sample jumps to 0, or var within
+    1e-3 of the 0.1 cut-off; such pixels are counted and must stay below
+    0.5 %), where a pixel whose scores differ by more counts as agreeing
+    only if the GPU is the closer of the two to the FP64 oracle, and on
+    every pixel with the same plane the GPU must be the closer one.
   * PatchMatch (different random schedule): accuracy against ray-cast ground
     truth (|d - gt| / gt <= 1 %) no lower than the reference's minus 0.02,
     and >= 70 % agreement with the reference's depth where both are valid.
@@ -161,7 +164,11 @@ def _check_brute_force(Ks, Rs, ts, images, patch, depth, plane, score, r_depth, 
           "%.4f, |d|>2e-3 on %d safe px (gpu err max %.2e, ref err min %.2e)"
           % (same.mean(), np.percentile(d, 99.9), d.max(), 1 - safe.mean(), big.sum(),
              e_gpu[big].max() if big.any() else 0, e_ref[big].min() if big.any() else 0))
-    assert np.mean(d[safe] <= 2e-3) >= 0.999
+    # A pixel passes when the scores agree within 2e-3 or the GPU is the
+    # closer of the two to FP64 (the reference's raw moments lose digits on
+    # patches far from zero mean, e.g. flat bright sky).
+    within = (d <= 2e-3) | (e_gpu < e_ref)
+    assert np.mean(within[safe]) >= 0.999
     assert np.all(e_gpu[big] <= e_ref[big])
     assert (1 - safe.mean()) < 0.005
     # Where both chose the same plane the plane is bit-identical.
@@ -181,6 +188,65 @@ def test_brute_force_golden(golden, name):
     # Border pixels (outside the patch interior) stay zero.
     hpz = (patch - 1) // 2
     assert (depth[:hpz] == 0).all() and (depth[:, -hpz:] == 0).all()
+
+
+def _mixed(g):
+    n = int(g["n_views"])
+    return ([g[f"K_{k}"] for k in range(n)], [g[f"R_{k}"] for k in range(n)],
+            [g[f"t_{k}"] for k in range(n)], [g[f"image_{k}"] for k in range(n)],
+            [g[f"gt_{k}"] for k in range(n)])
+
+
+def test_mixed_sizes_golden(golden):
+    """Matching views of sizes different from the reference view's (each
+    sampled with its own size, depthmap.cc:16): brute force and plane
+    scores against the reference's own outputs."""
+    g = golden("estimator_mixed_v4_p7.npz")
+    Ks, Rs, ts, ims, _ = _mixed(g)
+    masks = [np.ones_like(im) for im in ims]
+    patch = int(g["patch_size"])
+    e = _estimator(Ks, Rs, ts, ims, masks, float(g["min_depth"]), float(g["max_depth"]),
+                   planes=int(g["num_planes"]), patch=patch, sd=float(g["min_patch_sd"]))
+    depth, plane, score, nghbr = e.compute_brute_force()
+    _check_brute_force(Ks, Rs, ts, ims, patch, depth, plane, score, g["bf_depth"], g["bf_plane"],
+                       g["bf_score"])
+    s, n = e.score_planes(g["planes"])
+    d = np.abs(s - g["sp_score"])
+    assert np.mean(d <= 2e-3) >= 0.995
+    assert np.mean((n == g["sp_nghbr"]) | (d <= 2e-3)) >= 0.995
+
+
+def test_mixed_size_batch_persistent_graph(golden):
+    """A batch of depthmaps of different sizes (each view a depthmap against
+    the others): one persistent launch in a CUDA graph reproduces the
+    per-stage launches, and the cleaner and pruner run on the mixed maps."""
+    g = golden("estimator_mixed_v4_p7.npz")
+    Ks, Rs, ts, ims, gts = _mixed(g)
+    n = len(ims)
+    b = pydense.Batch()
+    for K, R, t, im in zip(Ks, Rs, ts, ims):
+        b.add_view(K, R, t, im)
+    for v in range(n):
+        mn, mx = S.depth_range(gts[v])
+        b.add_depthmap(v, [o for o in range(n) if o != v], mn, mx)
+    for v in range(n):
+        b.set_clean_views(v, [o for o in range(n) if o != v])
+    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=3, same_depth_threshold=0.01,
+                 min_consistent_views=2, seed=4)
+    results = []
+    for variant, graph in ((4, False), (20, True)):
+        b.set_tuning(32, 4, variant)
+        b.run(graph=graph, prune=True)
+        b.synchronize()
+        results.append(([b.get(v, clean=True) for v in range(n)], b.pruned_count()))
+    for v in range(n):
+        assert results[0][0][v][0].shape == ims[v].shape
+        for a, w in zip(results[1][0][v], results[0][0][v]):
+            assert np.array_equal(a, w)
+    assert results[0][1] == results[1][1] > 0
+    acc = [S.accuracy(results[0][0][v][0], gts[v]) for v in range(n)]
+    print("mixed-size batch accuracy", np.round(acc, 3))
+    assert np.mean(acc) > 0.3
 
 
 def test_brute_force_fresh_scene(scene):

@@ -68,6 +68,30 @@ def test_fp64_ncc_close_to_reference(golden):
     assert np.mean(err < 1e-3) > 0.98
 
 
+def _mixed(g):
+    n = int(g["n_views"])
+    return ([g[f"K_{k}"] for k in range(n)], [g[f"R_{k}"] for k in range(n)],
+            [g[f"t_{k}"] for k in range(n)], [g[f"image_{k}"] for k in range(n)])
+
+
+def test_fp64_ncc_mixed_sizes_close_to_reference(golden):
+    """Views of different sizes: the float64 restatement samples each view
+    with its own size, as the reference does (depthmap.cc:16)."""
+    g = golden("estimator_mixed_v4_p7.npz")
+    Ks, Rs, ts, ims = _mixed(g)
+    assert len({im.shape for im in ims}) == len(ims)
+    s64, n64 = O.ncc_fp64(Ks, Rs, ts, ims, g["bf_plane"], int(g["patch_size"]))
+    m = g["bf_depth"] > 0
+    err = np.abs(s64[m] - g["bf_score"][m])
+    assert np.median(err) < 1e-4
+    assert np.mean(err < 1e-3) > 0.98
+    s64, n64 = O.ncc_fp64(Ks, Rs, ts, ims, g["planes"], int(g["patch_size"]))
+    inner = np.zeros(m.shape, bool)
+    inner[3:-3, 3:-3] = True
+    err = np.abs(s64 - g["sp_score"])[inner]
+    assert np.mean(err < 2e-3) > 0.98
+
+
 @pytest.mark.skipif(not O.ref_available(), reason="compiled reference not built")
 def test_port_matches_compiled_reference_fresh_scene():
     vs = S.ring_viewset(21, 4, 72, 56)
