@@ -261,10 +261,21 @@ dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float
  * [H][W][4]); the next dn_batch_run with DN_RUN_INIT starts from them. */
 dn_status dn_batch_init_from_output(dn_batch* b, int map_id, const float* out);
 /* y = act(conv3x3(x, w) + bias) over n_pix pixels of images H x W; relu 0/1;
- * y (BF16) and/or y32 (FP32) may be NULL.  cin 32; cout 32 or 4. */
+ * y (BF16) and/or y32 (FP32) may be NULL.  cin 32; cout 32 or 4.  Runs on
+ * the tcgen05 tensor cores (implicit GEMM, M = 128 pixels per tile, FP32
+ * accumulators in tensor memory); asynchronous on `stream`, errors of its
+ * bounded waits are reported by dn_nn_synchronize. */
 dn_status dn_nn_conv3x3_forward(const void* x, const void* w, const float* bias, int64_t n_pix,
                                 int H, int W, int cin, int cout, int relu, void* y, float* y32,
                                 void* stream);
+/* The same forward with warp-level mma.sync (m16n8k16) tensor-core
+ * instructions, kept for comparison. */
+dn_status dn_nn_conv3x3_forward_mma_sync(const void* x, const void* w, const float* bias,
+                                         int64_t n_pix, int H, int W, int cin, int cout, int relu,
+                                         void* y, float* y32, void* stream);
+/* Waits for `stream`; DN_TIMEOUT if a tensor-core wait expired since the
+ * last call (the outputs of that launch are then invalid). */
+dn_status dn_nn_synchronize(void* stream);
 /* Backward of one layer given dy, the gradient of its pre-activation output
  * (BF16 [n_pix][cout]): accumulates dw [cout][9 cin] and db [cout] (FP32,
  * atomic adds) and writes dx (BF16 [n_pix][cin]) multiplied by (x_mask > 0)

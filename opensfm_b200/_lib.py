@@ -96,6 +96,9 @@ _SIGNATURES = {
     "dn_batch_targets": ([_vp, _vp, ctypes.c_int64, ctypes.c_float], _i),
     "dn_batch_init_from_output": ([_vp, _i, _vp], _i),
     "dn_nn_conv3x3_forward": ([_vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _i, _vp, _vp, _vp], _i),
+    "dn_nn_conv3x3_forward_mma_sync": ([_vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _i, _vp,
+                                        _vp, _vp], _i),
+    "dn_nn_synchronize": ([_vp], _i),
     "dn_nn_conv3x3_backward": ([_vp, _vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _vp, _vp, _vp,
                                 _vp, _vp], _i),
     "dn_nn_l1_loss": ([_vp, _vp, ctypes.c_int64, ctypes.c_float, _vp, _vp, _vp, _vp], _i),

@@ -1430,9 +1430,9 @@ dn_status dn_batch_init_from_output(dn_batch* b, int map_id, const float* out) {
 
 static bool nn_shape_ok(int cin, int cout) { return cin == 32 && (cout == 32 || cout == 4); }
 
-dn_status dn_nn_conv3x3_forward(const void* x, const void* w, const float* bias, int64_t n_pix,
-                                int H, int W, int cin, int cout, int relu, void* y, float* y32,
-                                void* stream) {
+static dn_status nn_forward(cudaError_t (*fn)(const dn::ConvArgs&, cudaStream_t), const void* x,
+                            const void* w, const float* bias, int64_t n_pix, int H, int W, int cin,
+                            int cout, int relu, void* y, float* y32, void* stream) {
   DN_CHECK(x && w && bias && (y || y32), "NULL argument");
   DN_CHECK(nn_shape_ok(cin, cout), "supported shapes: cin 32, cout 32 or 4");
   DN_CHECK(H > 0 && W > 0 && n_pix > 0 && n_pix % ((int64_t)H * W) == 0, "bad n_pix / H / W");
@@ -1448,7 +1448,28 @@ dn_status dn_nn_conv3x3_forward(const void* x, const void* w, const float* bias,
   c.relu = relu;
   c.y = static_cast<__nv_bfloat16*>(y);
   c.y32 = y32;
-  DN_CUDA(dn::conv3x3_forward(c, static_cast<cudaStream_t>(stream)));
+  DN_CUDA(fn(c, static_cast<cudaStream_t>(stream)));
+  return DN_OK;
+}
+dn_status dn_nn_conv3x3_forward(const void* x, const void* w, const float* bias, int64_t n_pix,
+                                int H, int W, int cin, int cout, int relu, void* y, float* y32,
+                                void* stream) {
+  return nn_forward(dn::conv3x3_forward, x, w, bias, n_pix, H, W, cin, cout, relu, y, y32, stream);
+}
+dn_status dn_nn_conv3x3_forward_mma_sync(const void* x, const void* w, const float* bias,
+                                         int64_t n_pix, int H, int W, int cin, int cout, int relu,
+                                         void* y, float* y32, void* stream) {
+  return nn_forward(dn::conv3x3_forward_mma_sync, x, w, bias, n_pix, H, W, cin, cout, relu, y, y32,
+                    stream);
+}
+dn_status dn_nn_synchronize(void* stream) {
+  DN_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  const int e = dn::take_tc_error();
+  DN_CHECK(e >= 0, "could not read the tensor-core error word");
+  if (e) {
+    g_last_error = "a tensor-core convolution's bounded wait expired";
+    return DN_TIMEOUT;
+  }
   return DN_OK;
 }
 dn_status dn_nn_conv3x3_backward(const void* dy, const void* x, const void* w,

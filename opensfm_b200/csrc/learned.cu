@@ -13,6 +13,8 @@
 //    (inverse depth, normal slopes) into PatchMatch initial planes.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "learned.h"
@@ -170,6 +172,229 @@ conv3x3_fwd_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __r
       }
     }
   }
+}
+
+// ------------------------------------------------ conv forward, tcgen05
+// The same convolution on the 5th-generation tensor cores: one CTA of 4
+// warps per tile of 128 pixels (the GEMM's M), N = the output channels
+// (32, or 16 holding the 4 outputs of the last layer), K = 9 taps x 32
+// input channels = 288 in 18 MMAs of K = 16.  The implicit-GEMM A tile
+// (128 x 288 BF16, 72 KB) is gathered by the 128 threads (one pixel row
+// each, 64 contiguous bytes per tap) into shared memory in the canonical
+// no-swizzle K-major layout: 16-byte rows of 8 K values, 8-row core
+// matrices 128 bytes apart (SBO), the two 8-value halves of one MMA's K
+// 2 KB apart (LBO).  The weights (B, [cout][288]) are staged once per CTA
+// in the same layout.  Thread 0 issues the MMAs into a 128 x N FP32
+// accumulator in tensor memory and commits them to an mbarrier; every warp
+// then reads its 32 accumulator lanes (= its 32 pixels) with tcgen05.ld,
+// adds the bias, applies the ReLU and stores BF16 (or FP32) rows.  CTAs
+// loop over tiles; each wait is bounded and sets an error word on expiry.
+namespace tc {
+
+__device__ int g_error;
+
+constexpr int kBM = 128;               // pixels per tile (MMA M)
+constexpr int kK = 9 * 32;             // GEMM K
+constexpr int kKC = kK / 8;            // 16-byte K chunks
+constexpr long long kSpins = 1LL << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, K-major without swizzle: start address,
+// leading-dimension byte offset (between the K halves), stride-dimension
+// byte offset (between 8-row groups), all in 16-byte units; bit 46 is the
+// sm_100 descriptor version.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1),
+// A and B BF16 (bits 7-9, 10-12 = 1), both K-major, N / 8 at bit 17,
+// M / 16 at bit 24.
+constexpr uint32_t idesc_bf16(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(kBM >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase) {
+  for (long long i = 0; i < kSpins; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <int NP>
+__device__ __forceinline__ void tmem_load(uint32_t taddr, uint32_t (&r)[NP]);
+
+template <>
+__device__ __forceinline__ void tmem_load<32>(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+      "%28, %29, %30, %31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+template <>
+__device__ __forceinline__ void tmem_load<16>(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+constexpr size_t smem_bytes(int np) {
+  return (size_t)kKC * kBM * 16 + (size_t)kKC * np * 16 + 16;
+}
+
+}  // namespace tc
+
+template <int NP>
+__global__ void __launch_bounds__(128, 1)
+conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ w,
+                      const float* __restrict__ bias, long long n_pix, int H, int W, int cout,
+                      int relu, __nv_bfloat16* __restrict__ y, float* __restrict__ y32,
+                      long long n_tiles) {
+  using namespace tc;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* As = smem;                         // [kKC][kBM][16 B]
+  unsigned char* Bs = smem + (size_t)kKC * kBM * 16;  // [kKC][NP][16 B]
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(Bs + (size_t)kKC * NP * 16);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  for (int e = tid; e < kKC * NP; e += blockDim.x) {
+    const int kc = e / NP, n = e - kc * NP;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (n < cout) v = *reinterpret_cast<const uint4*>(w + (size_t)n * kK + kc * 8);
+    *reinterpret_cast<uint4*>(Bs + (size_t)e * 16) = v;
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;\n" ::"r"(
+                     smem_u32(tslot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs), mb = smem_u32(mbar);
+  constexpr uint32_t idesc = idesc_bf16(NP);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const long long p = t * kBM + tid;
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      const long long q = p < n_pix ? nbr_pixel(p, H, W, tap / 3 - 1, tap % 3 - 1) : -1;
+      const uint4* src = reinterpret_cast<const uint4*>(x + (q < 0 ? 0 : q) * 32);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const uint4 v = q >= 0 ? __ldg(src + j) : make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(As + ((size_t)(tap * 4 + j) * kBM + tid) * 16) = v;
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+      for (int ks = 0; ks < kK / 16; ++ks) {
+        const uint64_t ad = smem_desc(a_base + (uint32_t)(2 * ks * kBM * 16), kBM * 16, 128);
+        const uint64_t bd = smem_desc(b_base + (uint32_t)(2 * ks * NP * 16), NP * 16, 128);
+        const uint32_t acc = ks > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+              mb)
+          : "memory");
+    }
+    bool done = mbar_wait(mb, phase);
+    phase ^= 1u;
+    if (!done) done = mbar_wait(mb, phase ^ 1u);  // a late completion of this tile
+    ok = __syncthreads_and(done) != 0;
+    if (!ok) break;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    uint32_t r[NP];
+    tmem_load<NP>(tmem + ((uint32_t)(warp * 32) << 16), r);
+    if (p < n_pix) {
+      if (NP == 32) {
+        uint32_t o[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          float v0 = __uint_as_float(r[2 * c]) + bias[2 * c];
+          float v1 = __uint_as_float(r[2 * c + 1]) + bias[2 * c + 1];
+          if (relu) {
+            v0 = fmaxf(v0, 0.f);
+            v1 = fmaxf(v1, 0.f);
+          }
+          o[c] = pack2(__float2bfloat16_rn(v0), __float2bfloat16_rn(v1));
+        }
+        if (y) {
+          uint4* dst = reinterpret_cast<uint4*>(y + p * 32);
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            dst[j] = make_uint4(o[4 * j], o[4 * j + 1], o[4 * j + 2], o[4 * j + 3]);
+        }
+        if (y32)
+#pragma unroll
+          for (int c = 0; c < 32; ++c) {
+            const float v = __uint_as_float(r[c]) + bias[c];
+            y32[p * 32 + c] = relu ? fmaxf(v, 0.f) : v;
+          }
+      } else {
+        for (int c = 0; c < cout; ++c) {
+          float v = __uint_as_float(r[c]) + bias[c];
+          if (relu) v = fmaxf(v, 0.f);
+          if (y) y[p * cout + c] = __float2bfloat16_rn(v);
+          if (y32) y32[p * cout + c] = v;
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+  }
+  if (!ok && tid == 0) atomicExch(&g_error, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;\n" ::"r"(tmem) : "memory");
 }
 
 // ------------------------------------------------------- conv backward-data
@@ -445,10 +670,43 @@ static cudaError_t conv_bwd_t(const ConvArgs& c, __nv_bfloat16* wt_scratch, cuda
   return cudaGetLastError();
 }
 
+template <int NP>
+static cudaError_t conv_fwd_tc(const ConvArgs& c, cudaStream_t s) {
+  auto kern = conv3x3_fwd_tc_kernel<NP>;
+  const size_t smem = tc::smem_bytes(NP);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long tiles = (c.n_pix + tc::kBM - 1) / tc::kBM;
+  const long long grid = std::min<long long>(tiles, 2LL * sms);
+  kern<<<(unsigned)grid, 128, smem, s>>>(c.x, c.w, c.bias, c.n_pix, c.H, c.W, c.cout, c.relu,
+                                         c.y, c.y32, tiles);
+  return cudaGetLastError();
+}
+
 cudaError_t conv3x3_forward(const ConvArgs& c, cudaStream_t s) {
+  if (c.cin == 32 && c.cout == 32) return conv_fwd_tc<32>(c, s);
+  if (c.cin == 32 && c.cout == 4) return conv_fwd_tc<16>(c, s);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t conv3x3_forward_mma_sync(const ConvArgs& c, cudaStream_t s) {
   if (c.cin == 32 && c.cout == 32) return conv_fwd_t<32, 32>(c, s);
   if (c.cin == 32 && c.cout == 4) return conv_fwd_t<32, 4>(c, s);
   return cudaErrorInvalidValue;
+}
+
+int take_tc_error() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, tc::g_error, sizeof(int)) != cudaSuccess) return -1;
+  if (v) {
+    const int zero = 0;
+    cudaMemcpyToSymbol(tc::g_error, &zero, sizeof(int));
+  }
+  return v;
 }
 cudaError_t conv3x3_backward(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaStream_t s) {
   if (c.cin == 32 && c.cout == 32) return conv_bwd_t<32, 32>(c, wt_scratch, s);

@@ -25,7 +25,13 @@ struct ConvArgs {
   float* db;                    // [cout] accumulated
 };
 
+// Forward on the tcgen05 tensor cores (TMEM accumulators); the mma.sync
+// variant is kept as the comparison the tests and the bench time it against.
 cudaError_t conv3x3_forward(const ConvArgs& c, cudaStream_t s);
+cudaError_t conv3x3_forward_mma_sync(const ConvArgs& c, cudaStream_t s);
+// 1 if a bounded wait of the tcgen05 forward expired since the last call
+// (and clears it), 0 if not, -1 if the flag could not be read.
+int take_tc_error();
 cudaError_t conv3x3_backward(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaStream_t s);
 cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
                          int n_planes, cudaStream_t s);

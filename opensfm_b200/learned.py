@@ -291,7 +291,7 @@ def propose(net: ProposalNet, b: pydense.Batch, maps: Sequence[int], H: int, W: 
     n = len(maps)
     feat = features(b, n, H, W)
     out = net.forward(feat, n * H * W, H, W)
-    torch.cuda.synchronize()
+    _lib.check(_lib.load().dn_nn_synchronize(_stream()))
     for k, m in enumerate(maps):
         _lib.check(b._L.dn_batch_init_from_output(b._h, int(m), _ptr(out[k * H * W:])))
     b.synchronize()

@@ -53,10 +53,36 @@ def test_conv_forward_matches_float64(cout, relu):
     _lib.check(L.dn_nn_conv3x3_forward(learned._ptr(xd), learned._ptr(wd), learned._ptr(bd), n_pix,
                                        H, W, cin, cout, relu, learned._ptr(y16), learned._ptr(y32),
                                        None))
-    torch.cuda.synchronize()
+    _lib.check(L.dn_nn_synchronize(None))
     ref = _ref_conv(x.double(), w.double(), b.double(), relu).reshape(n_pix, cout)
     assert _rel(y32.cpu().double(), ref) < 1e-4  # FP32 accumulation of BF16 products
     assert _rel(y16.view(n_pix, cout).cpu().double(), ref) < 1e-2
+
+
+@pytest.mark.parametrize("cout,relu", [(32, 1), (32, 0), (4, 0)])
+def test_conv_forward_tcgen05_matches_mma_sync(cout, relu):
+    """The tcgen05 forward (tensor-memory accumulators, 128-pixel tiles, CTAs
+    looping over tiles) against the warp-level mma.sync forward on a batch
+    large enough that every CTA takes several tiles, with a ragged last tile."""
+    g = torch.Generator().manual_seed(7 + cout)
+    n, H, W, cin = 2, 121, 203, 32
+    n_pix = n * H * W
+    x = _bf(torch.randn((n_pix, cin), generator=g)).cuda().contiguous()
+    w = _bf(torch.randn((cout, 9 * cin), generator=g) * 0.1).cuda().contiguous()
+    b = (torch.randn(cout, generator=g) * 0.1).cuda().contiguous()
+    L = _lib.load()
+    outs = []
+    for fn in (L.dn_nn_conv3x3_forward, L.dn_nn_conv3x3_forward_mma_sync):
+        y32 = torch.full((n_pix, cout), float("nan"), dtype=torch.float32, device="cuda")
+        y16 = torch.full((n_pix * cout,), float("nan"), dtype=torch.bfloat16, device="cuda")
+        _lib.check(fn(learned._ptr(x), learned._ptr(w), learned._ptr(b), n_pix, H, W, cin, cout,
+                      relu, learned._ptr(y16), learned._ptr(y32), None))
+        _lib.check(L.dn_nn_synchronize(None))
+        outs.append((y32.cpu().double(), y16.cpu().double().view(n_pix, cout)))
+    (a32, a16), (b32, b16) = outs
+    assert torch.isfinite(a32).all() and torch.isfinite(a16).all()
+    assert _rel(a32, b32) < 2e-6  # same BF16 products, FP32 sums in another order
+    assert float((a16 - b16).abs().max()) <= float(b16.abs().max()) * 2 ** -7
 
 
 @pytest.mark.parametrize("cout", [32, 4])
