@@ -774,4 +774,25 @@ __device__ inline float patch_max(const Patch<HPZ, L>& pt, const ViewDev* views,
   return pt.max(views, pairs, n_pairs, h, j, i, best_view, taps);
 }
 
+// ----------------------------------------------------------------------
+// The depthmap's matching-view records (pair factors and view tables),
+// copied to shared memory at the start of a tile: every candidate's
+// homography setup and walk reads them there instead of through L1.
+// p[k].view indexes v.
+struct PairViewSm {
+  ViewDev v[kMaxNbr];
+  PairDev p[kMaxNbr];
+};
+
+__device__ inline void stage_pairs(PairViewSm& s, const MapDev& m, const ViewDev* views,
+                                   const PairDev* pairs) {
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  if (t < m.n_pairs) {
+    PairDev pr = pairs[m.pair0 + t];
+    s.v[t] = views[pr.view];
+    pr.view = t;
+    s.p[t] = pr;
+  }
+}
+
 }  // namespace dn

@@ -65,27 +65,6 @@ __device__ inline void stage_tile(float* tile, int pitch, int rows, const __half
   }
 }
 
-// ----------------------------------------------------------------------
-// The depthmap's matching-view records (pair factors and view tables),
-// copied to shared memory at the start of a tile: every candidate's
-// homography setup and walk reads them there instead of through L1.
-// p[k].view indexes v.
-struct PairViewSm {
-  ViewDev v[kMaxNbr];
-  PairDev p[kMaxNbr];
-};
-
-__device__ inline void stage_pairs(PairViewSm& s, const MapDev& m, const ViewDev* views,
-                                   const PairDev* pairs) {
-  const int t = threadIdx.y * blockDim.x + threadIdx.x;
-  if (t < m.n_pairs) {
-    PairDev pr = pairs[m.pair0 + t];
-    s.v[t] = views[pr.view];
-    pr.view = t;
-    s.p[t] = pr;
-  }
-}
-
 __device__ inline void flush_taps(unsigned taps, unsigned long long* counter) {
   __shared__ unsigned long long block_taps;
   if (threadIdx.x == 0 && threadIdx.y == 0) block_taps = 0;

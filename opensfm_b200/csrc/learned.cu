@@ -36,12 +36,14 @@ sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict
   const int px = blockDim.x / L;
   const int x0 = tl.y * px, y0 = tl.z * blockDim.y;
   const int pitch = px + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  __shared__ PairViewSm spv;
   for (int k = threadIdx.y * blockDim.x + threadIdx.x; k < pitch * rows;
        k += blockDim.x * blockDim.y) {
     const int r = k / pitch, c = k - r * pitch;
     const int y = min(max(y0 - HPZ + r, 0), H - 1), x = min(max(x0 - HPZ + c, 0), W - 1);
     tile[k] = __half2float(rv.img[(size_t)y * W + x]);
   }
+  stage_pairs(spv, m, views, pairs);
   __syncthreads();
   const int g = threadIdx.x / L, lane = threadIdx.x % L;
   const unsigned mask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
@@ -63,8 +65,8 @@ sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict
                                                make_float3(0.f, 0.f, -1.f));
       const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
       for (int k = 0; k < nv; ++k) {
-        const PairDev& pr = pairs[m.pair0 + k];
-        f[1 + 2 * p + k] = pt.view(views[pr.view], pr, h, (float)j, (float)i, taps);
+        const PairDev& pr = spv.p[k];
+        f[1 + 2 * p + k] = pt.view(spv.v[pr.view], pr, h, (float)j, (float)i, taps);
       }
     }
   }
@@ -175,27 +177,34 @@ conv3x3_fwd_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __r
 }
 
 // ------------------------------------------------ conv forward, tcgen05
-// The same convolution on the 5th-generation tensor cores: one CTA of 4
-// warps per tile of 128 pixels (the GEMM's M), N = the output channels
-// (32, or 16 holding the 4 outputs of the last layer), K = 9 taps x 32
-// input channels = 288 in 18 MMAs of K = 16.  The implicit-GEMM A tile
-// (128 x 288 BF16, 72 KB) is gathered by the 128 threads (one pixel row
-// each, 64 contiguous bytes per tap) into shared memory in the canonical
-// no-swizzle K-major layout: 16-byte rows of 8 K values, 8-row core
-// matrices 128 bytes apart (SBO), the two 8-value halves of one MMA's K
-// 2 KB apart (LBO).  The weights (B, [cout][288]) are staged once per CTA
-// in the same layout.  Thread 0 issues the MMAs into a 128 x N FP32
-// accumulator in tensor memory and commits them to an mbarrier; every warp
-// then reads its 32 accumulator lanes (= its 32 pixels) with tcgen05.ld,
-// adds the bias, applies the ReLU and stores BF16 (or FP32) rows.  CTAs
-// loop over tiles; each wait is bounded and sets an error word on expiry.
+// The same convolution on the 5th-generation tensor cores.  A CTA of 4
+// warps computes a spatial tile of 16 rows x 8 columns of one image (128
+// pixels, the GEMM's M) for N = the output channels (32, or 16 holding the
+// 4 outputs of the last layer), K = 9 taps x 32 input channels in 18 MMAs
+// of K = 16.  The tile's input with a one-pixel halo (18 x 10 pixels x 32
+// channels, 11.5 KB) is copied once into shared memory, as four planes of
+// 8 channels, 16 bytes per pixel: for tap (dy, dx) the A operand of the
+// tile is then a strided view of that buffer in the canonical no-swizzle
+// K-major layout -- 8-pixel core-matrix rows of 16 bytes, 8-row groups one
+// halo row (160 bytes) apart (SBO), the two 8-channel halves of one MMA's
+// K one plane (2880 bytes) apart (LBO) -- so no im2col copy is made.  The
+// weights (B, [cout][9 x 32]) are staged once per CTA in the same layout
+// (8-row groups 128 bytes apart).  Thread 0 issues the MMAs into a 128 x N
+// FP32 accumulator in tensor memory and commits them to an mbarrier; the
+// halo of the CTA's next tile streams in with cp.async meanwhile (two
+// buffers).  Every warp then reads its 32 accumulator lanes (its 32
+// pixels) with tcgen05.ld, adds the bias, applies the ReLU and stores.
+// Each wait is bounded and sets an error word on expiry.
 namespace tc {
 
 __device__ int g_error;
 
-constexpr int kBM = 128;               // pixels per tile (MMA M)
-constexpr int kK = 9 * 32;             // GEMM K
-constexpr int kKC = kK / 8;            // 16-byte K chunks
+constexpr int kTR = 16, kTC = 8;             // tile rows x columns (M = 128)
+constexpr int kHR = kTR + 2, kHC = kTC + 2;  // halo buffer rows x columns
+constexpr int kPlane = kHR * kHC * 16;       // bytes of one 8-channel plane
+constexpr int kHalo = 4 * kPlane;            // 32 channels
+constexpr int kK = 9 * 32;                   // GEMM K
+constexpr int kKC = kK / 8;                  // 16-byte K chunks of the weights
 constexpr long long kSpins = 1LL << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -213,10 +222,9 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 
 // Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1),
 // A and B BF16 (bits 7-9, 10-12 = 1), both K-major, N / 8 at bit 17,
-// M / 16 at bit 24.
+// M / 16 = 8 at bit 24.
 constexpr uint32_t idesc_bf16(int n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
-         ((uint32_t)(kBM >> 4) << 24);
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | (8u << 24);
 }
 
 __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase) {
@@ -232,6 +240,13 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase) {
     if (done) return true;
   }
   return false;
+}
+
+// 16-byte asynchronous copy; src_bytes = 0 writes zeros (outside the image).
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+               "r"(src_bytes)
+               : "memory");
 }
 
 template <int NP>
@@ -265,26 +280,56 @@ __device__ __forceinline__ void tmem_load<16>(uint32_t taddr, uint32_t (&r)[16])
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-constexpr size_t smem_bytes(int np) {
-  return (size_t)kKC * kBM * 16 + (size_t)kKC * np * 16 + 16;
+constexpr size_t smem_bytes(int np) { return 2 * (size_t)kHalo + (size_t)kKC * np * 16 + 16; }
+
+// Tile t of the batch: image, first row, first column.
+struct TileXY {
+  long long img;
+  int y0, x0;
+};
+__device__ __forceinline__ TileXY tile_xy(long long t, int H, int W) {
+  const int ty = (H + kTR - 1) / kTR, tx = (W + kTC - 1) / kTC;
+  const long long per = (long long)ty * tx;
+  TileXY r;
+  r.img = t / per;
+  const int k = (int)(t - r.img * per);
+  r.y0 = (k / tx) * kTR;
+  r.x0 = (k % tx) * kTC;
+  return r;
+}
+
+// Issues the copies of tile t's halo into `buf` (one commit group).
+__device__ __forceinline__ void load_halo(uint32_t buf, const __nv_bfloat16* x, long long t, int H,
+                                          int W) {
+  const TileXY tt = tile_xy(t, H, W);
+  for (int e = threadIdx.x; e < kHR * kHC * 4; e += blockDim.x) {
+    const int hp = e >> 2, j = e & 3;
+    const int y = tt.y0 - 1 + hp / kHC, xx = tt.x0 - 1 + hp % kHC;
+    const bool in = y >= 0 && y < H && xx >= 0 && xx < W;
+    const long long q = in ? (tt.img * H + y) * (long long)W + xx : 0;
+    cp_async16(buf + (uint32_t)(j * kPlane + hp * 16), x + q * 32 + j * 8, in ? 16u : 0u);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
 }  // namespace tc
 
 template <int NP>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 4)
 conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ w,
-                      const float* __restrict__ bias, long long n_pix, int H, int W, int cout,
-                      int relu, __nv_bfloat16* __restrict__ y, float* __restrict__ y32,
-                      long long n_tiles) {
+                      const float* __restrict__ bias, int H, int W, int cout, int relu,
+                      __nv_bfloat16* __restrict__ y, float* __restrict__ y32, long long n_tiles) {
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* As = smem;                         // [kKC][kBM][16 B]
-  unsigned char* Bs = smem + (size_t)kKC * kBM * 16;  // [kKC][NP][16 B]
+  unsigned char* halo = smem;                    // 2 x [4 planes][kHR][kHC][16 B]
+  unsigned char* Bs = smem + 2 * kHalo;          // [kKC][NP][16 B]
   uint64_t* mbar = reinterpret_cast<uint64_t*>(Bs + (size_t)kKC * NP * 16);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
 
+  long long t = blockIdx.x;
+  const uint32_t h_base = smem_u32(halo);
+  if (t < n_tiles) load_halo(h_base, x, t, H, W);
   for (int e = tid; e < kKC * NP; e += blockDim.x) {
     const int kc = e / NP, n = e - kc * NP;
     uint4 v = make_uint4(0u, 0u, 0u, 0u);
@@ -301,58 +346,61 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tslot;
-  const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs), mb = smem_u32(mbar);
+  const uint32_t b_base = smem_u32(Bs), mb = smem_u32(mbar);
   constexpr uint32_t idesc = idesc_bf16(NP);
   uint32_t phase = 0;
+  int cur = 0;
   bool ok = true;
-  for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-    const long long p = t * kBM + tid;
-#pragma unroll
-    for (int tap = 0; tap < 9; ++tap) {
-      const long long q = p < n_pix ? nbr_pixel(p, H, W, tap / 3 - 1, tap % 3 - 1) : -1;
-      const uint4* src = reinterpret_cast<const uint4*>(x + (q < 0 ? 0 : q) * 32);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const uint4 v = q >= 0 ? __ldg(src + j) : make_uint4(0u, 0u, 0u, 0u);
-        *reinterpret_cast<uint4*>(As + ((size_t)(tap * 4 + j) * kBM + tid) * 16) = v;
-      }
-    }
+  for (; t < n_tiles; t += gridDim.x) {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
+    const uint32_t a_base = h_base + (uint32_t)(cur * kHalo);
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
-      for (int ks = 0; ks < kK / 16; ++ks) {
-        const uint64_t ad = smem_desc(a_base + (uint32_t)(2 * ks * kBM * 16), kBM * 16, 128);
-        const uint64_t bd = smem_desc(b_base + (uint32_t)(2 * ks * NP * 16), NP * 16, 128);
-        const uint32_t acc = ks > 0 ? 1u : 0u;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-            : "memory");
+      for (int tap = 0; tap < 9; ++tap) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t a_off = (uint32_t)(2 * h * kPlane + ((tap / 3) * kHC + tap % 3) * 16);
+          const uint64_t ad = smem_desc(a_base + a_off, kPlane, kHC * 16);
+          const uint64_t bd =
+              smem_desc(b_base + (uint32_t)((tap * 4 + 2 * h) * NP * 16), NP * 16, 128);
+          const uint32_t acc = (tap | h) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+              : "memory");
+        }
       }
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
               mb)
           : "memory");
     }
+    // The next tile's halo streams in while the MMAs run and the epilogue
+    // stores; its buffer was last read by the MMAs of the previous tile.
+    const long long tn = t + gridDim.x;
+    if (tn < n_tiles) load_halo(h_base + (uint32_t)((cur ^ 1) * kHalo), x, tn, H, W);
     bool done = mbar_wait(mb, phase);
+    if (!done) done = mbar_wait(mb, phase);  // a late completion
     phase ^= 1u;
-    if (!done) done = mbar_wait(mb, phase ^ 1u);  // a late completion of this tile
     ok = __syncthreads_and(done) != 0;
     if (!ok) break;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     uint32_t r[NP];
     tmem_load<NP>(tmem + ((uint32_t)(warp * 32) << 16), r);
-    if (p < n_pix) {
+    const TileXY tt = tile_xy(t, H, W);
+    const int py = tt.y0 + (tid >> 3), px = tt.x0 + (tid & 7);
+    if (py < H && px < W) {
+      const long long p = (tt.img * H + py) * (long long)W + px;
       if (NP == 32) {
         uint32_t o[16];
 #pragma unroll
@@ -378,7 +426,9 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
             y32[p * 32 + c] = relu ? fmaxf(v, 0.f) : v;
           }
       } else {
-        for (int c = 0; c < cout; ++c) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (c >= cout) break;
           float v = __uint_as_float(r[c]) + bias[c];
           if (relu) v = fmaxf(v, 0.f);
           if (y) y[p * cout + c] = __float2bfloat16_rn(v);
@@ -388,7 +438,9 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
+    cur ^= 1;
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   if (!ok && tid == 0) atomicExch(&g_error, 1);
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
@@ -677,13 +729,16 @@ static cudaError_t conv_fwd_tc(const ConvArgs& c, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
-  int dev = 0, sms = 0;
+  int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long tiles = (c.n_pix + tc::kBM - 1) / tc::kBM;
-  const long long grid = std::min<long long>(tiles, 2LL * sms);
-  kern<<<(unsigned)grid, 128, smem, s>>>(c.x, c.w, c.bias, c.n_pix, c.H, c.W, c.cout, c.relu,
-                                         c.y, c.y32, tiles);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem);
+  if (e != cudaSuccess) return e;
+  const long long n_img = c.n_pix / ((long long)c.H * c.W);
+  const long long tiles = n_img * ((c.H + tc::kTR - 1) / tc::kTR) * ((c.W + tc::kTC - 1) / tc::kTC);
+  const long long grid = std::min<long long>(tiles, (long long)std::max(per_sm, 1) * sms);
+  kern<<<(unsigned)grid, 128, smem, s>>>(c.x, c.w, c.bias, c.H, c.W, c.cout, c.relu, c.y, c.y32,
+                                         tiles);
   return cudaGetLastError();
 }
 
