@@ -350,7 +350,10 @@ SCHEDULES = [
     ("learned-0hp", "learned", 0, {}),
     ("learned-1hp", "learned", 1, {}),
     ("learned-2hp", "learned", 2, {}),
+    ("learned-3hp", "learned", 3, {}),
     ("learned-4hp", "learned", 4, {}),
+    ("learned-5hp", "learned", 5, {}),
+    ("learned-6hp", "learned", 6, {}),
     ("learned-near-2hp", "learned", 2, dict(use_far=False, depth_range0=0.05, normal_range0=0.3)),
     ("learned-near-3hp", "learned", 3, dict(use_far=False, depth_range0=0.05, normal_range0=0.3)),
     ("learned-near-4hp", "learned", 4, dict(use_far=False, depth_range0=0.05, normal_range0=0.3)),
