@@ -53,7 +53,7 @@ HALFPASS_DRAM_BYTES = 283_666_432 + 103_742_464
 
 
 # ---------------------------------------------------------------- workload
-WORKLOADS = ("ring24", "mixed-box", "mixed-terrain")
+WORKLOADS = ("ring24", "mixed-box", "mixed-terrain", "aerial")
 
 
 def make_workload(seed=SEED, n_views=N_VIEWS, W=W_, H=H_, kind="ring24"):
@@ -70,6 +70,10 @@ def make_workload(seed=SEED, n_views=N_VIEWS, W=W_, H=H_, kind="ring24"):
         vs = S.ring_viewset(seed, n_views, W, H)
         cands = [vs.neighbors(v, N_CAND) for v in range(n_views)]
         matches = [c[:N_MATCH] for c in cands]
+    elif kind == "aerial":
+        vs = S.aerial_viewset(seed)
+        cands = [vs.neighbors_by_footprint(v, N_CAND) for v in range(len(vs.cameras))]
+        matches = [c[:N_MATCH] for c in cands]
     else:
         vs = S.mixed_viewset(seed, 64, kind.split("-")[1], gpu=True)
         rng = np.random.default_rng(seed + 3)
@@ -78,6 +82,37 @@ def make_workload(seed=SEED, n_views=N_VIEWS, W=W_, H=H_, kind="ring24"):
         matches = cands
     ranges = [S.depth_range(d) for d in vs.depths]
     return vs, ranges, cands, matches
+
+
+def learned_leg(b, n_maps, shapes, steps, vs):
+    """Learned initialisation on the same batch: the feature sweep and the
+    tcgen05 network propose every map's initial planes, then the same
+    PatchMatch + cleaner + pruner run.  Timed on the batch stream around the
+    whole sequence (host launches included); returns depthmaps/s, ms per
+    step and the median accuracy."""
+    from opensfm_b200 import learned as LN
+    from opensfm_b200 import synthetic as S
+
+    if len({tuple(sh) for sh in shapes[:n_maps]}) != 1:
+        return {"skipped": "the proposal network runs on batches of one image size"}
+    H, W = shapes[0]
+    net = LN.ProposalNet.load()
+    maps = list(range(n_maps))
+    LN.propose(net, b, maps, H, W)
+    b.run(prune=True, graph=True)
+    b.synchronize()
+    b.timer_record(0)
+    for _ in range(steps):
+        LN.propose(net, b, maps, H, W)
+        b.run(prune=True, graph=True)
+    b.timer_record(1)
+    b.synchronize()
+    ms = b.timer_elapsed()
+    acc = [S.accuracy(b.get_depth(v), vs.depths[v]) for v in maps]
+    return {"value": n_maps * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+            "accuracy_1pct_median": float(np.median(acc)),
+            "schedule": "proposal (8-plane sweep x 2 views + 6-layer tcgen05 network) then the "
+                        "same 3 iterations, cleaner and pruner"}
 
 
 # ------------------------------------------------------------------ clocks
@@ -303,7 +338,10 @@ def run_ours(args):
         from opensfm_b200 import autotune
 
         key = autotune.workload_key(shapes[:n_maps], [len(m) for m in matches[:n_maps]], PATCH)
-        t = autotune.tune(b, key, {"prune": True, "graph": True})
+        cands = autotune.CANDIDATES
+        if args.workload == "aerial":  # a step takes seconds: the two leading choices only
+            cands = [(32, 4, 2), (32, 4, 18)]
+        t = autotune.tune(b, key, {"prune": True, "graph": True}, candidates=cands)
         tuning = {"choice": list(t["choice"]), "ms": t["ms"], "cached": t["cached"],
                   "source": "opensfm_b200.autotune"}
 
@@ -376,6 +414,12 @@ def run_ours(args):
                 f"{N_MATCH} matching views, {N_CAND} cleaner neighbours, PatchMatch "
                 f"{ITERS} iterations (red-black), patch {PATCH}, min_patch_sd {MIN_SD}, "
                 f"cleaner 0.01 / 3 views, pruner 0.01; plain random initialisation")
+    elif args.workload == "aerial":
+        desc = (f"aerial block: terrain 300x300 m with 40 buildings, {n_maps} reference views "
+                f"1280x960 (128 nadir + 128 at 45 deg, 60 m), {N_MATCH} matching views, "
+                f"{N_CAND} cleaner neighbours (nearest footprints, similar directions), "
+                f"PatchMatch {ITERS} iterations (red-black), patch {PATCH}, cleaner 0.01 / 3 "
+                f"views, pruner 0.01; plain random initialisation")
     else:
         sizes = {}
         for h, w in shapes[:n_maps]:
@@ -387,8 +431,10 @@ def run_ours(args):
                 f"random initialisation; {sum(h * w for h, w in shapes[:n_maps]) / 1e6:.2f} "
                 f"Mpx per step")
     line = {
-        "metric": METRIC if ring else "depthmaps/s (64 mixed-size views, 4-10 matching views, "
-                                      "3 iters, cleaner + pruner)",
+        "metric": METRIC if ring else (
+            "1280px depthmaps/s (256-view aerial block, 6 views, 3 iters, cleaner + pruner)"
+            if args.workload == "aerial" else
+            "depthmaps/s (64 mixed-size views, 4-10 matching views, 3 iters, cleaner + pruner)"),
         "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -426,6 +472,8 @@ def run_ours(args):
     # cleaner launch and three pruner launches per map.
     pm_launches = 1 if (tuning and tuning["choice"][2] & 16) else (1 + 2 * ITERS + 1)
     line["gpu_launches"] = args.steps * (pm_launches + 4 * n_maps)
+    if args.learned:
+        line["config"]["learned"] = learned_leg(b, n_maps, shapes, args.steps, vs)
     if rank == 0 and world == 1 and not args.no_cpu and ring:
         try:
             line["cpu_baseline"] = cpu_sample(work, seconds=args.cpu_seconds)
@@ -480,8 +528,10 @@ def main():
     ap.add_argument("--maps", type=int, default=0,
                     help="depthmaps per step (default: all; smaller for profiling)")
     ap.add_argument("--workload", default="ring24", choices=WORKLOADS,
-                    help="ring24 (640x480, the headline configuration) or 64 mixed-size "
-                         "views of the box or terrain scene")
+                    help="ring24 (640x480, the headline configuration), 64 mixed-size views "
+                         "of the box or terrain scene, or the 256-view 1280x960 aerial block")
+    ap.add_argument("--learned", action="store_true",
+                    help="also time the learned initialisation on the same batch")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

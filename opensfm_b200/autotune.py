@@ -29,7 +29,7 @@ def workload_key(shapes: Sequence[Tuple[int, int]], n_views: Sequence[int], patc
     counts: Dict[str, int] = {}
     for s in sig:
         counts[s] = counts.get(s, 0) + 1
-    return f"p{patch}:" + ",".join(f"{k}*{v}" for k, v in sorted(counts.items()))
+    return f"v2:p{patch}:" + ",".join(f"{k}*{v}" for k, v in sorted(counts.items()))
 
 
 def _load() -> dict:

@@ -1387,11 +1387,10 @@ dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, i
     const View& r = *e.views[m->ref];
     DN_CHECK((int64_t)r.W * r.H * dn::kFeatC <= map_stride, "map_stride too small");
   }
-  DN_CHECK(e.variant == 4, "the feature sweep runs with 4 lanes per pixel (tuning variant 4)");
   DN_TRY(e.check_params(Mode::kPatchMatch));
   DN_TRY(e.prepare());
   dn::LaunchArgs a = e.args(false);
-  a.tiles = e.d_tiles_init.p;  // 4 lanes per pixel tiling
+  a.tiles = e.d_tiles_init.p;  // the initialisation tiling of the current lanes
   a.n_tiles = e.n_tiles_init;
   DN_CUDA(dn::launch_sweep(a, static_cast<__nv_bfloat16*>(feat), map_stride, n_planes, e.stream));
   return DN_OK;

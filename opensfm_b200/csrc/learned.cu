@@ -22,13 +22,15 @@
 namespace dn {
 
 // ---------------------------------------------------------------- sweep
-// 4 lanes per pixel (the 7 x 7 cooperative patch of the PatchMatch kernels).
+// L lanes per pixel, as the PatchMatch initialisation (the 7 x 7 patch; the
+// tiles are the batch's initialisation tiles for its tuning).
+template <int L>
 __global__ void __launch_bounds__(128)
 sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
                       const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
                       __nv_bfloat16* __restrict__ feat, long long map_stride, int n_planes) {
   extern __shared__ float tile[];
-  constexpr int HPZ = 3, L = 4;
+  constexpr int HPZ = 3;
   const int4 tl = tiles[blockIdx.x];
   const MapDev& m = maps[tl.x];
   const ViewDev& rv = views[m.ref_view];
@@ -46,7 +48,8 @@ sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict
   stage_pairs(spv, m, views, pairs);
   __syncthreads();
   const int g = threadIdx.x / L, lane = threadIdx.x % L;
-  const unsigned mask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
+  const unsigned mask = (L == 1) ? (1u << (threadIdx.x & 31))
+                                 : (((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1)));
   const int i = y0 + threadIdx.y, j = x0 + g;
   if (i >= H || j >= W) return;
   float f[kFeatC];
@@ -768,13 +771,24 @@ cudaError_t conv3x3_backward(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaS
   if (c.cin == 32 && c.cout == 4) return conv_bwd_t<32, 4>(c, wt_scratch, s);
   return cudaErrorInvalidValue;
 }
+template <int L>
+static cudaError_t sweep_l(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
+                           int n_planes, cudaStream_t s) {
+  // a.tiles: the initialisation tiling for L lanes (bx / L pixels per row).
+  const size_t smem = sizeof(float) * (a.bx / L + 6) * (a.by + 6);
+  sweep_features_kernel<L><<<a.n_tiles, dim3(a.bx, a.by), smem, s>>>(
+      a.maps, a.views, a.pairs, a.tiles, feat, map_stride, n_planes);
+  return cudaGetLastError();
+}
 cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
                          int n_planes, cudaStream_t s) {
-  // a.tiles must be the 4-lanes-per-pixel tiling (bx / 4 pixels per row).
-  const size_t smem = sizeof(float) * (a.bx / 4 + 6) * (a.by + 6);
-  sweep_features_kernel<<<a.n_tiles, dim3(a.bx, a.by), smem, s>>>(a.maps, a.views, a.pairs, a.tiles,
-                                                                   feat, map_stride, n_planes);
-  return cudaGetLastError();
+  switch (a.p.variant) {
+    case 1: return sweep_l<1>(a, feat, map_stride, n_planes, s);
+    case 2: return sweep_l<2>(a, feat, map_stride, n_planes, s);
+    case 4: return sweep_l<4>(a, feat, map_stride, n_planes, s);
+    case 8: return sweep_l<8>(a, feat, map_stride, n_planes, s);
+  }
+  return cudaErrorInvalidValue;
 }
 cudaError_t launch_l1_loss(const float* pred, const float* target, long long n_pix,
                            float normal_weight, __nv_bfloat16* dpred, float* loss_sum, float* count,

@@ -313,6 +313,28 @@ class ViewSet:
         d.sort()
         return [v for _, v in d[:k]]
 
+    def neighbors_by_footprint(self, ref: int, k: int, min_cos: float = 0.9,
+                               ground_z: float = 0.0) -> List[int]:
+        """The k views looking the most alike at the nearest ground point:
+        among views whose optical axes are within acos(min_cos) of ``ref``'s,
+        the ones whose axes meet the plane z = ground_z nearest to where
+        ``ref``'s does (for mixed nadir and oblique sets)."""
+        def axis(c):
+            d = c.R[2]
+            s = (ground_z - c.center[2]) / d[2] if abs(d[2]) > 1e-9 else 1e9
+            return d, c.center + s * d
+
+        d0, g0 = axis(self.cameras[ref])
+        cand = []
+        for v, c in enumerate(self.cameras):
+            if v == ref:
+                continue
+            d, g = axis(c)
+            if float(d @ d0) >= min_cos:
+                cand.append((float(np.linalg.norm(g - g0)), v))
+        cand.sort()
+        return [v for _, v in cand[:k]]
+
 
 def ring_viewset(seed: int, n_views: int, width: int, height: int, step_deg: float = 10.0,
                  supersample: int = 2) -> ViewSet:
@@ -365,6 +387,42 @@ def mixed_viewset(seed: int, n_views: int = 64, kind: str = "box",
     if len(base) < n_views:
         raise ValueError(f"only {len(base)} cameras fit the {kind} layout")
     cams = [Camera(intrinsics(w, h), c.R, c.t, w, h) for c, (w, h) in zip(base, dims)]
+    imgs, deps = [], []
+    for c in cams:
+        if gpu:
+            im, de = render_gpu(scene, [c], supersample)
+            im, de = im[0].cpu().numpy(), de[0].cpu().numpy()
+        else:
+            im, de = render(scene, c, supersample)
+        imgs.append(im)
+        deps.append(de)
+    return ViewSet(scene, cams, imgs, deps)
+
+
+def aerial_viewset(seed: int, n_nadir: int = 128, n_oblique: int = 128, width: int = 1280,
+                   height: int = 960, size: float = 300.0, n_buildings: int = 40,
+                   altitude: float = 60.0, oblique_deg: float = 45.0, supersample: int = 1,
+                   gpu: bool = True) -> ViewSet:
+    """A large aerial block: terrain of size x size m (amplitude 8 m) with
+    ``n_buildings`` buildings, seen by ``n_nadir`` nadir views and
+    ``n_oblique`` views tilted by ``oblique_deg`` (a quarter looking each
+    way), all width x height, spread evenly over grids with 70 % forward and
+    60 % side overlap at ``altitude``."""
+    scene = terrain_scene(seed, size=size, amp=8.0, n_buildings=n_buildings)
+
+    def spread(cams, n):
+        if n >= len(cams):
+            return cams
+        idx = np.round(np.linspace(0, len(cams) - 1, n)).astype(int)
+        return [cams[i] for i in idx]
+
+    cams = spread(nadir_cameras(size, altitude, width, height), n_nadir)
+    per = [n_oblique // 4 + (1 if k < n_oblique % 4 else 0) for k in range(4)]
+    for k in range(4):
+        if per[k]:
+            grid = nadir_cameras(size, altitude, width, height, oblique_deg=oblique_deg,
+                                 yaw_deg=90.0 * k)
+            cams += spread(grid, per[k])
     imgs, deps = [], []
     for c in cams:
         if gpu:
