@@ -160,7 +160,7 @@ struct View {
   float cbias = 0.f;
   DevBuf<__half> img;
   DevBuf<uint8_t> mask;
-  DevBuf<float4> quad;
+  DevBuf<uint2> quad;  // bilinear coefficient table, 4 x FP16 per entry
   DevBuf<uint8_t> gray;  // u8 copy (pruner colour when none is given)
 };
 
@@ -271,8 +271,7 @@ struct Engine {
     const dn::TableGeom tg = dn::table_geom(W, H);
     DN_CHECK(W <= 8192 - 2 * dn::kPad, "image wider than the table layout supports (8176)");
     DN_CUDA(v->img.alloc((size_t)W * H));
-    // 64 spare entries after the last row: prefetches may reach past it.
-    DN_CUDA(v->quad.alloc((size_t)tg.TP * tg.TH + 64));
+    DN_CUDA(v->quad.alloc((size_t)tg.TP * tg.TH));
     DN_CUDA(v->gray.alloc((size_t)W * H));
     DN_CUDA(cudaMemcpy2DAsync(v->gray.p, W, image, stride, W, H, cudaMemcpyHostToDevice, stream));
     if (mask) {

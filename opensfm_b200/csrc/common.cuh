@@ -3,7 +3,9 @@
 // HBM layout (one reconstruction = a set of views + a set of depthmaps):
 //   ViewDev  per view:  FP16 image [H][W] (uint8 intensities are exact in
 //            FP16), optional uint8 mask, and a bilinear coefficient table
-//            `quad` [(H-1+2P)][(W-1+2P)] of float4 (see build_quad_kernel).
+//            `quad` [(H-1+2P)][TP] of 4 x FP16 (8 bytes; the coefficients
+//            are integers of magnitude <= 510, exact in FP16; see
+//            build_quad_kernel).
 //   PairDev  per (depthmap, matching view): the plane-induced homography
 //            split as H(v) = G + e f^T with G = K_o Q_o K_0^-1, e = K_o a_o,
 //            f = K_0^-T v (reference depthmap.cc:88-102 composes the same
@@ -31,8 +33,8 @@ constexpr int kFarStart = 3;     // first far sample distance (then +2)
 struct ViewDev {
   const __half* img;     // [H][W]
   const uint8_t* mask;   // [H][W] or null (all valid)
-  const float4* quad;    // [TH][TP], entry (ix, iy) at (iy + P) * TP + ix + P
-  const float4* quad0;   // &quad[entry (0, 0)]
+  const uint2* quad;     // [TH][TP] x 4 FP16, entry (ix, iy) at (iy + P) * TP + ix + P
+  const uint2* quad0;    // &quad[entry (0, 0)]
   int W, H, TP, TH;
   float cbias;           // intensity centring constant folded into quad.x
   float magic;           // M for this pitch
@@ -281,16 +283,25 @@ __device__ inline Warp warp_setup(const ViewDev& vw, const PairDev& pr, const Hy
   return wp;
 }
 
+// One coefficient entry (e0, e1, e2, e3) as FP32 (exact: the FP16 values are
+// small integers).
+__device__ __forceinline__ float4 quad_entry(const uint2* base, int off) {
+  const uint2 h = __ldg(base + off);
+  const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&h.x));
+  const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&h.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+
 // Bilinear sample at (x, y) inside the padded table: floor by adding the
 // magic constant rounding down, exact fractions, one IMAD for the entry
-// index, one 16-byte load and three FMAs:  y - cbias = e0 + fx e1 +
+// index, one 8-byte load and three FMAs:  y - cbias = e0 + fx e1 +
 // fy (e2 + fx e3).
 __device__ inline float table_sample(const ViewDev& vw, float x, float y) {
   const float M = vw.magic;
   const float tx = __fadd_rd(x, M), ty = __fadd_rd(y, M);
   const float fx = x - (tx - M), fy = y - (ty - M);
   const int off = (int)(__float_as_uint(ty) * (unsigned)vw.TP + __float_as_uint(tx));
-  const float4 q = __ldg(vw.quad0 + off);
+  const float4 q = quad_entry(vw.quad0, off);
   return fmaf(fy, fmaf(fx, q.w, q.z), fmaf(fx, q.y, q.x));
 }
 
@@ -300,7 +311,7 @@ __device__ inline float table_sample_clamped(const ViewDev& vw, float x, float y
   const float xlo = -(float)kPad, xhi = (float)(vw.W - 1 + kPad);
   const float ylo = -(float)kPad, yhi = (float)(vw.H - 1 + kPad);
   if (x >= xlo && x < xhi && y >= ylo && y < yhi) return table_sample(vw, x, y);
-  return vw.quad[0].x;
+  return quad_entry(vw.quad, 0).x;
 }
 
 // Per-patch centring value for the y sums: the table sample at the floor
@@ -315,7 +326,7 @@ __device__ inline float patch_shift(const ViewDev& vw, const Warp& wp) {
   const float M = vw.magic;
   const float tx = __fadd_rd(wp.X0, M), ty = __fadd_rd(wp.Y0, M);
   const int off = (int)(__float_as_uint(ty) * (unsigned)vw.TP + __float_as_uint(tx));
-  return __ldg(&vw.quad0[off].x);
+  return quad_entry(vw.quad0, off).x;
 }
 
 template <int HPZ>
@@ -583,13 +594,13 @@ __device__ inline float coop_walk_clamped(const CoopPatch<L>& cp, const ViewDev&
 // Two table samples at the packed positions (X, Y), as table_sample does
 // one: returns the packed samples.
 __device__ __forceinline__ u64 sample_pair(u64 X, u64 Y, u64 MM, unsigned TP,
-                                           const float4* __restrict__ q0) {
+                                           const uint2* __restrict__ q0) {
   const u64 TX = add2_rd(X, MM), TY = add2_rd(Y, MM);
   const u64 FX = sub2(X, sub2(TX, MM)), FY = sub2(Y, sub2(TY, MM));
   const unsigned oa = __float_as_uint(lo2(TY)) * TP + __float_as_uint(lo2(TX));
   const unsigned ob = __float_as_uint(hi2(TY)) * TP + __float_as_uint(hi2(TX));
-  const float4 qa = __ldg(q0 + (int)oa);
-  const float4 qb = __ldg(q0 + (int)ob);
+  const float4 qa = quad_entry(q0, (int)oa);
+  const float4 qb = quad_entry(q0, (int)ob);
   const float fxa = lo2(FX), fya = lo2(FY), fxb = hi2(FX), fyb = hi2(FY);
   const float ya = fmaf(fya, fmaf(fxa, qa.w, qa.z), fmaf(fxa, qa.y, qa.x));
   const float yb = fmaf(fyb, fmaf(fxb, qb.w, qb.z), fmaf(fxb, qb.y, qb.x));
@@ -611,7 +622,7 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
   const float yl = fmaf(wp.ay, dx0, fmaf(wp.by, -3.0f, wp.Y0));
   const u64 MM = pk2(vw.magic, vw.magic);
   const unsigned TP = (unsigned)vw.TP;
-  const float4* __restrict__ q0 = vw.quad0;
+  const uint2* __restrict__ q0 = vw.quad0;
   const float sh = patch_shift<false>(vw, wp);
   const u64 SH = pk2(sh, sh);
   u64 S1 = 0ull, S2 = 0ull, S3 = 0ull;  // (+0.0f, +0.0f) pairs

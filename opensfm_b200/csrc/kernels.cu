@@ -32,9 +32,10 @@ __global__ void u8_to_half_kernel(const uint8_t* __restrict__ src, int W, int H,
 // fractions:  y - cbias = e0 + fx e1 + fy (e2 + fx e3).  Blocks that reach
 // outside [0, W-1) x [0, H-1) hold the constant -cbias, i.e. the
 // reference's zero sample (LinearInterpolation, depthmap.cc:16-18).  All
-// coefficients are small integers, exact in FP32.  Rows have pitch TP.
+// coefficients are integers of magnitude <= 510 (cbias is an integer), so
+// the four are stored exactly as FP16 in 8 bytes.  Rows have pitch TP.
 __global__ void build_quad_kernel(const __half* __restrict__ img, int W, int H, float cbias,
-                                  float4* __restrict__ quad, int TP, int TW, int TH) {
+                                  uint2* __restrict__ quad, int TP, int TW, int TH) {
   const int tx = blockIdx.x * blockDim.x + threadIdx.x, ty = blockIdx.y;
   if (tx >= TP || ty >= TH) return;
   const int ix = tx - kPad, iy = ty - kPad;
@@ -46,7 +47,9 @@ __global__ void build_quad_kernel(const __half* __restrict__ img, int W, int H, 
     const float q11 = __half2float(img[(size_t)(iy + 1) * W + ix + 1]);
     q = make_float4(q00 - cbias, q01 - q00, q10 - q00, q11 - q10 - q01 + q00);
   }
-  quad[(size_t)ty * TP + tx] = q;
+  const __half2 lo = __floats2half2_rn(q.x, q.y), hi = __floats2half2_rn(q.z, q.w);
+  quad[(size_t)ty * TP + tx] = make_uint2(*reinterpret_cast<const unsigned*>(&lo),
+                                          *reinterpret_cast<const unsigned*>(&hi));
 }
 
 // ----------------------------------------------------------------------
@@ -705,7 +708,7 @@ cudaError_t launch_persistent(const PersistentArgs& pa, cudaStream_t s) {
 }
 
 cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, __half* d_img,
-                                float4* d_quad, int TP, int TW, int TH, float cbias,
+                                uint2* d_quad, int TP, int TW, int TH, float cbias,
                                 cudaStream_t s) {
   u8_to_half_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(d_u8, W, H, stride, d_img);
   build_quad_kernel<<<dim3((TP + 255) / 256, TH), 256, 0, s>>>(d_img, W, H, cbias, d_quad, TP, TW,

@@ -37,7 +37,7 @@ struct PersistentArgs {
 };
 cudaError_t launch_persistent(const PersistentArgs& pa, cudaStream_t s);
 cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, __half* d_img,
-                                float4* d_quad, int TP, int TW, int TH, float cbias,
+                                uint2* d_quad, int TP, int TW, int TH, float cbias,
                                 cudaStream_t s);
 
 // Table geometry of a W x H view: used width TW = W - 1 + 2P, rows
