@@ -182,6 +182,12 @@ dn_status dn_batch_synchronize(dn_batch* b);
  * pointer may be NULL to skip it.  clean may be NULL. */
 dn_status dn_batch_get_depthmap(dn_batch* b, int map_id, float* depth, float* plane,
                                 float* score, int32_t* nghbr, float* clean);
+/* The final (clean = 0) or cleaned (clean = 1) depth of n maps into host
+ * buffers depths[k] (f32 [H][W] of map map_ids[k]), with one stream
+ * synchronisation for all of them (no reference counterpart; the copies
+ * run asynchronously when the buffers are pinned). */
+dn_status dn_batch_get_depths(dn_batch* b, int n, const int* map_ids, float* const* depths,
+                              int clean);
 /* PatchMatch schedule: half-passes per run (-1: 2 x iterations), and per
  * half-pass the candidate sets: the 4 adjacent planes (use_near), the 4 far
  * planes (use_far), n_refine refinements whose first depth / normal-slope

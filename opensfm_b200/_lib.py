@@ -77,6 +77,7 @@ _SIGNATURES = {
     "dn_batch_run": ([_vp, ctypes.c_uint], _i),
     "dn_batch_synchronize": ([_vp], _i),
     "dn_batch_get_depthmap": ([_vp, _i, _f, _f, _f, _i32, _f], _i),
+    "dn_batch_get_depths": ([_vp, _i, _i32, _vp, _i], _i),
     "dn_batch_set_init": ([_vp, _i, _f], _i),
     "dn_batch_set_schedule": ([_vp, _i, _i, _i, _i, ctypes.c_float, ctypes.c_float], _i),
     "dn_batch_pruned_count": ([_vp, ctypes.POINTER(ctypes.c_int64)], _i),

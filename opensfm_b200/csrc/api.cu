@@ -718,6 +718,28 @@ struct Engine {
     return DN_OK;
   }
 
+  // Final depths of several maps into host buffers: every copy is queued on
+  // the batch stream (asynchronous for pinned buffers), one synchronisation.
+  dn_status fetch_depths(int n, const int* ids, float* const* outs, int clean) {
+    DN_CHECK(n >= 0 && (n == 0 || (ids && outs)), "NULL argument");
+    DN_CHECK(computed, "no result computed yet");
+    DN_CUDA(cudaSetDevice(device));
+    for (int k = 0; k < n; ++k) {
+      DN_CHECK(ids[k] >= 0 && ids[k] < (int)maps.size(), "depthmap id out of range");
+      DN_CHECK(outs[k], "NULL output buffer");
+      const Map& m = *maps[ids[k]];
+      DN_CHECK(!clean || m.clean.p, "the depthmap was not cleaned");
+    }
+    for (int k = 0; k < n; ++k) {
+      const Map& m = *maps[ids[k]];
+      const View& r = *views[m.ref];
+      DN_CUDA(cudaMemcpyAsync(outs[k], clean ? m.clean.p : m.depth.p,
+                              (size_t)r.W * r.H * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    }
+    DN_CUDA(cudaStreamSynchronize(stream));
+    return DN_OK;
+  }
+
   dn_status set_init(int map, const float* planes) {
     DN_CHECK(map >= 0 && map < (int)maps.size(), "depthmap id out of range");
     Map& m = *maps[map];
@@ -1276,6 +1298,11 @@ dn_status dn_batch_get_depthmap(dn_batch* b, int map_id, float* depth, float* pl
                                 float* score, int32_t* nghbr, float* clean) {
   DN_CHECK(b, "NULL batch");
   return b->eng.fetch(map_id, depth, plane, score, nghbr, clean);
+}
+dn_status dn_batch_get_depths(dn_batch* b, int n, const int* map_ids, float* const* depths,
+                              int clean) {
+  DN_CHECK(b, "NULL batch");
+  return b->eng.fetch_depths(n, map_ids, depths, clean);
 }
 dn_status dn_batch_pruned_count(dn_batch* b, int64_t* count) {
   DN_CHECK(b && count, "NULL argument");

@@ -409,6 +409,8 @@ def test_batch_matches_single_estimator(scene):
     want = e.compute_patch_match()
     for a, w in zip(got, want):
         assert np.array_equal(a, w)
+    # The batched fetch returns the same depth.
+    assert np.array_equal(b.get_depths([m0])[0], want[0])
     # Graph replay reproduces the eager run.
     b.run(graph=True)
     b.synchronize()
