@@ -336,6 +336,31 @@ dn_status dn_prune_noalloc(const dn_prune_view* views, int n_views, float same_d
 /* Message for the last failed dn_prune_noalloc call on this thread. */
 const char* dn_noalloc_last_error(void);
 
+/* ----------------------------------------------------------------------
+ * Depthmap files (host only, no GPU needed).  OpenSfM stores each view's
+ * raw and cleaned depthmap as an .npz archive wrapped in one LZ4 frame
+ * (opensfm/dataset.py:1080-1098 writes with lz4.frame.compress,
+ * 1100-1112 reads with lz4.frame.decompress).  These replace that
+ * dependency; opensfm_b200/dense_io.py uses them.
+ * ---------------------------------------------------------------------- */
+/* xxHash32 of n bytes (the LZ4 frame checksums). */
+uint32_t dn_xxh32(const void* data, int64_t n, uint32_t seed);
+/* Largest frame dn_lz4f_compress can write for n input bytes. */
+int64_t dn_lz4f_compress_bound(int64_t n);
+/* One LZ4 frame (independent 4 MB blocks, content size stored, stored
+ * blocks where compression does not pay): *out_len receives its size; dst
+ * may be NULL to query it, else it must hold `capacity` >= *out_len bytes. */
+dn_status dn_lz4f_compress(const void* src, int64_t n, void* dst, int64_t capacity,
+                           int64_t* out_len);
+/* Decodes one or more concatenated LZ4 frames (linked or independent
+ * blocks, optional block / content checksums and content size, skippable
+ * frames).  Call with dst NULL to get *out_len, then again with the same
+ * src and a buffer of at least that many bytes. */
+dn_status dn_lz4f_decompress(const void* src, int64_t n, void* dst, int64_t capacity,
+                             int64_t* out_len);
+/* Message for the last failed depthmap-file call on this thread. */
+const char* dn_io_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

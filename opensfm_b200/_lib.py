@@ -100,6 +100,13 @@ _SIGNATURES = {
     "dn_nn_conv3x3_forward_mma_sync": ([_vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _i, _vp,
                                         _vp, _vp], _i),
     "dn_nn_synchronize": ([_vp], _i),
+    "dn_xxh32": ([_vp, ctypes.c_int64, ctypes.c_uint32], ctypes.c_uint32),
+    "dn_lz4f_compress_bound": ([ctypes.c_int64], ctypes.c_int64),
+    "dn_lz4f_compress": ([_vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
+                         _i),
+    "dn_lz4f_decompress": ([_vp, ctypes.c_int64, _vp, ctypes.c_int64,
+                            ctypes.POINTER(ctypes.c_int64)], _i),
+    "dn_io_last_error": ([], ctypes.c_char_p),
     "dn_nn_conv3x3_backward": ([_vp, _vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _vp, _vp, _vp,
                                 _vp, _vp], _i),
     "dn_nn_l1_loss": ([_vp, _vp, ctypes.c_int64, ctypes.c_float, _vp, _vp, _vp, _vp], _i),

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_build", "libdense_b200.so")
-SOURCES = ["kernels.cu", "cleanprune.cu", "learned.cu", "api.cu", "noalloc.cu"]
+SOURCES = ["kernels.cu", "cleanprune.cu", "learned.cu", "api.cu", "noalloc.cu", "lz4io.cu"]
 HEADERS = ["common.cuh", "kernels.h", "learned.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -38,7 +38,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     objs = []
     for s in srcs:
         o = os.path.join(os.path.dirname(LIB), os.path.basename(s) + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, "-dc" if False else "-c", s, "-o", o]
+        cmd = [NVCC, *ARCH, *FLAGS, "-c", s, "-o", o]
         if ptxas_v:
             cmd += ["-Xptxas", "-v"]
         if verbose:
