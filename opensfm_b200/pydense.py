@@ -166,22 +166,6 @@ class DepthmapEstimator(_Handle):
                                                 ptr(nghbr, _i32)))
         return score, nghbr
 
-    def get_depths(self, map_ids, outs=None, clean: bool = False):
-        """Final (or cleaned) depths of several maps with one synchronisation.
-        ``outs`` (optional) are C-contiguous float32 (H, W) host arrays, pinned
-        ones copy asynchronously."""
-        ids = [int(m) for m in map_ids]
-        if outs is None:
-            outs = [np.zeros(self._map_shapes[m], np.float32) for m in ids]
-        for m, o in zip(ids, outs):
-            if o.dtype != np.float32 or not o.flags.c_contiguous or o.shape != self._map_shapes[m]:
-                raise ValueError("outputs must be C-contiguous float32 arrays of the map's shape")
-        id_arr = (ctypes.c_int32 * len(ids))(*ids)
-        ptr_arr = (ctypes.c_void_p * len(ids))(*[o.ctypes.data for o in outs])
-        check(self._L.dn_batch_get_depths(self._h, len(ids), id_arr,
-                                          ctypes.cast(ptr_arr, ctypes.c_void_p), int(bool(clean))))
-        return outs
-
     def last_taps(self) -> int:
         v = ctypes.c_uint64()
         check(self._L.dn_estimator_last_taps(self._h, ctypes.byref(v)))
@@ -413,6 +397,22 @@ class Batch(_Handle):
             check(self._L.dn_batch_get_depthmap(self._h, int(map_id), ptr(out, _f), None, None,
                                                 None, None))
         return out
+
+    def get_depths(self, map_ids, outs=None, clean: bool = False):
+        """Final (or cleaned) depths of several maps with one synchronisation.
+        ``outs`` (optional) are C-contiguous float32 (H, W) host arrays, pinned
+        ones copy asynchronously."""
+        ids = [int(m) for m in map_ids]
+        if outs is None:
+            outs = [np.zeros(self._map_shapes[m], np.float32) for m in ids]
+        for m, o in zip(ids, outs):
+            if o.dtype != np.float32 or not o.flags.c_contiguous or o.shape != self._map_shapes[m]:
+                raise ValueError("outputs must be C-contiguous float32 arrays of the map's shape")
+        id_arr = (ctypes.c_int32 * len(ids))(*ids)
+        ptr_arr = (ctypes.c_void_p * len(ids))(*[o.ctypes.data for o in outs])
+        check(self._L.dn_batch_get_depths(self._h, len(ids), id_arr,
+                                          ctypes.cast(ptr_arr, ctypes.c_void_p), int(bool(clean))))
+        return outs
 
     def last_taps(self) -> int:
         v = ctypes.c_uint64()
