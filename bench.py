@@ -49,7 +49,7 @@ FLOPS_PER_TAP = 25  # affine warp 8 + bilinear 11 + NCC sums 6 (FMA = 2)
 # DRAM bytes (read + write) of one half-pass launch over the 24 maps, from an
 # ncu capture of this workload: the depthmap state read and written once plus
 # the first touch of the coefficient tables; every other gather hits L2.
-HALFPASS_DRAM_BYTES = 283_666_432 + 103_742_464
+HALFPASS_DRAM_BYTES = 226_447_360 + 91_279_616
 
 
 # ---------------------------------------------------------------- workload
@@ -452,7 +452,7 @@ def run_ours(args):
             "init": "plain", "global_batch": n_maps * world, "parallelism": f"replicas x{world}",
             "tuning": tuning,
             "l2": "working set larger than L2 (views, tables and state ~%.0f MB)" % (
-                sum((w + 15) * (h + 15) * 16 + w * h * (16 + 4 + 4 + 4 + 4 + 2)
+                sum((w + 15) * (h + 15) * 8 + w * h * (16 + 4 + 4 + 4 + 4 + 2)
                     for h, w in shapes[:n_maps]) / 1e6),
             "accuracy_1pct_median": float(np.median(accs)),
             "stage_ms": {"init": stages[0], "halfpasses": stages[1], "post": stages[2],
@@ -463,7 +463,7 @@ def run_ours(args):
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "traffic": HALFPASS_DRAM_BYTES if (ring and n_maps == N_VIEWS) else None,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                              "half-pass launch over the 24 maps (4 lanes per pixel)",
+                              "half-pass launch over the 24 maps (2 lanes per pixel)",
             "peak_source": "measured FP32 FMA loop on this GPU (dn_fp32_peak); "
                            "MEASURED_PEAKS.json has no FP32 figure",
             "algorithmic": f"{FLOPS_PER_TAP} flops per NCC tap x {taps[1]} taps in "
