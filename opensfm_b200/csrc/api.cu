@@ -194,7 +194,7 @@ struct Engine {
   float same_depth_thr = 0.01f;
   int min_consistent = 2;
   int bx = 32, by = 4;  // thread block shape
-  int variant = 4;      // lanes per pixel in init / half-passes (1, 2, 4, 8)
+  int variant = 2;      // lanes per pixel in init / half-passes (1, 2, 4, 8); 2 measured fastest
   int half_passes = -1;  // -1: 2 x iterations
   int persistent = 0;    // one cooperative persistent launch per PatchMatch run
   DevBuf<unsigned> d_sync;

@@ -171,7 +171,7 @@ class DepthmapEstimator(_Handle):
         check(self._L.dn_estimator_last_taps(self._h, ctypes.byref(v)))
         return int(v.value)
 
-    def set_tuning(self, bx: int = 32, by: int = 4, variant: int = 4) -> None:
+    def set_tuning(self, bx: int = 32, by: int = 4, variant: int = 2) -> None:
         check(self._L.dn_estimator_set_tuning(self._h, int(bx), int(by), int(variant)))
 
 
@@ -351,7 +351,7 @@ class Batch(_Handle):
             raise ValueError("image must keep the view's size")
         check(self._L.dn_batch_set_view_image(self._h, int(view_id), ptr(im, _u8), W))
 
-    def set_tuning(self, bx: int = 32, by: int = 4, variant: int = 4) -> None:
+    def set_tuning(self, bx: int = 32, by: int = 4, variant: int = 2) -> None:
         check(self._L.dn_batch_set_tuning(self._h, int(bx), int(by), int(variant)))
 
     def timer_record(self, slot: int) -> None:
