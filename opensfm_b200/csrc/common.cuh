@@ -410,11 +410,13 @@ __device__ __forceinline__ u64 pk2(float a, float b) {
 __device__ __forceinline__ float lo2(u64 r) {
   float a, b;
   asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+  (void)b;
   return a;
 }
 __device__ __forceinline__ float hi2(u64 r) {
   float a, b;
   asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+  (void)a;
   return b;
 }
 __device__ __forceinline__ u64 add2(u64 a, u64 b) {
