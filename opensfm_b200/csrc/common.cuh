@@ -408,15 +408,13 @@ __device__ __forceinline__ u64 pk2(float a, float b) {
   return r;
 }
 __device__ __forceinline__ float lo2(u64 r) {
-  float a, b;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
-  (void)b;
+  float a;
+  asm("{\n\t.reg .f32 unused;\n\tmov.b64 {%0, unused}, %1;\n\t}" : "=f"(a) : "l"(r));
   return a;
 }
 __device__ __forceinline__ float hi2(u64 r) {
-  float a, b;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
-  (void)a;
+  float b;
+  asm("{\n\t.reg .f32 unused;\n\tmov.b64 {unused, %0}, %1;\n\t}" : "=f"(b) : "l"(r));
   return b;
 }
 __device__ __forceinline__ u64 add2(u64 a, u64 b) {
