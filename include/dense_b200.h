@@ -36,7 +36,8 @@ typedef enum {
   DN_OUT_OF_MEMORY = 2,  /* device or pinned allocation failed */
   DN_DEVICE_ERROR = 3,   /* CUDA runtime error, or no usable device */
   DN_TIMEOUT = 4,        /* a bounded device-side wait expired */
-  DN_NOT_READY = 5       /* result requested before it was computed */
+  DN_NOT_READY = 5,      /* result requested before it was computed */
+  DN_OUT_OF_RANGE = 6    /* an index out of range (the reference throws std::out_of_range) */
 } dn_status;
 
 /* Message for the last failed call on this thread ("" if none). */
@@ -335,6 +336,38 @@ dn_status dn_prune_noalloc(const dn_prune_view* views, int n_views, float same_d
                            int64_t capacity, unsigned long long* count, void* stream);
 /* Message for the last failed dn_prune_noalloc call on this thread. */
 const char* dn_noalloc_last_error(void);
+
+/* ----------------------------------------------------------------------
+ * GPUDepthmapCleaner (cleaner.h:16-60, cleaner.cc:19-170; kernel
+ * acmmp_clean_depthmap, opencl_kernels.h:2155-2273): per reference pixel,
+ * forward reprojection into each source (at most 16), space carving (a
+ * source seeing farther than (1 + carving_threshold) x the point carves it),
+ * and a backward check (the source's point projects back within 2 px and
+ * the threshold).  Keep if consistent views (counting the reference) >=
+ * min(min_consistent_views, 1 + neighbours) and carved < max_carved_views.
+ * FP32 in the kernel's operation order; the source depth is sampled
+ * bilinearly with exact fractions.  Sources must have the reference's size.
+ * Defaults: threshold 0.01, 3 views, carving 0.2, 1 carved view.
+ * ---------------------------------------------------------------------- */
+typedef struct dn_gpu_cleaner dn_gpu_cleaner;
+dn_status dn_gpu_cleaner_create(dn_gpu_cleaner** out);
+dn_status dn_gpu_cleaner_destroy(dn_gpu_cleaner* c);
+dn_status dn_gpu_cleaner_set_same_depth_threshold(dn_gpu_cleaner* c, float t);
+dn_status dn_gpu_cleaner_set_min_consistent_views(dn_gpu_cleaner* c, int n);
+dn_status dn_gpu_cleaner_set_carving_threshold(dn_gpu_cleaner* c, float t);
+dn_status dn_gpu_cleaner_set_max_carved_views(dn_gpu_cleaner* c, int n);
+/* AddView (cleaner.cc:39-54): depth f32 [height][stride]; *id (may be NULL)
+ * receives the view index. */
+dn_status dn_gpu_cleaner_add_view(dn_gpu_cleaner* c, const double K[9], const double R[9],
+                                  const double t[3], const float* depth, int width, int height,
+                                  int stride, int* id);
+/* Clean (cleaner.cc:56-170): the cleaned depth of view `ref` against
+ * `neighbor_ids` into out (f32 [H][W] of the reference view).
+ * DN_OUT_OF_RANGE for an index out of range. */
+dn_status dn_gpu_cleaner_clean(dn_gpu_cleaner* c, int ref, const int* neighbor_ids, int n,
+                               float* out);
+/* Clear (cleaner.cc:172-184): removes every view. */
+dn_status dn_gpu_cleaner_clear(dn_gpu_cleaner* c);
 
 /* ----------------------------------------------------------------------
  * Depthmap files (host only, no GPU needed).  OpenSfM stores each view's

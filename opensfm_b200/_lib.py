@@ -15,7 +15,8 @@ ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "_build", "libdense_b200.so")
 HEADER = os.path.join(ROOT, "include", "dense_b200.h")
 
-DN_OK, DN_INVALID_ARG, DN_OUT_OF_MEMORY, DN_DEVICE_ERROR, DN_TIMEOUT, DN_NOT_READY = range(6)
+(DN_OK, DN_INVALID_ARG, DN_OUT_OF_MEMORY, DN_DEVICE_ERROR, DN_TIMEOUT, DN_NOT_READY,
+ DN_OUT_OF_RANGE) = range(7)
 DN_RUN_CLEAN, DN_RUN_PRUNE, DN_RUN_GRAPH, DN_RUN_INIT, DN_RUN_TIMING = 1, 2, 4, 8, 16
 
 _lib = None
@@ -100,6 +101,15 @@ _SIGNATURES = {
     "dn_nn_conv3x3_forward_mma_sync": ([_vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _i, _vp,
                                         _vp, _vp], _i),
     "dn_nn_synchronize": ([_vp], _i),
+    "dn_gpu_cleaner_create": ([ctypes.POINTER(_vp)], _i),
+    "dn_gpu_cleaner_destroy": ([_vp], _i),
+    "dn_gpu_cleaner_set_same_depth_threshold": ([_vp, ctypes.c_float], _i),
+    "dn_gpu_cleaner_set_min_consistent_views": ([_vp, _i], _i),
+    "dn_gpu_cleaner_set_carving_threshold": ([_vp, ctypes.c_float], _i),
+    "dn_gpu_cleaner_set_max_carved_views": ([_vp, _i], _i),
+    "dn_gpu_cleaner_add_view": ([_vp, _d, _d, _d, _f, _i, _i, _i, ctypes.POINTER(_i)], _i),
+    "dn_gpu_cleaner_clean": ([_vp, _i, _i32, _i, _f], _i),
+    "dn_gpu_cleaner_clear": ([_vp], _i),
     "dn_xxh32": ([_vp, ctypes.c_int64, ctypes.c_uint32], ctypes.c_uint32),
     "dn_lz4f_compress_bound": ([ctypes.c_int64], ctypes.c_int64),
     "dn_lz4f_compress": ([_vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
@@ -156,6 +166,8 @@ def check(status: int) -> None:
         raise ValueError(msg)
     if status == DN_OUT_OF_MEMORY:
         raise MemoryError(msg)
+    if status == DN_OUT_OF_RANGE:
+        raise IndexError(msg)
     raise DenseError(status, msg)
 
 

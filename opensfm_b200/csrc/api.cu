@@ -796,6 +796,25 @@ struct dn_cleaner {
   }
 };
 
+struct dn_gpu_cleaner {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  float thr = 0.01f;
+  int min_views = 3;
+  float carving = 0.2f;
+  int max_carved = 1;
+  struct V {
+    dn::GpuCleanCam cam;
+    int W, H;
+    DevBuf<float> depth;
+  };
+  std::vector<V> views;
+  DevBuf<float> d_out;
+  ~dn_gpu_cleaner() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
 struct dn_pruner {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -975,6 +994,117 @@ dn_status dn_estimator_last_taps(dn_estimator* est, uint64_t* taps) {
 }
 
 // ---------------------------------------------------------------- cleaner
+// ------------------------------------------------------- GPUDepthmapCleaner
+dn_status dn_gpu_cleaner_create(dn_gpu_cleaner** out) {
+  DN_CHECK(out, "NULL output");
+  *out = nullptr;
+  DN_TRY(need_device());
+  auto c = std::make_unique<dn_gpu_cleaner>();
+  DN_CUDA(cudaGetDevice(&c->device));
+  DN_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  *out = c.release();
+  return DN_OK;
+}
+dn_status dn_gpu_cleaner_destroy(dn_gpu_cleaner* c) {
+  delete c;
+  return DN_OK;
+}
+dn_status dn_gpu_cleaner_set_same_depth_threshold(dn_gpu_cleaner* c, float t) {
+  DN_CHECK(c, "NULL cleaner");
+  c->thr = t;
+  return DN_OK;
+}
+dn_status dn_gpu_cleaner_set_min_consistent_views(dn_gpu_cleaner* c, int n) {
+  DN_CHECK(c, "NULL cleaner");
+  c->min_views = n;
+  return DN_OK;
+}
+dn_status dn_gpu_cleaner_set_carving_threshold(dn_gpu_cleaner* c, float t) {
+  DN_CHECK(c, "NULL cleaner");
+  c->carving = std::max(0.0f, t);  // cleaner.cc:31-33
+  return DN_OK;
+}
+dn_status dn_gpu_cleaner_set_max_carved_views(dn_gpu_cleaner* c, int n) {
+  DN_CHECK(c, "NULL cleaner");
+  c->max_carved = std::max(0, n);  // cleaner.cc:35-37
+  return DN_OK;
+}
+dn_status dn_gpu_cleaner_add_view(dn_gpu_cleaner* c, const double* K, const double* R,
+                                  const double* t, const float* depth, int width, int height,
+                                  int stride, int* id) {
+  DN_CHECK(c, "NULL cleaner");
+  DN_TRY(check_camera(K, R, t));
+  DN_CHECK(depth, "depth must not be NULL");
+  DN_CHECK(width >= 2 && height >= 2 && width <= 16384 && height <= 16384, "bad depthmap size");
+  if (stride <= 0) stride = width;
+  DN_CHECK(stride >= width, "stride must be >= width");
+  DN_CUDA(cudaSetDevice(c->device));
+  dn_gpu_cleaner::V v;
+  DN_CUDA(v.depth.alloc((size_t)width * height));
+  DN_CUDA(cudaMemcpy2DAsync(v.depth.p, width * sizeof(float), depth, stride * sizeof(float),
+                            width * sizeof(float), height, cudaMemcpyHostToDevice, c->stream));
+  DN_CUDA(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 9; ++k) {
+    v.cam.K[k] = (float)K[k];  // opencl_utils.h:238-252 casts the camera to FP32
+    v.cam.R[k] = (float)R[k];
+  }
+  for (int k = 0; k < 3; ++k) v.cam.t[k] = (float)t[k];
+  v.W = width;
+  v.H = height;
+  c->views.push_back(std::move(v));
+  if (id) *id = (int)c->views.size() - 1;
+  return DN_OK;
+}
+dn_status dn_gpu_cleaner_clean(dn_gpu_cleaner* c, int ref, const int* neighbor_ids, int n,
+                               float* out) {
+  DN_CHECK(c && out, "NULL argument");
+  DN_CHECK(n >= 0 && (n == 0 || neighbor_ids), "NULL neighbour list");
+  const int nv = (int)c->views.size();
+  if (ref < 0 || ref >= nv) {
+    g_last_error = "Clean: ref_idx out of range";
+    return DN_OUT_OF_RANGE;
+  }
+  for (int k = 0; k < n; ++k)
+    if (neighbor_ids[k] < 0 || neighbor_ids[k] >= nv) {
+      g_last_error = "Clean: neighbor id out of range";
+      return DN_OUT_OF_RANGE;
+    }
+  const auto& r = c->views[ref];
+  const int n_src = std::min(n, dn::kMaxGpuCleanSources);
+  dn::GpuCleanArgs a{};
+  a.ref = r.depth.p;
+  a.W = r.W;
+  a.H = r.H;
+  a.cam[0] = r.cam;
+  for (int k = 0; k < n_src; ++k) {
+    const auto& o = c->views[neighbor_ids[k]];
+    // The reference resizes a source of another size to the reference's but
+    // keeps its intrinsics (cleaner.cc:115-134); only equal sizes are taken.
+    DN_CHECK(o.W == r.W && o.H == r.H, "every source depthmap must have the reference's size");
+    a.src[k] = o.depth.p;
+    a.cam[k + 1] = o.cam;
+  }
+  a.n_src = n_src;
+  a.same_depth_threshold = c->thr;
+  a.min_consistent = std::min(c->min_views, 1 + n);  // effective_min, cleaner.cc:148
+  a.carving_threshold = c->carving;
+  a.max_carved = c->max_carved;
+  DN_CUDA(cudaSetDevice(c->device));
+  const size_t npx = (size_t)r.W * r.H;
+  if (c->d_out.n < npx) DN_CUDA(c->d_out.alloc(npx));
+  DN_CUDA(dn::launch_gpu_clean(a, c->d_out.p, c->stream));
+  DN_CUDA(cudaMemcpyAsync(out, c->d_out.p, npx * sizeof(float), cudaMemcpyDeviceToHost,
+                          c->stream));
+  DN_CUDA(cudaStreamSynchronize(c->stream));
+  return DN_OK;
+}
+dn_status dn_gpu_cleaner_clear(dn_gpu_cleaner* c) {
+  DN_CHECK(c, "NULL cleaner");
+  c->views.clear();
+  c->d_out.release();
+  return DN_OK;
+}
+
 dn_status dn_cleaner_create(dn_cleaner** out) {
   DN_CHECK(out, "NULL output");
   *out = nullptr;

@@ -139,6 +139,98 @@ cudaError_t launch_clean(const CleanView* d_views, int ref, const int* d_others,
 }
 
 // ----------------------------------------------------------------------
+// GPUDepthmapCleaner::Clean (cleaner.cc:56-170; kernel acmmp_clean_depthmap,
+// opencl_kernels.h:2155-2273).  Per pixel with depth > 0: back-project with
+// the reference camera, project into each source; a source whose depth at
+// that point is farther than (1 + carving) x the point's depth carves it;
+// one within the relative threshold whose own point projects back within
+// 2 px (L1) and the threshold of the reference depth counts as consistent.
+// Keep if consistent (starting at 1) >= min_consistent and carved <
+// max_carved.  All arithmetic is FP32 in the kernel's order with each
+// operation rounded (no contraction); the source depth is sampled bilinearly
+// with exact fractions (the reference asks the texture unit for a linear
+// filter at the texel centre, the same interpolant).
+struct Vec3f {
+  float x, y, z;
+};
+
+// R^T p for row-major R (the kernel's camera-to-world rotation).
+__device__ inline Vec3f rot_t(const float* R, float x, float y, float z) {
+  return {__fadd_rn(__fadd_rn(__fmul_rn(R[0], x), __fmul_rn(R[3], y)), __fmul_rn(R[6], z)),
+          __fadd_rn(__fadd_rn(__fmul_rn(R[1], x), __fmul_rn(R[4], y)), __fmul_rn(R[7], z)),
+          __fadd_rn(__fadd_rn(__fmul_rn(R[2], x), __fmul_rn(R[5], y)), __fmul_rn(R[8], z))};
+}
+// R p + t.
+__device__ inline Vec3f rot_add(const float* R, const float* t, Vec3f p) {
+  return {__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(R[0], p.x), __fmul_rn(R[1], p.y)),
+                              __fmul_rn(R[2], p.z)), t[0]),
+          __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(R[3], p.x), __fmul_rn(R[4], p.y)),
+                              __fmul_rn(R[5], p.z)), t[1]),
+          __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(R[6], p.x), __fmul_rn(R[7], p.y)),
+                              __fmul_rn(R[8], p.z)), t[2])};
+}
+// World point of pixel (u, v) at depth d: R^T ((u - cx) / fx * d - t, ...).
+__device__ inline Vec3f backproject_px(const GpuCleanCam& c, float u, float v, float d) {
+  const float cam_x = __fmul_rn(__fdiv_rn(__fsub_rn(u, c.K[2]), c.K[0]), d);
+  const float cam_y = __fmul_rn(__fdiv_rn(__fsub_rn(v, c.K[5]), c.K[4]), d);
+  return rot_t(c.R, __fsub_rn(cam_x, c.t[0]), __fsub_rn(cam_y, c.t[1]), __fsub_rn(d, c.t[2]));
+}
+
+__device__ inline float bilinear_exact(const float* d, int W, float u, float v) {
+  const int ix = (int)u, iy = (int)v;  // u, v >= 0 here
+  const float fx = __fsub_rn(u, (float)ix), fy = __fsub_rn(v, (float)iy);
+  const float gx = __fsub_rn(1.0f, fx), gy = __fsub_rn(1.0f, fy);
+  const float* p = d + (size_t)iy * W + ix;
+  const float top = __fadd_rn(__fmul_rn(gx, p[0]), __fmul_rn(fx, p[1]));
+  const float bot = __fadd_rn(__fmul_rn(gx, p[W]), __fmul_rn(fx, p[W + 1]));
+  return __fadd_rn(__fmul_rn(gy, top), __fmul_rn(fy, bot));
+}
+
+__global__ void gpu_clean_kernel(const __grid_constant__ GpuCleanArgs a, float* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= a.W || y >= a.H) return;
+  const size_t idx = (size_t)y * a.W + x;
+  const float d = a.ref[idx];
+  if (!(d > 0.0f)) {
+    out[idx] = 0.0f;
+    return;
+  }
+  const GpuCleanCam& rc = a.cam[0];
+  const Vec3f w = backproject_px(rc, (float)x, (float)y, d);
+  int consistent = 1, carved = 0;
+  for (int v = 0; v < a.n_src; ++v) {
+    const GpuCleanCam& sc = a.cam[v + 1];
+    const Vec3f s = rot_add(sc.R, sc.t, w);
+    if (s.z <= 1e-6f) continue;
+    const float su = __fadd_rn(__fdiv_rn(__fmul_rn(sc.K[0], s.x), s.z), sc.K[2]);
+    const float sv = __fadd_rn(__fdiv_rn(__fmul_rn(sc.K[4], s.y), s.z), sc.K[5]);
+    if (su < 0.0f || sv < 0.0f || su >= (float)(a.W - 1) || sv >= (float)(a.H - 1)) continue;
+    const float sd = bilinear_exact(a.src[v], a.W, su, sv);
+    if (!(sd > 0.0f)) continue;
+    if (sd > __fmul_rn(s.z, __fadd_rn(1.0f, a.carving_threshold))) {
+      ++carved;
+      continue;
+    }
+    if (fabsf(__fsub_rn(sd, s.z)) >= __fmul_rn(s.z, a.same_depth_threshold)) continue;
+    const Vec3f w2 = backproject_px(sc, su, sv, sd);
+    const Vec3f r = rot_add(rc.R, rc.t, w2);
+    if (r.z <= 1e-6f) continue;
+    const float ru = __fadd_rn(__fdiv_rn(__fmul_rn(rc.K[0], r.x), r.z), rc.K[2]);
+    const float rv = __fadd_rn(__fdiv_rn(__fmul_rn(rc.K[4], r.y), r.z), rc.K[5]);
+    if (__fadd_rn(fabsf(__fsub_rn(ru, (float)x)), fabsf(__fsub_rn(rv, (float)y))) > 2.0f) continue;
+    if (fabsf(__fsub_rn(r.z, d)) >= __fmul_rn(d, a.same_depth_threshold)) continue;
+    ++consistent;
+  }
+  out[idx] = (consistent >= a.min_consistent && carved < a.max_carved) ? d : 0.0f;
+}
+
+cudaError_t launch_gpu_clean(const GpuCleanArgs& a, float* out, cudaStream_t s) {
+  const dim3 blk(32, 8), grid((a.W + 31) / 32, (a.H + 7) / 8);
+  gpu_clean_kernel<<<grid, blk, 0, s>>>(a, out);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------
 // Pruner.
 
 // cv::normalize(Vec3f): multiply by 1 / ||v|| (norm in double).

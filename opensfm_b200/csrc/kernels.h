@@ -88,6 +88,23 @@ struct PruneOut {
 // Cleans map `ref` against views others[0..n) (DepthmapCleaner::Clean).
 cudaError_t launch_clean(const CleanView* d_views, int ref, const int* d_others, int n_others,
                          int W, int H, float thr, int min_views, float* out, cudaStream_t s);
+// GPUDepthmapCleaner::Clean (cleaner.cc:56-170): forward and backward
+// consistency with space carving, FP32, every source the reference's size.
+constexpr int kMaxGpuCleanSources = 16;
+struct GpuCleanCam {
+  float K[9], R[9], t[3];
+};
+struct GpuCleanArgs {
+  const float* ref;                           // [H][W]
+  const float* src[kMaxGpuCleanSources];      // [H][W] each
+  GpuCleanCam cam[kMaxGpuCleanSources + 1];   // reference first
+  int W, H, n_src;
+  float same_depth_threshold;
+  int min_consistent;
+  float carving_threshold;
+  int max_carved;
+};
+cudaError_t launch_gpu_clean(const GpuCleanArgs& a, float* out, cudaStream_t s);
 // Pruner in three kernels: keep flags + per-block counts, block-count scan,
 // ordered compaction.  `scratch` holds ceil(W*H/1024) + 1 uint32 counts and
 // W*H keep bytes (see prune_scratch_bytes).

@@ -209,6 +209,68 @@ class DepthmapCleaner(_Handle):
         return out
 
 
+class GPUDepthmapCleaner(_Handle):
+    """``dense::GPUDepthmapCleaner`` (``cleaner.h:16-60``, ``pydense.pyi:129-149``)
+    on the B200: forward and backward consistency with space carving."""
+
+    def __init__(self) -> None:
+        super().__init__("dn_gpu_cleaner_create", "dn_gpu_cleaner_destroy")
+        self._shapes = []
+
+    @staticmethod
+    def is_available() -> bool:
+        try:
+            return _lib.load().dn_device_count() > 0
+        except OSError:
+            return False
+
+    def set_same_depth_threshold(self, t: float) -> None:
+        check(self._L.dn_gpu_cleaner_set_same_depth_threshold(self._h, float(t)))
+
+    def set_min_consistent_views(self, n: int) -> None:
+        check(self._L.dn_gpu_cleaner_set_min_consistent_views(self._h, int(n)))
+
+    def set_carving_threshold(self, t: float) -> None:
+        check(self._L.dn_gpu_cleaner_set_carving_threshold(self._h, float(t)))
+
+    def set_max_carved_views(self, n: int) -> None:
+        check(self._L.dn_gpu_cleaner_set_max_carved_views(self._h, int(n)))
+
+    def set_device(self, device: int) -> None:
+        """Views added after this call live on `device` (the reference binds
+        one OpenCL device per cleaner)."""
+        if self._shapes:
+            raise ValueError("set_device must come before the first add_view")
+        check(self._L.dn_set_device(int(device)))
+        self.close()
+        super().__init__("dn_gpu_cleaner_create", "dn_gpu_cleaner_destroy")
+
+    def add_view(self, K, R, t, depth) -> None:
+        K = _mat(K, (3, 3), "K")
+        R = _mat(R, (3, 3), "R")
+        t = _mat(t, (3,), "t")
+        d = np.ascontiguousarray(depth, dtype=np.float32)
+        if d.ndim != 2:
+            raise ValueError("depth must be a 2-D array")
+        H, W = d.shape
+        check(self._L.dn_gpu_cleaner_add_view(self._h, ptr(K, _d), ptr(R, _d), ptr(t, _d),
+                                              ptr(d, _f), W, H, W, None))
+        self._shapes.append((H, W))
+
+    def clean(self, ref_idx: int, neighbor_ids) -> np.ndarray:
+        ids = np.ascontiguousarray(np.asarray(neighbor_ids).reshape(-1), dtype=np.int32)
+        if not 0 <= int(ref_idx) < len(self._shapes):
+            raise IndexError(f"Clean: ref_idx {ref_idx} out of range [0, {len(self._shapes)})")
+        out = np.zeros(self._shapes[int(ref_idx)], np.float32)
+        check(self._L.dn_gpu_cleaner_clean(self._h, int(ref_idx), ptr(ids, _i32), len(ids),
+                                           ptr(out, _f)))
+        return out
+
+    def clear(self) -> None:
+        check(self._L.dn_gpu_cleaner_clear(self._h))
+        self._shapes = []
+
+
 class DepthmapPruner(_Handle):
     """``dense::DepthmapPruner`` (``depthmap.h:131-153``) on the B200."""
 

@@ -428,3 +428,80 @@ def ncc_fp64(Ks, Rs, ts, images, planes, patch_size=7, pixels=None, margins=Fals
         vm[interior] = var_m
         return score, nghbr, em, vm
     return score, nghbr
+
+def gpu_clean_fp32(Ks, Rs, ts, depths, ref, neighbor_ids, same_depth_threshold=0.01,
+                   min_consistent_views=3, carving_threshold=0.2, max_carved_views=1):
+    """GPUDepthmapCleaner::Clean restated in numpy FP32 (kernel
+    acmmp_clean_depthmap, opencl_kernels.h:2155-2273; host cleaner.cc:56-170).
+
+    Every operation is an FP32 operation in the kernel's order, rounded by
+    itself; the source depth is sampled bilinearly with exact fractions.
+    Sources must have the reference's size.  This restates the OpenCL
+    kernel source: the reference cannot run it here (no OpenCL).
+    """
+    f32 = np.float32
+    K = [np.asarray(k, np.float64).astype(f32).ravel() for k in Ks]
+    R = [np.asarray(r, np.float64).astype(f32).ravel() for r in Rs]
+    t = [np.asarray(x, np.float64).astype(f32).ravel() for x in ts]
+    D = [np.asarray(d, f32) for d in depths]
+    H, W = D[ref].shape
+    ids = list(neighbor_ids)[:16]
+    carving = f32(max(0.0, carving_threshold))
+    max_carved = max(0, int(max_carved_views))
+    eff_min = min(int(min_consistent_views), 1 + len(list(neighbor_ids)))
+    thr = f32(same_depth_threshold)
+    yy, xx = np.mgrid[0:H, 0:W]
+    xf, yf = xx.astype(f32), yy.astype(f32)
+    d = D[ref]
+    valid = d > f32(0)
+
+    def rot_t(Rm, x, y, z):
+        return ((Rm[0] * x + Rm[3] * y) + Rm[6] * z, (Rm[1] * x + Rm[4] * y) + Rm[7] * z,
+                (Rm[2] * x + Rm[5] * y) + Rm[8] * z)
+
+    def rot_add(Rm, tv, p):
+        x, y, z = p
+        return (((Rm[0] * x + Rm[1] * y) + Rm[2] * z) + tv[0],
+                ((Rm[3] * x + Rm[4] * y) + Rm[5] * z) + tv[1],
+                ((Rm[6] * x + Rm[7] * y) + Rm[8] * z) + tv[2])
+
+    def backproject(Kv, Rv, tv, u, v, dd):
+        cx = (u - Kv[2]) / Kv[0] * dd
+        cy = (v - Kv[5]) / Kv[4] * dd
+        return rot_t(Rv, cx - tv[0], cy - tv[1], dd - tv[2])
+
+    with np.errstate(all="ignore"):
+        w = backproject(K[ref], R[ref], t[ref], xf, yf, d)
+        consistent = np.ones((H, W), np.int32)
+        carved = np.zeros((H, W), np.int32)
+        for o in ids:
+            sx, sy, sz = rot_add(R[o], t[o], w)
+            ok = valid & (sz > f32(1e-6))
+            su = (K[o][0] * sx) / sz + K[o][2]
+            sv = (K[o][4] * sy) / sz + K[o][5]
+            ok &= ~((su < f32(0)) | (sv < f32(0)) | (su >= f32(W - 1)) | (sv >= f32(H - 1)))
+            ix = np.where(ok, su, f32(0)).astype(np.int64)
+            iy = np.where(ok, sv, f32(0)).astype(np.int64)
+            fx = np.where(ok, su, f32(0)) - ix.astype(f32)
+            fy = np.where(ok, sv, f32(0)) - iy.astype(f32)
+            gx, gy = f32(1) - fx, f32(1) - fy
+            src = D[o]
+            ix1, iy1 = np.minimum(ix + 1, W - 1), np.minimum(iy + 1, H - 1)
+            top = gx * src[iy, ix] + fx * src[iy, ix1]
+            bot = gx * src[iy1, ix] + fx * src[iy1, ix1]
+            sd = gy * top + fy * bot
+            ok &= sd > f32(0)
+            carve = ok & (sd > sz * (f32(1) + carving))
+            carved += carve
+            ok &= ~carve
+            ok &= ~(np.abs(sd - sz) >= sz * thr)
+            w2 = backproject(K[o], R[o], t[o], su, sv, sd)
+            rx, ry, rz = rot_add(R[ref], t[ref], w2)
+            ok &= rz > f32(1e-6)
+            ru = (K[ref][0] * rx) / rz + K[ref][2]
+            rv = (K[ref][4] * ry) / rz + K[ref][5]
+            ok &= ~((np.abs(ru - xf) + np.abs(rv - yf)) > f32(2))
+            ok &= ~(np.abs(rz - d) >= d * thr)
+            consistent += ok
+    keep = valid & (consistent >= eff_min) & (carved < max_carved)
+    return np.where(keep, d, f32(0)).astype(f32)

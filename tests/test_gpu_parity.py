@@ -395,6 +395,44 @@ def test_pruner_bit_identical(golden):
     assert np.array_equal(lab, g["prune_labels"])
 
 
+@pytest.mark.parametrize("thr,min_views,carving,max_carved",
+                         [(0.01, 3, 0.2, 1), (0.02, 2, 0.1, 2), (0.005, 1, 0.0, 0)])
+def test_gpu_cleaner_bit_identical_to_fp32_oracle(golden, scene, thr, min_views, carving,
+                                                  max_carved):
+    """GPUDepthmapCleaner (forward + backward check, space carving) against
+    its FP32 restatement, on the pruner fixture and on noisy ray-cast depths."""
+    cases = []
+    g = golden("clean_prune_64x48_v4.npz")
+    cases.append((list(g["K"]), list(g["R"]), list(g["t"]), list(g["depths"])))
+    Ks, Rs, ts = cams(scene)
+    rng = np.random.default_rng(5)
+    noisy = []
+    for d in scene.depths:
+        n = (d * (1 + 0.003 * rng.standard_normal(d.shape))).astype(np.float32)
+        n[rng.random(d.shape) < 0.05] = 0
+        n[rng.random(d.shape) < 0.02] *= 0.7  # floaters in front
+        noisy.append(n)
+    cases.append((Ks, Rs, ts, noisy))
+    for K, R, t, D in cases:
+        c = pydense.GPUDepthmapCleaner()
+        c.set_same_depth_threshold(thr)
+        c.set_min_consistent_views(min_views)
+        c.set_carving_threshold(carving)
+        c.set_max_carved_views(max_carved)
+        for k in range(len(D)):
+            c.add_view(K[k], R[k], t[k], D[k])
+        for ref in range(len(D)):
+            nb = [o for o in range(len(D)) if o != ref]
+            got = c.clean(ref, np.array(nb))
+            want = O.gpu_clean_fp32(K, R, t, D, ref, nb, thr, min_views, carving, max_carved)
+            assert np.array_equal(got, want)
+        with pytest.raises(IndexError):
+            c.clean(len(D), np.array([0]))
+        with pytest.raises(IndexError):
+            c.clean(0, np.array([len(D)]))
+        c.clear()
+
+
 def test_invalid_arguments_raise(scene):
     e = pydense.DepthmapEstimator()
     with pytest.raises(ValueError):

@@ -233,3 +233,23 @@ def test_kat_plane_depth_round_trip():
     p = g["bf_plane"]
     m = d > 0
     assert np.allclose(-1.0 / p[m][:, 2], d[m], rtol=1e-6)
+
+
+def test_gpu_cleaner_oracle_known_answers():
+    """GPUDepthmapCleaner restatement: a view against itself is consistent
+    everywhere; a neighbour that sees farther everywhere carves every point;
+    one that sees nearer (an occluder) neither confirms nor carves."""
+    vs = S.ring_viewset(3, 2, 48, 36)
+    Ks, Rs, ts = cams(vs)
+    d = vs.depths[0].astype(np.float32)
+    same = O.gpu_clean_fp32([Ks[0]] * 2, [Rs[0]] * 2, [ts[0]] * 2, [d, d], 0, [1],
+                            0.01, 2, 0.2, 1)
+    inner = np.zeros_like(d, bool)
+    inner[1:-2, 1:-2] = True
+    assert np.array_equal(same[inner], d[inner])
+    far = O.gpu_clean_fp32([Ks[0]] * 2, [Rs[0]] * 2, [ts[0]] * 2, [d, d * 1.5], 0, [1],
+                           0.01, 1, 0.2, 1)
+    assert not far[inner].any()
+    near = O.gpu_clean_fp32([Ks[0]] * 2, [Rs[0]] * 2, [ts[0]] * 2, [d, d * 0.5], 0, [1],
+                            0.01, 1, 0.2, 1)
+    assert np.array_equal(near, d)
