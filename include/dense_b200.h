@@ -370,6 +370,42 @@ dn_status dn_gpu_cleaner_clean(dn_gpu_cleaner* c, int ref, const int* neighbor_i
 dn_status dn_gpu_cleaner_clear(dn_gpu_cleaner* c);
 
 /* ----------------------------------------------------------------------
+ * DepthmapFuser (fuser.h:28-77, fuser.cc:35-372): per-pixel fusion of
+ * depthmaps into points, the reference's single-thread order (primary views
+ * in order, pixels in raster order, fused pixels marking themselves and the
+ * source pixels they used).  The candidate observations of every pixel are
+ * computed on the GPU, the marks and medians on the host.  FP32 in the
+ * reference's expression order.  The statistical outlier removal
+ * (fuser.cc:374-482) is not built: knn must be 0.  Defaults: 3 consistent
+ * observations, 2 px, 0.01, 10 degrees, border 5, behind factor 0.3.
+ * ---------------------------------------------------------------------- */
+typedef struct dn_fuser dn_fuser;
+dn_status dn_fuser_create(dn_fuser** out);
+dn_status dn_fuser_destroy(dn_fuser* f);
+dn_status dn_fuser_set_min_num_consistent(dn_fuser* f, int n);
+dn_status dn_fuser_set_max_reproj_error(dn_fuser* f, float px);
+dn_status dn_fuser_set_max_depth_error(dn_fuser* f, float ratio);
+dn_status dn_fuser_set_max_normal_error(dn_fuser* f, float degrees);
+dn_status dn_fuser_set_border_margin(dn_fuser* f, int px);
+dn_status dn_fuser_set_sor_params(dn_fuser* f, int knn, float stddev_factor);
+dn_status dn_fuser_set_behind_depth_factor(dn_fuser* f, float factor);
+/* AddView (fuser.cc:82-97): depth f32 [H][W], normal f32 [H][W][3] (camera
+ * frame), color u8 [H][W][3], mask u8 [H][W] or NULL (0 = invalid), the
+ * indices of the views to check against, and whether the view is fused. */
+dn_status dn_fuser_add_view(dn_fuser* f, const double K[9], const double R[9], const double t[3],
+                            const float* depth, const float* normal, const uint8_t* color,
+                            const uint8_t* mask, int width, int height, const int* neighbor_ids,
+                            int n_neighbors, int primary);
+/* Fuse (fuser.cc:115-372): *count receives the number of fused points. */
+dn_status dn_fuser_fuse(dn_fuser* f, int64_t* count);
+/* The last fuse's points, unit normals (world frame) and colours, each
+ * `capacity` >= count rows of 3; any pointer may be NULL. */
+dn_status dn_fuser_get(dn_fuser* f, float* points, float* normals, uint8_t* colors,
+                       int64_t capacity);
+/* Message for the last failed dn_fuser_* call on this thread. */
+const char* dn_fuser_last_error(void);
+
+/* ----------------------------------------------------------------------
  * Depthmap files (host only, no GPU needed).  OpenSfM stores each view's
  * raw and cleaned depthmap as an .npz archive wrapped in one LZ4 frame
  * (opensfm/dataset.py:1080-1098 writes with lz4.frame.compress,

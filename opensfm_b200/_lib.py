@@ -110,6 +110,19 @@ _SIGNATURES = {
     "dn_gpu_cleaner_add_view": ([_vp, _d, _d, _d, _f, _i, _i, _i, ctypes.POINTER(_i)], _i),
     "dn_gpu_cleaner_clean": ([_vp, _i, _i32, _i, _f], _i),
     "dn_gpu_cleaner_clear": ([_vp], _i),
+    "dn_fuser_create": ([ctypes.POINTER(_vp)], _i),
+    "dn_fuser_destroy": ([_vp], _i),
+    "dn_fuser_set_min_num_consistent": ([_vp, _i], _i),
+    "dn_fuser_set_max_reproj_error": ([_vp, ctypes.c_float], _i),
+    "dn_fuser_set_max_depth_error": ([_vp, ctypes.c_float], _i),
+    "dn_fuser_set_max_normal_error": ([_vp, ctypes.c_float], _i),
+    "dn_fuser_set_border_margin": ([_vp, _i], _i),
+    "dn_fuser_set_sor_params": ([_vp, _i, ctypes.c_float], _i),
+    "dn_fuser_set_behind_depth_factor": ([_vp, ctypes.c_float], _i),
+    "dn_fuser_add_view": ([_vp, _d, _d, _d, _f, _f, _u8, _u8, _i, _i, _i32, _i, _i], _i),
+    "dn_fuser_fuse": ([_vp, ctypes.POINTER(ctypes.c_int64)], _i),
+    "dn_fuser_get": ([_vp, _f, _f, _u8, ctypes.c_int64], _i),
+    "dn_fuser_last_error": ([], ctypes.c_char_p),
     "dn_xxh32": ([_vp, ctypes.c_int64, ctypes.c_uint32], ctypes.c_uint32),
     "dn_lz4f_compress_bound": ([ctypes.c_int64], ctypes.c_int64),
     "dn_lz4f_compress": ([_vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],

@@ -271,6 +271,87 @@ class GPUDepthmapCleaner(_Handle):
         self._shapes = []
 
 
+class DepthmapFuser(_Handle):
+    """``dense::DepthmapFuser`` (``fuser.h:28-77``, ``pydense.pyi:80-102``):
+    per-pixel fusion into points; the candidate observations of every pixel
+    run on the B200, the raster-order marks and medians on the host."""
+
+    def __init__(self) -> None:
+        super().__init__("dn_fuser_create", "dn_fuser_destroy")
+        self._n_primary_px = 0
+
+    def _check(self, st: int) -> None:
+        if st == _lib.DN_OK:
+            return
+        msg = self._L.dn_fuser_last_error().decode(errors="replace")
+        if st == _lib.DN_INVALID_ARG:
+            raise ValueError(msg)
+        if st == _lib.DN_OUT_OF_MEMORY:
+            raise MemoryError(msg)
+        raise _lib.DenseError(st, msg)
+
+    def set_min_num_consistent(self, n: int) -> None:
+        self._check(self._L.dn_fuser_set_min_num_consistent(self._h, int(n)))
+
+    def set_max_reproj_error(self, px: float) -> None:
+        self._check(self._L.dn_fuser_set_max_reproj_error(self._h, float(px)))
+
+    def set_max_depth_error(self, ratio: float) -> None:
+        self._check(self._L.dn_fuser_set_max_depth_error(self._h, float(ratio)))
+
+    def set_max_normal_error(self, degrees: float) -> None:
+        self._check(self._L.dn_fuser_set_max_normal_error(self._h, float(degrees)))
+
+    def set_border_margin(self, px: int) -> None:
+        self._check(self._L.dn_fuser_set_border_margin(self._h, int(px)))
+
+    def set_num_threads(self, n: int) -> None:
+        """Accepted for compatibility: the result is the reference's
+        single-thread result whatever the count."""
+
+    def set_sor_params(self, knn: int, stddev_factor: float) -> None:
+        self._check(self._L.dn_fuser_set_sor_params(self._h, int(knn), float(stddev_factor)))
+
+    def set_behind_depth_factor(self, factor: float) -> None:
+        self._check(self._L.dn_fuser_set_behind_depth_factor(self._h, float(factor)))
+
+    def add_view(self, K, R, t, depth, normal, color, mask, neighbor_ids,
+                 primary: bool = True) -> None:
+        K = _mat(K, (3, 3), "K")
+        R = _mat(R, (3, 3), "R")
+        t = _mat(t, (3,), "t")
+        d = np.ascontiguousarray(depth, dtype=np.float32)
+        if d.ndim != 2:
+            raise ValueError("depth must be a 2-D array")
+        H, W = d.shape
+        n = np.ascontiguousarray(normal, dtype=np.float32)
+        c = np.ascontiguousarray(color, dtype=np.uint8)
+        if n.shape != (H, W, 3):
+            raise ValueError("depth and normal must have matching shapes.")
+        if c.shape != (H, W, 3):
+            raise ValueError("depth and color must have matching shapes.")
+        m = None
+        if mask is not None and np.asarray(mask).size:
+            m = np.ascontiguousarray(mask, dtype=np.uint8)
+            if m.shape != (H, W):
+                raise ValueError("mask must have the depth's shape")
+        nb = np.ascontiguousarray(np.asarray(neighbor_ids).reshape(-1), dtype=np.int32)
+        self._check(self._L.dn_fuser_add_view(
+            self._h, ptr(K, _d), ptr(R, _d), ptr(t, _d), ptr(d, _f), ptr(n, _f), ptr(c, _u8),
+            ptr(m, _u8) if m is not None else None, W, H, ptr(nb, _i32), int(nb.size),
+            int(bool(primary))))
+
+    def fuse(self) -> list:
+        cnt = ctypes.c_int64()
+        self._check(self._L.dn_fuser_fuse(self._h, ctypes.byref(cnt)))
+        n = int(cnt.value)
+        pts = np.zeros((n, 3), np.float32)
+        nrm = np.zeros((n, 3), np.float32)
+        clr = np.zeros((n, 3), np.uint8)
+        self._check(self._L.dn_fuser_get(self._h, ptr(pts, _f), ptr(nrm, _f), ptr(clr, _u8), n))
+        return [pts, nrm, clr]
+
+
 class DepthmapPruner(_Handle):
     """``dense::DepthmapPruner`` (``depthmap.h:131-153``) on the B200."""
 

@@ -505,3 +505,55 @@ def gpu_clean_fp32(Ks, Rs, ts, depths, ref, neighbor_ids, same_depth_threshold=0
             consistent += ok
     keep = valid & (consistent >= eff_min) & (carved < max_carved)
     return np.where(keep, d, f32(0)).astype(f32)
+
+
+class _FuseView(ctypes.Structure):
+    _fields_ = [("K", ctypes.c_void_p), ("R", ctypes.c_void_p), ("t", ctypes.c_void_p),
+                ("W", ctypes.c_int), ("H", ctypes.c_int), ("depth", ctypes.c_void_p),
+                ("normal", ctypes.c_void_p), ("color", ctypes.c_void_p),
+                ("mask", ctypes.c_void_p), ("nbrs", ctypes.c_void_p), ("n_nbrs", ctypes.c_int),
+                ("primary", ctypes.c_int)]
+
+
+def port_fuse(views, min_num_consistent=3, max_reproj_error=2.0, max_depth_error=0.01,
+              max_normal_error=10.0, border_margin=5, behind_depth_factor=0.3):
+    """DepthmapFuser::Fuse (fuser.cc:115-372, no outlier removal) in the C
+    restatement.  views: dicts with K, R, t, depth (H, W), normal (H, W, 3),
+    color (H, W, 3) uint8, mask (H, W) uint8 or None, neighbor_ids, primary.
+    Returns (points (N, 3) f32, normals (N, 3) f32, colors (N, 3) u8)."""
+    L = port()
+    if not hasattr(L, "_fuse_ready"):
+        L.or_fuse.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                              ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float,
+                              _f, _f, _u8, ctypes.c_long]
+        L.or_fuse.restype = ctypes.c_long
+        L._fuse_ready = True
+    keep = []
+    arr = (_FuseView * len(views))()
+    cap = 0
+    for k, v in enumerate(views):
+        K = np.ascontiguousarray(v["K"], np.float64)
+        R = np.ascontiguousarray(v["R"], np.float64)
+        t = np.ascontiguousarray(v["t"], np.float64).reshape(3)
+        d = np.ascontiguousarray(v["depth"], np.float32)
+        n = np.ascontiguousarray(v["normal"], np.float32)
+        c = np.ascontiguousarray(v["color"], np.uint8)
+        m = v.get("mask")
+        m = None if m is None else np.ascontiguousarray(m, np.uint8)
+        nb = np.ascontiguousarray(v["neighbor_ids"], np.int32).reshape(-1)
+        keep += [K, R, t, d, n, c, m, nb]
+        H, W = d.shape
+        arr[k] = _FuseView(K.ctypes.data, R.ctypes.data, t.ctypes.data, W, H, d.ctypes.data,
+                           n.ctypes.data, c.ctypes.data, None if m is None else m.ctypes.data,
+                           nb.ctypes.data if nb.size else None, int(nb.size),
+                           int(bool(v.get("primary", True))))
+        if v.get("primary", True):
+            cap += H * W
+    pts = np.zeros((max(cap, 1), 3), np.float32)
+    nrm = np.zeros((max(cap, 1), 3), np.float32)
+    clr = np.zeros((max(cap, 1), 3), np.uint8)
+    cnt = L.or_fuse(ctypes.cast(arr, ctypes.c_void_p), len(views), int(min_num_consistent),
+                    float(max_reproj_error), float(max_depth_error), float(max_normal_error),
+                    int(border_margin), float(behind_depth_factor), _P(pts, _f), _P(nrm, _f),
+                    _P(clr, _u8), cap)
+    return pts[:cnt].copy(), nrm[:cnt].copy(), clr[:cnt].copy()

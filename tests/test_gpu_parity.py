@@ -433,6 +433,54 @@ def test_gpu_cleaner_bit_identical_to_fp32_oracle(golden, scene, thr, min_views,
         c.clear()
 
 
+def test_fuser_bit_identical_to_oracle(scene):
+    """DepthmapFuser (GPU candidates, host raster marks and medians) against
+    its C restatement: noisy depths, normals of the true planes, a mask, each
+    view's neighbour list holding every view (itself too, as dense.py builds
+    it), and one non-primary view."""
+    Ks, Rs, ts = cams(scene)
+    rng = np.random.default_rng(9)
+    views = []
+    n_v = len(scene.images)
+    for k in range(n_v):
+        d = scene.depths[k]
+        H, W = d.shape
+        dn = (d * (1 + 0.002 * rng.standard_normal(d.shape))).astype(np.float32)
+        dn[rng.random(d.shape) < 0.03] = 0
+        nrm = np.zeros((H, W, 3), np.float32)
+        nrm[..., 2] = -1.0
+        nrm[..., :2] = 0.2 * rng.standard_normal((H, W, 2))
+        col = np.stack([scene.images[k], 255 - scene.images[k], scene.images[k] // 2], -1)
+        mask = np.ones((H, W), np.uint8)
+        mask[:, : W // 10] = 0
+        views.append(dict(K=Ks[k], R=Rs[k], t=ts[k], depth=dn, normal=nrm, color=col,
+                          mask=mask if k % 2 else None, neighbor_ids=list(range(n_v)),
+                          primary=(k != n_v - 1)))
+    for params in (dict(min_num_consistent=3, max_reproj_error=2.0, max_depth_error=0.01,
+                        max_normal_error=30.0, border_margin=5, behind_depth_factor=0.3),
+                   dict(min_num_consistent=2, max_reproj_error=1.0, max_depth_error=0.02,
+                        max_normal_error=60.0, border_margin=2, behind_depth_factor=1.0)):
+        want = O.port_fuse(views, **params)
+        f = pydense.DepthmapFuser()
+        f.set_min_num_consistent(params["min_num_consistent"])
+        f.set_max_reproj_error(params["max_reproj_error"])
+        f.set_max_depth_error(params["max_depth_error"])
+        f.set_max_normal_error(params["max_normal_error"])
+        f.set_border_margin(params["border_margin"])
+        f.set_behind_depth_factor(params["behind_depth_factor"])
+        f.set_sor_params(0, 2.5)
+        for v in views:
+            f.add_view(v["K"], v["R"], v["t"], v["depth"], v["normal"], v["color"], v["mask"],
+                       np.array(v["neighbor_ids"]), primary=v["primary"])
+        got = f.fuse()
+        print("fused points", len(got[0]), "oracle", len(want[0]))
+        assert len(want[0]) > 1000
+        for a, w in zip(got, want):
+            assert a.dtype == w.dtype and np.array_equal(a, w)
+    with pytest.raises(ValueError):
+        f.set_sor_params(12, 2.5)
+
+
 def test_invalid_arguments_raise(scene):
     e = pydense.DepthmapEstimator()
     with pytest.raises(ValueError):

@@ -253,3 +253,31 @@ def test_gpu_cleaner_oracle_known_answers():
     near = O.gpu_clean_fp32([Ks[0]] * 2, [Rs[0]] * 2, [ts[0]] * 2, [d, d * 0.5], 0, [1],
                             0.01, 1, 0.2, 1)
     assert np.array_equal(near, d)
+
+
+def test_fuser_oracle_known_answers():
+    """DepthmapFuser restatement: with two identical views each pixel of the
+    first fuses with its twin (2 observations, the point it back-projects
+    to), the twin's pixels are then used up, and asking for 3 observations
+    fuses nothing."""
+    vs = S.ring_viewset(3, 1, 40, 30)
+    c = vs.cameras[0]
+    d = vs.depths[0].astype(np.float32)
+    H, W = d.shape
+    n = np.zeros((H, W, 3), np.float32)
+    n[..., 2] = -1.0
+    col = np.stack([vs.images[0]] * 3, -1)
+    view = dict(K=c.K, R=c.R, t=c.t, depth=d, normal=n, color=col, mask=None)
+    views = [dict(view, neighbor_ids=[1]), dict(view, neighbor_ids=[0])]
+    pts, nrm, clr = O.port_fuse(views, min_num_consistent=2, border_margin=2)
+    inner = np.zeros((H, W), bool)
+    inner[2:-2, 2:-2] = True
+    assert len(pts) == int((inner & (d > 0)).sum())
+    ii, jj = np.nonzero(inner & (d > 0))
+    ray = np.stack([jj, ii, np.ones_like(jj)], -1) @ np.linalg.inv(c.K).T
+    world = (ray * d[ii, jj][:, None] - c.t) @ c.R
+    assert np.allclose(pts, world, rtol=1e-5, atol=1e-4)
+    assert np.array_equal(clr, col[ii, jj])
+    assert np.allclose(nrm, np.tile(-c.R[2], (len(pts), 1)), atol=1e-6)
+    none = O.port_fuse(views, min_num_consistent=3, border_margin=2)
+    assert len(none[0]) == 0
