@@ -115,6 +115,47 @@ def learned_leg(b, n_maps, shapes, steps, vs):
                         "same 3 iterations, cleaner and pruner"}
 
 
+def fusion_leg(b, vs, cands, n_maps, repeats=3, oracle=True):
+    """DepthmapFuser over the batch's cleaned depthmaps (normals from the
+    PatchMatch planes, grey colours, each view checked against itself and its
+    cleaner neighbours, as dense.py lists a cluster).  Times fuse() on the
+    host clock (GPU candidates + host marks and medians) and, with `oracle`,
+    the single-thread C restatement on the same views, and checks that the
+    two point clouds are identical."""
+    from opensfm_b200 import pydense
+
+    views = []
+    for v in range(n_maps):
+        depth, plane, score, nghbr, clean = b.get(v, clean=True)
+        img = vs.images[v]
+        c = vs.cameras[v]
+        views.append(dict(K=c.K, R=c.R, t=c.t, depth=clean, normal=plane,
+                          color=np.stack([img, img, img], -1), mask=None,
+                          neighbor_ids=sorted({v} | {o for o in cands[v] if o < n_maps}),
+                          primary=True))
+    f = pydense.DepthmapFuser()
+    for v in views:
+        f.add_view(v["K"], v["R"], v["t"], v["depth"], v["normal"], v["color"], None,
+                   np.array(v["neighbor_ids"]))
+    got = f.fuse()  # warm-up
+    ts = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        got = f.fuse()
+        ts.append(time.perf_counter() - t0)
+    out = {"points": int(len(got[0])), "fuse_s": float(np.median(ts)),
+           "views": n_maps, "neighbours_per_view": float(np.mean([len(v["neighbor_ids"])
+                                                                  for v in views]))}
+    if oracle:
+        import oracle as O
+
+        t0 = time.perf_counter()
+        want = O.port_fuse(views)
+        out["oracle_1thread_s"] = time.perf_counter() - t0
+        out["identical_to_oracle"] = bool(all(np.array_equal(a, w) for a, w in zip(got, want)))
+    return out
+
+
 # ------------------------------------------------------------------ clocks
 class Clocks:
     """Samples nvidia-smi clocks and throttle reasons during the timed region."""
@@ -338,10 +379,10 @@ def run_ours(args):
         from opensfm_b200 import autotune
 
         key = autotune.workload_key(shapes[:n_maps], [len(m) for m in matches[:n_maps]], PATCH)
-        cands = autotune.CANDIDATES
+        tune_cands = autotune.CANDIDATES
         if args.workload == "aerial":  # a step takes seconds: the two leading choices only
-            cands = [(32, 4, 2), (32, 4, 18)]
-        t = autotune.tune(b, key, {"prune": True, "graph": True}, candidates=cands)
+            tune_cands = [(32, 4, 2), (32, 4, 18)]
+        t = autotune.tune(b, key, {"prune": True, "graph": True}, candidates=tune_cands)
         tuning = {"choice": list(t["choice"]), "ms": t["ms"], "cached": t["cached"],
                   "source": "opensfm_b200.autotune"}
 
@@ -480,6 +521,8 @@ def run_ours(args):
     # cleaner launch and three pruner launches per map.
     pm_launches = 1 if (tuning and tuning["choice"][2] & 16) else (1 + 2 * ITERS + 1)
     line["gpu_launches"] = args.steps * (pm_launches + 4 * n_maps)
+    if args.fuse:
+        line["config"]["fusion"] = fusion_leg(b, vs, cands, n_maps)
     if args.learned:
         line["config"]["learned"] = learned_leg(b, n_maps, shapes, args.steps, vs)
     if rank == 0 and world == 1 and not args.no_cpu and ring:
@@ -538,6 +581,8 @@ def main():
     ap.add_argument("--workload", default="ring24", choices=WORKLOADS,
                     help="ring24 (640x480, the headline configuration), 64 mixed-size views "
                          "of the box or terrain scene, or the 256-view 1280x960 aerial block")
+    ap.add_argument("--fuse", action="store_true",
+                    help="also time DepthmapFuser on the cleaned maps against its C oracle")
     ap.add_argument("--learned", action="store_true",
                     help="also time the learned initialisation on the same batch")
     args = ap.parse_args()

@@ -19,6 +19,7 @@
 // reference.  The statistical outlier removal (fuser.cc:374-482) is not
 // built: set_sor_params accepts only knn = 0, its setting in OpenSfM's
 // dense pipeline (depthmap_fusion_sor_knn = 0).
+#include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -78,6 +79,16 @@ struct ViewDevF {
   const float* depth;    // [H][W]
   const float* normal;   // [H][W][3]
   const uint8_t* mask;   // [H][W] or null
+  const uint8_t* fused;  // [H][W] marks as of the start of the current view
+  const uint8_t* color;  // [H][W][3]
+};
+
+// One observation handed to the host: the reference pixel's own (view
+// slot -1, pix = its index) followed by its neighbours' (slot k, pix = the
+// source pixel), in raster order of the reference pixels.
+struct FuseRec {
+  int slot, pix;
+  float pt[3], nrm[3];
 };
 
 struct Params {
@@ -141,7 +152,8 @@ __global__ void fuse_candidates_kernel(const ViewDevF* __restrict__ views, int n
                                        const int* __restrict__ nbrs, int n_nbrs, Params p,
                                        uint8_t* __restrict__ ref_ok, float* __restrict__ ref_pt,
                                        float* __restrict__ ref_nrm, int* __restrict__ cand_pix,
-                                       float* __restrict__ cand_pt, float* __restrict__ cand_nrm) {
+                                       float* __restrict__ cand_pt, float* __restrict__ cand_nrm,
+                                       unsigned* __restrict__ n_rec) {
   const ViewDevF& ref = views[ri];
   const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y * blockDim.y + threadIdx.y;
   if (c >= ref.W || r >= ref.H) return;
@@ -149,6 +161,7 @@ __global__ void fuse_candidates_kernel(const ViewDevF* __restrict__ views, int n
   const int bm = p.border;
   bool ok = r >= bm && r < ref.H - bm && c >= bm && c < ref.W - bm;
   ok = ok && !(ref.mask && ref.mask[rp] == 0);
+  ok = ok && ref.fused[rp] == 0;  // fused by an earlier view: the host skips it
   const float rd = ref.depth[rp];
   ok = ok && rd > 0.0f;
   float rpt[3] = {0.f, 0.f, 0.f}, rnw[3] = {0.f, 0.f, 0.f};
@@ -165,6 +178,7 @@ __global__ void fuse_candidates_kernel(const ViewDevF* __restrict__ views, int n
     ref_pt[3 * rp + d] = rpt[d];
     ref_nrm[3 * rp + d] = rnw[d];
   }
+  unsigned recs = ok ? 1u : 0u;
   for (int k = 0; k < n_nbrs; ++k) {
     const size_t slot = rp * n_nbrs + k;
     int pix = -1;
@@ -180,7 +194,8 @@ __global__ void fuse_candidates_kernel(const ViewDevF* __restrict__ views, int n
           const int scol = (int)roundf(su), srow = (int)roundf(sv);
           if (scol >= bm && scol < src.W - bm && srow >= bm && srow < src.H - bm) {
             const size_t sp = (size_t)srow * src.W + scol;
-            if (!(src.mask && src.mask[sp] == 0)) {
+            // A source pixel marked before this view stays marked: drop it.
+            if (!(src.mask && src.mask[sp] == 0) && src.fused[sp] == 0) {
               float sd = bilinear_depth(src.depth, src.W, src.H, su, sv);
               if (sd <= 0.0f) sd = src.depth[sp];
               if (sd > 0.0f) {
@@ -215,12 +230,106 @@ __global__ void fuse_candidates_kernel(const ViewDevF* __restrict__ views, int n
       }
     }
     cand_pix[slot] = pix;
+    recs += pix >= 0 ? 1u : 0u;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       cand_pt[3 * slot + d] = spt[d];
       cand_nrm[3 * slot + d] = snw[d];
     }
   }
+  n_rec[rp] = recs;
+}
+
+// Packs each fusable pixel's own observation and its neighbours' into the
+// record stream at the pixel's exclusive-scan offset.
+__global__ void fuse_compact_kernel(int W, int H, int n_nbrs, const uint8_t* __restrict__ ref_ok,
+                                    const float* __restrict__ ref_pt,
+                                    const float* __restrict__ ref_nrm,
+                                    const int* __restrict__ cand_pix,
+                                    const float* __restrict__ cand_pt,
+                                    const float* __restrict__ cand_nrm,
+                                    const unsigned* __restrict__ offset,
+                                    FuseRec* __restrict__ out) {
+  const size_t rp = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (rp >= (size_t)W * H || !ref_ok[rp]) return;
+  FuseRec* o = out + offset[rp];
+  FuseRec r;
+  r.slot = -1;
+  r.pix = (int)rp;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    r.pt[d] = ref_pt[3 * rp + d];
+    r.nrm[d] = ref_nrm[3 * rp + d];
+  }
+  *o++ = r;
+  for (int k = 0; k < n_nbrs; ++k) {
+    const size_t slot = rp * n_nbrs + k;
+    if (cand_pix[slot] < 0) continue;
+    r.slot = k;
+    r.pix = cand_pix[slot];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      r.pt[d] = cand_pt[3 * slot + d];
+      r.nrm[d] = cand_nrm[3 * slot + d];
+    }
+    *o++ = r;
+  }
+}
+
+// VectorMedian (fuser.cc:23-31) is the value nth_element puts at n / 2: the
+// n/2-th smallest.  Picked here by rank, the first value in record order
+// with fewer than n/2 + 1 values below it and at least n/2 + 1 values at
+// or below it (the same value; only -0 and +0 could tell two picks apart).
+template <typename T, typename Get>
+__device__ inline T rank_median(int n, Get get) {
+  const int h = n / 2;
+  for (int a = 0; a < n; ++a) {
+    const T va = get(a);
+    int less = 0, le = 0;
+    for (int b = 0; b < n; ++b) {
+      const T vb = get(b);
+      less += vb < va;
+      le += !(va < vb);
+    }
+    if (less <= h && h < le) return va;
+  }
+  return get(h);  // only with NaN among the values
+}
+
+// One thread per fused point: the component-wise medians of its surviving
+// observations (fuser.cc:312-346), the normal renormalised when its length
+// exceeds 1e-6.  idx[start[i] .. start[i + 1]) lists the point's records,
+// its own first.
+__global__ void fuse_median_kernel(const FuseRec* __restrict__ rec,
+                                   const unsigned* __restrict__ start,
+                                   const unsigned* __restrict__ idx, int n_pts,
+                                   const ViewDevF* __restrict__ views, int ri,
+                                   const int* __restrict__ nbrs, float* __restrict__ out_pt,
+                                   float* __restrict__ out_nrm, uint8_t* __restrict__ out_clr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_pts) return;
+  const unsigned* ix = idx + start[i];
+  const int n = (int)(start[i + 1] - start[i]);
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d)
+    out_pt[3 * i + d] = rank_median<float>(n, [&](int a) { return rec[ix[a]].pt[d]; });
+  float mn[3];
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d)
+    mn[d] = rank_median<float>(n, [&](int a) { return rec[ix[a]].nrm[d]; });
+  const float ml = __fsqrt_rn(
+      __fadd_rn(__fadd_rn(__fmul_rn(mn[0], mn[0]), __fmul_rn(mn[1], mn[1])), __fmul_rn(mn[2], mn[2])));
+  if (ml > 1e-6f)
+    for (int d = 0; d < 3; ++d) mn[d] = __fdiv_rn(mn[d], ml);
+  for (int d = 0; d < 3; ++d) out_nrm[3 * i + d] = mn[d];
+  auto color_of = [&](int a, int d) -> uint8_t {
+    const FuseRec& r = rec[ix[a]];
+    const int v = r.slot < 0 ? ri : nbrs[r.slot];
+    return views[v].color[3 * (size_t)r.pix + d];
+  };
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d)
+    out_clr[3 * i + d] = rank_median<uint8_t>(n, [&](int a) { return color_of(a, d); });
 }
 
 // ------------------------------------------------------------------ host
@@ -270,19 +379,12 @@ struct HBuf {  // pinned host buffer
 struct FView {
   FCam cam;
   int W = 0, H = 0;
-  std::vector<uint8_t> color;  // [H][W][3], host: colours are read by the host pass
   std::vector<int> nbrs;
   bool primary = true;
   bool has_mask = false;
   DBuf<float> depth, normal;
-  DBuf<uint8_t> mask;
+  DBuf<uint8_t> mask, color;
 };
-
-template <typename T>
-T nth_median(T* v, int n) {
-  std::nth_element(v, v + n / 2, v + n);
-  return v[n / 2];
-}
 
 }  // namespace
 
@@ -386,11 +488,12 @@ extern "C" dn_status dn_fuser_add_view(dn_fuser* f, const double* K, const doubl
   v->W = width;
   v->H = height;
   const size_t npx = (size_t)width * height;
-  v->color.assign(color, color + 3 * npx);
   v->nbrs.assign(neighbor_ids, neighbor_ids + n_neighbors);
   v->primary = primary != 0;
   FCUDA(v->depth.alloc(npx));
   FCUDA(v->normal.alloc(3 * npx));
+  FCUDA(v->color.alloc(3 * npx));
+  FCUDA(cudaMemcpyAsync(v->color.p, color, 3 * npx, cudaMemcpyHostToDevice, f->stream));
   FCUDA(cudaMemcpyAsync(v->depth.p, depth, npx * sizeof(float), cudaMemcpyHostToDevice, f->stream));
   FCUDA(cudaMemcpyAsync(v->normal.p, normal, 3 * npx * sizeof(float), cudaMemcpyHostToDevice,
                         f->stream));
@@ -422,11 +525,10 @@ extern "C" dn_status dn_fuser_fuse(dn_fuser* f, int64_t* count) {
     hv[i].depth = v.depth.p;
     hv[i].normal = v.normal.p;
     hv[i].mask = v.has_mask ? v.mask.p : nullptr;
+    hv[i].color = v.color.p;
   }
   DBuf<ViewDevF> d_views;
   FCUDA(d_views.alloc(nv));
-  FCUDA(cudaMemcpyAsync(d_views.p, hv.data(), nv * sizeof(ViewDevF), cudaMemcpyHostToDevice,
-                        f->stream));
   Params p;
   p.max_reproj_sq = f->max_reproj_error_sq;
   p.max_depth_error = f->max_depth_error;
@@ -434,20 +536,57 @@ extern "C" dn_status dn_fuser_fuse(dn_fuser* f, int64_t* count) {
   p.behind = f->behind;
   p.border = f->border;
 
-  std::vector<std::vector<uint8_t>> fused(nv);
-  for (int i = 0; i < nv; ++i) fused[i].assign((size_t)f->views[i]->W * f->views[i]->H, 0);
+  // Fused marks: host copy (pinned, written by the raster walk) and device
+  // copy (read by the candidate kernel), one byte per pixel of every view.
+  std::vector<size_t> moff(nv + 1, 0);
+  for (int i = 0; i < nv; ++i) moff[i + 1] = moff[i] + (size_t)f->views[i]->W * f->views[i]->H;
+  HBuf<uint8_t> h_marks;
+  DBuf<uint8_t> d_marks;
+  FCUDA(h_marks.alloc(moff[nv]));
+  FCUDA(d_marks.alloc(moff[nv]));
+  std::memset(h_marks.p, 0, moff[nv]);
+  FCUDA(cudaMemsetAsync(d_marks.p, 0, moff[nv], f->stream));
+  std::vector<uint8_t> dirty(nv, 0);
+  for (int i = 0; i < nv; ++i) hv[i].fused = d_marks.p + moff[i];
+  FCUDA(cudaMemcpyAsync(d_views.p, hv.data(), nv * sizeof(ViewDevF), cudaMemcpyHostToDevice,
+                        f->stream));
+
   DBuf<int> d_nbrs;
   DBuf<uint8_t> d_ok;
   DBuf<float> d_rpt, d_rnrm, d_cpt, d_cnrm;
   DBuf<int> d_cpix;
-  HBuf<uint8_t> h_ok;
-  HBuf<float> h_rpt, h_rnrm, h_cpt, h_cnrm;
-  HBuf<int> h_cpix;
-  int max_obs = 1;
-  for (int i = 0; i < nv; ++i) max_obs = std::max(max_obs, 1 + (int)f->views[i]->nbrs.size());
-  std::vector<float> comp(max_obs), pts(3 * max_obs), nrm(3 * max_obs);
-  std::vector<uint8_t> comp8(max_obs), clr(3 * max_obs);
-  std::vector<int> used_v(max_obs), used_p(max_obs);
+  DBuf<unsigned> d_nrec, d_off;
+  DBuf<FuseRec> d_rec;
+  DBuf<uint8_t> d_scan_tmp;
+  HBuf<FuseRec> h_rec;
+  HBuf<unsigned> h_tail;
+  FCUDA(h_tail.alloc(2));
+  // Sized once: the median kernel of one view may still read it when the
+  // next view's list is queued behind it.
+  size_t max_nn = 1;
+  for (int i = 0; i < nv; ++i) {
+    const FView& v = *f->views[i];
+    max_nn = std::max(max_nn, v.nbrs.size());
+    // Record counts and offsets are 32-bit.
+    FCHECK(!v.primary || (size_t)v.W * v.H * (1 + v.nbrs.size()) < (size_t(1) << 32),
+           "primary view too large for its neighbour count");
+  }
+  FCUDA(d_nbrs.alloc(max_nn));
+  // Per fused point of the current view: its records (start / idx), and the
+  // medians the GPU computes from them, staged for the host.
+  HBuf<unsigned> h_start, h_idx;
+  DBuf<unsigned> d_start, d_idx;
+  DBuf<float> d_vpt, d_vnrm;
+  DBuf<uint8_t> d_vclr;
+  HBuf<float> h_vpt, h_vnrm;
+  HBuf<uint8_t> h_vclr;
+  size_t staged = 0;  // points of the previous view in h_v*, not yet appended
+  auto append_staged = [&]() {
+    f->out_pts.insert(f->out_pts.end(), h_vpt.p, h_vpt.p + 3 * staged);
+    f->out_nrm.insert(f->out_nrm.end(), h_vnrm.p, h_vnrm.p + 3 * staged);
+    f->out_clr.insert(f->out_clr.end(), h_vclr.p, h_vclr.p + 3 * staged);
+    staged = 0;
+  };
 
   for (int ri = 0; ri < nv; ++ri) {
     const FView& ref = *f->views[ri];
@@ -455,7 +594,15 @@ extern "C" dn_status dn_fuser_fuse(dn_fuser* f, int64_t* count) {
     const int nn = (int)ref.nbrs.size();
     const size_t npx = (size_t)ref.W * ref.H;
     const size_t nslot = npx * (size_t)std::max(nn, 1);
-    FCUDA(d_nbrs.alloc(std::max(nn, 1)));
+    // Marks set by earlier views, for the views this one reads.
+    auto push_marks = [&](int v) -> cudaError_t {
+      if (v < 0 || v >= nv || !dirty[v]) return cudaSuccess;
+      dirty[v] = 0;
+      return cudaMemcpyAsync(d_marks.p + moff[v], h_marks.p + moff[v], moff[v + 1] - moff[v],
+                             cudaMemcpyHostToDevice, f->stream);
+    };
+    FCUDA(push_marks(ri));
+    for (int k = 0; k < nn; ++k) FCUDA(push_marks(ref.nbrs[k]));
     if (nn)
       FCUDA(cudaMemcpyAsync(d_nbrs.p, ref.nbrs.data(), nn * sizeof(int), cudaMemcpyHostToDevice,
                             f->stream));
@@ -465,83 +612,104 @@ extern "C" dn_status dn_fuser_fuse(dn_fuser* f, int64_t* count) {
     FCUDA(d_cpix.alloc(nslot));
     FCUDA(d_cpt.alloc(3 * nslot));
     FCUDA(d_cnrm.alloc(3 * nslot));
+    FCUDA(d_nrec.alloc(npx));
+    FCUDA(d_off.alloc(npx));
     const dim3 blk(32, 8), grid((ref.W + 31) / 32, (ref.H + 7) / 8);
     fuse_candidates_kernel<<<grid, blk, 0, f->stream>>>(d_views.p, nv, ri, d_nbrs.p, nn, p,
                                                         d_ok.p, d_rpt.p, d_rnrm.p, d_cpix.p,
-                                                        d_cpt.p, d_cnrm.p);
+                                                        d_cpt.p, d_cnrm.p, d_nrec.p);
     FCUDA(cudaGetLastError());
-    FCUDA(h_ok.alloc(npx));
-    FCUDA(h_rpt.alloc(3 * npx));
-    FCUDA(h_rnrm.alloc(3 * npx));
-    FCUDA(h_cpix.alloc(nslot));
-    FCUDA(h_cpt.alloc(3 * nslot));
-    FCUDA(h_cnrm.alloc(3 * nslot));
-    FCUDA(cudaMemcpyAsync(h_ok.p, d_ok.p, npx, cudaMemcpyDeviceToHost, f->stream));
-    FCUDA(cudaMemcpyAsync(h_rpt.p, d_rpt.p, 3 * npx * sizeof(float), cudaMemcpyDeviceToHost,
+    // Record offsets: exclusive scan of the per-pixel record counts.
+    size_t tmp_bytes = 0;
+    FCUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_nrec.p, d_off.p, (int)npx,
+                                        f->stream));
+    FCUDA(d_scan_tmp.alloc(std::max<size_t>(tmp_bytes, 1)));
+    FCUDA(cub::DeviceScan::ExclusiveSum(d_scan_tmp.p, tmp_bytes, d_nrec.p, d_off.p, (int)npx,
+                                        f->stream));
+    FCUDA(cudaMemcpyAsync(h_tail.p, d_off.p + npx - 1, sizeof(unsigned), cudaMemcpyDeviceToHost,
                           f->stream));
-    FCUDA(cudaMemcpyAsync(h_rnrm.p, d_rnrm.p, 3 * npx * sizeof(float), cudaMemcpyDeviceToHost,
+    FCUDA(cudaMemcpyAsync(h_tail.p + 1, d_nrec.p + npx - 1, sizeof(unsigned),
+                          cudaMemcpyDeviceToHost, f->stream));
+    FCUDA(cudaStreamSynchronize(f->stream));
+    append_staged();  // the previous view's medians arrived before the tail
+    const size_t n_rec = (size_t)h_tail.p[0] + h_tail.p[1];
+    if (!n_rec) continue;
+    FCUDA(d_rec.alloc(n_rec));
+    FCUDA(h_rec.alloc(n_rec));
+    FCUDA(h_idx.alloc(n_rec));
+    FCUDA(h_start.alloc(n_rec + 1));
+    fuse_compact_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, f->stream>>>(
+        ref.W, ref.H, nn, d_ok.p, d_rpt.p, d_rnrm.p, d_cpix.p, d_cpt.p, d_cnrm.p, d_off.p,
+        d_rec.p);
+    FCUDA(cudaGetLastError());
+    FCUDA(cudaMemcpyAsync(h_rec.p, d_rec.p, n_rec * sizeof(FuseRec), cudaMemcpyDeviceToHost,
                           f->stream));
-    if (nn) {
-      FCUDA(cudaMemcpyAsync(h_cpix.p, d_cpix.p, npx * nn * sizeof(int), cudaMemcpyDeviceToHost,
-                            f->stream));
-      FCUDA(cudaMemcpyAsync(h_cpt.p, d_cpt.p, 3 * npx * nn * sizeof(float),
-                            cudaMemcpyDeviceToHost, f->stream));
-      FCUDA(cudaMemcpyAsync(h_cnrm.p, d_cnrm.p, 3 * npx * nn * sizeof(float),
-                            cudaMemcpyDeviceToHost, f->stream));
-    }
     FCUDA(cudaStreamSynchronize(f->stream));
 
-    // The reference's raster walk: marks, then medians (fuser.cc:163-355).
-    std::vector<uint8_t>& rf = fused[ri];
-    for (size_t rp = 0; rp < npx; ++rp) {
-      if (rf[rp] || !h_ok.p[rp]) continue;
-      int n_obs = 1, n_used = 0;
-      for (int d = 0; d < 3; ++d) {
-        pts[d] = h_rpt.p[3 * rp + d];
-        nrm[d] = h_rnrm.p[3 * rp + d];
-        clr[d] = ref.color[3 * rp + d];
+    // The reference's raster walk over the records (fuser.cc:163-355): a
+    // pixel's own record (slot -1) opens its run; a pixel or source pixel
+    // marked earlier is skipped; a pixel with enough observations is fused
+    // and marks itself and the source pixels it used.
+    uint8_t* rf = h_marks.p + moff[ri];
+    size_t q = 0, n_idx = 0;
+    size_t n_pts = 0;
+    while (q < n_rec) {
+      const size_t own = q++;
+      const size_t rp = (size_t)h_rec.p[own].pix;
+      size_t q_end = q;
+      while (q_end < n_rec && h_rec.p[q_end].slot >= 0) ++q_end;
+      if (rf[rp]) {
+        q = q_end;
+        continue;
       }
-      for (int k = 0; k < nn; ++k) {
-        const size_t slot = rp * nn + k;
-        const int sp = h_cpix.p[slot];
-        if (sp < 0) continue;
-        const int si = ref.nbrs[k];
-        if (fused[si][sp]) continue;
-        for (int d = 0; d < 3; ++d) {
-          pts[3 * n_obs + d] = h_cpt.p[3 * slot + d];
-          nrm[3 * n_obs + d] = h_cnrm.p[3 * slot + d];
-          clr[3 * n_obs + d] = f->views[si]->color[3 * (size_t)sp + d];
-        }
-        ++n_obs;
-        used_v[n_used] = si;
-        used_p[n_used] = sp;
-        ++n_used;
+      const size_t first = n_idx;
+      h_idx.p[n_idx++] = (unsigned)own;
+      for (; q < q_end; ++q) {
+        const FuseRec& o = h_rec.p[q];
+        if (h_marks.p[moff[ref.nbrs[o.slot]] + o.pix]) continue;
+        h_idx.p[n_idx++] = (unsigned)q;
       }
-      if (n_obs < f->min_num_consistent) continue;
-      float mp[3], mn[3];
-      uint8_t mc[3];
-      for (int d = 0; d < 3; ++d) {
-        for (int k = 0; k < n_obs; ++k) comp[k] = pts[3 * k + d];
-        mp[d] = nth_median(comp.data(), n_obs);
+      if ((int)(n_idx - first) < f->min_num_consistent) {
+        n_idx = first;
+        continue;
       }
-      for (int d = 0; d < 3; ++d) {
-        for (int k = 0; k < n_obs; ++k) comp[k] = nrm[3 * k + d];
-        mn[d] = nth_median(comp.data(), n_obs);
-      }
-      const float ml = std::sqrt((mn[0] * mn[0] + mn[1] * mn[1]) + mn[2] * mn[2]);
-      if (ml > 1e-6f)
-        for (int d = 0; d < 3; ++d) mn[d] = mn[d] / ml;
-      for (int d = 0; d < 3; ++d) {
-        for (int k = 0; k < n_obs; ++k) comp8[k] = clr[3 * k + d];
-        mc[d] = nth_median(comp8.data(), n_obs);
-      }
-      f->out_pts.insert(f->out_pts.end(), mp, mp + 3);
-      f->out_nrm.insert(f->out_nrm.end(), mn, mn + 3);
-      f->out_clr.insert(f->out_clr.end(), mc, mc + 3);
+      h_start.p[n_pts++] = (unsigned)first;
       rf[rp] = 1;
-      for (int k = 0; k < n_used; ++k) fused[used_v[k]][used_p[k]] = 1;
+      dirty[ri] = 1;
+      for (size_t k = first + 1; k < n_idx; ++k) {
+        const FuseRec& o = h_rec.p[h_idx.p[k]];
+        const int si = ref.nbrs[o.slot];
+        h_marks.p[moff[si] + o.pix] = 1;
+        dirty[si] = 1;
+      }
     }
+    if (!n_pts) continue;
+    h_start.p[n_pts] = (unsigned)n_idx;
+    FCUDA(d_start.alloc(n_pts + 1));
+    FCUDA(d_idx.alloc(n_idx));
+    FCUDA(d_vpt.alloc(3 * n_pts));
+    FCUDA(d_vnrm.alloc(3 * n_pts));
+    FCUDA(d_vclr.alloc(3 * n_pts));
+    FCUDA(h_vpt.alloc(3 * n_pts));
+    FCUDA(h_vnrm.alloc(3 * n_pts));
+    FCUDA(h_vclr.alloc(3 * n_pts));
+    FCUDA(cudaMemcpyAsync(d_start.p, h_start.p, (n_pts + 1) * sizeof(unsigned),
+                          cudaMemcpyHostToDevice, f->stream));
+    FCUDA(cudaMemcpyAsync(d_idx.p, h_idx.p, n_idx * sizeof(unsigned), cudaMemcpyHostToDevice,
+                          f->stream));
+    fuse_median_kernel<<<(unsigned)((n_pts + 127) / 128), 128, 0, f->stream>>>(
+        d_rec.p, d_start.p, d_idx.p, (int)n_pts, d_views.p, ri, d_nbrs.p, d_vpt.p, d_vnrm.p,
+        d_vclr.p);
+    FCUDA(cudaGetLastError());
+    FCUDA(cudaMemcpyAsync(h_vpt.p, d_vpt.p, 3 * n_pts * sizeof(float), cudaMemcpyDeviceToHost,
+                          f->stream));
+    FCUDA(cudaMemcpyAsync(h_vnrm.p, d_vnrm.p, 3 * n_pts * sizeof(float), cudaMemcpyDeviceToHost,
+                          f->stream));
+    FCUDA(cudaMemcpyAsync(h_vclr.p, d_vclr.p, 3 * n_pts, cudaMemcpyDeviceToHost, f->stream));
+    staged = n_pts;
   }
+  FCUDA(cudaStreamSynchronize(f->stream));
+  append_staged();
   *count = (int64_t)(f->out_pts.size() / 3);
   return DN_OK;
 }
