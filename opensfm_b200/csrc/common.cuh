@@ -443,6 +443,25 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
   return d;
 }
 
+// FP16 halves of a 32-bit word as FP32 (exact), and the low half plus an
+// FP32 value in one rounding: sm_100's mixed-precision add (.f32.f16).
+__device__ __forceinline__ float h16lo(unsigned w) {
+  float r;
+  asm("{\n\t.reg .b16 l, h;\n\tmov.b32 {l, h}, %1;\n\tcvt.f32.f16 %0, l;\n\t}" : "=f"(r) : "r"(w));
+  return r;
+}
+__device__ __forceinline__ float h16hi(unsigned w) {
+  float r;
+  asm("{\n\t.reg .b16 l, h;\n\tmov.b32 {l, h}, %1;\n\tcvt.f32.f16 %0, h;\n\t}" : "=f"(r) : "r"(w));
+  return r;
+}
+__device__ __forceinline__ float h16lo_add(unsigned w, float c) {
+  float r;
+  asm("{\n\t.reg .b16 l, h;\n\tmov.b32 {l, h}, %1;\n\tadd.rn.f32.f16 %0, l, %2;\n\t}"
+      : "=f"(r) : "r"(w), "f"(c));
+  return r;
+}
+
 // ------------------------------------------------------------------------
 // Cooperative 7 x 7 patch: L lanes (2, 4 or 8, adjacent in the warp) share
 // one pixel.  The patch is padded to 8 columns; lane l owns columns l, l + L,
@@ -591,26 +610,32 @@ __device__ inline float coop_walk_clamped(const CoopPatch<L>& cp, const ViewDev&
   return coop_finish<L>(cp, s1, s2, s3);
 }
 
-// Two table samples at the packed positions (X, Y), as table_sample does
-// one: returns the packed samples.
+// Two table samples at the packed positions (X, Y), centred by nsh (minus
+// the patch shift): returns the packed (sample - shift) values,
+//   (e0 - shift) + fx e1 + fy (e2 + fx e3),
+// with e0 - shift formed by the mixed-precision add while e0 is converted
+// (exact when the shift is itself a table value) and the polynomial on
+// packed pairs.
 __device__ __forceinline__ u64 sample_pair(u64 X, u64 Y, u64 MM, unsigned TP,
-                                           const uint2* __restrict__ q0) {
+                                           const uint2* __restrict__ q0, float nsh) {
   const u64 TX = add2_rd(X, MM), TY = add2_rd(Y, MM);
   const u64 FX = sub2(X, sub2(TX, MM)), FY = sub2(Y, sub2(TY, MM));
-  const unsigned oa = __float_as_uint(lo2(TY)) * TP + __float_as_uint(lo2(TX));
-  const unsigned ob = __float_as_uint(hi2(TY)) * TP + __float_as_uint(hi2(TX));
-  const float4 qa = quad_entry(q0, (int)oa);
-  const float4 qb = quad_entry(q0, (int)ob);
-  const float fxa = lo2(FX), fya = lo2(FY), fxb = hi2(FX), fyb = hi2(FY);
-  const float ya = fmaf(fya, fmaf(fxa, qa.w, qa.z), fmaf(fxa, qa.y, qa.x));
-  const float yb = fmaf(fyb, fmaf(fxb, qb.w, qb.z), fmaf(fxb, qb.y, qb.x));
-  return pk2(ya, yb);
+  // The index wraps modulo 2^32 by design: q0 is biased so that the
+  // offset, read as a signed int, lands inside the table.
+  const int oa = (int)(__float_as_uint(lo2(TY)) * TP + __float_as_uint(lo2(TX)));
+  const int ob = (int)(__float_as_uint(hi2(TY)) * TP + __float_as_uint(hi2(TX)));
+  const uint2 ha = __ldg(q0 + oa), hb = __ldg(q0 + ob);
+  const u64 E0 = pk2(h16lo_add(ha.x, nsh), h16lo_add(hb.x, nsh));
+  const u64 E1 = pk2(h16hi(ha.x), h16hi(hb.x));
+  const u64 E2 = pk2(h16lo(ha.y), h16lo(hb.y));
+  const u64 E3 = pk2(h16hi(ha.y), h16hi(hb.y));
+  return fma2(FY, fma2(FX, E3, E2), fma2(FX, E1, E0));
 }
 
 // The same walk inside the padded table (kFast), two slots per step on
 // packed FP32 pairs: tap positions, the floor (add rounding down to the
-// magic constant), the fractions and the three weighted sums all run as
-// .f32x2; the entry index and the bilinear polynomial stay scalar.  With
+// magic constant), the fractions, the bilinear polynomial and the three
+// weighted sums all run as .f32x2; the entry index stays scalar.  With
 // 2 or 4 lanes a pair is two columns of one row; with 8 lanes (one column
 // per lane) it is two rows, and row 6 is sampled alone.
 template <int L>
@@ -623,8 +648,7 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
   const u64 MM = pk2(vw.magic, vw.magic);
   const unsigned TP = (unsigned)vw.TP;
   const uint2* __restrict__ q0 = vw.quad0;
-  const float sh = patch_shift<false>(vw, wp);
-  const u64 SH = pk2(sh, sh);
+  const float nsh = -patch_shift<false>(vw, wp);
   u64 S1 = 0ull, S2 = 0ull, S3 = 0ull;  // (+0.0f, +0.0f) pairs
   float t1 = 0.f, t2 = 0.f, t3 = 0.f;   // the unpaired slot
   if constexpr (C == 1) {
@@ -634,7 +658,7 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
     const u64 BX = pk2(2.0f * wp.bx, 2.0f * wp.bx), BY = pk2(2.0f * wp.by, 2.0f * wp.by);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const u64 YY = sub2(sample_pair(X, Y, MM, TP, q0), SH);
+      const u64 YY = sample_pair(X, Y, MM, TP, q0, nsh);
       const u64 WY = mul2(cp.w2[k], YY);
       S1 = add2(S1, WY);
       S2 = fma2(WY, YY, S2);
@@ -642,7 +666,7 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
       X = add2(X, BX);
       Y = add2(Y, BY);
     }
-    const float y6 = table_sample(vw, fmaf(wp.bx, 6.0f, xc), fmaf(wp.by, 6.0f, yc)) - sh;
+    const float y6 = table_sample(vw, fmaf(wp.bx, 6.0f, xc), fmaf(wp.by, 6.0f, yc)) + nsh;
     const float wy = cp.wt * y6;
     t1 = wy;
     t2 = wy * y6;
@@ -661,7 +685,7 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
     for (int r = 0; r < 7; ++r) {
 #pragma unroll
       for (int m = 0; m < NP; ++m) {
-        const u64 YY = sub2(sample_pair(X[m], Y[m], MM, TP, q0), SH);
+        const u64 YY = sample_pair(X[m], Y[m], MM, TP, q0, nsh);
         const int k = r * NP + m;
         const u64 WY = mul2(cp.w2[k], YY);
         S1 = add2(S1, WY);
