@@ -119,9 +119,11 @@ def fusion_leg(b, vs, cands, n_maps, repeats=3, oracle=True):
     """DepthmapFuser over the batch's cleaned depthmaps (normals from the
     PatchMatch planes, grey colours, each view checked against itself and its
     cleaner neighbours, as dense.py lists a cluster).  Times fuse() on the
-    host clock (GPU candidates + host marks and medians) and, with `oracle`,
-    the single-thread C restatement on the same views, and checks that the
-    two point clouds are identical."""
+    host clock, without outlier removal (the dense pipeline's setting,
+    depthmap_fusion_sor_knn = 0) and with the fuser's default removal (K = 12,
+    factor 2.5).  With `oracle`, the single-thread C restatement fuses the
+    same views (without removal: its exact kNN is a brute force) and the two
+    point clouds are compared."""
     from opensfm_b200 import pydense
 
     views = []
@@ -137,13 +139,23 @@ def fusion_leg(b, vs, cands, n_maps, repeats=3, oracle=True):
     for v in views:
         f.add_view(v["K"], v["R"], v["t"], v["depth"], v["normal"], v["color"], None,
                    np.array(v["neighbor_ids"]))
-    got = f.fuse()  # warm-up
-    ts = []
-    for _ in range(repeats):
-        t0 = time.perf_counter()
-        got = f.fuse()
-        ts.append(time.perf_counter() - t0)
-    out = {"points": int(len(got[0])), "fuse_s": float(np.median(ts)),
+
+    def timed():
+        f.fuse()  # warm-up
+        ts = []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            res = f.fuse()
+            ts.append(time.perf_counter() - t0)
+        return res, float(np.median(ts))
+
+    got_sor, t_sor = timed()  # the fuser's defaults: removal with K = 12
+    removal_ms = f.last_removal_ms()
+    f.set_sor_params(0, 2.5)
+    got, t_plain = timed()
+    out = {"points": int(len(got[0])), "fuse_s": t_plain,
+           "points_after_outlier_removal": int(len(got_sor[0])), "fuse_with_removal_s": t_sor,
+           "removal_device_ms": removal_ms,
            "views": n_maps, "neighbours_per_view": float(np.mean([len(v["neighbor_ids"])
                                                                   for v in views]))}
     if oracle:

@@ -370,14 +370,16 @@ dn_status dn_gpu_cleaner_clean(dn_gpu_cleaner* c, int ref, const int* neighbor_i
 dn_status dn_gpu_cleaner_clear(dn_gpu_cleaner* c);
 
 /* ----------------------------------------------------------------------
- * DepthmapFuser (fuser.h:28-77, fuser.cc:35-372): per-pixel fusion of
+ * DepthmapFuser (fuser.h:28-77, fuser.cc:35-482): per-pixel fusion of
  * depthmaps into points, the reference's single-thread order (primary views
  * in order, pixels in raster order, fused pixels marking themselves and the
- * source pixels they used).  The candidate observations of every pixel are
- * computed on the GPU, the marks and medians on the host.  FP32 in the
- * reference's expression order.  The statistical outlier removal
- * (fuser.cc:374-482) is not built: knn must be 0.  Defaults: 3 consistent
- * observations, 2 px, 0.01, 10 degrees, border 5, behind factor 0.3.
+ * source pixels they used).  The candidate observations of every pixel and
+ * the medians are computed on the GPU, the marks on the host.  FP32 in the
+ * reference's expression order.  Then the statistical outlier removal
+ * (fuser.cc:374-482): exact mean distance to the K nearest other points on
+ * the GPU (uniform grid), mean + factor x std threshold on the host.
+ * Defaults: 3 consistent observations, 2 px, 0.01, 10 degrees, border 5,
+ * behind factor 0.3, outlier removal with K = 12 and factor 2.5.
  * ---------------------------------------------------------------------- */
 typedef struct dn_fuser dn_fuser;
 dn_status dn_fuser_create(dn_fuser** out);
@@ -387,6 +389,8 @@ dn_status dn_fuser_set_max_reproj_error(dn_fuser* f, float px);
 dn_status dn_fuser_set_max_depth_error(dn_fuser* f, float ratio);
 dn_status dn_fuser_set_max_normal_error(dn_fuser* f, float degrees);
 dn_status dn_fuser_set_border_margin(dn_fuser* f, int px);
+/* SetSORParams (fuser.cc:66-69): knn <= 0 skips the outlier removal;
+ * knn above 64 is rejected (DN_INVALID_ARG). */
 dn_status dn_fuser_set_sor_params(dn_fuser* f, int knn, float stddev_factor);
 dn_status dn_fuser_set_behind_depth_factor(dn_fuser* f, float factor);
 /* AddView (fuser.cc:82-97): depth f32 [H][W], normal f32 [H][W][3] (camera
@@ -396,13 +400,25 @@ dn_status dn_fuser_add_view(dn_fuser* f, const double K[9], const double R[9], c
                             const float* depth, const float* normal, const uint8_t* color,
                             const uint8_t* mask, int width, int height, const int* neighbor_ids,
                             int n_neighbors, int primary);
-/* Fuse (fuser.cc:115-372): *count receives the number of fused points. */
+/* Fuse (fuser.cc:115-482): *count receives the number of fused points
+ * left after the outlier removal. */
 dn_status dn_fuser_fuse(dn_fuser* f, int64_t* count);
 /* The last fuse's points, unit normals (world frame) and colours, each
  * `capacity` >= count rows of 3; any pointer may be NULL. */
 dn_status dn_fuser_get(dn_fuser* f, float* points, float* normals, uint8_t* colors,
                        int64_t capacity);
-/* Message for the last failed dn_fuser_* call on this thread. */
+/* Device time (ms) of the last fuse's outlier removal; 0 when skipped. */
+dn_status dn_fuser_last_removal_ms(dn_fuser* f, float* ms);
+/* The fuser's statistical outlier removal on any points (xyz rows, n of
+ * them): keep[i] = 1 for points whose mean distance to their knn nearest
+ * other points is at most mean + factor x std of those means; mean_knn
+ * (may be NULL) receives the means.  knn <= 0 or n <= knn + 1 keeps all
+ * (as the reference skips the step); knn above 64 is rejected.  Runs on the
+ * current device; errors are reported by dn_fuser_last_error. */
+dn_status dn_sor_filter(const float* points, int64_t n, int knn, float stddev_factor,
+                        uint8_t* keep, float* mean_knn);
+/* Message for the last failed dn_fuser_* or dn_sor_filter call on this
+ * thread. */
 const char* dn_fuser_last_error(void);
 
 /* ----------------------------------------------------------------------

@@ -123,6 +123,8 @@ _SIGNATURES = {
     "dn_fuser_fuse": ([_vp, ctypes.POINTER(ctypes.c_int64)], _i),
     "dn_fuser_get": ([_vp, _f, _f, _u8, ctypes.c_int64], _i),
     "dn_fuser_last_error": ([], ctypes.c_char_p),
+    "dn_fuser_last_removal_ms": ([_vp, ctypes.POINTER(ctypes.c_float)], _i),
+    "dn_sor_filter": ([_f, ctypes.c_int64, _i, ctypes.c_float, _u8, _f], _i),
     "dn_xxh32": ([_vp, ctypes.c_int64, ctypes.c_uint32], ctypes.c_uint32),
     "dn_lz4f_compress_bound": ([ctypes.c_int64], ctypes.c_int64),
     "dn_lz4f_compress": ([_vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],

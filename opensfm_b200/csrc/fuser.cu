@@ -1,5 +1,5 @@
-// DepthmapFuser (fuser.h:28-77, fuser.cc:35-372): per-pixel fusion of
-// depthmaps into a point cloud.
+// DepthmapFuser (fuser.h:28-77, fuser.cc:35-482): per-pixel fusion of
+// depthmaps into a point cloud, then statistical outlier removal.
 //
 // The reference fuses primary views one after another; within a view it
 // walks the pixels in raster order, and every fused pixel marks itself and
@@ -9,16 +9,15 @@
 // depth, the asymmetric depth test, the forward-backward reprojection test
 // and the normal test -- depends on the inputs alone.  So the GPU computes,
 // for every pixel of a primary view and every neighbour, the candidate
-// observation (source pixel, world point, world normal) in one launch, and
-// the host walks the pixels in the reference's order, applies the marks,
-// and takes the component-wise medians of the surviving observations.
+// observation (source pixel, world point, world normal) in one launch; the
+// host walks the pixels in the reference's order and applies the marks; and
+// the GPU takes the component-wise medians of the surviving observations.
 //
 // Arithmetic is FP32 in the order of the reference's expressions, every
 // operation rounded by itself (no contraction), with the 3x3 inverses in
 // Eigen's cofactor order; the result is the single-thread result of the
-// reference.  The statistical outlier removal (fuser.cc:374-482) is not
-// built: set_sor_params accepts only knn = 0, its setting in OpenSfM's
-// dense pipeline (depthmap_fusion_sor_knn = 0).
+// reference.  The statistical outlier removal (fuser.cc:374-482) follows
+// at the end of the file.
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
@@ -332,6 +331,194 @@ __global__ void fuse_median_kernel(const FuseRec* __restrict__ rec,
     out_clr[3 * i + d] = rank_median<uint8_t>(n, [&](int a) { return color_of(a, d); });
 }
 
+// ------------------------------------------------------- outlier removal
+// Statistical outlier removal (fuser.cc:374-482).  The reference takes the
+// K + 1 nearest neighbours of each point from a vlfeat kd-forest of one tree
+// with no comparison limit (an exact search), skips the point itself and
+// averages the float square roots of the K remaining float L2 distances
+// (squared distance summed over x, y, z) in ascending order.  That is the
+// mean of the K smallest distances to other points, whatever the tie order,
+// and it is computed here exactly on a uniform grid: points are sorted by
+// cell, each query scans shells of cells around its own until the K-th
+// distance is provably below every unscanned cell's distance (with a slack
+// for the cell rounding), and the few queries still open after kSorRings
+// shells are finished by one warp each over all points.  The statistics,
+// the threshold and the filter follow on the host in point order, in double
+// as the reference accumulates them.
+constexpr int kSorMaxK = 64;
+constexpr int kSorRings = 3;
+
+struct SorGrid {
+  float ox, oy, oz, h, slack;
+  int nx, ny, nz;
+};
+
+__device__ inline float sor_d2(float4 q, float4 p) {
+  const float dx = __fsub_rn(q.x, p.x), dy = __fsub_rn(q.y, p.y), dz = __fsub_rn(q.z, p.z);
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// Keeps best[0 .. cnt) as the smallest values seen, ascending, cnt <= K.
+__device__ inline void sor_insert(float* best, int& cnt, int K, float d2) {
+  if (cnt == K && !(d2 < best[K - 1])) return;
+  int m = cnt < K ? cnt++ : K - 1;
+  while (m > 0 && best[m - 1] > d2) {
+    best[m] = best[m - 1];
+    --m;
+  }
+  best[m] = d2;
+}
+
+__device__ inline int sor_cell(float v, float o, float h, int n) {
+  const int c = (int)floorf(__fdiv_rn(__fsub_rn(v, o), h));
+  return min(max(c, 0), n - 1);
+}
+
+__global__ void sor_keys_kernel(const float* __restrict__ pts, int n, SorGrid g,
+                                unsigned long long* __restrict__ key, int* __restrict__ idx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int cx = sor_cell(pts[3 * i], g.ox, g.h, g.nx);
+  const int cy = sor_cell(pts[3 * i + 1], g.oy, g.h, g.ny);
+  const int cz = sor_cell(pts[3 * i + 2], g.oz, g.h, g.nz);
+  key[i] = ((unsigned long long)cz * g.ny + cy) * g.nx + cx;
+  idx[i] = i;
+}
+
+// Points in cell order, the original index in w.
+__global__ void sor_gather_kernel(const float* __restrict__ pts, const int* __restrict__ idx,
+                                  int n, float4* __restrict__ sp) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int i = idx[s];
+  sp[s] = make_float4(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], __int_as_float(i));
+}
+
+__device__ inline int sor_lower_bound(const unsigned long long* __restrict__ a, int n,
+                                      unsigned long long v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__device__ inline float sor_mean(const float* best, int K) {
+  float sum = 0.0f;
+  for (int m = 0; m < K; ++m) sum = __fadd_rn(sum, __fsqrt_rn(best[m]));
+  return __fdiv_rn(sum, (float)K);
+}
+
+// One thread per point, in cell order.  Writes mean_knn[original index], or
+// queues the point for the brute-force pass.
+__global__ void sor_knn_kernel(const float4* __restrict__ sp,
+                               const unsigned long long* __restrict__ skey, int n, SorGrid g,
+                               int K, float* __restrict__ mean_knn, int* __restrict__ open_q,
+                               unsigned* __restrict__ n_open) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float4 q = sp[s];
+  const int self = __float_as_int(q.w);
+  const unsigned long long ck = skey[s];
+  const int cx = (int)(ck % (unsigned long long)g.nx);
+  const int cy = (int)((ck / (unsigned long long)g.nx) % (unsigned long long)g.ny);
+  const int cz = (int)(ck / ((unsigned long long)g.nx * g.ny));
+  float best[kSorMaxK];
+  int cnt = 0;
+  auto scan = [&](int lo, int hi) {
+    for (int j = lo; j < hi; ++j) {
+      const float4 p = sp[j];
+      if (__float_as_int(p.w) == self) continue;
+      sor_insert(best, cnt, K, sor_d2(q, p));
+    }
+  };
+  auto key = [&](int x, int y, int z) {
+    return ((unsigned long long)z * g.ny + y) * g.nx + x;
+  };
+  bool done = false;
+  for (int r = 0; r <= kSorRings && !done; ++r) {
+    for (int dz = -r; dz <= r; ++dz) {
+      const int z = cz + dz;
+      if (z < 0 || z >= g.nz) continue;
+      for (int dy = -r; dy <= r; ++dy) {
+        const int y = cy + dy;
+        if (y < 0 || y >= g.ny) continue;
+        if (abs(dz) == r || abs(dy) == r) {  // a face row: the whole run of x
+          const int x0 = max(cx - r, 0), x1 = min(cx + r, g.nx - 1);
+          scan(sor_lower_bound(skey, n, key(x0, y, z)), sor_lower_bound(skey, n, key(x1, y, z) + 1));
+        } else {  // inside the shell's cross-section: only its two end cells
+          for (int e = 0; e < 2; ++e) {
+            const int x = e ? cx + r : cx - r;
+            if (x >= 0 && x < g.nx)
+              scan(sor_lower_bound(skey, n, key(x, y, z)), sor_lower_bound(skey, n, key(x, y, z) + 1));
+          }
+        }
+      }
+    }
+    // Distance from q to the nearest face of the scanned box that has cells
+    // beyond it; none left means every point has been scanned.
+    float dmin = INFINITY;
+    if (cx - r > 0) dmin = fminf(dmin, q.x - (g.ox + (float)(cx - r) * g.h));
+    if (cx + r < g.nx - 1) dmin = fminf(dmin, (g.ox + (float)(cx + r + 1) * g.h) - q.x);
+    if (cy - r > 0) dmin = fminf(dmin, q.y - (g.oy + (float)(cy - r) * g.h));
+    if (cy + r < g.ny - 1) dmin = fminf(dmin, (g.oy + (float)(cy + r + 1) * g.h) - q.y);
+    if (cz - r > 0) dmin = fminf(dmin, q.z - (g.oz + (float)(cz - r) * g.h));
+    if (cz + r < g.nz - 1) dmin = fminf(dmin, (g.oz + (float)(cz + r + 1) * g.h) - q.z);
+    if (dmin == INFINITY) {
+      done = true;
+    } else {
+      dmin -= g.slack;
+      done = cnt == K && dmin > 0.0f && best[K - 1] <= dmin * dmin * (1.0f - 1e-5f);
+    }
+  }
+  if (done && cnt == K)
+    mean_knn[self] = sor_mean(best, K);
+  else
+    open_q[atomicAdd(n_open, 1u)] = s;
+}
+
+// One warp per open query: every lane keeps the K smallest distances of its
+// stride over all points; K rounds of a warp-wide minimum then merge them in
+// ascending order.
+__global__ void sor_brute_kernel(const float4* __restrict__ sp, int n,
+                                 const int* __restrict__ open_q, int n_open, int K,
+                                 float* __restrict__ mean_knn) {
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= n_open) return;  // whole warps leave together
+  const float4 q = sp[open_q[w]];
+  const int self = __float_as_int(q.w);
+  float best[kSorMaxK];
+  int cnt = 0;
+  for (int j = lane; j < n; j += 32) {
+    const float4 p = sp[j];
+    if (__float_as_int(p.w) == self) continue;
+    sor_insert(best, cnt, K, sor_d2(q, p));
+  }
+  int head = 0;
+  float sum = 0.0f;
+  for (int m = 0; m < K; ++m) {
+    const float v = head < cnt ? best[head] : INFINITY;
+    float mv = v;
+    int ml = lane;
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, mv, o);
+      const int ol = __shfl_xor_sync(0xffffffffu, ml, o);
+      if (ov < mv || (ov == mv && ol < ml)) {
+        mv = ov;
+        ml = ol;
+      }
+    }
+    if (lane == ml) ++head;
+    sum = __fadd_rn(sum, __fsqrt_rn(mv));
+  }
+  if (lane == 0) mean_knn[self] = __fdiv_rn(sum, (float)K);
+}
+
 // ------------------------------------------------------------------ host
 template <typename T>
 struct DBuf {
@@ -397,8 +584,9 @@ struct dn_fuser {
   float max_normal_deg = 10.0f;
   int border = 5;
   float behind = 0.3f;
-  int sor_knn = 0;
+  int sor_knn = 12;  // the reference's defaults (fuser.cc:45-46)
   float sor_factor = 2.5f;
+  float sor_ms = 0.0f;  // device time of the last outlier removal
   std::vector<std::unique_ptr<FView>> views;
   std::vector<float> out_pts, out_nrm;
   std::vector<uint8_t> out_clr;
@@ -452,10 +640,8 @@ extern "C" dn_status dn_fuser_set_border_margin(dn_fuser* f, int px) {
 }
 extern "C" dn_status dn_fuser_set_sor_params(dn_fuser* f, int knn, float stddev_factor) {
   FCHECK(f, "NULL fuser");
-  FCHECK(knn <= 0,
-         "statistical outlier removal is not built: knn must be 0 (OpenSfM's dense pipeline "
-         "sets depthmap_fusion_sor_knn = 0)");
-  f->sor_knn = 0;
+  FCHECK(knn <= kSorMaxK, "knn above 64 is not supported");
+  f->sor_knn = std::max(0, knn);  // knn <= 0 skips the step, as the reference does
   f->sor_factor = stddev_factor;
   return DN_OK;
 }
@@ -504,6 +690,181 @@ extern "C" dn_status dn_fuser_add_view(dn_fuser* f, const double* K, const doubl
   }
   FCUDA(cudaStreamSynchronize(f->stream));
   f->views.push_back(std::move(v));
+  return DN_OK;
+}
+
+// Mean distance to the K nearest other points (fuser.cc:405-438) for each
+// of the N points P (xyz rows), on the device; mk receives them in point
+// order, *ms the device time.  Requires N > K + 1 and 1 <= K <= kSorMaxK.
+static dn_status sor_mean_knn(cudaStream_t s, const float* P, size_t N, int K,
+                              std::vector<float>& mk, float* ms) {
+  FCHECK(N < (size_t(1) << 31), "too many points for the outlier removal");
+  const int n = (int)N;
+  // Grid over the bounding box: cell edge from the volume per point, K + 1
+  // points to a cell on average if they filled the box, halved because
+  // surface points are denser than that where they lie.
+  float lo[3] = {P[0], P[1], P[2]}, hi[3] = {P[0], P[1], P[2]};
+  float amax = 0.0f;
+  for (size_t i = 0; i < N; ++i)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], P[3 * i + d]);
+      hi[d] = std::max(hi[d], P[3 * i + d]);
+      amax = std::max(amax, std::fabs(P[3 * i + d]));
+    }
+  FCHECK(std::isfinite(amax), "points must be finite for the outlier removal");
+  double ext[3], emax = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    ext[d] = (double)hi[d] - (double)lo[d];
+    emax = std::max(emax, ext[d]);
+  }
+  const double floor_ext = std::max(emax * 1e-3, 1e-6);
+  const double vol = std::max(ext[0], floor_ext) * std::max(ext[1], floor_ext) *
+                     std::max(ext[2], floor_ext);
+  double h = 0.5 * std::cbrt(vol * (K + 1) / (double)N);
+  h = std::max(h, std::max(emax, 1e-6) / (double)(1 << 20));  // at most 2^20 cells an axis
+  SorGrid g;
+  g.ox = lo[0];
+  g.oy = lo[1];
+  g.oz = lo[2];
+  g.h = (float)h;
+  g.nx = (int)(ext[0] / h) + 1;
+  g.ny = (int)(ext[1] / h) + 1;
+  g.nz = (int)(ext[2] / h) + 1;
+  // Cell rounding moves a point across a face by a few ULPs of its
+  // coordinates at most; the bound keeps a far wider margin.
+  g.slack = (float)(1e-5 * ((double)amax + h));
+
+  cudaEvent_t e0, e1;
+  FCUDA(cudaEventCreate(&e0));
+  FCUDA(cudaEventCreate(&e1));
+  struct EvGuard {
+    cudaEvent_t a, b;
+    ~EvGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } evg{e0, e1};
+  DBuf<float> d_pts, d_mean;
+  DBuf<unsigned long long> d_key, d_skey;
+  DBuf<int> d_idx, d_sidx, d_open;
+  DBuf<float4> d_sp;
+  DBuf<unsigned> d_nopen;
+  DBuf<uint8_t> d_tmp;
+  FCUDA(d_pts.alloc(3 * N));
+  FCUDA(d_mean.alloc(N));
+  FCUDA(d_key.alloc(N));
+  FCUDA(d_skey.alloc(N));
+  FCUDA(d_idx.alloc(N));
+  FCUDA(d_sidx.alloc(N));
+  FCUDA(d_open.alloc(N));
+  FCUDA(d_sp.alloc(N));
+  FCUDA(d_nopen.alloc(1));
+  FCUDA(cudaMemcpyAsync(d_pts.p, P, 3 * N * sizeof(float), cudaMemcpyHostToDevice, s));
+  FCUDA(cudaEventRecord(e0, s));
+  FCUDA(cudaMemsetAsync(d_nopen.p, 0, sizeof(unsigned), s));
+  const unsigned blocks = (unsigned)((N + 255) / 256);
+  sor_keys_kernel<<<blocks, 256, 0, s>>>(d_pts.p, n, g, d_key.p, d_idx.p);
+  FCUDA(cudaGetLastError());
+  size_t tmp_bytes = 0;
+  FCUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_key.p, d_skey.p, d_idx.p, d_sidx.p,
+                                        n, 0, 64, s));
+  FCUDA(d_tmp.alloc(std::max<size_t>(tmp_bytes, 1)));
+  FCUDA(cub::DeviceRadixSort::SortPairs(d_tmp.p, tmp_bytes, d_key.p, d_skey.p, d_idx.p,
+                                        d_sidx.p, n, 0, 64, s));
+  sor_gather_kernel<<<blocks, 256, 0, s>>>(d_pts.p, d_sidx.p, n, d_sp.p);
+  FCUDA(cudaGetLastError());
+  sor_knn_kernel<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(d_sp.p, d_skey.p, n, g, K,
+                                                             d_mean.p, d_open.p, d_nopen.p);
+  FCUDA(cudaGetLastError());
+  unsigned n_open = 0;
+  FCUDA(cudaMemcpyAsync(&n_open, d_nopen.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  FCUDA(cudaStreamSynchronize(s));
+  if (n_open) {
+    const unsigned warps_per_block = 4;
+    sor_brute_kernel<<<(n_open + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0,
+                       s>>>(d_sp.p, n, d_open.p, (int)n_open, K, d_mean.p);
+    FCUDA(cudaGetLastError());
+  }
+  FCUDA(cudaEventRecord(e1, s));
+  mk.resize(N);
+  FCUDA(cudaMemcpyAsync(mk.data(), d_mean.p, N * sizeof(float), cudaMemcpyDeviceToHost, s));
+  FCUDA(cudaStreamSynchronize(s));
+  FCUDA(cudaEventElapsedTime(ms, e0, e1));
+  return DN_OK;
+}
+
+// The reference's statistics over the means (fuser.cc:442-455): double
+// sums in point order, threshold mean + factor * std rounded to float.
+static float sor_threshold(const std::vector<float>& mk, float factor) {
+  double sum_d = 0.0, sum_d2 = 0.0;
+  for (size_t i = 0; i < mk.size(); ++i) {
+    const double d = mk[i];
+    if (d < 1e20f) {
+      sum_d += d;
+      sum_d2 += d * d;
+    }
+  }
+  const double mean_d = sum_d / (double)mk.size();
+  const double var_d = sum_d2 / (double)mk.size() - mean_d * mean_d;
+  const double std_d = std::sqrt(std::max(0.0, var_d));
+  return (float)(mean_d + factor * std_d);
+}
+
+// The outlier removal over the fused points (fuser.cc:374-482).
+static dn_status run_sor(dn_fuser* f) {
+  const int K = f->sor_knn;
+  const size_t N = f->out_pts.size() / 3;
+  f->sor_ms = 0.0f;
+  if (K <= 0 || N <= (size_t)K + 1) return DN_OK;
+  std::vector<float> mk;
+  const dn_status st = sor_mean_knn(f->stream, f->out_pts.data(), N, K, mk, &f->sor_ms);
+  if (st != DN_OK) return st;
+  const float threshold = sor_threshold(mk, f->sor_factor);
+  size_t kept = 0;
+  for (size_t i = 0; i < N; ++i) {
+    if (!(mk[i] <= threshold)) continue;
+    if (kept != i) {
+      std::memcpy(&f->out_pts[3 * kept], &f->out_pts[3 * i], 3 * sizeof(float));
+      std::memcpy(&f->out_nrm[3 * kept], &f->out_nrm[3 * i], 3 * sizeof(float));
+      std::memcpy(&f->out_clr[3 * kept], &f->out_clr[3 * i], 3);
+    }
+    ++kept;
+  }
+  f->out_pts.resize(3 * kept);
+  f->out_nrm.resize(3 * kept);
+  f->out_clr.resize(3 * kept);
+  return DN_OK;
+}
+
+extern "C" dn_status dn_sor_filter(const float* points, int64_t n, int knn, float stddev_factor,
+                                   uint8_t* keep, float* mean_knn) {
+  FCHECK(n >= 0 && (n == 0 || points) && (n == 0 || keep), "NULL argument");
+  FCHECK(knn <= kSorMaxK, "knn above 64 is not supported");
+  if (knn <= 0 || n <= (int64_t)knn + 1) {
+    std::memset(keep, 1, (size_t)n);
+    return DN_OK;
+  }
+  int dev = 0;
+  FCUDA(cudaGetDevice(&dev));
+  cudaStream_t s;
+  FCUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } sg{s};
+  std::vector<float> mk;
+  float ms = 0.0f;
+  const dn_status st = sor_mean_knn(s, points, (size_t)n, knn, mk, &ms);
+  if (st != DN_OK) return st;
+  const float threshold = sor_threshold(mk, stddev_factor);
+  for (int64_t i = 0; i < n; ++i) keep[i] = mk[i] <= threshold ? 1 : 0;
+  if (mean_knn) std::memcpy(mean_knn, mk.data(), (size_t)n * sizeof(float));
+  return DN_OK;
+}
+
+extern "C" dn_status dn_fuser_last_removal_ms(dn_fuser* f, float* ms) {
+  FCHECK(f && ms, "NULL argument");
+  *ms = f->sor_ms;
   return DN_OK;
 }
 
@@ -710,6 +1071,8 @@ extern "C" dn_status dn_fuser_fuse(dn_fuser* f, int64_t* count) {
   }
   FCUDA(cudaStreamSynchronize(f->stream));
   append_staged();
+  const dn_status st = run_sor(f);
+  if (st != DN_OK) return st;
   *count = (int64_t)(f->out_pts.size() / 3);
   return DN_OK;
 }

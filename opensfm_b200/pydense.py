@@ -27,8 +27,8 @@ import numpy as np
 from . import _lib
 from ._lib import _d, _f, _i32, _u8, check, ptr
 
-__all__ = ["DepthmapEstimator", "DepthmapCleaner", "DepthmapPruner", "Batch", "postprocess_depth",
-           "fp32_peak"]
+__all__ = ["DepthmapEstimator", "DepthmapCleaner", "DepthmapPruner", "GPUDepthmapCleaner",
+           "DepthmapFuser", "Batch", "postprocess_depth", "sor_filter", "fp32_peak"]
 
 
 def postprocess_depth(depth: np.ndarray) -> np.ndarray:
@@ -310,7 +310,15 @@ class DepthmapFuser(_Handle):
         single-thread result whatever the count."""
 
     def set_sor_params(self, knn: int, stddev_factor: float) -> None:
+        """Statistical outlier removal after fusion (fuser.cc:66-69,
+        374-482): knn <= 0 skips it; the default is knn 12, factor 2.5."""
         self._check(self._L.dn_fuser_set_sor_params(self._h, int(knn), float(stddev_factor)))
+
+    def last_removal_ms(self) -> float:
+        """Device time of the last fuse's outlier removal (0 when skipped)."""
+        ms = ctypes.c_float()
+        self._check(self._L.dn_fuser_last_removal_ms(self._h, ctypes.byref(ms)))
+        return float(ms.value)
 
     def set_behind_depth_factor(self, factor: float) -> None:
         self._check(self._L.dn_fuser_set_behind_depth_factor(self._h, float(factor)))
@@ -350,6 +358,28 @@ class DepthmapFuser(_Handle):
         clr = np.zeros((n, 3), np.uint8)
         self._check(self._L.dn_fuser_get(self._h, ptr(pts, _f), ptr(nrm, _f), ptr(clr, _u8), n))
         return [pts, nrm, clr]
+
+
+def sor_filter(points, knn: int = 12, stddev_factor: float = 2.5):
+    """The fuser's statistical outlier removal (``fuser.cc:374-482``) on any
+    (N, 3) points: returns (keep (N,) bool, mean distance to the knn nearest
+    other points (N,) f32).  knn <= 0 or N <= knn + 1 keeps every point."""
+    p = np.ascontiguousarray(points, dtype=np.float32)
+    if p.ndim != 2 or p.shape[1] != 3:
+        raise ValueError("points must have shape (N, 3)")
+    keep = np.ones(len(p), np.uint8)
+    mk = np.zeros(len(p), np.float32)
+    L = _lib.load()
+    st = L.dn_sor_filter(ptr(p, _f), len(p), int(knn), float(stddev_factor), ptr(keep, _u8),
+                         ptr(mk, _f))
+    if st != _lib.DN_OK:
+        msg = L.dn_fuser_last_error().decode(errors="replace")
+        if st == _lib.DN_INVALID_ARG:
+            raise ValueError(msg)
+        if st == _lib.DN_OUT_OF_MEMORY:
+            raise MemoryError(msg)
+        raise _lib.DenseError(st, msg)
+    return keep.astype(bool), mk
 
 
 class DepthmapPruner(_Handle):

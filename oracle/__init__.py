@@ -516,9 +516,11 @@ class _FuseView(ctypes.Structure):
 
 
 def port_fuse(views, min_num_consistent=3, max_reproj_error=2.0, max_depth_error=0.01,
-              max_normal_error=10.0, border_margin=5, behind_depth_factor=0.3):
-    """DepthmapFuser::Fuse (fuser.cc:115-372, no outlier removal) in the C
-    restatement.  views: dicts with K, R, t, depth (H, W), normal (H, W, 3),
+              max_normal_error=10.0, border_margin=5, behind_depth_factor=0.3, sor_knn=0,
+              sor_stddev_factor=2.5):
+    """DepthmapFuser::Fuse (fuser.cc:115-372) in the C restatement, followed
+    by the statistical outlier removal (fuser.cc:374-482, port_sor) when
+    sor_knn > 0.  views: dicts with K, R, t, depth (H, W), normal (H, W, 3),
     color (H, W, 3) uint8, mask (H, W) uint8 or None, neighbor_ids, primary.
     Returns (points (N, 3) f32, normals (N, 3) f32, colors (N, 3) u8)."""
     L = port()
@@ -556,4 +558,24 @@ def port_fuse(views, min_num_consistent=3, max_reproj_error=2.0, max_depth_error
                     float(max_reproj_error), float(max_depth_error), float(max_normal_error),
                     int(border_margin), float(behind_depth_factor), _P(pts, _f), _P(nrm, _f),
                     _P(clr, _u8), cap)
-    return pts[:cnt].copy(), nrm[:cnt].copy(), clr[:cnt].copy()
+    pts, nrm, clr = pts[:cnt].copy(), nrm[:cnt].copy(), clr[:cnt].copy()
+    if sor_knn > 0:
+        keep, _ = port_sor(pts, sor_knn, sor_stddev_factor)
+        pts, nrm, clr = pts[keep], nrm[keep], clr[keep]
+    return pts, nrm, clr
+
+
+def port_sor(points, knn, stddev_factor):
+    """The fuser's statistical outlier removal (fuser.cc:374-482) in the C
+    restatement (or_sor: exact K nearest neighbours by brute force, so small
+    inputs only).  Returns (keep (N,) bool, mean kNN distance (N,) f32)."""
+    L = port()
+    if not getattr(L, "_sor_ready", False):
+        L.or_sor.argtypes = [_f, ctypes.c_long, ctypes.c_int, ctypes.c_float, _u8, _f]
+        L.or_sor.restype = ctypes.c_long
+        L._sor_ready = True
+    p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    keep = np.zeros(len(p), np.uint8)
+    mk = np.zeros(len(p), np.float32)
+    L.or_sor(_P(p, _f), len(p), int(knn), float(stddev_factor), _P(keep, _u8), _P(mk, _f))
+    return keep.astype(bool), mk

@@ -1,7 +1,7 @@
 /* DepthmapFuser::Fuse restated in C.  TEST INFRASTRUCTURE ONLY.
  *
- * Follows opensfm/src/lib/dense/src/fuser.cc:115-372 (per-pixel fusion,
- * without the statistical outlier removal of 374-482) with the reference's
+ * Follows opensfm/src/lib/dense/src/fuser.cc:115-372 (per-pixel fusion;
+ * or_sor below restates the statistical outlier removal of 374-482) with the reference's
  * single-thread order: primary views in index order, pixels in raster
  * order, each fused pixel marking itself and the source pixels it used.
  * Arithmetic is FP32 with every operation rounded by itself, in the order
@@ -255,4 +255,68 @@ done:
   free(comp);
   free(comp8);
   return count;
+}
+
+/* Statistical outlier removal (fuser.cc:374-482).  The reference finds the
+ * K + 1 nearest neighbours of every point with a vlfeat kd-forest of one
+ * tree and vlfeat's default comparison limit 0, which vlfeat defines as an
+ * exact search; the distances are vlfeat's float L2, the squared distance
+ * summed over x, y, z in that order.  Skipping the point itself leaves the
+ * K smallest distances to other points, so that set is found here by brute
+ * force (O(N^2): small inputs only), summed as float square roots in
+ * ascending order and divided by K.  Mean and variance of those means are
+ * accumulated in double in point order; points with a mean at or below
+ * mean + factor * std (rounded to float) are kept.  keep[i] is set to 0/1;
+ * mean_knn (optional) receives the per-point means.  Returns the kept count,
+ * or n (all kept) when k <= 0 or n <= k + 1, as the reference skips the step. */
+long or_sor(const float* pts, long n, int k, float factor, uint8_t* keep, float* mean_knn) {
+  if (k <= 0 || n <= (long)k + 1) {
+    for (long i = 0; i < n; ++i) keep[i] = 1;
+    return n;
+  }
+  float* best = (float*)malloc(sizeof(float) * (size_t)k);
+  float* mk = (float*)malloc(sizeof(float) * (size_t)n);
+  for (long i = 0; i < n; ++i) {
+    const float* q = pts + 3 * i;
+    int cnt = 0;
+    for (long j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const float* p = pts + 3 * j;
+      const float dx = q[0] - p[0], dy = q[1] - p[1], dz = q[2] - p[2];
+      float d2 = dx * dx;
+      d2 = d2 + dy * dy;
+      d2 = d2 + dz * dz;
+      if (cnt == k && !(d2 < best[k - 1])) continue;
+      int m = cnt < k ? cnt++ : k - 1;
+      while (m > 0 && best[m - 1] > d2) {
+        best[m] = best[m - 1];
+        --m;
+      }
+      best[m] = d2;
+    }
+    float sum = 0.0f;
+    for (int m = 0; m < k; ++m) sum += sqrtf(best[m]);
+    mk[i] = sum / (float)k;
+  }
+  double sum_d = 0.0, sum_d2 = 0.0;
+  for (long i = 0; i < n; ++i) {
+    const double d = mk[i];
+    if (d < 1e20f) {
+      sum_d += d;
+      sum_d2 += d * d;
+    }
+  }
+  const double mean_d = sum_d / (double)n;
+  const double var_d = sum_d2 / (double)n - mean_d * mean_d;
+  const double std_d = sqrt(var_d > 0.0 ? var_d : 0.0);
+  const float threshold = (float)(mean_d + factor * std_d);
+  long kept = 0;
+  for (long i = 0; i < n; ++i) {
+    keep[i] = mk[i] <= threshold;
+    kept += keep[i];
+    if (mean_knn) mean_knn[i] = mk[i];
+  }
+  free(best);
+  free(mk);
+  return kept;
 }

@@ -478,7 +478,56 @@ def test_fuser_bit_identical_to_oracle(scene):
         for a, w in zip(got, want):
             assert a.dtype == w.dtype and np.array_equal(a, w)
     with pytest.raises(ValueError):
-        f.set_sor_params(12, 2.5)
+        f.set_sor_params(65, 2.5)
+    # With the reference's default outlier removal (K = 12, factor 2.5).
+    want = O.port_fuse(views, **params, sor_knn=12, sor_stddev_factor=2.5)
+    f.set_sor_params(12, 2.5)
+    got = f.fuse()
+    print("after outlier removal", len(got[0]), "oracle", len(want[0]))
+    assert 0 < len(want[0]) < len(O.port_fuse(views, **params)[0])
+    for a, w in zip(got, want):
+        assert a.dtype == w.dtype and np.array_equal(a, w)
+    assert f.last_removal_ms() > 0
+
+
+def _sor_sets():
+    """Point sets for the outlier removal: clustered surfaces with scattered
+    far points, exact duplicates, a flat plane (one degenerate axis), a line
+    (two), points on cell-sized lattice steps, and tiny and huge scales."""
+    rng = np.random.default_rng(21)
+    out = []
+    a = rng.uniform(0, 10, (6000, 2))
+    surf = np.c_[a, 0.3 * np.sin(a[:, 0]) + 0.01 * rng.standard_normal(6000)]
+    far = rng.uniform(-50, 60, (120, 3))
+    out.append(("surface+far", np.r_[surf, far]))
+    dup = np.r_[surf[:3000], surf[:40], surf[:40]]
+    out.append(("duplicates", dup))
+    out.append(("plane", np.c_[rng.uniform(0, 5, (5000, 2)), np.zeros(5000)]))
+    out.append(("line", np.c_[rng.uniform(0, 5, 3000), np.zeros(3000), np.ones(3000)]))
+    g = np.stack(np.meshgrid(*[np.arange(14.0)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    out.append(("lattice", 0.25 * g))
+    out.append(("tiny", 1e-4 * rng.standard_normal((4000, 3)) + 1000.0))
+    out.append(("huge", 1e4 * rng.standard_normal((4000, 3))))
+    clusters = np.concatenate([c + 0.05 * rng.standard_normal((500, 3))
+                               for c in rng.uniform(-100, 100, (8, 3))])
+    out.append(("clusters", np.r_[clusters, rng.uniform(-100, 100, (30, 3))]))
+    return [(n, p.astype(np.float32)) for n, p in out]
+
+
+@pytest.mark.parametrize("knn,factor", [(12, 2.5), (1, 1.0), (30, 0.5)])
+def test_sor_filter_bit_identical_to_oracle(knn, factor):
+    """Grid kNN on the device (exact, with the brute-force finish for open
+    queries) against the oracle's brute force: identical per-point means and
+    keep masks."""
+    for name, pts in _sor_sets():
+        keep, mk = pydense.sor_filter(pts, knn, factor)
+        want_keep, want_mk = O.port_sor(pts, knn, factor)
+        assert np.array_equal(mk, want_mk), name
+        assert np.array_equal(keep, want_keep), name
+    keep, _ = pydense.sor_filter(pts[:knn + 1], knn, factor)
+    assert keep.all()
+    with pytest.raises(ValueError):
+        pydense.sor_filter(pts, 65, 1.0)
 
 
 def test_invalid_arguments_raise(scene):

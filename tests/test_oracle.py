@@ -281,3 +281,49 @@ def test_fuser_oracle_known_answers():
     assert np.allclose(nrm, np.tile(-c.R[2], (len(pts), 1)), atol=1e-6)
     none = O.port_fuse(views, min_num_consistent=3, border_margin=2)
     assert len(none[0]) == 0
+
+
+def test_sor_oracle_known_answers():
+    """Outlier removal restatement: on a unit grid every interior point's 4
+    nearest neighbours lie at distance 1 (mean exactly 1), a far point is
+    removed, and with knn = 0 or too few points nothing is removed."""
+    g = np.stack(np.meshgrid(np.arange(10.0), np.arange(10.0), indexing="ij"), -1).reshape(-1, 2)
+    pts = np.concatenate([np.c_[g, np.zeros(len(g))], [[100.0, 100.0, 100.0]]]).astype(np.float32)
+    keep, mk = O.port_sor(pts, 4, 2.5)
+    interior = (g[:, 0] > 0) & (g[:, 0] < 9) & (g[:, 1] > 0) & (g[:, 1] < 9)
+    assert np.all(mk[:-1][interior] == 1.0)
+    corner = np.float32((np.float32(1) + np.float32(1) + np.sqrt(np.float32(2))
+                         + np.float32(2)) / np.float32(4))
+    assert mk[0] == corner
+    assert keep[:-1].all() and not keep[-1]
+    assert O.port_sor(pts, 0, 2.5)[0].all()
+    assert O.port_sor(pts[:5], 4, 2.5)[0].all()  # n <= k + 1: skipped
+
+
+def test_sor_oracle_matches_numpy_restatement():
+    """The C brute force against a float32 numpy restatement of the same
+    arithmetic (squared distance summed x, y, z; K smallest; float square
+    roots summed in ascending order; double statistics)."""
+    rng = np.random.default_rng(5)
+    pts = rng.normal(0, 1, (600, 3)).astype(np.float32)
+    pts[:20] *= 8  # a few far points
+    K, fac = 6, 1.5
+    keep, mk = O.port_sor(pts, K, fac)
+    d = pts[:, None, :] - pts[None, :, :]
+    d2 = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+    np.fill_diagonal(d2, np.inf)
+    nn = np.sort(d2, axis=1)[:, :K]
+    want = np.zeros(len(pts), np.float32)
+    for m in range(K):
+        want = want + np.sqrt(nn[:, m])
+    want = want / np.float32(K)
+    assert np.array_equal(mk, want)
+    s = 0.0
+    s2 = 0.0
+    for v in want.astype(np.float64):
+        s += v
+        s2 += v * v
+    mean = s / len(pts)
+    thr = np.float32(mean + np.float64(np.float32(fac)) * np.sqrt(max(0.0, s2 / len(pts) - mean * mean)))
+    assert np.array_equal(keep, want <= thr)
+    assert 0 < (~keep).sum() < 40
