@@ -422,6 +422,47 @@ dn_status dn_sor_filter(const float* points, int64_t n, int knn, float stddev_fa
 const char* dn_fuser_last_error(void);
 
 /* ----------------------------------------------------------------------
+ * SVOFuser (svo_fuser.h:14-68, svo_fuser.cc:12-183; kernels
+ * svo_opencl_kernels.h:187-651): TSDF fusion of depthmaps into a sparse
+ * voxel hash (one 64-bit key per voxel, fixed-point integer sums), then
+ * surface points where the TSDF changes sign between a voxel and its +X,
+ * +Y or +Z neighbour.  Points come in ascending voxel order (x, y, z
+ * signed), +X, +Y, +Z per voxel.  FP32 in the kernel source's order.
+ * Defaults: voxel 0.02, truncation 4 voxels, minimum weight 3.
+ * ---------------------------------------------------------------------- */
+typedef struct dn_svo dn_svo;
+dn_status dn_svo_create(dn_svo** out);
+dn_status dn_svo_destroy(dn_svo* f);
+/* SetVoxelSize / SetTruncFactor / SetMinWeight (svo_fuser.cc:15-21),
+ * clamped to >= 1e-6, >= 1, >= 0 as the reference does. */
+dn_status dn_svo_set_voxel_size(dn_svo* f, float size);
+dn_status dn_svo_set_trunc_factor(dn_svo* f, float factor);
+dn_status dn_svo_set_min_weight(dn_svo* f, float w);
+/* SetDevice (svo_fuser.cc:23): before the first add_view. */
+dn_status dn_svo_set_device(dn_svo* f, int device);
+/* SetBBox (svo_fuser.cc:25-31): clip to the voxels of [min, max] (world). */
+dn_status dn_svo_set_bbox(dn_svo* f, const float min_world[3], const float max_world[3]);
+/* AddView (svo_fuser.cc:37-50): depth f32 [H][W]; normal f32 [H][W][3]
+ * (camera frame), color u8 [H][W][3], mask u8 [H][W] (0 = skip), weight
+ * f32 [H][W] (confidence): each may be NULL. */
+dn_status dn_svo_add_view(dn_svo* f, const double K[9], const double R[9], const double t[3],
+                          const float* depth, const float* normal, const uint8_t* color,
+                          const uint8_t* mask, const float* weight, int width, int height);
+/* CountVoxels (svo_fuser.cc:52-106): distinct voxels the views' truncation
+ * bands touch; 0 without views. */
+dn_status dn_svo_count_voxels(dn_svo* f, uint32_t* count);
+/* Fuse (svo_fuser.cc:108-183): *count receives the number of points.
+ * DN_INVALID_ARG if there are views but count_voxels has not run. */
+dn_status dn_svo_fuse(dn_svo* f, int64_t* count);
+/* The last fuse's points, unit normals and colours (rows of 3). */
+dn_status dn_svo_get(dn_svo* f, float* points, float* normals, uint8_t* colors,
+                     int64_t capacity);
+/* Device time (ms) of the last fuse: integration and extraction. */
+dn_status dn_svo_last_fuse_ms(dn_svo* f, float* ms);
+/* Message for the last failed dn_svo_* call on this thread. */
+const char* dn_svo_last_error(void);
+
+/* ----------------------------------------------------------------------
  * Depthmap files (host only, no GPU needed).  OpenSfM stores each view's
  * raw and cleaned depthmap as an .npz archive wrapped in one LZ4 frame
  * (opensfm/dataset.py:1080-1098 writes with lz4.frame.compress,

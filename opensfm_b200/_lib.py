@@ -125,6 +125,19 @@ _SIGNATURES = {
     "dn_fuser_last_error": ([], ctypes.c_char_p),
     "dn_fuser_last_removal_ms": ([_vp, ctypes.POINTER(ctypes.c_float)], _i),
     "dn_sor_filter": ([_f, ctypes.c_int64, _i, ctypes.c_float, _u8, _f], _i),
+    "dn_svo_create": ([ctypes.POINTER(_vp)], _i),
+    "dn_svo_destroy": ([_vp], _i),
+    "dn_svo_set_voxel_size": ([_vp, ctypes.c_float], _i),
+    "dn_svo_set_trunc_factor": ([_vp, ctypes.c_float], _i),
+    "dn_svo_set_min_weight": ([_vp, ctypes.c_float], _i),
+    "dn_svo_set_device": ([_vp, _i], _i),
+    "dn_svo_set_bbox": ([_vp, _f, _f], _i),
+    "dn_svo_add_view": ([_vp, _d, _d, _d, _f, _f, _u8, _u8, _f, _i, _i], _i),
+    "dn_svo_count_voxels": ([_vp, ctypes.POINTER(ctypes.c_uint32)], _i),
+    "dn_svo_fuse": ([_vp, ctypes.POINTER(ctypes.c_int64)], _i),
+    "dn_svo_get": ([_vp, _f, _f, _u8, ctypes.c_int64], _i),
+    "dn_svo_last_fuse_ms": ([_vp, ctypes.POINTER(ctypes.c_float)], _i),
+    "dn_svo_last_error": ([], ctypes.c_char_p),
     "dn_xxh32": ([_vp, ctypes.c_int64, ctypes.c_uint32], ctypes.c_uint32),
     "dn_lz4f_compress_bound": ([ctypes.c_int64], ctypes.c_int64),
     "dn_lz4f_compress": ([_vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],

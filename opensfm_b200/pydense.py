@@ -28,7 +28,7 @@ from . import _lib
 from ._lib import _d, _f, _i32, _u8, check, ptr
 
 __all__ = ["DepthmapEstimator", "DepthmapCleaner", "DepthmapPruner", "GPUDepthmapCleaner",
-           "DepthmapFuser", "Batch", "postprocess_depth", "sor_filter", "fp32_peak"]
+           "DepthmapFuser", "SVOFuser", "Batch", "postprocess_depth", "sor_filter", "fp32_peak"]
 
 
 def postprocess_depth(depth: np.ndarray) -> np.ndarray:
@@ -358,6 +358,109 @@ class DepthmapFuser(_Handle):
         clr = np.zeros((n, 3), np.uint8)
         self._check(self._L.dn_fuser_get(self._h, ptr(pts, _f), ptr(nrm, _f), ptr(clr, _u8), n))
         return [pts, nrm, clr]
+
+
+class SVOFuser(_Handle):
+    """``dense::SVOFuser`` (``svo_fuser.h:14-68``, bound at
+    ``python/pybind.cc:37-51``): TSDF fusion into a sparse voxel hash on the
+    B200, surface points at the TSDF's zero crossings.  Points come in
+    ascending voxel order (the reference's order follows an atomic counter)."""
+
+    def __init__(self) -> None:
+        super().__init__("dn_svo_create", "dn_svo_destroy")
+        self._counted = False
+
+    def _check(self, st: int) -> None:
+        if st == _lib.DN_OK:
+            return
+        msg = self._L.dn_svo_last_error().decode(errors="replace")
+        if st == _lib.DN_INVALID_ARG:
+            raise ValueError(msg)
+        if st == _lib.DN_OUT_OF_MEMORY:
+            raise MemoryError(msg)
+        raise _lib.DenseError(st, msg)
+
+    @staticmethod
+    def is_gpu_available() -> bool:
+        try:
+            return GPUDepthmapCleaner.is_available()
+        except Exception:
+            return False
+
+    def set_voxel_size(self, size: float) -> None:
+        self._check(self._L.dn_svo_set_voxel_size(self._h, float(size)))
+
+    def set_trunc_factor(self, factor: float) -> None:
+        self._check(self._L.dn_svo_set_trunc_factor(self._h, float(factor)))
+
+    def set_min_weight(self, w: float) -> None:
+        self._check(self._L.dn_svo_set_min_weight(self._h, float(w)))
+
+    def set_device(self, device_idx: int) -> None:
+        self._check(self._L.dn_svo_set_device(self._h, int(device_idx)))
+
+    def set_bbox(self, min_world, max_world) -> None:
+        lo = np.ascontiguousarray(min_world, dtype=np.float32).reshape(3)
+        hi = np.ascontiguousarray(max_world, dtype=np.float32).reshape(3)
+        self._check(self._L.dn_svo_set_bbox(self._h, ptr(lo, _f), ptr(hi, _f)))
+
+    def add_view(self, K, R, t, depth, normal, color, mask, confidence=None,
+                 name: str = "") -> None:
+        K = _mat(K, (3, 3), "K")
+        R = _mat(R, (3, 3), "R")
+        t = _mat(t, (3,), "t")
+        d = np.ascontiguousarray(depth, dtype=np.float32)
+        if d.ndim != 2:
+            raise ValueError("depth must be a 2-D array")
+        H, W = d.shape
+        n = np.ascontiguousarray(normal, dtype=np.float32)
+        c = np.ascontiguousarray(color, dtype=np.uint8)
+        if n.ndim != 3 or n.shape[:2] != (H, W):
+            raise ValueError("depth and normal must have matching shapes.")
+        if c.ndim != 3 or c.shape[:2] != (H, W):
+            raise ValueError("depth and color must have matching shapes.")
+        if n.shape[2] != 3 or c.shape[2] != 3:
+            raise ValueError("normal and color must have 3 channels")
+        m = None
+        if mask is not None and np.asarray(mask).size:
+            m = np.ascontiguousarray(mask, dtype=np.uint8)
+            if m.shape != (H, W):
+                raise ValueError("mask must have the depth's shape")
+        w = None
+        if confidence is not None:
+            cf = np.ascontiguousarray(confidence, dtype=np.float32)
+            if cf.shape == (H, W):  # any other shape is ignored, as the reference does
+                w = cf
+        self._check(self._L.dn_svo_add_view(
+            self._h, ptr(K, _d), ptr(R, _d), ptr(t, _d), ptr(d, _f), ptr(n, _f), ptr(c, _u8),
+            ptr(m, _u8) if m is not None else None, ptr(w, _f) if w is not None else None,
+            W, H))
+
+    def count_voxels(self) -> int:
+        n = ctypes.c_uint32()
+        self._check(self._L.dn_svo_count_voxels(self._h, ctypes.byref(n)))
+        self._counted = self._counted or n.value > 0
+        return int(n.value)
+
+    def fuse(self) -> list:
+        cnt = ctypes.c_int64()
+        st = self._L.dn_svo_fuse(self._h, ctypes.byref(cnt))
+        if st == _lib.DN_INVALID_ARG:
+            # The reference throws std::runtime_error here.
+            raise RuntimeError(self._L.dn_svo_last_error().decode(errors="replace"))
+        self._check(st)
+        n = int(cnt.value)
+        pts = np.zeros((n, 3), np.float32)
+        nrm = np.zeros((n, 3), np.float32)
+        clr = np.zeros((n, 3), np.uint8)
+        self._check(self._L.dn_svo_get(self._h, ptr(pts, _f), ptr(nrm, _f), ptr(clr, _u8), n))
+        return [pts, nrm, clr]
+
+    def last_fuse_ms(self) -> float:
+        """Device time of the last fuse (integration and extraction)."""
+        ms = ctypes.c_float()
+        self._check(self._L.dn_svo_last_fuse_ms(self._h, ctypes.byref(ms)))
+        return float(ms.value)
 
 
 def sor_filter(points, knn: int = 12, stddev_factor: float = 2.5):

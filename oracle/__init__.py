@@ -579,3 +579,86 @@ def port_sor(points, knn, stddev_factor):
     mk = np.zeros(len(p), np.float32)
     L.or_sor(_P(p, _f), len(p), int(knn), float(stddev_factor), _P(keep, _u8), _P(mk, _f))
     return keep.astype(bool), mk
+
+
+class _SvoView(ctypes.Structure):
+    _fields_ = [("K", ctypes.c_void_p), ("R", ctypes.c_void_p), ("t", ctypes.c_void_p),
+                ("W", ctypes.c_int), ("H", ctypes.c_int), ("depth", ctypes.c_void_p),
+                ("normal", ctypes.c_void_p), ("color", ctypes.c_void_p),
+                ("mask", ctypes.c_void_p), ("weight", ctypes.c_void_p)]
+
+
+def _svo_views(views):
+    keep = []
+    arr = (_SvoView * max(len(views), 1))()
+    for k, v in enumerate(views):
+        K = np.ascontiguousarray(v["K"], np.float64)
+        R = np.ascontiguousarray(v["R"], np.float64)
+        t = np.ascontiguousarray(v["t"], np.float64).reshape(3)
+        d = np.ascontiguousarray(v["depth"], np.float32)
+        H, W = d.shape
+
+        def opt(name, dt):
+            a = v.get(name)
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dt)
+            keep.append(a)
+            return a.ctypes.data
+
+        keep += [K, R, t, d]
+        arr[k] = _SvoView(K.ctypes.data, R.ctypes.data, t.ctypes.data, W, H, d.ctypes.data,
+                          opt("normal", np.float32), opt("color", np.uint8),
+                          opt("mask", np.uint8), opt("weight", np.float32))
+    return arr, keep
+
+
+def _svo_lib():
+    L = port()
+    if not getattr(L, "_svo_ready", False):
+        fp3 = ctypes.POINTER(ctypes.c_float)
+        L.or_svo_count.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                   fp3, fp3]
+        L.or_svo_count.restype = ctypes.c_long
+        L.or_svo_fuse.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                  ctypes.c_float, fp3, fp3, ctypes.c_long, _f, _f, _u8,
+                                  ctypes.c_long]
+        L.or_svo_fuse.restype = ctypes.c_long
+        L._svo_ready = True
+    return L
+
+
+def port_svo(views, voxel_size=0.02, trunc_factor=4.0, min_weight=3.0, bbox=None):
+    """SVOFuser (svo_fuser.cc:52-183 over the kernels of
+    svo_opencl_kernels.h:187-651) in the C restatement.  views: dicts with K,
+    R, t, depth (H, W) and optional normal (H, W, 3), color (H, W, 3) uint8,
+    mask (H, W) uint8, weight (H, W) f32.  bbox: (min_world, max_world) or
+    None.  The setters' clamps (svo_fuser.cc:15-21) are applied here.
+    Returns (count, points (N, 3) f32, normals (N, 3) f32, colors (N, 3) u8),
+    the points in ascending voxel order, +X, +Y, +Z per voxel."""
+    L = _svo_lib()
+    vs = max(1e-6, float(np.float32(voxel_size)))
+    tf = max(1.0, float(np.float32(trunc_factor)))
+    mw = max(0.0, float(np.float32(min_weight)))
+    arr, keep = _svo_views(views)
+    if bbox is not None:
+        bmin = np.ascontiguousarray(bbox[0], np.float32).reshape(3)
+        bmax = np.ascontiguousarray(bbox[1], np.float32).reshape(3)
+        pb = (_P(bmin, _f), _P(bmax, _f))
+    else:
+        pb = (None, None)
+    n_views = len(views)
+    cnt = L.or_svo_count(ctypes.cast(arr, ctypes.c_void_p), n_views, vs, tf, *pb)
+    if cnt < 0:
+        raise MemoryError("or_svo_count")
+    n = L.or_svo_fuse(ctypes.cast(arr, ctypes.c_void_p), n_views, vs, tf, mw, *pb, cnt,
+                      None, None, None, 0)
+    if n < 0:
+        raise MemoryError("or_svo_fuse")
+    pts = np.zeros((max(n, 1), 3), np.float32)
+    nrm = np.zeros((max(n, 1), 3), np.float32)
+    clr = np.zeros((max(n, 1), 3), np.uint8)
+    L.or_svo_fuse(ctypes.cast(arr, ctypes.c_void_p), n_views, vs, tf, mw, *pb, cnt,
+                  _P(pts, _f), _P(nrm, _f), _P(clr, _u8), n)
+    del keep
+    return int(cnt), pts[:n].copy(), nrm[:n].copy(), clr[:n].copy()

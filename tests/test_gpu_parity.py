@@ -530,6 +530,75 @@ def test_sor_filter_bit_identical_to_oracle(knn, factor):
         pydense.sor_filter(pts, 65, 1.0)
 
 
+def _svo_views(scene, seed=3):
+    Ks, Rs, ts = cams(scene)
+    rng = np.random.default_rng(seed)
+    views = []
+    for k in range(len(scene.images)):
+        d = scene.depths[k]
+        H, W = d.shape
+        dn = (d * (1 + 0.001 * rng.standard_normal(d.shape))).astype(np.float32)
+        dn[rng.random(d.shape) < 0.02] = 0
+        nrm = np.zeros((H, W, 3), np.float32)
+        nrm[..., 2] = -1.0
+        nrm[..., :2] = 0.3 * rng.standard_normal((H, W, 2))
+        nrm[rng.random((H, W)) < 0.05] = 0  # no normal: no grazing test
+        col = np.stack([scene.images[k], 255 - scene.images[k], scene.images[k] // 3], -1)
+        mask = (rng.random((H, W)) > 0.1).astype(np.uint8) if k % 2 else None
+        conf = rng.uniform(0, 3, (H, W)).astype(np.float32) if k % 3 == 1 else None
+        views.append(dict(K=Ks[k], R=Rs[k], t=ts[k], depth=dn, normal=nrm, color=col,
+                          mask=mask, weight=conf))
+    return views
+
+
+@pytest.mark.parametrize("params", [
+    dict(voxel_size=0.1, trunc_factor=4.0, min_weight=1.0),
+    dict(voxel_size=0.06, trunc_factor=2.5, min_weight=2.0),
+    dict(voxel_size=0.08, trunc_factor=1.0, min_weight=0.0, bbox=([-3, -3, -1], [3, 2, 2])),
+])
+def test_svo_fuser_bit_identical_to_oracle(scene, params):
+    """SVOFuser (one-word hash keys, all views in one march, sorted
+    extraction) against its C restatement: noisy depths, per-pixel normals
+    (some missing), colours, masks and confidences on some views; identical
+    voxel count and identical points, normals and colours in voxel order."""
+    views = _svo_views(scene)
+    want_cnt, wp, wn, wc = O.port_svo(views, **params)
+    f = pydense.SVOFuser()
+    f.set_voxel_size(params["voxel_size"])
+    f.set_trunc_factor(params["trunc_factor"])
+    f.set_min_weight(params["min_weight"])
+    if "bbox" in params:
+        f.set_bbox(*params["bbox"])
+    for v in views:
+        f.add_view(v["K"], v["R"], v["t"], v["depth"], v["normal"], v["color"], v["mask"],
+                   confidence=v["weight"])
+    with pytest.raises(RuntimeError):
+        f.fuse()  # count_voxels first, as the reference requires
+    cnt = f.count_voxels()
+    pts, nrm, clr = f.fuse()
+    print("voxels", cnt, "points", len(pts), "ms", f.last_fuse_ms())
+    assert cnt == want_cnt and len(wp) > 500
+    assert np.array_equal(pts, wp) and np.array_equal(nrm, wn) and np.array_equal(clr, wc)
+
+
+def test_svo_fuser_edges(scene):
+    f = pydense.SVOFuser()
+    assert f.count_voxels() == 0 and all(len(a) == 0 for a in f.fuse())
+    v = _svo_views(scene)[0]
+    with pytest.raises(ValueError):
+        f.add_view(v["K"], v["R"], v["t"], v["depth"], v["normal"][:-1], v["color"], None)
+    # A confidence of another shape is ignored, as the reference does.
+    f.set_voxel_size(0.1)
+    f.set_min_weight(0.5)
+    f.add_view(v["K"], v["R"], v["t"], v["depth"], v["normal"], v["color"], None,
+               confidence=np.ones((3, 3), np.float32))
+    f.count_voxels()
+    got = f.fuse()
+    v2 = dict(v, mask=None, weight=None)
+    want = O.port_svo([v2], voxel_size=0.1, min_weight=0.5)
+    assert all(np.array_equal(a, b) for a, b in zip(got, want[1:]))
+
+
 def test_invalid_arguments_raise(scene):
     e = pydense.DepthmapEstimator()
     with pytest.raises(ValueError):

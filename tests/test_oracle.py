@@ -327,3 +327,39 @@ def test_sor_oracle_matches_numpy_restatement():
     thr = np.float32(mean + np.float64(np.float32(fac)) * np.sqrt(max(0.0, s2 / len(pts) - mean * mean)))
     assert np.array_equal(keep, want <= thr)
     assert 0 < (~keep).sum() < 40
+
+
+def _plane_view(Z=2.0, W=64, H=48, f=60.0, color=(100, 150, 200)):
+    K = np.array([[f, 0, W / 2], [0, f, H / 2], [0, 0, 1.0]])
+    nrm = np.zeros((H, W, 3), np.float32)
+    nrm[..., 2] = -1.0
+    return dict(K=K, R=np.eye(3), t=np.zeros(3), depth=np.full((H, W), Z, np.float32),
+                normal=nrm, color=np.tile(np.array(color, np.uint8), (H, W, 1)))
+
+
+def test_svo_oracle_known_answers():
+    """SVO fusion restatement on a fronto-parallel plane seen by a camera at
+    the origin: the TSDF's zero crossing lies on the plane, the normals are
+    the plane's, the colour is the views' (within the truncation of the
+    weighted average), and the counting pass covers every fused voxel."""
+    v = _plane_view()
+    cnt, pts, nrm, clr = O.port_svo([v], voxel_size=0.05, trunc_factor=4.0, min_weight=1.0)
+    assert len(pts) > 100 and cnt >= len(pts) // 3
+    assert np.all(np.abs(pts[:, 2] - 2.0) < 1e-3)
+    assert np.allclose(nrm, [0, 0, -1], atol=1e-6)
+    assert np.all(np.abs(clr.astype(int) - [100, 150, 200]) <= 1)
+    # min_weight above what the view gives: nothing is extracted.
+    assert len(O.port_svo([v], voxel_size=0.05, min_weight=1e4)[1]) == 0
+    # The same view twice doubles every sum: the averages, the voxels and
+    # the points stay the same.
+    cnt2, pts2, _, _ = O.port_svo([v, v], voxel_size=0.05, min_weight=1.0)
+    assert cnt2 == cnt and np.array_equal(pts2, pts)
+    # A box around part of the plane keeps only its voxels.
+    _, pb, _, _ = O.port_svo([v], voxel_size=0.05, min_weight=1.0,
+                             bbox=([-0.5, -0.5, 1.5], [0.0, 0.5, 2.5]))
+    assert 0 < len(pb) < len(pts)
+    assert np.all(pb[:, 0] <= 0.0 + 0.05) and np.all(pb[:, 0] >= -0.5 - 0.05)
+    # Points come in ascending voxel order.
+    k = np.floor(pts / 0.05).astype(np.int64)
+    order = np.lexsort((k[:, 2], k[:, 1], k[:, 0]))
+    assert np.array_equal(order, np.arange(len(pts))) or len(np.unique(k, axis=0)) < len(k)
