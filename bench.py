@@ -165,6 +165,42 @@ def fusion_leg(b, vs, cands, n_maps, repeats=3, oracle=True):
         want = O.port_fuse(views)
         out["oracle_1thread_s"] = time.perf_counter() - t0
         out["identical_to_oracle"] = bool(all(np.array_equal(a, w) for a, w in zip(got, want)))
+    out["svo"] = svo_leg(views, repeats, oracle)
+    return out
+
+
+def svo_leg(views, repeats=3, oracle=True, voxel_size=0.05, trunc_factor=4.0, min_weight=3.0):
+    """SVOFuser (TSDF fusion) over the same views: count_voxels() + fuse()
+    timed on the host clock, the device time of the fuse, and with `oracle`
+    the single-thread C restatement and an identity check."""
+    from opensfm_b200 import pydense
+
+    f = pydense.SVOFuser()
+    f.set_voxel_size(voxel_size)
+    f.set_trunc_factor(trunc_factor)
+    f.set_min_weight(min_weight)
+    for v in views:
+        f.add_view(v["K"], v["R"], v["t"], v["depth"], v["normal"], v["color"], None)
+    f.count_voxels()
+    f.fuse()  # warm-up
+    ts = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        n_vox = f.count_voxels()
+        got = f.fuse()
+        ts.append(time.perf_counter() - t0)
+    out = {"voxel_size": voxel_size, "trunc_factor": trunc_factor, "min_weight": min_weight,
+           "voxels": int(n_vox), "points": int(len(got[0])), "count_and_fuse_s": float(np.median(ts)),
+           "fuse_device_ms": f.last_fuse_ms()}
+    if oracle:
+        import oracle as O
+
+        t0 = time.perf_counter()
+        cnt, wp, wn, wc = O.port_svo([dict(v, mask=None) for v in views], voxel_size=voxel_size,
+                                     trunc_factor=trunc_factor, min_weight=min_weight)
+        out["oracle_1thread_s"] = time.perf_counter() - t0
+        out["identical_to_oracle"] = bool(cnt == n_vox and all(
+            np.array_equal(a, w) for a, w in zip(got, (wp, wn, wc))))
     return out
 
 
