@@ -463,6 +463,65 @@ dn_status dn_svo_last_fuse_ms(dn_svo* f, float* ms);
 const char* dn_svo_last_error(void);
 
 /* ----------------------------------------------------------------------
+ * DepthmapClusterEstimator (cluster.h, cluster_estimator.cc:21-147, bound
+ * at python/pybind.cc:53-104) over the live path's PatchMatch estimator
+ * (estimator.cc:120-243, 941-1040; kernels opencl_kernels.h:44-1124,
+ * 1298-1826, 1897-2099): one pyramid level, no SfM planar prior.  Per
+ * reference view: random initialisation, then red/black PatchMatch passes
+ * (bilateral NCC over strides 1-3, census fallback, joint view selection,
+ * refinement) and a checkerboard median filter per iteration; readback
+ * with a 5x5 median rejection and a logistic confidence.  FP32 with every
+ * operation rounded by itself and the library's own exp / log.
+ * Defaults: 3 iterations, patch 11, sigma 5 / (3/255), top-k 4, census
+ * weight 0.3, smoothness 0, one level.
+ * ---------------------------------------------------------------------- */
+typedef struct dn_acmmp dn_acmmp;
+dn_status dn_acmmp_create(dn_acmmp** out);
+dn_status dn_acmmp_destroy(dn_acmmp* e);
+/* DepthmapParams setters (depthmap_bind.h:21-33). */
+dn_status dn_acmmp_set_max_iterations(dn_acmmp* e, int n);
+dn_status dn_acmmp_set_patch_size(dn_acmmp* e, int size);
+dn_status dn_acmmp_set_max_image_size(dn_acmmp* e, int size);
+/* Levels above 1 make dn_acmmp_run fail with DN_INVALID_ARG. */
+dn_status dn_acmmp_set_hierarchy_levels(dn_acmmp* e, int levels);
+dn_status dn_acmmp_set_sigma_spatial(dn_acmmp* e, float v);
+dn_status dn_acmmp_set_sigma_color(dn_acmmp* e, float v);
+dn_status dn_acmmp_set_top_k(dn_acmmp* e, int k);
+dn_status dn_acmmp_set_census_weight(dn_acmmp* e, float w);
+dn_status dn_acmmp_set_smooth_weight(dn_acmmp* e, float w);
+dn_status dn_acmmp_set_geom_consistency_weight(dn_acmmp* e, float w);
+dn_status dn_acmmp_set_device(dn_acmmp* e, int device);
+/* BeginRefView (cluster_estimator.cc:41-53): image u8 [h][stride]; *ref_idx
+ * (may be NULL) receives the reference's index. */
+dn_status dn_acmmp_begin_ref_view(dn_acmmp* e, const double K[9], const double R[9],
+                                  const double t[3], const uint8_t* image, int width, int height,
+                                  int stride, float depth_min, float depth_max, int* ref_idx);
+/* AddSourceView (cluster_estimator.cc:55-62): a source of the last reference
+ * (at most 16 are used). */
+dn_status dn_acmmp_add_source_view(dn_acmmp* e, const double K[9], const double R[9],
+                                   const double t[3], const uint8_t* image, int width, int height,
+                                   int stride);
+/* SetSfMPoints: only n = 0 is accepted (the planar prior is not built). */
+dn_status dn_acmmp_set_sfm_points(dn_acmmp* e, const double* points, int64_t n);
+/* AddGeomLink (cluster_estimator.cc:73-80): stored; it acts only between
+ * pyramid levels. */
+dn_status dn_acmmp_add_geom_link(dn_acmmp* e, int ref_idx, int source_view_idx, int from_ref_idx);
+/* Run (cluster_estimator.cc:82-138): every reference view in turn. */
+dn_status dn_acmmp_run(dn_acmmp* e);
+dn_status dn_acmmp_num_refs(dn_acmmp* e, int* n);
+dn_status dn_acmmp_result_size(dn_acmmp* e, int ref_idx, int* width, int* height);
+/* A reference's result: depth [H][W], normal [H][W][3], cost, confidence;
+ * any pointer may be NULL.  DN_OUT_OF_RANGE for a bad index. */
+dn_status dn_acmmp_get_result(dn_acmmp* e, int ref_idx, float* depth, float* normal, float* cost,
+                              float* confidence);
+/* Device time (ms) of the last run's kernels, over all references. */
+dn_status dn_acmmp_last_run_ms(dn_acmmp* e, float* ms);
+/* Clear (cluster_estimator.cc:140). */
+dn_status dn_acmmp_clear(dn_acmmp* e);
+/* Message for the last failed dn_acmmp_* call on this thread. */
+const char* dn_acmmp_last_error(void);
+
+/* ----------------------------------------------------------------------
  * Depthmap files (host only, no GPU needed).  OpenSfM stores each view's
  * raw and cleaned depthmap as an .npz archive wrapped in one LZ4 frame
  * (opensfm/dataset.py:1080-1098 writes with lz4.frame.compress,

@@ -138,6 +138,31 @@ _SIGNATURES = {
     "dn_svo_get": ([_vp, _f, _f, _u8, ctypes.c_int64], _i),
     "dn_svo_last_fuse_ms": ([_vp, ctypes.POINTER(ctypes.c_float)], _i),
     "dn_svo_last_error": ([], ctypes.c_char_p),
+    "dn_acmmp_create": ([ctypes.POINTER(_vp)], _i),
+    "dn_acmmp_destroy": ([_vp], _i),
+    "dn_acmmp_set_max_iterations": ([_vp, _i], _i),
+    "dn_acmmp_set_patch_size": ([_vp, _i], _i),
+    "dn_acmmp_set_max_image_size": ([_vp, _i], _i),
+    "dn_acmmp_set_hierarchy_levels": ([_vp, _i], _i),
+    "dn_acmmp_set_sigma_spatial": ([_vp, ctypes.c_float], _i),
+    "dn_acmmp_set_sigma_color": ([_vp, ctypes.c_float], _i),
+    "dn_acmmp_set_top_k": ([_vp, _i], _i),
+    "dn_acmmp_set_census_weight": ([_vp, ctypes.c_float], _i),
+    "dn_acmmp_set_smooth_weight": ([_vp, ctypes.c_float], _i),
+    "dn_acmmp_set_geom_consistency_weight": ([_vp, ctypes.c_float], _i),
+    "dn_acmmp_set_device": ([_vp, _i], _i),
+    "dn_acmmp_begin_ref_view": ([_vp, _d, _d, _d, _u8, _i, _i, _i, ctypes.c_float,
+                                 ctypes.c_float, ctypes.POINTER(_i)], _i),
+    "dn_acmmp_add_source_view": ([_vp, _d, _d, _d, _u8, _i, _i, _i], _i),
+    "dn_acmmp_set_sfm_points": ([_vp, _d, ctypes.c_int64], _i),
+    "dn_acmmp_add_geom_link": ([_vp, _i, _i, _i], _i),
+    "dn_acmmp_run": ([_vp], _i),
+    "dn_acmmp_num_refs": ([_vp, ctypes.POINTER(_i)], _i),
+    "dn_acmmp_result_size": ([_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i)], _i),
+    "dn_acmmp_get_result": ([_vp, _i, _f, _f, _f, _f], _i),
+    "dn_acmmp_last_run_ms": ([_vp, ctypes.POINTER(ctypes.c_float)], _i),
+    "dn_acmmp_clear": ([_vp], _i),
+    "dn_acmmp_last_error": ([], ctypes.c_char_p),
     "dn_xxh32": ([_vp, ctypes.c_int64, ctypes.c_uint32], ctypes.c_uint32),
     "dn_lz4f_compress_bound": ([ctypes.c_int64], ctypes.c_int64),
     "dn_lz4f_compress": ([_vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],

@@ -14,7 +14,10 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_build", "libdense_b200.so")
 SOURCES = ["kernels.cu", "cleanprune.cu", "learned.cu", "api.cu", "noalloc.cu", "lz4io.cu",
-           "fuser.cu", "svo.cu"]
+           "fuser.cu", "svo.cu", "acmmp.cu"]
+# Per-file flags: the live-path estimator fixes its arithmetic without FMA
+# contraction (every operation rounded by itself, as its C oracle).
+FILE_FLAGS = {"acmmp.cu": ["--fmad=false"]}
 HEADERS = ["common.cuh", "kernels.h", "learned.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -39,7 +42,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     objs = []
     for s in srcs:
         o = os.path.join(os.path.dirname(LIB), os.path.basename(s) + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", s, "-o", o]
+        cmd = [NVCC, *ARCH, *FLAGS, *FILE_FLAGS.get(os.path.basename(s), []), "-c", s, "-o", o]
         if ptxas_v:
             cmd += ["-Xptxas", "-v"]
         if verbose:

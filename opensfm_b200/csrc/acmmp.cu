@@ -1,0 +1,1061 @@
+// DepthmapClusterEstimator (cluster.h, cluster_estimator.cc:21-147) over the
+// live path's PatchMatch estimator (estimator.h:33-135, estimator.cc:120-243,
+// 473-558, 941-1040) and its kernels (opencl_kernels.h:44-1124, 1298-1826,
+// 1897-2099): one pyramid level, no SfM planar prior.
+//
+// Per reference view: a random initialisation with top-k view selection,
+// then per iteration a red and a black PatchMatch pass (8 propagation
+// candidates, multi-hypothesis joint view selection, 5 refinement
+// hypotheses; the matching cost is a bilateral NCC over strides 1, 2, 3
+// with a census-transform fallback and blend) and a red and a black
+// checkerboard median filter; then the readback (depth and normal from the
+// planes, a 5x5 median rejection, a logistic confidence).
+//
+// The reference's float results depend on its OpenCL device
+// (hardware-filtered image reads, exp/log/normalize precision,
+// contraction).  This file fixes one arithmetic, the one the C oracle
+// restates, and matches it bit for bit:
+//   - FP32, every operation rounded by itself in the written order: the
+//     file is compiled without FMA contraction (--fmad=false);
+//   - acm_exp / acm_log below (Cody-Waite reduction, fixed polynomials);
+//   - images as float(v) * float(1/255); linear, clamp-to-edge reads as the
+//     OpenCL specification defines them, with exact fractions;
+//   - normalize(v) = v / sqrt((x*x + y*y) + z*z).
+// Images live in HBM as FP32 planes; every kernel is one thread per pixel
+// (per pixel of the pass's colour), and the state (planes, costs, RNG
+// states, selected views) stays on the device between the passes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dense_b200.h"
+
+namespace {
+
+thread_local std::string g_acm_error;
+
+dn_status afail(dn_status s, const std::string& m) {
+  g_acm_error = m;
+  return s;
+}
+
+#define ACHECK(cond, msg) \
+  do {                    \
+    if (!(cond)) return afail(DN_INVALID_ARG, msg); \
+  } while (0)
+#define ACUDA(expr)                                                        \
+  do {                                                                     \
+    cudaError_t e_ = (expr);                                               \
+    if (e_ != cudaSuccess) {                                               \
+      return afail(e_ == cudaErrorMemoryAllocation ? DN_OUT_OF_MEMORY      \
+                                                   : DN_DEVICE_ERROR,      \
+                   cudaGetErrorString(e_));                                \
+    }                                                                      \
+  } while (0)
+
+constexpr int kMaxSrc = 16;  // MAX_SOURCES
+
+struct AImg {
+  const float* px;
+  int W, H;
+};
+struct ACam {
+  float K[9], R[9], t[3];
+};
+struct AScene {
+  AImg img[1 + kMaxSrc];  // [0] reference
+  ACam cam[1 + kMaxSrc];
+  int W, H, n_src, half_patch, top_k;
+  float sigma_spatial, sigma_color, census_weight, smooth_weight, geom_weight;
+  float depth_min, depth_max;
+};
+struct AState {
+  float4* planes;  // (nx, ny, nz, d): n . X + d = 0 in the camera frame
+  float* costs;
+  uint2* rs;
+  unsigned* sel;
+};
+
+// ------------------------------------------------------------ arithmetic
+__device__ inline float acm_ldexp(float p, int n) {
+  const int n1 = n / 2, n2 = n - n1;
+  if (n1 < -126 || n2 < -126 || n1 > 127 || n2 > 127) return n < 0 ? 0.0f : INFINITY;
+  return (p * __int_as_float((n1 + 127) << 23)) * __int_as_float((n2 + 127) << 23);
+}
+
+// e^x: n = round(x log2 e), r = x - n ln2 in two parts, degree-7 Taylor.
+__device__ inline float acm_exp(float x) {
+  if (x != x) return x;
+  if (x > 88.72283f) return INFINITY;
+  if (x < -103.97208f) return 0.0f;
+  const float t = x * 1.44269502f;
+  const float nf = floorf(t + 0.5f);
+  const int n = (int)nf;
+  const float r = (x - nf * 0.693145752f) - nf * 1.42860677e-06f;
+  float p = 1.98412701e-04f;
+  p = p * r + 1.38888892e-03f;
+  p = p * r + 8.33333377e-03f;
+  p = p * r + 4.16666679e-02f;
+  p = p * r + 1.66666672e-01f;
+  p = p * r + 0.5f;
+  p = p * r + 1.0f;
+  p = p * r + 1.0f;
+  return acm_ldexp(p, n);
+}
+
+// ln x: x = m 2^e, m in [sqrt(1/2), sqrt(2)), 2 atanh((m - 1) / (m + 1)).
+__device__ inline float acm_log(float x) {
+  if (!(x > 0.0f)) return x == 0.0f ? -INFINITY : NAN;
+  if (x == INFINITY) return x;
+  unsigned u = __float_as_uint(x);
+  int e = 0;
+  if (u < 0x00800000u) {
+    u = __float_as_uint(x * 16777216.0f);
+    e = -24;
+  }
+  e += (int)(u >> 23) - 127;
+  float m = __uint_as_float((u & 0x007FFFFFu) | 0x3F800000u);
+  if (m > 1.41421354f) {
+    m = m * 0.5f;
+    e += 1;
+  }
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float s2 = s * s;
+  float q = 0.0909090936f;
+  q = q * s2 + 0.111111112f;
+  q = q * s2 + 0.142857149f;
+  q = q * s2 + 0.200000003f;
+  q = q * s2 + 0.333333343f;
+  q = q * s2 + 1.0f;
+  const float lnm = 2.0f * (s * q);
+  const float ef = (float)e;
+  return (ef * 0.693145752f + lnm) + ef * 1.42860677e-06f;
+}
+
+__device__ inline float3 acm_normalize(float3 v) {
+  const float len = sqrtf((v.x * v.x + v.y * v.y) + v.z * v.z);
+  if (len == 0.0f) return v;
+  return make_float3(v.x / len, v.y / len, v.z / len);
+}
+
+__device__ inline float acm_clamp(float x, float lo, float hi) {
+  const float m = x > lo ? x : lo;
+  return m < hi ? m : hi;
+}
+
+__device__ inline int clampi(int i, int n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
+
+// read_imagef(linear, clamp-to-edge) at unnormalised (u, v).
+__device__ inline float acm_sample(const AImg& im, float u, float v) {
+  float xm = u - 0.5f, ym = v - 0.5f;
+  if (!(xm >= -16.0f)) xm = -16.0f;
+  if (!(xm <= (float)im.W + 16.0f)) xm = (float)im.W + 16.0f;
+  if (!(ym >= -16.0f)) ym = -16.0f;
+  if (!(ym <= (float)im.H + 16.0f)) ym = (float)im.H + 16.0f;
+  const float fx = floorf(xm), fy = floorf(ym);
+  const float a = xm - fx, b = ym - fy;
+  const int i0 = (int)fx, j0 = (int)fy;
+  const int xa = clampi(i0, im.W), xb = clampi(i0 + 1, im.W);
+  const int ya = clampi(j0, im.H), yb = clampi(j0 + 1, im.H);
+  const float* p = im.px;
+  const float t00 = __ldg(p + (size_t)ya * im.W + xa), t10 = __ldg(p + (size_t)ya * im.W + xb);
+  const float t01 = __ldg(p + (size_t)yb * im.W + xa), t11 = __ldg(p + (size_t)yb * im.W + xb);
+  return (((1.0f - a) * (1.0f - b)) * t00 + (a * (1.0f - b)) * t10) + ((1.0f - a) * b) * t01 +
+         (a * b) * t11;
+}
+
+__device__ inline float3 acm_project(const ACam& c, float3 X) {
+  const float x0 = ((c.R[0] * X.x + c.R[1] * X.y) + c.R[2] * X.z) + c.t[0];
+  const float x1 = ((c.R[3] * X.x + c.R[4] * X.y) + c.R[5] * X.z) + c.t[1];
+  const float x2 = ((c.R[6] * X.x + c.R[7] * X.y) + c.R[8] * X.z) + c.t[2];
+  return make_float3((c.K[0] * x0 + c.K[1] * x1) + c.K[2] * x2,
+                     (c.K[3] * x0 + c.K[4] * x1) + c.K[5] * x2,
+                     (c.K[6] * x0 + c.K[7] * x1) + c.K[8] * x2);
+}
+
+__device__ inline float3 acm_backproject(const ACam& c, float x, float y, float depth) {
+  const float px = depth * (x - c.K[2]) / c.K[0];
+  const float py = depth * (y - c.K[5]) / c.K[4];
+  const float d0 = px - c.t[0], d1 = py - c.t[1], d2 = depth - c.t[2];
+  return make_float3((c.R[0] * d0 + c.R[3] * d1) + c.R[6] * d2,
+                     (c.R[1] * d0 + c.R[4] * d1) + c.R[7] * d2,
+                     (c.R[2] * d0 + c.R[5] * d1) + c.R[8] * d2);
+}
+
+__device__ inline float acm_depth(const ACam& c, float x, float y, float4 pl) {
+  const float den = (pl.x * (x - c.K[2]) / c.K[0] + pl.y * (y - c.K[5]) / c.K[4]) + pl.z;
+  if (fabsf(den) < 1e-6f) return 0.0f;
+  return -pl.w / den;
+}
+
+__device__ inline float4 acm_plane(const ACam& c, float x, float y, float depth, float3 n) {
+  const float p0 = depth * (x - c.K[2]) / c.K[0];
+  const float p1 = depth * (y - c.K[5]) / c.K[4];
+  return make_float4(n.x, n.y, n.z, -((n.x * p0 + n.y * p1) + n.z * depth));
+}
+
+__device__ inline float acm_rand(uint2& st, unsigned key) {
+#pragma unroll
+  for (unsigned i = 0; i < 4; ++i) {
+    const unsigned k = key + i * 0x9E3779B9u;
+    const unsigned lo = st.x * 0xD256D193u, hi = __umulhi(st.x, 0xD256D193u);
+    st = make_uint2(st.y ^ k ^ hi, lo);
+  }
+  return (float)st.x / 4294967296.0f;
+}
+
+// ------------------------------------------------------------------ costs
+__device__ float ncc_at_stride(const AImg& ref, const AImg& src, float rc, float sc, float scx,
+                               float scy, int cx, int cy, int hp, float stride, float ax,
+                               float ay, float bx, float by, float sf, float cf) {
+  float sw = 0.0f, sr = 0.0f, ss = 0.0f, srr = 0.0f, sss = 0.0f, srs = 0.0f;
+  for (int iy = -hp; iy <= hp; ++iy)
+    for (int ix = -hp; ix <= hp; ++ix) {
+      const float fdx = stride * (float)ix, fdy = stride * (float)iy;
+      const float rv = acm_sample(ref, ((float)cx + fdx) + 0.5f, ((float)cy + fdy) + 0.5f);
+      const float sx = (scx + ax * fdx) + bx * fdy;
+      const float sy = (scy + ay * fdx) + by * fdy;
+      const float sv = acm_sample(src, sx + 0.5f, sy + 0.5f);
+      const float dist2 = fdx * fdx + fdy * fdy;
+      const float r = rv - rc;
+      const float w = acm_exp(dist2 * sf + (r * r) * cf);
+      const float s = sv - sc;
+      sr += w * r;
+      ss += w * s;
+      srr += (w * r) * r;
+      sss += (w * s) * s;
+      srs += (w * r) * s;
+      sw += w;
+    }
+  if (sw < 1e-6f) return -1.0f;
+  const float inv = 1.0f / sw;
+  const float mr = sr * inv, ms = ss * inv;
+  const float vr = srr * inv - mr * mr, vs = sss * inv - ms * ms;
+  if (vr < 1.5e-10f || vs < 1.5e-10f) return -1.0f;
+  return (srs * inv - mr * ms) / sqrtf(vr * vs);
+}
+
+__device__ float ncc_multiscale(const AImg& ref, const AImg& src, float rc, float sc, float scx,
+                                float scy, int cx, int cy, int hp, float ax, float ay, float bx,
+                                float by, float sf, float cf) {
+  float best = -1.0f;
+  bool textureless = false;
+  for (int s = 0; s < 3; ++s) {
+    float ncc = ncc_at_stride(ref, src, rc, sc, scx, scy, cx, cy, hp, (float)(s + 1), ax, ay, bx,
+                              by, sf, cf);
+    if (s == 0 && ncc < -0.5f) textureless = true;
+    if (textureless && ncc > 0.0f) ncc = 0.0f;
+    if (ncc > best) best = ncc;
+    if (best > 0.1f) return best;
+  }
+  return best;
+}
+
+__device__ float census(const AImg& ref, const AImg& src, float rc, float sc, int cx, int cy,
+                        float scx, float scy, float ax, float ay, float bx, float by) {
+  unsigned rb = 0, sb = 0;
+  int bit = 0;
+  for (int dy = -2; dy <= 2; ++dy)
+    for (int dx = -2; dx <= 2; ++dx) {
+      if (dx == 0 && dy == 0) continue;
+      const float rv = acm_sample(ref, (float)(cx + dx) + 0.5f, (float)(cy + dy) + 0.5f);
+      const float sx = (scx + ax * (float)dx) + bx * (float)dy;
+      const float sy = (scy + ay * (float)dx) + by * (float)dy;
+      const float sv = acm_sample(src, sx + 0.5f, sy + 0.5f);
+      if (rv > rc) rb |= 1u << bit;
+      if (sv > sc) sb |= 1u << bit;
+      ++bit;
+    }
+  const int ham = __popc(rb ^ sb);
+  if (__popc(rb) < 3 && __popc(sb) < 3) return 1.0f;
+  return (float)ham / 24.0f;
+}
+
+__device__ float single_cost(const AScene& S, int i, float3 cw, float3 wdx, float3 wdy, float rc,
+                             int cx, int cy, float sf, float cf) {
+  const ACam& c = S.cam[1 + i];
+  const AImg& ref = S.img[0];
+  const AImg& src = S.img[1 + i];
+  const float3 p = acm_project(c, cw);
+  if (p.z < 1e-6f) return 2.0f;
+  const float scx = p.x / p.z, scy = p.y / p.z;
+  const float3 pdx = acm_project(c, wdx), pdy = acm_project(c, wdy);
+  if (pdx.z < 1e-6f || pdy.z < 1e-6f) return 2.0f;
+  const float ax = pdx.x / pdx.z - scx, ay = pdx.y / pdx.z - scy;
+  const float bx = pdy.x / pdy.z - scx, by = pdy.y / pdy.z - scy;
+  const float sc = acm_sample(src, scx + 0.5f, scy + 0.5f);
+  const float ncc =
+      ncc_multiscale(ref, src, rc, sc, scx, scy, cx, cy, S.half_patch, ax, ay, bx, by, sf, cf);
+  if (ncc <= -0.5f) {
+    if (S.census_weight > 1e-6f) return census(ref, src, rc, sc, cx, cy, scx, scy, ax, ay, bx, by);
+    return 2.0f;
+  }
+  const float nc = 1.0f - ncc;
+  if (S.census_weight < 1e-6f) return nc;
+  const float t = acm_clamp((nc - 0.1f) / (0.6f - 0.1f), 0.0f, 1.0f);
+  const float blend = S.census_weight * ((t * t) * (3.0f - 2.0f * t));
+  if (blend < 1e-4f) return nc;
+  const float cen = census(ref, src, rc, sc, cx, cy, scx, scy, ax, ay, bx, by);
+  return (1.0f - blend) * nc + blend * cen;
+}
+
+// compute_cost_vector (opencl_kernels.h:659-750): out[0 .. n_src).
+__device__ void cost_vector(const AScene& S, int x, int y, float4 plane, float* out) {
+  const ACam& c0 = S.cam[0];
+  const float depth = acm_depth(c0, (float)x, (float)y, plane);
+  const float ddx = depth > 0.0f ? acm_depth(c0, (float)(x + 1), (float)y, plane) : 0.0f;
+  const float ddy = depth > 0.0f ? acm_depth(c0, (float)x, (float)(y + 1), plane) : 0.0f;
+  if (depth <= 0.0f || ddx <= 0.0f || ddy <= 0.0f) {
+    for (int i = 0; i < S.n_src; ++i) out[i] = 2.0f;
+    return;
+  }
+  const float3 cw = acm_backproject(c0, (float)x, (float)y, depth);
+  const float3 wdx = acm_backproject(c0, (float)(x + 1), (float)y, ddx);
+  const float3 wdy = acm_backproject(c0, (float)x, (float)(y + 1), ddy);
+  const float rc = acm_sample(S.img[0], (float)x + 0.5f, (float)y + 0.5f);
+  const float sf = -1.0f / (2.0f * S.sigma_spatial * S.sigma_spatial);
+  const float cf = -1.0f / (2.0f * S.sigma_color * S.sigma_color);
+  for (int i = 0; i < S.n_src; ++i) out[i] = single_cost(S, i, cw, wdx, wdy, rc, x, y, sf, cf);
+}
+
+__device__ float smoothness(const AScene& S, const float4* __restrict__ planes, float4 cur, int x,
+                            int y) {
+  const ACam& c = S.cam[0];
+  const float cd = acm_depth(c, (float)x, (float)y, cur);
+  if (cd <= 0.0f) return 0.0f;
+  const float3 cn = acm_normalize(make_float3(cur.x, cur.y, cur.z));
+  const float sig = 0.02f;
+  float tw = 0.0f, tc = 0.0f;
+  for (int k = 0; k < 4; ++k) {
+    const int nx = x + (k == 0 ? -1 : (k == 1 ? 1 : 0));
+    const int ny = y + (k == 2 ? -1 : (k == 3 ? 1 : 0));
+    if (nx < 0 || nx >= S.W || ny < 0 || ny >= S.H) continue;
+    const float4 nb = planes[(size_t)ny * S.W + nx];
+    const float nd = acm_depth(c, (float)nx, (float)ny, nb);
+    if (nd <= 0.0f) continue;
+    const float rel = fabsf(cd - nd) / cd;
+    const float w = acm_exp(-rel * rel / (2.0f * sig * sig));
+    const float3 nn = acm_normalize(make_float3(nb.x, nb.y, nb.z));
+    const float ncost = 1.0f - ((cn.x * nn.x + cn.y * nn.y) + cn.z * nn.z);
+    const float pred = acm_depth(c, (float)nx, (float)ny, cur);
+    const float dev = pred > 0.0f ? fabsf(nd - pred) / cd : 0.0f;
+    const float cost =
+        0.5f * acm_clamp(ncost, 0.0f, 1.0f) + 0.5f * acm_clamp(dev * 10.0f, 0.0f, 1.0f);
+    tc += w * cost;
+    tw += w;
+  }
+  if (tw < 1e-6f) return 0.0f;
+  return tc / tw;
+}
+
+// compute_weighted_cost_geom without previous-level depths (geometric term 0).
+__device__ inline float weighted(const float* cv, const float* vw, float norm, int n_src,
+                                 float geom_w) {
+  if (norm < 1e-6f) return 2.0f;
+  float total = 0.0f;
+  for (int i = 0; i < n_src; ++i)
+    if (vw[i] > 0.0f) total += vw[i] * (cv[i] + geom_w * 0.0f);
+  return total / norm;
+}
+
+// ---------------------------------------------------------------- kernels
+// acmmp_random_init (opencl_kernels.h:1055-1124), one thread per pixel.
+__global__ void acm_init_kernel(const AScene* __restrict__ Sp, AState st) {
+  const AScene& S = *Sp;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= S.W || y >= S.H) return;
+  const int idx = y * S.W + x;
+  uint2 s = make_uint2((unsigned)idx * 1099087573u + 2654435769u, (unsigned)idx * 2246822519u + 13u);
+  const unsigned key = (unsigned)(idx + 7919);
+  const float lmin = acm_log(S.depth_min > 1e-6f ? S.depth_min : 1e-6f);
+  const float lmax = acm_log(S.depth_max > 1e-5f ? S.depth_max : 1e-5f);
+  const float depth = acm_exp(lmin + acm_rand(s, key) * (lmax - lmin));
+  float3 n;
+  n.x = acm_rand(s, key + 3u) * 2.0f - 1.0f;
+  n.y = acm_rand(s, key + 5u) * 2.0f - 1.0f;
+  n.z = -1.0f;
+  n = acm_normalize(n);
+  const float4 pl = acm_plane(S.cam[0], (float)x, (float)y, depth, n);
+  st.planes[idx] = pl;
+  st.rs[idx] = s;
+  // compute_initial_cost_and_views (752-829): mean of the top-k costs and
+  // the views at or below the k-th.
+  float cv[kMaxSrc], cc[kMaxSrc];
+  for (int i = 0; i < kMaxSrc; ++i) cv[i] = cc[i] = 2.0f;
+  cost_vector(S, x, y, pl, cv);
+  int nv = 0;
+  for (int i = 0; i < S.n_src; ++i) {
+    cc[i] = cv[i];
+    nv += cv[i] < 2.0f;
+  }
+  for (int i = 1; i < S.n_src; ++i) {
+    const float tmp = cv[i];
+    int j = i;
+    for (; j >= 1 && tmp < cv[j - 1]; --j) cv[j] = cv[j - 1];
+    cv[j] = tmp;
+  }
+  unsigned sel = 0;
+  const int k = min(min(S.top_k, nv), S.n_src);
+  float cost = 2.0f;
+  if (k > 0) {
+    float total = 0.0f;
+    for (int i = 0; i < k; ++i) total += cv[i];
+    const float thr = cv[k - 1];
+    for (int i = 0; i < S.n_src; ++i)
+      if (cc[i] <= thr) sel |= 1u << i;
+    cost = total / (float)k;
+  }
+  st.costs[idx] = cost;
+  st.sel[idx] = sel;
+}
+
+// acmmp_patchmatch (opencl_kernels.h:1298-1826) for the pixels of one colour:
+// x = 2 gx + ((y + colour) & 1).
+__global__ void __launch_bounds__(64) acm_pm_kernel(const AScene* __restrict__ Sp, AState st,
+                                                    int colour, int iteration) {
+  const AScene& S = *Sp;
+  const int W = S.W, H = S.H, npix = W * H;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + colour) & 1);
+  if (x >= W || y >= H) return;
+  const int idx = y * W + x;
+  const ACam& c0 = S.cam[0];
+  uint2 s = st.rs[idx];
+  const unsigned key = (unsigned)(idx + iteration * 7919 + 42);
+  const int n_src = S.n_src;
+  const float* C = st.costs;
+  int pos[8];
+  bool flags[8];
+  float ca[8 * kMaxSrc];
+  for (int i = 0; i < 8; ++i) {
+    pos[i] = idx;
+    flags[i] = false;
+  }
+  for (int i = 0; i < 8 * kMaxSrc; ++i) ca[i] = 2.0f;
+  // Candidate positions in the reference's evaluation order: far up, down,
+  // left, right (slots 1, 3, 5, 7), then near up, down, left, right (0, 2,
+  // 4, 6).  Each slot takes the lowest-cost pixel of its pattern.
+  for (int slot_i = 0; slot_i < 8; ++slot_i) {
+    const int slot = slot_i < 4 ? 2 * slot_i + 1 : 2 * (slot_i - 4);
+    const int dir = slot >> 1;  // 0 up, 1 down, 2 left, 3 right
+    const bool vert = dir < 2;
+    const int sgn = (dir & 1) ? 1 : -1;
+    int base;
+    float bc;
+    int bp;
+    if (slot & 1) {  // far
+      const bool ok = dir == 0 ? y > 2 : (dir == 1 ? y < H - 3 : (dir == 2 ? x > 2 : x < W - 3));
+      if (!ok) continue;
+      base = vert ? (y + 3 * sgn) * W + x : y * W + (x + 3 * sgn);
+      bc = C[base];
+      bp = base;
+      for (int i = 1; i < 11; ++i) {
+        const int q = vert ? y + sgn * (3 + 2 * i) : x + sgn * (3 + 2 * i);
+        if (q < 0 || q >= (vert ? H : W)) break;
+        const int pp = vert ? q * W + x : y * W + q;
+        if (C[pp] < bc) {
+          bc = C[pp];
+          bp = pp;
+        }
+      }
+    } else {  // near, with a V of diagonals behind the neighbour
+      const bool ok = dir == 0 ? y > 0 : (dir == 1 ? y < H - 1 : (dir == 2 ? x > 0 : x < W - 1));
+      if (!ok) continue;
+      base = vert ? (y + sgn) * W + x : y * W + (x + sgn);
+      bc = C[base];
+      bp = base;
+      for (int i = 0; i < 3; ++i) {
+        for (int side = 0; side < 2; ++side) {
+          bool cond;
+          int pp;
+          if (vert) {
+            const bool along = dir == 0 ? y > 1 + i : y < H - 2 - i;
+            cond = along && (side == 0 ? x > i : x < W - 1 - i);
+            pp = (y + sgn * (2 + i)) * W + (side == 0 ? x - i - 1 : x + i + 1);
+          } else {
+            const bool along = dir == 2 ? x > 1 + i : x < W - 2 - i;
+            cond = along && (side == 0 ? y > i : y < H - 1 - i);
+            pp = (side == 0 ? y - i - 1 : y + i + 1) * W + (x + sgn * (2 + i));
+          }
+          if (cond && pp >= 0 && pp < npix && C[pp] < bc) {
+            bc = C[pp];
+            bp = pp;
+          }
+        }
+      }
+    }
+    pos[slot] = bp;
+    flags[slot] = true;
+    cost_vector(S, x, y, st.planes[bp], &ca[slot * kMaxSrc]);
+  }
+
+  // View selection priors from the four direct neighbours (last one wins).
+  float pri[kMaxSrc];
+  for (int i = 0; i < kMaxSrc; ++i) pri[i] = 0.0f;
+  const int npos[4] = {idx - W, idx + W, idx - 1, idx + 1};
+  for (int i = 0; i < 4; ++i) {
+    const int np = npos[i];
+    if (flags[2 * i] && np >= 0 && np < npix) {
+      const unsigned sv = st.sel[np];
+      for (int j = 0; j < n_src; ++j) pri[j] = (sv & (1u << j)) ? 0.9f : 0.1f;
+    }
+  }
+  const float thr = 0.8f * acm_exp((float)(iteration * iteration) / (-90.0f));
+  float prob[kMaxSrc];
+  for (int i = 0; i < kMaxSrc; ++i) prob[i] = 0.0f;
+  for (int i = 0; i < n_src; ++i) {
+    float count = 0.0f, tw = 0.0f;
+    int cfalse = 0;
+    for (int j = 0; j < 8; ++j) {
+      const float cv = ca[j * kMaxSrc + i];
+      if (flags[j] && cv < thr) {
+        tw += acm_exp(cv * cv / (-0.18f));
+        count += 1.0f;
+      }
+      if (flags[j] && cv > 1.2f) ++cfalse;
+    }
+    if (count > 2.0f && cfalse < 3)
+      prob[i] = tw / count;
+    else if (cfalse < 3)
+      prob[i] = acm_exp(thr * thr / (-0.32f));
+    prob[i] *= pri[i];
+  }
+  {
+    float sum = 0.0f;
+    for (int i = 0; i < n_src; ++i) sum += prob[i];
+    if (!(sum < 1e-12f)) {
+      const float inv = 1.0f / sum;
+      float cum = 0.0f;
+      for (int i = 0; i < n_src; ++i) {
+        cum += prob[i] * inv;
+        prob[i] = cum;
+      }
+    }
+  }
+  float vw[kMaxSrc];
+  for (int i = 0; i < kMaxSrc; ++i) vw[i] = 0.0f;
+  for (int smp = 0; smp < 15; ++smp) {
+    const float r = acm_rand(s, key + (unsigned)smp * 997u) - 1e-7f;
+    for (int j = 0; j < n_src; ++j)
+      if (prob[j] > r) {
+        vw[j] += 1.0f;
+        break;
+      }
+  }
+  unsigned new_sel = 0;
+  float norm = 0.0f;
+  for (int i = 0; i < n_src; ++i)
+    if (vw[i] > 0.0f) {
+      new_sel |= 1u << i;
+      norm += vw[i];
+    }
+
+  int best = 0;
+  float bcost = 0.0f;
+  for (int i = 0; i < 8; ++i) {
+    float fc = 2.0f;
+    if (flags[i]) {
+      const float photo = weighted(&ca[i * kMaxSrc], vw, norm, n_src, S.geom_weight);
+      fc = S.smooth_weight > 1e-6f
+               ? photo + S.smooth_weight * smoothness(S, st.planes, st.planes[pos[i]], x, y)
+               : photo;
+    }
+    if (i == 0 || fc < bcost) {
+      bcost = fc;
+      best = i;
+    }
+  }
+  float cvn[kMaxSrc];
+  for (int i = 0; i < kMaxSrc; ++i) cvn[i] = 2.0f;
+  const float4 own = st.planes[idx];
+  cost_vector(S, x, y, own, cvn);
+  float cost_now = weighted(cvn, vw, norm, n_src, S.geom_weight);
+  if (S.smooth_weight > 1e-6f) cost_now += S.smooth_weight * smoothness(S, st.planes, own, x, y);
+  float4 plane_now = own;
+  float depth_now = acm_depth(c0, (float)x, (float)y, plane_now);
+  if (flags[best] && bcost < cost_now) {
+    const float4 bpl = st.planes[pos[best]];
+    const float db = acm_depth(c0, (float)x, (float)y, bpl);
+    if (db >= S.depth_min && db <= S.depth_max) {
+      depth_now = db;
+      plane_now = bpl;
+      cost_now = bcost;
+      st.sel[idx] = new_sel;
+    }
+  }
+
+  // Refinement: (random depth, current normal), (current depth, random
+  // normal), (random, random), (current, perturbed normal), (perturbed
+  // depth, current normal).
+  const float pert = 0.02f;
+  const float PI_F = 3.14159274101257324f;
+  const float3 cur_n = acm_normalize(make_float3(plane_now.x, plane_now.y, plane_now.z));
+  const float lmin = acm_log(S.depth_min > 1e-6f ? S.depth_min : 1e-6f);
+  const float lmax = acm_log(S.depth_max > 1e-5f ? S.depth_max : 1e-5f);
+  const float depth_rand = acm_exp(lmin + acm_rand(s, key + 503u) * (lmax - lmin));
+  float3 nr;
+  nr.x = acm_rand(s, key + 504u) * 2.0f - 1.0f;
+  nr.y = acm_rand(s, key + 505u) * 2.0f - 1.0f;
+  nr.z = -1.0f;
+  nr = acm_normalize(nr);
+  const float dmn = (1.0f - pert) * depth_now, dmx = (1.0f + pert) * depth_now;
+  const float depth_pert =
+      acm_clamp(dmn + acm_rand(s, key + 510u) * (dmx - dmn), S.depth_min, S.depth_max);
+  const float pa1 = ((acm_rand(s, key + 520u) - 0.5f) * pert) * PI_F;
+  const float pa2 = ((acm_rand(s, key + 521u) - 0.5f) * pert) * PI_F;
+  float3 np_ = acm_normalize(make_float3(cur_n.x + pa1, cur_n.y + pa2, cur_n.z));
+  if (np_.z > 0.0f) np_.z = -np_.z;
+  const float depth_cur = depth_now;  // the five hypotheses are fixed before any is taken
+  for (int h = 0; h < 5; ++h) {
+    const float dh = h == 0 || h == 2 ? depth_rand : (h == 4 ? depth_pert : depth_cur);
+    const float3 nh = h == 1 || h == 2 ? nr : (h == 3 ? np_ : cur_n);
+    const float4 cand = acm_plane(c0, (float)x, (float)y, dh, nh);
+    float cv[kMaxSrc];
+    for (int i = 0; i < kMaxSrc; ++i) cv[i] = 2.0f;
+    cost_vector(S, x, y, cand, cv);
+    float tc = weighted(cv, vw, norm, n_src, S.geom_weight);
+    if (S.smooth_weight > 1e-6f) tc += S.smooth_weight * smoothness(S, st.planes, cand, x, y);
+    const float db = acm_depth(c0, (float)x, (float)y, cand);
+    if (db < S.depth_min || db > S.depth_max) continue;
+    if (tc < cost_now) {
+      depth_now = db;
+      plane_now = cand;
+      cost_now = tc;
+    }
+  }
+  st.planes[idx] = plane_now;
+  st.costs[idx] = cost_now;
+  st.rs[idx] = s;
+}
+
+// acmmp_checkerboard_filter (opencl_kernels.h:1919-2099) for one colour.
+__global__ void acm_filter_kernel(const AScene* __restrict__ Sp, AState st, int colour) {
+  const AScene& S = *Sp;
+  const int W = S.W, H = S.H;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + colour) & 1);
+  if (x >= W || y >= H) return;
+  const int c = y * W + x;
+  if (st.costs[c] < 0.001f) return;
+  const ACam& c0 = S.cam[0];
+  // The 20 neighbours in the reference's order: (dx, dy) and their bounds.
+  const int ox[20] = {0, 0, 0, 0, 0, 0, -1, -3, -5, 1, 3, 5, 2, 2, -2, -2, -1, 1, -1, 1};
+  const int oy[20] = {-1, -3, -5, 1, 3, 5, 0, 0, 0, 0, 0, 0, -1, 1, -1, 1, -2, -2, 2, 2};
+  float buf[21];
+  int n = 0;
+  buf[n++] = acm_depth(c0, (float)x, (float)y, st.planes[c]);
+  for (int k = 0; k < 20; ++k) {
+    const int dx = ox[k], dy = oy[k];
+    bool ok;
+    if (k < 6)
+      ok = dy < 0 ? y > -dy - 1 : y < H - dy;
+    else if (k < 12)
+      ok = dx < 0 ? x > -dx - 1 : x < W - dx;
+    else if (k < 16)
+      ok = (dy < 0 ? y > 0 : y < H - 1) && (dx > 0 ? x < W - 2 : x > 1);
+    else
+      ok = (dx < 0 ? x > 0 : x < W - 1) && (dy < 0 ? y > 2 : y < H - 2);
+    if (ok) buf[n++] = acm_depth(c0, (float)(x + dx), (float)(y + dy), st.planes[c + dy * W + dx]);
+  }
+  const float cd = buf[0];
+  if (cd > 0.0f) {
+    const float lo = cd * (1 - 0.15f), hi = cd * (1 + 0.15f);
+    int m = 1;
+    for (int i = 1; i < n; ++i)
+      if (buf[i] > lo && buf[i] < hi) buf[m++] = buf[i];
+    n = m;
+  }
+  for (int i = 1; i < n; ++i) {
+    const float t = buf[i];
+    int j = i;
+    for (; j >= 1 && t < buf[j - 1]; --j) buf[j] = buf[j - 1];
+    buf[j] = t;
+  }
+  const int mid = n / 2;
+  const float med = (n % 2 == 0) ? (buf[mid - 1] + buf[mid]) * 0.5f : buf[mid];
+  if (med > 0.0f) {
+    const float4 p = st.planes[c];
+    st.planes[c] = acm_plane(c0, (float)x, (float)y, med, acm_normalize(make_float3(p.x, p.y, p.z)));
+  }
+}
+
+// ReadBackResults (estimator.cc:958-1000): depth, unit normal, cost.
+__global__ void acm_readback_kernel(const AScene* __restrict__ Sp, AState st,
+                                    float* __restrict__ depth, float* __restrict__ normal,
+                                    float* __restrict__ cost) {
+  const AScene& S = *Sp;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= S.W || y >= S.H) return;
+  const size_t i = (size_t)y * S.W + x;
+  const float4 p = st.planes[i];
+  float d = 0.0f, n0 = 0.0f, n1 = 0.0f, n2 = 0.0f, cs = 0.0f;
+  if (isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(p.w)) {
+    const ACam& c = S.cam[0];
+    const float r0 = ((float)x - c.K[2]) / c.K[0], r1 = ((float)y - c.K[5]) / c.K[4];
+    const float den = (p.x * r0 + p.y * r1) + p.z * 1.0f;
+    float dd = fabsf(den) > 1e-6f ? -p.w / den : 0.0f;
+    if (!isfinite(dd)) dd = 0.0f;
+    if (dd > 0.0f && dd >= S.depth_min && dd <= S.depth_max) {
+      d = dd;
+      const float len = sqrtf((p.x * p.x + p.y * p.y) + p.z * p.z);
+      if (len > 1e-6f) {
+        n0 = p.x / len;
+        n1 = p.y / len;
+        n2 = p.z / len;
+      }
+    }
+    const float cc = st.costs[i];
+    cs = isfinite(cc) ? cc : 0.0f;
+  }
+  depth[i] = d;
+  normal[3 * i] = n0;
+  normal[3 * i + 1] = n1;
+  normal[3 * i + 2] = n2;
+  cost[i] = cs;
+}
+
+// The 5x5 median rejection (estimator.cc:1004-1021, cv::medianBlur with
+// replicated borders): depth d is zeroed where the median m > 0 and
+// |d - m| / d > 0.10.
+__global__ void acm_median_kernel(int W, int H, const float* __restrict__ depth,
+                                  float* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  float v[25];
+  int k = 0;
+  for (int a = -2; a <= 2; ++a)
+    for (int b = -2; b <= 2; ++b) v[k++] = depth[(size_t)clampi(y + a, H) * W + clampi(x + b, W)];
+  for (int i = 1; i < 25; ++i) {
+    const float t = v[i];
+    int j = i;
+    for (; j >= 1 && t < v[j - 1]; --j) v[j] = v[j - 1];
+    v[j] = t;
+  }
+  const float d = depth[(size_t)y * W + x], m = v[12];
+  out[(size_t)y * W + x] = (d > 0.0f && m > 0.0f && fabsf(d - m) / d > 0.10f) ? 0.0f : d;
+}
+
+// ------------------------------------------------------------------ host
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(count, 1) * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    return e;
+  }
+};
+
+struct AView {
+  double K[9], R[9], t[3];
+  int W, H;
+  std::vector<uint8_t> img;
+};
+struct ARef {
+  std::vector<AView> views;  // [0] the reference
+  float depth_min, depth_max;
+  std::vector<float> depth, normal, cost, conf;
+};
+
+}  // namespace
+
+struct dn_acmmp {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // DepthmapParams defaults (estimator.h:17-31).
+  int max_iterations = 3, patch_size = 11, max_image_size = 3200, hierarchy_levels = 1;
+  float sigma_spatial = 5.0f, sigma_color = 3.0f / 255.0f;
+  int top_k = 4;
+  float census_weight = 0.3f, smooth_weight = 0.0f, geom_weight = 0.0f;
+  std::vector<ARef> refs;
+  std::vector<int> geom_links;  // (ref, source, from) triples
+  float last_ms = 0.0f;
+  ~dn_acmmp() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+extern "C" const char* dn_acmmp_last_error(void) { return g_acm_error.c_str(); }
+
+extern "C" dn_status dn_acmmp_create(dn_acmmp** out) {
+  ACHECK(out, "NULL output");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return afail(DN_DEVICE_ERROR, "no CUDA device");
+  auto e = std::make_unique<dn_acmmp>();
+  ACUDA(cudaGetDevice(&e->device));
+  ACUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  *out = e.release();
+  return DN_OK;
+}
+extern "C" dn_status dn_acmmp_destroy(dn_acmmp* e) {
+  delete e;
+  return DN_OK;
+}
+
+#define ACM_SETTER(name, field, type)                           \
+  extern "C" dn_status dn_acmmp_set_##name(dn_acmmp* e, type v) { \
+    ACHECK(e, "NULL estimator");                                \
+    e->field = v;                                               \
+    return DN_OK;                                               \
+  }
+ACM_SETTER(max_iterations, max_iterations, int)
+ACM_SETTER(max_image_size, max_image_size, int)
+ACM_SETTER(hierarchy_levels, hierarchy_levels, int)
+ACM_SETTER(sigma_spatial, sigma_spatial, float)
+ACM_SETTER(sigma_color, sigma_color, float)
+ACM_SETTER(top_k, top_k, int)
+ACM_SETTER(census_weight, census_weight, float)
+ACM_SETTER(smooth_weight, smooth_weight, float)
+ACM_SETTER(geom_consistency_weight, geom_weight, float)
+#undef ACM_SETTER
+
+extern "C" dn_status dn_acmmp_set_patch_size(dn_acmmp* e, int size) {
+  ACHECK(e, "NULL estimator");
+  ACHECK(size >= 1 && size <= 63, "patch size must be in [1, 63]");
+  e->patch_size = size;
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_set_device(dn_acmmp* e, int device) {
+  ACHECK(e, "NULL estimator");
+  int n = 0;
+  ACUDA(cudaGetDeviceCount(&n));
+  ACHECK(device >= 0 && device < n, "no such CUDA device");
+  ACUDA(cudaSetDevice(device));
+  cudaStream_t s;
+  ACUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaSetDevice(e->device);
+  cudaStreamDestroy(e->stream);
+  e->stream = s;
+  e->device = device;
+  return DN_OK;
+}
+
+static dn_status make_view(const double* K, const double* R, const double* t,
+                           const uint8_t* img, int w, int h, int stride, AView* v) {
+  ACHECK(K && R && t && img, "NULL argument");
+  ACHECK(w >= 1 && h >= 1 && w <= 16384 && h <= 16384, "bad image size");
+  ACHECK(stride >= w, "stride below width");
+  for (int i = 0; i < 9; ++i) ACHECK(std::isfinite(K[i]) && std::isfinite(R[i]), "K, R must be finite");
+  for (int i = 0; i < 3; ++i) ACHECK(std::isfinite(t[i]), "t must be finite");
+  std::memcpy(v->K, K, sizeof(v->K));
+  std::memcpy(v->R, R, sizeof(v->R));
+  std::memcpy(v->t, t, sizeof(v->t));
+  v->W = w;
+  v->H = h;
+  v->img.resize((size_t)w * h);
+  for (int r = 0; r < h; ++r) std::memcpy(&v->img[(size_t)r * w], img + (size_t)r * stride, w);
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_begin_ref_view(dn_acmmp* e, const double* K, const double* R,
+                                             const double* t, const uint8_t* img, int w, int h,
+                                             int stride, float depth_min, float depth_max,
+                                             int* ref_idx) {
+  ACHECK(e, "NULL estimator");
+  ARef ref;
+  ref.depth_min = depth_min;
+  ref.depth_max = depth_max;
+  ref.views.emplace_back();
+  const dn_status st = make_view(K, R, t, img, w, h, stride, &ref.views.back());
+  if (st != DN_OK) return st;
+  e->refs.push_back(std::move(ref));
+  if (ref_idx) *ref_idx = (int)e->refs.size() - 1;
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_add_source_view(dn_acmmp* e, const double* K, const double* R,
+                                              const double* t, const uint8_t* img, int w, int h,
+                                              int stride) {
+  ACHECK(e, "NULL estimator");
+  if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no ref view started");
+  AView v;
+  const dn_status st = make_view(K, R, t, img, w, h, stride, &v);
+  if (st != DN_OK) return st;
+  e->refs.back().views.push_back(std::move(v));
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_set_sfm_points(dn_acmmp* e, const double* points, int64_t n) {
+  ACHECK(e, "NULL estimator");
+  if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no ref view started");
+  (void)points;
+  ACHECK(n == 0, "the SfM planar prior (estimator.cc:108-118, 644-940) is not built");
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_add_geom_link(dn_acmmp* e, int ref_idx, int source_view_idx,
+                                            int from_ref_idx) {
+  ACHECK(e, "NULL estimator");
+  ACHECK(ref_idx >= 0 && ref_idx < (int)e->refs.size(),
+         "DepthmapClusterEstimator::AddGeomLink: invalid ref_idx");
+  // Used only between pyramid levels (cluster_estimator.cc:107-125); with
+  // one level the link has no effect, as in the reference.
+  e->geom_links.insert(e->geom_links.end(), {ref_idx, source_view_idx, from_ref_idx});
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_clear(dn_acmmp* e) {
+  ACHECK(e, "NULL estimator");
+  e->refs.clear();
+  e->geom_links.clear();
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_num_refs(dn_acmmp* e, int* n) {
+  ACHECK(e && n, "NULL argument");
+  *n = (int)e->refs.size();
+  return DN_OK;
+}
+
+static dn_status run_ref(dn_acmmp* e, ARef& ref, float* ms) {
+  const int nv = (int)ref.views.size();
+  ACHECK(nv >= 2, "a reference view needs at least one source view");
+  const int n_img = std::min(nv, 1 + kMaxSrc);
+  cudaStream_t s = e->stream;
+  std::vector<std::unique_ptr<DBuf<float>>> imgs;
+  AScene S{};
+  for (int i = 0; i < n_img; ++i) {
+    const AView& v = ref.views[i];
+    // cv::Mat::convertTo(CV_32F, 1/255): float(v) * float(1/255).
+    std::vector<float> f(v.img.size());
+    const float scale = (float)(1.0 / 255.0);
+    for (size_t k = 0; k < f.size(); ++k) f[k] = (float)v.img[k] * scale;
+    imgs.emplace_back(new DBuf<float>());
+    ACUDA(imgs.back()->alloc(f.size()));
+    ACUDA(cudaMemcpyAsync(imgs.back()->p, f.data(), f.size() * sizeof(float),
+                          cudaMemcpyHostToDevice, s));
+    ACUDA(cudaStreamSynchronize(s));  // f is released at the end of this iteration
+    S.img[i] = AImg{imgs.back()->p, v.W, v.H};
+    for (int k = 0; k < 9; ++k) {
+      S.cam[i].K[k] = (float)v.K[k];
+      S.cam[i].R[k] = (float)v.R[k];
+    }
+    for (int k = 0; k < 3; ++k) S.cam[i].t[k] = (float)v.t[k];
+  }
+  const int W = ref.views[0].W, H = ref.views[0].H;
+  S.W = W;
+  S.H = H;
+  S.n_src = n_img - 1;
+  S.half_patch = e->patch_size / 2;
+  S.top_k = e->top_k;
+  S.sigma_spatial = e->sigma_spatial;
+  S.sigma_color = e->sigma_color;
+  S.census_weight = e->census_weight;
+  S.smooth_weight = e->smooth_weight;
+  S.geom_weight = e->geom_weight;
+  S.depth_min = ref.depth_min;
+  S.depth_max = ref.depth_max;
+  const size_t npix = (size_t)W * H;
+  DBuf<AScene> dS;
+  DBuf<float4> planes;
+  DBuf<float> costs, depth, normal, cost, depth2;
+  DBuf<uint2> rs;
+  DBuf<unsigned> sel;
+  ACUDA(dS.alloc(1));
+  ACUDA(planes.alloc(npix));
+  ACUDA(costs.alloc(npix));
+  ACUDA(rs.alloc(npix));
+  ACUDA(sel.alloc(npix));
+  ACUDA(depth.alloc(npix));
+  ACUDA(depth2.alloc(npix));
+  ACUDA(normal.alloc(3 * npix));
+  ACUDA(cost.alloc(npix));
+  ACUDA(cudaMemcpyAsync(dS.p, &S, sizeof(S), cudaMemcpyHostToDevice, s));
+  AState st{planes.p, costs.p, rs.p, sel.p};
+  cudaEvent_t e0, e1;
+  ACUDA(cudaEventCreate(&e0));
+  ACUDA(cudaEventCreate(&e1));
+  ACUDA(cudaEventRecord(e0, s));
+  const dim3 blk(16, 8), grid((W + 15) / 16, (H + 7) / 8);
+  const dim3 pblk(16, 4), pgrid(((W + 1) / 2 + 15) / 16, (H + 3) / 4);
+  acm_init_kernel<<<grid, blk, 0, s>>>(dS.p, st);
+  for (int it = 0; it < e->max_iterations; ++it) {
+    acm_pm_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 0, it);
+    acm_pm_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 1, it);
+    acm_filter_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 0);
+    acm_filter_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 1);
+  }
+  acm_readback_kernel<<<grid, blk, 0, s>>>(dS.p, st, depth.p, normal.p, cost.p);
+  acm_median_kernel<<<grid, blk, 0, s>>>(W, H, depth.p, depth2.p);
+  ACUDA(cudaGetLastError());
+  ACUDA(cudaEventRecord(e1, s));
+  ref.depth.resize(npix);
+  ref.normal.resize(3 * npix);
+  ref.cost.resize(npix);
+  ref.conf.assign(npix, 0.0f);
+  ACUDA(cudaMemcpyAsync(ref.depth.data(), depth2.p, npix * sizeof(float), cudaMemcpyDeviceToHost, s));
+  ACUDA(cudaMemcpyAsync(ref.normal.data(), normal.p, 3 * npix * sizeof(float),
+                        cudaMemcpyDeviceToHost, s));
+  ACUDA(cudaMemcpyAsync(ref.cost.data(), cost.p, npix * sizeof(float), cudaMemcpyDeviceToHost, s));
+  const cudaError_t err = cudaStreamSynchronize(s);
+  float t = 0.0f;
+  if (err == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ACUDA(err);
+  *ms += t;
+  // Logistic confidence on the host, as the reference computes it
+  // (estimator.cc:1023-1037).
+  for (size_t i = 0; i < npix; ++i)
+    if (ref.depth[i] > 0.0f) ref.conf[i] = 1.0f / (1.0f + std::exp((ref.cost[i] - 0.5f) * 5.0f));
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_run(dn_acmmp* e) {
+  ACHECK(e, "NULL estimator");
+  if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no reference views");
+  ACHECK(e->hierarchy_levels <= 1,
+         "hierarchy levels above 1 (image pyramid, upsampling, geometric consistency) are not built");
+  ACUDA(cudaSetDevice(e->device));
+  e->last_ms = 0.0f;
+  for (auto& ref : e->refs) {
+    const dn_status st = run_ref(e, ref, &e->last_ms);
+    if (st != DN_OK) return st;
+  }
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_result_size(dn_acmmp* e, int ref_idx, int* w, int* h) {
+  ACHECK(e && w && h, "NULL argument");
+  if (ref_idx < 0 || ref_idx >= (int)e->refs.size()) return afail(DN_OUT_OF_RANGE, "ref index out of range");
+  *w = e->refs[ref_idx].views[0].W;
+  *h = e->refs[ref_idx].views[0].H;
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_get_result(dn_acmmp* e, int ref_idx, float* depth, float* normal,
+                                         float* cost, float* confidence) {
+  ACHECK(e, "NULL estimator");
+  if (ref_idx < 0 || ref_idx >= (int)e->refs.size()) return afail(DN_OUT_OF_RANGE, "ref index out of range");
+  const ARef& r = e->refs[ref_idx];
+  ACHECK(!r.depth.empty(), "run() has not produced this result");
+  if (depth) std::memcpy(depth, r.depth.data(), r.depth.size() * sizeof(float));
+  if (normal) std::memcpy(normal, r.normal.data(), r.normal.size() * sizeof(float));
+  if (cost) std::memcpy(cost, r.cost.data(), r.cost.size() * sizeof(float));
+  if (confidence) std::memcpy(confidence, r.conf.data(), r.conf.size() * sizeof(float));
+  return DN_OK;
+}
+
+extern "C" dn_status dn_acmmp_last_run_ms(dn_acmmp* e, float* ms) {
+  ACHECK(e && ms, "NULL argument");
+  *ms = e->last_ms;
+  return DN_OK;
+}

@@ -28,7 +28,8 @@ from . import _lib
 from ._lib import _d, _f, _i32, _u8, check, ptr
 
 __all__ = ["DepthmapEstimator", "DepthmapCleaner", "DepthmapPruner", "GPUDepthmapCleaner",
-           "DepthmapFuser", "SVOFuser", "Batch", "postprocess_depth", "sor_filter", "fp32_peak"]
+           "DepthmapFuser", "SVOFuser", "DepthmapClusterEstimator", "Batch", "postprocess_depth",
+           "sor_filter", "fp32_peak"]
 
 
 def postprocess_depth(depth: np.ndarray) -> np.ndarray:
@@ -461,6 +462,134 @@ class SVOFuser(_Handle):
         ms = ctypes.c_float()
         self._check(self._L.dn_svo_last_fuse_ms(self._h, ctypes.byref(ms)))
         return float(ms.value)
+
+
+class DepthmapClusterEstimator(_Handle):
+    """``dense::DepthmapClusterEstimator`` (``cluster.h``, bound at
+    ``python/pybind.cc:53-104``) on the B200: the live path's PatchMatch
+    estimator, one pyramid level, no SfM planar prior.  ``run()`` returns,
+    per reference view, ``[depth (H,W) f32, normal (H,W,3) f32, cost (H,W)
+    f32, confidence (H,W) f32]``."""
+
+    def __init__(self) -> None:
+        super().__init__("dn_acmmp_create", "dn_acmmp_destroy")
+
+    def _check(self, st: int) -> None:
+        if st == _lib.DN_OK:
+            return
+        msg = self._L.dn_acmmp_last_error().decode(errors="replace")
+        if st == _lib.DN_INVALID_ARG:
+            raise ValueError(msg)
+        if st == _lib.DN_OUT_OF_MEMORY:
+            raise MemoryError(msg)
+        if st == _lib.DN_OUT_OF_RANGE:
+            raise IndexError(msg)
+        raise _lib.DenseError(st, msg)
+
+    @staticmethod
+    def is_available() -> bool:
+        return GPUDepthmapCleaner.is_available()
+
+    @staticmethod
+    def num_devices() -> int:
+        try:
+            return int(_lib.load().dn_device_count())
+        except OSError:
+            return 0
+
+    def set_max_iterations(self, n: int) -> None:
+        self._check(self._L.dn_acmmp_set_max_iterations(self._h, int(n)))
+
+    def set_patch_size(self, size: int) -> None:
+        self._check(self._L.dn_acmmp_set_patch_size(self._h, int(size)))
+
+    def set_max_image_size(self, size: int) -> None:
+        self._check(self._L.dn_acmmp_set_max_image_size(self._h, int(size)))
+
+    def set_hierarchy_levels(self, levels: int) -> None:
+        self._check(self._L.dn_acmmp_set_hierarchy_levels(self._h, int(levels)))
+
+    def set_sigma_spatial(self, v: float) -> None:
+        self._check(self._L.dn_acmmp_set_sigma_spatial(self._h, float(v)))
+
+    def set_sigma_color(self, v: float) -> None:
+        self._check(self._L.dn_acmmp_set_sigma_color(self._h, float(v)))
+
+    def set_top_k(self, k: int) -> None:
+        self._check(self._L.dn_acmmp_set_top_k(self._h, int(k)))
+
+    def set_census_weight(self, w: float) -> None:
+        self._check(self._L.dn_acmmp_set_census_weight(self._h, float(w)))
+
+    def set_smooth_weight(self, w: float) -> None:
+        self._check(self._L.dn_acmmp_set_smooth_weight(self._h, float(w)))
+
+    def set_geom_consistency_weight(self, w: float) -> None:
+        self._check(self._L.dn_acmmp_set_geom_consistency_weight(self._h, float(w)))
+
+    def set_device(self, idx: int) -> None:
+        self._check(self._L.dn_acmmp_set_device(self._h, int(idx)))
+
+    def begin_ref_view(self, K, R, t, image, depth_min: float, depth_max: float) -> int:
+        K, R, t = _mat(K, (3, 3), "K"), _mat(R, (3, 3), "R"), _mat(t, (3,), "t")
+        im = _image(image, "image")
+        idx = ctypes.c_int()
+        self._check(self._L.dn_acmmp_begin_ref_view(
+            self._h, ptr(K, _d), ptr(R, _d), ptr(t, _d), ptr(im, _u8), im.shape[1], im.shape[0],
+            im.shape[1], float(depth_min), float(depth_max), ctypes.byref(idx)))
+        return int(idx.value)
+
+    def add_source_view(self, K, R, t, image) -> None:
+        K, R, t = _mat(K, (3, 3), "K"), _mat(R, (3, 3), "R"), _mat(t, (3,), "t")
+        im = _image(image, "image")
+        st = self._L.dn_acmmp_add_source_view(self._h, ptr(K, _d), ptr(R, _d), ptr(t, _d),
+                                               ptr(im, _u8), im.shape[1], im.shape[0],
+                                               im.shape[1])
+        if st == _lib.DN_INVALID_ARG and b"no ref view" in self._L.dn_acmmp_last_error():
+            raise RuntimeError(self._L.dn_acmmp_last_error().decode())
+        self._check(st)
+
+    def set_sfm_points(self, points) -> None:
+        p = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        self._check(self._L.dn_acmmp_set_sfm_points(self._h, ptr(p, _d), len(p)))
+
+    def add_geom_link(self, ref_idx: int, source_view_idx: int, from_ref_idx: int) -> None:
+        st = self._L.dn_acmmp_add_geom_link(self._h, int(ref_idx), int(source_view_idx),
+                                             int(from_ref_idx))
+        if st == _lib.DN_INVALID_ARG:
+            raise RuntimeError(self._L.dn_acmmp_last_error().decode())
+        self._check(st)
+
+    def run(self) -> list:
+        st = self._L.dn_acmmp_run(self._h)
+        if st == _lib.DN_INVALID_ARG and b"no reference views" in self._L.dn_acmmp_last_error():
+            raise RuntimeError(self._L.dn_acmmp_last_error().decode())
+        self._check(st)
+        n = ctypes.c_int()
+        self._check(self._L.dn_acmmp_num_refs(self._h, ctypes.byref(n)))
+        out = []
+        for i in range(n.value):
+            w, h = ctypes.c_int(), ctypes.c_int()
+            self._check(self._L.dn_acmmp_result_size(self._h, i, ctypes.byref(w),
+                                                      ctypes.byref(h)))
+            H, W = h.value, w.value
+            d = np.zeros((H, W), np.float32)
+            nrm = np.zeros((H, W, 3), np.float32)
+            c = np.zeros((H, W), np.float32)
+            cf = np.zeros((H, W), np.float32)
+            self._check(self._L.dn_acmmp_get_result(self._h, i, ptr(d, _f), ptr(nrm, _f),
+                                                     ptr(c, _f), ptr(cf, _f)))
+            out.append([d, nrm, c, cf])
+        return out
+
+    def last_run_ms(self) -> float:
+        """Device time of the last run's kernels (all references)."""
+        ms = ctypes.c_float()
+        self._check(self._L.dn_acmmp_last_run_ms(self._h, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def clear(self) -> None:
+        self._check(self._L.dn_acmmp_clear(self._h))
 
 
 def sor_filter(points, knn: int = 12, stddev_factor: float = 2.5):

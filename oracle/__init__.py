@@ -662,3 +662,89 @@ def port_svo(views, voxel_size=0.02, trunc_factor=4.0, min_weight=3.0, bbox=None
                   _P(pts, _f), _P(nrm, _f), _P(clr, _u8), n)
     del keep
     return int(cnt), pts[:n].copy(), nrm[:n].copy(), clr[:n].copy()
+
+
+def acm_float_image(img):
+    """An 8-bit image as the live estimator uploads it (cv::Mat::convertTo
+    with scale 1/255: float(v) * float(1/255))."""
+    return np.ascontiguousarray(img, np.float32) * np.float32(1.0 / 255.0)
+
+
+def _acm_args(views):
+    L = port()
+    if not getattr(L, "_acm_ready", False):
+        pp = ctypes.POINTER(ctypes.c_void_p)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.or_acmmp_run.argtypes = [pp, ip, ip, pp, pp, pp, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                   ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                   ctypes.c_float, ctypes.c_float, _f, _f, _f, _f]
+        L.or_acmmp_run.restype = ctypes.c_int
+        L.or_acmmp_init.argtypes = [pp, ip, ip, pp, pp, pp, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_float, _f, _f,
+                                    ctypes.POINTER(ctypes.c_uint32)]
+        L.or_acmmp_init.restype = ctypes.c_int
+        L._acm_ready = True
+    keep = []
+    n = len(views)
+    imgs = (ctypes.c_void_p * n)()
+    Ks = (ctypes.c_void_p * n)()
+    Rs = (ctypes.c_void_p * n)()
+    ts = (ctypes.c_void_p * n)()
+    ws = (ctypes.c_int * n)()
+    hs = (ctypes.c_int * n)()
+    for i, (K, R, t, img) in enumerate(views):
+        f = acm_float_image(img)
+        K = np.ascontiguousarray(K, np.float64)
+        R = np.ascontiguousarray(R, np.float64)
+        t = np.ascontiguousarray(t, np.float64).reshape(3)
+        keep += [f, K, R, t]
+        imgs[i], Ks[i], Rs[i], ts[i] = f.ctypes.data, K.ctypes.data, R.ctypes.data, t.ctypes.data
+        hs[i], ws[i] = f.shape
+    return L, keep, imgs, ws, hs, Ks, Rs, ts
+
+
+def port_acmmp(views, depth_min, depth_max, iterations=3, patch_size=11, sigma_spatial=5.0,
+               sigma_color=3.0 / 255.0, top_k=4, census_weight=0.3, smooth_weight=0.0,
+               geom_weight=0.0):
+    """The live path's PatchMatch estimator for one reference view, one
+    level, no SfM prior (estimator.cc:120-243, 941-1040 over the kernels of
+    opencl_kernels.h) in the C restatement.  views: [(K, R, t, image u8)],
+    the reference first.  Returns (depth, normal (H, W, 3), cost,
+    confidence), all float32."""
+    L, keep, imgs, ws, hs, Ks, Rs, ts = _acm_args(views)
+    H, W = hs[0], ws[0]
+    depth = np.zeros((H, W), np.float32)
+    nrm = np.zeros((H, W, 3), np.float32)
+    cost = np.zeros((H, W), np.float32)
+    conf = np.zeros((H, W), np.float32)
+    rc = L.or_acmmp_run(imgs, ws, hs, Ks, Rs, ts, len(views), int(iterations), int(patch_size),
+                        float(sigma_spatial), float(sigma_color), int(top_k),
+                        float(census_weight), float(smooth_weight), float(geom_weight),
+                        float(depth_min), float(depth_max), _P(depth, _f), _P(nrm, _f),
+                        _P(cost, _f), _P(conf, _f))
+    if rc:
+        raise ValueError(f"or_acmmp_run failed ({rc})")
+    del keep
+    return depth, nrm, cost, conf
+
+
+def port_acmmp_init(views, depth_min, depth_max, patch_size=11, sigma_spatial=5.0,
+                    sigma_color=3.0 / 255.0, top_k=4, census_weight=0.3):
+    """The random initialisation alone (opencl_kernels.h:1055-1124):
+    (planes (H, W, 4), costs (H, W), selected views (H, W) uint32)."""
+    L, keep, imgs, ws, hs, Ks, Rs, ts = _acm_args(views)
+    H, W = hs[0], ws[0]
+    planes = np.zeros((H, W, 4), np.float32)
+    costs = np.zeros((H, W), np.float32)
+    sel = np.zeros((H, W), np.uint32)
+    rc = L.or_acmmp_init(imgs, ws, hs, Ks, Rs, ts, len(views), int(patch_size),
+                         float(sigma_spatial), float(sigma_color), int(top_k),
+                         float(census_weight), float(depth_min), float(depth_max),
+                         _P(planes, _f), _P(costs, _f),
+                         sel.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    if rc:
+        raise ValueError(f"or_acmmp_init failed ({rc})")
+    del keep
+    return planes, costs, sel

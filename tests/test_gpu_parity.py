@@ -599,6 +599,75 @@ def test_svo_fuser_edges(scene):
     assert all(np.array_equal(a, b) for a, b in zip(got, want[1:]))
 
 
+@pytest.mark.parametrize("params", [
+    dict(iterations=2, patch_size=5),
+    dict(iterations=1, patch_size=7, top_k=2, census_weight=0.0, smooth_weight=0.2),
+    dict(iterations=2, patch_size=3, sigma_spatial=3.0, sigma_color=0.05, census_weight=0.8),
+])
+def test_cluster_estimator_bit_identical_to_oracle(params):
+    """The live path's PatchMatch estimator (one level, no prior) against its
+    C restatement: a cluster of two reference views with 3 and 4 sources,
+    the random initialisation, the red/black passes with view selection
+    and refinement, the checkerboard filter and the readback; depth,
+    normal, cost and confidence identical."""
+    vs = S.ring_viewset(11, 5, 64, 48)
+    cams_ = vs.cameras
+    e = pydense.DepthmapClusterEstimator()
+    e.set_max_iterations(params["iterations"])
+    e.set_patch_size(params["patch_size"])
+    for k in ("top_k", "census_weight", "smooth_weight", "sigma_spatial", "sigma_color"):
+        if k in params:
+            getattr(e, "set_" + k)(params[k])
+    clusters = [(0, [1, 2, 4]), (2, [1, 3, 4, 0])]
+    want = []
+    for ref, srcs in clusters:
+        dmin, dmax = S.depth_range(vs.depths[ref])
+        c = cams_[ref]
+        e.begin_ref_view(c.K, c.R, c.t, vs.images[ref], dmin, dmax)
+        for s_ in srcs:
+            e.add_source_view(cams_[s_].K, cams_[s_].R, cams_[s_].t, vs.images[s_])
+        views = [(cams_[i].K, cams_[i].R, cams_[i].t, vs.images[i]) for i in [ref] + srcs]
+        kw = {k: v for k, v in params.items() if k != "iterations"}
+        want.append(O.port_acmmp(views, dmin, dmax, iterations=params["iterations"], **kw))
+    got = e.run()
+    assert len(got) == 2
+    for g, w in zip(got, want):
+        print("valid", (w[0] > 0).mean(), "run ms", e.last_run_ms())
+        assert (w[0] > 0).mean() > 0.2
+        for a, b in zip(g, w):
+            assert a.dtype == b.dtype and a.shape == b.shape
+            assert np.array_equal(a, b)
+
+
+def test_cluster_estimator_errors(scene):
+    e = pydense.DepthmapClusterEstimator()
+    with pytest.raises(RuntimeError):
+        e.run()
+    with pytest.raises(RuntimeError):
+        e.add_source_view(np.eye(3), np.eye(3), np.zeros(3), np.zeros((8, 8), np.uint8))
+    c = scene.cameras[0]
+    e.begin_ref_view(c.K, c.R, c.t, scene.images[0], 5.0, 30.0)
+    e.add_source_view(scene.cameras[1].K, scene.cameras[1].R, scene.cameras[1].t,
+                      scene.images[1])
+    with pytest.raises(ValueError):
+        e.set_sfm_points(np.ones((4, 3)))
+    e.set_sfm_points(np.zeros((0, 3)))
+    e.add_geom_link(0, 0, 0)
+    with pytest.raises(RuntimeError):
+        e.add_geom_link(3, 0, 0)
+    e.set_hierarchy_levels(2)
+    with pytest.raises(ValueError):
+        e.run()
+    e.set_hierarchy_levels(1)
+    e.set_max_iterations(1)
+    e.set_patch_size(5)
+    out = e.run()
+    assert len(out) == 1 and out[0][0].shape == scene.images[0].shape
+    e.clear()
+    with pytest.raises(RuntimeError):
+        e.run()
+
+
 def test_invalid_arguments_raise(scene):
     e = pydense.DepthmapEstimator()
     with pytest.raises(ValueError):
