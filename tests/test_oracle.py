@@ -363,3 +363,54 @@ def test_svo_oracle_known_answers():
     k = np.floor(pts / 0.05).astype(np.int64)
     order = np.lexsort((k[:, 2], k[:, 1], k[:, 0]))
     assert np.array_equal(order, np.arange(len(pts))) or len(np.unique(k, axis=0)) < len(k)
+
+
+def test_acmmp_oracle_exp_log_accuracy():
+    """The live estimator's own exp and log (Cody-Waite reduction, fixed
+    polynomials), which the library and the oracle share by construction:
+    within 2 ulp of float64 over the ranges the estimator uses."""
+    import ctypes
+    L = O.port()
+    L.acm_exp.argtypes = [ctypes.c_float]
+    L.acm_exp.restype = ctypes.c_float
+    L.acm_log.argtypes = [ctypes.c_float]
+    L.acm_log.restype = ctypes.c_float
+    rng = np.random.default_rng(0)
+    xs = np.concatenate([rng.uniform(-87, 88, 3000), rng.uniform(-2, 2, 3000),
+                         [0.0, -0.0, 1.0, -1.0, 88.7, -87.0]]).astype(np.float32)
+    for x in xs:
+        got = np.float32(L.acm_exp(float(x)))
+        want = np.exp(np.float64(x))
+        assert abs(float(got) - want) <= 2 * float(np.spacing(np.float32(want))), x
+    ys = np.concatenate([10.0 ** rng.uniform(-6, 6, 3000), rng.uniform(0.5, 2, 2000)]).astype(np.float32)
+    for y in ys:
+        got = np.float32(L.acm_log(float(y)))
+        want = np.log(np.float64(y))
+        assert abs(float(got) - want) <= 2 * float(np.spacing(np.float32(max(abs(want), 1e-7)))) + 1e-7, y
+    assert L.acm_exp(-200.0) == 0.0 and np.isinf(L.acm_exp(100.0))
+
+
+def test_acmmp_oracle_known_answers():
+    """The live estimator restated: with the source identical to the
+    reference (same camera), every plane maps each pixel onto itself, so on
+    texture the NCC is 1 and the initial cost 0 (to rounding); and on a
+    textured ring scene the estimator recovers most depths within 5 %."""
+    vs = S.ring_viewset(3, 4, 96, 72)
+    c = vs.cameras[0]
+    views = [(c.K, c.R, c.t, vs.images[0])] * 2
+    dmin, dmax = S.depth_range(vs.depths[0])
+    planes, costs, sel = O.port_acmmp_init(views, dmin, dmax, patch_size=5)
+    assert planes.shape == (72, 96, 4) and np.isfinite(planes).all()
+    assert np.all((costs >= -1e-5) & (costs <= 2)) and np.all(sel <= 1)
+    textured = vs.images[0][2:-2, 2:-2].std() > 5
+    assert textured and np.median(costs[4:-4, 4:-4]) < 1e-3
+    d, n, cost, conf = O.port_acmmp([(cc.K, cc.R, cc.t, im) for cc, im in
+                                     zip(vs.cameras, vs.images)], dmin, dmax, iterations=3,
+                                    patch_size=7)
+    gt = vs.depths[0]
+    m = (d > 0) & (gt > 0)
+    assert m.mean() > 0.3
+    rel = np.abs(d[m] - gt[m]) / gt[m]
+    assert np.median(rel) < 0.05
+    assert np.all((conf[d > 0] > 0) & (conf[d > 0] < 1)) and np.all(conf[d == 0] == 0)
+    assert np.allclose(np.linalg.norm(n[d > 0], axis=-1), 1, atol=1e-5)
