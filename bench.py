@@ -169,6 +169,57 @@ def fusion_leg(b, vs, cands, n_maps, repeats=3, oracle=True):
     return out
 
 
+def acmmp_leg(vs, cands, n_refs=4, n_src=6, repeats=2, oracle=True):
+    """The live path's PatchMatch estimator (DepthmapClusterEstimator, one
+    level, its default parameters: patch 11, 3 iterations, top-k 4, census
+    0.3) on the first `n_refs` ring views at full size, each with its
+    `n_src` nearest views: device time and depthmaps/s.  With `oracle`, the
+    single-thread C restatement runs one reference at an eighth of the size
+    in each axis, the GPU runs the same case, and the outputs are compared."""
+    from opensfm_b200 import pydense
+    from opensfm_b200 import synthetic as S
+
+    def build(scale_views, refs):
+        e = pydense.DepthmapClusterEstimator()
+        for ref in refs:
+            dmin, dmax = S.depth_range(scale_views.depths[ref])
+            c = scale_views.cameras[ref]
+            e.begin_ref_view(c.K, c.R, c.t, scale_views.images[ref], dmin, dmax)
+            for s_ in cands[ref][:n_src]:
+                cs = scale_views.cameras[s_]
+                e.add_source_view(cs.K, cs.R, cs.t, scale_views.images[s_])
+        return e
+
+    e = build(vs, range(n_refs))
+    out = e.run()  # warm-up
+    ms = []
+    for _ in range(repeats):
+        out = e.run()
+        ms.append(e.last_run_ms())
+    t = float(np.median(ms))
+    res = {"refs": n_refs, "sources": n_src, "size": list(vs.images[0].shape[::-1]),
+           "device_ms": t, "depthmaps_per_s": n_refs / (t * 1e-3),
+           "accuracy_1pct_median": float(np.median([S.accuracy(o[0], vs.depths[i])
+                                                     for i, o in enumerate(out)]))}
+    if oracle:
+        import oracle as O
+
+        H, W = vs.images[0].shape
+        small = S.ring_viewset(SEED, len(vs.images), W // 8, H // 8)
+        es = build(small, [0])
+        got = es.run()[0]
+        views = [(small.cameras[i].K, small.cameras[i].R, small.cameras[i].t, small.images[i])
+                 for i in [0] + list(cands[0][:n_src])]
+        dmin, dmax = S.depth_range(small.depths[0])
+        t0 = time.perf_counter()
+        want = O.port_acmmp(views, dmin, dmax)
+        res["oracle_sample"] = f"one {W // 8}x{H // 8} reference view, {n_src} sources"
+        res["oracle_1thread_s"] = time.perf_counter() - t0
+        res["sample_device_ms"] = es.last_run_ms()
+        res["identical_to_oracle"] = bool(all(np.array_equal(a, b) for a, b in zip(got, want)))
+    return res
+
+
 def svo_leg(views, repeats=3, oracle=True, voxel_size=0.05, trunc_factor=4.0, min_weight=3.0):
     """SVOFuser (TSDF fusion) over the same views: count_voxels() + fuse()
     timed on the host clock, the device time of the fuse, and with `oracle`
@@ -573,6 +624,8 @@ def run_ours(args):
         line["config"]["fusion"] = fusion_leg(b, vs, cands, n_maps)
     if args.learned:
         line["config"]["learned"] = learned_leg(b, n_maps, shapes, args.steps, vs)
+    if args.acmmp:
+        line["config"]["acmmp"] = acmmp_leg(vs, cands)
     if rank == 0 and world == 1 and not args.no_cpu and ring:
         try:
             line["cpu_baseline"] = cpu_sample(work, seconds=args.cpu_seconds)
@@ -631,6 +684,8 @@ def main():
                          "of the box or terrain scene, or the 256-view 1280x960 aerial block")
     ap.add_argument("--fuse", action="store_true",
                     help="also time DepthmapFuser on the cleaned maps against its C oracle")
+    ap.add_argument("--acmmp", action="store_true",
+                    help="also time the live path's PatchMatch estimator (DepthmapClusterEstimator)")
     ap.add_argument("--learned", action="store_true",
                     help="also time the learned initialisation on the same batch")
     args = ap.parse_args()
