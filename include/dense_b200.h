@@ -466,12 +466,15 @@ const char* dn_svo_last_error(void);
  * DepthmapClusterEstimator (cluster.h, cluster_estimator.cc:21-147, bound
  * at python/pybind.cc:53-104) over the live path's PatchMatch estimator
  * (estimator.cc:120-243, 941-1040; kernels opencl_kernels.h:44-1124,
- * 1298-1826, 1897-2099): one pyramid level, no SfM planar prior.  Per
- * reference view: random initialisation, then red/black PatchMatch passes
- * (bilateral NCC over strides 1-3, census fallback, joint view selection,
- * refinement) and a checkerboard median filter per iteration; readback
- * with a 5x5 median rejection and a logistic confidence.  FP32 with every
- * operation rounded by itself and the library's own exp / log.
+ * 1298-2099), no SfM planar prior.  Levels run coarsest first: images
+ * area-downscaled by 2^k (sizes must divide), each reference initialised
+ * randomly on the first level and from its own coarser result above it,
+ * with the linked references' previous-level depths in a geometric term.
+ * Per level: red/black PatchMatch passes (bilateral NCC over strides 1-3,
+ * census fallback, joint view selection, refinement) and a checkerboard
+ * median filter per iteration; readback (a 5x5 median rejection on the
+ * last level) and a logistic confidence.  FP32 with every operation
+ * rounded by itself and the library's own exp / log.
  * Defaults: 3 iterations, patch 11, sigma 5 / (3/255), top-k 4, census
  * weight 0.3, smoothness 0, one level.
  * ---------------------------------------------------------------------- */
@@ -482,7 +485,7 @@ dn_status dn_acmmp_destroy(dn_acmmp* e);
 dn_status dn_acmmp_set_max_iterations(dn_acmmp* e, int n);
 dn_status dn_acmmp_set_patch_size(dn_acmmp* e, int size);
 dn_status dn_acmmp_set_max_image_size(dn_acmmp* e, int size);
-/* Levels above 1 make dn_acmmp_run fail with DN_INVALID_ARG. */
+/* Pyramid levels; image sizes must divide by 2^(levels - 1). */
 dn_status dn_acmmp_set_hierarchy_levels(dn_acmmp* e, int levels);
 dn_status dn_acmmp_set_sigma_spatial(dn_acmmp* e, float v);
 dn_status dn_acmmp_set_sigma_color(dn_acmmp* e, float v);
@@ -503,8 +506,8 @@ dn_status dn_acmmp_add_source_view(dn_acmmp* e, const double K[9], const double 
                                    int stride);
 /* SetSfMPoints: only n = 0 is accepted (the planar prior is not built). */
 dn_status dn_acmmp_set_sfm_points(dn_acmmp* e, const double* points, int64_t n);
-/* AddGeomLink (cluster_estimator.cc:73-80): stored; it acts only between
- * pyramid levels. */
+/* AddGeomLink (cluster_estimator.cc:73-80): above the first level, source
+ * `source_view_idx` of `ref_idx` takes `from_ref_idx`'s previous depths. */
 dn_status dn_acmmp_add_geom_link(dn_acmmp* e, int ref_idx, int source_view_idx, int from_ref_idx);
 /* Run (cluster_estimator.cc:82-138): every reference view in turn. */
 dn_status dn_acmmp_run(dn_acmmp* e);

@@ -1,9 +1,11 @@
 // DepthmapClusterEstimator (cluster.h, cluster_estimator.cc:21-147) over the
 // live path's PatchMatch estimator (estimator.h:33-135, estimator.cc:120-243,
 // 473-558, 941-1040) and its kernels (opencl_kernels.h:44-1124, 1298-1826,
-// 1897-2099): one pyramid level, no SfM planar prior.
+// 1828-2099): pyramid levels with upsampling and geometric consistency, no
+// SfM planar prior.
 //
-// Per reference view: a random initialisation with top-k view selection,
+// Per reference view and level: a random initialisation with top-k view
+// selection (or, above the coarsest level, the coarser result upsampled),
 // then per iteration a red and a black PatchMatch pass (8 propagation
 // candidates, multi-hypothesis joint view selection, 5 refinement
 // hypotheses; the matching cost is a bilateral NCC over strides 1, 2, 3
@@ -73,6 +75,8 @@ struct AScene {
   int W, H, n_src, half_patch, top_k;
   float sigma_spatial, sigma_color, census_weight, smooth_weight, geom_weight;
   float depth_min, depth_max;
+  const float* prev;   // [16][H][W] previous-level source depths, or null
+  unsigned prev_mask;  // sources with a previous depth (0 without a geometric weight)
 };
 struct AState {
   float4* planes;  // (nx, ny, nz, d): n . X + d = 0 in the camera frame
@@ -353,13 +357,40 @@ __device__ float smoothness(const AScene& S, const float4* __restrict__ planes, 
   return tc / tw;
 }
 
-// compute_weighted_cost_geom without previous-level depths (geometric term 0).
-__device__ inline float weighted(const float* cv, const float* vw, float norm, int n_src,
-                                 float geom_w) {
+// compute_geom_consistency_cost (opencl_kernels.h:945-990): the forward-
+// backward reprojection error through source i's previous-level depth
+// (nearest pixel), at most 5 px.
+__device__ float geom_cost(const AScene& S, int i, float4 plane, int px, int py) {
+  const float maxc = 5.0f;
+  const ACam& rc = S.cam[0];
+  const ACam& sc = S.cam[1 + i];
+  const float depth = acm_depth(rc, (float)px, (float)py, plane);
+  if (depth <= 0.0f) return maxc;
+  const float3 p = acm_project(sc, acm_backproject(rc, (float)px, (float)py, depth));
+  if (p.z < 1e-6f) return maxc;
+  const float sx = p.x / p.z, sy = p.y / p.z;
+  if (sx < 0.0f || sx >= (float)S.W || sy < 0.0f || sy >= (float)S.H) return maxc;
+  const int ix = clampi((int)(sx + 0.5f), S.W), iy = clampi((int)(sy + 0.5f), S.H);
+  const float sd = S.prev[(size_t)i * S.W * S.H + (size_t)iy * S.W + ix];
+  if (sd <= 0.0f) return maxc;
+  const float3 rp = acm_project(rc, acm_backproject(sc, sx, sy, sd));
+  if (rp.z < 1e-6f) return maxc;
+  const float dx = (float)px - rp.x / rp.z, dy = (float)py - rp.y / rp.z;
+  const float e = sqrtf(dx * dx + dy * dy);
+  return e < maxc ? e : maxc;
+}
+
+// compute_weighted_cost_geom (opencl_kernels.h:1017-1045).
+__device__ inline float weighted(const AScene& S, const float* cv, const float* vw, float norm,
+                                 float4 plane, int x, int y) {
   if (norm < 1e-6f) return 2.0f;
   float total = 0.0f;
-  for (int i = 0; i < n_src; ++i)
-    if (vw[i] > 0.0f) total += vw[i] * (cv[i] + geom_w * 0.0f);
+  for (int i = 0; i < S.n_src; ++i)
+    if (vw[i] > 0.0f) {
+      float geom = 0.0f;
+      if (S.geom_weight > 0.0f && (S.prev_mask & (1u << i))) geom = geom_cost(S, i, plane, x, y);
+      total += vw[i] * (cv[i] + S.geom_weight * geom);
+    }
   return total / norm;
 }
 
@@ -412,6 +443,39 @@ __global__ void acm_init_kernel(const AScene* __restrict__ Sp, AState st) {
   }
   st.costs[idx] = cost;
   st.sel[idx] = sel;
+}
+
+// acmmp_upsample (opencl_kernels.h:1828-1892): each fine pixel takes its
+// nearest coarse plane re-anchored at itself, or a random plane where the
+// coarse depth is invalid; costs 2, views unselected, RNG states reset.
+__global__ void acm_upsample_kernel(const AScene* __restrict__ Sp, AState st,
+                                    const float4* __restrict__ src, int sw, int sh) {
+  const AScene& S = *Sp;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= S.W || y >= S.H) return;
+  const int idx = y * S.W + x;
+  uint2 s = make_uint2((unsigned)idx * 1099087573u + 2654435769u, (unsigned)idx * 2246822519u + 13u);
+  const float scx = (float)sw / (float)S.W, scy = (float)sh / (float)S.H;
+  const int sx = clampi((int)((float)x * scx), sw), sy = clampi((int)((float)y * scy), sh);
+  const float4 pl = src[(size_t)sy * sw + sx];
+  const ACam& c0 = S.cam[0];
+  const float depth = acm_depth(c0, (float)x, (float)y, pl);
+  if (depth > 0.0f) {
+    st.planes[idx] = acm_plane(c0, (float)x, (float)y, depth, acm_normalize(make_float3(pl.x, pl.y, pl.z)));
+  } else {
+    const unsigned key = (unsigned)(idx + 7919);
+    const float lmin = acm_log(S.depth_min > 1e-6f ? S.depth_min : 1e-6f);
+    const float lmax = acm_log(S.depth_max > 1e-5f ? S.depth_max : 1e-5f);
+    const float rd = acm_exp(lmin + acm_rand(s, key) * (lmax - lmin));
+    float3 n;
+    n.x = acm_rand(s, key + 3u) * 2.0f - 1.0f;
+    n.y = acm_rand(s, key + 5u) * 2.0f - 1.0f;
+    n.z = -1.0f;
+    st.planes[idx] = acm_plane(c0, (float)x, (float)y, rd, acm_normalize(n));
+  }
+  st.rs[idx] = s;
+  st.costs[idx] = 2.0f;
+  st.sel[idx] = 0u;
 }
 
 // acmmp_patchmatch (opencl_kernels.h:1298-1826) for the pixels of one colour:
@@ -560,7 +624,7 @@ __global__ void __launch_bounds__(64) acm_pm_kernel(const AScene* __restrict__ S
   for (int i = 0; i < 8; ++i) {
     float fc = 2.0f;
     if (flags[i]) {
-      const float photo = weighted(&ca[i * kMaxSrc], vw, norm, n_src, S.geom_weight);
+      const float photo = weighted(S, &ca[i * kMaxSrc], vw, norm, st.planes[pos[i]], x, y);
       fc = S.smooth_weight > 1e-6f
                ? photo + S.smooth_weight * smoothness(S, st.planes, st.planes[pos[i]], x, y)
                : photo;
@@ -574,7 +638,7 @@ __global__ void __launch_bounds__(64) acm_pm_kernel(const AScene* __restrict__ S
   for (int i = 0; i < kMaxSrc; ++i) cvn[i] = 2.0f;
   const float4 own = st.planes[idx];
   cost_vector(S, x, y, own, cvn);
-  float cost_now = weighted(cvn, vw, norm, n_src, S.geom_weight);
+  float cost_now = weighted(S, cvn, vw, norm, own, x, y);
   if (S.smooth_weight > 1e-6f) cost_now += S.smooth_weight * smoothness(S, st.planes, own, x, y);
   float4 plane_now = own;
   float depth_now = acm_depth(c0, (float)x, (float)y, plane_now);
@@ -618,7 +682,7 @@ __global__ void __launch_bounds__(64) acm_pm_kernel(const AScene* __restrict__ S
     float cv[kMaxSrc];
     for (int i = 0; i < kMaxSrc; ++i) cv[i] = 2.0f;
     cost_vector(S, x, y, cand, cv);
-    float tc = weighted(cv, vw, norm, n_src, S.geom_weight);
+    float tc = weighted(S, cv, vw, norm, cand, x, y);
     if (S.smooth_weight > 1e-6f) tc += S.smooth_weight * smoothness(S, st.planes, cand, x, y);
     const float db = acm_depth(c0, (float)x, (float)y, cand);
     if (db < S.depth_min || db > S.depth_max) continue;
@@ -770,6 +834,7 @@ struct AView {
 struct ARef {
   std::vector<AView> views;  // [0] the reference
   float depth_min, depth_max;
+  int W = 0, H = 0;  // size of the result
   std::vector<float> depth, normal, cost, conf;
 };
 
@@ -925,32 +990,134 @@ extern "C" dn_status dn_acmmp_num_refs(dn_acmmp* e, int* n) {
   return DN_OK;
 }
 
-static dn_status run_ref(dn_acmmp* e, ARef& ref, float* ms) {
+// cv::resize(INTER_AREA) of an 8-bit image by an integer factor k that
+// divides both sizes (OpenCV's fast area path): the k x k block mean, rounded
+// half up for k = 2, else float(sum) * float(1/k^2) rounded to nearest even.
+static void resize_area_u8(const uint8_t* src, int W, int H, int k, uint8_t* dst) {
+  const int w = W / k, h = H / k;
+  const float inv = 1.0f / (float)(k * k);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      int sum = 0;
+      for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) sum += src[(size_t)(k * y + a) * W + (k * x + b)];
+      const int v = k == 2 ? (sum + 2) >> 2 : (int)std::nearbyint((float)sum * inv);
+      dst[(size_t)y * w + x] = (uint8_t)std::min(255, std::max(0, v));
+    }
+}
+
+// The previous-level depth resize (UploadPreviousDepths uses INTER_LINEAR):
+// OpenCV's pixel-centre mapping, FP32 weights, each operation rounded by
+// itself.  OpenCV's SIMD arithmetic can differ from this in the last bits.
+static void resize_linear_f32(const float* src, int w, int h, float* dst, int W, int H) {
+  for (int y = 0; y < H; ++y) {
+    const double fyd = (y + 0.5) * ((double)h / H) - 0.5;
+    int sy = (int)std::floor(fyd);
+    float fy = (float)(fyd - sy);
+    if (sy < 0) {
+      sy = 0;
+      fy = 0.0f;
+    }
+    if (sy >= h - 1) {
+      sy = h - 1;
+      fy = 0.0f;
+    }
+    const int sy1 = std::min(sy + 1, h - 1);
+    for (int x = 0; x < W; ++x) {
+      const double fxd = (x + 0.5) * ((double)w / W) - 0.5;
+      int sx = (int)std::floor(fxd);
+      float fx = (float)(fxd - sx);
+      if (sx < 0) {
+        sx = 0;
+        fx = 0.0f;
+      }
+      if (sx >= w - 1) {
+        sx = w - 1;
+        fx = 0.0f;
+      }
+      const int sx1 = std::min(sx + 1, w - 1);
+      const float a0 = 1.0f - fx, b0 = 1.0f - fy;
+      const float r0 = src[(size_t)sy * w + sx] * a0 + src[(size_t)sy * w + sx1] * fx;
+      const float r1 = src[(size_t)sy1 * w + sx] * a0 + src[(size_t)sy1 * w + sx1] * fx;
+      dst[(size_t)y * W + x] = r0 * b0 + r1 * fy;
+    }
+  }
+}
+
+// A view at one pyramid level (BuildImagePyramid, estimator.cc:562-588).
+struct LevelView {
+  int W, H;
+  const uint8_t* img;
+  std::vector<uint8_t> scaled;
+  double K[9];
+};
+
+static dn_status level_view(const AView& v, float scale, LevelView* out) {
+  std::memcpy(out->K, v.K, sizeof(out->K));
+  if (!(scale < 0.999f)) {
+    out->W = v.W;
+    out->H = v.H;
+    out->img = v.img.data();
+    return DN_OK;
+  }
+  const int nw = std::max((int)((float)v.W * scale), 1), nh = std::max((int)((float)v.H * scale), 1);
+  const int k = v.W / nw;
+  ACHECK(nw * k == v.W && nh * k == v.H && v.H / nh == k,
+         "hierarchy levels need image sizes divisible by 2^(levels - 1)");
+  out->W = nw;
+  out->H = nh;
+  out->scaled.resize((size_t)nw * nh);
+  resize_area_u8(v.img.data(), v.W, v.H, k, out->scaled.data());
+  out->img = out->scaled.data();
+  const float sx = (float)nw / (float)v.W, sy = (float)nh / (float)v.H;
+  out->K[0] *= (double)sx;
+  out->K[2] *= (double)sx;
+  out->K[4] *= (double)sy;
+  out->K[5] *= (double)sy;
+  return DN_OK;
+}
+
+// The coarser level's result of one reference: what UpsampleDepthNormal
+// starts from.
+struct Coarse {
+  int W = 0, H = 0;
+  std::vector<float> depth, normal, cost;
+};
+
+// RunLevel (estimator.cc:159-243) for one reference: pyramid images, random
+// initialisation or upsampling from `coarse`, previous-level depths of the
+// linked sources, the iterations and the readback (with the median only on
+// the last level).  The result goes to ref.depth / normal / cost / conf.
+static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, const Coarse* coarse,
+                           const std::vector<std::pair<int, const Coarse*>>& prev, float* ms) {
   const int nv = (int)ref.views.size();
   ACHECK(nv >= 2, "a reference view needs at least one source view");
   const int n_img = std::min(nv, 1 + kMaxSrc);
   cudaStream_t s = e->stream;
+  const float scale = (float)(1.0 / std::pow(2.0, n_levels - 1 - level));
   std::vector<std::unique_ptr<DBuf<float>>> imgs;
   AScene S{};
   for (int i = 0; i < n_img; ++i) {
-    const AView& v = ref.views[i];
+    LevelView lv;
+    dn_status st = level_view(ref.views[i], scale, &lv);
+    if (st != DN_OK) return st;
     // cv::Mat::convertTo(CV_32F, 1/255): float(v) * float(1/255).
-    std::vector<float> f(v.img.size());
-    const float scale = (float)(1.0 / 255.0);
-    for (size_t k = 0; k < f.size(); ++k) f[k] = (float)v.img[k] * scale;
+    std::vector<float> f((size_t)lv.W * lv.H);
+    const float sc = (float)(1.0 / 255.0);
+    for (size_t k = 0; k < f.size(); ++k) f[k] = (float)lv.img[k] * sc;
     imgs.emplace_back(new DBuf<float>());
     ACUDA(imgs.back()->alloc(f.size()));
     ACUDA(cudaMemcpyAsync(imgs.back()->p, f.data(), f.size() * sizeof(float),
                           cudaMemcpyHostToDevice, s));
     ACUDA(cudaStreamSynchronize(s));  // f is released at the end of this iteration
-    S.img[i] = AImg{imgs.back()->p, v.W, v.H};
+    S.img[i] = AImg{imgs.back()->p, lv.W, lv.H};
     for (int k = 0; k < 9; ++k) {
-      S.cam[i].K[k] = (float)v.K[k];
-      S.cam[i].R[k] = (float)v.R[k];
+      S.cam[i].K[k] = (float)lv.K[k];
+      S.cam[i].R[k] = (float)ref.views[i].R[k];
     }
-    for (int k = 0; k < 3; ++k) S.cam[i].t[k] = (float)v.t[k];
+    for (int k = 0; k < 3; ++k) S.cam[i].t[k] = (float)ref.views[i].t[k];
   }
-  const int W = ref.views[0].W, H = ref.views[0].H;
+  const int W = S.img[0].W, H = S.img[0].H;
   S.W = W;
   S.H = H;
   S.n_src = n_img - 1;
@@ -964,8 +1131,31 @@ static dn_status run_ref(dn_acmmp* e, ARef& ref, float* ms) {
   S.depth_min = ref.depth_min;
   S.depth_max = ref.depth_max;
   const size_t npix = (size_t)W * H;
+  // UploadPreviousDepths (estimator.cc:56-106).
+  DBuf<float> d_prev;
+  S.prev = nullptr;
+  S.prev_mask = 0u;
+  if (!prev.empty() && e->geom_weight > 0.0f) {
+    std::vector<float> flat((size_t)kMaxSrc * npix, 0.0f);
+    for (const auto& pe : prev) {
+      const int si = pe.first;
+      if (si < 0 || si >= kMaxSrc) continue;
+      const Coarse& c = *pe.second;
+      float* dst = flat.data() + (size_t)si * npix;
+      if (c.W != W || c.H != H)
+        resize_linear_f32(c.depth.data(), c.W, c.H, dst, W, H);
+      else
+        std::memcpy(dst, c.depth.data(), npix * sizeof(float));
+      S.prev_mask |= 1u << si;
+    }
+    ACUDA(d_prev.alloc(flat.size()));
+    ACUDA(cudaMemcpyAsync(d_prev.p, flat.data(), flat.size() * sizeof(float),
+                          cudaMemcpyHostToDevice, s));
+    ACUDA(cudaStreamSynchronize(s));
+    S.prev = d_prev.p;
+  }
   DBuf<AScene> dS;
-  DBuf<float4> planes;
+  DBuf<float4> planes, src_planes;
   DBuf<float> costs, depth, normal, cost, depth2;
   DBuf<uint2> rs;
   DBuf<unsigned> sel;
@@ -980,13 +1170,37 @@ static dn_status run_ref(dn_acmmp* e, ARef& ref, float* ms) {
   ACUDA(cost.alloc(npix));
   ACUDA(cudaMemcpyAsync(dS.p, &S, sizeof(S), cudaMemcpyHostToDevice, s));
   AState st{planes.p, costs.p, rs.p, sel.p};
+  const dim3 blk(16, 8), grid((W + 15) / 16, (H + 7) / 8);
+  const dim3 pblk(16, 4), pgrid(((W + 1) / 2 + 15) / 16, (H + 3) / 4);
+  std::vector<float4> hsrc;
+  if (coarse) {
+    // UpsampleDepthNormal's host part (estimator.cc:600-640): coarse
+    // (depth, normal) -> planes, with the fine K scaled to the coarse size.
+    const ACam& c0 = S.cam[0];
+    const int sw = coarse->W, sh = coarse->H;
+    const float fx = c0.K[0] * (float)sw / (float)W, fy = c0.K[4] * (float)sh / (float)H;
+    const float cxs = c0.K[2] * (float)sw / (float)W, cys = c0.K[5] * (float)sh / (float)H;
+    hsrc.resize((size_t)sw * sh);
+    for (int y = 0; y < sh; ++y)
+      for (int x = 0; x < sw; ++x) {
+        const size_t i = (size_t)y * sw + x;
+        const float d = coarse->depth[i];
+        const float* n = &coarse->normal[3 * i];
+        const float p0 = d * ((float)x - cxs) / fx, p1 = d * ((float)y - cys) / fy, p2 = d;
+        hsrc[i] = make_float4(n[0], n[1], n[2], -((n[0] * p0 + n[1] * p1) + n[2] * p2));
+      }
+    ACUDA(src_planes.alloc(hsrc.size()));
+    ACUDA(cudaMemcpyAsync(src_planes.p, hsrc.data(), hsrc.size() * sizeof(float4),
+                          cudaMemcpyHostToDevice, s));
+  }
   cudaEvent_t e0, e1;
   ACUDA(cudaEventCreate(&e0));
   ACUDA(cudaEventCreate(&e1));
   ACUDA(cudaEventRecord(e0, s));
-  const dim3 blk(16, 8), grid((W + 15) / 16, (H + 7) / 8);
-  const dim3 pblk(16, 4), pgrid(((W + 1) / 2 + 15) / 16, (H + 3) / 4);
-  acm_init_kernel<<<grid, blk, 0, s>>>(dS.p, st);
+  if (coarse)
+    acm_upsample_kernel<<<grid, blk, 0, s>>>(dS.p, st, src_planes.p, coarse->W, coarse->H);
+  else
+    acm_init_kernel<<<grid, blk, 0, s>>>(dS.p, st);
   for (int it = 0; it < e->max_iterations; ++it) {
     acm_pm_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 0, it);
     acm_pm_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 1, it);
@@ -994,14 +1208,18 @@ static dn_status run_ref(dn_acmmp* e, ARef& ref, float* ms) {
     acm_filter_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 1);
   }
   acm_readback_kernel<<<grid, blk, 0, s>>>(dS.p, st, depth.p, normal.p, cost.p);
-  acm_median_kernel<<<grid, blk, 0, s>>>(W, H, depth.p, depth2.p);
+  const bool last = level == n_levels - 1;
+  if (last) acm_median_kernel<<<grid, blk, 0, s>>>(W, H, depth.p, depth2.p);
   ACUDA(cudaGetLastError());
   ACUDA(cudaEventRecord(e1, s));
+  ref.W = W;
+  ref.H = H;
   ref.depth.resize(npix);
   ref.normal.resize(3 * npix);
   ref.cost.resize(npix);
   ref.conf.assign(npix, 0.0f);
-  ACUDA(cudaMemcpyAsync(ref.depth.data(), depth2.p, npix * sizeof(float), cudaMemcpyDeviceToHost, s));
+  ACUDA(cudaMemcpyAsync(ref.depth.data(), last ? depth2.p : depth.p, npix * sizeof(float),
+                        cudaMemcpyDeviceToHost, s));
   ACUDA(cudaMemcpyAsync(ref.normal.data(), normal.p, 3 * npix * sizeof(float),
                         cudaMemcpyDeviceToHost, s));
   ACUDA(cudaMemcpyAsync(ref.cost.data(), cost.p, npix * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -1019,16 +1237,42 @@ static dn_status run_ref(dn_acmmp* e, ARef& ref, float* ms) {
   return DN_OK;
 }
 
+// Run (cluster_estimator.cc:82-138): levels outermost, references in turn;
+// a reference's previous-level depths for the geometric term come from the
+// linked references' latest results (those of this level for references
+// already done, of the last level for the rest), as in the reference.
 extern "C" dn_status dn_acmmp_run(dn_acmmp* e) {
   ACHECK(e, "NULL estimator");
   if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no reference views");
-  ACHECK(e->hierarchy_levels <= 1,
-         "hierarchy levels above 1 (image pyramid, upsampling, geometric consistency) are not built");
   ACUDA(cudaSetDevice(e->device));
   e->last_ms = 0.0f;
-  for (auto& ref : e->refs) {
-    const dn_status st = run_ref(e, ref, &e->last_ms);
-    if (st != DN_OK) return st;
+  const int n_levels = std::max(1, e->hierarchy_levels);
+  const int n_refs = (int)e->refs.size();
+  std::vector<Coarse> latest(n_refs);  // each reference's latest intermediate result
+  for (int level = 0; level < n_levels; ++level) {
+    for (int i = 0; i < n_refs; ++i) {
+      ARef& ref = e->refs[i];
+      std::vector<std::pair<int, const Coarse*>> prev;
+      if (level > 0 && e->geom_weight > 0.0f)
+        for (size_t l = 0; l + 2 < e->geom_links.size(); l += 3)
+          if (e->geom_links[l] == i) {
+            const int fr = e->geom_links[l + 2];
+            if (fr >= 0 && fr < n_refs && !latest[fr].depth.empty())
+              prev.emplace_back(e->geom_links[l + 1], &latest[fr]);
+          }
+      Coarse own;
+      const bool up = level > 0;
+      if (up) own = latest[i];  // a copy: latest[i] is replaced below
+      const dn_status st = run_level(e, ref, level, n_levels, up ? &own : nullptr, prev, &e->last_ms);
+      if (st != DN_OK) return st;
+      if (level < n_levels - 1) {
+        latest[i].W = ref.W;
+        latest[i].H = ref.H;
+        latest[i].depth = ref.depth;
+        latest[i].normal = ref.normal;
+        latest[i].cost = ref.cost;
+      }
+    }
   }
   return DN_OK;
 }
@@ -1036,8 +1280,8 @@ extern "C" dn_status dn_acmmp_run(dn_acmmp* e) {
 extern "C" dn_status dn_acmmp_result_size(dn_acmmp* e, int ref_idx, int* w, int* h) {
   ACHECK(e && w && h, "NULL argument");
   if (ref_idx < 0 || ref_idx >= (int)e->refs.size()) return afail(DN_OUT_OF_RANGE, "ref index out of range");
-  *w = e->refs[ref_idx].views[0].W;
-  *h = e->refs[ref_idx].views[0].H;
+  *w = e->refs[ref_idx].W ? e->refs[ref_idx].W : e->refs[ref_idx].views[0].W;
+  *h = e->refs[ref_idx].H ? e->refs[ref_idx].H : e->refs[ref_idx].views[0].H;
   return DN_OK;
 }
 

@@ -748,3 +748,129 @@ def port_acmmp_init(views, depth_min, depth_max, patch_size=11, sigma_spatial=5.
         raise ValueError(f"or_acmmp_init failed ({rc})")
     del keep
     return planes, costs, sel
+
+
+def _acm_level_lib():
+    L = port()
+    if not getattr(L, "_acm_level_ready", False):
+        pp = ctypes.POINTER(ctypes.c_void_p)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.or_acmmp_level.argtypes = [pp, ip, ip, pp, pp, pp, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                     ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_float, ctypes.c_float, _f, _f, ctypes.c_int,
+                                     ctypes.c_int, _f, ctypes.c_uint32, ctypes.c_int, _f, _f, _f,
+                                     _f]
+        L.or_acmmp_level.restype = ctypes.c_int
+        L.or_resize_area_u8.argtypes = [_u8, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8]
+        L.or_resize_linear_f32.argtypes = [_f, ctypes.c_int, ctypes.c_int, _f, ctypes.c_int,
+                                           ctypes.c_int]
+        L._acm_level_ready = True
+    return L
+
+
+def acm_resize_area(img, k):
+    """cv::resize(INTER_AREA) by an integer factor k dividing both sizes."""
+    L = _acm_level_lib()
+    im = np.ascontiguousarray(img, np.uint8)
+    H, W = im.shape
+    out = np.zeros((H // k, W // k), np.uint8)
+    L.or_resize_area_u8(_P(im, _u8), W, H, int(k), _P(out, _u8))
+    return out
+
+
+def acm_resize_linear(depth, W, H):
+    """The previous-level depth resize (OpenCV's pixel-centre bilinear in
+    FP32, each operation rounded by itself)."""
+    L = _acm_level_lib()
+    d = np.ascontiguousarray(depth, np.float32)
+    out = np.zeros((H, W), np.float32)
+    L.or_resize_linear_f32(_P(d, _f), d.shape[1], d.shape[0], _P(out, _f), int(W), int(H))
+    return out
+
+
+def port_acmmp_cluster(refs, hierarchy_levels=1, iterations=3, patch_size=11, sigma_spatial=5.0,
+                       sigma_color=3.0 / 255.0, top_k=4, census_weight=0.3, smooth_weight=0.0,
+                       geom_weight=0.0, geom_links=()):
+    """DepthmapClusterEstimator::Run (cluster_estimator.cc:82-138) over
+    RunLevel (estimator.cc:159-243) in the C restatement, levels outermost:
+    the pyramid (estimator.cc:562-588; sizes must divide by 2^(levels-1)),
+    upsampling from each reference's own coarser result, and previous-level
+    depths of linked references for the geometric term (updated in place as
+    the references of a level finish, as the reference does).
+    refs: [dict(views=[(K, R, t, image u8), ...] (reference first),
+    depth_min, depth_max)]; geom_links: (ref, source index, from ref).
+    Returns [(depth, normal, cost, confidence)] per reference."""
+    L = _acm_level_lib()
+    N = max(1, int(hierarchy_levels))
+    n_refs = len(refs)
+    links = {}
+    for r, s, fr in geom_links:
+        links.setdefault(r, []).append((s, fr))
+    prev_depths = [None] * n_refs
+    coarse = [None] * n_refs
+    results = [None] * n_refs
+    for level in range(N):
+        scale = np.float32(1.0 / 2.0 ** (N - 1 - level))
+        for i, ref in enumerate(refs):
+            views = []
+            for K, R, t, img in ref["views"]:
+                K = np.array(K, np.float64).reshape(3, 3)
+                img = np.ascontiguousarray(img, np.uint8)
+                if scale < np.float32(0.999):
+                    h0, w0 = img.shape
+                    nw = max(int(np.float32(w0) * scale), 1)
+                    nh = max(int(np.float32(h0) * scale), 1)
+                    k = w0 // nw
+                    if w0 != nw * k or h0 != nh * k or h0 // nh != k:
+                        raise ValueError("image sizes must divide by 2^(levels - 1)")
+                    img = acm_resize_area(img, k)
+                    sx = np.float32(nw) / np.float32(w0)
+                    sy = np.float32(nh) / np.float32(h0)
+                    K = K.copy()
+                    K[0, 0] *= np.float64(sx)
+                    K[0, 2] *= np.float64(sx)
+                    K[1, 1] *= np.float64(sy)
+                    K[1, 2] *= np.float64(sy)
+                views.append((K, R, t, img))
+            _, keep, imgs, ws, hs, Ks, Rs, ts = _acm_args(views)
+            H, W = hs[0], ws[0]
+            entries = []
+            if level > 0 and geom_weight > 0 and links.get(i):
+                for s_idx, fr in links[i]:
+                    if 0 <= fr < n_refs and prev_depths[fr] is not None:
+                        entries.append((s_idx, prev_depths[fr]))
+            pd, mask = None, 0
+            if entries:
+                pd = np.zeros((16, H, W), np.float32)
+                for s_idx, d in entries:
+                    if not 0 <= s_idx < 16:
+                        continue
+                    if d.shape != (H, W):
+                        d = acm_resize_linear(d, W, H)
+                    pd[s_idx] = d
+                    mask |= 1 << s_idx
+            cd = cn = None
+            cw = ch = 0
+            if level > 0:
+                cd, cn, _, cw, ch = coarse[i]
+            depth = np.zeros((H, W), np.float32)
+            nrm = np.zeros((H, W, 3), np.float32)
+            cost = np.zeros((H, W), np.float32)
+            conf = np.zeros((H, W), np.float32)
+            rc = L.or_acmmp_level(
+                imgs, ws, hs, Ks, Rs, ts, len(views), int(iterations), int(patch_size),
+                float(sigma_spatial), float(sigma_color), int(top_k), float(census_weight),
+                float(smooth_weight), float(geom_weight), float(ref["depth_min"]),
+                float(ref["depth_max"]), None if cd is None else _P(cd, _f),
+                None if cn is None else _P(cn, _f), cw, ch,
+                None if pd is None else _P(pd, _f), mask, int(level == N - 1), _P(depth, _f),
+                _P(nrm, _f), _P(cost, _f), _P(conf, _f))
+            if rc:
+                raise ValueError(f"or_acmmp_level failed ({rc})")
+            del keep
+            results[i] = (depth, nrm, cost, conf)
+            if level < N - 1:
+                coarse[i] = (depth, nrm, cost, W, H)
+                prev_depths[i] = depth
+    return results

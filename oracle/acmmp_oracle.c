@@ -1,5 +1,8 @@
-/* The live path's PatchMatch estimator (ACMMP-style) restated in C, one
- * pyramid level, no SfM planar prior.  TEST INFRASTRUCTURE ONLY.
+/* The live path's PatchMatch estimator (ACMMP-style) restated in C: one
+ * pyramid level per call, with the upsampling from the coarser level and
+ * the geometric consistency against previous-level depths (the level loop
+ * and the cluster's links are driven from oracle/__init__.py); no SfM
+ * planar prior.  TEST INFRASTRUCTURE ONLY.
  *
  * Follows opensfm/src/lib/dense/src/estimator.cc:120-243 (Run / RunLevel:
  * random initialisation, then per iteration a red and a black PatchMatch
@@ -405,13 +408,54 @@ static float acm_smoothness(const float* planes, const acm_cam* c, const float* 
   return tc / tw;
 }
 
-/* compute_weighted_cost_geom without previous-level depths: the geometric
- * term is 0 for every view. */
-static float acm_weighted(const float* cv, const float* vw, float norm, int n_src, float geom_w) {
+/* Previous-level depths of the sources (geometric consistency): [16][H][W]
+ * at the current level's size, and which sources have one. */
+typedef struct {
+  const float* depths;
+  uint32_t mask;
+} acm_prev;
+
+/* compute_geom_consistency_cost (opencl_kernels.h:945-990): the forward-
+ * backward reprojection error through the source's previous depth, at most
+ * 5 px. */
+static float acm_geom_cost(const acm_cam* rc, const acm_cam* sc, const float* plane, int px,
+                           int py, const float* prev, int W, int H) {
+  const float maxc = 5.0f;
+  const float depth = acm_depth_from_plane(rc, (float)px, (float)py, plane);
+  if (depth <= 0.0f) return maxc;
+  float w[3], p[3];
+  acm_backproject(rc, (float)px, (float)py, depth, w);
+  acm_project(sc, w, p);
+  if (p[2] < 1e-6f) return maxc;
+  const float sx = p[0] / p[2], sy = p[1] / p[2];
+  if (sx < 0.0f || sx >= (float)W || sy < 0.0f || sy >= (float)H) return maxc;
+  const int ix = acm_clampi((int)(sx + 0.5f), W), iy = acm_clampi((int)(sy + 0.5f), H);
+  const float sd = prev[(size_t)iy * W + ix];
+  if (sd <= 0.0f) return maxc;
+  float sw[3], rp[3];
+  acm_backproject(sc, sx, sy, sd, sw);
+  acm_project(rc, sw, rp);
+  if (rp[2] < 1e-6f) return maxc;
+  const float bx = rp[0] / rp[2], by = rp[1] / rp[2];
+  const float dx = (float)px - bx, dy = (float)py - by;
+  const float e = sqrtf(dx * dx + dy * dy);
+  return e < maxc ? e : maxc;
+}
+
+/* compute_weighted_cost_geom (opencl_kernels.h:1017-1045). */
+static float acm_weighted(const float* cv, const float* vw, float norm, int n_src, float geom_w,
+                          const acm_cam* cams, const float* plane, int x, int y,
+                          const acm_prev* prev, int W, int H) {
   if (norm < 1e-6f) return 2.0f;
   float total = 0.0f;
   for (int i = 0; i < n_src; ++i)
-    if (vw[i] > 0.0f) total += vw[i] * (cv[i] + geom_w * 0.0f);
+    if (vw[i] > 0.0f) {
+      float geom = 0.0f;
+      if (geom_w > 0.0f && (prev->mask & (1u << i)))
+        geom = acm_geom_cost(&cams[0], &cams[i + 1], plane, x, y,
+                             prev->depths + (size_t)i * W * H, W, H);
+      total += vw[i] * (cv[i] + geom_w * geom);
+    }
   return total / norm;
 }
 
@@ -450,7 +494,7 @@ static void acm_random_init(const acm_scene* S, const acm_params* P, acm_state* 
 }
 
 static void acm_pm_pixel(const acm_scene* S, const acm_params* P, acm_state* st, int x, int y,
-                         int iteration) {
+                         int iteration, const acm_prev* prev) {
   const int W = S->W, H = S->H, npix = W * H;
   const int idx = y * W + x;
   const acm_cam* c0 = &S->cams[0];
@@ -569,7 +613,8 @@ static void acm_pm_pixel(const acm_scene* S, const acm_params* P, acm_state* st,
   for (int i = 0; i < 8; ++i) {
     if (flags[i]) {
       const float* pl = st->planes + 4 * (size_t)pos[i];
-      const float photo = acm_weighted(&ca[i * ACM_MAX_SRC], vw, norm, n_src, P->geom_weight);
+      const float photo = acm_weighted(&ca[i * ACM_MAX_SRC], vw, norm, n_src, P->geom_weight,
+                                       S->cams, pl, x, y, prev, W, H);
       fc[i] = P->smooth_weight > 1e-6f
                   ? photo + P->smooth_weight * acm_smoothness(st->planes, c0, pl, x, y, W, H)
                   : photo;
@@ -588,7 +633,7 @@ static void acm_pm_pixel(const acm_scene* S, const acm_params* P, acm_state* st,
   for (int i = 0; i < ACM_MAX_SRC; ++i) cvn[i] = 2.0f;
   float* own = st->planes + 4 * (size_t)idx;
   acm_cost_vector(S, P, x, y, own, cvn);
-  float cost_now = acm_weighted(cvn, vw, norm, n_src, P->geom_weight);
+  float cost_now = acm_weighted(cvn, vw, norm, n_src, P->geom_weight, S->cams, own, x, y, prev, W, H);
   if (P->smooth_weight > 1e-6f)
     cost_now += P->smooth_weight * acm_smoothness(st->planes, c0, own, x, y, W, H);
   st->costs[idx] = cost_now;
@@ -635,7 +680,7 @@ static void acm_pm_pixel(const acm_scene* S, const acm_params* P, acm_state* st,
     float cv[ACM_MAX_SRC];
     for (int i = 0; i < ACM_MAX_SRC; ++i) cv[i] = 2.0f;
     acm_cost_vector(S, P, x, y, cand, cv);
-    float tc = acm_weighted(cv, vw, norm, n_src, P->geom_weight);
+    float tc = acm_weighted(cv, vw, norm, n_src, P->geom_weight, S->cams, cand, x, y, prev, W, H);
     if (P->smooth_weight > 1e-6f)
       tc += P->smooth_weight * acm_smoothness(st->planes, c0, cand, x, y, W, H);
     const float db = acm_depth_from_plane(c0, (float)x, (float)y, cand);
@@ -722,14 +767,141 @@ static float acm_median5(const float* d, int W, int H, int x, int y) {
   return v[12];
 }
 
-/* One reference view: images[0] the reference, images[1..n_src] sources;
+/* acmmp_upsample (opencl_kernels.h:1828-1892) after UpsampleDepthNormal's
+ * host part (estimator.cc:600-640): the coarse level's depth, normal and
+ * cost become planes at the coarse pixel, each fine pixel takes its
+ * nearest coarse plane re-anchored at itself (or a random plane where the
+ * coarse depth is invalid); every cost is 2, every view unselected. */
+static void acm_upsample(const acm_scene* S, const acm_params* P, acm_state* st,
+                         const float* cd, const float* cn, int sw, int sh) {
+  const int W = S->W, H = S->H;
+  const acm_cam* c0 = &S->cams[0];
+  float* sp = (float*)malloc(sizeof(float) * 4 * (size_t)sw * sh);
+  const float fx = c0->K[0] * (float)sw / (float)W, fy = c0->K[4] * (float)sh / (float)H;
+  const float cxs = c0->K[2] * (float)sw / (float)W, cys = c0->K[5] * (float)sh / (float)H;
+  for (int y = 0; y < sh; ++y)
+    for (int x = 0; x < sw; ++x) {
+      const size_t i = (size_t)y * sw + x;
+      const float d = cd[i];
+      const float* n = cn + 3 * i;
+      const float p0 = d * ((float)x - cxs) / fx, p1 = d * ((float)y - cys) / fy, p2 = d;
+      sp[4 * i] = n[0];
+      sp[4 * i + 1] = n[1];
+      sp[4 * i + 2] = n[2];
+      sp[4 * i + 3] = -((n[0] * p0 + n[1] * p1) + n[2] * p2);
+    }
+  const float scx = (float)sw / (float)W, scy = (float)sh / (float)H;
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      const int idx = y * W + x;
+      uint32_t s[2] = {(uint32_t)idx * 1099087573u + 2654435769u,
+                       (uint32_t)idx * 2246822519u + 13u};
+      st->rs[2 * idx] = s[0];
+      st->rs[2 * idx + 1] = s[1];
+      const int sx = acm_clampi((int)((float)x * scx), sw), sy = acm_clampi((int)((float)y * scy), sh);
+      const float* pl = sp + 4 * ((size_t)sy * sw + sx);
+      float* out = st->planes + 4 * (size_t)idx;
+      const float depth = acm_depth_from_plane(c0, (float)x, (float)y, pl);
+      if (depth > 0.0f) {
+        float n[3] = {pl[0], pl[1], pl[2]};
+        acm_normalize(n);
+        acm_plane_from_depth_normal(c0, (float)x, (float)y, depth, n, out);
+      } else {
+        const uint32_t key = (uint32_t)(idx + 7919);
+        const float lmin = acm_log(P->depth_min > 1e-6f ? P->depth_min : 1e-6f);
+        const float lmax = acm_log(P->depth_max > 1e-5f ? P->depth_max : 1e-5f);
+        const float rd = acm_exp(lmin + acm_rand(s, key) * (lmax - lmin));
+        float n[3];
+        n[0] = acm_rand(s, key + 3u) * 2.0f - 1.0f;
+        n[1] = acm_rand(s, key + 5u) * 2.0f - 1.0f;
+        n[2] = -1.0f;
+        acm_normalize(n);
+        acm_plane_from_depth_normal(c0, (float)x, (float)y, rd, n, out);
+        st->rs[2 * idx] = s[0];
+        st->rs[2 * idx + 1] = s[1];
+      }
+      st->costs[idx] = 2.0f;
+      st->sel[idx] = 0;
+    }
+  free(sp);
+}
+
+/* cv::resize(INTER_AREA) of an 8-bit image by an integer factor k that
+ * divides both sizes (OpenCV's fast area path): the k x k block mean,
+ * rounded half up for k = 2, else float(sum) * float(1/k^2) rounded to
+ * nearest even. */
+void or_resize_area_u8(const uint8_t* src, int W, int H, int k, uint8_t* dst) {
+  const int w = W / k, h = H / k;
+  const float inv = 1.0f / (float)(k * k);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      int sum = 0;
+      for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) sum += src[(size_t)(k * y + a) * W + (k * x + b)];
+      int v;
+      if (k == 2)
+        v = (sum + 2) >> 2;
+      else
+        v = (int)nearbyintf((float)sum * inv);
+      dst[(size_t)y * w + x] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
+    }
+}
+
+/* Bilinear resize of a float image with OpenCV's pixel-centre mapping
+ * (f = (d + 0.5) src/dst - 0.5 in double, clamped to the border pixels),
+ * FP32 weights 1 - f and f, the horizontal then the vertical blend, each
+ * product and sum rounded by itself.  OpenCV's own INTER_LINEAR runs SIMD
+ * arithmetic and differs from this in the last bits. */
+void or_resize_linear_f32(const float* src, int w, int h, float* dst, int W, int H) {
+  for (int y = 0; y < H; ++y) {
+    double fyd = (y + 0.5) * ((double)h / H) - 0.5;
+    int sy = (int)floor(fyd);
+    float fy = (float)(fyd - sy);
+    if (sy < 0) {
+      sy = 0;
+      fy = 0.0f;
+    }
+    if (sy >= h - 1) {
+      sy = h - 1;
+      fy = 0.0f;
+    }
+    const int sy1 = sy + 1 < h ? sy + 1 : h - 1;
+    for (int x = 0; x < W; ++x) {
+      double fxd = (x + 0.5) * ((double)w / W) - 0.5;
+      int sx = (int)floor(fxd);
+      float fx = (float)(fxd - sx);
+      if (sx < 0) {
+        sx = 0;
+        fx = 0.0f;
+      }
+      if (sx >= w - 1) {
+        sx = w - 1;
+        fx = 0.0f;
+      }
+      const int sx1 = sx + 1 < w ? sx + 1 : w - 1;
+      const float a0 = 1.0f - fx, b0 = 1.0f - fy;
+      const float r0 = src[(size_t)sy * w + sx] * a0 + src[(size_t)sy * w + sx1] * fx;
+      const float r1 = src[(size_t)sy1 * w + sx] * a0 + src[(size_t)sy1 * w + sx1] * fx;
+      dst[(size_t)y * W + x] = r0 * b0 + r1 * fy;
+    }
+  }
+}
+
+/* One pyramid level of one reference view (RunLevel, estimator.cc:159-243):
+ * images[0] the reference, images[1 .. n_src] sources, already at this
+ * level's size (Ks scaled).  Initialised randomly, or from the coarse
+ * level's result (cd, cn, cw x ch) when cd is not NULL.  prev_depths
+ * [16][H][W] / prev_mask: the sources' previous-level depths for the
+ * geometric term (NULL / 0 for none).  apply_median: the final readback.
  * out: depth, normal [H][W][3], cost, confidence. */
-int or_acmmp_run(const float* const* images, const int* widths, const int* heights,
-                 const double* const* Ks, const double* const* Rs, const double* const* ts,
-                 int num_images, int iterations, int patch_size, float sigma_spatial,
-                 float sigma_color, int top_k, float census_weight, float smooth_weight,
-                 float geom_weight, float depth_min, float depth_max, float* out_depth,
-                 float* out_normal, float* out_cost, float* out_conf) {
+int or_acmmp_level(const float* const* images, const int* widths, const int* heights,
+                   const double* const* Ks, const double* const* Rs, const double* const* ts,
+                   int num_images, int iterations, int patch_size, float sigma_spatial,
+                   float sigma_color, int top_k, float census_weight, float smooth_weight,
+                   float geom_weight, float depth_min, float depth_max, const float* cd,
+                   const float* cn, int cw, int ch, const float* prev_depths, uint32_t prev_mask,
+                   int apply_median, float* out_depth, float* out_normal, float* out_cost,
+                   float* out_conf) {
   if (num_images < 2) return -1;
   acm_params P;
   P.n_src = num_images - 1 < ACM_MAX_SRC ? num_images - 1 : ACM_MAX_SRC;
@@ -763,12 +935,18 @@ int or_acmmp_run(const float* const* images, const int* widths, const int* heigh
   st.rs = (uint32_t*)calloc(2 * npix, sizeof(uint32_t));
   st.sel = (uint32_t*)calloc(npix, sizeof(uint32_t));
   if (!st.planes || !st.costs || !st.rs || !st.sel) return -2;
-  acm_random_init(&S, &P, &st);
+  /* UploadPreviousDepths (estimator.cc:56-106) zeroes the mask without a
+   * geometric weight. */
+  acm_prev prev = {prev_depths, (prev_depths && geom_weight > 0.0f) ? prev_mask : 0u};
+  if (cd)
+    acm_upsample(&S, &P, &st, cd, cn, cw, ch);
+  else
+    acm_random_init(&S, &P, &st);
   for (int it = 0; it < iterations; ++it) {
     for (int colour = 0; colour < 2; ++colour)
       for (int y = 0; y < H; ++y)
         for (int x = 0; x < W; ++x)
-          if (((x + y) & 1) == colour) acm_pm_pixel(&S, &P, &st, x, y, it);
+          if (((x + y) & 1) == colour) acm_pm_pixel(&S, &P, &st, x, y, it, &prev);
     for (int colour = 0; colour < 2; ++colour)
       for (int y = 0; y < H; ++y)
         for (int x = 0; x < W; ++x)
@@ -800,21 +978,37 @@ int or_acmmp_run(const float* const* images, const int* widths, const int* heigh
       const float cst = st.costs[i];
       out_cost[i] = isfinite(cst) ? cst : 0.0f;
     }
-  float* med = (float*)malloc(npix * sizeof(float));
-  for (int y = 0; y < H; ++y)
-    for (int x = 0; x < W; ++x) med[(size_t)y * W + x] = acm_median5(out_depth, W, H, x, y);
-  for (size_t i = 0; i < npix; ++i) {
-    const float d = out_depth[i], m = med[i];
-    if (d > 0.0f && m > 0.0f && fabsf(d - m) / d > 0.10f) out_depth[i] = 0.0f;
+  if (apply_median) {
+    float* med = (float*)malloc(npix * sizeof(float));
+    for (int y = 0; y < H; ++y)
+      for (int x = 0; x < W; ++x) med[(size_t)y * W + x] = acm_median5(out_depth, W, H, x, y);
+    for (size_t i = 0; i < npix; ++i) {
+      const float d = out_depth[i], m = med[i];
+      if (d > 0.0f && m > 0.0f && fabsf(d - m) / d > 0.10f) out_depth[i] = 0.0f;
+    }
+    free(med);
   }
   for (size_t i = 0; i < npix; ++i)
     if (out_depth[i] > 0.0f) out_conf[i] = 1.0f / (1.0f + expf((out_cost[i] - 0.5f) * 5.0f));
-  free(med);
   free(st.planes);
   free(st.costs);
   free(st.rs);
   free(st.sel);
   return 0;
+}
+
+/* One reference view on one level: random initialisation, no previous
+ * depths, the final readback. */
+int or_acmmp_run(const float* const* images, const int* widths, const int* heights,
+                 const double* const* Ks, const double* const* Rs, const double* const* ts,
+                 int num_images, int iterations, int patch_size, float sigma_spatial,
+                 float sigma_color, int top_k, float census_weight, float smooth_weight,
+                 float geom_weight, float depth_min, float depth_max, float* out_depth,
+                 float* out_normal, float* out_cost, float* out_conf) {
+  return or_acmmp_level(images, widths, heights, Ks, Rs, ts, num_images, iterations, patch_size,
+                        sigma_spatial, sigma_color, top_k, census_weight, smooth_weight,
+                        geom_weight, depth_min, depth_max, NULL, NULL, 0, 0, NULL, 0, 1,
+                        out_depth, out_normal, out_cost, out_conf);
 }
 
 /* The random initialisation alone (planes [H][W][4], costs, selected views),

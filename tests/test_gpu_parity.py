@@ -639,6 +639,43 @@ def test_cluster_estimator_bit_identical_to_oracle(params):
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("levels,geom", [(2, 0.2), (3, 0.0), (2, 1.0)])
+def test_cluster_estimator_levels_bit_identical_to_oracle(levels, geom):
+    """Pyramid levels: area-downscaled images and scaled intrinsics, the
+    coarser result upsampled, and the linked references' previous-level
+    depths in the geometric term (some links refer to references run later
+    in the level, some to ones run earlier, one to itself), against the
+    C restatement driven level by level."""
+    vs = S.ring_viewset(13, 5, 64, 48)
+    cams_ = vs.cameras
+    clusters = [(0, [1, 2, 4]), (2, [1, 3, 4, 0]), (4, [3, 2])]
+    links = [(0, 1, 1), (1, 3, 0), (1, 0, 2), (2, 1, 0), (2, 0, 1)]
+    e = pydense.DepthmapClusterEstimator()
+    e.set_max_iterations(2)
+    e.set_patch_size(5)
+    e.set_hierarchy_levels(levels)
+    e.set_geom_consistency_weight(geom)
+    refs = []
+    for ref, srcs in clusters:
+        dmin, dmax = S.depth_range(vs.depths[ref])
+        c = cams_[ref]
+        e.begin_ref_view(c.K, c.R, c.t, vs.images[ref], dmin, dmax)
+        for s_ in srcs:
+            e.add_source_view(cams_[s_].K, cams_[s_].R, cams_[s_].t, vs.images[s_])
+        refs.append(dict(views=[(cams_[i].K, cams_[i].R, cams_[i].t, vs.images[i])
+                                for i in [ref] + srcs], depth_min=dmin, depth_max=dmax))
+    for l in links:
+        e.add_geom_link(*l)
+    got = e.run()
+    want = O.port_acmmp_cluster(refs, hierarchy_levels=levels, iterations=2, patch_size=5,
+                                geom_weight=geom, geom_links=links)
+    for g, w in zip(got, want):
+        print("valid", (w[0] > 0).mean(), "run ms", e.last_run_ms())
+        assert g[0].shape == (48, 64) and (w[0] > 0).mean() > 0.2
+        for a, b in zip(g, w):
+            assert a.dtype == b.dtype and np.array_equal(a, b)
+
+
 def test_cluster_estimator_errors(scene):
     e = pydense.DepthmapClusterEstimator()
     with pytest.raises(RuntimeError):
@@ -655,7 +692,7 @@ def test_cluster_estimator_errors(scene):
     e.add_geom_link(0, 0, 0)
     with pytest.raises(RuntimeError):
         e.add_geom_link(3, 0, 0)
-    e.set_hierarchy_levels(2)
+    e.set_hierarchy_levels(5)  # 120 rows do not divide by 16
     with pytest.raises(ValueError):
         e.run()
     e.set_hierarchy_levels(1)

@@ -414,3 +414,24 @@ def test_acmmp_oracle_known_answers():
     assert np.median(rel) < 0.05
     assert np.all((conf[d > 0] > 0) & (conf[d > 0] < 1)) and np.all(conf[d == 0] == 0)
     assert np.allclose(np.linalg.norm(n[d > 0], axis=-1), 1, atol=1e-5)
+
+
+def test_acmmp_pyramid_resizes_against_opencv():
+    """The estimator's pyramid: cv::resize(INTER_AREA) by 2, 4 and 8 is
+    reproduced exactly; the previous-depth bilinear resize follows OpenCV's
+    INTER_LINEAR mapping and agrees to a few ulp (OpenCV's SIMD arithmetic
+    differs in the last bits, so the library fixes its own order)."""
+    cv2 = pytest.importorskip("cv2")
+    rng = np.random.default_rng(7)
+    for k in (2, 4, 8):
+        for H, W in ((48, 64), (96, 128), (40, 56)):
+            if H % k or W % k:
+                continue
+            im = rng.integers(0, 256, (H, W), dtype=np.uint8)
+            want = cv2.resize(im, (W // k, H // k), interpolation=cv2.INTER_AREA)
+            assert np.array_equal(O.acm_resize_area(im, k), want), (k, H, W)
+    d = rng.uniform(1, 30, (24, 32)).astype(np.float32)
+    d[rng.random(d.shape) < 0.2] = 0
+    got = O.acm_resize_linear(d, 64, 48)
+    want = cv2.resize(d, (64, 48), interpolation=cv2.INTER_LINEAR)
+    assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
