@@ -173,6 +173,25 @@ __device__ inline float acm_sample(const AImg& im, float u, float v) {
          (a * b) * t11;
 }
 
+// The same read at an integer texel (x + 0.5, y + 0.5): the fractions are
+// 0, so the formula above returns the (clamped) texel itself exactly.
+__device__ inline float acm_texel(const AImg& im, int x, int y) {
+  return __ldg(im.px + (size_t)clampi(y, im.H) * im.W + clampi(x, im.W));
+}
+
+// The read of acm_sample for a (u, v) known to satisfy 1 <= u - 0.5 and
+// u - 0.5 <= W - 2 (likewise v): no clamp changes anything there.
+__device__ inline float acm_sample_inside(const AImg& im, float u, float v) {
+  const float xm = u - 0.5f, ym = v - 0.5f;
+  const float fx = floorf(xm), fy = floorf(ym);
+  const float a = xm - fx, b = ym - fy;
+  const float* p = im.px + (size_t)(int)fy * im.W + (int)fx;
+  const float t00 = __ldg(p), t10 = __ldg(p + 1);
+  const float t01 = __ldg(p + im.W), t11 = __ldg(p + im.W + 1);
+  return (((1.0f - a) * (1.0f - b)) * t00 + (a * (1.0f - b)) * t10) + ((1.0f - a) * b) * t01 +
+         (a * b) * t11;
+}
+
 __device__ inline float3 acm_project(const ACam& c, float3 X) {
   const float x0 = ((c.R[0] * X.x + c.R[1] * X.y) + c.R[2] * X.z) + c.t[0];
   const float x1 = ((c.R[3] * X.x + c.R[4] * X.y) + c.R[5] * X.z) + c.t[1];
@@ -218,13 +237,23 @@ __device__ float ncc_at_stride(const AImg& ref, const AImg& src, float rc, float
                                float scy, int cx, int cy, int hp, float stride, float ax,
                                float ay, float bx, float by, float sf, float cf) {
   float sw = 0.0f, sr = 0.0f, ss = 0.0f, srr = 0.0f, sss = 0.0f, srs = 0.0f;
+  // The warped patch is affine: if its corners lie at least a texel inside
+  // the source (with a margin for the rounding of the inner taps), no tap
+  // is clamped and the reads skip the clamps.
+  const float e = stride * (float)hp;
+  const float ex = fabsf(ax) * e + fabsf(bx) * e, ey = fabsf(ay) * e + fabsf(by) * e;
+  const bool inside = scx - ex >= 1.5f && scx + ex <= (float)src.W - 3.5f &&
+                      scy - ey >= 1.5f && scy + ey <= (float)src.H - 3.5f;
+  const int istride = (int)stride;
   for (int iy = -hp; iy <= hp; ++iy)
     for (int ix = -hp; ix <= hp; ++ix) {
       const float fdx = stride * (float)ix, fdy = stride * (float)iy;
-      const float rv = acm_sample(ref, ((float)cx + fdx) + 0.5f, ((float)cy + fdy) + 0.5f);
+      // Reference taps sit on integer texels (integer strides).
+      const float rv = acm_texel(ref, cx + istride * ix, cy + istride * iy);
       const float sx = (scx + ax * fdx) + bx * fdy;
       const float sy = (scy + ay * fdx) + by * fdy;
-      const float sv = acm_sample(src, sx + 0.5f, sy + 0.5f);
+      const float sv = inside ? acm_sample_inside(src, sx + 0.5f, sy + 0.5f)
+                              : acm_sample(src, sx + 0.5f, sy + 0.5f);
       const float dist2 = fdx * fdx + fdy * fdy;
       const float r = rv - rc;
       const float w = acm_exp(dist2 * sf + (r * r) * cf);
@@ -267,7 +296,7 @@ __device__ float census(const AImg& ref, const AImg& src, float rc, float sc, in
   for (int dy = -2; dy <= 2; ++dy)
     for (int dx = -2; dx <= 2; ++dx) {
       if (dx == 0 && dy == 0) continue;
-      const float rv = acm_sample(ref, (float)(cx + dx) + 0.5f, (float)(cy + dy) + 0.5f);
+      const float rv = acm_texel(ref, cx + dx, cy + dy);
       const float sx = (scx + ax * (float)dx) + bx * (float)dy;
       const float sy = (scy + ay * (float)dx) + by * (float)dy;
       const float sv = acm_sample(src, sx + 0.5f, sy + 0.5f);
@@ -321,7 +350,7 @@ __device__ void cost_vector(const AScene& S, int x, int y, float4 plane, float* 
   const float3 cw = acm_backproject(c0, (float)x, (float)y, depth);
   const float3 wdx = acm_backproject(c0, (float)(x + 1), (float)y, ddx);
   const float3 wdy = acm_backproject(c0, (float)x, (float)(y + 1), ddy);
-  const float rc = acm_sample(S.img[0], (float)x + 0.5f, (float)y + 0.5f);
+  const float rc = acm_texel(S.img[0], x, y);
   const float sf = -1.0f / (2.0f * S.sigma_spatial * S.sigma_spatial);
   const float cf = -1.0f / (2.0f * S.sigma_color * S.sigma_color);
   for (int i = 0; i < S.n_src; ++i) out[i] = single_cost(S, i, cw, wdx, wdy, rc, x, y, sf, cf);
