@@ -33,6 +33,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "dense_b200.h"
@@ -834,6 +835,11 @@ __global__ void acm_median_kernel(int W, int H, const float* __restrict__ depth,
 }
 
 // ------------------------------------------------------------------ host
+// The stream a level runs on, for stream-ordered allocation: references run
+// concurrently on their own streams, and a plain cudaFree would wait for the
+// whole device.
+thread_local cudaStream_t tl_stream = nullptr;
+
 template <typename T>
 struct DBuf {
   T* p = nullptr;
@@ -841,15 +847,17 @@ struct DBuf {
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
-  ~DBuf() {
-    if (p) cudaFree(p);
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFreeAsync(p, tl_stream);
+    p = nullptr;
+    n = 0;
   }
   cudaError_t alloc(size_t count) {
     if (count <= n && p) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(count, 1) * sizeof(T));
+    release();
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&p),
+                                    std::max<size_t>(count, 1) * sizeof(T), tl_stream);
     if (e == cudaSuccess) n = count;
     return e;
   }
@@ -1117,12 +1125,18 @@ struct Coarse {
 // initialisation or upsampling from `coarse`, previous-level depths of the
 // linked sources, the iterations and the readback (with the median only on
 // the last level).  The result goes to ref.depth / normal / cost / conf.
+// The device work runs on stream s between events ev0 and ev1.
 static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, const Coarse* coarse,
-                           const std::vector<std::pair<int, const Coarse*>>& prev, float* ms) {
+                           const std::vector<std::pair<int, const Coarse*>>& prev, cudaStream_t s,
+                           cudaEvent_t ev0, cudaEvent_t ev1) {
   const int nv = (int)ref.views.size();
   ACHECK(nv >= 2, "a reference view needs at least one source view");
   const int n_img = std::min(nv, 1 + kMaxSrc);
-  cudaStream_t s = e->stream;
+  struct StreamScope {
+    cudaStream_t old;
+    explicit StreamScope(cudaStream_t s) : old(tl_stream) { tl_stream = s; }
+    ~StreamScope() { tl_stream = old; }
+  } scope(s);
   const float scale = (float)(1.0 / std::pow(2.0, n_levels - 1 - level));
   std::vector<std::unique_ptr<DBuf<float>>> imgs;
   AScene S{};
@@ -1222,10 +1236,7 @@ static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, cons
     ACUDA(cudaMemcpyAsync(src_planes.p, hsrc.data(), hsrc.size() * sizeof(float4),
                           cudaMemcpyHostToDevice, s));
   }
-  cudaEvent_t e0, e1;
-  ACUDA(cudaEventCreate(&e0));
-  ACUDA(cudaEventCreate(&e1));
-  ACUDA(cudaEventRecord(e0, s));
+  ACUDA(cudaEventRecord(ev0, s));
   if (coarse)
     acm_upsample_kernel<<<grid, blk, 0, s>>>(dS.p, st, src_planes.p, coarse->W, coarse->H);
   else
@@ -1240,7 +1251,7 @@ static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, cons
   const bool last = level == n_levels - 1;
   if (last) acm_median_kernel<<<grid, blk, 0, s>>>(W, H, depth.p, depth2.p);
   ACUDA(cudaGetLastError());
-  ACUDA(cudaEventRecord(e1, s));
+  ACUDA(cudaEventRecord(ev1, s));
   ref.W = W;
   ref.H = H;
   ref.depth.resize(npix);
@@ -1252,24 +1263,18 @@ static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, cons
   ACUDA(cudaMemcpyAsync(ref.normal.data(), normal.p, 3 * npix * sizeof(float),
                         cudaMemcpyDeviceToHost, s));
   ACUDA(cudaMemcpyAsync(ref.cost.data(), cost.p, npix * sizeof(float), cudaMemcpyDeviceToHost, s));
-  const cudaError_t err = cudaStreamSynchronize(s);
-  float t = 0.0f;
-  if (err == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  ACUDA(err);
-  *ms += t;
-  // Logistic confidence on the host, as the reference computes it
-  // (estimator.cc:1023-1037).
-  for (size_t i = 0; i < npix; ++i)
-    if (ref.depth[i] > 0.0f) ref.conf[i] = 1.0f / (1.0f + std::exp((ref.cost[i] - 0.5f) * 5.0f));
+  ACUDA(cudaStreamSynchronize(s));
   return DN_OK;
 }
 
-// Run (cluster_estimator.cc:82-138): levels outermost, references in turn;
-// a reference's previous-level depths for the geometric term come from the
-// linked references' latest results (those of this level for references
-// already done, of the last level for the rest), as in the reference.
+// Run (cluster_estimator.cc:82-138): levels outermost, references in turn.
+// A reference's previous-level depths for the geometric term come from the
+// linked references' latest results: those of this level for references
+// already done, of the last level for the rest, as in the reference.  That
+// order matters only when a level uses previous depths; otherwise the
+// references of a level are independent and run concurrently, each on its
+// own stream (up to 8 at a time).  last_ms sums, over the levels, the device
+// span from the first reference's start to the last one's end.
 extern "C" dn_status dn_acmmp_run(dn_acmmp* e) {
   ACHECK(e, "NULL estimator");
   if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no reference views");
@@ -1278,31 +1283,100 @@ extern "C" dn_status dn_acmmp_run(dn_acmmp* e) {
   const int n_levels = std::max(1, e->hierarchy_levels);
   const int n_refs = (int)e->refs.size();
   std::vector<Coarse> latest(n_refs);  // each reference's latest intermediate result
-  for (int level = 0; level < n_levels; ++level) {
-    for (int i = 0; i < n_refs; ++i) {
-      ARef& ref = e->refs[i];
-      std::vector<std::pair<int, const Coarse*>> prev;
-      if (level > 0 && e->geom_weight > 0.0f)
-        for (size_t l = 0; l + 2 < e->geom_links.size(); l += 3)
-          if (e->geom_links[l] == i) {
-            const int fr = e->geom_links[l + 2];
-            if (fr >= 0 && fr < n_refs && !latest[fr].depth.empty())
-              prev.emplace_back(e->geom_links[l + 1], &latest[fr]);
-          }
-      Coarse own;
-      const bool up = level > 0;
-      if (up) own = latest[i];  // a copy: latest[i] is replaced below
-      const dn_status st = run_level(e, ref, level, n_levels, up ? &own : nullptr, prev, &e->last_ms);
-      if (st != DN_OK) return st;
-      if (level < n_levels - 1) {
-        latest[i].W = ref.W;
-        latest[i].H = ref.H;
-        latest[i].depth = ref.depth;
-        latest[i].normal = ref.normal;
-        latest[i].cost = ref.cost;
-      }
+  const int n_par = std::min(n_refs, 8);
+  std::vector<cudaStream_t> streams(n_par, nullptr);
+  std::vector<cudaEvent_t> ev0(n_refs, nullptr), ev1(n_refs, nullptr);
+  cudaEvent_t eref = nullptr;
+  struct Cleanup {
+    std::vector<cudaStream_t>& s;
+    std::vector<cudaEvent_t>& a;
+    std::vector<cudaEvent_t>& b;
+    cudaEvent_t& r;
+    ~Cleanup() {
+      for (auto x : s)
+        if (x) cudaStreamDestroy(x);
+      for (auto x : a)
+        if (x) cudaEventDestroy(x);
+      for (auto x : b)
+        if (x) cudaEventDestroy(x);
+      if (r) cudaEventDestroy(r);
     }
+  } cleanup{streams, ev0, ev1, eref};
+  for (auto& x : streams) ACUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+  for (int i = 0; i < n_refs; ++i) {
+    ACUDA(cudaEventCreate(&ev0[i]));
+    ACUDA(cudaEventCreate(&ev1[i]));
   }
+  ACUDA(cudaEventCreate(&eref));
+
+  auto links_of = [&](int i) {
+    std::vector<std::pair<int, const Coarse*>> prev;
+    for (size_t l = 0; l + 2 < e->geom_links.size(); l += 3)
+      if (e->geom_links[l] == i) {
+        const int fr = e->geom_links[l + 2];
+        if (fr >= 0 && fr < n_refs && !latest[fr].depth.empty())
+          prev.emplace_back(e->geom_links[l + 1], &latest[fr]);
+      }
+    return prev;
+  };
+  auto keep = [&](int i, int level) {
+    if (level < n_levels - 1) {
+      const ARef& ref = e->refs[i];
+      latest[i].W = ref.W;
+      latest[i].H = ref.H;
+      latest[i].depth = ref.depth;
+      latest[i].normal = ref.normal;
+      latest[i].cost = ref.cost;
+    }
+  };
+
+  for (int level = 0; level < n_levels; ++level) {
+    const bool uses_prev = level > 0 && e->geom_weight > 0.0f && !e->geom_links.empty();
+    ACUDA(cudaEventRecord(eref, e->stream));
+    ACUDA(cudaStreamSynchronize(e->stream));
+    if (uses_prev) {
+      for (int i = 0; i < n_refs; ++i) {
+        Coarse own = latest[i];  // a copy: latest[i] is replaced below
+        const dn_status st = run_level(e, e->refs[i], level, n_levels, level > 0 ? &own : nullptr,
+                                       links_of(i), streams[0], ev0[i], ev1[i]);
+        if (st != DN_OK) return st;
+        keep(i, level);
+      }
+    } else {
+      const std::vector<Coarse> own = latest;  // the upsampling inputs of this level
+      std::vector<dn_status> sts(n_refs, DN_OK);
+      std::vector<std::string> msgs(n_refs);
+      for (int i0 = 0; i0 < n_refs; i0 += n_par) {
+        std::vector<std::thread> pool;
+        for (int i = i0; i < std::min(n_refs, i0 + n_par); ++i)
+          pool.emplace_back([&, i]() {
+            cudaSetDevice(e->device);
+            const std::vector<std::pair<int, const Coarse*>> none;
+            sts[i] = run_level(e, e->refs[i], level, n_levels, level > 0 ? &own[i] : nullptr,
+                               none, streams[i - i0], ev0[i], ev1[i]);
+            if (sts[i] != DN_OK) msgs[i] = g_acm_error;
+          });
+        for (auto& t : pool) t.join();
+      }
+      for (int i = 0; i < n_refs; ++i)
+        if (sts[i] != DN_OK) return afail(sts[i], msgs[i]);
+      for (int i = 0; i < n_refs; ++i) keep(i, level);
+    }
+    float t_first = 0.0f, t_last = 0.0f;
+    for (int i = 0; i < n_refs; ++i) {
+      float a = 0.0f, b = 0.0f;
+      ACUDA(cudaEventElapsedTime(&a, eref, ev0[i]));
+      ACUDA(cudaEventElapsedTime(&b, eref, ev1[i]));
+      t_first = i == 0 ? a : std::min(t_first, a);
+      t_last = i == 0 ? b : std::max(t_last, b);
+    }
+    e->last_ms += t_last - t_first;
+  }
+  // Logistic confidence on the host, as the reference computes it
+  // (estimator.cc:1023-1037).
+  for (auto& ref : e->refs)
+    for (size_t i = 0; i < ref.depth.size(); ++i)
+      if (ref.depth[i] > 0.0f) ref.conf[i] = 1.0f / (1.0f + std::exp((ref.cost[i] - 0.5f) * 5.0f));
   return DN_OK;
 }
 
