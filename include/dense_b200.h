@@ -467,7 +467,7 @@ const char* dn_svo_last_error(void);
  * at python/pybind.cc:53-104) over the live path's PatchMatch estimator
  * (estimator.cc:120-243, 941-1040; kernels opencl_kernels.h:44-1124,
  * 1298-2099), no SfM planar prior.  Levels run coarsest first: images
- * area-downscaled by 2^k (sizes must divide), each reference initialised
+ * area-downscaled by 2^k (OpenCV's INTER_AREA), each reference initialised
  * randomly on the first level and from its own coarser result above it,
  * with the linked references' previous-level depths in a geometric term.
  * Per level: red/black PatchMatch passes (bilateral NCC over strides 1-3,
@@ -485,7 +485,7 @@ dn_status dn_acmmp_destroy(dn_acmmp* e);
 dn_status dn_acmmp_set_max_iterations(dn_acmmp* e, int n);
 dn_status dn_acmmp_set_patch_size(dn_acmmp* e, int size);
 dn_status dn_acmmp_set_max_image_size(dn_acmmp* e, int size);
-/* Pyramid levels; image sizes must divide by 2^(levels - 1). */
+/* Pyramid levels (the reference's default pipeline uses 4). */
 dn_status dn_acmmp_set_hierarchy_levels(dn_acmmp* e, int levels);
 dn_status dn_acmmp_set_sigma_spatial(dn_acmmp* e, float v);
 dn_status dn_acmmp_set_sigma_color(dn_acmmp* e, float v);

@@ -1043,6 +1043,60 @@ static void resize_area_u8(const uint8_t* src, int W, int H, int k, uint8_t* dst
     }
 }
 
+// cv::resize(INTER_AREA) of an 8-bit image to (w, h) when the ratios are not
+// both integers (OpenCV's general area path): per axis a table of source
+// cells and float weights (overlap over cell width), a horizontal pass per
+// source row and a vertical accumulation in float, rounded half to even.
+struct AreaTab {
+  int di, si;
+  float alpha;
+};
+
+static int area_table(int ssize, int dsize, double scale, AreaTab* t) {
+  int k = 0;
+  for (int dx = 0; dx < dsize; ++dx) {
+    const double fsx1 = dx * scale, fsx2 = fsx1 + scale;
+    const double cell = std::min(scale, ssize - fsx1);
+    int sx1 = (int)std::ceil(fsx1), sx2 = (int)std::floor(fsx2);
+    sx2 = std::min(sx2, ssize - 1);
+    sx1 = std::min(sx1, sx2);
+    if (sx1 - fsx1 > 1e-3) t[k++] = AreaTab{dx, sx1 - 1, (float)((sx1 - fsx1) / cell)};
+    for (int sx = sx1; sx < sx2; ++sx) t[k++] = AreaTab{dx, sx, (float)(1.0 / cell)};
+    if (fsx2 - sx2 > 1e-3)
+      t[k++] = AreaTab{dx, sx2, (float)(std::min(std::min(fsx2 - sx2, 1.0), cell) / cell)};
+  }
+  return k;
+}
+
+static void resize_area_general_u8(const uint8_t* src, int W, int H, uint8_t* dst, int w, int h) {
+  const double sx = 1.0 / ((double)w / W), sy = 1.0 / ((double)h / H);
+  std::vector<AreaTab> xt(2 * (size_t)(W + 2)), yt(2 * (size_t)(H + 2));
+  std::vector<float> buf(w), sum(w);
+  const int nx = area_table(W, w, sx, xt.data()), ny = area_table(H, h, sy, yt.data());
+  auto flush = [&](int row) {
+    for (int dx = 0; dx < w; ++dx) {
+      const int v = (int)std::nearbyint(sum[dx]);
+      dst[(size_t)row * w + dx] = (uint8_t)std::min(255, std::max(0, v));
+    }
+  };
+  int prev = -1;
+  for (int j = 0; j < ny; ++j) {
+    const int dy = yt[j].di;
+    const float beta = yt[j].alpha;
+    const uint8_t* S = src + (size_t)yt[j].si * W;
+    std::fill(buf.begin(), buf.end(), 0.0f);
+    for (int k = 0; k < nx; ++k) buf[xt[k].di] += (float)S[xt[k].si] * xt[k].alpha;
+    if (dy != prev) {
+      if (prev >= 0) flush(prev);
+      for (int dx = 0; dx < w; ++dx) sum[dx] = beta * buf[dx];
+      prev = dy;
+    } else {
+      for (int dx = 0; dx < w; ++dx) sum[dx] += beta * buf[dx];
+    }
+  }
+  if (prev >= 0) flush(prev);
+}
+
 // The previous-level depth resize (UploadPreviousDepths uses INTER_LINEAR):
 // OpenCV's pixel-centre mapping, FP32 weights, each operation rounded by
 // itself.  OpenCV's SIMD arithmetic can differ from this in the last bits.
@@ -1099,12 +1153,13 @@ static dn_status level_view(const AView& v, float scale, LevelView* out) {
   }
   const int nw = std::max((int)((float)v.W * scale), 1), nh = std::max((int)((float)v.H * scale), 1);
   const int k = v.W / nw;
-  ACHECK(nw * k == v.W && nh * k == v.H && v.H / nh == k,
-         "hierarchy levels need image sizes divisible by 2^(levels - 1)");
   out->W = nw;
   out->H = nh;
   out->scaled.resize((size_t)nw * nh);
-  resize_area_u8(v.img.data(), v.W, v.H, k, out->scaled.data());
+  if (nw * k == v.W && nh * k == v.H && v.H / nh == k)
+    resize_area_u8(v.img.data(), v.W, v.H, k, out->scaled.data());  // integer ratio
+  else
+    resize_area_general_u8(v.img.data(), v.W, v.H, out->scaled.data(), nw, nh);
   out->img = out->scaled.data();
   const float sx = (float)nw / (float)v.W, sy = (float)nh / (float)v.H;
   out->K[0] *= (double)sx;

@@ -763,6 +763,8 @@ def _acm_level_lib():
                                      _f]
         L.or_acmmp_level.restype = ctypes.c_int
         L.or_resize_area_u8.argtypes = [_u8, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8]
+        L.or_resize_area_general_u8.argtypes = [_u8, ctypes.c_int, ctypes.c_int, _u8,
+                                                ctypes.c_int, ctypes.c_int]
         L.or_resize_linear_f32.argtypes = [_f, ctypes.c_int, ctypes.c_int, _f, ctypes.c_int,
                                            ctypes.c_int]
         L._acm_level_ready = True
@@ -776,6 +778,19 @@ def acm_resize_area(img, k):
     H, W = im.shape
     out = np.zeros((H // k, W // k), np.uint8)
     L.or_resize_area_u8(_P(im, _u8), W, H, int(k), _P(out, _u8))
+    return out
+
+
+def acm_resize_area_to(img, w, h):
+    """cv::resize(INTER_AREA) of an 8-bit image to (w, h): the fast path for
+    integer ratios, the general area path otherwise."""
+    L = _acm_level_lib()
+    im = np.ascontiguousarray(img, np.uint8)
+    H, W = im.shape
+    if W % w == 0 and H % h == 0 and W // w == H // h:
+        return acm_resize_area(im, W // w)
+    out = np.zeros((h, w), np.uint8)
+    L.or_resize_area_general_u8(_P(im, _u8), W, H, _P(out, _u8), int(w), int(h))
     return out
 
 
@@ -794,7 +809,7 @@ def port_acmmp_cluster(refs, hierarchy_levels=1, iterations=3, patch_size=11, si
                        geom_weight=0.0, geom_links=()):
     """DepthmapClusterEstimator::Run (cluster_estimator.cc:82-138) over
     RunLevel (estimator.cc:159-243) in the C restatement, levels outermost:
-    the pyramid (estimator.cc:562-588; sizes must divide by 2^(levels-1)),
+    the pyramid (estimator.cc:562-588, OpenCV's area resize),
     upsampling from each reference's own coarser result, and previous-level
     depths of linked references for the geometric term (updated in place as
     the references of a level finish, as the reference does).
@@ -821,10 +836,7 @@ def port_acmmp_cluster(refs, hierarchy_levels=1, iterations=3, patch_size=11, si
                     h0, w0 = img.shape
                     nw = max(int(np.float32(w0) * scale), 1)
                     nh = max(int(np.float32(h0) * scale), 1)
-                    k = w0 // nw
-                    if w0 != nw * k or h0 != nh * k or h0 // nh != k:
-                        raise ValueError("image sizes must divide by 2^(levels - 1)")
-                    img = acm_resize_area(img, k)
+                    img = acm_resize_area_to(img, nw, nh)
                     sx = np.float32(nw) / np.float32(w0)
                     sy = np.float32(nh) / np.float32(h0)
                     K = K.copy()

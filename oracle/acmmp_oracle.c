@@ -847,6 +847,82 @@ void or_resize_area_u8(const uint8_t* src, int W, int H, int k, uint8_t* dst) {
     }
 }
 
+/* cv::resize(INTER_AREA) of an 8-bit image to (w, h) when the ratios are not
+ * both integers (OpenCV's general area path): per axis a table of source
+ * cells and float weights (the overlap of each source pixel with the
+ * destination cell over the cell width), a horizontal pass per source row
+ * and a vertical accumulation, all in float, rounded half to even. */
+typedef struct {
+  int di, si;
+  float alpha;
+} acm_area_tab;
+
+static int acm_area_table(int ssize, int dsize, double scale, acm_area_tab* t) {
+  int k = 0;
+  for (int dx = 0; dx < dsize; ++dx) {
+    const double fsx1 = dx * scale, fsx2 = fsx1 + scale;
+    const double cell = scale < ssize - fsx1 ? scale : ssize - fsx1;
+    int sx1 = (int)ceil(fsx1), sx2 = (int)floor(fsx2);
+    if (sx2 > ssize - 1) sx2 = ssize - 1;
+    if (sx1 > sx2) sx1 = sx2;
+    if (sx1 - fsx1 > 1e-3) {
+      t[k].di = dx;
+      t[k].si = sx1 - 1;
+      t[k++].alpha = (float)((sx1 - fsx1) / cell);
+    }
+    for (int sx = sx1; sx < sx2; ++sx) {
+      t[k].di = dx;
+      t[k].si = sx;
+      t[k++].alpha = (float)(1.0 / cell);
+    }
+    if (fsx2 - sx2 > 1e-3) {
+      double a = fsx2 - sx2 < 1.0 ? fsx2 - sx2 : 1.0;
+      if (a > cell) a = cell;
+      t[k].di = dx;
+      t[k].si = sx2;
+      t[k++].alpha = (float)(a / cell);
+    }
+  }
+  return k;
+}
+
+void or_resize_area_general_u8(const uint8_t* src, int W, int H, uint8_t* dst, int w, int h) {
+  const double sx = 1.0 / ((double)w / W), sy = 1.0 / ((double)h / H);
+  acm_area_tab* xt = (acm_area_tab*)malloc(sizeof(acm_area_tab) * 2 * (size_t)(W + 2));
+  acm_area_tab* yt = (acm_area_tab*)malloc(sizeof(acm_area_tab) * 2 * (size_t)(H + 2));
+  float* buf = (float*)malloc(sizeof(float) * (size_t)w);
+  float* sum = (float*)malloc(sizeof(float) * (size_t)w);
+  const int nx = acm_area_table(W, w, sx, xt), ny = acm_area_table(H, h, sy, yt);
+  int prev = -1;
+  for (int j = 0; j < ny; ++j) {
+    const int dy = yt[j].di;
+    const float beta = yt[j].alpha;
+    const uint8_t* S = src + (size_t)yt[j].si * W;
+    for (int dx = 0; dx < w; ++dx) buf[dx] = 0.0f;
+    for (int k = 0; k < nx; ++k) buf[xt[k].di] += (float)S[xt[k].si] * xt[k].alpha;
+    if (dy != prev) {
+      if (prev >= 0)
+        for (int dx = 0; dx < w; ++dx) {
+          const int v = (int)nearbyintf(sum[dx]);
+          dst[(size_t)prev * w + dx] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
+        }
+      for (int dx = 0; dx < w; ++dx) sum[dx] = beta * buf[dx];
+      prev = dy;
+    } else {
+      for (int dx = 0; dx < w; ++dx) sum[dx] += beta * buf[dx];
+    }
+  }
+  if (prev >= 0)
+    for (int dx = 0; dx < w; ++dx) {
+      const int v = (int)nearbyintf(sum[dx]);
+      dst[(size_t)prev * w + dx] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
+    }
+  free(xt);
+  free(yt);
+  free(buf);
+  free(sum);
+}
+
 /* Bilinear resize of a float image with OpenCV's pixel-centre mapping
  * (f = (d + 0.5) src/dst - 0.5 in double, clamped to the border pixels),
  * FP32 weights 1 - f and f, the horizontal then the vertical blend, each

@@ -418,7 +418,9 @@ def test_acmmp_oracle_known_answers():
 
 def test_acmmp_pyramid_resizes_against_opencv():
     """The estimator's pyramid: cv::resize(INTER_AREA) by 2, 4 and 8 is
-    reproduced exactly; the previous-depth bilinear resize follows OpenCV's
+    reproduced exactly, on the fast path (integer ratios) and on the general
+    area path (sizes that do not divide); the previous-depth bilinear resize
+    follows OpenCV's
     INTER_LINEAR mapping and agrees to a few ulp (OpenCV's SIMD arithmetic
     differs in the last bits, so the library fixes its own order)."""
     cv2 = pytest.importorskip("cv2")
@@ -430,6 +432,13 @@ def test_acmmp_pyramid_resizes_against_opencv():
             im = rng.integers(0, 256, (H, W), dtype=np.uint8)
             want = cv2.resize(im, (W // k, H // k), interpolation=cv2.INTER_AREA)
             assert np.array_equal(O.acm_resize_area(im, k), want), (k, H, W)
+    for _ in range(60):
+        H, W = (int(v) for v in rng.integers(5, 150, 2))
+        s = float(rng.choice([0.5, 0.25, 0.125]))
+        h, w = max(1, int(H * s)), max(1, int(W * s))
+        im = rng.integers(0, 256, (H, W), dtype=np.uint8)
+        want = cv2.resize(im, (w, h), interpolation=cv2.INTER_AREA)
+        assert np.array_equal(O.acm_resize_area_to(im, w, h), want), (H, W, h, w)
     d = rng.uniform(1, 30, (24, 32)).astype(np.float32)
     d[rng.random(d.shape) < 0.2] = 0
     got = O.acm_resize_linear(d, 64, 48)
