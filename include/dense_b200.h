@@ -465,8 +465,8 @@ const char* dn_svo_last_error(void);
 /* ----------------------------------------------------------------------
  * DepthmapClusterEstimator (cluster.h, cluster_estimator.cc:21-147, bound
  * at python/pybind.cc:53-104) over the live path's PatchMatch estimator
- * (estimator.cc:120-243, 941-1040; kernels opencl_kernels.h:44-1124,
- * 1298-2099), no SfM planar prior.  Levels run coarsest first: images
+ * (estimator.cc:120-243, 664-1040; kernels opencl_kernels.h:44-1124,
+ * 1298-2099), with the SfM planar prior.  Levels run coarsest first: images
  * area-downscaled by 2^k (OpenCV's INTER_AREA), each reference initialised
  * randomly on the first level and from its own coarser result above it,
  * with the linked references' previous-level depths in a geometric term.
@@ -504,7 +504,10 @@ dn_status dn_acmmp_begin_ref_view(dn_acmmp* e, const double K[9], const double R
 dn_status dn_acmmp_add_source_view(dn_acmmp* e, const double K[9], const double R[9],
                                    const double t[3], const uint8_t* image, int width, int height,
                                    int stride);
-/* SetSfMPoints: only n = 0 is accepted (the planar prior is not built). */
+/* SetSfMPoints (estimator.cc:108-118): world points (rows of 3) of the last
+ * reference; each level projects them, triangulates (Delaunay), fits a
+ * plane per triangle and centres the refinement hypotheses of the covered
+ * pixels on it (estimator.cc:664-940). */
 dn_status dn_acmmp_set_sfm_points(dn_acmmp* e, const double* points, int64_t n);
 /* AddGeomLink (cluster_estimator.cc:73-80): above the first level, source
  * `source_view_idx` of `ref_idx` takes `from_ref_idx`'s previous depths. */

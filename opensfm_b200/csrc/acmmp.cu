@@ -1,8 +1,8 @@
 // DepthmapClusterEstimator (cluster.h, cluster_estimator.cc:21-147) over the
 // live path's PatchMatch estimator (estimator.h:33-135, estimator.cc:120-243,
 // 473-558, 941-1040) and its kernels (opencl_kernels.h:44-1124, 1298-1826,
-// 1828-2099): pyramid levels with upsampling and geometric consistency, no
-// SfM planar prior.
+// 1828-2099): pyramid levels with upsampling and geometric consistency, and
+// the SfM planar prior (estimator.cc:664-940).
 //
 // Per reference view and level: a random initialisation with top-k view
 // selection (or, above the coarsest level, the coarser result upsampled),
@@ -78,6 +78,8 @@ struct AScene {
   float depth_min, depth_max;
   const float* prev;   // [16][H][W] previous-level source depths, or null
   unsigned prev_mask;  // sources with a previous depth (0 without a geometric weight)
+  const float4* prior_planes;  // SfM planar prior per pixel, or null
+  const unsigned* prior_mask;  // pixels the prior covers
 };
 struct AState {
   float4* planes;  // (nx, ny, nz, d): n . X + d = 0 in the camera frame
@@ -689,14 +691,36 @@ __global__ void __launch_bounds__(64) acm_pm_kernel(const AScene* __restrict__ S
   const float pert = 0.02f;
   const float PI_F = 3.14159274101257324f;
   const float3 cur_n = acm_normalize(make_float3(plane_now.x, plane_now.y, plane_now.z));
-  const float lmin = acm_log(S.depth_min > 1e-6f ? S.depth_min : 1e-6f);
-  const float lmax = acm_log(S.depth_max > 1e-5f ? S.depth_max : 1e-5f);
-  const float depth_rand = acm_exp(lmin + acm_rand(s, key + 503u) * (lmax - lmin));
+  // The SfM planar prior (where it covers the pixel) centres the random
+  // hypothesis on its plane: depth within 3 sigma, normal within 5 degrees.
+  const bool have_prior = S.prior_mask != nullptr && S.prior_mask[idx] > 0u;
+  float depth_prior = 0.0f;
+  float3 prior_n = make_float3(0.0f, 0.0f, -1.0f);
+  if (have_prior) {
+    const float4 pp = S.prior_planes[idx];
+    depth_prior = acm_depth(c0, (float)x, (float)y, pp);
+    prior_n = acm_normalize(make_float3(pp.x, pp.y, pp.z));
+  }
+  float depth_rand;
   float3 nr;
-  nr.x = acm_rand(s, key + 504u) * 2.0f - 1.0f;
-  nr.y = acm_rand(s, key + 505u) * 2.0f - 1.0f;
-  nr.z = -1.0f;
-  nr = acm_normalize(nr);
+  if (have_prior && depth_prior > 0.0f) {
+    const float depth_sigma = (S.depth_max - S.depth_min) / 32.0f;
+    const float angle_sigma = PI_F * (5.0f / 180.0f);
+    depth_rand = depth_prior - 3.0f * depth_sigma + acm_rand(s, key + 503u) * 6.0f * depth_sigma;
+    depth_rand = acm_clamp(depth_rand, S.depth_min, S.depth_max);
+    const float q1 = (acm_rand(s, key + 504u) - 0.5f) * angle_sigma;
+    const float q2 = (acm_rand(s, key + 505u) - 0.5f) * angle_sigma;
+    nr = acm_normalize(make_float3(prior_n.x + q1, prior_n.y + q2, prior_n.z));
+    if (nr.z > 0.0f) nr.z = -nr.z;
+  } else {
+    const float lmin = acm_log(S.depth_min > 1e-6f ? S.depth_min : 1e-6f);
+    const float lmax = acm_log(S.depth_max > 1e-5f ? S.depth_max : 1e-5f);
+    depth_rand = acm_exp(lmin + acm_rand(s, key + 503u) * (lmax - lmin));
+    nr.x = acm_rand(s, key + 504u) * 2.0f - 1.0f;
+    nr.y = acm_rand(s, key + 505u) * 2.0f - 1.0f;
+    nr.z = -1.0f;
+    nr = acm_normalize(nr);
+  }
   const float dmn = (1.0f - pert) * depth_now, dmx = (1.0f + pert) * depth_now;
   const float depth_pert =
       acm_clamp(dmn + acm_rand(s, key + 510u) * (dmx - dmn), S.depth_min, S.depth_max);
@@ -871,6 +895,7 @@ struct AView {
 struct ARef {
   std::vector<AView> views;  // [0] the reference
   float depth_min, depth_max;
+  std::vector<double> sfm;  // SfM points (world, rows of 3) for the planar prior
   int W = 0, H = 0;  // size of the result
   std::vector<float> depth, normal, cost, conf;
 };
@@ -998,8 +1023,10 @@ extern "C" dn_status dn_acmmp_add_source_view(dn_acmmp* e, const double* K, cons
 extern "C" dn_status dn_acmmp_set_sfm_points(dn_acmmp* e, const double* points, int64_t n) {
   ACHECK(e, "NULL estimator");
   if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no ref view started");
-  (void)points;
-  ACHECK(n == 0, "the SfM planar prior (estimator.cc:108-118, 644-940) is not built");
+  ACHECK(n >= 0 && (n == 0 || points), "NULL points");
+  for (int64_t i = 0; i < 3 * n; ++i) ACHECK(std::isfinite(points[i]), "SfM points must be finite");
+  // SetSfMPoints (estimator.cc:108-118) replaces the reference's points.
+  e->refs.back().sfm.assign(points, points + 3 * n);
   return DN_OK;
 }
 
@@ -1135,6 +1162,230 @@ static void resize_linear_f32(const float* src, int w, int h, float* dst, int W,
   }
 }
 
+// Delaunay triangulation of 2-D points (Bowyer-Watson, double precision,
+// inside a super-triangle 1000 times the points' extent).  Exact duplicates
+// join the first.  Returns triangles as ascending index triples, sorted.
+struct Tri {
+  int a, b, c;
+};
+
+static std::vector<Tri> delaunay(const std::vector<double>& px, const std::vector<double>& py) {
+  const int n = (int)px.size();
+  std::vector<Tri> out;
+  if (n < 3) return out;
+  double x0 = px[0], x1 = px[0], y0 = py[0], y1 = py[0];
+  for (int i = 0; i < n; ++i) {
+    x0 = std::min(x0, px[i]);
+    x1 = std::max(x1, px[i]);
+    y0 = std::min(y0, py[i]);
+    y1 = std::max(y1, py[i]);
+  }
+  const double span = std::max(std::max(x1 - x0, y1 - y0), 1.0) * 1000.0;
+  const double mx = 0.5 * (x0 + x1), my = 0.5 * (y0 + y1);
+  std::vector<double> X(px), Y(py);
+  X.push_back(mx - 2 * span);
+  Y.push_back(my - span);
+  X.push_back(mx + 2 * span);
+  Y.push_back(my - span);
+  X.push_back(mx);
+  Y.push_back(my + 2 * span);
+  struct T {
+    int v[3];
+    double cx, cy, r2;
+  };
+  auto make = [&](int a, int b, int c) {
+    T t;
+    t.v[0] = a;
+    t.v[1] = b;
+    t.v[2] = c;
+    const double ax = X[a], ay = Y[a], bx = X[b], by = Y[b], cx = X[c], cy = Y[c];
+    const double d = 2.0 * (ax * (by - cy) + bx * (cy - ay) + cx * (ay - by));
+    if (d == 0.0) {
+      t.cx = t.cy = 0.0;
+      t.r2 = -1.0;  // degenerate: never contains a point, removed by the next insert near it
+      return t;
+    }
+    const double a2 = ax * ax + ay * ay, b2 = bx * bx + by * by, c2 = cx * cx + cy * cy;
+    t.cx = (a2 * (by - cy) + b2 * (cy - ay) + c2 * (ay - by)) / d;
+    t.cy = (a2 * (cx - bx) + b2 * (ax - cx) + c2 * (bx - ax)) / d;
+    t.r2 = (ax - t.cx) * (ax - t.cx) + (ay - t.cy) * (ay - t.cy);
+    return t;
+  };
+  std::vector<T> tris;
+  tris.push_back(make(n, n + 1, n + 2));
+  std::vector<int> seen;  // first index of each distinct position
+  for (int i = 0; i < n; ++i) {
+    bool dup = false;
+    for (int j : seen)
+      if (X[j] == X[i] && Y[j] == Y[i]) {
+        dup = true;
+        break;
+      }
+    if (dup) continue;
+    seen.push_back(i);
+    std::vector<std::pair<int, int>> edges;
+    std::vector<T> keep;
+    keep.reserve(tris.size() + 2);
+    for (const T& t : tris) {
+      const double dx = X[i] - t.cx, dy = Y[i] - t.cy;
+      if (t.r2 >= 0.0 && dx * dx + dy * dy < t.r2) {
+        for (int k = 0; k < 3; ++k) edges.emplace_back(t.v[k], t.v[(k + 1) % 3]);
+      } else {
+        keep.push_back(t);
+      }
+    }
+    // The boundary of the cavity: edges of exactly one removed triangle.
+    for (size_t a = 0; a < edges.size(); ++a) {
+      bool shared = false;
+      for (size_t b = 0; b < edges.size(); ++b)
+        if (a != b && ((edges[a].first == edges[b].second && edges[a].second == edges[b].first) ||
+                       (edges[a].first == edges[b].first && edges[a].second == edges[b].second))) {
+          shared = true;
+          break;
+        }
+      if (!shared) keep.push_back(make(edges[a].first, edges[a].second, i));
+    }
+    tris.swap(keep);
+  }
+  for (const T& t : tris) {
+    if (t.v[0] >= n || t.v[1] >= n || t.v[2] >= n) continue;
+    int v[3] = {t.v[0], t.v[1], t.v[2]};
+    std::sort(v, v + 3);
+    out.push_back(Tri{v[0], v[1], v[2]});
+  }
+  std::sort(out.begin(), out.end(), [](const Tri& p, const Tri& q) {
+    return p.a != q.a ? p.a < q.a : (p.b != q.b ? p.b < q.b : p.c < q.c);
+  });
+  return out;
+}
+
+// ComputeSfMPlanarPrior (estimator.cc:664-940) at one level: the SfM points
+// projected into the reference (K of this level), a Delaunay triangulation
+// of their pixels, a plane per triangle through its three camera-frame
+// points (the triangle skipped across a depth ratio above 1.5 or over 20000
+// px^2), the triangles rasterised in order with the reference's parametric
+// loop, and the pixels whose prior depth lies in the range.  The plane is
+// the unit normal of the two edge vectors' cross product with d >= 0 (the
+// reference takes the SVD null vector of the 3 x 4 system: the same plane).
+// Returns false when fewer than 4 points project.
+static bool sfm_prior(const ARef& ref, const double* K, int w, int h, std::vector<float4>& planes,
+                      std::vector<unsigned>& mask) {
+  const float fx = (float)K[0], fy = (float)K[4], cx = (float)K[2], cy = (float)K[5];
+  const double* R = ref.views[0].R;
+  const double* t = ref.views[0].t;
+  struct Proj {
+    float u, v, depth, cam[3];
+  };
+  std::vector<Proj> pr;
+  const size_t n = ref.sfm.size() / 3;
+  for (size_t i = 0; i < n; ++i) {
+    const double* X = &ref.sfm[3 * i];
+    double c[3];
+    for (int r = 0; r < 3; ++r) c[r] = ((R[3 * r] * X[0] + R[3 * r + 1] * X[1]) + R[3 * r + 2] * X[2]) + t[r];
+    if (c[2] <= 0.0) continue;
+    const float depth = (float)c[2];
+    if (depth < ref.depth_min || depth > ref.depth_max) continue;
+    const float u = (float)((double)fx * (c[0] / c[2]) + (double)cx);
+    const float v = (float)((double)fy * (c[1] / c[2]) + (double)cy);
+    if (u < 0.0f || u >= (float)w || v < 0.0f || v >= (float)h) continue;
+    pr.push_back(Proj{u, v, depth, {(float)c[0], (float)c[1], (float)c[2]}});
+  }
+  planes.assign((size_t)w * h, make_float4(0.0f, 0.0f, -1.0f, 0.0f));
+  mask.assign((size_t)w * h, 0u);
+  if (pr.size() < 4) return false;
+  std::vector<double> px(pr.size()), py(pr.size());
+  for (size_t i = 0; i < pr.size(); ++i) {
+    px[i] = pr[i].u;
+    py[i] = pr[i].v;
+  }
+  const std::vector<Tri> tris = delaunay(px, py);
+  // The vertex lookup keys on the integer pixel; the last point wins.
+  std::vector<int> key_to(pr.size());
+  std::vector<std::pair<long long, int>> keys;
+  for (size_t i = 0; i < pr.size(); ++i) keys.emplace_back((long long)(int)pr[i].v * w + (int)pr[i].u, (int)i);
+  auto lookup = [&](long long k) {
+    int best = -1;
+    for (const auto& kv : keys)
+      if (kv.first == k) best = kv.second;
+    return best;
+  };
+  struct TriPlane {
+    int x[3], y[3];
+    float4 plane;
+  };
+  std::vector<TriPlane> kept;
+  for (const Tri& tr : tris) {
+    const int id[3] = {tr.a, tr.b, tr.c};
+    TriPlane tp;
+    int src[3];
+    bool ok = true;
+    for (int k = 0; k < 3; ++k) {
+      tp.x[k] = (int)pr[id[k]].u;
+      tp.y[k] = (int)pr[id[k]].v;
+      if (tp.x[k] < 0 || tp.x[k] >= w || tp.y[k] < 0 || tp.y[k] >= h) ok = false;
+      src[k] = ok ? lookup((long long)tp.y[k] * w + tp.x[k]) : -1;
+      if (src[k] < 0) ok = false;
+    }
+    if (!ok) continue;
+    const float d1 = pr[src[0]].depth, d2 = pr[src[1]].depth, d3 = pr[src[2]].depth;
+    const float dmin = std::min(d1, std::min(d2, d3)), dmax = std::max(d1, std::max(d2, d3));
+    if (dmin > 0.0f && dmax / dmin > 1.5f) continue;
+    const float ax = (float)(tp.x[1] - tp.x[0]), ay = (float)(tp.y[1] - tp.y[0]);
+    const float bx = (float)(tp.x[2] - tp.x[0]), by = (float)(tp.y[2] - tp.y[0]);
+    if (0.5f * std::fabs(ax * by - ay * bx) > 20000.0f) continue;
+    const float* P1 = pr[src[0]].cam;
+    const float* P2 = pr[src[1]].cam;
+    const float* P3 = pr[src[2]].cam;
+    const float e1[3] = {P2[0] - P1[0], P2[1] - P1[1], P2[2] - P1[2]};
+    const float e2[3] = {P3[0] - P1[0], P3[1] - P1[1], P3[2] - P1[2]};
+    float nn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                   e1[0] * e2[1] - e1[1] * e2[0]};
+    const float len = std::sqrt((nn[0] * nn[0] + nn[1] * nn[1]) + nn[2] * nn[2]);
+    if (!(len > 0.0f)) continue;
+    for (int k = 0; k < 3; ++k) nn[k] = nn[k] / len;
+    float d = -((nn[0] * P1[0] + nn[1] * P1[1]) + nn[2] * P1[2]);
+    if (1.0f / std::sqrt(1.0f + d * d) < 1e-8f) continue;
+    if (d < 0.0f) {
+      for (int k = 0; k < 3; ++k) nn[k] = -nn[k];
+      d = -d;
+    }
+    tp.plane = make_float4(nn[0], nn[1], nn[2], d);
+    kept.push_back(tp);
+  }
+  std::vector<int> tri_at((size_t)w * h, 0);
+  for (size_t ti = 0; ti < kept.size(); ++ti) {
+    const TriPlane& tp = kept[ti];
+    const float l01 = std::hypot((float)(tp.x[0] - tp.x[1]), (float)(tp.y[0] - tp.y[1]));
+    const float l02 = std::hypot((float)(tp.x[0] - tp.x[2]), (float)(tp.y[0] - tp.y[2]));
+    const float l12 = std::hypot((float)(tp.x[1] - tp.x[2]), (float)(tp.y[1] - tp.y[2]));
+    const float max_edge = std::max(l01, std::max(l02, l12));
+    if (max_edge < 1.0f) continue;
+    const float step = 1.0f / max_edge;
+    for (float p = 0.0f; p < 1.0f; p += step)
+      for (float q = 0.0f; q < 1.0f - p; q += step) {
+        const int xx = (int)(p * (float)tp.x[0] + q * (float)tp.x[1] + (1.0f - p - q) * (float)tp.x[2]);
+        const int yy = (int)(p * (float)tp.y[0] + q * (float)tp.y[1] + (1.0f - p - q) * (float)tp.y[2]);
+        if (xx >= 0 && xx < w && yy >= 0 && yy < h) tri_at[(size_t)yy * w + xx] = (int)ti + 1;
+      }
+  }
+  bool any = false;
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const size_t i = (size_t)y * w + x;
+      if (!tri_at[i]) continue;
+      const float4 pl = kept[tri_at[i] - 1].plane;
+      const float r0 = ((float)x - cx) / fx, r1 = ((float)y - cy) / fy;
+      const float den = (pl.x * r0 + pl.y * r1) + pl.z * 1.0f;
+      const float d = std::fabs(den) > 1e-6f ? -pl.w / den : 0.0f;
+      if (d >= ref.depth_min && d <= ref.depth_max) {
+        planes[i] = pl;
+        mask[i] = 1u;
+        any = true;
+      }
+    }
+  return any;
+}
+
 // A view at one pyramid level (BuildImagePyramid, estimator.cc:562-588).
 struct LevelView {
   int W, H;
@@ -1229,6 +1480,27 @@ static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, cons
   S.depth_min = ref.depth_min;
   S.depth_max = ref.depth_max;
   const size_t npix = (size_t)W * H;
+  // ComputeSfMPlanarPrior at this level's size and K.
+  DBuf<float4> d_prior;
+  DBuf<unsigned> d_pmask;
+  S.prior_planes = nullptr;
+  S.prior_mask = nullptr;
+  if (!ref.sfm.empty()) {
+    LevelView lv0;
+    dn_status st0 = level_view(ref.views[0], scale, &lv0);
+    if (st0 != DN_OK) return st0;
+    std::vector<float4> hp;
+    std::vector<unsigned> hm;
+    if (sfm_prior(ref, lv0.K, W, H, hp, hm)) {
+      ACUDA(d_prior.alloc(npix));
+      ACUDA(d_pmask.alloc(npix));
+      ACUDA(cudaMemcpyAsync(d_prior.p, hp.data(), npix * sizeof(float4), cudaMemcpyHostToDevice, s));
+      ACUDA(cudaMemcpyAsync(d_pmask.p, hm.data(), npix * sizeof(unsigned), cudaMemcpyHostToDevice, s));
+      ACUDA(cudaStreamSynchronize(s));
+      S.prior_planes = d_prior.p;
+      S.prior_mask = d_pmask.p;
+    }
+  }
   // UploadPreviousDepths (estimator.cc:56-106).
   DBuf<float> d_prev;
   S.prev = nullptr;

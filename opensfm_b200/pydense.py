@@ -467,8 +467,8 @@ class SVOFuser(_Handle):
 class DepthmapClusterEstimator(_Handle):
     """``dense::DepthmapClusterEstimator`` (``cluster.h``, bound at
     ``python/pybind.cc:53-104``) on the B200: the live path's PatchMatch
-    estimator with its pyramid levels and geometric consistency, no SfM
-    planar prior.  ``run()`` returns,
+    estimator with its pyramid levels, geometric consistency and SfM planar
+    prior.  ``run()`` returns,
     per reference view, ``[depth (H,W) f32, normal (H,W,3) f32, cost (H,W)
     f32, confidence (H,W) f32]``."""
 

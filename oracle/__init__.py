@@ -755,12 +755,23 @@ def _acm_level_lib():
     if not getattr(L, "_acm_level_ready", False):
         pp = ctypes.POINTER(ctypes.c_void_p)
         ip = ctypes.POINTER(ctypes.c_int)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        dp = ctypes.POINTER(ctypes.c_double)
         L.or_acmmp_level.argtypes = [pp, ip, ip, pp, pp, pp, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int,
                                      ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                      ctypes.c_float, ctypes.c_float, _f, _f, ctypes.c_int,
-                                     ctypes.c_int, _f, ctypes.c_uint32, ctypes.c_int, _f, _f, _f,
-                                     _f]
+                                     ctypes.c_int, _f, ctypes.c_uint32, _f, u32p, ctypes.c_int,
+                                     _f, _f, _f, _f]
+        L.or_acmmp_sfm_project.argtypes = [dp, ctypes.c_long, dp, dp, dp, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_float, ctypes.c_float, _f, _f,
+                                           _f]
+        L.or_acmmp_sfm_project.restype = ctypes.c_long
+        L.or_acmmp_sfm_prior.argtypes = [_f, _f, _f, ctypes.c_long,
+                                         ctypes.POINTER(ctypes.c_int), ctypes.c_long, dp,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                         ctypes.c_float, _f, u32p]
+        L.or_acmmp_sfm_prior.restype = ctypes.c_long
         L.or_acmmp_level.restype = ctypes.c_int
         L.or_resize_area_u8.argtypes = [_u8, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8]
         L.or_resize_area_general_u8.argtypes = [_u8, ctypes.c_int, ctypes.c_int, _u8,
@@ -804,6 +815,42 @@ def acm_resize_linear(depth, W, H):
     return out
 
 
+def acm_sfm_prior(points, K, R, t, W, H, depth_min, depth_max):
+    """ComputeSfMPlanarPrior (estimator.cc:664-940) in the restatement: the
+    projection and the per-triangle planes, rasterisation and depth check in
+    C; the Delaunay triangulation by scipy (Qhull), whose triangles are the
+    unique Delaunay ones for points in general position (the reference uses
+    cv::Subdiv2D).  Returns (planes (H, W, 4) f32, mask (H, W) uint32), or
+    None when fewer than 4 points project."""
+    from scipy.spatial import Delaunay
+
+    L = _acm_level_lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    p = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    K = np.ascontiguousarray(K, np.float64).reshape(9)
+    R = np.ascontiguousarray(R, np.float64).reshape(9)
+    t = np.ascontiguousarray(t, np.float64).reshape(3)
+    n = len(p)
+    uv = np.zeros((max(n, 1), 2), np.float32)
+    dep = np.zeros(max(n, 1), np.float32)
+    cam = np.zeros((max(n, 1), 3), np.float32)
+    m = L.or_acmmp_sfm_project(p.ctypes.data_as(dp), n, K.ctypes.data_as(dp),
+                               R.ctypes.data_as(dp), t.ctypes.data_as(dp), int(W), int(H),
+                               float(depth_min), float(depth_max), _P(uv, _f), _P(dep, _f),
+                               _P(cam, _f))
+    if m < 4:
+        return None
+    tri = np.sort(Delaunay(uv[:m].astype(np.float64)).simplices, axis=1)
+    tri = tri[np.lexsort((tri[:, 2], tri[:, 1], tri[:, 0]))].astype(np.int32).copy()
+    planes = np.zeros((H, W, 4), np.float32)
+    mask = np.zeros((H, W), np.uint32)
+    L.or_acmmp_sfm_prior(_P(uv, _f), _P(dep, _f), _P(cam, _f), m,
+                         tri.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(tri),
+                         K.ctypes.data_as(dp), int(W), int(H), float(depth_min), float(depth_max),
+                         _P(planes, _f), mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    return planes, mask
+
+
 def port_acmmp_cluster(refs, hierarchy_levels=1, iterations=3, patch_size=11, sigma_spatial=5.0,
                        sigma_color=3.0 / 255.0, top_k=4, census_weight=0.3, smooth_weight=0.0,
                        geom_weight=0.0, geom_links=()):
@@ -812,9 +859,11 @@ def port_acmmp_cluster(refs, hierarchy_levels=1, iterations=3, patch_size=11, si
     the pyramid (estimator.cc:562-588, OpenCV's area resize),
     upsampling from each reference's own coarser result, and previous-level
     depths of linked references for the geometric term (updated in place as
-    the references of a level finish, as the reference does).
+    the references of a level finish, as the reference does), and each
+    level's SfM planar prior where a reference has "sfm" points.
     refs: [dict(views=[(K, R, t, image u8), ...] (reference first),
-    depth_min, depth_max)]; geom_links: (ref, source index, from ref).
+    depth_min, depth_max, optional sfm (N, 3))]; geom_links: (ref, source
+    index, from ref).
     Returns [(depth, normal, cost, confidence)] per reference."""
     L = _acm_level_lib()
     N = max(1, int(hierarchy_levels))
@@ -866,6 +915,13 @@ def port_acmmp_cluster(refs, hierarchy_levels=1, iterations=3, patch_size=11, si
             cw = ch = 0
             if level > 0:
                 cd, cn, _, cw, ch = coarse[i]
+            prior = None
+            if ref.get("sfm") is not None and len(ref["sfm"]):
+                K0, R0, t0, _ = views[0]
+                prior = acm_sfm_prior(ref["sfm"], K0, R0, t0, W, H, ref["depth_min"],
+                                      ref["depth_max"])
+                if prior is not None and not prior[1].any():
+                    prior = None
             depth = np.zeros((H, W), np.float32)
             nrm = np.zeros((H, W, 3), np.float32)
             cost = np.zeros((H, W), np.float32)
@@ -876,7 +932,10 @@ def port_acmmp_cluster(refs, hierarchy_levels=1, iterations=3, patch_size=11, si
                 float(smooth_weight), float(geom_weight), float(ref["depth_min"]),
                 float(ref["depth_max"]), None if cd is None else _P(cd, _f),
                 None if cn is None else _P(cn, _f), cw, ch,
-                None if pd is None else _P(pd, _f), mask, int(level == N - 1), _P(depth, _f),
+                None if pd is None else _P(pd, _f), mask,
+                None if prior is None else _P(prior[0], _f),
+                None if prior is None else prior[1].ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                int(level == N - 1), _P(depth, _f),
                 _P(nrm, _f), _P(cost, _f), _P(conf, _f))
             if rc:
                 raise ValueError(f"or_acmmp_level failed ({rc})")

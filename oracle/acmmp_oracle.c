@@ -413,6 +413,8 @@ static float acm_smoothness(const float* planes, const acm_cam* c, const float* 
 typedef struct {
   const float* depths;
   uint32_t mask;
+  const float* prior_planes; /* [H][W][4] SfM planar prior, or NULL */
+  const uint32_t* prior_mask;
 } acm_prev;
 
 /* compute_geom_consistency_cost (opencl_kernels.h:945-990): the forward-
@@ -653,17 +655,43 @@ static void acm_pm_pixel(const acm_scene* S, const acm_params* P, acm_state* st,
 
   /* Refinement: five combinations of random / perturbed depth and normal. */
   const float pert = 0.02f;
-  const float PI_F = 3.14159274101257324f;
   float cur_n[3] = {plane_now[0], plane_now[1], plane_now[2]};
   acm_normalize(cur_n);
-  const float lmin = acm_log(P->depth_min > 1e-6f ? P->depth_min : 1e-6f);
-  const float lmax = acm_log(P->depth_max > 1e-5f ? P->depth_max : 1e-5f);
-  const float depth_rand = acm_exp(lmin + acm_rand(s, key + 503u) * (lmax - lmin));
-  float nr[3];
-  nr[0] = acm_rand(s, key + 504u) * 2.0f - 1.0f;
-  nr[1] = acm_rand(s, key + 505u) * 2.0f - 1.0f;
-  nr[2] = -1.0f;
-  acm_normalize(nr);
+  const float PI_F = 3.14159274101257324f;
+  /* The SfM planar prior (opencl_kernels.h:1660-1740) centres the random
+   * hypothesis on its plane where it covers the pixel. */
+  const int have_prior = prev->prior_mask && prev->prior_mask[idx] > 0u;
+  float depth_prior = 0.0f, prior_n[3] = {0.0f, 0.0f, -1.0f};
+  if (have_prior) {
+    const float* pp = prev->prior_planes + 4 * (size_t)idx;
+    depth_prior = acm_depth_from_plane(c0, (float)x, (float)y, pp);
+    prior_n[0] = pp[0];
+    prior_n[1] = pp[1];
+    prior_n[2] = pp[2];
+    acm_normalize(prior_n);
+  }
+  float depth_rand, nr[3];
+  if (have_prior && depth_prior > 0.0f) {
+    const float dsig = (P->depth_max - P->depth_min) / 32.0f;
+    const float asig = PI_F * (5.0f / 180.0f);
+    depth_rand = depth_prior - 3.0f * dsig + acm_rand(s, key + 503u) * 6.0f * dsig;
+    depth_rand = acm_clampf(depth_rand, P->depth_min, P->depth_max);
+    const float q1 = (acm_rand(s, key + 504u) - 0.5f) * asig;
+    const float q2 = (acm_rand(s, key + 505u) - 0.5f) * asig;
+    nr[0] = prior_n[0] + q1;
+    nr[1] = prior_n[1] + q2;
+    nr[2] = prior_n[2];
+    acm_normalize(nr);
+    if (nr[2] > 0.0f) nr[2] = -nr[2];
+  } else {
+    const float lmin = acm_log(P->depth_min > 1e-6f ? P->depth_min : 1e-6f);
+    const float lmax = acm_log(P->depth_max > 1e-5f ? P->depth_max : 1e-5f);
+    depth_rand = acm_exp(lmin + acm_rand(s, key + 503u) * (lmax - lmin));
+    nr[0] = acm_rand(s, key + 504u) * 2.0f - 1.0f;
+    nr[1] = acm_rand(s, key + 505u) * 2.0f - 1.0f;
+    nr[2] = -1.0f;
+    acm_normalize(nr);
+  }
   const float dmn = (1.0f - pert) * depth_now, dmx = (1.0f + pert) * depth_now;
   float depth_pert = dmn + acm_rand(s, key + 510u) * (dmx - dmn);
   depth_pert = acm_clampf(depth_pert, P->depth_min, P->depth_max);
@@ -976,8 +1004,8 @@ int or_acmmp_level(const float* const* images, const int* widths, const int* hei
                    float sigma_color, int top_k, float census_weight, float smooth_weight,
                    float geom_weight, float depth_min, float depth_max, const float* cd,
                    const float* cn, int cw, int ch, const float* prev_depths, uint32_t prev_mask,
-                   int apply_median, float* out_depth, float* out_normal, float* out_cost,
-                   float* out_conf) {
+                   const float* prior_planes, const uint32_t* prior_mask, int apply_median,
+                   float* out_depth, float* out_normal, float* out_cost, float* out_conf) {
   if (num_images < 2) return -1;
   acm_params P;
   P.n_src = num_images - 1 < ACM_MAX_SRC ? num_images - 1 : ACM_MAX_SRC;
@@ -1013,7 +1041,8 @@ int or_acmmp_level(const float* const* images, const int* widths, const int* hei
   if (!st.planes || !st.costs || !st.rs || !st.sel) return -2;
   /* UploadPreviousDepths (estimator.cc:56-106) zeroes the mask without a
    * geometric weight. */
-  acm_prev prev = {prev_depths, (prev_depths && geom_weight > 0.0f) ? prev_mask : 0u};
+  acm_prev prev = {prev_depths, (prev_depths && geom_weight > 0.0f) ? prev_mask : 0u,
+                   prior_planes, prior_planes ? prior_mask : NULL};
   if (cd)
     acm_upsample(&S, &P, &st, cd, cn, cw, ch);
   else
@@ -1083,8 +1112,8 @@ int or_acmmp_run(const float* const* images, const int* widths, const int* heigh
                  float* out_normal, float* out_cost, float* out_conf) {
   return or_acmmp_level(images, widths, heights, Ks, Rs, ts, num_images, iterations, patch_size,
                         sigma_spatial, sigma_color, top_k, census_weight, smooth_weight,
-                        geom_weight, depth_min, depth_max, NULL, NULL, 0, 0, NULL, 0, 1,
-                        out_depth, out_normal, out_cost, out_conf);
+                        geom_weight, depth_min, depth_max, NULL, NULL, 0, 0, NULL, 0, NULL, NULL,
+                        1, out_depth, out_normal, out_cost, out_conf);
 }
 
 /* The random initialisation alone (planes [H][W][4], costs, selected views),
@@ -1129,4 +1158,144 @@ int or_acmmp_init(const float* const* images, const int* widths, const int* heig
   acm_random_init(&S, &P, &st);
   free(st.rs);
   return 0;
+}
+
+/* ComputeSfMPlanarPrior, first half (estimator.cc:683-728): the SfM points
+ * (world, double) projected with the level's K (cast to float) and the
+ * reference pose; those in front, in the depth range and inside the image
+ * are kept.  uv [2N], depth [N], cam [3N]; returns the count. */
+long or_acmmp_sfm_project(const double* pts, long n, const double* K, const double* R,
+                          const double* t, int w, int h, float depth_min, float depth_max,
+                          float* uv, float* depth, float* cam) {
+  const float fx = (float)K[0], fy = (float)K[4], cx = (float)K[2], cy = (float)K[5];
+  long m = 0;
+  for (long i = 0; i < n; ++i) {
+    const double* X = pts + 3 * i;
+    double c[3];
+    for (int r = 0; r < 3; ++r) c[r] = ((R[3 * r] * X[0] + R[3 * r + 1] * X[1]) + R[3 * r + 2] * X[2]) + t[r];
+    if (c[2] <= 0.0) continue;
+    const float d = (float)c[2];
+    if (d < depth_min || d > depth_max) continue;
+    const float u = (float)((double)fx * (c[0] / c[2]) + (double)cx);
+    const float v = (float)((double)fy * (c[1] / c[2]) + (double)cy);
+    if (u < 0.0f || u >= (float)w || v < 0.0f || v >= (float)h) continue;
+    uv[2 * m] = u;
+    uv[2 * m + 1] = v;
+    depth[m] = d;
+    cam[3 * m] = (float)c[0];
+    cam[3 * m + 1] = (float)c[1];
+    cam[3 * m + 2] = (float)c[2];
+    ++m;
+  }
+  return m;
+}
+
+/* ComputeSfMPlanarPrior, second half (estimator.cc:740-940) over given
+ * Delaunay triangles (ascending index triples, sorted): the integer-pixel
+ * vertex lookup (last point wins), the depth-ratio and area gates, the
+ * plane through the three camera points (unit cross-product normal, d >= 0),
+ * the parametric rasterisation in order and the depth-range check.  planes
+ * [H][W][4] (unset: 0, 0, -1, 0), mask [H][W].  Returns the masked count. */
+long or_acmmp_sfm_prior(const float* uv, const float* depth, const float* cam, long m,
+                        const int* tris, long n_tris, const double* K, int w, int h,
+                        float depth_min, float depth_max, float* planes, uint32_t* mask) {
+  const float fx = (float)K[0], fy = (float)K[4], cx = (float)K[2], cy = (float)K[5];
+  const size_t npix = (size_t)w * h;
+  for (size_t i = 0; i < npix; ++i) {
+    planes[4 * i] = 0.0f;
+    planes[4 * i + 1] = 0.0f;
+    planes[4 * i + 2] = -1.0f;
+    planes[4 * i + 3] = 0.0f;
+    mask[i] = 0u;
+  }
+  if (m < 4) return 0;
+  float* tp = (float*)malloc(sizeof(float) * 4 * (size_t)(n_tris + 1));
+  int* tx = (int*)malloc(sizeof(int) * 6 * (size_t)(n_tris + 1));
+  long kept = 0;
+  for (long ti = 0; ti < n_tris; ++ti) {
+    int px[3], py[3], src[3], ok = 1;
+    for (int k = 0; k < 3; ++k) {
+      const int v = tris[3 * ti + k];
+      px[k] = (int)uv[2 * v];
+      py[k] = (int)uv[2 * v + 1];
+      if (px[k] < 0 || px[k] >= w || py[k] < 0 || py[k] >= h) ok = 0;
+      src[k] = -1;
+      for (long j = 0; j < m; ++j)
+        if ((int)uv[2 * j + 1] == py[k] && (int)uv[2 * j] == px[k]) src[k] = (int)j;
+      if (src[k] < 0) ok = 0;
+    }
+    if (!ok) continue;
+    float dmin = depth[src[0]], dmax = depth[src[0]];
+    for (int k = 1; k < 3; ++k) {
+      if (depth[src[k]] < dmin) dmin = depth[src[k]];
+      if (depth[src[k]] > dmax) dmax = depth[src[k]];
+    }
+    if (dmin > 0.0f && dmax / dmin > 1.5f) continue;
+    const float ax = (float)(px[1] - px[0]), ay = (float)(py[1] - py[0]);
+    const float bx = (float)(px[2] - px[0]), by = (float)(py[2] - py[0]);
+    if (0.5f * fabsf(ax * by - ay * bx) > 20000.0f) continue;
+    const float* P1 = cam + 3 * src[0];
+    const float* P2 = cam + 3 * src[1];
+    const float* P3 = cam + 3 * src[2];
+    const float e1[3] = {P2[0] - P1[0], P2[1] - P1[1], P2[2] - P1[2]};
+    const float e2[3] = {P3[0] - P1[0], P3[1] - P1[1], P3[2] - P1[2]};
+    float nn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                   e1[0] * e2[1] - e1[1] * e2[0]};
+    const float len = sqrtf((nn[0] * nn[0] + nn[1] * nn[1]) + nn[2] * nn[2]);
+    if (!(len > 0.0f)) continue;
+    for (int k = 0; k < 3; ++k) nn[k] = nn[k] / len;
+    float d = -((nn[0] * P1[0] + nn[1] * P1[1]) + nn[2] * P1[2]);
+    if (1.0f / sqrtf(1.0f + d * d) < 1e-8f) continue;
+    if (d < 0.0f) {
+      for (int k = 0; k < 3; ++k) nn[k] = -nn[k];
+      d = -d;
+    }
+    float* pl = tp + 4 * kept;
+    pl[0] = nn[0];
+    pl[1] = nn[1];
+    pl[2] = nn[2];
+    pl[3] = d;
+    for (int k = 0; k < 3; ++k) {
+      tx[6 * kept + k] = px[k];
+      tx[6 * kept + 3 + k] = py[k];
+    }
+    ++kept;
+  }
+  int* at = (int*)calloc(npix, sizeof(int));
+  for (long ti = 0; ti < kept; ++ti) {
+    const int* X = tx + 6 * ti;
+    const int* Y = X + 3;
+    const float l01 = hypotf((float)(X[0] - X[1]), (float)(Y[0] - Y[1]));
+    const float l02 = hypotf((float)(X[0] - X[2]), (float)(Y[0] - Y[2]));
+    const float l12 = hypotf((float)(X[1] - X[2]), (float)(Y[1] - Y[2]));
+    float me = l01 > l02 ? l01 : l02;
+    if (l12 > me) me = l12;
+    if (me < 1.0f) continue;
+    const float step = 1.0f / me;
+    for (float p = 0.0f; p < 1.0f; p += step)
+      for (float q = 0.0f; q < 1.0f - p; q += step) {
+        const int xx = (int)(p * (float)X[0] + q * (float)X[1] + (1.0f - p - q) * (float)X[2]);
+        const int yy = (int)(p * (float)Y[0] + q * (float)Y[1] + (1.0f - p - q) * (float)Y[2]);
+        if (xx >= 0 && xx < w && yy >= 0 && yy < h) at[(size_t)yy * w + xx] = (int)ti + 1;
+      }
+  }
+  long filled = 0;
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const size_t i = (size_t)y * w + x;
+      if (!at[i]) continue;
+      const float* pl = tp + 4 * (at[i] - 1);
+      const float r0 = ((float)x - cx) / fx, r1 = ((float)y - cy) / fy;
+      const float den = (pl[0] * r0 + pl[1] * r1) + pl[2] * 1.0f;
+      const float dd = fabsf(den) > 1e-6f ? -pl[3] / den : 0.0f;
+      if (dd >= depth_min && dd <= depth_max) {
+        for (int k = 0; k < 4; ++k) planes[4 * i + k] = pl[k];
+        mask[i] = 1u;
+        ++filled;
+      }
+    }
+  free(at);
+  free(tp);
+  free(tx);
+  return filled;
 }

@@ -677,6 +677,51 @@ def test_cluster_estimator_levels_bit_identical_to_oracle(levels, geom, size):
             assert a.dtype == b.dtype and np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("levels", [1, 2])
+def test_cluster_estimator_sfm_prior_bit_identical_to_oracle(levels):
+    """The SfM planar prior: world points sampled on the scene's surface (as
+    a reconstruction's tracks would be), projected into each reference per
+    level, triangulated (the library's Bowyer-Watson against the oracle's
+    Qhull: the same unique Delaunay triangles), gated, planes fitted,
+    rasterised, and used to centre the refinement hypotheses."""
+    vs = S.ring_viewset(13, 5, 64, 48)
+    cams_ = vs.cameras
+    rng = np.random.default_rng(21)
+
+    def surface_points(k, n=300):
+        d, c = vs.depths[k], cams_[k]
+        H, W = d.shape
+        ys, xs = rng.integers(0, H, n), rng.integers(0, W, n)
+        dd = d[ys, xs]
+        ray = np.stack([xs + rng.uniform(0, 1, n), ys + rng.uniform(0, 1, n), np.ones(n)], -1)
+        Xc = (ray @ np.linalg.inv(c.K).T) * dd[:, None]
+        return ((Xc - c.t) @ c.R)[dd > 0]
+
+    e = pydense.DepthmapClusterEstimator()
+    e.set_max_iterations(2)
+    e.set_patch_size(5)
+    e.set_hierarchy_levels(levels)
+    refs = []
+    for ref, srcs in [(0, [1, 2, 4]), (3, [2, 4])]:
+        dmin, dmax = S.depth_range(vs.depths[ref])
+        c = cams_[ref]
+        e.begin_ref_view(c.K, c.R, c.t, vs.images[ref], dmin, dmax)
+        pts = surface_points(ref)
+        e.set_sfm_points(pts)
+        for s_ in srcs:
+            e.add_source_view(cams_[s_].K, cams_[s_].R, cams_[s_].t, vs.images[s_])
+        refs.append(dict(views=[(cams_[i].K, cams_[i].R, cams_[i].t, vs.images[i])
+                                for i in [ref] + srcs], depth_min=dmin, depth_max=dmax, sfm=pts))
+    got = e.run()
+    want = O.port_acmmp_cluster(refs, hierarchy_levels=levels, iterations=2, patch_size=5)
+    for g, w in zip(got, want):
+        for a, b in zip(g, w):
+            assert a.dtype == b.dtype and np.array_equal(a, b)
+    no_prior = O.port_acmmp_cluster([dict(r, sfm=None) for r in refs], hierarchy_levels=levels,
+                                    iterations=2, patch_size=5)
+    assert not all(np.array_equal(a[0], b[0]) for a, b in zip(want, no_prior))
+
+
 def test_cluster_estimator_errors(scene):
     e = pydense.DepthmapClusterEstimator()
     with pytest.raises(RuntimeError):
@@ -688,7 +733,7 @@ def test_cluster_estimator_errors(scene):
     e.add_source_view(scene.cameras[1].K, scene.cameras[1].R, scene.cameras[1].t,
                       scene.images[1])
     with pytest.raises(ValueError):
-        e.set_sfm_points(np.ones((4, 3)))
+        e.set_sfm_points(np.full((4, 3), np.nan))
     e.set_sfm_points(np.zeros((0, 3)))
     e.add_geom_link(0, 0, 0)
     with pytest.raises(RuntimeError):
