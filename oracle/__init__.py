@@ -4,13 +4,17 @@ Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 and reference legs import this package, and only as the checker or as the
 timed CPU baseline.  The product (``opensfm_b200``) never imports it.
 
-Three oracles:
+The oracles:
 
 ``port``
     ``depthmap_oracle.c``: this project's plain-C restatement of the
     reference's legacy path (``opensfm/src/lib/dense/src/depthmap.cc``):
     brute force, PatchMatch (raster schedule, seeded RNG), plane scoring,
-    median post-process, cleaner, pruner.
+    median post-process, cleaner, pruner.  The same library holds the C
+    restatements of the steps either side of it: ``fuser_oracle.c``
+    (``port_fuse``, ``port_sor``), ``svo_oracle.c`` (``port_svo``) and
+    ``acmmp_oracle.c`` (``port_acmmp``, ``port_acmmp_cluster``); and
+    ``gpu_clean_fp32`` restates the GPU cleaner's kernel in numpy.
 ``ref``
     The reference's own ``depthmap.cc`` compiled unmodified against the
     project's OpenCV shim (``oracle/Makefile`` -> ``oracle/_ref/``), driven
