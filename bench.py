@@ -169,54 +169,104 @@ def fusion_leg(b, vs, cands, n_maps, repeats=3, oracle=True):
     return out
 
 
-def acmmp_leg(vs, cands, n_refs=4, n_src=6, repeats=2, oracle=True):
-    """The live path's PatchMatch estimator (DepthmapClusterEstimator, one
-    level, its default parameters: patch 11, 3 iterations, top-k 4, census
-    0.3) on the first `n_refs` ring views at full size, each with its
-    `n_src` nearest views: device time and depthmaps/s.  With `oracle`, the
-    single-thread C restatement runs one reference at an eighth of the size
-    in each axis, the GPU runs the same case, and the outputs are compared."""
+ACMMP_SETTINGS = {
+    # DepthmapParams' own defaults (estimator.h:17-31), 6 sources.
+    "estimator_defaults": dict(n_src=6, levels=1, iterations=3, patch_size=11, top_k=4,
+                               smooth=0.0, geom=0.0, sfm=False),
+    # OpenSfM's dense pipeline (config.py:379-420, dense.py:608-735): 4 matching
+    # views, 4 iterations, patch 5, 4 pyramid levels, smoothness 0.3, geometric
+    # consistency 0.05 between the cluster's references, the SfM planar prior.
+    "pipeline_defaults": dict(n_src=4, levels=4, iterations=4, patch_size=5, top_k=4,
+                              smooth=0.3, geom=0.05, sfm=True),
+}
+
+
+def acmmp_leg(vs, cands, n_refs=4, repeats=2, oracle=True):
+    """The live path's PatchMatch estimator (DepthmapClusterEstimator) on the
+    first `n_refs` ring views at full size as one cluster, under its own
+    defaults and under the dense pipeline's: device time and depthmaps/s.
+    The SfM points for the prior are 2000 points per reference sampled on
+    the ray-cast surface (as a reconstruction's tracks would be).  With
+    `oracle`, the single-thread C restatement runs the same cluster at an
+    eighth of the size in each axis, the GPU runs it too, and the outputs
+    are compared."""
     from opensfm_b200 import pydense
     from opensfm_b200 import synthetic as S
 
-    def build(scale_views, refs):
+    def surface_points(views, k, n, seed):
+        rng = np.random.default_rng(seed)
+        d, c = views.depths[k], views.cameras[k]
+        H, W = d.shape
+        ys, xs = rng.integers(0, H, n), rng.integers(0, W, n)
+        dd = d[ys, xs]
+        ray = np.stack([xs + rng.uniform(0, 1, n), ys + rng.uniform(0, 1, n), np.ones(n)], -1)
+        Xc = (ray @ np.linalg.inv(c.K).T) * dd[:, None]
+        return ((Xc - c.t) @ c.R)[dd > 0]
+
+    def setup(views, refs, cfg, sfm_n):
         e = pydense.DepthmapClusterEstimator()
+        e.set_max_iterations(cfg["iterations"])
+        e.set_patch_size(cfg["patch_size"])
+        e.set_top_k(cfg["top_k"])
+        e.set_hierarchy_levels(cfg["levels"])
+        e.set_smooth_weight(cfg["smooth"])
+        e.set_geom_consistency_weight(cfg["geom"])
+        oracle_refs, links = [], []
         for ref in refs:
-            dmin, dmax = S.depth_range(scale_views.depths[ref])
-            c = scale_views.cameras[ref]
-            e.begin_ref_view(c.K, c.R, c.t, scale_views.images[ref], dmin, dmax)
-            for s_ in cands[ref][:n_src]:
-                cs = scale_views.cameras[s_]
-                e.add_source_view(cs.K, cs.R, cs.t, scale_views.images[s_])
-        return e
+            dmin, dmax = S.depth_range(views.depths[ref])
+            c = views.cameras[ref]
+            e.begin_ref_view(c.K, c.R, c.t, views.images[ref], dmin, dmax)
+            pts = surface_points(views, ref, sfm_n, 100 + ref) if cfg["sfm"] else None
+            if pts is not None:
+                e.set_sfm_points(pts)
+            srcs = list(cands[ref][:cfg["n_src"]])
+            for s_ in srcs:
+                cs = views.cameras[s_]
+                e.add_source_view(cs.K, cs.R, cs.t, views.images[s_])
+            oracle_refs.append(dict(views=[(views.cameras[i].K, views.cameras[i].R,
+                                            views.cameras[i].t, views.images[i])
+                                           for i in [ref] + srcs],
+                                    depth_min=dmin, depth_max=dmax, sfm=pts))
+        # dense.py:718-728: a reference's sources that are references too.
+        for i, ref in enumerate(refs):
+            srcs = list(cands[ref][:cfg["n_src"]])
+            for j, other in enumerate(refs):
+                if other != ref and other in srcs:
+                    links.append((i, srcs.index(other), j))
+                    e.add_geom_link(i, srcs.index(other), j)
+        return e, oracle_refs, links
 
-    e = build(vs, range(n_refs))
-    out = e.run()  # warm-up
-    ms = []
-    for _ in range(repeats):
-        out = e.run()
-        ms.append(e.last_run_ms())
-    t = float(np.median(ms))
-    res = {"refs": n_refs, "sources": n_src, "size": list(vs.images[0].shape[::-1]),
-           "device_ms": t, "depthmaps_per_s": n_refs / (t * 1e-3),
-           "accuracy_1pct_median": float(np.median([S.accuracy(o[0], vs.depths[i])
-                                                     for i, o in enumerate(out)]))}
-    if oracle:
-        import oracle as O
+    res = {"refs": n_refs, "size": list(vs.images[0].shape[::-1])}
+    for name, cfg in ACMMP_SETTINGS.items():
+        e, _, _ = setup(vs, list(range(n_refs)), cfg, 2000)
+        out = e.run()  # warm-up
+        ms = []
+        for _ in range(repeats):
+            out = e.run()
+            ms.append(e.last_run_ms())
+        t = float(np.median(ms))
+        r = dict(cfg, device_ms=t, depthmaps_per_s=n_refs / (t * 1e-3),
+                 accuracy_1pct_median=float(np.median([S.accuracy(o[0], vs.depths[i])
+                                                       for i, o in enumerate(out)])))
+        if oracle:
+            import oracle as O
 
-        H, W = vs.images[0].shape
-        small = S.ring_viewset(SEED, len(vs.images), W // 8, H // 8)
-        es = build(small, [0])
-        got = es.run()[0]
-        views = [(small.cameras[i].K, small.cameras[i].R, small.cameras[i].t, small.images[i])
-                 for i in [0] + list(cands[0][:n_src])]
-        dmin, dmax = S.depth_range(small.depths[0])
-        t0 = time.perf_counter()
-        want = O.port_acmmp(views, dmin, dmax)
-        res["oracle_sample"] = f"one {W // 8}x{H // 8} reference view, {n_src} sources"
-        res["oracle_1thread_s"] = time.perf_counter() - t0
-        res["sample_device_ms"] = es.last_run_ms()
-        res["identical_to_oracle"] = bool(all(np.array_equal(a, b) for a, b in zip(got, want)))
+            H, W = vs.images[0].shape
+            small = S.ring_viewset(SEED, len(vs.images), W // 8, H // 8)
+            es, orefs, links = setup(small, list(range(n_refs)), cfg, 200)
+            got = es.run()
+            t0 = time.perf_counter()
+            want = O.port_acmmp_cluster(orefs, hierarchy_levels=cfg["levels"],
+                                        iterations=cfg["iterations"],
+                                        patch_size=cfg["patch_size"], top_k=cfg["top_k"],
+                                        smooth_weight=cfg["smooth"], geom_weight=cfg["geom"],
+                                        geom_links=links)
+            r["oracle_sample"] = f"the same {n_refs}-view cluster at {W // 8}x{H // 8}"
+            r["oracle_1thread_s"] = time.perf_counter() - t0
+            r["sample_device_ms"] = es.last_run_ms()
+            r["identical_to_oracle"] = bool(all(np.array_equal(a, b) for g, w in zip(got, want)
+                                                for a, b in zip(g, w)))
+        res[name] = r
     return res
 
 

@@ -526,6 +526,12 @@ dn_status dn_acmmp_last_run_ms(dn_acmmp* e, float* ms);
 dn_status dn_acmmp_clear(dn_acmmp* e);
 /* Message for the last failed dn_acmmp_* call on this thread. */
 const char* dn_acmmp_last_error(void);
+/* The planar prior's Delaunay triangulation of n points (xy rows of 2)
+ * inside [0, w) x [0, h), with cv::Subdiv2D's virtual outer triangle;
+ * host only: *count triangles as ascending index triples, sorted, into
+ * tris (capacity triangles; NULL to query the count). */
+dn_status dn_delaunay_2d(const double* xy, int n, int w, int h, int* tris, int capacity,
+                         int* count);
 
 /* ----------------------------------------------------------------------
  * Depthmap files (host only, no GPU needed).  OpenSfM stores each view's

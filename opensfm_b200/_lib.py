@@ -163,6 +163,7 @@ _SIGNATURES = {
     "dn_acmmp_last_run_ms": ([_vp, ctypes.POINTER(ctypes.c_float)], _i),
     "dn_acmmp_clear": ([_vp], _i),
     "dn_acmmp_last_error": ([], ctypes.c_char_p),
+    "dn_delaunay_2d": ([_d, _i, _i, _i, ctypes.POINTER(_i), _i, ctypes.POINTER(_i)], _i),
     "dn_xxh32": ([_vp, ctypes.c_int64, ctypes.c_uint32], ctypes.c_uint32),
     "dn_lz4f_compress_bound": ([ctypes.c_int64], ctypes.c_int64),
     "dn_lz4f_compress": ([_vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],

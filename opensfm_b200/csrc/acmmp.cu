@@ -920,6 +920,8 @@ struct dn_acmmp {
 
 extern "C" const char* dn_acmmp_last_error(void) { return g_acm_error.c_str(); }
 
+
+
 extern "C" dn_status dn_acmmp_create(dn_acmmp** out) {
   ACHECK(out, "NULL output");
   *out = nullptr;
@@ -1162,33 +1164,30 @@ static void resize_linear_f32(const float* src, int w, int h, float* dst, int W,
   }
 }
 
-// Delaunay triangulation of 2-D points (Bowyer-Watson, double precision,
-// inside a super-triangle 1000 times the points' extent).  Exact duplicates
-// join the first.  Returns triangles as ascending index triples, sorted.
+// Delaunay triangulation of 2-D points inside the image rectangle
+// [0, w) x [0, h) (Bowyer-Watson, double precision).  The reference builds
+// it with cv::Subdiv2D, which starts from the virtual triangle (3M, 0),
+// (0, 3M), (-3M, -3M), M = max(w, h), and drops the triangles that touch
+// it; so does this, and the result is the Delaunay triangulation of the
+// points with those three vertices, less theirs.  Exact duplicates join the
+// first.  Returns triangles as ascending index triples, sorted.
 struct Tri {
   int a, b, c;
 };
 
-static std::vector<Tri> delaunay(const std::vector<double>& px, const std::vector<double>& py) {
+static std::vector<Tri> delaunay(const std::vector<double>& px, const std::vector<double>& py,
+                                 int w, int h) {
   const int n = (int)px.size();
   std::vector<Tri> out;
   if (n < 3) return out;
-  double x0 = px[0], x1 = px[0], y0 = py[0], y1 = py[0];
-  for (int i = 0; i < n; ++i) {
-    x0 = std::min(x0, px[i]);
-    x1 = std::max(x1, px[i]);
-    y0 = std::min(y0, py[i]);
-    y1 = std::max(y1, py[i]);
-  }
-  const double span = std::max(std::max(x1 - x0, y1 - y0), 1.0) * 1000.0;
-  const double mx = 0.5 * (x0 + x1), my = 0.5 * (y0 + y1);
+  const double big = 3.0 * (double)std::max(w, h);
   std::vector<double> X(px), Y(py);
-  X.push_back(mx - 2 * span);
-  Y.push_back(my - span);
-  X.push_back(mx + 2 * span);
-  Y.push_back(my - span);
-  X.push_back(mx);
-  Y.push_back(my + 2 * span);
+  X.push_back(big);
+  Y.push_back(0.0);
+  X.push_back(0.0);
+  Y.push_back(big);
+  X.push_back(-big);
+  Y.push_back(-big);
   struct T {
     int v[3];
     double cx, cy, r2;
@@ -1212,7 +1211,7 @@ static std::vector<Tri> delaunay(const std::vector<double>& px, const std::vecto
     return t;
   };
   std::vector<T> tris;
-  tris.push_back(make(n, n + 1, n + 2));
+  tris.push_back(make(n, n + 1, n + 2));  // counter-clockwise
   std::vector<int> seen;  // first index of each distinct position
   for (int i = 0; i < n; ++i) {
     bool dup = false;
@@ -1298,7 +1297,7 @@ static bool sfm_prior(const ARef& ref, const double* K, int w, int h, std::vecto
     px[i] = pr[i].u;
     py[i] = pr[i].v;
   }
-  const std::vector<Tri> tris = delaunay(px, py);
+  const std::vector<Tri> tris = delaunay(px, py, w, h);
   // The vertex lookup keys on the integer pixel; the last point wins.
   std::vector<int> key_to(pr.size());
   std::vector<std::pair<long long, int>> keys;
@@ -1731,5 +1730,25 @@ extern "C" dn_status dn_acmmp_get_result(dn_acmmp* e, int ref_idx, float* depth,
 extern "C" dn_status dn_acmmp_last_run_ms(dn_acmmp* e, float* ms) {
   ACHECK(e && ms, "NULL argument");
   *ms = e->last_ms;
+  return DN_OK;
+}
+
+extern "C" dn_status dn_delaunay_2d(const double* xy, int n, int w, int h, int* tris, int capacity,
+                                     int* count) {
+  ACHECK(count && (n == 0 || xy) && n >= 0 && w > 0 && h > 0, "bad argument");
+  std::vector<double> px(n), py(n);
+  for (int i = 0; i < n; ++i) {
+    px[i] = xy[2 * i];
+    py[i] = xy[2 * i + 1];
+  }
+  const std::vector<Tri> t = delaunay(px, py, w, h);
+  *count = (int)t.size();
+  ACHECK(!tris || capacity >= (int)t.size(), "capacity below the triangle count");
+  if (tris)
+    for (size_t i = 0; i < t.size(); ++i) {
+      tris[3 * i] = t[i].a;
+      tris[3 * i + 1] = t[i].b;
+      tris[3 * i + 2] = t[i].c;
+    }
   return DN_OK;
 }

@@ -819,12 +819,28 @@ def acm_resize_linear(depth, W, H):
     return out
 
 
+def acm_delaunay(xy, W, H):
+    """The prior's triangulation as cv::Subdiv2D builds it: the Delaunay
+    triangles (scipy's Qhull) of the points with the virtual vertices
+    (3M, 0), (0, 3M), (-3M, -3M), M = max(W, H), less those touching them;
+    ascending index triples, sorted."""
+    from scipy.spatial import Delaunay
+
+    xy = np.asarray(xy, np.float64).reshape(-1, 2)
+    n = len(xy)
+    big = 3.0 * max(W, H)
+    aug = np.concatenate([xy, [[big, 0.0], [0.0, big], [-big, -big]]])
+    t = Delaunay(aug).simplices
+    t = np.sort(t[(t < n).all(axis=1)], axis=1)
+    return t[np.lexsort((t[:, 2], t[:, 1], t[:, 0]))].astype(np.int32).copy()
+
+
 def acm_sfm_prior(points, K, R, t, W, H, depth_min, depth_max):
     """ComputeSfMPlanarPrior (estimator.cc:664-940) in the restatement: the
     projection and the per-triangle planes, rasterisation and depth check in
-    C; the Delaunay triangulation by scipy (Qhull), whose triangles are the
-    unique Delaunay ones for points in general position (the reference uses
-    cv::Subdiv2D).  Returns (planes (H, W, 4) f32, mask (H, W) uint32), or
+    C; the triangulation by acm_delaunay (scipy's Qhull over the points and
+    cv::Subdiv2D's virtual vertices).  Returns (planes (H, W, 4) f32, mask
+    (H, W) uint32), or
     None when fewer than 4 points project."""
     from scipy.spatial import Delaunay
 
@@ -844,8 +860,7 @@ def acm_sfm_prior(points, K, R, t, W, H, depth_min, depth_max):
                                _P(cam, _f))
     if m < 4:
         return None
-    tri = np.sort(Delaunay(uv[:m].astype(np.float64)).simplices, axis=1)
-    tri = tri[np.lexsort((tri[:, 2], tri[:, 1], tri[:, 0]))].astype(np.int32).copy()
+    tri = acm_delaunay(uv[:m].astype(np.float64), W, H)
     planes = np.zeros((H, W, 4), np.float32)
     mask = np.zeros((H, W), np.uint32)
     L.or_acmmp_sfm_prior(_P(uv, _f), _P(dep, _f), _P(cam, _f), m,

