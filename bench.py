@@ -240,12 +240,15 @@ def acmmp_leg(vs, cands, n_refs=4, repeats=2, oracle=True):
     for name, cfg in ACMMP_SETTINGS.items():
         e, _, _ = setup(vs, list(range(n_refs)), cfg, 2000)
         out = e.run()  # warm-up
-        ms = []
+        ms, host = [], []
         for _ in range(repeats):
+            t0 = time.perf_counter()
             out = e.run()
+            host.append(time.perf_counter() - t0)
             ms.append(e.last_run_ms())
         t = float(np.median(ms))
         r = dict(cfg, device_ms=t, depthmaps_per_s=n_refs / (t * 1e-3),
+                 host_s=float(np.median(host)),
                  accuracy_1pct_median=float(np.median([S.accuracy(o[0], vs.depths[i])
                                                        for i, o in enumerate(out)])))
         if oracle:

@@ -1600,7 +1600,9 @@ static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, cons
 // order matters only when a level uses previous depths; otherwise the
 // references of a level are independent and run concurrently, each on its
 // own stream (up to 8 at a time).  last_ms sums, over the levels, the device
-// span from the first reference's start to the last one's end.
+// time: the span from the first reference's start to the last one's end
+// where they run concurrently, the sum of their spans where they run in
+// turn (the host work between them is not device time).
 extern "C" dn_status dn_acmmp_run(dn_acmmp* e) {
   ACHECK(e, "NULL estimator");
   if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no reference views");
@@ -1688,15 +1690,16 @@ extern "C" dn_status dn_acmmp_run(dn_acmmp* e) {
         if (sts[i] != DN_OK) return afail(sts[i], msgs[i]);
       for (int i = 0; i < n_refs; ++i) keep(i, level);
     }
-    float t_first = 0.0f, t_last = 0.0f;
+    float t_first = 0.0f, t_last = 0.0f, t_sum = 0.0f;
     for (int i = 0; i < n_refs; ++i) {
       float a = 0.0f, b = 0.0f;
       ACUDA(cudaEventElapsedTime(&a, eref, ev0[i]));
       ACUDA(cudaEventElapsedTime(&b, eref, ev1[i]));
       t_first = i == 0 ? a : std::min(t_first, a);
       t_last = i == 0 ? b : std::max(t_last, b);
+      t_sum += b - a;
     }
-    e->last_ms += t_last - t_first;
+    e->last_ms += uses_prev ? t_sum : t_last - t_first;
   }
   // Logistic confidence on the host, as the reference computes it
   // (estimator.cc:1023-1037).
