@@ -340,6 +340,51 @@ __device__ float single_cost(const AScene& S, int i, float3 cw, float3 wdx, floa
   return (1.0f - blend) * nc + blend * cen;
 }
 
+// The warp of the reference patch into one source (compute_cost_vector's
+// per-view set-up, opencl_kernels.h:659-750): centre, the two affine steps
+// and the source value at the centre.
+struct SrcWarp {
+  float scx, scy, ax, ay, bx, by, sc;
+};
+
+// single_cost's set-up of source i; false (cost 2) where a projection falls
+// behind the source camera.
+__device__ inline bool warp_setup(const AScene& S, int i, float3 cw, float3 wdx, float3 wdy,
+                                  SrcWarp& w) {
+  const ACam& c = S.cam[1 + i];
+  const float3 p = acm_project(c, cw);
+  if (p.z < 1e-6f) return false;
+  w.scx = p.x / p.z;
+  w.scy = p.y / p.z;
+  const float3 pdx = acm_project(c, wdx), pdy = acm_project(c, wdy);
+  if (pdx.z < 1e-6f || pdy.z < 1e-6f) return false;
+  w.ax = pdx.x / pdx.z - w.scx;
+  w.ay = pdx.y / pdx.z - w.scy;
+  w.bx = pdy.x / pdy.z - w.scx;
+  w.by = pdy.y / pdy.z - w.scy;
+  w.sc = acm_sample(S.img[1 + i], w.scx + 0.5f, w.scy + 0.5f);
+  return true;
+}
+
+// single_cost's tail from the multi-scale NCC of source i.
+__device__ inline float finish_cost(const AScene& S, int i, const SrcWarp& w, float ncc, float rc,
+                                    int cx, int cy) {
+  const AImg& ref = S.img[0];
+  const AImg& src = S.img[1 + i];
+  if (ncc <= -0.5f) {
+    if (S.census_weight > 1e-6f)
+      return census(ref, src, rc, w.sc, cx, cy, w.scx, w.scy, w.ax, w.ay, w.bx, w.by);
+    return 2.0f;
+  }
+  const float nc = 1.0f - ncc;
+  if (S.census_weight < 1e-6f) return nc;
+  const float t = acm_clamp((nc - 0.1f) / (0.6f - 0.1f), 0.0f, 1.0f);
+  const float blend = S.census_weight * ((t * t) * (3.0f - 2.0f * t));
+  if (blend < 1e-4f) return nc;
+  const float cen = census(ref, src, rc, w.sc, cx, cy, w.scx, w.scy, w.ax, w.ay, w.bx, w.by);
+  return (1.0f - blend) * nc + blend * cen;
+}
+
 // compute_cost_vector (opencl_kernels.h:659-750): out[0 .. n_src).
 __device__ void cost_vector(const AScene& S, int x, int y, float4 plane, float* out) {
   const ACam& c0 = S.cam[0];
@@ -512,13 +557,127 @@ __global__ void acm_upsample_kernel(const AScene* __restrict__ Sp, AState st,
 
 // acmmp_patchmatch (opencl_kernels.h:1298-1826) for the pixels of one colour:
 // x = 2 gx + ((y + colour) & 1).
-__global__ void __launch_bounds__(64) acm_pm_kernel(const AScene* __restrict__ Sp, AState st,
-                                                    int colour, int iteration) {
+// The NCC work queue of one warp in shared memory, for n sources: the
+// lanes' pixels, the per-(lane, source) warps and NCC results, and the list
+// of evaluations of the current stride.  96 + 272 n words.
+__host__ __device__ constexpr int acm_queue_words(int n) { return 96 + 272 * n; }
+
+struct WarpQueue {
+  int* cx;
+  int* cy;
+  float* rc;
+  SrcWarp* prm;          // [32][n]
+  float* res;            // [32][n]
+  unsigned short* list;  // [32 n]: lane << 4 | source
+};
+
+__device__ inline WarpQueue warp_queue(float* base, int n) {
+  WarpQueue q;
+  q.cx = reinterpret_cast<int*>(base);
+  q.cy = reinterpret_cast<int*>(base + 32);
+  q.rc = base + 64;
+  q.prm = reinterpret_cast<SrcWarp*>(base + 96);
+  q.res = base + 96 + 224 * n;
+  q.list = reinterpret_cast<unsigned short*>(base + 96 + 256 * n);
+  return q;
+}
+
+// cost_vector for the 32 pixels of a warp, called by all its lanes together
+// (`act` false: the lane wants no costs and `out` is left alone).  Per
+// stride, the NCC evaluations still needed, one per (pixel, source), are
+// listed and spread over the lanes, so the warp walks each stride's patch
+// once per 32 evaluations instead of once per source with the lanes that
+// are done idle.  Each evaluation is the sequential walk of ncc_at_stride,
+// and each pixel's strides are decided as in ncc_multiscale, so the costs
+// are those of cost_vector.
+__device__ void cost_vector_warp(const AScene& S, const WarpQueue& q, int lane, bool act, int x,
+                                 int y, float4 plane, float* out) {
+  const int n_src = S.n_src;
+  unsigned on = 0u;
+  float rc = 0.0f;
+  if (act) {
+    const ACam& c0 = S.cam[0];
+    const float depth = acm_depth(c0, (float)x, (float)y, plane);
+    const float ddx = depth > 0.0f ? acm_depth(c0, (float)(x + 1), (float)y, plane) : 0.0f;
+    const float ddy = depth > 0.0f ? acm_depth(c0, (float)x, (float)(y + 1), plane) : 0.0f;
+    if (depth > 0.0f && ddx > 0.0f && ddy > 0.0f) {
+      const float3 cw = acm_backproject(c0, (float)x, (float)y, depth);
+      const float3 wdx = acm_backproject(c0, (float)(x + 1), (float)y, ddx);
+      const float3 wdy = acm_backproject(c0, (float)x, (float)(y + 1), ddy);
+      rc = acm_texel(S.img[0], x, y);
+      for (int i = 0; i < n_src; ++i) {
+        SrcWarp w;
+        if (warp_setup(S, i, cw, wdx, wdy, w)) {
+          on |= 1u << i;
+          q.prm[lane * n_src + i] = w;
+        }
+      }
+    }
+    for (int i = 0; i < n_src; ++i) out[i] = -1.0f;  // the best NCC so far
+  }
+  q.cx[lane] = x;
+  q.cy[lane] = y;
+  q.rc[lane] = rc;
+  const float sf = -1.0f / (2.0f * S.sigma_spatial * S.sigma_spatial);
+  const float cf = -1.0f / (2.0f * S.sigma_color * S.sigma_color);
+  unsigned need = on, textureless = 0u;
+  for (int st = 0; st < 3; ++st) {
+    // Source-major order: consecutive lanes take neighbouring pixels of one
+    // source, so their reads of that image stay close together.
+    int total = 0;
+    const unsigned below = (1u << lane) - 1u;
+    for (int v = 0; v < n_src; ++v) {
+      const bool mine = (need >> v) & 1u;
+      const unsigned ball = __ballot_sync(0xffffffffu, mine);
+      if (mine) q.list[total + __popc(ball & below)] = (unsigned short)((lane << 4) | v);
+      total += __popc(ball);
+    }
+    if (total == 0) break;
+    __syncwarp();
+    const float stride = (float)(st + 1);
+    for (int k = lane; k < total; k += 32) {
+      const int item = q.list[k], l = item >> 4, v = item & 15;
+      const SrcWarp w = q.prm[l * n_src + v];
+      q.res[l * n_src + v] =
+          ncc_at_stride(S.img[0], S.img[1 + v], q.rc[l], w.sc, w.scx, w.scy, q.cx[l], q.cy[l],
+                        S.half_patch, stride, w.ax, w.ay, w.bx, w.by, sf, cf);
+    }
+    __syncwarp();
+    for (unsigned m = need; m; m &= m - 1u) {
+      const int i = __ffs((int)m) - 1;
+      const unsigned bit = 1u << i;
+      float n = q.res[lane * n_src + i];
+      if (st == 0 && n < -0.5f) textureless |= bit;
+      if ((textureless & bit) && n > 0.0f) n = 0.0f;
+      if (n > out[i]) out[i] = n;
+      if (out[i] > 0.1f) need &= ~bit;
+    }
+    __syncwarp();
+  }
+  if (act)
+    for (int i = 0; i < n_src; ++i)
+      out[i] = (on >> i) & 1u ? finish_cost(S, i, q.prm[lane * n_src + i], out[i], rc, x, y)
+                              : 2.0f;
+}
+
+// acmmp_patchmatch (opencl_kernels.h:1298-1826) for one colour, one thread
+// per pixel.  The 14 cost vectors of a pixel (8 propagation candidates, the
+// current plane, 5 refinement hypotheses) are computed in that order by one
+// call site, cost_vector_warp, which the whole warp enters together.  Eight
+// blocks of two warps per SM (128 registers).
+__global__ void __launch_bounds__(64, 8) acm_pm_kernel(const AScene* __restrict__ Sp, AState st,
+                                                       int colour, int iteration) {
+  extern __shared__ float acm_smem[];
   const AScene& S = *Sp;
   const int W = S.W, H = S.H, npix = W * H;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + colour) & 1);
-  if (x >= W || y >= H) return;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x, lane = tid & 31;
+  const WarpQueue q = warp_queue(acm_smem + (tid >> 5) * acm_queue_words(S.n_src), S.n_src);
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + colour) & 1);
+  // A lane outside the image stays with its warp on pixel (0, 0), asks for
+  // no costs and writes nothing.
+  const bool valid = x < W && y < H;
+  if (!valid) x = y = 0;
   const int idx = y * W + x;
   const ACam& c0 = S.cam[0];
   uint2 s = st.rs[idx];
@@ -533,222 +692,247 @@ __global__ void __launch_bounds__(64) acm_pm_kernel(const AScene* __restrict__ S
     flags[i] = false;
   }
   for (int i = 0; i < 8 * kMaxSrc; ++i) ca[i] = 2.0f;
-  // Candidate positions in the reference's evaluation order: far up, down,
-  // left, right (slots 1, 3, 5, 7), then near up, down, left, right (0, 2,
-  // 4, 6).  Each slot takes the lowest-cost pixel of its pattern.
-  for (int slot_i = 0; slot_i < 8; ++slot_i) {
-    const int slot = slot_i < 4 ? 2 * slot_i + 1 : 2 * (slot_i - 4);
-    const int dir = slot >> 1;  // 0 up, 1 down, 2 left, 3 right
-    const bool vert = dir < 2;
-    const int sgn = (dir & 1) ? 1 : -1;
-    int base;
-    float bc;
-    int bp;
-    if (slot & 1) {  // far
-      const bool ok = dir == 0 ? y > 2 : (dir == 1 ? y < H - 3 : (dir == 2 ? x > 2 : x < W - 3));
-      if (!ok) continue;
-      base = vert ? (y + 3 * sgn) * W + x : y * W + (x + 3 * sgn);
-      bc = C[base];
-      bp = base;
-      for (int i = 1; i < 11; ++i) {
-        const int q = vert ? y + sgn * (3 + 2 * i) : x + sgn * (3 + 2 * i);
-        if (q < 0 || q >= (vert ? H : W)) break;
-        const int pp = vert ? q * W + x : y * W + q;
-        if (C[pp] < bc) {
-          bc = C[pp];
-          bp = pp;
-        }
-      }
-    } else {  // near, with a V of diagonals behind the neighbour
-      const bool ok = dir == 0 ? y > 0 : (dir == 1 ? y < H - 1 : (dir == 2 ? x > 0 : x < W - 1));
-      if (!ok) continue;
-      base = vert ? (y + sgn) * W + x : y * W + (x + sgn);
-      bc = C[base];
-      bp = base;
-      for (int i = 0; i < 3; ++i) {
-        for (int side = 0; side < 2; ++side) {
-          bool cond;
-          int pp;
-          if (vert) {
-            const bool along = dir == 0 ? y > 1 + i : y < H - 2 - i;
-            cond = along && (side == 0 ? x > i : x < W - 1 - i);
-            pp = (y + sgn * (2 + i)) * W + (side == 0 ? x - i - 1 : x + i + 1);
-          } else {
-            const bool along = dir == 2 ? x > 1 + i : x < W - 2 - i;
-            cond = along && (side == 0 ? y > i : y < H - 1 - i);
-            pp = (side == 0 ? y - i - 1 : y + i + 1) * W + (x + sgn * (2 + i));
-          }
-          if (cond && pp >= 0 && pp < npix && C[pp] < bc) {
-            bc = C[pp];
-            bp = pp;
-          }
-        }
-      }
-    }
-    pos[slot] = bp;
-    flags[slot] = true;
-    cost_vector(S, x, y, st.planes[bp], &ca[slot * kMaxSrc]);
-  }
-
-  // View selection priors from the four direct neighbours (last one wins).
-  float pri[kMaxSrc];
-  for (int i = 0; i < kMaxSrc; ++i) pri[i] = 0.0f;
-  const int npos[4] = {idx - W, idx + W, idx - 1, idx + 1};
-  for (int i = 0; i < 4; ++i) {
-    const int np = npos[i];
-    if (flags[2 * i] && np >= 0 && np < npix) {
-      const unsigned sv = st.sel[np];
-      for (int j = 0; j < n_src; ++j) pri[j] = (sv & (1u << j)) ? 0.9f : 0.1f;
-    }
-  }
-  const float thr = 0.8f * acm_exp((float)(iteration * iteration) / (-90.0f));
-  float prob[kMaxSrc];
-  for (int i = 0; i < kMaxSrc; ++i) prob[i] = 0.0f;
-  for (int i = 0; i < n_src; ++i) {
-    float count = 0.0f, tw = 0.0f;
-    int cfalse = 0;
-    for (int j = 0; j < 8; ++j) {
-      const float cv = ca[j * kMaxSrc + i];
-      if (flags[j] && cv < thr) {
-        tw += acm_exp(cv * cv / (-0.18f));
-        count += 1.0f;
-      }
-      if (flags[j] && cv > 1.2f) ++cfalse;
-    }
-    if (count > 2.0f && cfalse < 3)
-      prob[i] = tw / count;
-    else if (cfalse < 3)
-      prob[i] = acm_exp(thr * thr / (-0.32f));
-    prob[i] *= pri[i];
-  }
-  {
-    float sum = 0.0f;
-    for (int i = 0; i < n_src; ++i) sum += prob[i];
-    if (!(sum < 1e-12f)) {
-      const float inv = 1.0f / sum;
-      float cum = 0.0f;
-      for (int i = 0; i < n_src; ++i) {
-        cum += prob[i] * inv;
-        prob[i] = cum;
-      }
-    }
-  }
   float vw[kMaxSrc];
-  for (int i = 0; i < kMaxSrc; ++i) vw[i] = 0.0f;
-  for (int smp = 0; smp < 15; ++smp) {
-    const float r = acm_rand(s, key + (unsigned)smp * 997u) - 1e-7f;
-    for (int j = 0; j < n_src; ++j)
-      if (prob[j] > r) {
-        vw[j] += 1.0f;
-        break;
-      }
-  }
-  unsigned new_sel = 0;
   float norm = 0.0f;
-  for (int i = 0; i < n_src; ++i)
-    if (vw[i] > 0.0f) {
-      new_sel |= 1u << i;
-      norm += vw[i];
-    }
-
+  unsigned new_sel = 0;
   int best = 0;
   float bcost = 0.0f;
-  for (int i = 0; i < 8; ++i) {
-    float fc = 2.0f;
-    if (flags[i]) {
-      const float photo = weighted(S, &ca[i * kMaxSrc], vw, norm, st.planes[pos[i]], x, y);
-      fc = S.smooth_weight > 1e-6f
-               ? photo + S.smooth_weight * smoothness(S, st.planes, st.planes[pos[i]], x, y)
-               : photo;
+  float4 plane_now = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float cost_now = 0.0f, depth_now = 0.0f, depth_rand = 0.0f, depth_pert = 0.0f,
+        depth_cur = 0.0f;
+  float3 cur_n = make_float3(0.0f, 0.0f, -1.0f), nr = cur_n, np_ = cur_n;
+  float cvh[kMaxSrc];
+  for (int h = 0; h < 14; ++h) {
+    bool act = valid;
+    float4 pl = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float* outp = cvh;
+    if (h < 8) {
+      // Candidate positions in the reference's evaluation order: far up,
+      // down, left, right (slots 1, 3, 5, 7), then near up, down, left,
+      // right (0, 2, 4, 6).  Each slot takes the lowest-cost pixel of its
+      // pattern.
+      const int slot_i = h;
+      bool found = false;
+      do {
+        const int slot = slot_i < 4 ? 2 * slot_i + 1 : 2 * (slot_i - 4);
+        const int dir = slot >> 1;  // 0 up, 1 down, 2 left, 3 right
+        const bool vert = dir < 2;
+        const int sgn = (dir & 1) ? 1 : -1;
+        int base;
+        float bc;
+        int bp;
+        if (slot & 1) {  // far
+          const bool ok =
+              dir == 0 ? y > 2 : (dir == 1 ? y < H - 3 : (dir == 2 ? x > 2 : x < W - 3));
+          if (!ok) break;
+          base = vert ? (y + 3 * sgn) * W + x : y * W + (x + 3 * sgn);
+          bc = C[base];
+          bp = base;
+          for (int i = 1; i < 11; ++i) {
+            const int qc = vert ? y + sgn * (3 + 2 * i) : x + sgn * (3 + 2 * i);
+            if (qc < 0 || qc >= (vert ? H : W)) break;
+            const int pp = vert ? qc * W + x : y * W + qc;
+            if (C[pp] < bc) {
+              bc = C[pp];
+              bp = pp;
+            }
+          }
+        } else {  // near, with a V of diagonals behind the neighbour
+          const bool ok =
+              dir == 0 ? y > 0 : (dir == 1 ? y < H - 1 : (dir == 2 ? x > 0 : x < W - 1));
+          if (!ok) break;
+          base = vert ? (y + sgn) * W + x : y * W + (x + sgn);
+          bc = C[base];
+          bp = base;
+          for (int i = 0; i < 3; ++i) {
+            for (int side = 0; side < 2; ++side) {
+              bool cond;
+              int pp;
+              if (vert) {
+                const bool along = dir == 0 ? y > 1 + i : y < H - 2 - i;
+                cond = along && (side == 0 ? x > i : x < W - 1 - i);
+                pp = (y + sgn * (2 + i)) * W + (side == 0 ? x - i - 1 : x + i + 1);
+              } else {
+                const bool along = dir == 2 ? x > 1 + i : x < W - 2 - i;
+                cond = along && (side == 0 ? y > i : y < H - 1 - i);
+                pp = (side == 0 ? y - i - 1 : y + i + 1) * W + (x + sgn * (2 + i));
+              }
+              if (cond && pp >= 0 && pp < npix && C[pp] < bc) {
+                bc = C[pp];
+                bp = pp;
+              }
+            }
+          }
+        }
+        pos[slot] = bp;
+        flags[slot] = true;
+        pl = st.planes[bp];
+        outp = &ca[slot * kMaxSrc];
+        found = true;
+      } while (false);
+      act = act && found;
+    } else {
+      for (int i = 0; i < kMaxSrc; ++i) cvh[i] = 2.0f;
+      if (h == 8) {
+        pl = st.planes[idx];
+      } else {
+        const int r = h - 9;
+        const float dh = r == 0 || r == 2 ? depth_rand : (r == 4 ? depth_pert : depth_cur);
+        const float3 nh = r == 1 || r == 2 ? nr : (r == 3 ? np_ : cur_n);
+        pl = acm_plane(c0, (float)x, (float)y, dh, nh);
+      }
     }
-    if (i == 0 || fc < bcost) {
-      bcost = fc;
-      best = i;
+    cost_vector_warp(S, q, lane, act, x, y, pl, outp);
+    if (h == 7) {
+      // View selection priors from the four direct neighbours (last one wins).
+      float pri[kMaxSrc];
+      for (int i = 0; i < kMaxSrc; ++i) pri[i] = 0.0f;
+      const int npos[4] = {idx - W, idx + W, idx - 1, idx + 1};
+      for (int i = 0; i < 4; ++i) {
+        const int np = npos[i];
+        if (flags[2 * i] && np >= 0 && np < npix) {
+          const unsigned sv = st.sel[np];
+          for (int j = 0; j < n_src; ++j) pri[j] = (sv & (1u << j)) ? 0.9f : 0.1f;
+        }
+      }
+      const float thr = 0.8f * acm_exp((float)(iteration * iteration) / (-90.0f));
+      float prob[kMaxSrc];
+      for (int i = 0; i < kMaxSrc; ++i) prob[i] = 0.0f;
+      for (int i = 0; i < n_src; ++i) {
+        float count = 0.0f, tw = 0.0f;
+        int cfalse = 0;
+        for (int j = 0; j < 8; ++j) {
+          const float cv = ca[j * kMaxSrc + i];
+          if (flags[j] && cv < thr) {
+            tw += acm_exp(cv * cv / (-0.18f));
+            count += 1.0f;
+          }
+          if (flags[j] && cv > 1.2f) ++cfalse;
+        }
+        if (count > 2.0f && cfalse < 3)
+          prob[i] = tw / count;
+        else if (cfalse < 3)
+          prob[i] = acm_exp(thr * thr / (-0.32f));
+        prob[i] *= pri[i];
+      }
+      {
+        float sum = 0.0f;
+        for (int i = 0; i < n_src; ++i) sum += prob[i];
+        if (!(sum < 1e-12f)) {
+          const float inv = 1.0f / sum;
+          float cum = 0.0f;
+          for (int i = 0; i < n_src; ++i) {
+            cum += prob[i] * inv;
+            prob[i] = cum;
+          }
+        }
+      }
+      for (int i = 0; i < kMaxSrc; ++i) vw[i] = 0.0f;
+      for (int smp = 0; smp < 15; ++smp) {
+        const float r = acm_rand(s, key + (unsigned)smp * 997u) - 1e-7f;
+        for (int j = 0; j < n_src; ++j)
+          if (prob[j] > r) {
+            vw[j] += 1.0f;
+            break;
+          }
+      }
+      for (int i = 0; i < n_src; ++i)
+        if (vw[i] > 0.0f) {
+          new_sel |= 1u << i;
+          norm += vw[i];
+        }
+      for (int i = 0; i < 8; ++i) {
+        float fc = 2.0f;
+        if (flags[i]) {
+          const float photo =
+              weighted(S, &ca[i * kMaxSrc], vw, norm, st.planes[pos[i]], x, y);
+          fc = S.smooth_weight > 1e-6f
+                   ? photo + S.smooth_weight * smoothness(S, st.planes, st.planes[pos[i]], x, y)
+                   : photo;
+        }
+        if (i == 0 || fc < bcost) {
+          bcost = fc;
+          best = i;
+        }
+      }
+    } else if (h == 8) {
+      const float4 own = pl;
+      cost_now = weighted(S, cvh, vw, norm, own, x, y);
+      if (S.smooth_weight > 1e-6f)
+        cost_now += S.smooth_weight * smoothness(S, st.planes, own, x, y);
+      plane_now = own;
+      depth_now = acm_depth(c0, (float)x, (float)y, plane_now);
+      if (flags[best] && bcost < cost_now) {
+        const float4 bpl = st.planes[pos[best]];
+        const float db = acm_depth(c0, (float)x, (float)y, bpl);
+        if (db >= S.depth_min && db <= S.depth_max) {
+          depth_now = db;
+          plane_now = bpl;
+          cost_now = bcost;
+          if (valid) st.sel[idx] = new_sel;
+        }
+      }
+      // Refinement: (random depth, current normal), (current depth, random
+      // normal), (random, random), (current, perturbed normal), (perturbed
+      // depth, current normal).
+      const float pert = 0.02f;
+      const float PI_F = 3.14159274101257324f;
+      cur_n = acm_normalize(make_float3(plane_now.x, plane_now.y, plane_now.z));
+      // The SfM planar prior (where it covers the pixel) centres the random
+      // hypothesis on its plane: depth within 3 sigma, normal within 5
+      // degrees.
+      const bool have_prior = S.prior_mask != nullptr && S.prior_mask[idx] > 0u;
+      float depth_prior = 0.0f;
+      float3 prior_n = make_float3(0.0f, 0.0f, -1.0f);
+      if (have_prior) {
+        const float4 pp = S.prior_planes[idx];
+        depth_prior = acm_depth(c0, (float)x, (float)y, pp);
+        prior_n = acm_normalize(make_float3(pp.x, pp.y, pp.z));
+      }
+      if (have_prior && depth_prior > 0.0f) {
+        const float depth_sigma = (S.depth_max - S.depth_min) / 32.0f;
+        const float angle_sigma = PI_F * (5.0f / 180.0f);
+        depth_rand =
+            depth_prior - 3.0f * depth_sigma + acm_rand(s, key + 503u) * 6.0f * depth_sigma;
+        depth_rand = acm_clamp(depth_rand, S.depth_min, S.depth_max);
+        const float q1 = (acm_rand(s, key + 504u) - 0.5f) * angle_sigma;
+        const float q2 = (acm_rand(s, key + 505u) - 0.5f) * angle_sigma;
+        nr = acm_normalize(make_float3(prior_n.x + q1, prior_n.y + q2, prior_n.z));
+        if (nr.z > 0.0f) nr.z = -nr.z;
+      } else {
+        const float lmin = acm_log(S.depth_min > 1e-6f ? S.depth_min : 1e-6f);
+        const float lmax = acm_log(S.depth_max > 1e-5f ? S.depth_max : 1e-5f);
+        depth_rand = acm_exp(lmin + acm_rand(s, key + 503u) * (lmax - lmin));
+        nr.x = acm_rand(s, key + 504u) * 2.0f - 1.0f;
+        nr.y = acm_rand(s, key + 505u) * 2.0f - 1.0f;
+        nr.z = -1.0f;
+        nr = acm_normalize(nr);
+      }
+      const float dmn = (1.0f - pert) * depth_now, dmx = (1.0f + pert) * depth_now;
+      depth_pert =
+          acm_clamp(dmn + acm_rand(s, key + 510u) * (dmx - dmn), S.depth_min, S.depth_max);
+      const float pa1 = ((acm_rand(s, key + 520u) - 0.5f) * pert) * PI_F;
+      const float pa2 = ((acm_rand(s, key + 521u) - 0.5f) * pert) * PI_F;
+      np_ = acm_normalize(make_float3(cur_n.x + pa1, cur_n.y + pa2, cur_n.z));
+      if (np_.z > 0.0f) np_.z = -np_.z;
+      depth_cur = depth_now;  // the five hypotheses are fixed before any is taken
+    } else if (h > 8) {
+      const float4 cand = pl;
+      float tc = weighted(S, cvh, vw, norm, cand, x, y);
+      if (S.smooth_weight > 1e-6f) tc += S.smooth_weight * smoothness(S, st.planes, cand, x, y);
+      const float db = acm_depth(c0, (float)x, (float)y, cand);
+      if (!(db < S.depth_min || db > S.depth_max) && tc < cost_now) {
+        depth_now = db;
+        plane_now = cand;
+        cost_now = tc;
+      }
     }
   }
-  float cvn[kMaxSrc];
-  for (int i = 0; i < kMaxSrc; ++i) cvn[i] = 2.0f;
-  const float4 own = st.planes[idx];
-  cost_vector(S, x, y, own, cvn);
-  float cost_now = weighted(S, cvn, vw, norm, own, x, y);
-  if (S.smooth_weight > 1e-6f) cost_now += S.smooth_weight * smoothness(S, st.planes, own, x, y);
-  float4 plane_now = own;
-  float depth_now = acm_depth(c0, (float)x, (float)y, plane_now);
-  if (flags[best] && bcost < cost_now) {
-    const float4 bpl = st.planes[pos[best]];
-    const float db = acm_depth(c0, (float)x, (float)y, bpl);
-    if (db >= S.depth_min && db <= S.depth_max) {
-      depth_now = db;
-      plane_now = bpl;
-      cost_now = bcost;
-      st.sel[idx] = new_sel;
-    }
+  if (valid) {
+    st.planes[idx] = plane_now;
+    st.costs[idx] = cost_now;
+    st.rs[idx] = s;
   }
-
-  // Refinement: (random depth, current normal), (current depth, random
-  // normal), (random, random), (current, perturbed normal), (perturbed
-  // depth, current normal).
-  const float pert = 0.02f;
-  const float PI_F = 3.14159274101257324f;
-  const float3 cur_n = acm_normalize(make_float3(plane_now.x, plane_now.y, plane_now.z));
-  // The SfM planar prior (where it covers the pixel) centres the random
-  // hypothesis on its plane: depth within 3 sigma, normal within 5 degrees.
-  const bool have_prior = S.prior_mask != nullptr && S.prior_mask[idx] > 0u;
-  float depth_prior = 0.0f;
-  float3 prior_n = make_float3(0.0f, 0.0f, -1.0f);
-  if (have_prior) {
-    const float4 pp = S.prior_planes[idx];
-    depth_prior = acm_depth(c0, (float)x, (float)y, pp);
-    prior_n = acm_normalize(make_float3(pp.x, pp.y, pp.z));
-  }
-  float depth_rand;
-  float3 nr;
-  if (have_prior && depth_prior > 0.0f) {
-    const float depth_sigma = (S.depth_max - S.depth_min) / 32.0f;
-    const float angle_sigma = PI_F * (5.0f / 180.0f);
-    depth_rand = depth_prior - 3.0f * depth_sigma + acm_rand(s, key + 503u) * 6.0f * depth_sigma;
-    depth_rand = acm_clamp(depth_rand, S.depth_min, S.depth_max);
-    const float q1 = (acm_rand(s, key + 504u) - 0.5f) * angle_sigma;
-    const float q2 = (acm_rand(s, key + 505u) - 0.5f) * angle_sigma;
-    nr = acm_normalize(make_float3(prior_n.x + q1, prior_n.y + q2, prior_n.z));
-    if (nr.z > 0.0f) nr.z = -nr.z;
-  } else {
-    const float lmin = acm_log(S.depth_min > 1e-6f ? S.depth_min : 1e-6f);
-    const float lmax = acm_log(S.depth_max > 1e-5f ? S.depth_max : 1e-5f);
-    depth_rand = acm_exp(lmin + acm_rand(s, key + 503u) * (lmax - lmin));
-    nr.x = acm_rand(s, key + 504u) * 2.0f - 1.0f;
-    nr.y = acm_rand(s, key + 505u) * 2.0f - 1.0f;
-    nr.z = -1.0f;
-    nr = acm_normalize(nr);
-  }
-  const float dmn = (1.0f - pert) * depth_now, dmx = (1.0f + pert) * depth_now;
-  const float depth_pert =
-      acm_clamp(dmn + acm_rand(s, key + 510u) * (dmx - dmn), S.depth_min, S.depth_max);
-  const float pa1 = ((acm_rand(s, key + 520u) - 0.5f) * pert) * PI_F;
-  const float pa2 = ((acm_rand(s, key + 521u) - 0.5f) * pert) * PI_F;
-  float3 np_ = acm_normalize(make_float3(cur_n.x + pa1, cur_n.y + pa2, cur_n.z));
-  if (np_.z > 0.0f) np_.z = -np_.z;
-  const float depth_cur = depth_now;  // the five hypotheses are fixed before any is taken
-  for (int h = 0; h < 5; ++h) {
-    const float dh = h == 0 || h == 2 ? depth_rand : (h == 4 ? depth_pert : depth_cur);
-    const float3 nh = h == 1 || h == 2 ? nr : (h == 3 ? np_ : cur_n);
-    const float4 cand = acm_plane(c0, (float)x, (float)y, dh, nh);
-    float cv[kMaxSrc];
-    for (int i = 0; i < kMaxSrc; ++i) cv[i] = 2.0f;
-    cost_vector(S, x, y, cand, cv);
-    float tc = weighted(S, cv, vw, norm, cand, x, y);
-    if (S.smooth_weight > 1e-6f) tc += S.smooth_weight * smoothness(S, st.planes, cand, x, y);
-    const float db = acm_depth(c0, (float)x, (float)y, cand);
-    if (db < S.depth_min || db > S.depth_max) continue;
-    if (tc < cost_now) {
-      depth_now = db;
-      plane_now = cand;
-      cost_now = tc;
-    }
-  }
-  st.planes[idx] = plane_now;
-  st.costs[idx] = cost_now;
-  st.rs[idx] = s;
 }
 
 // acmmp_checkerboard_filter (opencl_kernels.h:1919-2099) for one colour.
@@ -1541,6 +1725,8 @@ static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, cons
   AState st{planes.p, costs.p, rs.p, sel.p};
   const dim3 blk(16, 8), grid((W + 15) / 16, (H + 7) / 8);
   const dim3 pblk(16, 4), pgrid(((W + 1) / 2 + 15) / 16, (H + 3) / 4);
+  // Two warps per block, each with its NCC queue (at most 35.6 KB).
+  const size_t pm_smem = 2 * sizeof(float) * (size_t)acm_queue_words(S.n_src);
   std::vector<float4> hsrc;
   if (coarse) {
     // UpsampleDepthNormal's host part (estimator.cc:600-640): coarse
@@ -1568,8 +1754,8 @@ static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, cons
   else
     acm_init_kernel<<<grid, blk, 0, s>>>(dS.p, st);
   for (int it = 0; it < e->max_iterations; ++it) {
-    acm_pm_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 0, it);
-    acm_pm_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 1, it);
+    acm_pm_kernel<<<pgrid, pblk, pm_smem, s>>>(dS.p, st, 0, it);
+    acm_pm_kernel<<<pgrid, pblk, pm_smem, s>>>(dS.p, st, 1, it);
     acm_filter_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 0);
     acm_filter_kernel<<<pgrid, pblk, 0, s>>>(dS.p, st, 1);
   }
