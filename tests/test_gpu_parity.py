@@ -639,6 +639,39 @@ def test_cluster_estimator_bit_identical_to_oracle(params):
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("n_src,size,params", [
+    (16, (45, 37), dict(patch_size=5, census_weight=0.8)),
+    (7, (33, 29), dict(patch_size=7, smooth_weight=0.3, top_k=3)),
+    (1, (31, 23), dict(patch_size=3)),
+])
+def test_cluster_estimator_sources_and_odd_sizes(n_src, size, params):
+    """The pass kernel's warp-wide NCC queue at its extremes: the maximum of
+    16 sources (the largest queue in shared memory), one source, and odd
+    sizes whose last warps hold lanes outside the image.  One reference,
+    one level, one iteration; identical to the C restatement."""
+    W, H = size
+    vs = S.ring_viewset(5, n_src + 1, W, H)
+    e = pydense.DepthmapClusterEstimator()
+    e.set_max_iterations(1)
+    e.set_patch_size(params["patch_size"])
+    for k in ("top_k", "census_weight", "smooth_weight"):
+        if k in params:
+            getattr(e, "set_" + k)(params[k])
+    srcs = list(vs.neighbors(0, n_src))
+    dmin, dmax = S.depth_range(vs.depths[0])
+    c = vs.cameras[0]
+    e.begin_ref_view(c.K, c.R, c.t, vs.images[0], dmin, dmax)
+    for s_ in srcs:
+        e.add_source_view(vs.cameras[s_].K, vs.cameras[s_].R, vs.cameras[s_].t, vs.images[s_])
+    views = [(vs.cameras[i].K, vs.cameras[i].R, vs.cameras[i].t, vs.images[i]) for i in [0] + srcs]
+    want = O.port_acmmp(views, dmin, dmax, iterations=1, **params)
+    got = e.run()[0]
+    assert (want[0] > 0).mean() > 0.1
+    for a, b in zip(got, want):
+        assert a.dtype == b.dtype and a.shape == b.shape
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("levels,geom,size", [(2, 0.2, (64, 48)), (3, 0.0, (64, 48)),
                                              (2, 1.0, (64, 48)), (3, 0.05, (66, 50))])
 def test_cluster_estimator_levels_bit_identical_to_oracle(levels, geom, size):
