@@ -16,7 +16,8 @@ LIB = os.path.join(HERE, "_build", "libdense_b200.so")
 SOURCES = ["kernels.cu", "cleanprune.cu", "learned.cu", "api.cu", "noalloc.cu", "lz4io.cu",
            "fuser.cu", "svo.cu", "acmmp.cu"]
 # Per-file flags: the live-path estimator fixes its arithmetic without FMA
-# contraction (every operation rounded by itself, as its C oracle).
+# contraction (every operation rounded by itself, as its C oracle, apart
+# from the fused multiply-adds its source writes out).
 FILE_FLAGS = {"acmmp.cu": ["--fmad=false"]}
 HEADERS = ["common.cuh", "kernels.h", "learned.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -18,7 +18,10 @@
 // contraction).  This file fixes one arithmetic, the one the C oracle
 // restates, and matches it bit for bit:
 //   - FP32, every operation rounded by itself in the written order: the
-//     file is compiled without FMA contraction (--fmad=false);
+//     file is compiled without FMA contraction (--fmad=false), and the
+//     only fused multiply-adds are the __fmaf_rn written out in the NCC
+//     tap, the bilinear blend and acm_exp (fmaf at the same places in the
+//     oracle);
 //   - acm_exp / acm_log below (Cody-Waite reduction, fixed polynomials);
 //   - images as float(v) * float(1/255); linear, clamp-to-edge reads as the
 //     OpenCL specification defines them, with exact fractions;
@@ -95,7 +98,9 @@ __device__ inline float acm_ldexp(float p, int n) {
   return (p * __int_as_float((n1 + 127) << 23)) * __int_as_float((n2 + 127) << 23);
 }
 
-// e^x: n = round(x log2 e), r = x - n ln2 in two parts, degree-7 Taylor.
+// e^x: n = round(x log2 e), r = x - n ln2 in two parts, degree-7 Taylor
+// in Horner form; the reduction and the Horner steps are fused
+// multiply-adds.
 __device__ inline float acm_exp(float x) {
   if (x != x) return x;
   if (x > 88.72283f) return INFINITY;
@@ -103,15 +108,15 @@ __device__ inline float acm_exp(float x) {
   const float t = x * 1.44269502f;
   const float nf = floorf(t + 0.5f);
   const int n = (int)nf;
-  const float r = (x - nf * 0.693145752f) - nf * 1.42860677e-06f;
+  const float r = __fmaf_rn(-nf, 1.42860677e-06f, __fmaf_rn(-nf, 0.693145752f, x));
   float p = 1.98412701e-04f;
-  p = p * r + 1.38888892e-03f;
-  p = p * r + 8.33333377e-03f;
-  p = p * r + 4.16666679e-02f;
-  p = p * r + 1.66666672e-01f;
-  p = p * r + 0.5f;
-  p = p * r + 1.0f;
-  p = p * r + 1.0f;
+  p = __fmaf_rn(p, r, 1.38888892e-03f);
+  p = __fmaf_rn(p, r, 8.33333377e-03f);
+  p = __fmaf_rn(p, r, 4.16666679e-02f);
+  p = __fmaf_rn(p, r, 1.66666672e-01f);
+  p = __fmaf_rn(p, r, 0.5f);
+  p = __fmaf_rn(p, r, 1.0f);
+  p = __fmaf_rn(p, r, 1.0f);
   return acm_ldexp(p, n);
 }
 
@@ -157,6 +162,13 @@ __device__ inline float acm_clamp(float x, float lo, float hi) {
 
 __device__ inline int clampi(int i, int n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
 
+// The bilinear blend ((w00 t00 + w10 t10) + w01 t01) + w11 t11 of the
+// texels at fractions (a, b), the last three terms as fused multiply-adds.
+__device__ inline float acm_lerp4(float a, float b, float t00, float t10, float t01, float t11) {
+  const float ia = 1.0f - a, ib = 1.0f - b;
+  return __fmaf_rn(a * b, t11, __fmaf_rn(ia * b, t01, __fmaf_rn(a * ib, t10, (ia * ib) * t00)));
+}
+
 // read_imagef(linear, clamp-to-edge) at unnormalised (u, v).
 __device__ inline float acm_sample(const AImg& im, float u, float v) {
   float xm = u - 0.5f, ym = v - 0.5f;
@@ -172,8 +184,7 @@ __device__ inline float acm_sample(const AImg& im, float u, float v) {
   const float* p = im.px;
   const float t00 = __ldg(p + (size_t)ya * im.W + xa), t10 = __ldg(p + (size_t)ya * im.W + xb);
   const float t01 = __ldg(p + (size_t)yb * im.W + xa), t11 = __ldg(p + (size_t)yb * im.W + xb);
-  return (((1.0f - a) * (1.0f - b)) * t00 + (a * (1.0f - b)) * t10) + ((1.0f - a) * b) * t01 +
-         (a * b) * t11;
+  return acm_lerp4(a, b, t00, t10, t01, t11);
 }
 
 // The same read at an integer texel (x + 0.5, y + 0.5): the fractions are
@@ -191,8 +202,7 @@ __device__ inline float acm_sample_inside(const AImg& im, float u, float v) {
   const float* p = im.px + (size_t)(int)fy * im.W + (int)fx;
   const float t00 = __ldg(p), t10 = __ldg(p + 1);
   const float t01 = __ldg(p + im.W), t11 = __ldg(p + im.W + 1);
-  return (((1.0f - a) * (1.0f - b)) * t00 + (a * (1.0f - b)) * t10) + ((1.0f - a) * b) * t01 +
-         (a * b) * t11;
+  return acm_lerp4(a, b, t00, t10, t01, t11);
 }
 
 __device__ inline float3 acm_project(const ACam& c, float3 X) {
@@ -253,19 +263,20 @@ __device__ float ncc_at_stride(const AImg& ref, const AImg& src, float rc, float
       const float fdx = stride * (float)ix, fdy = stride * (float)iy;
       // Reference taps sit on integer texels (integer strides).
       const float rv = acm_texel(ref, cx + istride * ix, cy + istride * iy);
-      const float sx = (scx + ax * fdx) + bx * fdy;
-      const float sy = (scy + ay * fdx) + by * fdy;
+      const float sx = __fmaf_rn(bx, fdy, __fmaf_rn(ax, fdx, scx));
+      const float sy = __fmaf_rn(by, fdy, __fmaf_rn(ay, fdx, scy));
       const float sv = inside ? acm_sample_inside(src, sx + 0.5f, sy + 0.5f)
                               : acm_sample(src, sx + 0.5f, sy + 0.5f);
-      const float dist2 = fdx * fdx + fdy * fdy;
+      const float dist2 = __fmaf_rn(fdy, fdy, fdx * fdx);
       const float r = rv - rc;
-      const float w = acm_exp(dist2 * sf + (r * r) * cf);
+      const float w = acm_exp(__fmaf_rn(r * r, cf, dist2 * sf));
       const float s = sv - sc;
-      sr += w * r;
-      ss += w * s;
-      srr += (w * r) * r;
-      sss += (w * s) * s;
-      srs += (w * r) * s;
+      const float wr = w * r, ws = w * s;
+      sr += wr;
+      ss += ws;
+      srr = __fmaf_rn(wr, r, srr);
+      sss = __fmaf_rn(ws, s, sss);
+      srs = __fmaf_rn(wr, s, srs);
       sw += w;
     }
   if (sw < 1e-6f) return -1.0f;

@@ -21,7 +21,9 @@
  * reference's outputs; this file fixes one arithmetic instead, which the
  * library's kernels match bit for bit:
  *   - FP32, every operation rounded by itself in the written order (no
- *     contraction), IEEE division and square root;
+ *     contraction), except the fmaf written out in the NCC tap, the
+ *     bilinear blend and acm_exp (rounded once, as the kernels' fused
+ *     multiply-adds); IEEE division and square root;
  *   - exp and log by the functions below (Cody-Waite reduction and fixed
  *     polynomials), not the C library's;
  *   - images as float(v) * float(1/255) (cv::Mat::convertTo with 1/255);
@@ -59,7 +61,8 @@ static float acm_ldexp(float p, int n) {
 }
 
 /* e^x: n = round(x log2 e), r = x - n ln2 (two-part ln2), e^r by its
- * degree-7 Taylor polynomial in Horner form (|r| <= 0.347). */
+ * degree-7 Taylor polynomial in Horner form (|r| <= 0.347); the reduction
+ * and the Horner steps are fused multiply-adds (fmaf, rounded once). */
 float acm_exp(float x) {
   if (x != x) return x;
   if (x > 88.72283f) return INFINITY;
@@ -67,15 +70,15 @@ float acm_exp(float x) {
   const float t = x * 1.44269502f;
   const float nf = floorf(t + 0.5f);
   const int n = (int)nf;
-  const float r = (x - nf * 0.693145752f) - nf * 1.42860677e-06f;
+  const float r = fmaf(-nf, 1.42860677e-06f, fmaf(-nf, 0.693145752f, x));
   float p = 1.98412701e-04f;
-  p = p * r + 1.38888892e-03f;
-  p = p * r + 8.33333377e-03f;
-  p = p * r + 4.16666679e-02f;
-  p = p * r + 1.66666672e-01f;
-  p = p * r + 0.5f;
-  p = p * r + 1.0f;
-  p = p * r + 1.0f;
+  p = fmaf(p, r, 1.38888892e-03f);
+  p = fmaf(p, r, 8.33333377e-03f);
+  p = fmaf(p, r, 4.16666679e-02f);
+  p = fmaf(p, r, 1.66666672e-01f);
+  p = fmaf(p, r, 0.5f);
+  p = fmaf(p, r, 1.0f);
+  p = fmaf(p, r, 1.0f);
   return acm_ldexp(p, n);
 }
 
@@ -149,8 +152,9 @@ static float acm_sample(const acm_img* im, float u, float v) {
   const int ya = acm_clampi(j0, im->H), yb = acm_clampi(j0 + 1, im->H);
   const float t00 = im->px[(size_t)ya * im->W + xa], t10 = im->px[(size_t)ya * im->W + xb];
   const float t01 = im->px[(size_t)yb * im->W + xa], t11 = im->px[(size_t)yb * im->W + xb];
-  return (((1.0f - a) * (1.0f - b)) * t00 + (a * (1.0f - b)) * t10) +
-         ((1.0f - a) * b) * t01 + (a * b) * t11;
+  /* ((w00 t00 + w10 t10) + w01 t01) + w11 t11, the last three fused. */
+  const float ia = 1.0f - a, ib = 1.0f - b;
+  return fmaf(a * b, t11, fmaf(ia * b, t01, fmaf(a * ib, t10, (ia * ib) * t00)));
 }
 
 /* --------------------------------------------------------------- cameras */
@@ -224,18 +228,19 @@ static float acm_ncc_at_stride(const acm_img* ref, const acm_img* src, float ref
       const float fdx = stride * (float)ix, fdy = stride * (float)iy;
       const float rx = (float)cx + fdx, ry = (float)cy + fdy;
       const float rv = acm_sample(ref, rx + 0.5f, ry + 0.5f);
-      const float sx = (scx + ax * fdx) + bx * fdy;
-      const float sy = (scy + ay * fdx) + by * fdy;
+      const float sx = fmaf(bx, fdy, fmaf(ax, fdx, scx));
+      const float sy = fmaf(by, fdy, fmaf(ay, fdx, scy));
       const float sv = acm_sample(src, sx + 0.5f, sy + 0.5f);
-      const float dist2 = fdx * fdx + fdy * fdy;
+      const float dist2 = fmaf(fdy, fdy, fdx * fdx);
       const float r = rv - ref_center;
-      const float w = acm_exp(dist2 * sf + (r * r) * cf);
+      const float w = acm_exp(fmaf(r * r, cf, dist2 * sf));
       const float s = sv - src_center;
-      sr += w * r;
-      ss += w * s;
-      srr += (w * r) * r;
-      sss += (w * s) * s;
-      srs += (w * r) * s;
+      const float wr = w * r, ws = w * s;
+      sr += wr;
+      ss += ws;
+      srr = fmaf(wr, r, srr);
+      sss = fmaf(ws, s, sss);
+      srs = fmaf(wr, s, srs);
       sw += w;
     }
   if (sw < 1e-6f) return -1.0f;
