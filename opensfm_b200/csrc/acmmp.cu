@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 #include <thread>
@@ -1383,66 +1384,123 @@ static std::vector<Tri> delaunay(const std::vector<double>& px, const std::vecto
   Y.push_back(big);
   X.push_back(-big);
   Y.push_back(-big);
+  // Counter-clockwise triangles; nb[k] is the triangle across the edge
+  // opposite v[k] (-1 on the outer triangle's edges).
   struct T {
-    int v[3];
+    int v[3], nb[3];
     double cx, cy, r2;
+    bool alive;
   };
+  std::vector<T> tris;
+  tris.reserve(8 * (size_t)n + 16);
   auto make = [&](int a, int b, int c) {
     T t;
     t.v[0] = a;
     t.v[1] = b;
     t.v[2] = c;
+    t.nb[0] = t.nb[1] = t.nb[2] = -1;
+    t.alive = true;
     const double ax = X[a], ay = Y[a], bx = X[b], by = Y[b], cx = X[c], cy = Y[c];
     const double d = 2.0 * (ax * (by - cy) + bx * (cy - ay) + cx * (ay - by));
     if (d == 0.0) {
       t.cx = t.cy = 0.0;
-      t.r2 = -1.0;  // degenerate: never contains a point, removed by the next insert near it
-      return t;
+      t.r2 = -1.0;  // degenerate: its circle contains no point
+    } else {
+      const double a2 = ax * ax + ay * ay, b2 = bx * bx + by * by, c2 = cx * cx + cy * cy;
+      t.cx = (a2 * (by - cy) + b2 * (cy - ay) + c2 * (ay - by)) / d;
+      t.cy = (a2 * (cx - bx) + b2 * (ax - cx) + c2 * (bx - ax)) / d;
+      t.r2 = (ax - t.cx) * (ax - t.cx) + (ay - t.cy) * (ay - t.cy);
     }
-    const double a2 = ax * ax + ay * ay, b2 = bx * bx + by * by, c2 = cx * cx + cy * cy;
-    t.cx = (a2 * (by - cy) + b2 * (cy - ay) + c2 * (ay - by)) / d;
-    t.cy = (a2 * (cx - bx) + b2 * (ax - cx) + c2 * (bx - ax)) / d;
-    t.r2 = (ax - t.cx) * (ax - t.cx) + (ay - t.cy) * (ay - t.cy);
-    return t;
+    tris.push_back(t);
+    return (int)tris.size() - 1;
   };
-  std::vector<T> tris;
-  tris.push_back(make(n, n + 1, n + 2));  // counter-clockwise
-  std::vector<int> seen;  // first index of each distinct position
+  // The strict circumcircle test of Bowyer-Watson.
+  auto bad = [&](const T& t, int i) {
+    const double dx = X[i] - t.cx, dy = Y[i] - t.cy;
+    return t.alive && t.r2 >= 0.0 && dx * dx + dy * dy < t.r2;
+  };
+  auto orient = [&](int a, int b, int i) {  // > 0: i left of a -> b
+    return (X[b] - X[a]) * (Y[i] - Y[a]) - (Y[b] - Y[a]) * (X[i] - X[a]);
+  };
+  make(n, n + 1, n + 2);
+  std::map<std::pair<double, double>, int> seen;  // distinct positions
+  std::vector<int> mark;  // mark[u] == i: triangle u is in point i's cavity
+  std::vector<int> cavity, stack, first_of(n + 3, -1), last_of(n + 3, -1), fresh;
+  int last = 0;
   for (int i = 0; i < n; ++i) {
-    bool dup = false;
-    for (int j : seen)
-      if (X[j] == X[i] && Y[j] == Y[i]) {
-        dup = true;
-        break;
-      }
-    if (dup) continue;
-    seen.push_back(i);
-    std::vector<std::pair<int, int>> edges;
-    std::vector<T> keep;
-    keep.reserve(tris.size() + 2);
-    for (const T& t : tris) {
-      const double dx = X[i] - t.cx, dy = Y[i] - t.cy;
-      if (t.r2 >= 0.0 && dx * dx + dy * dy < t.r2) {
-        for (int k = 0; k < 3; ++k) edges.emplace_back(t.v[k], t.v[(k + 1) % 3]);
-      } else {
-        keep.push_back(t);
-      }
-    }
-    // The boundary of the cavity: edges of exactly one removed triangle.
-    for (size_t a = 0; a < edges.size(); ++a) {
-      bool shared = false;
-      for (size_t b = 0; b < edges.size(); ++b)
-        if (a != b && ((edges[a].first == edges[b].second && edges[a].second == edges[b].first) ||
-                       (edges[a].first == edges[b].first && edges[a].second == edges[b].second))) {
-          shared = true;
+    if (!std::isfinite(X[i]) || !std::isfinite(Y[i])) continue;
+    if (!seen.emplace(std::make_pair(X[i], Y[i]), i).second) continue;  // a duplicate
+    // Locate: walk from the last new triangle towards the point.
+    int t = last, steps = 0;
+    const int max_steps = 4 * (int)tris.size() + 16;
+    while (t >= 0 && steps++ < max_steps) {
+      const T& c = tris[t];
+      int next = -2;
+      for (int k = 0; k < 3; ++k)
+        if (orient(c.v[(k + 1) % 3], c.v[(k + 2) % 3], i) < 0.0) {
+          next = c.nb[k];
           break;
         }
-      if (!shared) keep.push_back(make(edges[a].first, edges[a].second, i));
+      if (next == -2) break;  // inside (or on an edge of) t
+      t = next;
     }
-    tris.swap(keep);
+    // The cavity: the triangles whose circles contain the point, grown
+    // across neighbours from the located one; a full scan where the walk
+    // or the located triangle's test fails numerically.
+    mark.resize(tris.size(), -1);
+    cavity.clear();
+    if (t >= 0 && steps <= max_steps && bad(tris[t], i)) {
+      stack.assign(1, t);
+      mark[t] = i;
+      while (!stack.empty()) {
+        const int u = stack.back();
+        stack.pop_back();
+        cavity.push_back(u);
+        for (int k = 0; k < 3; ++k) {
+          const int v = tris[u].nb[k];
+          if (v >= 0 && mark[v] != i && bad(tris[v], i)) {
+            mark[v] = i;
+            stack.push_back(v);
+          }
+        }
+      }
+    } else {
+      for (int u = 0; u < (int)tris.size(); ++u)
+        if (bad(tris[u], i)) {
+          mark[u] = i;
+          cavity.push_back(u);
+        }
+    }
+    // A fan from the point over the cavity's boundary edges, linked to the
+    // triangles outside and to each other.
+    fresh.clear();
+    for (int u : cavity) {
+      for (int k = 0; k < 3; ++k) {
+        const int o = tris[u].nb[k];
+        if (o >= 0 && mark[o] == i) continue;
+        const int a = tris[u].v[(k + 1) % 3], b = tris[u].v[(k + 2) % 3];
+        const int nt = make(a, b, i);
+        mark.push_back(-1);
+        tris[nt].nb[2] = o;
+        if (o >= 0)
+          for (int m = 0; m < 3; ++m)
+            if (tris[o].v[(m + 1) % 3] == b && tris[o].v[(m + 2) % 3] == a) tris[o].nb[m] = nt;
+        first_of[a] = nt;
+        last_of[b] = nt;
+        fresh.push_back(nt);
+      }
+    }
+    for (int u : cavity) tris[u].alive = false;
+    for (int nt : fresh) {
+      T& c = tris[nt];  // (a, b, i): across (b, i) starts at b, across (i, a) ends at a
+      c.nb[0] = first_of[c.v[1]];
+      c.nb[1] = last_of[c.v[0]];
+    }
+    for (int nt : fresh) first_of[tris[nt].v[0]] = last_of[tris[nt].v[1]] = -1;
+    if (!fresh.empty()) last = fresh.back();
   }
   for (const T& t : tris) {
-    if (t.v[0] >= n || t.v[1] >= n || t.v[2] >= n) continue;
+    if (!t.alive || t.v[0] >= n || t.v[1] >= n || t.v[2] >= n) continue;
     int v[3] = {t.v[0], t.v[1], t.v[2]};
     std::sort(v, v + 3);
     out.push_back(Tri{v[0], v[1], v[2]});
@@ -1936,6 +1994,7 @@ extern "C" dn_status dn_acmmp_last_run_ms(dn_acmmp* e, float* ms) {
 extern "C" dn_status dn_delaunay_2d(const double* xy, int n, int w, int h, int* tris, int capacity,
                                      int* count) {
   ACHECK(count && (n == 0 || xy) && n >= 0 && w > 0 && h > 0, "bad argument");
+  for (int i = 0; i < 2 * n; ++i) ACHECK(std::isfinite(xy[i]), "non-finite coordinate");
   std::vector<double> px(n), py(n);
   for (int i = 0; i < n; ++i) {
     px[i] = xy[2 * i];

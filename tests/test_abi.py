@@ -95,3 +95,13 @@ def test_prior_delaunay_matches_oracle():
             # must then cover the same area with the same triangle count.
             assert xy is grid or len(xy) == 5, (W, H, len(xy))
             assert cnt.value == len(ref)
+
+
+def test_prior_delaunay_rejects_non_finite_points():
+    lib = _lib.load()
+    xy = np.array([[1.0, 2.0], [np.nan, 3.0], [4.0, 5.0], [6.0, 1.0]])
+    cnt = ctypes.c_int(0)
+    st = lib.dn_delaunay_2d(xy.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 4, 8, 8, None, 0,
+                            ctypes.byref(cnt))
+    assert st == _lib.DN_INVALID_ARG
+    assert b"non-finite" in lib.dn_acmmp_last_error()
