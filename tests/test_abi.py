@@ -105,3 +105,31 @@ def test_prior_delaunay_rejects_non_finite_points():
                             ctypes.byref(cnt))
     assert st == _lib.DN_INVALID_ARG
     assert b"non-finite" in lib.dn_acmmp_last_error()
+
+
+def test_prior_delaunay_duplicates_join_the_first():
+    """Exact duplicate positions are inserted once, under their first index;
+    the triangles equal Qhull's once every index is mapped to the first
+    point at its position."""
+    import oracle
+
+    lib = _lib.load()
+    rng = np.random.default_rng(3)
+    for _ in range(6):
+        base = rng.uniform(0, [320, 240], (60, 2))
+        xy = np.ascontiguousarray(base[rng.integers(0, 60, 150)])
+        cnt = ctypes.c_int(0)
+        p = xy.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        assert lib.dn_delaunay_2d(p, len(xy), 320, 240, None, 0, ctypes.byref(cnt)) == _lib.DN_OK
+        out = np.zeros((cnt.value, 3), np.int32)
+        assert lib.dn_delaunay_2d(p, len(xy), 320, 240, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                  cnt.value, ctypes.byref(cnt)) == _lib.DN_OK
+        _, first, inv = np.unique(xy, axis=0, return_index=True, return_inverse=True)
+        canon = first[inv.ravel()]
+        assert np.array_equal(canon[out], out)  # only first indices are used
+
+        def norm(t):
+            t = np.sort(canon[t], axis=1)
+            return t[np.lexsort((t[:, 2], t[:, 1], t[:, 0]))]
+
+        assert np.array_equal(norm(out), norm(oracle.acm_delaunay(xy, 320, 240)))
