@@ -324,34 +324,6 @@ __device__ float census(const AImg& ref, const AImg& src, float rc, float sc, in
   return (float)ham / 24.0f;
 }
 
-__device__ float single_cost(const AScene& S, int i, float3 cw, float3 wdx, float3 wdy, float rc,
-                             int cx, int cy, float sf, float cf) {
-  const ACam& c = S.cam[1 + i];
-  const AImg& ref = S.img[0];
-  const AImg& src = S.img[1 + i];
-  const float3 p = acm_project(c, cw);
-  if (p.z < 1e-6f) return 2.0f;
-  const float scx = p.x / p.z, scy = p.y / p.z;
-  const float3 pdx = acm_project(c, wdx), pdy = acm_project(c, wdy);
-  if (pdx.z < 1e-6f || pdy.z < 1e-6f) return 2.0f;
-  const float ax = pdx.x / pdx.z - scx, ay = pdx.y / pdx.z - scy;
-  const float bx = pdy.x / pdy.z - scx, by = pdy.y / pdy.z - scy;
-  const float sc = acm_sample(src, scx + 0.5f, scy + 0.5f);
-  const float ncc =
-      ncc_multiscale(ref, src, rc, sc, scx, scy, cx, cy, S.half_patch, ax, ay, bx, by, sf, cf);
-  if (ncc <= -0.5f) {
-    if (S.census_weight > 1e-6f) return census(ref, src, rc, sc, cx, cy, scx, scy, ax, ay, bx, by);
-    return 2.0f;
-  }
-  const float nc = 1.0f - ncc;
-  if (S.census_weight < 1e-6f) return nc;
-  const float t = acm_clamp((nc - 0.1f) / (0.6f - 0.1f), 0.0f, 1.0f);
-  const float blend = S.census_weight * ((t * t) * (3.0f - 2.0f * t));
-  if (blend < 1e-4f) return nc;
-  const float cen = census(ref, src, rc, sc, cx, cy, scx, scy, ax, ay, bx, by);
-  return (1.0f - blend) * nc + blend * cen;
-}
-
 // The warp of the reference patch into one source (compute_cost_vector's
 // per-view set-up, opencl_kernels.h:659-750): centre, the two affine steps
 // and the source value at the centre.
@@ -395,6 +367,16 @@ __device__ inline float finish_cost(const AScene& S, int i, const SrcWarp& w, fl
   if (blend < 1e-4f) return nc;
   const float cen = census(ref, src, rc, w.sc, cx, cy, w.scx, w.scy, w.ax, w.ay, w.bx, w.by);
   return (1.0f - blend) * nc + blend * cen;
+}
+
+// One source's cost: the warp set-up, the multi-scale NCC and the tail.
+__device__ float single_cost(const AScene& S, int i, float3 cw, float3 wdx, float3 wdy, float rc,
+                             int cx, int cy, float sf, float cf) {
+  SrcWarp w;
+  if (!warp_setup(S, i, cw, wdx, wdy, w)) return 2.0f;
+  const float ncc = ncc_multiscale(S.img[0], S.img[1 + i], rc, w.sc, w.scx, w.scy, cx, cy,
+                                   S.half_patch, w.ax, w.ay, w.bx, w.by, sf, cf);
+  return finish_cost(S, i, w, ncc, rc, cx, cy);
 }
 
 // compute_cost_vector (opencl_kernels.h:659-750): out[0 .. n_src).
