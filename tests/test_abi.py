@@ -133,3 +133,44 @@ def test_prior_delaunay_duplicates_join_the_first():
             return t[np.lexsort((t[:, 2], t[:, 1], t[:, 0]))]
 
         assert np.array_equal(norm(out), norm(oracle.acm_delaunay(xy, 320, 240)))
+
+
+def test_plain_c_caller_compiles_links_and_runs(tmp_path):
+    """A C99 program includes the header, links the library by name and
+    calls it: the version string, the device count, a host-only
+    triangulation and an estimator constructor, whose status is DN_OK with
+    a device and an error (not a crash) without one."""
+    import os
+    import shutil
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "caller.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include <string.h>
+#include "dense_b200.h"
+int main(void) {
+  if (!strstr(dn_version(), "sm_100a")) return 2;
+  const int devices = dn_device_count();
+  const double xy[8] = {0, 0, 10, 0, 0, 10, 10, 10};
+  int tris[6], count = 0;
+  if (dn_delaunay_2d(xy, 4, 16, 16, tris, 2, &count) != DN_OK || count != 2) return 3;
+  dn_acmmp* c = NULL;
+  const dn_status st = dn_acmmp_create(&c);
+  if (devices > 0 && st != DN_OK) return 4;
+  if (devices == 0 && st == DN_OK) return 5;
+  if (c) dn_acmmp_destroy(c);
+  printf("ok %d\n", devices);
+  return 0;
+}
+''')
+    exe = tmp_path / "caller"
+    lib_dir = os.path.dirname(_lib.LIB_PATH)
+    subprocess.check_call(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(root, "include"),
+                           str(src), "-o", str(exe), "-L", lib_dir, "-ldense_b200",
+                           "-Wl,-rpath," + lib_dir])
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
+    assert out.stdout.startswith("ok")
