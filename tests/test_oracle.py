@@ -444,3 +444,27 @@ def test_acmmp_pyramid_resizes_against_opencv():
     got = O.acm_resize_linear(d, 64, 48)
     want = cv2.resize(d, (64, 48), interpolation=cv2.INTER_LINEAR)
     assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
+
+
+def test_acmmp_oracle_matches_its_regression_fixture():
+    """The cluster estimator's C restatement reproduces, bit for bit, the
+    outputs stored by tests/golden/make_acmmp_regression.py: one level with
+    smoothness, and two levels with geometric links and the planar prior."""
+    import os
+
+    f = np.load(os.path.join(os.path.dirname(__file__), "golden", "acmmp_oracle_regression.npz"))
+    view = lambda i: (f["K"][i], f["R"][i], f["t"][i], f["images"][i])  # noqa: E731
+    rg = f["ranges"]
+    a = O.port_acmmp([view(i) for i in (0, 1, 2, 5)], rg[0, 0], rg[0, 1], iterations=2,
+                     patch_size=5, smooth_weight=0.2)
+    for name, arr in zip(("depth", "normal", "cost", "conf"), a):
+        assert np.array_equal(arr, f["a_" + name]), name
+    refs = [dict(views=[view(i) for i in (0, 1, 2, 5)], depth_min=rg[0, 0], depth_max=rg[0, 1],
+                 sfm=f["sfm0"]),
+            dict(views=[view(i) for i in (1, 0, 2, 3)], depth_min=rg[1, 0], depth_max=rg[1, 1],
+                 sfm=f["sfm1"])]
+    b = O.port_acmmp_cluster(refs, hierarchy_levels=2, iterations=2, patch_size=5,
+                             geom_weight=0.2, geom_links=[(0, 0, 1), (1, 0, 0)])
+    for r, res in enumerate(b):
+        for name, arr in zip(("depth", "normal", "cost", "conf"), res):
+            assert np.array_equal(arr, f[f"b{r}_" + name]), (r, name)
