@@ -468,3 +468,24 @@ def test_acmmp_oracle_matches_its_regression_fixture():
     for r, res in enumerate(b):
         for name, arr in zip(("depth", "normal", "cost", "conf"), res):
             assert np.array_equal(arr, f[f"b{r}_" + name]), (r, name)
+
+
+def test_fusion_oracles_match_their_regression_fixture():
+    """The restatements of the live cleaner, the per-pixel fuser (with and
+    without outlier removal) and the SVO fuser reproduce, bit for bit, the
+    outputs stored by tests/golden/make_fusion_regression.py."""
+    import importlib.util
+    import os
+
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    spec = importlib.util.spec_from_file_location(
+        "make_fusion_regression", os.path.join(here, "make_fusion_regression.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    f = dict(np.load(os.path.join(here, "fusion_oracle_regression.npz")))
+    got = gen.outputs(f)
+    assert set(got) <= set(f)
+    for name, arr in got.items():
+        assert np.array_equal(np.asarray(arr), f[name]), name
+    assert 0 < len(f["fuse_sor_points"]) < len(f["fuse_points"])
+    assert all(0 < (f[f"clean{r}"] > 0).sum() < (f["depth"][r] > 0).sum() for r in range(4))
