@@ -218,6 +218,12 @@ typedef struct {
   float depth_min, depth_max;
 } acm_params;
 
+/* The tap loop is compiled twice, with and without the FMA instruction set,
+ * and the loader picks the clone the host runs; fmaf rounds once either
+ * way, so both give the same bits (a library call without FMA). */
+#if defined(__GNUC__) && defined(__x86_64__) && !defined(__clang__)
+__attribute__((target_clones("fma", "default")))
+#endif
 static float acm_ncc_at_stride(const acm_img* ref, const acm_img* src, float ref_center,
                                float src_center, float scx, float scy, int cx, int cy, int hp,
                                float stride, float ax, float ay, float bx, float by, float sf,
