@@ -175,6 +175,11 @@ dn_status dn_batch_set_params(dn_batch* b, int patch_size, float min_patch_sd, i
 #define DN_RUN_GRAPH 4u  /* capture the run in a CUDA graph once, replay after */
 #define DN_RUN_INIT 8u   /* initialise from planes set by dn_batch_set_init */
 #define DN_RUN_TIMING 16u /* record CUDA events around each stage */
+/* Learned initialisation: the feature sweep, the proposal network set by
+ * dn_batch_set_proposal_net and the plane install run on the batch stream
+ * before PatchMatch (inside the graph with DN_RUN_GRAPH); every pixel with
+ * a proposal starts from it, the others from the random initialisation. */
+#define DN_RUN_LEARNED 32u
 /* Enqueues PatchMatch for every declared depthmap (and clean/prune per
  * flags) on the batch's stream; returns without waiting. */
 dn_status dn_batch_run(dn_batch* b, unsigned flags);
@@ -197,6 +202,19 @@ dn_status dn_batch_get_depths(dn_batch* b, int n, const int* map_ids, float* con
  * (depthmap.cc:305-374). */
 dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int use_far,
                                 int n_refine, float depth_range0, float normal_range0);
+/* Views scored per PatchMatch candidate in the half-passes (no reference
+ * counterpart as a switch): mode 0 scores every matching view and keeps the
+ * maximum (ComputePlaneScore, depthmap.cc:408-419); mode 1 scores one view
+ * per candidate -- the view the candidate's source pixel found best, the
+ * current view for refinements -- plus one random other view of the
+ * current plane per update, as ComputePatchMatchSample does
+ * (depthmap.cc:215-227, 305-374). */
+dn_status dn_batch_set_candidate_views(dn_batch* b, int mode);
+/* Active pixels (no reference counterpart): with on = 1, from the third
+ * half-pass of a run on, a pixel is updated only if its own plane or one of
+ * its 4 neighbours' planes changed at their last update; the others keep
+ * their state. */
+dn_status dn_batch_set_active_pixels(dn_batch* b, int on);
 /* Initial planes (f32 [H][W][3], reference camera) for one depthmap. */
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes);
 /* Total kept pruner points over all maps of the last run (after sync). */
@@ -216,8 +234,10 @@ dn_status dn_batch_last_taps(dn_batch* b, uint64_t* taps);
 dn_status dn_batch_set_view_image(dn_batch* b, int view_id, const uint8_t* image, int stride);
 /* Per-stage device times (ms) of the last run made with DN_RUN_TIMING:
  * out[0] init, out[1] all PatchMatch half-passes, out[2] post-process,
- * out[3] cleaner, out[4] whole run.  taps_out (may be NULL) receives the
- * NCC taps of init (taps_out[0]) and of the half-passes (taps_out[1]). */
+ * out[3] cleaner and pruner, out[4] whole run, out[5] the learned proposal
+ * (sweep, network and plane install; 0 without DN_RUN_LEARNED, and not part
+ * of out[0]).  taps_out (may be NULL) receives the NCC taps of init
+ * (taps_out[0]) and of the half-passes (taps_out[1]). */
 dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_out);
 /* Launch tuning (no reference counterpart): thread block shape bx x by
  * (bx * by <= 128, bx a multiple of 32); variant = the lanes that share one
@@ -256,14 +276,30 @@ dn_status dn_fp32_peak(double* tflops, double* ms);
  * buffers; `stream` is a cudaStream_t (NULL: default stream); every call
  * enqueues work and returns.
  * ---------------------------------------------------------------------- */
-/* Network input features of every depthmap of the batch: feat is a device
- * BF16 buffer [n_maps][H][W][32] with map stride `map_stride` elements
- * (>= H * W * 32 of the largest map).  Runs on the batch stream. */
-dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, int n_planes);
-/* Training targets from the last PatchMatch run: target is a device f32
- * buffer [n_maps][H][W][4] = (inverse-depth fraction, sx, sy, weight), with
- * weight 1 where the depth is valid and its score >= min_score. */
-dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float min_score);
+/* Network input features of every depthmap of the batch on the grid of
+ * every `stride`-th pixel (1 or 2; grid point (ys, xs) is pixel
+ * (stride ys, stride xs), grid size ceil(W / stride) x ceil(H / stride)):
+ * feat is a device BF16 buffer [n_maps][Hs][Ws][32] with map stride
+ * `map_stride` elements (>= Hs * Ws * 32 of the largest map).  Runs on the
+ * batch stream. */
+dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, int n_planes,
+                                  int stride);
+/* Training targets from the last PatchMatch run on the same grid: target is
+ * a device f32 buffer [n_maps][Hs][Ws][4] = (inverse-depth fraction, sx,
+ * sy, weight), with weight 1 where the depth is valid and its score >=
+ * min_score. */
+dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float min_score,
+                           int stride);
+/* The proposal network of DN_RUN_LEARNED runs, copied to the device:
+ * weights = BF16 bit patterns of the 6 layers' [cout][9 x 32] matrices one
+ * after the other (cout 32 for layers 0-4, 4 for layer 5: 46,080 values),
+ * biases = FP32 [32] x 5 then [4] (164 values).  Features are swept with
+ * n_planes planes (1..8) on the grid of every `stride`-th pixel (1 or 2),
+ * the network runs on that grid (maps of one grid size in one batch) and
+ * its output is interpolated back to every pixel.  weights = NULL removes
+ * the network. */
+dn_status dn_batch_set_proposal_net(dn_batch* b, const uint16_t* weights, const float* biases,
+                                    int n_planes, int stride);
 /* Initial planes of one depthmap from the network output (device f32
  * [H][W][4]); the next dn_batch_run with DN_RUN_INIT starts from them. */
 dn_status dn_batch_init_from_output(dn_batch* b, int map_id, const float* out);

@@ -18,6 +18,7 @@ HEADER = os.path.join(ROOT, "include", "dense_b200.h")
 (DN_OK, DN_INVALID_ARG, DN_OUT_OF_MEMORY, DN_DEVICE_ERROR, DN_TIMEOUT, DN_NOT_READY,
  DN_OUT_OF_RANGE) = range(7)
 DN_RUN_CLEAN, DN_RUN_PRUNE, DN_RUN_GRAPH, DN_RUN_INIT, DN_RUN_TIMING = 1, 2, 4, 8, 16
+DN_RUN_LEARNED = 32
 
 _lib = None
 
@@ -81,6 +82,9 @@ _SIGNATURES = {
     "dn_batch_get_depths": ([_vp, _i, _i32, _vp, _i], _i),
     "dn_batch_set_init": ([_vp, _i, _f], _i),
     "dn_batch_set_schedule": ([_vp, _i, _i, _i, _i, ctypes.c_float, ctypes.c_float], _i),
+    "dn_batch_set_candidate_views": ([_vp, _i], _i),
+    "dn_batch_set_active_pixels": ([_vp, _i], _i),
+    "dn_batch_set_proposal_net": ([_vp, ctypes.POINTER(ctypes.c_uint16), _f, _i, _i], _i),
     "dn_batch_pruned_count": ([_vp, ctypes.POINTER(ctypes.c_int64)], _i),
     "dn_batch_get_points": ([_vp, _i, _f, _f, _u8, _u8, ctypes.c_int64,
                              ctypes.POINTER(ctypes.c_int64)], _i),
@@ -94,8 +98,8 @@ _SIGNATURES = {
     "dn_batch_timer_elapsed": ([_vp, _f], _i),
     "dn_postprocess_depth": ([_f, _f, _i, _i], _i),
     "dn_fp32_peak": ([ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], _i),
-    "dn_batch_sweep_features": ([_vp, _vp, ctypes.c_int64, _i], _i),
-    "dn_batch_targets": ([_vp, _vp, ctypes.c_int64, ctypes.c_float], _i),
+    "dn_batch_sweep_features": ([_vp, _vp, ctypes.c_int64, _i, _i], _i),
+    "dn_batch_targets": ([_vp, _vp, ctypes.c_int64, ctypes.c_float, _i], _i),
     "dn_batch_init_from_output": ([_vp, _i, _vp], _i),
     "dn_nn_conv3x3_forward": ([_vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _i, _vp, _vp, _vp], _i),
     "dn_nn_conv3x3_forward_mma_sync": ([_vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _i, _vp,

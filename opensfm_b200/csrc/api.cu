@@ -173,6 +173,8 @@ struct Map {
   DevBuf<float> score, depth, clean, init, plane_out;
   DevBuf<int> nghbr;
   bool has_init = false;
+  DevBuf<float> prop_init;   // learned proposal planes [H][W][3]
+  DevBuf<uint8_t> changed;   // active-pixel flags [H][W]
   // Pruner (DN_RUN_PRUNE): views (this map first), scratch, outputs.
   DevBuf<dn::PruneView> prune_views;
   DevBuf<uint8_t> prune_scratch, prune_colors, prune_labels;
@@ -200,6 +202,24 @@ struct Engine {
   DevBuf<unsigned> d_sync;
   int use_near = 1, use_far = 1, n_refine = 6;
   float depth_range0 = 0.02f, normal_range0 = 0.5f;
+  int sample_hp = 0;  // half-passes score one view per candidate (sample mode)
+  int active = 0;     // active-pixel half-passes
+  // Learned proposal (DN_RUN_LEARNED): network weights, the feature grid of
+  // every map (maps of one grid size contiguous, one network launch per
+  // size), activations and outputs.
+  struct PropGroup {
+    int W, H, n;
+    long long off;  // first grid point
+  };
+  bool prop_on = false;
+  int prop_stride = 2, prop_planes = 8;
+  DevBuf<__nv_bfloat16> d_prop_w;
+  DevBuf<float> d_prop_b;
+  DevBuf<__nv_bfloat16> d_feat, d_act0, d_act1;
+  DevBuf<float> d_prop_out;
+  DevBuf<int4> d_tiles_prop, d_tiles_sweep;
+  int n_tiles_prop = 0, prop_max_pixels = 0;
+  std::vector<PropGroup> prop_groups;
   DevBuf<dn::ViewDev> d_views;
   DevBuf<dn::PairDev> d_pairs;
   DevBuf<dn::MapDev> d_maps;
@@ -214,7 +234,9 @@ struct Engine {
   cudaGraphExec_t graph = nullptr;
   unsigned graph_flags = 0;
   Mode graph_mode = Mode::kPatchMatch;
-  static constexpr int kEvents = 7;  // run start, init, half-passes, post, clean, timer x2
+  // run start, init, half-passes, post, clean, timer x2, proposal
+  static constexpr int kEvents = 8;
+  bool timed_learned = false;
   cudaEvent_t ev[kEvents] = {};
   bool timed = false;
 
@@ -348,8 +370,32 @@ struct Engine {
     }
     std::vector<dn::PairDev> hp;
     std::vector<dn::MapDev> hm(maps.size());
-    std::vector<int4> t1, t2, ti;
+    std::vector<int4> t1, t2, ti, tp;
     const int lanes = (patch == 7) ? variant : 1;
+    // Proposal grid: maps grouped by grid size in order of first appearance,
+    // each group's maps contiguous.
+    std::vector<long long> prop_off(maps.size(), 0);
+    prop_groups.clear();
+    prop_max_pixels = 0;
+    long long prop_points = 0;
+    if (prop_on) {
+      const int S = prop_stride;
+      std::vector<int> done(maps.size(), 0);
+      for (size_t a = 0; a < maps.size(); ++a) {
+        if (done[a]) continue;
+        const View& ra = *views[maps[a]->ref];
+        PropGroup g{(ra.W + S - 1) / S, (ra.H + S - 1) / S, 0, prop_points};
+        for (size_t b2 = a; b2 < maps.size(); ++b2) {
+          const View& rb = *views[maps[b2]->ref];
+          if (done[b2] || (rb.W + S - 1) / S != g.W || (rb.H + S - 1) / S != g.H) continue;
+          done[b2] = 1;
+          prop_off[b2] = prop_points;
+          prop_points += (long long)g.W * g.H;
+          ++g.n;
+        }
+        prop_groups.push_back(g);
+      }
+    }
     for (size_t mi = 0; mi < maps.size(); ++mi) {
       Map& m = *maps[mi];
       const View& r = *views[m.ref];
@@ -384,6 +430,23 @@ struct Engine {
       d.depth = m.depth.p;
       d.clean = m.clean.p;
       d.init = m.has_init ? m.init.p : nullptr;
+      if (active) {
+        DN_CUDA(m.changed.alloc(npx));
+        d.changed = m.changed.p;
+      }
+      if (prop_on) {
+        DN_CUDA(m.prop_init.alloc(3 * npx));
+        d.prop_init = m.prop_init.p;
+        d.prop_off = prop_off[mi];
+        d.prop_W = (r.W + prop_stride - 1) / prop_stride;
+        d.prop_H = (r.H + prop_stride - 1) / prop_stride;
+        prop_max_pixels = std::max(prop_max_pixels, r.W * r.H);
+        // Sweep tiles: (bx / lanes) x by grid points per block.
+        const int pxs = bx / lanes;
+        for (int y = 0; y < (d.prop_H + by - 1) / by; ++y)
+          for (int x = 0; x < (d.prop_W + pxs - 1) / pxs; ++x)
+            tp.push_back(make_int4((int)mi, x, y, 0));
+      }
       for (int o : m.nbrs) {
         const View& ov = *views[o];
         // Q = R_o R_0^T, a = Q t_0 - t_o (depthmap.cc:152-155);
@@ -432,6 +495,20 @@ struct Engine {
                             cudaMemcpyHostToDevice, stream));
     DN_CUDA(cudaMemcpyAsync(d_tiles_init.p, ti.data(), ti.size() * sizeof(int4),
                             cudaMemcpyHostToDevice, stream));
+    n_tiles_prop = 0;
+    if (prop_on) {
+      DN_CUDA(d_tiles_prop.alloc(std::max<size_t>(tp.size(), 1)));
+      DN_CUDA(cudaMemcpyAsync(d_tiles_prop.p, tp.data(), tp.size() * sizeof(int4),
+                              cudaMemcpyHostToDevice, stream));
+      n_tiles_prop = (int)tp.size();
+      const size_t n = (size_t)std::max<long long>(prop_points, 1);
+      DN_CUDA(d_feat.alloc(n * dn::kFeatC));
+      DN_CUDA(d_act0.alloc(n * dn::kFeatC));
+      DN_CUDA(d_act1.alloc(n * dn::kFeatC));
+      DN_CUDA(d_prop_out.alloc(n * 4));
+      // Grid points that no sweep thread reaches keep zero features.
+      DN_CUDA(cudaMemsetAsync(d_feat.p, 0, n * dn::kFeatC * sizeof(__nv_bfloat16), stream));
+    }
     DN_CUDA(cudaStreamSynchronize(stream));
     n_tiles1 = (int)t1.size();
     n_tiles2 = (int)t2.size();
@@ -467,11 +544,50 @@ struct Engine {
     a.p.n_refine = n_refine;
     a.p.depth_range0 = depth_range0;
     a.p.normal_range0 = normal_range0;
+    a.p.active = active;
     return a;
   }
 
+  // The learned proposal of every map: feature sweep on the proposal grid,
+  // the 6-layer network per grid size (tcgen05 forward), planes installed
+  // into MapDev::prop_init at full resolution.
+  static constexpr int kPropLayers = 6;
+  dn_status enqueue_proposal() {
+    DN_CHECK(prop_on && d_prop_w.p, "DN_RUN_LEARNED needs dn_batch_set_proposal_net");
+    DN_CHECK(patch == 7, "the learned initialisation uses the 7 x 7 patch");
+    dn::LaunchArgs a = args(false);
+    a.tiles = d_tiles_prop.p;
+    a.n_tiles = n_tiles_prop;
+    DN_CUDA(dn::launch_sweep(a, d_feat.p, -1, prop_planes, prop_stride, stream));
+    for (const PropGroup& g : prop_groups) {
+      const long long n_pix = (long long)g.n * g.W * g.H;
+      const __nv_bfloat16* x = d_feat.p + g.off * dn::kFeatC;
+      for (int k = 0; k < kPropLayers; ++k) {
+        const bool last = k == kPropLayers - 1;
+        __nv_bfloat16* y = (k & 1) ? d_act1.p : d_act0.p;
+        dn::ConvArgs c{};
+        c.x = x;
+        c.w = d_prop_w.p + (size_t)k * 32 * 9 * 32;
+        c.bias = d_prop_b.p + 32 * k;
+        c.n_pix = n_pix;
+        c.H = g.H;
+        c.W = g.W;
+        c.cin = 32;
+        c.cout = last ? 4 : 32;
+        c.relu = last ? 0 : 1;
+        c.y = last ? nullptr : y + g.off * dn::kFeatC;
+        c.y32 = last ? d_prop_out.p + 4 * g.off : nullptr;
+        DN_CUDA(dn::conv3x3_forward(c, stream));
+        x = c.y;
+      }
+    }
+    DN_CUDA(dn::launch_proposal_to_planes(d_prop_out.p, d_maps.p, (int)maps.size(),
+                                          prop_max_pixels, prop_stride, stream));
+    return DN_OK;
+  }
+
   // Enqueues the whole computation for every map on `stream`.
-  dn_status enqueue(Mode mode, bool timing = false) {
+  dn_status enqueue(Mode mode, bool timing = false, bool learned = false) {
     for (auto& m : maps) {
       const View& r = *views[m->ref];
       const size_t npx = (size_t)r.W * r.H;
@@ -479,12 +595,19 @@ struct Engine {
         DN_CUDA(cudaMemsetAsync(m->state.p, 0, npx * sizeof(float4), stream));
         DN_CUDA(cudaMemsetAsync(m->score.p, 0, npx * sizeof(float), stream));
         DN_CUDA(cudaMemsetAsync(m->nghbr.p, 0, npx * sizeof(int), stream));
+        if (active) DN_CUDA(cudaMemsetAsync(m->changed.p, 0, npx, stream));
       }
     }
     DN_CUDA(cudaMemsetAsync(d_taps.p, 0, 4 * sizeof(unsigned long long), stream));
     DN_CUDA(cudaMemsetAsync(d_error.p, 0, sizeof(int), stream));
     DN_TRY(mark(0, timing));
+    timed_learned = learned && timing;
+    if (learned) {
+      DN_TRY(enqueue_proposal());
+      DN_TRY(mark(7, timing));
+    }
     dn::LaunchArgs a1 = args(false);
+    a1.p.learned = learned ? 1 : 0;
     if (mode == Mode::kScorePlanes) {
       DN_CUDA(dn::launch_stage(dn::Stage::kScorePlanes, false, a1, stream));
       return DN_OK;
@@ -496,8 +619,11 @@ struct Engine {
       return DN_OK;
     }
     const bool sample = (mode == Mode::kPatchMatchSample);
+    // Half-passes in sample mode: the mode itself, or one view per candidate
+    // after a full initialisation (dn_batch_set_candidate_views).
+    const bool sample_half = sample || sample_hp;
     const int hp = half_passes >= 0 ? half_passes : 2 * iterations;
-    if (persistent && !sample && patch == 7) {
+    if (persistent && !sample_half && patch == 7) {
       DN_CHECK(d_sync.p && d_sync.n >= (size_t)(4 + hp), "persistent launch buffers not prepared");
       DN_CUDA(cudaMemsetAsync(d_sync.p, 0, (4 + hp) * sizeof(unsigned), stream));
       dn::PersistentArgs pa{};
@@ -528,7 +654,7 @@ struct Engine {
     for (int k = 0; k < hp; ++k) {
       a2.p.colour = k & 1;
       a2.p.pass = k;
-      DN_CUDA(dn::launch_stage(dn::Stage::kHalfPass, sample, a2, stream));
+      DN_CUDA(dn::launch_stage(dn::Stage::kHalfPass, sample_half, a2, stream));
     }
     DN_TRY(mark(2, timing));
     a1.flag = 1;
@@ -657,13 +783,15 @@ struct Engine {
     DN_CHECK(timed, "the last run was not made with DN_RUN_TIMING");
     DN_CUDA(cudaSetDevice(device));
     DN_CUDA(cudaStreamSynchronize(stream));
-    float t[5] = {0, 0, 0, 0, 0};
-    DN_CUDA(cudaEventElapsedTime(&t[0], ev[0], ev[1]));
+    float t[6] = {0, 0, 0, 0, 0, 0};
+    // With the learned proposal, init starts at its end event (7).
+    DN_CUDA(cudaEventElapsedTime(&t[0], ev[timed_learned ? 7 : 0], ev[1]));
     DN_CUDA(cudaEventElapsedTime(&t[1], ev[1], ev[2]));
     DN_CUDA(cudaEventElapsedTime(&t[2], ev[2], ev[3]));
     DN_CUDA(cudaEventElapsedTime(&t[3], ev[3], ev[4]));
     DN_CUDA(cudaEventElapsedTime(&t[4], ev[0], ev[4]));
-    for (int k = 0; k < n && k < 5; ++k) out[k] = t[k];
+    if (timed_learned) DN_CUDA(cudaEventElapsedTime(&t[5], ev[0], ev[7]));
+    for (int k = 0; k < n && k < 6; ++k) out[k] = t[k];
     if (taps_out) {
       unsigned long long v[4];
       DN_CUDA(cudaMemcpy(v, d_taps.p, sizeof(v), cudaMemcpyDeviceToHost));
@@ -678,6 +806,8 @@ struct Engine {
     int err = 0;
     DN_CUDA(cudaMemcpy(&err, d_error.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return fail(DN_TIMEOUT, "a bounded device-side wait expired");
+    if (prop_on && dn::take_tc_error() != 0)
+      return fail(DN_TIMEOUT, "a bounded wait of the proposal network expired");
     computed = true;
     return DN_OK;
   }
@@ -1360,6 +1490,59 @@ dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int 
   e.invalidate();
   return DN_OK;
 }
+dn_status dn_batch_set_candidate_views(dn_batch* b, int mode) {
+  DN_CHECK(b, "NULL batch");
+  DN_CHECK(mode == 0 || mode == 1, "candidate view mode must be 0 (all views) or 1 (sample)");
+  b->eng.sample_hp = mode;
+  b->eng.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_active_pixels(dn_batch* b, int on) {
+  DN_CHECK(b, "NULL batch");
+  b->eng.active = on ? 1 : 0;
+  b->eng.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_proposal_net(dn_batch* b, const uint16_t* weights, const float* biases,
+                                    int n_planes, int stride) {
+  DN_CHECK(b, "NULL batch");
+  Engine& e = b->eng;
+  DN_CUDA(cudaSetDevice(e.device));
+  if (!weights) {
+    e.prop_on = false;
+    e.d_prop_w.release();
+    e.d_prop_b.release();
+    e.invalidate();
+    return DN_OK;
+  }
+  DN_CHECK(biases, "biases must not be NULL");
+  DN_CHECK(n_planes >= 1 && n_planes <= 8, "n_planes must be 1..8");
+  DN_CHECK(stride == 1 || stride == 2, "stride must be 1 or 2");
+  // Layers 0-4: [32][288]; layer 5: [4][288] stored in a [32][288] slot
+  // whose rows 4..31 stay zero (the kernel reads only cout rows).
+  constexpr int kL = Engine::kPropLayers, kRow = 9 * 32;
+  std::vector<uint16_t> w((size_t)kL * 32 * kRow, 0);
+  std::vector<float> bias((size_t)kL * 32, 0.f);
+  size_t off = 0;
+  for (int k = 0; k < kL; ++k) {
+    const int cout = k == kL - 1 ? 4 : 32;
+    std::memcpy(w.data() + (size_t)k * 32 * kRow, weights + off, (size_t)cout * kRow * 2);
+    std::memcpy(bias.data() + 32 * k, biases + 32 * k, (size_t)cout * sizeof(float));
+    off += (size_t)cout * kRow;
+  }
+  for (float v : bias) DN_CHECK(std::isfinite(v), "biases must be finite");
+  DN_CUDA(e.d_prop_w.alloc(w.size()));
+  DN_CUDA(e.d_prop_b.alloc(bias.size()));
+  DN_CUDA(cudaMemcpyAsync(e.d_prop_w.p, w.data(), w.size() * 2, cudaMemcpyHostToDevice, e.stream));
+  DN_CUDA(cudaMemcpyAsync(e.d_prop_b.p, bias.data(), bias.size() * sizeof(float),
+                          cudaMemcpyHostToDevice, e.stream));
+  DN_CUDA(cudaStreamSynchronize(e.stream));
+  e.prop_on = true;
+  e.prop_planes = n_planes;
+  e.prop_stride = stride;
+  e.invalidate();
+  return DN_OK;
+}
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes) {
   DN_CHECK(b, "NULL batch");
   return b->eng.set_init(map_id, planes);
@@ -1374,6 +1557,9 @@ dn_status dn_batch_run(dn_batch* b, unsigned flags) {
            "DN_RUN_PRUNE prunes the cleaned depthmaps: add DN_RUN_CLEAN");
   const bool use_graph = (flags & DN_RUN_GRAPH) != 0;
   const bool timing = (flags & DN_RUN_TIMING) != 0;
+  const bool learned = (flags & DN_RUN_LEARNED) != 0;
+  DN_CHECK(!learned || (e.prop_on && e.d_prop_w.p),
+           "DN_RUN_LEARNED needs a network (dn_batch_set_proposal_net)");
   e.timed = timing;
   if (!(flags & DN_RUN_CLEAN) && timing) {
     // No cleaner stage: its event marks the end of the run.
@@ -1394,7 +1580,7 @@ dn_status dn_batch_run(dn_batch* b, unsigned flags) {
     if (flags & DN_RUN_PRUNE) DN_TRY(e.prepare_prune());
     cudaGraph_t g = nullptr;
     DN_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
-    dn_status s = e.enqueue(Mode::kPatchMatch, timing);
+    dn_status s = e.enqueue(Mode::kPatchMatch, timing, learned);
     if (s == DN_OK && (flags & DN_RUN_CLEAN)) s = e.enqueue_clean(timing);
     if (s == DN_OK && (flags & DN_RUN_PRUNE)) s = e.enqueue_prune();
     cudaError_t ce = cudaStreamEndCapture(e.stream, &g);
@@ -1411,7 +1597,7 @@ dn_status dn_batch_run(dn_batch* b, unsigned flags) {
   } else {
     if (flags & DN_RUN_CLEAN) DN_TRY(e.prepare_clean());
     if (flags & DN_RUN_PRUNE) DN_TRY(e.prepare_prune());
-    DN_TRY(e.enqueue(Mode::kPatchMatch, timing));
+    DN_TRY(e.enqueue(Mode::kPatchMatch, timing, learned));
     if (flags & DN_RUN_CLEAN) DN_TRY(e.enqueue_clean(timing));
     if (flags & DN_RUN_PRUNE) DN_TRY(e.enqueue_prune());
   }
@@ -1533,35 +1719,55 @@ dn_status dn_batch_copy_depth_device(dn_batch* b, int map_id, float* d_out) {
   return DN_OK;
 }
 
-dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, int n_planes) {
+dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, int n_planes,
+                                  int stride) {
   DN_CHECK(b && feat, "NULL argument");
   DN_CHECK(n_planes >= 1 && n_planes <= 8, "n_planes must be 1..8");
+  DN_CHECK(stride == 1 || stride == 2, "stride must be 1 or 2");
   Engine& e = b->eng;
   DN_CUDA(cudaSetDevice(e.device));
   DN_CHECK(e.patch == 7, "the learned initialisation uses the 7 x 7 patch");
   for (auto& m : e.maps) {
     const View& r = *e.views[m->ref];
-    DN_CHECK((int64_t)r.W * r.H * dn::kFeatC <= map_stride, "map_stride too small");
+    const int64_t grid = (int64_t)((r.W + stride - 1) / stride) * ((r.H + stride - 1) / stride);
+    DN_CHECK(grid * dn::kFeatC <= map_stride, "map_stride too small");
   }
   DN_TRY(e.check_params(Mode::kPatchMatch));
   DN_TRY(e.prepare());
+  // Tiles of (bx / lanes) x by grid points, uploaded before the launch.
+  const int lanes = e.variant, pxs = e.bx / lanes;
+  std::vector<int4> tl;
+  for (size_t k = 0; k < e.maps.size(); ++k) {
+    const View& r = *e.views[e.maps[k]->ref];
+    const int Ws = (r.W + stride - 1) / stride, Hs = (r.H + stride - 1) / stride;
+    for (int y = 0; y < (Hs + e.by - 1) / e.by; ++y)
+      for (int x = 0; x < (Ws + pxs - 1) / pxs; ++x) tl.push_back(make_int4((int)k, x, y, 0));
+  }
+  DN_CUDA(e.d_tiles_sweep.alloc(std::max<size_t>(tl.size(), 1)));
+  DN_CUDA(cudaMemcpyAsync(e.d_tiles_sweep.p, tl.data(), tl.size() * sizeof(int4),
+                          cudaMemcpyHostToDevice, e.stream));
+  DN_CUDA(cudaStreamSynchronize(e.stream));
   dn::LaunchArgs a = e.args(false);
-  a.tiles = e.d_tiles_init.p;  // the initialisation tiling of the current lanes
-  a.n_tiles = e.n_tiles_init;
-  DN_CUDA(dn::launch_sweep(a, static_cast<__nv_bfloat16*>(feat), map_stride, n_planes, e.stream));
+  a.tiles = e.d_tiles_sweep.p;
+  a.n_tiles = (int)tl.size();
+  DN_CUDA(dn::launch_sweep(a, static_cast<__nv_bfloat16*>(feat), map_stride, n_planes, stride,
+                           e.stream));
   return DN_OK;
 }
-dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float min_score) {
+dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float min_score,
+                           int stride) {
   DN_CHECK(b && target, "NULL argument");
+  DN_CHECK(stride == 1 || stride == 2, "stride must be 1 or 2");
   Engine& e = b->eng;
   DN_CHECK(e.computed, "no PatchMatch result computed yet");
   DN_CUDA(cudaSetDevice(e.device));
   for (size_t k = 0; k < e.maps.size(); ++k) {
     const Map& m = *e.maps[k];
     const View& r = *e.views[m.ref];
-    DN_CHECK((int64_t)r.W * r.H * 4 <= map_stride, "map_stride too small");
-    DN_CUDA(dn::launch_planes_to_target(m.state.p, m.score.p, r.W, r.H, e.d_maps.p, (int)k,
-                                        min_score, target + k * map_stride, e.stream));
+    const int64_t grid = (int64_t)((r.W + stride - 1) / stride) * ((r.H + stride - 1) / stride);
+    DN_CHECK(grid * 4 <= map_stride, "map_stride too small");
+    DN_CUDA(dn::launch_planes_to_target(m.state.p, m.score.p, r.W, r.H, stride, e.d_maps.p,
+                                        (int)k, min_score, target + k * map_stride, e.stream));
   }
   return DN_OK;
 }

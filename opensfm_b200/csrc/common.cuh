@@ -63,6 +63,10 @@ struct MapDev {
   float* clean;                            // [H][W] cleaned depth
   const float* init;                       // [H][W][3] optional initial planes
   uint8_t* keep;                           // [H][W] pruner flags (scratch)
+  uint8_t* changed;                        // [H][W] plane changed at the last update
+  float* prop_init;                        // [H][W][3] learned proposal planes
+  long long prop_off;                      // first point of the map in the proposal grid
+  int prop_W, prop_H;                      // proposal grid (W, H divided by the stride)
 };
 
 struct RunParams {
@@ -82,6 +86,11 @@ struct RunParams {
   // first refinement's depth / normal-slope ranges.
   int use_near, use_far, n_refine;
   float depth_range0, normal_range0;
+  // Active pixels: from half-pass 2 on, a pixel is updated only if its own
+  // plane or one of its 4 neighbours' planes changed at their last update
+  // (MapDev::changed); otherwise its state is kept as it is.
+  int active;
+  int learned;  // initialise from MapDev::prop_init instead of MapDev::init
 };
 
 // ------------------------------------------------------------------ RNG

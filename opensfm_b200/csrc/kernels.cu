@@ -141,8 +141,9 @@ __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev*
       float3 v;
       float depth;
       bool given = false;
-      if (m.init) {
-        v = make_float3(m.init[3 * pix], m.init[3 * pix + 1], m.init[3 * pix + 2]);
+      const float* ip = p.learned ? m.prop_init : m.init;
+      if (ip) {
+        v = make_float3(ip[3 * pix], ip[3 * pix + 1], ip[3 * pix + 2]);
         given = v.z != 0.0f;
         if (given) depth = depth_of_plane(j, i, m.Kinv_d, v);
       }
@@ -312,7 +313,15 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
   const size_t pix = (size_t)i * W + j;
   float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
   if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) st = m.state[pix];
-  if (st.w != 0.0f) {
+  bool run = st.w != 0.0f;
+  if (run && p.active && p.pass >= 2) {
+    // Interior pixel, so the 4 neighbours are inside the map.  Their flags
+    // were written by the previous half-pass, the pixel's own by the one
+    // before; this half-pass writes only pixels of its own colour.
+    const uint8_t* ch = m.changed;
+    run = (ch[pix] | ch[pix - W] | ch[pix + W] | ch[pix - 1] | ch[pix + 1]) != 0;
+  }
+  if (run) {
     Patch<HPZ, L> pt;
     pt.build(tile, pitch, threadIdx.y + HPZ, (j - x0) + HPZ, lane, mask);
     const float fj = (float)j, fi = (float)i;
@@ -423,8 +432,10 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
       m.state[pix] = make_float4(cv.x, cv.y, cv.z, cd);
       m.score[pix] = cur;
       m.nghbr[pix] = curn;
+      if (p.active) m.changed[pix] = same_plane(cv, make_float3(st.x, st.y, st.z)) ? 0 : 1;
     }
   }
+  // A skipped pixel's own flag is 0 already (it was part of the test).
   flush_taps(taps, p.taps);
 }
 

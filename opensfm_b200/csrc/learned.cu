@@ -22,9 +22,16 @@
 namespace dn {
 
 // ---------------------------------------------------------------- sweep
-// L lanes per pixel, as the PatchMatch initialisation (the 7 x 7 patch; the
-// tiles are the batch's initialisation tiles for its tuning).
-template <int L>
+// L lanes per pixel, as the PatchMatch initialisation (the 7 x 7 patch).
+// The features are computed on a grid of every S-th pixel in x and y
+// (S = 1: every pixel): grid point (ys, xs) is the full-resolution pixel
+// (S ys, S xs), scored with the full-resolution 7 x 7 patch around it.
+// Blocks cover (blockDim.x / L) x blockDim.y grid points; the staged tile
+// is the full-resolution region under them plus the patch halo.  Output:
+// map k's grid point (ys, xs) at feat + base_k + (ys Ws + xs) 32, with
+// base_k = k map_stride, or the map's proposal offset (MapDev::prop_off)
+// times 32 when map_stride < 0.
+template <int L, int S>
 __global__ void __launch_bounds__(128)
 sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
                       const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
@@ -35,9 +42,11 @@ sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict
   const MapDev& m = maps[tl.x];
   const ViewDev& rv = views[m.ref_view];
   const int W = m.W, H = m.H;
+  const int Ws = (W + S - 1) / S, Hs = (H + S - 1) / S;
   const int px = blockDim.x / L;
-  const int x0 = tl.y * px, y0 = tl.z * blockDim.y;
-  const int pitch = px + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
+  const int xs0 = tl.y * px, ys0 = tl.z * blockDim.y;
+  const int x0 = S * xs0, y0 = S * ys0;
+  const int pitch = S * px + 2 * HPZ, rows = S * blockDim.y + 2 * HPZ;
   __shared__ PairViewSm spv;
   for (int k = threadIdx.y * blockDim.x + threadIdx.x; k < pitch * rows;
        k += blockDim.x * blockDim.y) {
@@ -50,15 +59,18 @@ sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict
   const int g = threadIdx.x / L, lane = threadIdx.x % L;
   const unsigned mask = (L == 1) ? (1u << (threadIdx.x & 31))
                                  : (((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1)));
-  const int i = y0 + threadIdx.y, j = x0 + g;
-  if (i >= H || j >= W) return;
+  const int ys = ys0 + threadIdx.y, xs = xs0 + g;
+  // The lanes of a group share (ys, xs): a group leaves together.
+  if (ys >= Hs || xs >= Ws) return;
+  const int i = S * ys, j = S * xs;
+  const int ly = S * threadIdx.y + HPZ, lx = S * g + HPZ;
   float f[kFeatC];
 #pragma unroll
   for (int c = 0; c < kFeatC; ++c) f[c] = 0.f;
-  f[0] = (tile[(threadIdx.y + HPZ) * pitch + g + HPZ] - 128.0f) * (1.0f / 64.0f);
+  f[0] = (tile[ly * pitch + lx] - 128.0f) * (1.0f / 64.0f);
   if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) {
     Patch<HPZ, L> pt;
-    pt.build(tile, pitch, threadIdx.y + HPZ, g + HPZ, lane, mask);
+    pt.build(tile, pitch, ly, lx, lane, mask);
     const double a = 1.0 / m.min_depth, b = 1.0 / m.max_depth;
     unsigned taps = 0;
     const int nv = min(2, m.n_pairs);
@@ -74,7 +86,8 @@ sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict
     }
   }
   if (lane != 0) return;
-  __nv_bfloat16* out = feat + (long long)tl.x * map_stride + ((size_t)i * W + j) * kFeatC;
+  const long long base = map_stride >= 0 ? (long long)tl.x * map_stride : m.prop_off * kFeatC;
+  __nv_bfloat16* out = feat + base + ((size_t)ys * Ws + xs) * kFeatC;
 #pragma unroll
   for (int c = 0; c < kFeatC; c += 2)
     *reinterpret_cast<__nv_bfloat162*>(out + c) = __floats2bfloat162_rn(f[c], f[c + 1]);
@@ -681,14 +694,71 @@ __global__ void output_to_planes_kernel(const float* __restrict__ out, int W, in
   planes[3 * (size_t)k + 2] = v.z;
 }
 
-// PatchMatch result -> training target (t, sx, sy, weight).
+// Proposal grid output -> initial planes of every map of the batch
+// (blockIdx.y = map): the network's (t, sx, sy) at full-resolution pixel
+// (i, j) are the bilinear interpolation of the grid values around
+// (i / S, j / S) (grid point (ys, xs) sits on pixel (S ys, S xs); clamped
+// at the grid's last row and column), then the same depth and plane as
+// output_to_planes_kernel.  Writes MapDev::prop_init.
+template <int S>
+__global__ void proposal_to_planes_kernel(const float* __restrict__ out,
+                                          const MapDev* __restrict__ maps) {
+  const MapDev& m = maps[blockIdx.y];
+  const int W = m.W, H = m.H;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= W * H) return;
+  const int i = k / W, j = k - i * W;
+  const int Ws = m.prop_W, Hs = m.prop_H;
+  const float* o = out + 4 * m.prop_off;
+  float t, sx, sy;
+  if (S == 1) {
+    t = o[4 * (size_t)k];
+    sx = o[4 * (size_t)k + 1];
+    sy = o[4 * (size_t)k + 2];
+  } else {
+    const int y0 = min(i / S, Hs - 1), x0 = min(j / S, Ws - 1);
+    const int y1 = min(y0 + 1, Hs - 1), x1 = min(x0 + 1, Ws - 1);
+    const float fy = (float)(i - S * y0) * (1.0f / S), fx = (float)(j - S * x0) * (1.0f / S);
+    const float* q00 = o + 4 * ((size_t)y0 * Ws + x0);
+    const float* q01 = o + 4 * ((size_t)y0 * Ws + x1);
+    const float* q10 = o + 4 * ((size_t)y1 * Ws + x0);
+    const float* q11 = o + 4 * ((size_t)y1 * Ws + x1);
+    float v[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float top = fmaf(fx, q01[c] - q00[c], q00[c]);
+      const float bot = fmaf(fx, q11[c] - q10[c], q10[c]);
+      v[c] = fmaf(fy, bot - top, top);
+    }
+    t = v[0];
+    sx = v[1];
+    sy = v[2];
+  }
+  t = fminf(fmaxf(t, 0.f), 1.f);
+  const double a = 1.0 / m.max_depth, b = 1.0 / m.min_depth;
+  const float depth = (float)(1.0 / (a + (b - a) * (double)t));
+  sx = fminf(fmaxf(sx, -4.f), 4.f);
+  sy = fminf(fmaxf(sy, -4.f), 4.f);
+  const float3 v = plane_from_depth_normal((float)j, (float)i, m.Kinv_d, depth,
+                                           make_float3(sx, sy, -1.f));
+  float* planes = m.prop_init;
+  planes[3 * (size_t)k] = v.x;
+  planes[3 * (size_t)k + 1] = v.y;
+  planes[3 * (size_t)k + 2] = v.z;
+}
+
+// PatchMatch result -> training target (t, sx, sy, weight) on the proposal
+// grid of stride S: grid point (ys, xs) takes pixel (S ys, S xs).
 __global__ void planes_to_target_kernel(const float4* __restrict__ state,
-                                        const float* __restrict__ score, int W, int H,
+                                        const float* __restrict__ score, int W, int H, int S,
                                         const MapDev* __restrict__ maps, int map,
                                         float min_score, float* __restrict__ target) {
   const MapDev& m = maps[map];
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= W * H) return;
+  const int Ws = (W + S - 1) / S, Hs = (H + S - 1) / S;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= Ws * Hs) return;
+  const int ys = g / Ws, xs = g - ys * Ws;
+  const size_t k = (size_t)(S * ys) * W + S * xs;
   const float4 s = state[k];
   float4 tg = make_float4(0.f, 0.f, 0.f, 0.f);
   if (s.w > 0.f && s.z != 0.f && score[k] >= min_score) {
@@ -697,7 +767,7 @@ __global__ void planes_to_target_kernel(const float4* __restrict__ state,
     tg = make_float4(fminf(fmaxf(t, 0.f), 1.f), fminf(fmaxf(-s.x / s.z, -4.f), 4.f),
                      fminf(fmaxf(-s.y / s.z, -4.f), 4.f), 1.f);
   }
-  *reinterpret_cast<float4*>(target + 4 * (size_t)k) = tg;
+  *reinterpret_cast<float4*>(target + 4 * (size_t)g) = tg;
 }
 
 // ------------------------------------------------------------ launchers
@@ -776,23 +846,31 @@ cudaError_t conv3x3_backward(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaS
   if (c.cin == 32 && c.cout == 4) return conv_bwd_t<32, 4>(c, wt_scratch, s);
   return cudaErrorInvalidValue;
 }
-template <int L>
+template <int L, int S>
 static cudaError_t sweep_l(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
                            int n_planes, cudaStream_t s) {
-  // a.tiles: the initialisation tiling for L lanes (bx / L pixels per row).
-  const size_t smem = sizeof(float) * (a.bx / L + 6) * (a.by + 6);
-  sweep_features_kernel<L><<<a.n_tiles, dim3(a.bx, a.by), smem, s>>>(
+  // a.tiles: (bx / L) x by grid points per block on the stride-S grid.
+  const size_t smem = sizeof(float) * (S * (a.bx / L) + 6) * (S * a.by + 6);
+  sweep_features_kernel<L, S><<<a.n_tiles, dim3(a.bx, a.by), smem, s>>>(
       a.maps, a.views, a.pairs, a.tiles, feat, map_stride, n_planes);
   return cudaGetLastError();
 }
-cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
-                         int n_planes, cudaStream_t s) {
+template <int S>
+static cudaError_t sweep_s(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
+                           int n_planes, cudaStream_t s) {
   switch (a.p.variant) {
-    case 1: return sweep_l<1>(a, feat, map_stride, n_planes, s);
-    case 2: return sweep_l<2>(a, feat, map_stride, n_planes, s);
-    case 4: return sweep_l<4>(a, feat, map_stride, n_planes, s);
-    case 8: return sweep_l<8>(a, feat, map_stride, n_planes, s);
+    case 1: return sweep_l<1, S>(a, feat, map_stride, n_planes, s);
+    case 2: return sweep_l<2, S>(a, feat, map_stride, n_planes, s);
+    case 4: return sweep_l<4, S>(a, feat, map_stride, n_planes, s);
+    case 8: return sweep_l<8, S>(a, feat, map_stride, n_planes, s);
   }
+  return cudaErrorInvalidValue;
+}
+cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
+                         int n_planes, int stride, cudaStream_t s) {
+  if (a.n_tiles == 0) return cudaSuccess;
+  if (stride == 1) return sweep_s<1>(a, feat, map_stride, n_planes, s);
+  if (stride == 2) return sweep_s<2>(a, feat, map_stride, n_planes, s);
   return cudaErrorInvalidValue;
 }
 cudaError_t launch_l1_loss(const float* pred, const float* target, long long n_pix,
@@ -814,10 +892,23 @@ cudaError_t launch_output_to_planes(const float* out, int W, int H, const MapDev
   return cudaGetLastError();
 }
 cudaError_t launch_planes_to_target(const float4* state, const float* score, int W, int H,
-                                    const MapDev* maps, int map, float min_score, float* target,
-                                    cudaStream_t s) {
-  planes_to_target_kernel<<<(W * H + 255) / 256, 256, 0, s>>>(state, score, W, H, maps, map,
-                                                              min_score, target);
+                                    int stride, const MapDev* maps, int map, float min_score,
+                                    float* target, cudaStream_t s) {
+  const int n = ((W + stride - 1) / stride) * ((H + stride - 1) / stride);
+  planes_to_target_kernel<<<(n + 255) / 256, 256, 0, s>>>(state, score, W, H, stride, maps, map,
+                                                          min_score, target);
+  return cudaGetLastError();
+}
+cudaError_t launch_proposal_to_planes(const float* out, const MapDev* maps, int n_maps,
+                                      int max_pixels, int stride, cudaStream_t s) {
+  if (n_maps == 0) return cudaSuccess;
+  const dim3 grid((unsigned)((max_pixels + 255) / 256), (unsigned)n_maps);
+  if (stride == 1)
+    proposal_to_planes_kernel<1><<<grid, 256, 0, s>>>(out, maps);
+  else if (stride == 2)
+    proposal_to_planes_kernel<2><<<grid, 256, 0, s>>>(out, maps);
+  else
+    return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 

@@ -33,8 +33,10 @@ cudaError_t conv3x3_forward_mma_sync(const ConvArgs& c, cudaStream_t s);
 // (and clears it), 0 if not, -1 if the flag could not be read.
 int take_tc_error();
 cudaError_t conv3x3_backward(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaStream_t s);
+// Sweep features on the grid of every `stride`-th pixel (1 or 2); map k's
+// grid at feat + k map_stride, or at its MapDev::prop_off when map_stride < 0.
 cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,
-                         int n_planes, cudaStream_t s);
+                         int n_planes, int stride, cudaStream_t s);
 cudaError_t launch_l1_loss(const float* pred, const float* target, long long n_pix,
                            float normal_weight, __nv_bfloat16* dpred, float* loss_sum, float* count,
                            cudaStream_t s);
@@ -44,7 +46,11 @@ cudaError_t launch_adam(float* w, float* m, float* v, const float* grad, int n, 
 cudaError_t launch_output_to_planes(const float* out, int W, int H, const MapDev* maps, int map,
                                     float* planes, cudaStream_t s);
 cudaError_t launch_planes_to_target(const float4* state, const float* score, int W, int H,
-                                    const MapDev* maps, int map, float min_score, float* target,
-                                    cudaStream_t s);
+                                    int stride, const MapDev* maps, int map, float min_score,
+                                    float* target, cudaStream_t s);
+// Network outputs on every map's proposal grid (out + 4 prop_off) -> the
+// maps' MapDev::prop_init planes, upsampled by `stride` (1 or 2).
+cudaError_t launch_proposal_to_planes(const float* out, const MapDev* maps, int n_maps,
+                                      int max_pixels, int stride, cudaStream_t s);
 
 }  // namespace dn

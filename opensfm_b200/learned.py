@@ -56,8 +56,9 @@ def _stream():
 class ProposalNet:
     """FP32 master weights + Adam state on the device, BF16 copies for the kernels."""
 
-    def __init__(self, seed: int = 0):
+    def __init__(self, seed: int = 0, stride: int = 2):
         torch = _torch()
+        self.stride = stride  # proposal grid the network was trained on
         g = torch.Generator().manual_seed(seed)
         self.w32, self.b32, self.w16 = [], [], []
         for cin, cout, relu in LAYERS:
@@ -75,6 +76,14 @@ class ProposalNet:
     def sync_bf16(self):
         self.w16 = [w.to(_torch().bfloat16).contiguous() for w in self.w32]
 
+    def packed(self) -> Tuple[np.ndarray, np.ndarray]:
+        """(BF16 bit patterns of every layer's [cout][288] weights one after
+        the other, FP32 biases), the layout of ``Batch.set_proposal_net``."""
+        torch = _torch()
+        w = torch.cat([t.reshape(-1) for t in self.w16]).view(torch.int16).cpu().numpy()
+        b = torch.cat([t.reshape(-1) for t in self.b32]).cpu().numpy()
+        return w.view(np.uint16).copy(), b.astype(np.float32)
+
     # ------------------------------------------------------------ state
     def state_dict(self) -> Dict[str, np.ndarray]:
         d = {}
@@ -82,6 +91,7 @@ class ProposalNet:
             d[f"w{k}"] = w.cpu().numpy()
             d[f"b{k}"] = b.cpu().numpy()
         d["step"] = np.array(self.step)
+        d["stride"] = np.array(self.stride)
         return d
 
     def save(self, path: str, **extra):
@@ -101,6 +111,7 @@ class ProposalNet:
         net.m = [torch.zeros_like(t) for t in net.w32 + net.b32]
         net.v = [torch.zeros_like(t) for t in net.w32 + net.b32]
         net.step = int(z["step"]) if "step" in z else 0
+        net.stride = int(z["stride"]) if "stride" in z else 1
         net.wt_scratch = torch.empty(32 * 9 * 32, dtype=torch.bfloat16, device="cuda")
         return net
 
@@ -211,27 +222,36 @@ def build_batch(scenes: Sequence[SceneViews], iterations: int = 3, seed: int = 1
     return b, maps
 
 
-def features(b: pydense.Batch, n_maps: int, H: int, W: int, n_planes: int = 8):
+def grid_shape(H: int, W: int, stride: int) -> Tuple[int, int]:
+    """The proposal grid of an H x W map: every ``stride``-th pixel."""
+    return (H + stride - 1) // stride, (W + stride - 1) // stride
+
+
+def features(b: pydense.Batch, n_maps: int, H: int, W: int, n_planes: int = 8, stride: int = 1):
     torch = _torch()
-    stride = H * W * FEAT_C
-    feat = torch.zeros(n_maps * stride, dtype=torch.bfloat16, device="cuda")
-    _lib.check(b._L.dn_batch_sweep_features(b._h, _ptr(feat), stride, n_planes))
+    Hs, Ws = grid_shape(H, W, stride)
+    per = Hs * Ws * FEAT_C
+    feat = torch.zeros(n_maps * per, dtype=torch.bfloat16, device="cuda")
+    _lib.check(b._L.dn_batch_sweep_features(b._h, _ptr(feat), per, n_planes, stride))
     b.synchronize()
     return feat
 
 
-def targets(b: pydense.Batch, n_maps: int, H: int, W: int, min_score: float = 0.5):
+def targets(b: pydense.Batch, n_maps: int, H: int, W: int, min_score: float = 0.5,
+            stride: int = 1):
     torch = _torch()
-    stride = H * W * 4
-    tg = torch.zeros(n_maps * stride, dtype=torch.float32, device="cuda")
-    _lib.check(b._L.dn_batch_targets(b._h, _ptr(tg), stride, min_score))
+    Hs, Ws = grid_shape(H, W, stride)
+    per = Hs * Ws * 4
+    tg = torch.zeros(n_maps * per, dtype=torch.float32, device="cuda")
+    _lib.check(b._L.dn_batch_targets(b._h, _ptr(tg), per, min_score, stride))
     b.synchronize()
     return tg
 
 
-def make_dataset(seeds: Sequence[int], W: int = 320, H: int = 240, chunk: int = 100,
-                 iterations: int = 3, log=None):
-    """Features and plain-PatchMatch targets for every seed (device tensors)."""
+def make_dataset(seeds: Sequence[int], W: int = 640, H: int = 480, chunk: int = 50,
+                 iterations: int = 3, stride: int = 2, log=None):
+    """Features on the proposal grid and plain-PatchMatch targets at the same
+    grid points for every seed (device tensors)."""
     torch = _torch()
     feats, tgs = [], []
     t0 = time.time()
@@ -240,8 +260,8 @@ def make_dataset(seeds: Sequence[int], W: int = 320, H: int = 240, chunk: int = 
         b, maps = build_batch(scenes, iterations=iterations, seed=int(seeds[c0]) + 7)
         b.run()
         b.synchronize()
-        tgs.append(targets(b, len(maps), H, W))
-        feats.append(features(b, len(maps), H, W))
+        tgs.append(targets(b, len(maps), H, W, stride=stride))
+        feats.append(features(b, len(maps), H, W, stride=stride))
         b.close()
         if log:
             log(f"dataset {c0 + len(scenes)}/{len(seeds)} scenes, {time.time() - t0:.1f} s")
@@ -285,8 +305,9 @@ def train(net: ProposalNet, feat, tgt, n_maps: int, H: int, W: int, steps: int =
 
 # ------------------------------------------------------------- inference
 def propose(net: ProposalNet, b: pydense.Batch, maps: Sequence[int], H: int, W: int):
-    """Runs the sweep and the network for every depthmap of the batch and
-    installs the proposals as the batch's initial planes."""
+    """Runs the sweep and the network for every depthmap of the batch at full
+    resolution and installs the proposals as the batch's initial planes (the
+    step-by-step form of ``run(learned=True)`` with stride 1)."""
     torch = _torch()
     n = len(maps)
     feat = features(b, n, H, W)
@@ -296,6 +317,13 @@ def propose(net: ProposalNet, b: pydense.Batch, maps: Sequence[int], H: int, W: 
         _lib.check(b._L.dn_batch_init_from_output(b._h, int(m), _ptr(out[k * H * W:])))
     b.synchronize()
     return out
+
+
+def install(net: ProposalNet, b: pydense.Batch, stride: int = 2, n_planes: int = 8) -> None:
+    """Hands the network to the batch: ``b.run(learned=True)`` then sweeps,
+    runs the network and installs the proposals on the batch stream."""
+    w, bias = net.packed()
+    b.set_proposal_net(w, bias, n_planes=n_planes, stride=stride)
 
 
 def main(argv=None):
@@ -310,6 +338,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--size", default="640x480", help="training scene size WxH")
+    ap.add_argument("--stride", type=int, default=2, help="proposal grid stride (1 or 2)")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--evaluate", action="store_true",
@@ -318,7 +348,6 @@ def main(argv=None):
                     help="held-out scene seeds, start:stop (training uses 100000 and up)")
     ap.add_argument("--repeats", type=int, default=3)
     args = ap.parse_args(argv)
-    torch = _torch()
     log = lambda s: print(s, flush=True)  # noqa: E731
     if args.evaluate:
         a, b = (int(x) for x in args.eval_seeds.split(":"))
@@ -326,109 +355,119 @@ def main(argv=None):
         res = evaluate(net, list(range(a, b)), repeats=args.repeats, log=log)
         print(json.dumps(res), flush=True)
         return
+    W, H = (int(x) for x in args.size.split("x"))
     seeds = list(range(100000, 100000 + args.scenes))
-    feat, tgt = make_dataset(seeds, log=log)
+    feat, tgt = make_dataset(seeds, W=W, H=H, stride=args.stride, log=log)
     valid = float((tgt.view(-1, 4)[:, 3] > 0).float().mean().item())
     log(f"target coverage {valid:.3f}")
+    Hs, Ws = grid_shape(H, W, args.stride)
     net = ProposalNet(seed=args.seed)
-    hist = train(net, feat, tgt, len(seeds), 240, 320, steps=args.steps, batch=args.batch,
+    hist = train(net, feat, tgt, len(seeds), Hs, Ws, steps=args.steps, batch=args.batch,
                  lr=args.lr, log=log)
     net.save(args.out, history=np.array(hist), scenes=np.array(args.scenes),
-             seeds_start=np.array(seeds[0]))
+             seeds_start=np.array(seeds[0]), stride=np.array(args.stride),
+             train_W=np.array(W), train_H=np.array(H))
     log(f"saved {args.out}")
 
 
 # ------------------------------------------------------------ evaluation
-# PatchMatch schedules compared by evaluate(): (name, init, half-passes,
-# set_schedule keyword arguments).  "plain" is the reference's random
-# initialisation with its candidate schedule.
-PLAIN_3IT = ("plain-3it", "plain", 6, {})
+@dataclass
+class Schedule:
+    """A PatchMatch schedule compared by ``evaluate``: the initialisation
+    ("plain" = the reference's random initialisation, "learned" = the
+    proposal network), the half-passes, the candidate sets of
+    ``Batch.set_schedule``, one view per candidate (``sample``) and the
+    active-pixel half-passes (``active``)."""
+    name: str
+    init: str
+    half_passes: int
+    kw: dict
+    sample: bool = False
+    active: bool = False
+
+    def apply(self, b: pydense.Batch) -> None:
+        b.set_schedule(half_passes=self.half_passes, **self.kw)
+        b.set_candidate_views(self.sample)
+        b.set_active_pixels(self.active)
+
+
+PLAIN_3IT = Schedule("plain-3it", "plain", 6, {})
+_NEAR = dict(use_far=False, depth_range0=0.02, normal_range0=0.3)
 SCHEDULES = [
-    ("plain-1it", "plain", 2, {}),
-    ("plain-2it", "plain", 4, {}),
+    Schedule("plain-1it", "plain", 2, {}),
+    Schedule("plain-2it", "plain", 4, {}),
     PLAIN_3IT,
-    ("learned-0hp", "learned", 0, {}),
-    ("learned-1hp", "learned", 1, {}),
-    ("learned-2hp", "learned", 2, {}),
-    ("learned-3hp", "learned", 3, {}),
-    ("learned-4hp", "learned", 4, {}),
-    ("learned-5hp", "learned", 5, {}),
-    ("learned-6hp", "learned", 6, {}),
-    ("learned-near-2hp", "learned", 2, dict(use_far=False, depth_range0=0.05, normal_range0=0.3)),
-    ("learned-near-3hp", "learned", 3, dict(use_far=False, depth_range0=0.05, normal_range0=0.3)),
-    ("learned-near-4hp", "learned", 4, dict(use_far=False, depth_range0=0.05, normal_range0=0.3)),
+    Schedule("plain-3it-active", "plain", 6, {}, active=True),
+    Schedule("learned-0hp", "learned", 0, {}),
+    Schedule("learned-2hp", "learned", 2, {}),
+    Schedule("learned-4hp", "learned", 4, {}),
+    Schedule("learned-6hp", "learned", 6, {}),
+    Schedule("learned-sample-2hp", "learned", 2, {}, sample=True),
+    Schedule("learned-sample-4hp", "learned", 4, {}, sample=True),
+    Schedule("learned-sample-6hp", "learned", 6, {}, sample=True),
+    Schedule("learned-sample-8hp", "learned", 8, {}, sample=True),
+    Schedule("learned-sample-active-6hp", "learned", 6, {}, sample=True, active=True),
+    Schedule("learned-sample-active-8hp", "learned", 8, {}, sample=True, active=True),
+    Schedule("learned-sample-near-4hp", "learned", 4, _NEAR, sample=True),
+    Schedule("learned-sample-near-6hp", "learned", 6, _NEAR, sample=True),
+    Schedule("learned-sample-near3-6hp", "learned", 6, dict(_NEAR, n_refine=3), sample=True),
+    Schedule("learned-active-4hp", "learned", 4, {}, active=True),
+    Schedule("learned-active-6hp", "learned", 6, {}, active=True),
 ]
 
 
 def evaluate(net: Optional[ProposalNet], seeds: Sequence[int], W: int = 640, H: int = 480,
-             schedules=SCHEDULES, repeats: int = 3, log=None) -> dict:
+             schedules=SCHEDULES, repeats: int = 3, stride: Optional[int] = None, log=None,
+             scenes=None) -> dict:
     """Plain (random init) vs learned-init PatchMatch on held-out scenes.
 
-    For every schedule: the mean accuracy (|d - gt| / gt <= 1 % over valid
-    ground-truth pixels) and the device time of one batched run over all the
-    scenes; learned settings add the feature sweep and the network time.
+    Every schedule runs as one captured CUDA graph over all the scenes'
+    depthmaps (for learned schedules the feature sweep, the network and the
+    plane install included, on the batch stream) and is timed with device
+    events around the replay.  Accuracy: the mean over the maps of the
+    fraction of valid ground-truth pixels with |d - gt| / gt <= 1 %.
     """
-    torch = _torch()
-    scenes = [make_scene(s, W, H) for s in seeds]
+    scenes = scenes or [make_scene(s, W, H) for s in seeds]
     b, maps = build_batch(scenes, iterations=3, seed=int(seeds[0]) + 11)
     gts = [sv.depths[sv.ref] for sv in scenes]
+    if net is not None:
+        install(net, b, stride=stride or net.stride)
 
     def acc():
         return float(np.mean([S.accuracy(b.get_depth(m), gt) for m, gt in zip(maps, gts)]))
 
-    def timed(fn):
-        fn()  # warm-up (and graph capture)
+    out = {"scenes": len(scenes), "W": W, "H": H, "runs": [],
+           "stride": (stride or net.stride) if net is not None else None}
+    plain_ms = None
+    for sc in schedules:
+        if sc.init == "learned" and net is None:
+            continue
+        sc.apply(b)
+        learned = sc.init == "learned"
+        b.run(graph=True, learned=learned)  # capture
         b.synchronize()
         ts = []
         for _ in range(repeats):
             b.timer_record(0)
-            fn()
+            b.run(graph=True, learned=learned)
             b.timer_record(1)
             b.synchronize()
             ts.append(b.timer_elapsed())
-        return float(np.median(ts))
-
-    out = {"scenes": len(seeds), "W": W, "H": H, "runs": []}
-    t_sweep = t_net = 0.0
-    if net is not None:
-        stride = H * W * FEAT_C
-        feat = torch.zeros(len(maps) * stride, dtype=torch.bfloat16, device="cuda")
-        _lib.check(b._L.dn_batch_sweep_features(b._h, _ptr(feat), stride, 8))
+        t = float(np.median(ts))
+        b.run(graph=False, learned=learned, timing=True)
         b.synchronize()
-        net.forward(feat, len(maps) * H * W, H, W)
-        torch.cuda.synchronize()
-        b.timer_record(0)
-        _lib.check(b._L.dn_batch_sweep_features(b._h, _ptr(feat), stride, 8))
-        b.timer_record(1)
-        b.synchronize()
-        t_sweep = b.timer_elapsed()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        res = net.forward(feat, len(maps) * H * W, H, W)
-        e1.record()
-        torch.cuda.synchronize()
-        t_net = e0.elapsed_time(e1)
-        out["proposal_ms"] = {"sweep": t_sweep, "network": t_net}
-    plain_ms = None
-    for name, init, hp, kw in schedules:
-        if init == "learned" and net is None:
-            continue
-        for k, m in enumerate(maps):
-            if init == "learned":
-                _lib.check(b._L.dn_batch_init_from_output(b._h, int(m), _ptr(res[k * H * W:])))
-            else:
-                b.set_init(m, None)
-        b.set_schedule(half_passes=hp, **kw)
-        t = timed(lambda: b.run(graph=True))
-        total = t + (t_sweep + t_net if init == "learned" else 0.0)
-        r = {"name": name, "init": init, "half_passes": hp, "schedule": kw, "accuracy": acc(),
-             "ms_patchmatch": t, "ms": total}
-        if name == PLAIN_3IT[0]:
-            plain_ms = total
+        stages, taps = b.timings()
+        r = {"name": sc.name, "init": sc.init, "half_passes": sc.half_passes, "schedule": sc.kw,
+             "sample": sc.sample, "active": sc.active, "accuracy": acc(), "ms": t,
+             "stage_ms": {"proposal": stages[5], "init": stages[0], "halfpasses": stages[1],
+                          "post": stages[2]},
+             "halfpass_taps": taps[1]}
+        if sc.name == PLAIN_3IT.name:
+            plain_ms = t
         out["runs"].append(r)
         if log:
-            log(f"{name:20s} acc {r['accuracy']:.4f} pm {t:7.2f} ms total {total:7.2f} ms")
+            log(f"{sc.name:28s} acc {r['accuracy']:.4f} {t:7.2f} ms  (proposal {stages[5]:.2f}, "
+                f"init {stages[0]:.2f}, half-passes {stages[1]:.2f}, taps {taps[1] / 1e9:.2f}e9)")
     if plain_ms:
         for r in out["runs"]:
             r["speedup_vs_plain_3it"] = plain_ms / r["ms"]

@@ -715,6 +715,33 @@ class Batch(_Handle):
                                             int(bool(use_far)), int(n_refine), float(depth_range0),
                                             float(normal_range0)))
 
+    def set_candidate_views(self, sample: bool) -> None:
+        """Half-passes score every matching view per candidate (False, the
+        reference's ComputePatchMatch), or one view per candidate plus one
+        random other view per update (True, as ComputePatchMatchSample)."""
+        check(self._L.dn_batch_set_candidate_views(self._h, int(bool(sample))))
+
+    def set_active_pixels(self, on: bool) -> None:
+        """From the third half-pass on, update only pixels whose own plane or a
+        neighbour's plane changed at their last update."""
+        check(self._L.dn_batch_set_active_pixels(self._h, int(bool(on))))
+
+    def set_proposal_net(self, weights: Optional[np.ndarray], biases: Optional[np.ndarray] = None,
+                         n_planes: int = 8, stride: int = 2) -> None:
+        """The network of learned runs (``run(learned=True)``): ``weights`` the
+        BF16 bit patterns (uint16) of the 6 layers' [cout][288] matrices one
+        after the other, ``biases`` their FP32 biases; None removes it."""
+        if weights is None:
+            check(self._L.dn_batch_set_proposal_net(self._h, None, None, 0, 0))
+            return
+        w = np.ascontiguousarray(weights, dtype=np.uint16)
+        b = np.ascontiguousarray(biases, dtype=np.float32)
+        if w.size != 5 * 32 * 288 + 4 * 288 or b.size != 5 * 32 + 4:
+            raise ValueError("weights must hold 46080 BF16 values and biases 164 floats")
+        check(self._L.dn_batch_set_proposal_net(
+            self._h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), ptr(b, _f), int(n_planes),
+            int(stride)))
+
     def set_init(self, map_id: int, planes: Optional[np.ndarray]) -> None:
         if planes is None:
             check(self._L.dn_batch_set_init(self._h, int(map_id), None))
@@ -725,9 +752,10 @@ class Batch(_Handle):
         check(self._L.dn_batch_set_init(self._h, int(map_id), ptr(pl, _f)))
 
     def run(self, clean: bool = False, graph: bool = False, timing: bool = False,
-            prune: bool = False) -> None:
+            prune: bool = False, learned: bool = False) -> None:
         flags = ((_lib.DN_RUN_CLEAN if clean or prune else 0) | (_lib.DN_RUN_GRAPH if graph else 0) |
-                 (_lib.DN_RUN_TIMING if timing else 0) | (_lib.DN_RUN_PRUNE if prune else 0))
+                 (_lib.DN_RUN_TIMING if timing else 0) | (_lib.DN_RUN_PRUNE if prune else 0) |
+                 (_lib.DN_RUN_LEARNED if learned else 0))
         check(self._L.dn_batch_run(self._h, flags))
 
     def pruned_count(self) -> int:
@@ -769,10 +797,11 @@ class Batch(_Handle):
         return float(ms.value)
 
     def timings(self):
-        """(per-stage ms [init, half-passes, post, clean, total], [init taps, half-pass taps])."""
-        t = np.zeros(5, np.float32)
+        """(per-stage ms [init, half-passes, post, clean and prune, total, learned
+        proposal], [init taps, half-pass taps])."""
+        t = np.zeros(6, np.float32)
         taps = (ctypes.c_uint64 * 2)()
-        check(self._L.dn_batch_last_timings(self._h, ptr(t, _f), 5, taps))
+        check(self._L.dn_batch_last_timings(self._h, ptr(t, _f), 6, taps))
         return t.astype(float).tolist(), [int(taps[0]), int(taps[1])]
 
     def synchronize(self) -> None:

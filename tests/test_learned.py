@@ -184,7 +184,7 @@ def test_adam_step_matches_formula():
 def test_short_training_reduces_loss():
     """Trains on 16 seeded scenes for 60 steps: the loss must drop."""
     seeds = list(range(500, 516))
-    feat, tgt = learned.make_dataset(seeds, W=160, H=120, chunk=16)
+    feat, tgt = learned.make_dataset(seeds, W=160, H=120, chunk=16, stride=1)
     net = learned.ProposalNet(seed=1)
     hist = learned.train(net, feat, tgt, len(seeds), 120, 160, steps=60, batch=4, lr=3e-3)
     assert hist[-1][1] < 0.8 * hist[0][1], hist

@@ -1,0 +1,138 @@
+"""PatchMatch and brute force at the benchmark sizes against the reference.
+
+Fixtures (tests/golden/make_pm_configs.py) hold the outputs of the
+reference's own depthmap.cc (compiled as oracle/_ref) on:
+  * config 1: box scene, 1 reference + 4 ring neighbours, 320 x 240,
+    patch 7, min_patch_sd 1.0, brute force with 64 planes, PatchMatch and
+    PatchMatch (sample) with 3 iterations;
+  * config 2: the benchmark's 24-view 640 x 480 ring, depthmaps 0, 8 and
+    16 against their 6 nearest views, PatchMatch with 3 iterations.
+The scenes are regenerated from their seeds (checked by SHA-256).
+
+Tolerances (asserted below):
+  * Brute force (deterministic): the same plane on >= 98 % of the interior
+    pixels, and on those the scores within 2e-3 on >= 99.5 % (the GPU's
+    mean-centred FP32 sums against the reference's raw-moment FP32 sums).
+  * PatchMatch and PatchMatch sample (random schedules, so statistical):
+    accuracy against the ray-cast ground truth (|d - gt| / gt <= 1 %),
+    averaged over runs, at least the reference's average over its runs, per
+    configuration; and the GPU depth agrees with the reference's within 1 %
+    on >= 80 % of the pixels where both are valid.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+from opensfm_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+if not gpu_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from opensfm_b200 import pydense  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+sys.path.insert(0, GOLDEN)
+import make_pm_configs as M  # noqa: E402
+
+SEEDS = (1, 2, 3)
+
+
+def _agreement(a, b):
+    both = (a > 0) & (b > 0)
+    return float(np.mean(np.abs(a[both] - b[both]) / b[both] <= 0.01))
+
+
+@pytest.fixture(scope="module")
+def config1():
+    z = np.load(os.path.join(GOLDEN, "pm_config1_320x240.npz"))
+    cams, images, depths = M.config1_views()
+    assert M.images_digest(images) == str(z["images_sha256"])
+    return z, cams, images, depths
+
+
+@pytest.fixture(scope="module")
+def config2():
+    z = np.load(os.path.join(GOLDEN, "pm_config2_640x480.npz"))
+    vs, matches = M.config2_views()
+    assert M.images_digest(vs.images) == str(z["images_sha256"])
+    return z, vs, matches
+
+
+def _estimator(z, cams, images, seed):
+    e = pydense.DepthmapEstimator()
+    for c, im in zip(cams, images):
+        e.add_view(c.K, c.R, c.t, im, np.ones_like(im))
+    e.set_depth_range(float(z["min_depth"]), float(z["max_depth"]), int(z["num_planes"]))
+    e.set_patch_size(int(z["patch_size"]))
+    e.set_min_patch_sd(float(z["min_patch_sd"]))
+    e.set_patchmatch_iterations(int(z["iterations"]))
+    e.set_seed(seed)
+    return e
+
+
+def test_config1_brute_force_64_planes(config1):
+    z, cams, images, depths = config1
+    depth, plane, score, nghbr = _estimator(z, cams, images, 1).compute_brute_force()
+    hpz = 3
+    inner = (slice(hpz, -hpz), slice(hpz, -hpz))
+    same = depth[inner] == z["bf_depth"][inner]
+    dscore = np.abs(score[inner] - z["bf_score"][inner])
+    print("config 1 brute force: same plane %.5f, |dscore| <= 2e-3 on %.5f of those, "
+          "same view %.5f" % (same.mean(), (dscore[same] <= 2e-3).mean(),
+                              (nghbr[inner][same] == z["bf_nghbr"][inner][same]).mean()))
+    assert same.mean() >= 0.98
+    assert (dscore[same] <= 2e-3).mean() >= 0.995
+    # Border pixels stay empty, as in the reference.
+    assert (depth[:hpz] == 0).all() and (depth[:, -hpz:] == 0).all()
+
+
+@pytest.mark.parametrize("mode", ["patch_match", "patch_match_sample"])
+def test_config1_patch_match_accuracy(config1, mode):
+    z, cams, images, depths = config1
+    gt = depths[0]
+    key = "pm" if mode == "patch_match" else "sample"
+    accs, agrees = [], []
+    for seed in SEEDS:
+        e = _estimator(z, cams, images, seed)
+        out = getattr(e, "compute_" + mode)()
+        accs.append(S.accuracy(out[0], gt))
+        agrees.append(_agreement(out[0], z[key + "_depth0"].astype(np.float32)))
+    ref = z[key + "_accuracy"]
+    print("config 1 %s: accuracy gpu %s (mean %.4f) reference %s (mean %.4f); agreement %s"
+          % (mode, np.round(accs, 4), np.mean(accs), np.round(ref, 4), ref.mean(),
+             np.round(agrees, 4)))
+    assert np.mean(accs) >= ref.mean()
+    assert min(agrees) >= 0.8
+
+
+def test_config2_patch_match_accuracy(config2):
+    z, vs, matches = config2
+    maps = [int(v) for v in z["maps"]]
+    b = pydense.Batch()
+    for c, im in zip(vs.cameras, vs.images):
+        b.add_view(c.K, c.R, c.t, im)
+    for v, mt in zip(maps, z["matches"]):
+        b.add_depthmap(v, [int(o) for o in mt], *S.depth_range(vs.depths[v]))
+    acc = np.zeros((len(maps), len(SEEDS)))
+    agree = np.zeros_like(acc)
+    for s, seed in enumerate(SEEDS):
+        b.set_params(patch_size=int(z["patch_size"]), min_patch_sd=float(z["min_patch_sd"]),
+                     iterations=int(z["iterations"]), seed=seed)
+        b.run()
+        b.synchronize()
+        for k, v in enumerate(maps):
+            d = b.get_depth(k)
+            acc[k, s] = S.accuracy(d, vs.depths[v])
+            agree[k, s] = _agreement(d, z["pm_depth0"][k].astype(np.float32))
+    b.close()
+    ref = z["pm_accuracy"]
+    print("config 2: accuracy gpu per map %s (mean %.4f), reference per map %s (mean %.4f); "
+          "agreement %s" % (np.round(acc.mean(1), 4), acc.mean(), np.round(ref.mean(1), 4),
+                            ref.mean(), np.round(agree.min(1), 4)))
+    assert acc.mean() >= ref.mean()
+    assert agree.min() >= 0.8
