@@ -351,9 +351,12 @@ dn_status dn_nn_adam(float* w, float* m, float* v, const float* grad, int n, con
  * into the library (about 4.3 MB per GPU, held until exit).  Limits: the
  * reference depthmap (view 0) has at most 4,194,304 pixels, at most 17 views,
  * and `capacity` (points the output buffers hold) is at least its
- * width * height.  The number of kept points is written to the device
- * counter *count.  Work is enqueued on `stream` (a cudaStream_t, NULL for
- * the default stream) and the call returns without waiting.  All calls share
+ * width * height; every view is at most 16384 pixels a side, with finite
+ * K, R, t and an invertible K (as dn_pruner_add_view checks).  The number of
+ * kept points is written to the device counter *count.  Work is enqueued on
+ * `stream` (a cudaStream_t, NULL for the default stream), the view table
+ * included (it is passed as a kernel argument, so the host array `views`
+ * may be freed on return), and the call returns without waiting.  All calls share
  * the static array: calls whose GPU work overlaps race and must be
  * serialised by the caller.  The first call on a device looks up the array's
  * address with that device current; make it before any stream capture.

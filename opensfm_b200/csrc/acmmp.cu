@@ -41,6 +41,7 @@
 #include <vector>
 
 #include "dense_b200.h"
+#include "device_guard.h"
 
 namespace {
 
@@ -1101,6 +1102,7 @@ extern "C" const char* dn_acmmp_last_error(void) { return g_acm_error.c_str(); }
 
 
 extern "C" dn_status dn_acmmp_create(dn_acmmp** out) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(out, "NULL output");
   *out = nullptr;
   int n = 0;
@@ -1112,6 +1114,7 @@ extern "C" dn_status dn_acmmp_create(dn_acmmp** out) {
   return DN_OK;
 }
 extern "C" dn_status dn_acmmp_destroy(dn_acmmp* e) {
+  const dn::DeviceRestore device_restore_;
   delete e;
   return DN_OK;
 }
@@ -1134,6 +1137,7 @@ ACM_SETTER(geom_consistency_weight, geom_weight, float)
 #undef ACM_SETTER
 
 extern "C" dn_status dn_acmmp_set_patch_size(dn_acmmp* e, int size) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e, "NULL estimator");
   ACHECK(size >= 1 && size <= 63, "patch size must be in [1, 63]");
   e->patch_size = size;
@@ -1141,6 +1145,7 @@ extern "C" dn_status dn_acmmp_set_patch_size(dn_acmmp* e, int size) {
 }
 
 extern "C" dn_status dn_acmmp_set_device(dn_acmmp* e, int device) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e, "NULL estimator");
   int n = 0;
   ACUDA(cudaGetDeviceCount(&n));
@@ -1176,6 +1181,7 @@ extern "C" dn_status dn_acmmp_begin_ref_view(dn_acmmp* e, const double* K, const
                                              const double* t, const uint8_t* img, int w, int h,
                                              int stride, float depth_min, float depth_max,
                                              int* ref_idx) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e, "NULL estimator");
   ARef ref;
   ref.depth_min = depth_min;
@@ -1191,6 +1197,7 @@ extern "C" dn_status dn_acmmp_begin_ref_view(dn_acmmp* e, const double* K, const
 extern "C" dn_status dn_acmmp_add_source_view(dn_acmmp* e, const double* K, const double* R,
                                               const double* t, const uint8_t* img, int w, int h,
                                               int stride) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e, "NULL estimator");
   if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no ref view started");
   AView v;
@@ -1201,6 +1208,7 @@ extern "C" dn_status dn_acmmp_add_source_view(dn_acmmp* e, const double* K, cons
 }
 
 extern "C" dn_status dn_acmmp_set_sfm_points(dn_acmmp* e, const double* points, int64_t n) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e, "NULL estimator");
   if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no ref view started");
   ACHECK(n >= 0 && (n == 0 || points), "NULL points");
@@ -1212,6 +1220,7 @@ extern "C" dn_status dn_acmmp_set_sfm_points(dn_acmmp* e, const double* points, 
 
 extern "C" dn_status dn_acmmp_add_geom_link(dn_acmmp* e, int ref_idx, int source_view_idx,
                                             int from_ref_idx) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e, "NULL estimator");
   ACHECK(ref_idx >= 0 && ref_idx < (int)e->refs.size(),
          "DepthmapClusterEstimator::AddGeomLink: invalid ref_idx");
@@ -1222,6 +1231,7 @@ extern "C" dn_status dn_acmmp_add_geom_link(dn_acmmp* e, int ref_idx, int source
 }
 
 extern "C" dn_status dn_acmmp_clear(dn_acmmp* e) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e, "NULL estimator");
   e->refs.clear();
   e->geom_links.clear();
@@ -1229,6 +1239,7 @@ extern "C" dn_status dn_acmmp_clear(dn_acmmp* e) {
 }
 
 extern "C" dn_status dn_acmmp_num_refs(dn_acmmp* e, int* n) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e && n, "NULL argument");
   *n = (int)e->refs.size();
   return DN_OK;
@@ -1841,6 +1852,7 @@ static dn_status run_level(dn_acmmp* e, ARef& ref, int level, int n_levels, cons
 // where they run concurrently, the sum of their spans where they run in
 // turn (the host work between them is not device time).
 extern "C" dn_status dn_acmmp_run(dn_acmmp* e) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e, "NULL estimator");
   if (e->refs.empty()) return afail(DN_INVALID_ARG, "DepthmapClusterEstimator: no reference views");
   ACUDA(cudaSetDevice(e->device));
@@ -1947,6 +1959,7 @@ extern "C" dn_status dn_acmmp_run(dn_acmmp* e) {
 }
 
 extern "C" dn_status dn_acmmp_result_size(dn_acmmp* e, int ref_idx, int* w, int* h) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e && w && h, "NULL argument");
   if (ref_idx < 0 || ref_idx >= (int)e->refs.size()) return afail(DN_OUT_OF_RANGE, "ref index out of range");
   *w = e->refs[ref_idx].W ? e->refs[ref_idx].W : e->refs[ref_idx].views[0].W;
@@ -1956,6 +1969,7 @@ extern "C" dn_status dn_acmmp_result_size(dn_acmmp* e, int ref_idx, int* w, int*
 
 extern "C" dn_status dn_acmmp_get_result(dn_acmmp* e, int ref_idx, float* depth, float* normal,
                                          float* cost, float* confidence) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e, "NULL estimator");
   if (ref_idx < 0 || ref_idx >= (int)e->refs.size()) return afail(DN_OUT_OF_RANGE, "ref index out of range");
   const ARef& r = e->refs[ref_idx];
@@ -1968,6 +1982,7 @@ extern "C" dn_status dn_acmmp_get_result(dn_acmmp* e, int ref_idx, float* depth,
 }
 
 extern "C" dn_status dn_acmmp_last_run_ms(dn_acmmp* e, float* ms) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(e && ms, "NULL argument");
   *ms = e->last_ms;
   return DN_OK;
@@ -1975,6 +1990,7 @@ extern "C" dn_status dn_acmmp_last_run_ms(dn_acmmp* e, float* ms) {
 
 extern "C" dn_status dn_delaunay_2d(const double* xy, int n, int w, int h, int* tris, int capacity,
                                      int* count) {
+  const dn::DeviceRestore device_restore_;
   ACHECK(count && (n == 0 || xy) && n >= 0 && w > 0 && h > 0, "bad argument");
   for (int i = 0; i < 2 * n; ++i) ACHECK(std::isfinite(xy[i]), "non-finite coordinate");
   std::vector<double> px(n), py(n);

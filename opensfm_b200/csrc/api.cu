@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "dense_b200.h"
+#include "device_guard.h"
 #include "kernels.h"
 #include "learned.h"
 
@@ -994,6 +995,7 @@ static dn_status need_device() {
 
 // ------------------------------------------------------------- estimator
 dn_status dn_estimator_create(dn_estimator** out) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(out, "NULL output");
   *out = nullptr;
   DN_TRY(need_device());
@@ -1004,6 +1006,7 @@ dn_status dn_estimator_create(dn_estimator** out) {
 }
 
 dn_status dn_estimator_destroy(dn_estimator* est) {
+  const dn::DeviceRestore device_restore_;
   delete est;
   return DN_OK;
 }
@@ -1011,6 +1014,7 @@ dn_status dn_estimator_destroy(dn_estimator* est) {
 dn_status dn_estimator_add_view(dn_estimator* est, const double* K, const double* R,
                                 const double* t, const uint8_t* image, const uint8_t* mask,
                                 int width, int height, int stride) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   DN_CHECK((int)est->eng.views.size() <= dn::kMaxNbr, "at most 17 views (reference + 16)");
   int id;
@@ -1030,6 +1034,7 @@ dn_status dn_estimator_add_view(dn_estimator* est, const double* K, const double
 }
 
 dn_status dn_estimator_set_depth_range(dn_estimator* est, double mn, double mx, int n) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   est->min_d = mn;
   est->max_d = mx;
@@ -1043,6 +1048,7 @@ dn_status dn_estimator_set_depth_range(dn_estimator* est, double mn, double mx, 
 }
 
 dn_status dn_estimator_set_patchmatch_iterations(dn_estimator* est, int n) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   est->eng.iterations = n;
   est->eng.invalidate();
@@ -1050,6 +1056,7 @@ dn_status dn_estimator_set_patchmatch_iterations(dn_estimator* est, int n) {
 }
 
 dn_status dn_estimator_set_patch_size(dn_estimator* est, int size) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   const int hpz = (size - 1) / 2;
   DN_CHECK(hpz >= 1 && hpz <= dn::kMaxHpz, "patch size must be in 3..12");
@@ -1058,12 +1065,14 @@ dn_status dn_estimator_set_patch_size(dn_estimator* est, int size) {
 }
 
 dn_status dn_estimator_set_min_patch_sd(dn_estimator* est, float sd) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   est->eng.min_var = sd * sd;
   return DN_OK;
 }
 
 dn_status dn_estimator_set_seed(dn_estimator* est, uint64_t seed) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   est->eng.seed = seed;
   return DN_OK;
@@ -1080,18 +1089,21 @@ static dn_status est_compute(dn_estimator* est, Mode mode, float* depth, float* 
 
 dn_status dn_estimator_compute_brute_force(dn_estimator* est, float* depth, float* plane,
                                            float* score, int32_t* nghbr) {
+  const dn::DeviceRestore device_restore_;
   if (est && est->eng.maps.size() == 1 && est->eng.maps[0]->has_init) est->eng.set_init(0, nullptr);
   return est_compute(est, Mode::kBruteForce, depth, plane, score, nghbr);
 }
 
 dn_status dn_estimator_compute_patch_match(dn_estimator* est, float* depth, float* plane,
                                            float* score, int32_t* nghbr) {
+  const dn::DeviceRestore device_restore_;
   if (est && est->eng.maps.size() == 1 && est->eng.maps[0]->has_init) est->eng.set_init(0, nullptr);
   return est_compute(est, Mode::kPatchMatch, depth, plane, score, nghbr);
 }
 
 dn_status dn_estimator_compute_patch_match_sample(dn_estimator* est, float* depth,
                                                   float* plane, float* score, int32_t* nghbr) {
+  const dn::DeviceRestore device_restore_;
   if (est && est->eng.maps.size() == 1 && est->eng.maps[0]->has_init) est->eng.set_init(0, nullptr);
   return est_compute(est, Mode::kPatchMatchSample, depth, plane, score, nghbr);
 }
@@ -1099,6 +1111,7 @@ dn_status dn_estimator_compute_patch_match_sample(dn_estimator* est, float* dept
 dn_status dn_estimator_compute_patch_match_init(dn_estimator* est, const float* init_planes,
                                                 float* depth, float* plane, float* score,
                                                 int32_t* nghbr) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   DN_CHECK(init_planes, "init planes must not be NULL");
   DN_CHECK(est->eng.maps.size() == 1, "DepthmapEstimator needs a reference and at least one other view");
@@ -1108,6 +1121,7 @@ dn_status dn_estimator_compute_patch_match_init(dn_estimator* est, const float* 
 
 dn_status dn_estimator_score_planes(dn_estimator* est, const float* planes, float* score,
                                     int32_t* nghbr) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   DN_CHECK(planes && score && nghbr, "buffers must not be NULL");
   DN_CHECK(est->eng.views.size() >= 2, "DepthmapEstimator needs a reference and at least one other view");
@@ -1119,6 +1133,7 @@ dn_status dn_estimator_score_planes(dn_estimator* est, const float* planes, floa
 }
 
 dn_status dn_estimator_last_taps(dn_estimator* est, uint64_t* taps) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   return est->eng.taps(taps);
 }
@@ -1126,6 +1141,7 @@ dn_status dn_estimator_last_taps(dn_estimator* est, uint64_t* taps) {
 // ---------------------------------------------------------------- cleaner
 // ------------------------------------------------------- GPUDepthmapCleaner
 dn_status dn_gpu_cleaner_create(dn_gpu_cleaner** out) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(out, "NULL output");
   *out = nullptr;
   DN_TRY(need_device());
@@ -1136,25 +1152,30 @@ dn_status dn_gpu_cleaner_create(dn_gpu_cleaner** out) {
   return DN_OK;
 }
 dn_status dn_gpu_cleaner_destroy(dn_gpu_cleaner* c) {
+  const dn::DeviceRestore device_restore_;
   delete c;
   return DN_OK;
 }
 dn_status dn_gpu_cleaner_set_same_depth_threshold(dn_gpu_cleaner* c, float t) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   c->thr = t;
   return DN_OK;
 }
 dn_status dn_gpu_cleaner_set_min_consistent_views(dn_gpu_cleaner* c, int n) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   c->min_views = n;
   return DN_OK;
 }
 dn_status dn_gpu_cleaner_set_carving_threshold(dn_gpu_cleaner* c, float t) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   c->carving = std::max(0.0f, t);  // cleaner.cc:31-33
   return DN_OK;
 }
 dn_status dn_gpu_cleaner_set_max_carved_views(dn_gpu_cleaner* c, int n) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   c->max_carved = std::max(0, n);  // cleaner.cc:35-37
   return DN_OK;
@@ -1162,6 +1183,7 @@ dn_status dn_gpu_cleaner_set_max_carved_views(dn_gpu_cleaner* c, int n) {
 dn_status dn_gpu_cleaner_add_view(dn_gpu_cleaner* c, const double* K, const double* R,
                                   const double* t, const float* depth, int width, int height,
                                   int stride, int* id) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   DN_TRY(check_camera(K, R, t));
   DN_CHECK(depth, "depth must not be NULL");
@@ -1187,6 +1209,7 @@ dn_status dn_gpu_cleaner_add_view(dn_gpu_cleaner* c, const double* K, const doub
 }
 dn_status dn_gpu_cleaner_clean(dn_gpu_cleaner* c, int ref, const int* neighbor_ids, int n,
                                float* out) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c && out, "NULL argument");
   DN_CHECK(n >= 0 && (n == 0 || neighbor_ids), "NULL neighbour list");
   const int nv = (int)c->views.size();
@@ -1229,6 +1252,7 @@ dn_status dn_gpu_cleaner_clean(dn_gpu_cleaner* c, int ref, const int* neighbor_i
   return DN_OK;
 }
 dn_status dn_gpu_cleaner_clear(dn_gpu_cleaner* c) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   c->views.clear();
   c->d_out.release();
@@ -1236,6 +1260,7 @@ dn_status dn_gpu_cleaner_clear(dn_gpu_cleaner* c) {
 }
 
 dn_status dn_cleaner_create(dn_cleaner** out) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(out, "NULL output");
   *out = nullptr;
   DN_TRY(need_device());
@@ -1246,21 +1271,25 @@ dn_status dn_cleaner_create(dn_cleaner** out) {
   return DN_OK;
 }
 dn_status dn_cleaner_destroy(dn_cleaner* c) {
+  const dn::DeviceRestore device_restore_;
   delete c;
   return DN_OK;
 }
 dn_status dn_cleaner_set_same_depth_threshold(dn_cleaner* c, float t) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   c->thr = t;
   return DN_OK;
 }
 dn_status dn_cleaner_set_min_consistent_views(dn_cleaner* c, int n) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   c->min_views = n;
   return DN_OK;
 }
 dn_status dn_cleaner_add_view(dn_cleaner* c, const double* K, const double* R, const double* t,
                               const float* depth, int width, int height, int stride) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   DN_TRY(check_camera(K, R, t));
   DN_CHECK(depth, "depth must not be NULL");
@@ -1286,6 +1315,7 @@ dn_status dn_cleaner_add_view(dn_cleaner* c, const double* K, const double* R, c
   return DN_OK;
 }
 dn_status dn_cleaner_clean(dn_cleaner* c, float* clean_depth) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(c, "NULL cleaner");
   DN_CHECK(clean_depth, "output must not be NULL");
   DN_CHECK(!c->views.empty(), "DepthmapCleaner has no views");
@@ -1312,6 +1342,7 @@ dn_status dn_cleaner_clean(dn_cleaner* c, float* clean_depth) {
 
 // ----------------------------------------------------------------- pruner
 dn_status dn_pruner_create(dn_pruner** out) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(out, "NULL output");
   *out = nullptr;
   DN_TRY(need_device());
@@ -1323,10 +1354,12 @@ dn_status dn_pruner_create(dn_pruner** out) {
   return DN_OK;
 }
 dn_status dn_pruner_destroy(dn_pruner* p) {
+  const dn::DeviceRestore device_restore_;
   delete p;
   return DN_OK;
 }
 dn_status dn_pruner_set_same_depth_threshold(dn_pruner* p, float t) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(p, "NULL pruner");
   p->thr = t;
   return DN_OK;
@@ -1334,6 +1367,7 @@ dn_status dn_pruner_set_same_depth_threshold(dn_pruner* p, float t) {
 dn_status dn_pruner_add_view(dn_pruner* p, const double* K, const double* R, const double* t,
                              const float* depth, const float* plane, const uint8_t* color,
                              const uint8_t* label, int width, int height) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(p, "NULL pruner");
   DN_TRY(check_camera(K, R, t));
   DN_CHECK(depth && plane && color && label, "depth, plane, color and label must not be NULL");
@@ -1371,6 +1405,7 @@ dn_status dn_pruner_add_view(dn_pruner* p, const double* K, const double* R, con
   return DN_OK;
 }
 dn_status dn_pruner_prune(dn_pruner* p, int64_t* count) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(p, "NULL pruner");
   DN_CHECK(count, "NULL count");
   DN_CHECK(!p->views.empty(), "DepthmapPruner has no views");
@@ -1398,6 +1433,7 @@ dn_status dn_pruner_prune(dn_pruner* p, int64_t* count) {
 }
 dn_status dn_pruner_fetch(dn_pruner* p, float* points, float* normals, uint8_t* colors,
                           uint8_t* labels, int64_t capacity) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(p, "NULL pruner");
   DN_CHECK(p->count >= 0, "dn_pruner_prune has not run since the last add_view");
   DN_CHECK(capacity >= p->count, "capacity is smaller than the pruned point count");
@@ -1419,6 +1455,7 @@ dn_status dn_pruner_fetch(dn_pruner* p, float* points, float* normals, uint8_t* 
 
 // ----------------------------------------------------------------- batch
 dn_status dn_batch_create(dn_batch** out) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(out, "NULL output");
   *out = nullptr;
   DN_TRY(need_device());
@@ -1428,23 +1465,27 @@ dn_status dn_batch_create(dn_batch** out) {
   return DN_OK;
 }
 dn_status dn_batch_destroy(dn_batch* b) {
+  const dn::DeviceRestore device_restore_;
   delete b;
   return DN_OK;
 }
 dn_status dn_batch_add_view(dn_batch* b, const double* K, const double* R, const double* t,
                             const uint8_t* image, const uint8_t* mask, int width, int height,
                             int stride, int* view_id) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   return b->eng.add_view(K, R, t, image, mask, width, height, stride, view_id);
 }
 dn_status dn_batch_add_depthmap(dn_batch* b, int ref_view, const int* matching, int n,
                                 double min_depth, double max_depth, int* map_id) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   DN_CHECK(matching || n == 0, "NULL matching view list");
   for (int k = 0; k < n; ++k) DN_CHECK(matching[k] != ref_view, "a view cannot match itself");
   return b->eng.add_map(ref_view, matching, n, min_depth, max_depth, map_id);
 }
 dn_status dn_batch_set_clean_views(dn_batch* b, int map_id, const int* other_maps, int n) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   DN_CHECK(map_id >= 0 && map_id < (int)b->eng.maps.size(), "depthmap id out of range");
   DN_CHECK(n >= 0 && n <= dn::kMaxNbr, "at most 16 cleaner views");
@@ -1461,6 +1502,7 @@ dn_status dn_batch_set_clean_views(dn_batch* b, int map_id, const int* other_map
 dn_status dn_batch_set_params(dn_batch* b, int patch_size, float min_patch_sd, int iterations,
                               float same_depth_threshold, int min_consistent_views,
                               uint64_t seed) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   const int hpz = (patch_size - 1) / 2;
   DN_CHECK(hpz >= 1 && hpz <= dn::kMaxHpz, "patch size must be in 3..12");
@@ -1476,6 +1518,7 @@ dn_status dn_batch_set_params(dn_batch* b, int patch_size, float min_patch_sd, i
 }
 dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int use_far,
                                 int n_refine, float depth_range0, float normal_range0) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   DN_CHECK(half_passes >= -1 && half_passes <= 2000, "half_passes must be -1..2000");
   DN_CHECK(n_refine >= 0 && n_refine <= 12, "n_refine must be 0..12");
@@ -1491,6 +1534,7 @@ dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int 
   return DN_OK;
 }
 dn_status dn_batch_set_candidate_views(dn_batch* b, int mode) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   DN_CHECK(mode == 0 || mode == 1, "candidate view mode must be 0 (all views) or 1 (sample)");
   b->eng.sample_hp = mode;
@@ -1498,6 +1542,7 @@ dn_status dn_batch_set_candidate_views(dn_batch* b, int mode) {
   return DN_OK;
 }
 dn_status dn_batch_set_active_pixels(dn_batch* b, int on) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   b->eng.active = on ? 1 : 0;
   b->eng.invalidate();
@@ -1505,6 +1550,7 @@ dn_status dn_batch_set_active_pixels(dn_batch* b, int on) {
 }
 dn_status dn_batch_set_proposal_net(dn_batch* b, const uint16_t* weights, const float* biases,
                                     int n_planes, int stride) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   Engine& e = b->eng;
   DN_CUDA(cudaSetDevice(e.device));
@@ -1544,10 +1590,12 @@ dn_status dn_batch_set_proposal_net(dn_batch* b, const uint16_t* weights, const 
   return DN_OK;
 }
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   return b->eng.set_init(map_id, planes);
 }
 dn_status dn_batch_run(dn_batch* b, unsigned flags) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   Engine& e = b->eng;
   DN_CUDA(cudaSetDevice(e.device));
@@ -1606,21 +1654,25 @@ dn_status dn_batch_run(dn_batch* b, unsigned flags) {
   return DN_OK;
 }
 dn_status dn_batch_synchronize(dn_batch* b) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   DN_CUDA(cudaSetDevice(b->eng.device));
   return b->eng.finish();
 }
 dn_status dn_batch_get_depthmap(dn_batch* b, int map_id, float* depth, float* plane,
                                 float* score, int32_t* nghbr, float* clean) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   return b->eng.fetch(map_id, depth, plane, score, nghbr, clean);
 }
 dn_status dn_batch_get_depths(dn_batch* b, int n, const int* map_ids, float* const* depths,
                               int clean) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   return b->eng.fetch_depths(n, map_ids, depths, clean);
 }
 dn_status dn_batch_pruned_count(dn_batch* b, int64_t* count) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b && count, "NULL argument");
   Engine& e = b->eng;
   DN_CHECK(e.d_prune_counts.p, "no pruner run yet (DN_RUN_PRUNE)");
@@ -1635,6 +1687,7 @@ dn_status dn_batch_pruned_count(dn_batch* b, int64_t* count) {
 }
 dn_status dn_batch_get_points(dn_batch* b, int map_id, float* points, float* normals,
                               uint8_t* colors, uint8_t* labels, int64_t capacity, int64_t* count) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b && count, "NULL argument");
   Engine& e = b->eng;
   DN_CHECK(map_id >= 0 && map_id < (int)e.maps.size(), "depthmap id out of range");
@@ -1656,14 +1709,17 @@ dn_status dn_batch_get_points(dn_batch* b, int map_id, float* points, float* nor
   return DN_OK;
 }
 dn_status dn_batch_last_taps(dn_batch* b, uint64_t* taps) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   return b->eng.taps(taps);
 }
 dn_status dn_batch_set_view_image(dn_batch* b, int view_id, const uint8_t* image, int stride) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   return b->eng.set_view_image(view_id, image, stride);
 }
 dn_status dn_batch_last_timings(dn_batch* b, float* out, int n, uint64_t* taps_out) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   return b->eng.timings(out, n, taps_out);
 }
@@ -1685,14 +1741,17 @@ static dn_status set_tuning(Engine& e, int bx, int by, int variant) {
   return DN_OK;
 }
 dn_status dn_batch_set_tuning(dn_batch* b, int bx, int by, int variant) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   return set_tuning(b->eng, bx, by, variant);
 }
 dn_status dn_estimator_set_tuning(dn_estimator* est, int bx, int by, int variant) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(est, "NULL estimator");
   return set_tuning(est->eng, bx, by, variant);
 }
 dn_status dn_batch_timer_record(dn_batch* b, int slot) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   DN_CHECK(slot == 0 || slot == 1, "timer slot must be 0 or 1");
   DN_CUDA(cudaSetDevice(b->eng.device));
@@ -1700,6 +1759,7 @@ dn_status dn_batch_timer_record(dn_batch* b, int slot) {
   return DN_OK;
 }
 dn_status dn_batch_timer_elapsed(dn_batch* b, float* ms) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b && ms, "NULL argument");
   DN_CUDA(cudaSetDevice(b->eng.device));
   DN_CUDA(cudaEventSynchronize(b->eng.ev[6]));
@@ -1707,6 +1767,7 @@ dn_status dn_batch_timer_elapsed(dn_batch* b, float* ms) {
   return DN_OK;
 }
 dn_status dn_batch_copy_depth_device(dn_batch* b, int map_id, float* d_out) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   DN_CHECK(d_out, "NULL output");
   Engine& e = b->eng;
@@ -1721,6 +1782,7 @@ dn_status dn_batch_copy_depth_device(dn_batch* b, int map_id, float* d_out) {
 
 dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, int n_planes,
                                   int stride) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b && feat, "NULL argument");
   DN_CHECK(n_planes >= 1 && n_planes <= 8, "n_planes must be 1..8");
   DN_CHECK(stride == 1 || stride == 2, "stride must be 1 or 2");
@@ -1756,6 +1818,7 @@ dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, i
 }
 dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float min_score,
                            int stride) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b && target, "NULL argument");
   DN_CHECK(stride == 1 || stride == 2, "stride must be 1 or 2");
   Engine& e = b->eng;
@@ -1772,6 +1835,7 @@ dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float
   return DN_OK;
 }
 dn_status dn_batch_init_from_output(dn_batch* b, int map_id, const float* out) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(b && out, "NULL argument");
   Engine& e = b->eng;
   DN_CHECK(map_id >= 0 && map_id < (int)e.maps.size(), "depthmap id out of range");
@@ -1815,15 +1879,18 @@ static dn_status nn_forward(cudaError_t (*fn)(const dn::ConvArgs&, cudaStream_t)
 dn_status dn_nn_conv3x3_forward(const void* x, const void* w, const float* bias, int64_t n_pix,
                                 int H, int W, int cin, int cout, int relu, void* y, float* y32,
                                 void* stream) {
+  const dn::DeviceRestore device_restore_;
   return nn_forward(dn::conv3x3_forward, x, w, bias, n_pix, H, W, cin, cout, relu, y, y32, stream);
 }
 dn_status dn_nn_conv3x3_forward_mma_sync(const void* x, const void* w, const float* bias,
                                          int64_t n_pix, int H, int W, int cin, int cout, int relu,
                                          void* y, float* y32, void* stream) {
+  const dn::DeviceRestore device_restore_;
   return nn_forward(dn::conv3x3_forward_mma_sync, x, w, bias, n_pix, H, W, cin, cout, relu, y, y32,
                     stream);
 }
 dn_status dn_nn_synchronize(void* stream) {
+  const dn::DeviceRestore device_restore_;
   DN_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
   const int e = dn::take_tc_error();
   DN_CHECK(e >= 0, "could not read the tensor-core error word");
@@ -1837,6 +1904,7 @@ dn_status dn_nn_conv3x3_backward(const void* dy, const void* x, const void* w,
                                  const void* x_mask, int64_t n_pix, int H, int W, int cin,
                                  int cout, void* dx, float* dw, float* db, void* wt_scratch,
                                  void* stream) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(dy && x && w && dw && db && wt_scratch, "NULL argument");
   DN_CHECK(nn_shape_ok(cin, cout), "supported shapes: cin 32, cout 32 or 4");
   DN_CHECK(H > 0 && W > 0 && n_pix > 0 && n_pix % ((int64_t)H * W) == 0, "bad n_pix / H / W");
@@ -1860,6 +1928,7 @@ dn_status dn_nn_conv3x3_backward(const void* dy, const void* x, const void* w,
 dn_status dn_nn_l1_loss(const float* pred, const float* target, int64_t n_pix,
                         float normal_weight, void* dpred, float* loss_sum, float* count,
                         void* stream) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(pred && target && dpred && loss_sum && count && n_pix > 0, "bad argument");
   DN_CUDA(dn::launch_l1_loss(pred, target, n_pix, normal_weight,
                              static_cast<__nv_bfloat16*>(dpred), loss_sum, count,
@@ -1869,6 +1938,7 @@ dn_status dn_nn_l1_loss(const float* pred, const float* target, int64_t n_pix,
 dn_status dn_nn_adam(float* w, float* m, float* v, const float* grad, int n, const float* count,
                      float lr, float beta1, float beta2, float eps, float bc1, float bc2,
                      void* w16, void* stream) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(w && m && v && grad && count && n > 0, "bad argument");
   DN_CUDA(dn::launch_adam(w, m, v, grad, n, count, lr, beta1, beta2, eps, bc1, bc2,
                           static_cast<__nv_bfloat16*>(w16), static_cast<cudaStream_t>(stream)));
@@ -1876,6 +1946,7 @@ dn_status dn_nn_adam(float* w, float* m, float* v, const float* grad, int n, con
 }
 
 dn_status dn_postprocess_depth(const float* depth, float* out, int width, int height) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(depth && out, "NULL buffer");
   DN_CHECK(width >= 1 && height >= 1 && width <= 16384 && height <= 16384, "bad size");
   DN_TRY(need_device());
@@ -1890,6 +1961,7 @@ dn_status dn_postprocess_depth(const float* depth, float* out, int width, int he
 }
 
 dn_status dn_fp32_peak(double* tflops, double* ms) {
+  const dn::DeviceRestore device_restore_;
   DN_CHECK(tflops && ms, "NULL output");
   DN_TRY(need_device());
   DN_CUDA(dn::fp32_peak(tflops, ms));

@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "dense_b200.h"
+#include "device_guard.h"
 
 namespace {
 
@@ -598,6 +599,7 @@ struct dn_fuser {
 extern "C" const char* dn_fuser_last_error(void) { return g_fuse_error.c_str(); }
 
 extern "C" dn_status dn_fuser_create(dn_fuser** out) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(out, "NULL output");
   *out = nullptr;
   int n = 0;
@@ -610,35 +612,42 @@ extern "C" dn_status dn_fuser_create(dn_fuser** out) {
   return DN_OK;
 }
 extern "C" dn_status dn_fuser_destroy(dn_fuser* f) {
+  const dn::DeviceRestore device_restore_;
   delete f;
   return DN_OK;
 }
 extern "C" dn_status dn_fuser_set_min_num_consistent(dn_fuser* f, int n) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f, "NULL fuser");
   f->min_num_consistent = n;
   return DN_OK;
 }
 extern "C" dn_status dn_fuser_set_max_reproj_error(dn_fuser* f, float px) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f, "NULL fuser");
   f->max_reproj_error_sq = px * px;  // fuser.cc:57-59
   return DN_OK;
 }
 extern "C" dn_status dn_fuser_set_max_depth_error(dn_fuser* f, float ratio) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f, "NULL fuser");
   f->max_depth_error = ratio;
   return DN_OK;
 }
 extern "C" dn_status dn_fuser_set_max_normal_error(dn_fuser* f, float degrees) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f, "NULL fuser");
   f->max_normal_deg = degrees;
   return DN_OK;
 }
 extern "C" dn_status dn_fuser_set_border_margin(dn_fuser* f, int px) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f, "NULL fuser");
   f->border = std::max(0, px);  // fuser.cc:67-69
   return DN_OK;
 }
 extern "C" dn_status dn_fuser_set_sor_params(dn_fuser* f, int knn, float stddev_factor) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f, "NULL fuser");
   FCHECK(knn <= kSorMaxK, "knn above 64 is not supported");
   f->sor_knn = std::max(0, knn);  // knn <= 0 skips the step, as the reference does
@@ -646,6 +655,7 @@ extern "C" dn_status dn_fuser_set_sor_params(dn_fuser* f, int knn, float stddev_
   return DN_OK;
 }
 extern "C" dn_status dn_fuser_set_behind_depth_factor(dn_fuser* f, float factor) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f, "NULL fuser");
   f->behind = std::min(1.0f, std::max(0.0f, factor));  // fuser.cc:78-80
   return DN_OK;
@@ -656,6 +666,7 @@ extern "C" dn_status dn_fuser_add_view(dn_fuser* f, const double* K, const doubl
                                        const uint8_t* color, const uint8_t* mask, int width,
                                        int height, const int* neighbor_ids, int n_neighbors,
                                        int primary) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f, "NULL fuser");
   FCHECK(K && R && t && depth && normal && color, "NULL argument");
   FCHECK(width >= 1 && height >= 1 && width <= 16384 && height <= 16384, "bad depthmap size");
@@ -838,6 +849,7 @@ static dn_status run_sor(dn_fuser* f) {
 
 extern "C" dn_status dn_sor_filter(const float* points, int64_t n, int knn, float stddev_factor,
                                    uint8_t* keep, float* mean_knn) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(n >= 0 && (n == 0 || points) && (n == 0 || keep), "NULL argument");
   FCHECK(knn <= kSorMaxK, "knn above 64 is not supported");
   if (knn <= 0 || n <= (int64_t)knn + 1) {
@@ -863,12 +875,14 @@ extern "C" dn_status dn_sor_filter(const float* points, int64_t n, int knn, floa
 }
 
 extern "C" dn_status dn_fuser_last_removal_ms(dn_fuser* f, float* ms) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f && ms, "NULL argument");
   *ms = f->sor_ms;
   return DN_OK;
 }
 
 extern "C" dn_status dn_fuser_fuse(dn_fuser* f, int64_t* count) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f && count, "NULL argument");
   *count = 0;
   f->out_pts.clear();
@@ -1079,6 +1093,7 @@ extern "C" dn_status dn_fuser_fuse(dn_fuser* f, int64_t* count) {
 
 extern "C" dn_status dn_fuser_get(dn_fuser* f, float* points, float* normals, uint8_t* colors,
                                   int64_t capacity) {
+  const dn::DeviceRestore device_restore_;
   FCHECK(f, "NULL fuser");
   const int64_t n = (int64_t)(f->out_pts.size() / 3);
   FCHECK(capacity >= n, "capacity below the fused point count");

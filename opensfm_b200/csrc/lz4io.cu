@@ -34,6 +34,7 @@ thread_local std::string g_io_error;
 thread_local std::vector<uint8_t> g_last_out;
 thread_local const void* g_last_src = nullptr;
 thread_local int64_t g_last_n = -1;
+thread_local uint32_t g_last_hash = 0;  // xxh32 of the cached input
 
 dn_status io_fail(dn_status s, const char* m) {
   g_io_error = m;
@@ -312,12 +313,17 @@ extern "C" dn_status dn_lz4f_compress(const void* src, int64_t n, void* dst, int
 extern "C" dn_status dn_lz4f_decompress(const void* src, int64_t n, void* dst, int64_t capacity,
                                         int64_t* out_len) {
   if (!src || n <= 0 || !out_len) return io_fail(DN_INVALID_ARG, "NULL or empty input");
-  if (src != g_last_src || n != g_last_n) {
+  // A size query keeps its decoded output for the fetch that follows; the
+  // cache is reused only for the same pointer, length and input bytes (the
+  // caller may have put another frame of the same length at that address).
+  const uint32_t hash = xxh32(static_cast<const uint8_t*>(src), (size_t)n, 0);
+  if (src != g_last_src || n != g_last_n || hash != g_last_hash) {
     g_last_src = nullptr;
     const dn_status st = decode_frames(static_cast<const uint8_t*>(src), (size_t)n, g_last_out);
     if (st != DN_OK) return st;
     g_last_src = src;
     g_last_n = n;
+    g_last_hash = hash;
   }
   *out_len = (int64_t)g_last_out.size();
   if (!dst) return DN_OK;

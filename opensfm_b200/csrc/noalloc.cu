@@ -22,6 +22,7 @@
 //    before any stream capture on the device.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <mutex>
 #include <string>
 
@@ -41,6 +42,35 @@ constexpr size_t kNoAllocScratchBytes =
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 static __device__ __align__(256) dn::PruneView g_noalloc_views[kNoAllocMaxViews];
+
+// The view table travels as a kernel argument (17 x 224 bytes, inside the
+// 4 KB parameter space) and one block writes it into g_noalloc_views, in
+// stream order: no host buffer has to outlive the call, and no copy from
+// pageable host memory waits for the stream's earlier work.
+struct NoAllocTable {
+  dn::PruneView v[kNoAllocMaxViews];
+};
+static_assert(sizeof(NoAllocTable) + 16 <= 4096, "view table must fit the kernel parameters");
+
+__global__ void install_views_kernel(NoAllocTable table, int n) {
+  const int k = threadIdx.x;
+  if (k < n) g_noalloc_views[k] = table.v[k];
+}
+
+bool finite_all(const double* a, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!std::isfinite(a[i])) return false;
+  return true;
+}
+
+// The checks dn_pruner_add_view makes: finite K, R, t and an invertible K.
+bool camera_ok(const dn_prune_view& v) {
+  if (!finite_all(v.K, 9) || !finite_all(v.R, 9) || !finite_all(v.t, 3)) return false;
+  const double* a = v.K;
+  const double det = a[0] * (a[4] * a[8] - a[7] * a[5]) - a[1] * (a[3] * a[8] - a[6] * a[5]) +
+                     a[2] * (a[3] * a[7] - a[6] * a[4]);
+  return det != 0.0 && std::isfinite(det);
+}
 
 constexpr int kMaxDevices = 64;
 struct DeviceAddrs {
@@ -80,8 +110,10 @@ extern "C" dn_status dn_prune_noalloc(const dn_prune_view* views, int n_views,
     return fail(DN_INVALID_ARG, "output capacity must be at least width * height points");
   for (int k = 0; k < n_views; ++k) {
     const dn_prune_view& v = views[k];
-    if (!v.depth || !v.plane || !v.color || !v.label || v.width < 1 || v.height < 1)
-      return fail(DN_INVALID_ARG, "view with NULL buffer or bad size");
+    if (!v.depth || !v.plane || !v.color || !v.label || v.width < 1 || v.height < 1 ||
+        v.width > 16384 || v.height > 16384)
+      return fail(DN_INVALID_ARG, "view with NULL buffer or a size outside 1..16384");
+    if (!camera_ok(v)) return fail(DN_INVALID_ARG, "camera K, R, t must be finite, K invertible");
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -102,7 +134,7 @@ extern "C" dn_status dn_prune_noalloc(const dn_prune_view* views, int n_views,
     }
     addrs = g_addrs[dev];
   }
-  dn::PruneView table[kNoAllocMaxViews];
+  NoAllocTable table{};
   for (int k = 0; k < n_views; ++k) {
     const dn_prune_view& v = views[k];
     dn::PruneView p{};
@@ -118,11 +150,11 @@ extern "C" dn_status dn_prune_noalloc(const dn_prune_view* views, int n_views,
       p.R[i] = v.R[i];
     }
     for (int i = 0; i < 3; ++i) p.t[i] = v.t[i];
-    table[k] = p;
+    table.v[k] = p;
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  e = cudaMemcpyAsync(addrs.views, table, n_views * sizeof(dn::PruneView), cudaMemcpyHostToDevice,
-                      s);
+  install_views_kernel<<<1, 32, 0, s>>>(table, n_views);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return fail(DN_DEVICE_ERROR, cudaGetErrorString(e));
   dn::PruneOut out{points, normals, colors, labels};
   e = dn::launch_prune(addrs.views, n_views, W, H, same_depth_threshold, addrs.scratch, out, count,

@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "dense_b200.h"
+#include "device_guard.h"
 
 namespace {
 
@@ -466,6 +467,7 @@ dn_status upload_views(dn_svo* f, DBuf<SvoViewDev>& d_views, int* max_w, int* ma
 extern "C" const char* dn_svo_last_error(void) { return g_svo_error.c_str(); }
 
 extern "C" dn_status dn_svo_create(dn_svo** out) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(out, "NULL output");
   *out = nullptr;
   int n = 0;
@@ -477,26 +479,31 @@ extern "C" dn_status dn_svo_create(dn_svo** out) {
   return DN_OK;
 }
 extern "C" dn_status dn_svo_destroy(dn_svo* f) {
+  const dn::DeviceRestore device_restore_;
   if (f) cudaSetDevice(f->device);
   delete f;
   return DN_OK;
 }
 extern "C" dn_status dn_svo_set_voxel_size(dn_svo* f, float size) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f, "NULL fuser");
   f->voxel_size = std::max(1e-6f, size);  // svo_fuser.cc:15
   return DN_OK;
 }
 extern "C" dn_status dn_svo_set_trunc_factor(dn_svo* f, float factor) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f, "NULL fuser");
   f->trunc_factor = std::max(1.0f, factor);  // svo_fuser.cc:17-19
   return DN_OK;
 }
 extern "C" dn_status dn_svo_set_min_weight(dn_svo* f, float w) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f, "NULL fuser");
   f->min_weight = std::max(0.0f, w);  // svo_fuser.cc:21
   return DN_OK;
 }
 extern "C" dn_status dn_svo_set_device(dn_svo* f, int device) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f, "NULL fuser");
   SCHECK(f->views.empty(), "set_device must come before add_view");
   int n = 0;
@@ -513,6 +520,7 @@ extern "C" dn_status dn_svo_set_device(dn_svo* f, int device) {
 }
 extern "C" dn_status dn_svo_set_bbox(dn_svo* f, const float min_world[3],
                                      const float max_world[3]) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f && min_world && max_world, "NULL argument");
   f->has_bbox = true;
   for (int i = 0; i < 3; ++i) {
@@ -526,6 +534,7 @@ extern "C" dn_status dn_svo_add_view(dn_svo* f, const double* K, const double* R
                                      const double* t, const float* depth, const float* normal,
                                      const uint8_t* color, const uint8_t* mask,
                                      const float* weight, int width, int height) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f, "NULL fuser");
   SCHECK(K && R && t && depth, "NULL argument");
   SCHECK(width >= 1 && height >= 1 && width <= 16384 && height <= 16384, "bad depthmap size");
@@ -593,6 +602,7 @@ static dn_status march(dn_svo* f, bool counting, const DBuf<SvoViewDev>& d_views
 }
 
 extern "C" dn_status dn_svo_count_voxels(dn_svo* f, uint32_t* count) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f && count, "NULL argument");
   *count = 0;
   if (f->views.empty()) return DN_OK;  // svo_fuser.cc:53-55
@@ -639,6 +649,7 @@ extern "C" dn_status dn_svo_count_voxels(dn_svo* f, uint32_t* count) {
 }
 
 extern "C" dn_status dn_svo_fuse(dn_svo* f, int64_t* count) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f && count, "NULL argument");
   *count = 0;
   f->out_pts.clear();
@@ -774,6 +785,7 @@ extern "C" dn_status dn_svo_fuse(dn_svo* f, int64_t* count) {
 
 extern "C" dn_status dn_svo_get(dn_svo* f, float* points, float* normals, uint8_t* colors,
                                 int64_t capacity) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f, "NULL fuser");
   const int64_t n = (int64_t)(f->out_pts.size() / 3);
   SCHECK(capacity >= n, "capacity below the fused point count");
@@ -784,6 +796,7 @@ extern "C" dn_status dn_svo_get(dn_svo* f, float* points, float* normals, uint8_
 }
 
 extern "C" dn_status dn_svo_last_fuse_ms(dn_svo* f, float* ms) {
+  const dn::DeviceRestore device_restore_;
   SCHECK(f && ms, "NULL argument");
   *ms = f->fuse_ms;
   return DN_OK;

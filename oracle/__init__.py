@@ -18,7 +18,7 @@ The oracles:
 ``ref``
     The reference's own ``depthmap.cc`` compiled unmodified against the
     project's OpenCV shim (``oracle/Makefile`` -> ``oracle/_ref/``), driven
-    through ``ref_capi.cc``.  Present wherever ``/root/reference`` was
+    through ``ref_capi.cc``.  Present wherever the reference's sources were
     available when ``make`` ran; ``ref_available()`` says whether it is.
 ``ncc_fp64``
     A numpy float64 restatement of ``ComputePlaneImageScore``
@@ -36,7 +36,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libdepthmap_ref.so")
-REF_DENSE = "/root/reference/opensfm/src/lib/dense"
+# The reference checkout: $OPENSFM_REFERENCE, else a "reference" folder beside
+# this repository.
+REF_ROOT = os.environ.get("OPENSFM_REFERENCE",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+REF_DENSE = os.path.join(REF_ROOT, "opensfm", "src", "lib", "dense")
 
 _port = None
 _ref = None
