@@ -202,19 +202,22 @@ dn_status dn_batch_get_depths(dn_batch* b, int n, const int* map_ids, float* con
  * (depthmap.cc:305-374). */
 dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int use_far,
                                 int n_refine, float depth_range0, float normal_range0);
-/* Views scored per PatchMatch candidate in the half-passes (no reference
- * counterpart as a switch): mode 0 scores every matching view and keeps the
- * maximum (ComputePlaneScore, depthmap.cc:408-419); mode 1 scores one view
- * per candidate -- the view the candidate's source pixel found best, the
+/* Views scored per PatchMatch candidate (no reference counterpart as a
+ * switch): mode 0 scores every matching view and keeps the maximum
+ * (ComputePlaneScore, depthmap.cc:408-419), as ComputePatchMatch does; mode
+ * 1 initialises with every view, then the half-passes score one view per
+ * candidate -- the view the candidate's source pixel found best, the
  * current view for refinements -- plus one random other view of the
- * current plane per update, as ComputePatchMatchSample does
- * (depthmap.cc:215-227, 305-374). */
+ * current plane per update; mode 2 is ComputePatchMatchSample
+ * (depthmap.cc:215-227, 305-374): a random view at the initialisation, then
+ * as mode 1. */
 dn_status dn_batch_set_candidate_views(dn_batch* b, int mode);
 /* Active pixels (no reference counterpart): with on = 1, from the third
- * half-pass of a run on, a pixel is updated only if its own plane or one of
- * its 4 neighbours' planes changed at their last update; the others keep
- * their state. */
-dn_status dn_batch_set_active_pixels(dn_batch* b, int on);
+ * half-pass of a run on, a pixel is updated only if its own depth or one of
+ * its 4 neighbours' depths moved at their last update -- by more than
+ * min_change relative, or, with min_change = 0, any change of the plane;
+ * the others keep their state. */
+dn_status dn_batch_set_active_pixels(dn_batch* b, int on, float min_change);
 /* Initial planes (f32 [H][W][3], reference camera) for one depthmap. */
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes);
 /* Total kept pruner points over all maps of the last run (after sync). */

@@ -19,7 +19,7 @@ SOURCES = ["kernels.cu", "cleanprune.cu", "learned.cu", "api.cu", "noalloc.cu", 
 # contraction (every operation rounded by itself, as its C oracle, apart
 # from the fused multiply-adds its source writes out).
 FILE_FLAGS = {"acmmp.cu": ["--fmad=false"]}
-HEADERS = ["common.cuh", "kernels.h", "learned.h", "device_guard.h"]
+HEADERS = ["common.cuh", "kernels.h", "learned.h", "device_guard.h", "cleanprune.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",

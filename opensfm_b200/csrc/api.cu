@@ -205,6 +205,7 @@ struct Engine {
   float depth_range0 = 0.02f, normal_range0 = 0.5f;
   int sample_hp = 0;  // half-passes score one view per candidate (sample mode)
   int active = 0;     // active-pixel half-passes
+  float active_tol = 0.f;
   // Learned proposal (DN_RUN_LEARNED): network weights, the feature grid of
   // every map (maps of one grid size contiguous, one network launch per
   // size), activations and outputs.
@@ -516,7 +517,7 @@ struct Engine {
     n_tiles_init = (int)ti.size();
     // Counters of the persistent launch (allocated here, outside any capture).
     const int n_half = half_passes >= 0 ? half_passes : 2 * iterations;
-    DN_CUDA(d_sync.alloc(4 + std::max(n_half, 0)));
+    DN_CUDA(d_sync.alloc(dn::kPersistentCounters + std::max(n_half, 0)));
     dirty = false;
     return DN_OK;
   }
@@ -546,6 +547,7 @@ struct Engine {
     a.p.depth_range0 = depth_range0;
     a.p.normal_range0 = normal_range0;
     a.p.active = active;
+    a.p.active_tol = active_tol;
     return a;
   }
 
@@ -588,7 +590,13 @@ struct Engine {
   }
 
   // Enqueues the whole computation for every map on `stream`.
-  dn_status enqueue(Mode mode, bool timing = false, bool learned = false) {
+  // With the persistent launch the cleaner (with_clean) and the pruner
+  // (with_prune) run inside it and tail_done is set; otherwise the caller
+  // enqueues them after.
+  bool tail_done = false;
+  dn_status enqueue(Mode mode, bool timing = false, bool learned = false, bool with_clean = false,
+                    bool with_prune = false) {
+    tail_done = false;
     for (auto& m : maps) {
       const View& r = *views[m->ref];
       const size_t npx = (size_t)r.W * r.H;
@@ -619,14 +627,16 @@ struct Engine {
       DN_CUDA(dn::launch_stage(dn::Stage::kPostProcess, false, a1, stream));
       return DN_OK;
     }
-    const bool sample = (mode == Mode::kPatchMatchSample);
-    // Half-passes in sample mode: the mode itself, or one view per candidate
-    // after a full initialisation (dn_batch_set_candidate_views).
+    // Sample mode (ComputePatchMatchSample): the mode itself, or candidate
+    // view mode 2; mode 1 keeps the full initialisation and scores one view
+    // per candidate in the half-passes (dn_batch_set_candidate_views).
+    const bool sample = (mode == Mode::kPatchMatchSample) || sample_hp == 2;
     const bool sample_half = sample || sample_hp;
     const int hp = half_passes >= 0 ? half_passes : 2 * iterations;
     if (persistent && !sample_half && patch == 7) {
-      DN_CHECK(d_sync.p && d_sync.n >= (size_t)(4 + hp), "persistent launch buffers not prepared");
-      DN_CUDA(cudaMemsetAsync(d_sync.p, 0, (4 + hp) * sizeof(unsigned), stream));
+      const int n_sync = dn::kPersistentCounters + hp;
+      DN_CHECK(d_sync.p && d_sync.n >= (size_t)n_sync, "persistent launch buffers not prepared");
+      DN_CUDA(cudaMemsetAsync(d_sync.p, 0, n_sync * sizeof(unsigned), stream));
       dn::PersistentArgs pa{};
       pa.base = a1;
       pa.tiles_init = d_tiles_init.p;
@@ -638,6 +648,22 @@ struct Engine {
       pa.n_half = hp;
       pa.sync = d_sync.p;
       pa.base.p.taps = d_taps.p + 1;
+      if (with_clean) {
+        pa.tail.clean_views = d_clean_views.p;
+        pa.tail.cmaps = d_clean_maps.p;
+        pa.tail.lists = d_clean_lists.p;
+        pa.tail.clean_tiles = d_clean_tiles.p;
+        pa.tail.n_clean = n_clean_tiles;
+        pa.tail.min_views = min_consistent;
+        pa.tail.thr = same_depth_thr;
+      }
+      if (with_clean && with_prune) {
+        pa.tail.pmaps = d_prune_maps.p;
+        pa.tail.n_pmaps = (int)maps.size();
+        pa.tail.prune_tiles = d_prune_tiles.p;
+        pa.tail.n_prune = n_prune_tiles;
+      }
+      tail_done = with_clean;
       DN_CUDA(dn::launch_persistent(pa, stream));
       DN_TRY(mark(1, timing));
       DN_TRY(mark(2, timing));
@@ -668,11 +694,11 @@ struct Engine {
   // Uploads the cleaner tables (outside any stream capture): one CleanView
   // per map (its final depth with its reference camera) and per map the
   // list of other maps it is checked against.
-  std::vector<int> clean_offs;
   dn_status prepare_clean() {
     std::vector<dn::CleanView> cv(maps.size());
+    std::vector<dn::CleanMap> cmaps;
+    std::vector<int4> tiles;
     std::vector<int> lists;
-    clean_offs.clear();
     for (size_t k = 0; k < maps.size(); ++k) {
       Map& m = *maps[k];
       const View& r = *views[m.ref];
@@ -686,25 +712,47 @@ struct Engine {
       std::memcpy(c.R, r.cam.R, sizeof(c.R));
       std::memcpy(c.t, r.cam.t, sizeof(c.t));
       cv[k] = c;
-      clean_offs.push_back((int)lists.size());
+      dn::CleanMap cm{};
+      cm.list_off = (int)lists.size();
+      cm.n = (int)m.clean_maps.size();
+      cm.out = m.clean.p;
+      cmaps.push_back(cm);
       for (int o : m.clean_maps) lists.push_back(o);
+      for (int y = 0; y < (r.H + dn::kCleanTileY - 1) / dn::kCleanTileY; ++y)
+        for (int x = 0; x < (r.W + dn::kCleanTileX - 1) / dn::kCleanTileX; ++x)
+          tiles.push_back(make_int4((int)k, x, y, 0));
     }
     DN_CUDA(d_clean_views.alloc(std::max<size_t>(cv.size(), 1)));
     DN_CUDA(d_clean_lists.alloc(std::max<size_t>(lists.size(), 1)));
+    DN_CUDA(d_clean_maps.alloc(std::max<size_t>(cmaps.size(), 1)));
+    DN_CUDA(d_clean_tiles.alloc(std::max<size_t>(tiles.size(), 1)));
     DN_CUDA(cudaMemcpyAsync(d_clean_views.p, cv.data(), cv.size() * sizeof(dn::CleanView),
                             cudaMemcpyHostToDevice, stream));
     if (!lists.empty())
       DN_CUDA(cudaMemcpyAsync(d_clean_lists.p, lists.data(), lists.size() * sizeof(int),
                               cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaMemcpyAsync(d_clean_maps.p, cmaps.data(), cmaps.size() * sizeof(dn::CleanMap),
+                            cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaMemcpyAsync(d_clean_tiles.p, tiles.data(), tiles.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, stream));
+    n_clean_tiles = (int)tiles.size();
     DN_CUDA(cudaStreamSynchronize(stream));
     return DN_OK;
   }
+  DevBuf<dn::CleanMap> d_clean_maps;
+  DevBuf<int4> d_clean_tiles;
+  int n_clean_tiles = 0;
 
   // Pruner tables and buffers (outside any stream capture): per map the
   // cleaned depth and PatchMatch planes of the map and its cleaner maps.
   DevBuf<unsigned long long> d_prune_counts;
+  DevBuf<dn::PruneMap> d_prune_maps;
+  DevBuf<int4> d_prune_tiles;
+  int n_prune_tiles = 0;
   dn_status prepare_prune() {
     DN_CUDA(d_prune_counts.alloc(std::max<size_t>(maps.size(), 1)));
+    std::vector<dn::PruneMap> pmaps;
+    std::vector<int4> tiles;
     for (size_t k = 0; k < maps.size(); ++k) {
       Map& m = *maps[k];
       const View& r = *views[m.ref];
@@ -730,37 +778,44 @@ struct Engine {
         pv.push_back(v);
       }
       DN_CUDA(m.prune_views.alloc(pv.size()));
-      DN_CUDA(m.prune_scratch.alloc(dn::prune_scratch_bytes(r.W, r.H)));
+      DN_CUDA(m.prune_scratch.alloc(dn::prune_batch_scratch_bytes(r.W, r.H)));
       DN_CUDA(m.prune_points.alloc(3 * npx));
       DN_CUDA(m.prune_normals.alloc(3 * npx));
       DN_CUDA(m.prune_colors.alloc(3 * npx));
       DN_CUDA(m.prune_labels.alloc(npx));
       DN_CUDA(cudaMemcpyAsync(m.prune_views.p, pv.data(), pv.size() * sizeof(dn::PruneView),
                               cudaMemcpyHostToDevice, stream));
+      const dn::PruneOut o{m.prune_points.p, m.prune_normals.p, m.prune_colors.p,
+                           m.prune_labels.p};
+      pmaps.push_back(dn::prune_batch_map(m.prune_views.p, (int)pv.size(), r.W, r.H,
+                                          m.prune_scratch.p, o, d_prune_counts.p + k));
+      for (int blk = 0; blk < pmaps.back().blocks; ++blk)
+        tiles.push_back(make_int4((int)k, blk, 0, 0));
     }
+    DN_CUDA(d_prune_maps.alloc(std::max<size_t>(pmaps.size(), 1)));
+    DN_CUDA(d_prune_tiles.alloc(std::max<size_t>(tiles.size(), 1)));
+    DN_CUDA(cudaMemcpyAsync(d_prune_maps.p, pmaps.data(), pmaps.size() * sizeof(dn::PruneMap),
+                            cudaMemcpyHostToDevice, stream));
+    DN_CUDA(cudaMemcpyAsync(d_prune_tiles.p, tiles.data(), tiles.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, stream));
+    n_prune_tiles = (int)tiles.size();
     DN_CUDA(cudaStreamSynchronize(stream));
     return DN_OK;
   }
+  // The pruner over every map in three launches (flags, per-map scans,
+  // ordered writes).
   dn_status enqueue_prune() {
-    for (size_t k = 0; k < maps.size(); ++k) {
-      Map& m = *maps[k];
-      const View& r = *views[m.ref];
-      dn::PruneOut o{m.prune_points.p, m.prune_normals.p, m.prune_colors.p, m.prune_labels.p};
-      DN_CUDA(dn::launch_prune(m.prune_views.p, 1 + (int)m.clean_maps.size(), r.W, r.H,
-                               same_depth_thr, m.prune_scratch.p, o, d_prune_counts.p + k, stream));
-    }
+    DN_CUDA(dn::launch_prune_batch(d_prune_maps.p, (int)maps.size(), d_prune_tiles.p,
+                                   n_prune_tiles, same_depth_thr, stream));
     DN_TRY(mark(4, timed));
     return DN_OK;
   }
 
+  // The cleaner over every map in one launch.
   dn_status enqueue_clean(bool timing = false) {
-    for (size_t k = 0; k < maps.size(); ++k) {
-      Map& m = *maps[k];
-      const View& r = *views[m.ref];
-      DN_CUDA(dn::launch_clean(d_clean_views.p, (int)k, d_clean_lists.p + clean_offs[k],
-                               (int)m.clean_maps.size(), r.W, r.H, same_depth_thr,
-                               min_consistent, m.clean.p, stream));
-    }
+    DN_CUDA(dn::launch_clean_batch(d_clean_views.p, d_clean_maps.p, d_clean_lists.p,
+                                   d_clean_tiles.p, n_clean_tiles, same_depth_thr, min_consistent,
+                                   stream));
     DN_TRY(mark(4, timing));
     return DN_OK;
   }
@@ -1536,15 +1591,18 @@ dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int 
 dn_status dn_batch_set_candidate_views(dn_batch* b, int mode) {
   const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
-  DN_CHECK(mode == 0 || mode == 1, "candidate view mode must be 0 (all views) or 1 (sample)");
+  DN_CHECK(mode >= 0 && mode <= 2,
+           "candidate view mode must be 0 (all views), 1 (sample half-passes) or 2 (sample)");
   b->eng.sample_hp = mode;
   b->eng.invalidate();
   return DN_OK;
 }
-dn_status dn_batch_set_active_pixels(dn_batch* b, int on) {
+dn_status dn_batch_set_active_pixels(dn_batch* b, int on, float min_change) {
   const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
+  DN_CHECK(min_change >= 0.f && min_change < 1.f, "min_change must be in [0, 1)");
   b->eng.active = on ? 1 : 0;
+  b->eng.active_tol = min_change;
   b->eng.invalidate();
   return DN_OK;
 }
@@ -1628,9 +1686,10 @@ dn_status dn_batch_run(dn_batch* b, unsigned flags) {
     if (flags & DN_RUN_PRUNE) DN_TRY(e.prepare_prune());
     cudaGraph_t g = nullptr;
     DN_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
-    dn_status s = e.enqueue(Mode::kPatchMatch, timing, learned);
-    if (s == DN_OK && (flags & DN_RUN_CLEAN)) s = e.enqueue_clean(timing);
-    if (s == DN_OK && (flags & DN_RUN_PRUNE)) s = e.enqueue_prune();
+    dn_status s = e.enqueue(Mode::kPatchMatch, timing, learned, (flags & DN_RUN_CLEAN) != 0,
+                            (flags & DN_RUN_PRUNE) != 0);
+    if (s == DN_OK && (flags & DN_RUN_CLEAN) && !e.tail_done) s = e.enqueue_clean(timing);
+    if (s == DN_OK && (flags & DN_RUN_PRUNE) && !e.tail_done) s = e.enqueue_prune();
     cudaError_t ce = cudaStreamEndCapture(e.stream, &g);
     if (s != DN_OK) {
       if (g) cudaGraphDestroy(g);
@@ -1645,9 +1704,10 @@ dn_status dn_batch_run(dn_batch* b, unsigned flags) {
   } else {
     if (flags & DN_RUN_CLEAN) DN_TRY(e.prepare_clean());
     if (flags & DN_RUN_PRUNE) DN_TRY(e.prepare_prune());
-    DN_TRY(e.enqueue(Mode::kPatchMatch, timing, learned));
-    if (flags & DN_RUN_CLEAN) DN_TRY(e.enqueue_clean(timing));
-    if (flags & DN_RUN_PRUNE) DN_TRY(e.enqueue_prune());
+    DN_TRY(e.enqueue(Mode::kPatchMatch, timing, learned, (flags & DN_RUN_CLEAN) != 0,
+                     (flags & DN_RUN_PRUNE) != 0));
+    if ((flags & DN_RUN_CLEAN) && !e.tail_done) DN_TRY(e.enqueue_clean(timing));
+    if ((flags & DN_RUN_PRUNE) && !e.tail_done) DN_TRY(e.enqueue_prune());
   }
   b->ran = true;
   e.computed = true;

@@ -87,9 +87,12 @@ struct RunParams {
   int use_near, use_far, n_refine;
   float depth_range0, normal_range0;
   // Active pixels: from half-pass 2 on, a pixel is updated only if its own
-  // plane or one of its 4 neighbours' planes changed at their last update
-  // (MapDev::changed); otherwise its state is kept as it is.
+  // depth or one of its 4 neighbours' depths moved at their last update
+  // (MapDev::changed); otherwise its state is kept as it is.  A depth moves
+  // when it changes by more than active_tol relative (active_tol = 0: any
+  // change of the plane counts).
   int active;
+  float active_tol;
   int learned;  // initialise from MapDev::prop_init instead of MapDev::init
 };
 

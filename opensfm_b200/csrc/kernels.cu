@@ -5,6 +5,7 @@
 // Every kernel works on a batch: blockIdx.x indexes a tile list of
 // (map, tile_x, tile_y) built on the host, so one launch covers every
 // depthmap of a reconstruction whatever their sizes.
+#include "cleanprune.cuh"
 #include "common.cuh"
 #include "kernels.h"
 
@@ -301,9 +302,6 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
   const int x0 = tl.y * (2 * px), y0 = tl.z * blockDim.y;
   const int pitch = 2 * px + 2 * HPZ, rows = blockDim.y + 2 * HPZ;
   __shared__ PairViewSm spv;
-  stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
-  stage_pairs(spv, m, views, pairs);
-  __syncthreads();
   const int g = threadIdx.x / L, lane = threadIdx.x % L;
   const unsigned mask = (L == 1) ? (1u << (threadIdx.x & 31))
                                  : (((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1)));
@@ -314,13 +312,21 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
   float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
   if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) st = m.state[pix];
   bool run = st.w != 0.0f;
-  if (run && p.active && p.pass >= 2) {
-    // Interior pixel, so the 4 neighbours are inside the map.  Their flags
-    // were written by the previous half-pass, the pixel's own by the one
-    // before; this half-pass writes only pixels of its own colour.
-    const uint8_t* ch = m.changed;
-    run = (ch[pix] | ch[pix - W] | ch[pix + W] | ch[pix - 1] | ch[pix + 1]) != 0;
+  if (p.active && p.pass >= 2) {
+    if (run) {
+      // Interior pixel, so the 4 neighbours are inside the map.  Their flags
+      // were written by the previous half-pass, the pixel's own by the one
+      // before; this half-pass writes only pixels of its own colour.
+      const uint8_t* ch = m.changed;
+      run = (ch[pix] | ch[pix - W] | ch[pix + W] | ch[pix - 1] | ch[pix + 1]) != 0;
+    }
+    // A tile without an active pixel leaves before staging (block-uniform:
+    // every thread of the block takes the same branch).
+    if (!__syncthreads_or(run)) return;
   }
+  stage_tile<HPZ>(tile, pitch, rows, rv.img, W, H, y0, x0);
+  stage_pairs(spv, m, views, pairs);
+  __syncthreads();
   if (run) {
     Patch<HPZ, L> pt;
     pt.build(tile, pitch, threadIdx.y + HPZ, (j - x0) + HPZ, lane, mask);
@@ -432,7 +438,12 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
       m.state[pix] = make_float4(cv.x, cv.y, cv.z, cd);
       m.score[pix] = cur;
       m.nghbr[pix] = curn;
-      if (p.active) m.changed[pix] = same_plane(cv, make_float3(st.x, st.y, st.z)) ? 0 : 1;
+      if (p.active) {
+        const bool moved = p.active_tol > 0.0f
+                               ? fabsf(cd - st.w) > p.active_tol * st.w
+                               : !same_plane(cv, make_float3(st.x, st.y, st.z));
+        m.changed[pix] = moved ? 1 : 0;
+      }
     }
   }
   // A skipped pixel's own flag is 0 already (it was part of the test).
@@ -559,7 +570,7 @@ patchmatch_persistent_kernel(const MapDev* __restrict__ maps, const ViewDev* __r
                              const int4* __restrict__ tiles_init, int n_init,
                              const int4* __restrict__ tiles_hp, int n_hp,
                              const int4* __restrict__ tiles_post, int n_post, int n_half,
-                             RunParams p, unsigned* sync) {
+                             RunParams p, unsigned* sync, const PersistentTail tail) {
   const unsigned nb = gridDim.x;
   for (int t = next_tile(sync + 2); t < n_init; t = next_tile(sync + 2))
     init_tile<HPZ, false, L>(maps, views, pairs, tiles_init[t], p);
@@ -576,6 +587,38 @@ patchmatch_persistent_kernel(const MapDev* __restrict__ maps, const ViewDev* __r
   // The post-process tiles are bx x by pixels of 32 x 4 threads.
   unsigned* ctr = sync + 3 + n_half;
   for (int t = next_tile(ctr); t < n_post; t = next_tile(ctr)) post_tile(maps, tiles_post[t], 1);
+  if (tail.n_clean == 0) return;
+  // DepthmapCleaner over every map (tiles of 32 x 4 pixels), once all the
+  // post-processed depths are final.
+  if (!grid_barrier(sync, nb, p.error)) return;
+  ctr = sync + 4 + n_half;
+  for (int t = next_tile(ctr); t < tail.n_clean; t = next_tile(ctr))
+    clean_tile(tail.clean_views, tail.cmaps, tail.lists, tail.clean_tiles[t], tail.thr,
+               tail.min_views);
+  if (tail.n_prune == 0) return;
+  // DepthmapPruner: keep flags per 128-pixel block, one scan per map, then
+  // the ordered writes, each stage after a grid barrier.
+  if (!grid_barrier(sync, nb, p.error)) return;
+  ctr = sync + 5 + n_half;
+  for (int t = next_tile(ctr); t < tail.n_prune; t = next_tile(ctr)) {
+    const int4 tl = tail.prune_tiles[t];
+    const PruneMap& m = tail.pmaps[tl.x];
+    prune_flags_block<kPruneBatchBlock>(m.views, m.n_views, tail.thr, m.keep, m.counts, tl.y);
+  }
+  if (!grid_barrier(sync, nb, p.error)) return;
+  ctr = sync + 6 + n_half;
+  for (int t = next_tile(ctr); t < tail.n_pmaps; t = next_tile(ctr)) {
+    const PruneMap& m = tail.pmaps[t];
+    scan_counts_block(m.counts, m.blocks, m.offsets, m.count);
+  }
+  if (!grid_barrier(sync, nb, p.error)) return;
+  ctr = sync + 7 + n_half;
+  for (int t = next_tile(ctr); t < tail.n_prune; t = next_tile(ctr)) {
+    const int4 tl = tail.prune_tiles[t];
+    const PruneMap& m = tail.pmaps[tl.x];
+    prune_write_block<kPruneBatchBlock>(m.views, m.n_views, tail.thr, m.keep, m.offsets, m.out,
+                                        tl.y);
+  }
 }
 
 __global__ void postprocess_plain_kernel(const float* __restrict__ in, float* __restrict__ out,
@@ -704,7 +747,7 @@ static cudaError_t launch_persistent_l(const PersistentArgs& pa, cudaStream_t s)
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kern, a.maps, a.views, a.pairs, pa.tiles_init, pa.n_init,
                             pa.tiles_hp, pa.n_hp, pa.tiles_post, pa.n_post, pa.n_half, a.p,
-                            pa.sync);
+                            pa.sync, pa.tail);
 }
 
 cudaError_t launch_persistent(const PersistentArgs& pa, cudaStream_t s) {

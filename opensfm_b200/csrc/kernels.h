@@ -22,8 +22,29 @@ struct LaunchArgs {
 
 cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStream_t s);
 
+struct CleanView;
+struct CleanMap;
+struct PruneMap;
+// The cleaner and pruner stages of the persistent launch (n_clean == 0:
+// none; n_prune == 0: no pruner).  Tiles as launch_clean_batch and
+// launch_prune_batch take them.
+struct PersistentTail {
+  const CleanView* clean_views;
+  const CleanMap* cmaps;
+  const int* lists;
+  const int4* clean_tiles;
+  int n_clean;
+  int min_views;
+  float thr;
+  int n_pmaps;
+  const PruneMap* pmaps;
+  const int4* prune_tiles;
+  int n_prune;
+  int pad_;
+};
 // A whole PatchMatch run (7 x 7 patch, non-sample) in one cooperative
-// persistent launch: init tiles, n_half half-pass stages, post tiles.
+// persistent launch: init tiles, n_half half-pass stages, post tiles, then
+// the cleaner and the pruner's three stages over every map.
 struct PersistentArgs {
   LaunchArgs base;
   const int4* tiles_init;
@@ -33,8 +54,13 @@ struct PersistentArgs {
   const int4* tiles_post;
   int n_post;
   int n_half;
-  unsigned* sync;  // 4 + n_half counters, zeroed before the launch
+  unsigned* sync;  // kPersistentCounters + n_half counters, zeroed before the launch
+  PersistentTail tail;
 };
+// Barrier words and stage counters of the persistent launch besides the
+// n_half half-pass counters: arrivals, generation, init, post, clean,
+// prune flags, scan, prune writes.
+constexpr int kPersistentCounters = 8;
 cudaError_t launch_persistent(const PersistentArgs& pa, cudaStream_t s);
 cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, __half* d_img,
                                 uint2* d_quad, int TP, int TW, int TH, float cbias,
@@ -88,6 +114,17 @@ struct PruneOut {
 // Cleans map `ref` against views others[0..n) (DepthmapCleaner::Clean).
 cudaError_t launch_clean(const CleanView* d_views, int ref, const int* d_others, int n_others,
                          int W, int H, float thr, int min_views, float* out, cudaStream_t s);
+// Every map of a batch in one launch: map k (CleanView k, reference of the
+// k-th map) against the views lists[cmaps[k].list_off ..][0..cmaps[k].n),
+// into cmaps[k].out; tiles (map, tx, ty) of kCleanTileX x kCleanTileY px.
+constexpr int kCleanTileX = 32, kCleanTileY = 4;
+struct CleanMap {
+  int list_off, n, pad_[2];
+  float* out;  // [H][W] cleaned depth
+};
+cudaError_t launch_clean_batch(const CleanView* d_views, const CleanMap* d_cmaps,
+                               const int* d_lists, const int4* d_tiles, int n_tiles, float thr,
+                               int min_views, cudaStream_t s);
 // GPUDepthmapCleaner::Clean (cleaner.cc:56-170): forward and backward
 // consistency with space carving, FP32, every source the reference's size.
 constexpr int kMaxGpuCleanSources = 16;
@@ -111,5 +148,23 @@ cudaError_t launch_gpu_clean(const GpuCleanArgs& a, float* out, cudaStream_t s);
 size_t prune_scratch_bytes(int W, int H);
 cudaError_t launch_prune(const PruneView* d_views, int n_views, int W, int H, float thr,
                          void* scratch, PruneOut out, unsigned long long* d_count, cudaStream_t s);
+// The pruner over every map of a batch: flags over tiles (map, block) of
+// kPruneBatchBlock pixels, one scan block per map, ordered writes; three
+// launches in all.  Same output order as launch_prune (row-major).
+constexpr int kPruneBatchBlock = 128;
+struct PruneMap {
+  const PruneView* views;  // this map first
+  int n_views, blocks;     // blocks of kPruneBatchBlock pixels
+  uint8_t* keep;           // [H][W]
+  uint32_t* counts;        // [blocks]
+  uint32_t* offsets;       // [blocks + 1]
+  PruneOut out;
+  unsigned long long* count;
+};
+size_t prune_batch_scratch_bytes(int W, int H);
+PruneMap prune_batch_map(const PruneView* d_views, int n_views, int W, int H, void* scratch,
+                         PruneOut out, unsigned long long* d_count);
+cudaError_t launch_prune_batch(const PruneMap* d_pm, int n_maps, const int4* d_tiles, int n_tiles,
+                               float thr, cudaStream_t s);
 
 }  // namespace dn

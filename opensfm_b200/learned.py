@@ -383,12 +383,12 @@ class Schedule:
     half_passes: int
     kw: dict
     sample: bool = False
-    active: bool = False
+    active: float = 0.0  # > 0: active pixels, a depth moves by more than this
 
     def apply(self, b: pydense.Batch) -> None:
         b.set_schedule(half_passes=self.half_passes, **self.kw)
         b.set_candidate_views(self.sample)
-        b.set_active_pixels(self.active)
+        b.set_active_pixels(self.active > 0, self.active)
 
 
 PLAIN_3IT = Schedule("plain-3it", "plain", 6, {})
@@ -397,7 +397,7 @@ SCHEDULES = [
     Schedule("plain-1it", "plain", 2, {}),
     Schedule("plain-2it", "plain", 4, {}),
     PLAIN_3IT,
-    Schedule("plain-3it-active", "plain", 6, {}, active=True),
+    Schedule("plain-3it-active", "plain", 6, {}, active=0.002),
     Schedule("learned-0hp", "learned", 0, {}),
     Schedule("learned-2hp", "learned", 2, {}),
     Schedule("learned-4hp", "learned", 4, {}),
@@ -406,13 +406,13 @@ SCHEDULES = [
     Schedule("learned-sample-4hp", "learned", 4, {}, sample=True),
     Schedule("learned-sample-6hp", "learned", 6, {}, sample=True),
     Schedule("learned-sample-8hp", "learned", 8, {}, sample=True),
-    Schedule("learned-sample-active-6hp", "learned", 6, {}, sample=True, active=True),
-    Schedule("learned-sample-active-8hp", "learned", 8, {}, sample=True, active=True),
+    Schedule("learned-sample-active-6hp", "learned", 6, {}, sample=True, active=0.002),
+    Schedule("learned-sample-active-8hp", "learned", 8, {}, sample=True, active=0.002),
     Schedule("learned-sample-near-4hp", "learned", 4, _NEAR, sample=True),
     Schedule("learned-sample-near-6hp", "learned", 6, _NEAR, sample=True),
     Schedule("learned-sample-near3-6hp", "learned", 6, dict(_NEAR, n_refine=3), sample=True),
-    Schedule("learned-active-4hp", "learned", 4, {}, active=True),
-    Schedule("learned-active-6hp", "learned", 6, {}, active=True),
+    Schedule("learned-active-4hp", "learned", 4, {}, active=0.002),
+    Schedule("learned-active-6hp", "learned", 6, {}, active=0.002),
 ]
 
 

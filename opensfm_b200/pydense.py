@@ -715,16 +715,18 @@ class Batch(_Handle):
                                             int(bool(use_far)), int(n_refine), float(depth_range0),
                                             float(normal_range0)))
 
-    def set_candidate_views(self, sample: bool) -> None:
-        """Half-passes score every matching view per candidate (False, the
-        reference's ComputePatchMatch), or one view per candidate plus one
-        random other view per update (True, as ComputePatchMatchSample)."""
-        check(self._L.dn_batch_set_candidate_views(self._h, int(bool(sample))))
+    def set_candidate_views(self, mode) -> None:
+        """0 / False: every matching view per candidate (ComputePatchMatch);
+        1 / True: full initialisation, then one view per candidate plus one
+        random other view per update in the half-passes; 2: the reference's
+        ComputePatchMatchSample (a random view at the initialisation too)."""
+        check(self._L.dn_batch_set_candidate_views(self._h, int(mode)))
 
-    def set_active_pixels(self, on: bool) -> None:
-        """From the third half-pass on, update only pixels whose own plane or a
-        neighbour's plane changed at their last update."""
-        check(self._L.dn_batch_set_active_pixels(self._h, int(bool(on))))
+    def set_active_pixels(self, on: bool, min_change: float = 0.0) -> None:
+        """From the third half-pass on, update only pixels whose own depth or a
+        neighbour's depth moved at their last update (by more than
+        ``min_change`` relative; 0: any change of the plane)."""
+        check(self._L.dn_batch_set_active_pixels(self._h, int(bool(on)), float(min_change)))
 
     def set_proposal_net(self, weights: Optional[np.ndarray], biases: Optional[np.ndarray] = None,
                          n_planes: int = 8, stride: int = 2) -> None:

@@ -877,15 +877,19 @@ def test_persistent_launch_matches_per_stage_launches(scene):
     for v in range(n):
         mn, mx = S.depth_range(scene.depths[v])
         b.add_depthmap(v, [o for o in range(n) if o != v][:4], mn, mx)
-    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=3, seed=5)
+    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=3, seed=5, min_consistent_views=2)
+    for v in range(n):
+        b.set_clean_views(v, [o for o in range(n) if o != v])
     results = []
     variants = (4, 20, 2, 18, 8, 24)
     for variant in variants:
         b.set_tuning(32, 4, variant)
-        b.run(graph=(variant >= 16))
+        # The persistent launch runs the cleaner and the pruner inside it.
+        b.run(graph=(variant >= 16), prune=True)
         b.synchronize()
-        results.append([b.get(v) for v in range(n)])
+        results.append([b.get(v, clean=True) + b.get_points(v) for v in range(n)])
     for v in range(n):
+        assert len(results[0][v][5]) > 0  # pruned points
         for k in range(0, len(variants), 2):
             for a, w in zip(results[k + 1][v], results[k][v]):
                 assert np.array_equal(a, w)
