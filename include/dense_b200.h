@@ -212,6 +212,10 @@ dn_status dn_batch_set_schedule(dn_batch* b, int half_passes, int use_near, int 
  * (depthmap.cc:215-227, 305-374): a random view at the initialisation, then
  * as mode 1. */
 dn_status dn_batch_set_candidate_views(dn_batch* b, int mode);
+/* Knight-move candidates (no reference counterpart): with on = 1 each
+ * half-pass update also tries the planes of the 8 pixels at (+-1, +-2) and
+ * (+-2, +-1), which have the opposite red-black colour. */
+dn_status dn_batch_set_knight_moves(dn_batch* b, int on);
 /* Active pixels (no reference counterpart): with on = 1, from the third
  * half-pass of a run on, a pixel is updated only if its own depth or one of
  * its 4 neighbours' depths moved at their last update -- by more than
@@ -265,6 +269,14 @@ dn_status dn_batch_copy_depth_device(dn_batch* b, int map_id, float* d_out);
 /* PostProcess (depthmap.cc:489-502) on a host depth map: 5x5 median with
  * replicated borders, then zero where |d - median| / d > 0.05 or d == 0. */
 dn_status dn_postprocess_depth(const float* depth, float* out, int width, int height);
+/* Check of the bounded device-side waits (no reference counterpart): runs
+ * the persistent launch's grid barrier on `blocks` blocks (1..64) with a
+ * barrier that can never open (it expects one block more), each block
+ * polling at most max_spins times (about 100 ns apart; 1..2^24).  Returns
+ * DN_TIMEOUT -- the status every persistent run reports when one of its
+ * waits expires -- with the device time in *ms (may be NULL); the device
+ * stays usable. */
+dn_status dn_check_bounded_wait(int blocks, int64_t max_spins, float* ms);
 /* Measures the device's FP32 FMA throughput (TFLOP/s, FMA = 2 flops) with a
  * register-resident FMA loop on every SM; used as the scoring roofline. */
 dn_status dn_fp32_peak(double* tflops, double* ms);

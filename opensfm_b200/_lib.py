@@ -84,6 +84,7 @@ _SIGNATURES = {
     "dn_batch_set_schedule": ([_vp, _i, _i, _i, _i, ctypes.c_float, ctypes.c_float], _i),
     "dn_batch_set_candidate_views": ([_vp, _i], _i),
     "dn_batch_set_active_pixels": ([_vp, _i, ctypes.c_float], _i),
+    "dn_batch_set_knight_moves": ([_vp, _i], _i),
     "dn_batch_set_proposal_net": ([_vp, ctypes.POINTER(ctypes.c_uint16), _f, _i, _i], _i),
     "dn_batch_pruned_count": ([_vp, ctypes.POINTER(ctypes.c_int64)], _i),
     "dn_batch_get_points": ([_vp, _i, _f, _f, _u8, _u8, ctypes.c_int64,
@@ -97,6 +98,7 @@ _SIGNATURES = {
     "dn_estimator_set_tuning": ([_vp, _i, _i, _i], _i),
     "dn_batch_timer_elapsed": ([_vp, _f], _i),
     "dn_postprocess_depth": ([_f, _f, _i, _i], _i),
+    "dn_check_bounded_wait": ([_i, ctypes.c_int64, _f], _i),
     "dn_fp32_peak": ([ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], _i),
     "dn_batch_sweep_features": ([_vp, _vp, ctypes.c_int64, _i, _i], _i),
     "dn_batch_targets": ([_vp, _vp, ctypes.c_int64, ctypes.c_float, _i], _i),

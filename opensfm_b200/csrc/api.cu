@@ -204,6 +204,7 @@ struct Engine {
   int use_near = 1, use_far = 1, n_refine = 6;
   float depth_range0 = 0.02f, normal_range0 = 0.5f;
   int sample_hp = 0;  // half-passes score one view per candidate (sample mode)
+  int use_knight = 0;  // knight-move candidates in the half-passes
   int active = 0;     // active-pixel half-passes
   float active_tol = 0.f;
   // Learned proposal (DN_RUN_LEARNED): network weights, the feature grid of
@@ -548,6 +549,7 @@ struct Engine {
     a.p.normal_range0 = normal_range0;
     a.p.active = active;
     a.p.active_tol = active_tol;
+    a.p.use_knight = use_knight;
     return a;
   }
 
@@ -1597,6 +1599,13 @@ dn_status dn_batch_set_candidate_views(dn_batch* b, int mode) {
   b->eng.invalidate();
   return DN_OK;
 }
+dn_status dn_batch_set_knight_moves(dn_batch* b, int on) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(b, "NULL batch");
+  b->eng.use_knight = on ? 1 : 0;
+  b->eng.invalidate();
+  return DN_OK;
+}
 dn_status dn_batch_set_active_pixels(dn_batch* b, int on, float min_change) {
   const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
@@ -2018,6 +2027,37 @@ dn_status dn_postprocess_depth(const float* depth, float* out, int width, int he
   DN_CUDA(dn::launch_postprocess_plain(a.p, b.p, width, height, 0));
   DN_CUDA(cudaMemcpy(out, b.p, n * sizeof(float), cudaMemcpyDeviceToHost));
   return DN_OK;
+}
+
+dn_status dn_check_bounded_wait(int blocks, int64_t max_spins, float* ms) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(blocks >= 1 && blocks <= 64, "blocks must be 1..64");
+  DN_CHECK(max_spins >= 1 && max_spins <= (int64_t)1 << 24, "max_spins must be 1..2^24");
+  DN_TRY(need_device());
+  DevBuf<unsigned> sync;
+  DevBuf<int> err;
+  DN_CUDA(sync.alloc(2));
+  DN_CUDA(err.alloc(1));
+  DN_CUDA(cudaMemset(sync.p, 0, 2 * sizeof(unsigned)));
+  DN_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+  cudaEvent_t e0, e1;
+  DN_CUDA(cudaEventCreate(&e0));
+  DN_CUDA(cudaEventCreate(&e1));
+  DN_CUDA(cudaEventRecord(e0, 0));
+  const cudaError_t le = dn::launch_barrier_expiry(sync.p, err.p, blocks, max_spins, 0);
+  DN_CUDA(cudaEventRecord(e1, 0));
+  const cudaError_t se = cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  DN_CUDA(le);
+  DN_CUDA(se);
+  if (ms) *ms = t;
+  int flag = 0;
+  DN_CUDA(cudaMemcpy(&flag, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) return fail(DN_TIMEOUT, "a bounded device-side wait expired (as this check intends)");
+  return fail(DN_DEVICE_ERROR, "the never-opening barrier did not report its expiry");
 }
 
 dn_status dn_fp32_peak(double* tflops, double* ms) {

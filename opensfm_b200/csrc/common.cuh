@@ -86,6 +86,7 @@ struct RunParams {
   // first refinement's depth / normal-slope ranges.
   int use_near, use_far, n_refine;
   float depth_range0, normal_range0;
+  int use_knight;  // the 8 knight-move pixels (+-1, +-2), (+-2, +-1) as candidates
   // Active pixels: from half-pass 2 on, a pixel is updated only if its own
   // depth or one of its 4 neighbours' depths moved at their last update
   // (MapDev::changed); otherwise its state is kept as it is.  A depth moves

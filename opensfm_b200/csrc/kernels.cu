@@ -359,12 +359,15 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
       }
     };
 
-    // One evaluation site for all 14 candidate slots keeps the kernel's code
+    // One evaluation site for all candidate slots keeps the kernel's code
     // small and the warp's lanes at the same slot: 0-3 adjacent pixels,
-    // 4-7 far samples, 8-13 refinements.
+    // 4-7 far samples, then (use_knight) the 8 knight-move pixels, then the
+    // refinements.
     int refn = curn;
     float depth_range = p.depth_range0, normal_range = p.normal_range0;
-    const int n_slots = 8 + p.n_refine;
+    const int n_knight = p.use_knight ? 8 : 0;
+    const int first_refine = 8 + n_knight;
+    const int n_slots = first_refine + p.n_refine;
 #pragma unroll 1
     for (int slot = 0; slot < n_slots; ++slot) {
       float3 v = make_float3(0.f, 0.f, 0.f);
@@ -372,7 +375,22 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
       bool valid = false;
       if (slot < 4 && !p.use_near) continue;
       if (slot >= 4 && slot < 8 && !p.use_far) continue;
-      if (slot < 8) {
+      if (slot >= 8 && slot < first_refine) {
+        // (+-1, +-2) and (+-2, +-1): the opposite colour, so no race.
+        const int k = slot - 8;
+        const int a = (k & 1) ? 1 : -1, b = (k & 2) ? 2 : -2;
+        const int di = (k & 4) ? b : a, dj = (k & 4) ? a : b;
+        const int qi = i + di, qj = j + dj;
+        if (qi >= 0 && qi < H && qj >= 0 && qj < W) {
+          const long q = (long)qi * W + qj;
+          const float4 sq = m.state[q];
+          if (sq.w != 0.0f) {
+            v = make_float3(sq.x, sq.y, sq.z);
+            view = SAMPLE ? m.nghbr[q] : 0;
+            valid = true;
+          }
+        }
+      } else if (slot < 8) {
         const int d = slot & 3;
         const int di = (d == 0) ? -1 : (d == 2 ? 1 : 0);
         const int dj = (d == 1) ? -1 : (d == 3 ? 1 : 0);
@@ -402,11 +420,11 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
           }
         }
       } else {
-        if (slot == 8) refn = curn;
+        if (slot == first_refine) refn = curn;
         if (cv.z != 0.0f) {
-          const uint4 r = philox4x32_10(
-              make_uint4((uint32_t)pix, (uint32_t)tl.x, (uint32_t)p.pass, (uint32_t)(slot - 8)),
-              p.seed_lo, p.seed_hi);
+          const uint4 r = philox4x32_10(make_uint4((uint32_t)pix, (uint32_t)tl.x, (uint32_t)p.pass,
+                                                   (uint32_t)(slot - first_refine)),
+                                        p.seed_lo, p.seed_hi);
           const float2 g0 = normal2(r.x, r.y), g1 = normal2(r.z, r.w);
           const float depth = cd * expf(depth_range * g0.x);
           const float3 n = make_float3(-cv.x / cv.z + normal_range * g0.y,
@@ -526,7 +544,8 @@ __global__ void postprocess_kernel(const MapDev* __restrict__ maps, const int4* 
 // sync: [0] arrivals, [1] generation, [2 + s] tile counter of stage s.
 constexpr long long kBarrierSpins = 1LL << 25;
 
-__device__ inline bool grid_barrier(unsigned* sync, unsigned n_blocks, int* error) {
+__device__ inline bool grid_barrier(unsigned* sync, unsigned n_blocks, int* error,
+                                    long long max_spins = kBarrierSpins) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -541,7 +560,7 @@ __device__ inline bool grid_barrier(unsigned* sync, unsigned n_blocks, int* erro
     } else {
       long long spins = 0;
       while (*gen == g) {
-        if (++spins > kBarrierSpins || *(volatile int*)error) {
+        if (++spins > max_spins || *(volatile int*)error) {
           atomicExch(error, 1);
           break;
         }
@@ -619,6 +638,21 @@ patchmatch_persistent_kernel(const MapDev* __restrict__ maps, const ViewDev* __r
     prune_write_block<kPruneBatchBlock>(m.views, m.n_views, tail.thr, m.keep, m.offsets, m.out,
                                         tl.y);
   }
+}
+
+// Check of the bounded wait: every block arrives at a grid barrier that
+// expects one block more than the grid has, so the barrier can never open;
+// each block's wait ends after max_spins polls (or once another block has
+// set the error word) and the kernel returns with *error set.
+__global__ void barrier_expiry_kernel(unsigned* sync, int* error, long long max_spins) {
+  grid_barrier(sync, gridDim.x + 1, error, max_spins);
+}
+
+cudaError_t launch_barrier_expiry(unsigned* sync, int* error, int blocks, long long max_spins,
+                                  cudaStream_t s) {
+  void* args[] = {&sync, &error, &max_spins};
+  return cudaLaunchCooperativeKernel((const void*)barrier_expiry_kernel, dim3(blocks), dim3(32, 4),
+                                     args, 0, s);
 }
 
 __global__ void postprocess_plain_kernel(const float* __restrict__ in, float* __restrict__ out,

@@ -62,6 +62,11 @@ struct PersistentArgs {
 // prune flags, scan, prune writes.
 constexpr int kPersistentCounters = 8;
 cudaError_t launch_persistent(const PersistentArgs& pa, cudaStream_t s);
+// The persistent launch's grid barrier with a barrier that never opens
+// (`blocks` blocks, one more expected): returns with *error = 1 after at
+// most max_spins polls of 100 ns per block.  sync: 2 zeroed words.
+cudaError_t launch_barrier_expiry(unsigned* sync, int* error, int blocks, long long max_spins,
+                                  cudaStream_t s);
 cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, __half* d_img,
                                 uint2* d_quad, int TP, int TW, int TH, float cbias,
                                 cudaStream_t s);

@@ -382,13 +382,15 @@ class Schedule:
     init: str
     half_passes: int
     kw: dict
-    sample: bool = False
+    sample: int = 0  # Batch.set_candidate_views mode
     active: float = 0.0  # > 0: active pixels, a depth moves by more than this
+    knights: bool = False
 
     def apply(self, b: pydense.Batch) -> None:
         b.set_schedule(half_passes=self.half_passes, **self.kw)
         b.set_candidate_views(self.sample)
         b.set_active_pixels(self.active > 0, self.active)
+        b.set_knight_moves(self.knights)
 
 
 PLAIN_3IT = Schedule("plain-3it", "plain", 6, {})

@@ -722,6 +722,10 @@ class Batch(_Handle):
         ComputePatchMatchSample (a random view at the initialisation too)."""
         check(self._L.dn_batch_set_candidate_views(self._h, int(mode)))
 
+    def set_knight_moves(self, on: bool) -> None:
+        """Also try the planes of the 8 knight-move pixels in every update."""
+        check(self._L.dn_batch_set_knight_moves(self._h, int(bool(on))))
+
     def set_active_pixels(self, on: bool, min_change: float = 0.0) -> None:
         """From the third half-pass on, update only pixels whose own depth or a
         neighbour's depth moved at their last update (by more than

@@ -893,3 +893,29 @@ def test_persistent_launch_matches_per_stage_launches(scene):
         for k in range(0, len(variants), 2):
             for a, w in zip(results[k + 1][v], results[k][v]):
                 assert np.array_equal(a, w)
+
+
+def test_bounded_wait_expiry_reports_timeout():
+    """A grid barrier that can never open (it expects one block more than the
+    grid has) ends after its poll limit: the call returns DN_TIMEOUT, the
+    status a persistent run reports when one of its waits expires, and the
+    device keeps working afterwards."""
+    from opensfm_b200 import _lib
+
+    import ctypes
+
+    L = _lib.load()
+    ms = ctypes.c_float()
+    st = L.dn_check_bounded_wait(8, 1 << 14, ctypes.byref(ms))
+    assert st == _lib.DN_TIMEOUT, (st, L.dn_last_error())
+    assert 0.0 < ms.value < 1000.0
+    # The context is intact: a regular run still works.
+    vs = S.ring_viewset(3, 3, 48, 40)
+    b = pydense.Batch()
+    for c, im in zip(vs.cameras, vs.images):
+        b.add_view(c.K, c.R, c.t, im)
+    b.add_depthmap(0, [1, 2], *S.depth_range(vs.depths[0]))
+    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=1)
+    b.run()
+    b.synchronize()
+    assert (b.get_depth(0) > 0).any()
