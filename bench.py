@@ -46,10 +46,12 @@ N_VIEWS, N_CAND, N_MATCH = 24, 10, 6
 PATCH, MIN_SD, ITERS = 7, 1.0, 3
 SEED = 2024
 FLOPS_PER_TAP = 25  # affine warp 8 + bilinear 11 + NCC sums 6 (FMA = 2)
-# DRAM bytes (read + write) of one half-pass launch over the 24 maps, from an
-# ncu capture of this workload: the depthmap state read and written once plus
-# the first touch of the coefficient tables; every other gather hits L2.
-HALFPASS_DRAM_BYTES = 226_447_360 + 91_279_616
+# The plain GPU PatchMatch: red-black half-passes with every matching view
+# scored per candidate; and the learned schedules tried in order of cost
+# (half-passes, active-pixel threshold, knight moves), each after the
+# proposal network's initialisation with one view per candidate.
+PLAIN_HALF_PASSES, PLAIN_KNIGHTS = 2 * ITERS, False
+LEARNED_SCHEDULES = ((12, 0.003, False), (16, 0.003, False), (20, 0.003, False))
 
 
 # ---------------------------------------------------------------- workload
@@ -84,35 +86,57 @@ def make_workload(seed=SEED, n_views=N_VIEWS, W=W_, H=H_, kind="ring24"):
     return vs, ranges, cands, matches
 
 
-def learned_leg(b, n_maps, shapes, steps, vs):
-    """Learned initialisation on the same batch: the feature sweep and the
-    tcgen05 network propose every map's initial planes, then the same
-    PatchMatch + cleaner + pruner run.  Timed on the batch stream around the
-    whole sequence (host launches included); returns depthmaps/s, ms per
-    step and the median accuracy."""
-    from opensfm_b200 import learned as LN
-    from opensfm_b200 import synthetic as S
+def schedules():
+    """(plain, learned candidates): the plain GPU PatchMatch, and the learned
+    schedules tried in order of cost; the first whose accuracy is no lower
+    than the plain method's is the headline."""
+    from opensfm_b200.learned import Schedule
 
-    if len({tuple(sh) for sh in shapes[:n_maps]}) != 1:
-        return {"skipped": "the proposal network runs on batches of one image size"}
-    H, W = shapes[0]
-    net = LN.ProposalNet.load()
-    maps = list(range(n_maps))
-    LN.propose(net, b, maps, H, W)
-    b.run(prune=True, graph=True)
+    plain = Schedule("plain", "plain", PLAIN_HALF_PASSES, {}, knights=PLAIN_KNIGHTS)
+    learned = [Schedule(f"learned-sample-{hp}hp-active{int(a * 1000)}", "learned", hp, {},
+                        sample=1, active=a, knights=kn) for hp, a, kn in LEARNED_SCHEDULES]
+    return plain, learned
+
+
+def timed_runs(b, steps, learned, group=None):
+    """Device ms of `steps` graph replays (batch stream events)."""
+    if group:
+        group.barrier()
     b.synchronize()
     b.timer_record(0)
     for _ in range(steps):
-        LN.propose(net, b, maps, H, W)
-        b.run(prune=True, graph=True)
+        b.run(prune=True, graph=True, learned=learned)
     b.timer_record(1)
     b.synchronize()
     ms = b.timer_elapsed()
-    acc = [S.accuracy(b.get_depth(v), vs.depths[v]) for v in maps]
-    return {"value": n_maps * steps / (ms * 1e-3), "ms_per_step": ms / steps,
-            "accuracy_1pct_median": float(np.median(acc)),
-            "schedule": "proposal (8-plane sweep x 2 views + 6-layer tcgen05 network) then the "
-                        "same 3 iterations, cleaner and pruner"}
+    if group:
+        group.barrier()
+    return ms
+
+
+def map_accuracy(b, vs, n_maps):
+    accs = [S_accuracy(b.get_depth(v), vs.depths[v]) for v in range(n_maps)]
+    return float(np.median(accs)), float(np.mean(accs))
+
+
+def S_accuracy(d, gt):
+    from opensfm_b200 import synthetic as S
+
+    return S.accuracy(d, gt)
+
+
+def stage_roofline(b, sched, learned, peak):
+    """One instrumented run of the schedule (per-stage launches, events per
+    stage; outside the timed region): stage ms, taps and the half-pass
+    kernel's algorithmic FP32 throughput."""
+    b.run(prune=True, graph=False, timing=True, learned=learned)
+    b.synchronize()
+    stages, taps = b.timings()
+    hp_ms = stages[1]
+    achieved = FLOPS_PER_TAP * taps[1] / (hp_ms * 1e-3) / 1e12 if hp_ms > 0 else 0.0
+    return {"stage_ms": {"proposal": stages[5], "init": stages[0], "halfpasses": stages[1],
+                         "post": stages[2], "clean_and_prune": stages[3], "total": stages[4]},
+            "halfpass_taps": taps[1], "achieved": achieved, "frac": achieved / peak}
 
 
 def fusion_leg(b, vs, cands, n_maps, repeats=3, oracle=True):
@@ -624,10 +648,43 @@ def build_batch(work, seed=1, n_maps=None):
     return b
 
 
+def mixed_leg(kind, learned_sched=None):
+    """Config 3: 64 views of mixed sizes (box or terrain).  The plain
+    schedule runs every depthmap with its cleaner and pruner in one
+    persistent cooperative launch replayed from a CUDA graph; the learned
+    schedule the ring leg chose (one view per candidate, so per-stage
+    launches) runs the network once per image size in the batch.
+    Device-timed over 3 replays."""
+    from opensfm_b200 import learned as LN
+
+    work = make_workload(kind=kind)
+    vs, ranges, cands, matches = work
+    b = build_batch(work)
+    b.set_tuning(32, 4, 18)  # 2 lanes per pixel, persistent launch (+16)
+    plain, _ = schedules()
+    out = {"views": len(vs.cameras), "sizes": {}}
+    for h, w in (im.shape for im in vs.images):
+        out["sizes"][f"{w}x{h}"] = out["sizes"].get(f"{w}x{h}", 0) + 1
+    for sch in [plain] + ([learned_sched] if learned_sched else []):
+        is_l = sch.init == "learned"
+        if is_l:
+            LN.install(LN.ProposalNet.load(), b)
+        sch.apply(b)
+        b.run(prune=True, graph=True, learned=is_l)
+        b.synchronize()
+        ms = timed_runs(b, 3, is_l) / 3
+        acc = map_accuracy(b, vs, len(vs.cameras))
+        out[sch.init] = {"schedule": sch.name, "value": len(vs.cameras) / (ms * 1e-3),
+                         "ms_per_step": ms, "accuracy_1pct_median": acc[0],
+                         "accuracy_1pct_mean": acc[1], "pruned_points": b.pruned_count()}
+    b.close()
+    return out
+
+
 def run_ours(args):
     rank, world, local = dist_env()
     from opensfm_b200 import _lib, pydense
-    from opensfm_b200 import synthetic as S
+    from opensfm_b200 import learned as LN
 
     group = Group(world, local)
     _lib.check(_lib.load().dn_set_device(local))
@@ -635,7 +692,10 @@ def run_ours(args):
     vs, ranges, cands, matches = work
     n_maps = args.maps or len(vs.cameras)
     shapes = [im.shape for im in vs.images]
+    ring = args.workload == "ring24"
     b = build_batch(work, n_maps=n_maps)
+    plain, learned_scheds = schedules()
+    plain.apply(b)
     tuning = None
     if args.tuning:
         bx, by, var = (int(x) for x in args.tuning.split(","))
@@ -651,52 +711,67 @@ def run_ours(args):
         t = autotune.tune(b, key, {"prune": True, "graph": True}, candidates=tune_cands)
         tuning = {"choice": list(t["choice"]), "ms": t["ms"], "cached": t["cached"],
                   "source": "opensfm_b200.autotune"}
-
-    # Warm-up (graph capture on the first run).
-    for _ in range(args.warmup):
-        b.run(prune=True, graph=True)
-    b.synchronize()
-
-    # Stage timings and tap counts from one instrumented run (outside the
-    # timed region): the roofline of the dominant kernel.  Stage events need
-    # one launch per stage, so a persistent choice is timed as its per-stage
-    # equivalent (same tiles and lanes; results are identical).
     choice = tuning["choice"]
-    if choice[2] & 16:
-        b.set_tuning(choice[0], choice[1], choice[2] & 15)
-    b.run(prune=True, graph=False, timing=True)
-    b.synchronize()
-    stages, taps = b.timings()
-    if choice[2] & 16:
-        b.set_tuning(*choice)
-        b.run(prune=True, graph=True)
-        b.synchronize()
-    hp_ms = stages[1]
-    achieved = FLOPS_PER_TAP * taps[1] / (hp_ms * 1e-3) / 1e12
     peak = pydense.fp32_peak()
 
-    # Accuracy of the plain method against ground truth (median over maps).
-    accs = []
-    for v in range(n_maps):
-        accs.append(S.accuracy(b.get_depth(v), vs.depths[v]))
-
-    # Timed region: K batched runs, device events on the batch stream.
-    with Clocks(local) as clk:
-        group.barrier()
+    def leg(sch, learned):
+        """Warm-up, one instrumented run (per-stage launches), accuracy, then
+        the K timed graph replays."""
+        sch.apply(b)
+        for _ in range(args.warmup):
+            b.run(prune=True, graph=True, learned=learned)
         b.synchronize()
-        b.timer_record(0)
-        for _ in range(args.steps):
-            b.run(prune=True, graph=True)
-        b.timer_record(1)
+        if choice[2] & 16:  # stage events need one launch per stage
+            b.set_tuning(choice[0], choice[1], choice[2] & 15)
+        roof = stage_roofline(b, sch, learned, peak)
+        if choice[2] & 16:
+            b.set_tuning(*choice)
+            b.run(prune=True, graph=True, learned=learned)
         b.synchronize()
-        ms = b.timer_elapsed()
-        group.barrier()
-    pruned = b.pruned_count()
-    ms_max = group.max(ms)
-    value = replica_throughput(world, n_maps, args.steps, ms_max)
+        acc = map_accuracy(b, vs, n_maps)
+        ms = group.max(timed_runs(b, args.steps, learned, group))
+        return {"schedule": sch.name, "half_passes": sch.half_passes,
+                "candidate_views": ["all", "one per candidate", "sample"][sch.sample],
+                "knight_moves": sch.knights, "active_pixels": sch.active,
+                "value": replica_throughput(world, n_maps, args.steps, ms),
+                "ms_per_step": ms / args.steps, "accuracy_1pct_median": acc[0],
+                "accuracy_1pct_mean": acc[1], "pruned_points": b.pruned_count(), **roof}
 
-    # End to end through the public API from pinned host buffers: every
-    # step uploads the images, runs, and reads every final depth back.
+    # Plain GPU PatchMatch (random initialisation, every view per candidate).
+    with Clocks(local) as clk_plain:
+        plain_res = leg(plain, False)
+    head, head_learned, clk = plain_res, False, clk_plain
+    learned_res, tried = None, []
+    if ring and len({tuple(sh) for sh in shapes[:n_maps]}) == 1:
+        LN.install(LN.ProposalNet.load(), b)
+        # The cheapest learned schedule whose accuracy is no lower than plain's
+        # (medians and means over the maps), from one graph replay each.
+        pick = learned_scheds[-1]
+        for sch in learned_scheds:
+            sch.apply(b)
+            b.run(prune=True, graph=True, learned=True)
+            b.synchronize()
+            ms = timed_runs(b, 2, True) / 2
+            acc = map_accuracy(b, vs, n_maps)
+            ok = acc[0] >= plain_res["accuracy_1pct_median"] and acc[1] >= plain_res["accuracy_1pct_mean"]
+            tried.append({"schedule": sch.name, "ms": ms, "accuracy_1pct_median": acc[0],
+                          "accuracy_1pct_mean": acc[1], "equal_accuracy": ok})
+            if ok:
+                pick = sch
+                break
+        with Clocks(local) as clk_learned:
+            learned_res = leg(pick, True)
+        learned_res["equal_accuracy"] = (
+            learned_res["accuracy_1pct_median"] >= plain_res["accuracy_1pct_median"]
+            and learned_res["accuracy_1pct_mean"] >= plain_res["accuracy_1pct_mean"])
+        head, head_learned, clk = learned_res, True, clk_learned
+        head_sched = pick
+    else:
+        head_sched = plain
+
+    # End to end through the public batch API from pinned host buffers: every
+    # step uploads the images, runs the headline schedule, and reads every
+    # final depth back.
     import torch
 
     def pinned(a):
@@ -704,6 +779,8 @@ def run_ours(args):
         t.numpy()[...] = a
         return t
 
+    head_sched.apply(b)
+    b.run(prune=True, graph=True, learned=head_learned)
     keep = [pinned(np.ascontiguousarray(im)) for im in vs.images[:n_maps]]
     imgs = [t.numpy() for t in keep]
     keep += [pinned(np.zeros(sh, np.float32)) for sh in shapes[:n_maps]]
@@ -715,7 +792,7 @@ def run_ours(args):
     for _ in range(args.steps):
         for v, im in enumerate(imgs):
             b.set_view_image(v, im)
-        b.run(prune=True, graph=True)
+        b.run(prune=True, graph=True, learned=head_learned)
         b.get_depths(map_ids, outs)
     b.timer_record(1)
     b.synchronize()
@@ -723,58 +800,61 @@ def run_ours(args):
     group.barrier()
     e2e = replica_throughput(world, n_maps, args.steps, e2e_ms)
 
-    ring = args.workload == "ring24"
     if ring:
         desc = (f"ring reconstruction, {n_maps} reference views {W_}x{H_}, "
                 f"{N_MATCH} matching views, {N_CAND} cleaner neighbours, PatchMatch "
-                f"{ITERS} iterations (red-black), patch {PATCH}, min_patch_sd {MIN_SD}, "
-                f"cleaner 0.01 / 3 views, pruner 0.01; plain random initialisation")
+                f"{ITERS} iterations, patch {PATCH}, min_patch_sd {MIN_SD}, "
+                f"cleaner 0.01 / 3 views, pruner 0.01")
     elif args.workload == "aerial":
         desc = (f"aerial block: terrain 300x300 m with 40 buildings, {n_maps} reference views "
                 f"1280x960 (128 nadir + 128 at 45 deg, 60 m), {N_MATCH} matching views, "
                 f"{N_CAND} cleaner neighbours (nearest footprints, similar directions), "
-                f"PatchMatch {ITERS} iterations (red-black), patch {PATCH}, cleaner 0.01 / 3 "
-                f"views, pruner 0.01; plain random initialisation")
+                f"PatchMatch {ITERS} iterations, patch {PATCH}, cleaner 0.01 / 3 views, "
+                f"pruner 0.01")
     else:
         sizes = {}
         for h, w in shapes[:n_maps]:
             sizes[f"{w}x{h}"] = sizes.get(f"{w}x{h}", 0) + 1
         desc = (f"{args.workload}: {n_maps} depthmaps of mixed sizes {sizes}, "
                 f"{min(len(m) for m in matches)}-{max(len(m) for m in matches)} matching "
-                f"(and cleaner) views, PatchMatch {ITERS} iterations (red-black), patch "
-                f"{PATCH}, min_patch_sd {MIN_SD}, cleaner 0.01 / 3 views, pruner 0.01; plain "
-                f"random initialisation; {sum(h * w for h, w in shapes[:n_maps]) / 1e6:.2f} "
-                f"Mpx per step")
+                f"(and cleaner) views, PatchMatch {ITERS} iterations, patch {PATCH}, "
+                f"min_patch_sd {MIN_SD}, cleaner 0.01 / 3 views, pruner 0.01; "
+                f"{sum(h * w for h, w in shapes[:n_maps]) / 1e6:.2f} Mpx per step")
+    hp_variant = choice[2] & 15
     line = {
         "metric": METRIC if ring else (
             "1280px depthmaps/s (256-view aerial block, 6 views, 3 iters, cleaner + pruner)"
             if args.workload == "aerial" else
             "depthmaps/s (64 mixed-size views, 4-10 matching views, 3 iters, cleaner + pruner)"),
-        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {
             "workload": desc,
-            "pruned_points": pruned,
-            "init": "plain", "global_batch": n_maps * world, "parallelism": f"replicas x{world}",
+            "init": "learned" if head_learned else "plain",
+            "global_batch": n_maps * world, "parallelism": f"replicas x{world}",
             "tuning": tuning,
             "l2": "working set larger than L2 (views, tables and state ~%.0f MB)" % (
                 sum((w + 15) * (h + 15) * 8 + w * h * (16 + 4 + 4 + 4 + 4 + 2)
                     for h, w in shapes[:n_maps]) / 1e6),
-            "accuracy_1pct_median": float(np.median(accs)),
-            "stage_ms": {"init": stages[0], "halfpasses": stages[1], "post": stages[2],
-                         "clean_and_prune": stages[3], "total": stages[4]},
+            "plain": plain_res,
+            "learned": learned_res,
+            "learned_schedules_tried": tried,
+            "learned_over_plain": (learned_res["value"] / plain_res["value"]) if learned_res else None,
+            "equal_accuracy": learned_res["equal_accuracy"] if learned_res else None,
         },
         "roofline": {
-            "kernel": "halfpass_kernel<3,false,%d>" % (choice[2] & 15), "bound": "fp32",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": HALFPASS_DRAM_BYTES if (ring and n_maps == N_VIEWS) else None,
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                              "half-pass launch over the 24 maps (2 lanes per pixel)",
+            "kernel": "halfpass_kernel<3,%s,%d>" % (
+                "true" if head_sched.sample else "false", hp_variant),
+            "bound": "fp32", "achieved": head["achieved"], "peak": peak, "unit": "TFLOP/s",
+            "frac": head["frac"], "traffic": None,
+            "traffic_source": "not measured inside the bench (ncu); the captures under "
+                              "profiles/ give the half-pass kernel's DRAM bytes",
             "peak_source": "measured FP32 FMA loop on this GPU (dn_fp32_peak); "
                            "MEASURED_PEAKS.json has no FP32 figure",
-            "algorithmic": f"{FLOPS_PER_TAP} flops per NCC tap x {taps[1]} taps in "
-                           f"{2 * ITERS} half-passes ({hp_ms:.2f} ms)",
+            "algorithmic": f"{FLOPS_PER_TAP} flops per NCC tap x {head['halfpass_taps']} taps "
+                           f"in {head_sched.half_passes} half-passes "
+                           f"({head['stage_ms']['halfpasses']:.2f} ms)",
         },
         "e2e": {"value": e2e, "unit": UNIT,
                 "h2d_bytes_per_step": int(sum(im.nbytes for im in imgs[:n_maps])),
@@ -782,15 +862,21 @@ def run_ours(args):
         "gpu_launches": None,
         "clocks": {k: v for k, v in clk.summary().items()},
     }
-    # Launch count per step: memsets are not kernels; init + 2*iters
-    # half-passes + post (or one persistent launch for all three) + one
-    # cleaner launch and three pruner launches per map.
-    pm_launches = 1 if (tuning and tuning["choice"][2] & 16) else (1 + 2 * ITERS + 1)
-    line["gpu_launches"] = args.steps * (pm_launches + 4 * n_maps)
+    # Kernel launches per step: the learned proposal (sweep, 6 network
+    # layers, plane install), then init + half-passes + post, one cleaner
+    # launch and three pruner launches over all maps -- or, with the
+    # persistent choice, one launch for all of PatchMatch, cleaner and pruner.
+    n_groups = len({tuple(sh) for sh in shapes[:n_maps]})
+    prop = (1 + 6 * n_groups + 1) if head_learned else 0
+    pm = 1 if (choice[2] & 16 and not head_sched.sample) else (
+        1 + head_sched.half_passes + 1 + 1 + 3)
+    line["gpu_launches"] = args.steps * (prop + pm)
+    if ring and not args.no_mixed:
+        line["config"]["mixed_size_batches"] = {
+            k: mixed_leg(k, head_sched if head_learned else None)
+            for k in ("mixed-box", "mixed-terrain")}
     if args.fuse:
         line["config"]["fusion"] = fusion_leg(b, vs, cands, n_maps)
-    if args.learned:
-        line["config"]["learned"] = learned_leg(b, n_maps, shapes, args.steps, vs)
     if args.acmmp:
         line["config"]["acmmp"] = acmmp_leg(vs, cands)
     if rank == 0 and world == 1 and not args.no_cpu and ring:
@@ -859,8 +945,8 @@ def main():
                     help="also time DepthmapFuser on the cleaned maps against its C oracle")
     ap.add_argument("--acmmp", action="store_true",
                     help="also time the live path's PatchMatch estimator (DepthmapClusterEstimator)")
-    ap.add_argument("--learned", action="store_true",
-                    help="also time the learned initialisation on the same batch")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the two 64-view mixed-size batches of the default run")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -76,6 +76,11 @@ def port():
                                  ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint64,
                                  _f, _f, _f, _i32]
+        L.or_compute_redblack.argtypes = [ctypes.c_int, ctypes.c_int, _d, _d, _d, _u8, _u8,
+                                          ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_float,
+                                          ctypes.c_uint64, _f, _f, _f, _i32]
         L.or_score_planes.argtypes = [ctypes.c_int, _d, _d, _d, _u8, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int, _f, _f, _i32]
         L.or_median5.argtypes = [_f, _f, ctypes.c_int, ctypes.c_int]
@@ -160,6 +165,26 @@ def port_compute(mode: int, Ks, Rs, ts, images, masks, patch_size=7, min_depth=1
     port().or_compute(mode, n, _P(K, _d), _P(R, _d), _P(t, _d), _P(im, _u8), _P(mk, _u8), W, H,
                       patch_size, min_depth, max_depth, num_planes, iterations, min_patch_sd,
                       seed, _P(depth, _f), _P(plane, _f), _P(score, _f), _P(nghbr, _i32))
+    return depth, plane, score, nghbr
+
+
+def port_compute_redblack(Ks, Rs, ts, images, masks, patch_size=7, min_depth=1.0,
+                          max_depth=10.0, half_passes=6, min_patch_sd=1.0, seed=1, sample=False):
+    """The GPU's red-black PatchMatch schedule with the reference's arithmetic
+    (or_compute_redblack in depthmap_oracle.c), or its sample mode:
+    [depth, plane, score, nghbr]."""
+    K, R, t = _stack_cams(Ks, Rs, ts)
+    im = np.ascontiguousarray(np.stack(images).astype(np.uint8))
+    mk = np.ascontiguousarray(np.stack(masks).astype(np.uint8))
+    n, H, W = im.shape
+    depth = np.zeros((H, W), np.float32)
+    plane = np.zeros((H, W, 3), np.float32)
+    score = np.zeros((H, W), np.float32)
+    nghbr = np.zeros((H, W), np.int32)
+    port().or_compute_redblack(int(bool(sample)), n, _P(K, _d), _P(R, _d), _P(t, _d), _P(im, _u8),
+                               _P(mk, _u8), W, H,
+                               patch_size, min_depth, max_depth, half_passes, min_patch_sd, seed,
+                               _P(depth, _f), _P(plane, _f), _P(score, _f), _P(nghbr, _i32))
     return depth, plane, score, nghbr
 
 

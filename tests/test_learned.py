@@ -188,3 +188,29 @@ def test_short_training_reduces_loss():
     net = learned.ProposalNet(seed=1)
     hist = learned.train(net, feat, tgt, len(seeds), 120, 160, steps=60, batch=4, lr=3e-3)
     assert hist[-1][1] < 0.8 * hist[0][1], hist
+
+
+def test_trained_network_gains_over_random_initialisation():
+    """The committed network (opensfm_b200/weights/proposal_net.npz) on 4
+    held-out scenes at 640 x 480 (seeds beyond the training range): learned
+    initialisation + k half-passes is more accurate than the reference's
+    random initialisation (RandomInitialization, depthmap.cc:237-256) + the
+    same k half-passes, for k = 1 and 2, with the same candidate sets.
+    Accuracy = fraction of ground-truth pixels within 1 % relative depth;
+    device time per run printed beside it."""
+    seeds = [910000, 910001, 910002, 910003]
+    scenes = [learned.make_scene(s, 640, 480) for s in seeds]
+    net = learned.ProposalNet.load()
+    scheds = []
+    for k in (1, 2):
+        scheds += [learned.Schedule(f"plain-{k}hp", "plain", k, {}),
+                   learned.Schedule(f"learned-{k}hp", "learned", k, {})]
+    res = learned.evaluate(net, seeds, scenes=scenes, schedules=scheds, repeats=2,
+                           log=lambda s: print(s, flush=True))
+    acc = {r["name"]: r["accuracy"] for r in res["runs"]}
+    ms = {r["name"]: r["ms"] for r in res["runs"]}
+    for k in (1, 2):
+        print("k = %d: learned %.4f (%.2f ms) vs random %.4f (%.2f ms)"
+              % (k, acc[f"learned-{k}hp"], ms[f"learned-{k}hp"], acc[f"plain-{k}hp"],
+                 ms[f"plain-{k}hp"]))
+        assert acc[f"learned-{k}hp"] > acc[f"plain-{k}hp"] + 0.05

@@ -151,6 +151,39 @@ def test_port_patchmatch_accuracy_close_to_reference():
     assert abs(a_ref - a_port) < 0.1
 
 
+def test_redblack_schedule_gap_to_the_raster_sweep():
+    """The GPU's red-black schedule, restated with the reference's arithmetic
+    (or_compute_redblack), against the reference's raster schedule with the
+    same arithmetic (or_compute, bit-identical to depthmap.cc), on the
+    320 x 240 benchmark scene with fixed seeds: the red-black result is
+    slightly less accurate (the pinned fixture's gap) because fewer of its
+    pixels survive the 5 x 5 median post-process; and the restatement
+    reproduces the fixture's red-black accuracies."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_pm_configs as M
+
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                             "pm_config1_320x240.npz"))
+    cams_, images, depths = M.config1_views()
+    Ks, Rs, ts = [c.K for c in cams_], [c.R for c in cams_], [c.t for c in cams_]
+    masks = [np.ones_like(im) for im in images]
+    mn, mx, gt = float(z["min_depth"]), float(z["max_depth"]), depths[0]
+    raster = O.port_compute(1, Ks, Rs, ts, images, masks, 7, mn, mx, 64, 3, 1.0, 1)[0]
+    rb = O.port_compute_redblack(Ks, Rs, ts, images, masks, 7, mn, mx, 6, 1.0, 1)[0]
+    a_raster, a_rb = S.accuracy(raster, gt), S.accuracy(rb, gt)
+    v_raster, v_rb = float((raster > 0).mean()), float((rb > 0).mean())
+    print("raster %.4f (valid %.4f) red-black %.4f (valid %.4f); fixture: reference %.4f, "
+          "red-black %.4f" % (a_raster, v_raster, a_rb, v_rb, z["pm_accuracy"].mean(),
+                              z["rb_accuracy"].mean()))
+    assert 0.0 < a_raster - a_rb < 0.01
+    assert v_rb < v_raster
+    assert abs(a_rb - z["rb_accuracy"].mean()) <= 0.003
+    assert abs(a_raster - z["pm_accuracy"].mean()) <= 0.003
+
+
 # ---------------------------------------------------------------- Philox
 def philox_py(ctr, key):
     M0, M1, W0, W1 = 0xD2511F53, 0xCD9E8D57, 0x9E3779B9, 0xBB67AE85
