@@ -51,7 +51,8 @@ FLOPS_PER_TAP = 25  # affine warp 8 + bilinear 11 + NCC sums 6 (FMA = 2)
 # (half-passes, active-pixel threshold, knight moves), each after the
 # proposal network's initialisation with one view per candidate.
 PLAIN_HALF_PASSES, PLAIN_KNIGHTS = 2 * ITERS, False
-LEARNED_SCHEDULES = ((12, 0.003, False), (16, 0.003, False), (20, 0.003, False))
+LEARNED_SCHEDULES = ((8, 0.003, False), (10, 0.003, False), (12, 0.003, False),
+                     (16, 0.003, False), (20, 0.003, False))
 
 
 # ---------------------------------------------------------------- workload
@@ -766,8 +767,22 @@ def run_ours(args):
             and learned_res["accuracy_1pct_mean"] >= plain_res["accuracy_1pct_mean"])
         head, head_learned, clk = learned_res, True, clk_learned
         head_sched = pick
+        # The same schedule from the reference's random initialisation: what
+        # the schedule gives without the proposal network.
+        from opensfm_b200.learned import Schedule
+
+        same = Schedule("plain-init-" + pick.name, "plain", pick.half_passes, dict(pick.kw),
+                        sample=pick.sample, active=pick.active, knights=pick.knights)
+        same.apply(b)
+        b.run(prune=True, graph=True)
+        b.synchronize()
+        ms = timed_runs(b, max(2, args.steps // 4), False) / max(2, args.steps // 4)
+        acc = map_accuracy(b, vs, n_maps)
+        plain_same = {"schedule": same.name, "value": n_maps / (ms * 1e-3), "ms_per_step": ms,
+                      "accuracy_1pct_median": acc[0], "accuracy_1pct_mean": acc[1]}
     else:
         head_sched = plain
+        plain_same = None
 
     # End to end through the public batch API from pinned host buffers: every
     # step uploads the images, runs the headline schedule, and reads every
@@ -840,6 +855,7 @@ def run_ours(args):
             "plain": plain_res,
             "learned": learned_res,
             "learned_schedules_tried": tried,
+            "plain_init_same_schedule": plain_same,
             "learned_over_plain": (learned_res["value"] / plain_res["value"]) if learned_res else None,
             "equal_accuracy": learned_res["equal_accuracy"] if learned_res else None,
         },

@@ -19,7 +19,8 @@ CACHE = os.path.join(HERE, "_build", "autotune.json")
 # (bx, by, variant): variant = lanes per pixel (1, 2, 4, 8) + 16 for the
 # persistent launch.
 CANDIDATES: List[Tuple[int, int, int]] = [
-    (32, 4, 4), (32, 4, 20), (32, 4, 8), (64, 2, 4), (32, 2, 4), (32, 4, 2), (32, 4, 1),
+    (32, 4, 4), (32, 4, 20), (32, 4, 8), (64, 2, 4), (32, 2, 4), (32, 4, 2), (32, 4, 18),
+    (32, 4, 1),
 ]
 
 
