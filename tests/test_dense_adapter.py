@@ -69,3 +69,74 @@ def test_raw_and_clean_files_match_the_library(tmp_path, views):
         assert np.array_equal(depth, want)
         assert np.array_equal(plane, raw[1]) and not score.any()
         assert (depth > 0).sum() < (raw[0] > 0).sum()
+
+
+def test_live_stages_write_what_the_live_classes_compute(tmp_path, views):
+    """run_cluster_raw / clean_cluster_gpu (the stand-ins for dense.py's
+    live call sites) write exactly what DepthmapClusterEstimator and
+    GPUDepthmapCleaner give when driven as dense.py drives them, in the live
+    path's raw fields (dense.py:741-775) and clean fields (dense.py:896-905)."""
+    ids, v, bn, dr, vs = views
+    d = str(tmp_path)
+    cfg = {"depthmap_num_matching_views": 3, "depthmap_hierarchy_levels": 2,
+           "depthmap_max_iterations": 2, "depthmap_patch_size": 5,
+           "depthmap_sfm_planar_prior": False, "depthmap_min_consistent_views": 2}
+    cluster = ids[1:4]
+    done = dense_adapter.run_cluster_raw(d, v, bn, cluster, dr, cfg)
+    assert done == cluster
+    # The same cluster, driven directly.
+    c = pydense.DepthmapClusterEstimator()
+    c.set_max_iterations(2)
+    c.set_patch_size(5)
+    c.set_max_image_size(3200)
+    c.set_sigma_spatial(5.0)
+    c.set_sigma_color(3.0 / 255.0)
+    c.set_top_k(3)
+    c.set_census_weight(0.3)
+    c.set_hierarchy_levels(2)
+    c.set_smooth_weight(0.3)
+    c.set_geom_consistency_weight(0.05)
+    idx, nb = {}, {}
+    for sid in cluster:
+        K, R, t, im = v[sid]
+        idx[sid] = c.begin_ref_view(K, R, t, im, *dr[sid])
+        nb[sid] = [sid] + bn[sid][1:4]
+        for s in bn[sid][1:4]:
+            Ks, Rs, ts, ims = v[s]
+            c.add_source_view(Ks, Rs, ts, ims)
+    for sid in cluster:
+        for o in cluster:
+            if o != sid and o in nb[sid]:
+                c.add_geom_link(idx[sid], nb[sid].index(o) - 1, idx[o])
+    want = c.run()
+    for sid, (depth, normal, cost, conf) in zip(cluster, want):
+        got = dense_io.load_raw_depthmap(d, sid)
+        exp_depth = depth.copy()
+        exp_depth[~np.isfinite(exp_depth)] = 0
+        exp_depth[cost > 0.9] = 0
+        assert np.array_equal(got[0], exp_depth)
+        assert np.array_equal(got[1], normal) and np.array_equal(got[2], cost)
+        assert got[3].shape == (0,) and list(got[4]) == bn[sid]
+        assert np.array_equal(got[5], conf)
+        assert (got[0] > 0).mean() > 0.3
+
+    done = dense_adapter.clean_cluster_gpu(d, v, bn, cluster, cfg, max_neighbors=3)
+    assert done == cluster
+    g = pydense.GPUDepthmapCleaner()
+    g.set_same_depth_threshold(0.01)
+    g.set_min_consistent_views(2)
+    g.set_carving_threshold(0.2)
+    g.set_max_carved_views(1)
+    have = set(cluster)  # only the cluster's shots have raw files
+    order = sorted(have)
+    for sid in order:
+        K, R, t, _ = v[sid]
+        g.add_view(K, R, t, dense_io.load_raw_depthmap(d, sid)[0])
+    for sid in cluster:
+        nbrs = [n for n in bn[sid] if n != sid and n in have][:3]
+        exp = g.clean(order.index(sid), np.array([order.index(n) for n in nbrs], np.int32))
+        depth, plane, score, conf = dense_io.load_clean_depthmap(d, sid)
+        raw = dense_io.load_raw_depthmap(d, sid)
+        assert np.array_equal(depth, exp)
+        assert np.array_equal(plane, raw[1]) and not score.any()
+        assert np.array_equal(conf, raw[5])
