@@ -715,9 +715,10 @@ def run_ours(args):
     choice = tuning["choice"]
     peak = pydense.fp32_peak()
 
-    def leg(sch, learned):
+    def leg(sch, learned, choice):
         """Warm-up, one instrumented run (per-stage launches), accuracy, then
-        the K timed graph replays."""
+        the K timed graph replays, with the launch tuning `choice`."""
+        b.set_tuning(*choice)
         sch.apply(b)
         for _ in range(args.warmup):
             b.run(prune=True, graph=True, learned=learned)
@@ -740,9 +741,10 @@ def run_ours(args):
 
     # Plain GPU PatchMatch (random initialisation, every view per candidate).
     with Clocks(local) as clk_plain:
-        plain_res = leg(plain, False)
+        plain_res = leg(plain, False, choice)
     head, head_learned, clk = plain_res, False, clk_plain
     learned_res, tried = None, []
+    choice_l = choice
     if ring and len({tuple(sh) for sh in shapes[:n_maps]}) == 1:
         LN.install(LN.ProposalNet.load(), b)
         # The cheapest learned schedule whose accuracy is no lower than plain's
@@ -760,8 +762,24 @@ def run_ours(args):
             if ok:
                 pick = sch
                 break
+        # The learned schedule's own launch tuning (one view per candidate
+        # runs shorter evaluations than the plain schedule; per-stage
+        # launches, as one view per candidate is not in the persistent
+        # launch).
+        choice_l = choice
+        if not args.tuning:
+            from opensfm_b200 import autotune
+
+            pick.apply(b)
+            key_l = autotune.workload_key(shapes[:n_maps], [len(m) for m in matches[:n_maps]],
+                                          PATCH) + ":learned:" + pick.name
+            t_l = autotune.tune(b, key_l, {"prune": True, "graph": True, "learned": True},
+                                candidates=[c for c in autotune.CANDIDATES if not c[2] & 16])
+            choice_l = tuple(t_l["choice"])
+            tuning["learned"] = {"choice": list(choice_l), "ms": t_l["ms"],
+                                 "cached": t_l["cached"]}
         with Clocks(local) as clk_learned:
-            learned_res = leg(pick, True)
+            learned_res = leg(pick, True, choice_l)
         learned_res["equal_accuracy"] = (
             learned_res["accuracy_1pct_median"] >= plain_res["accuracy_1pct_median"]
             and learned_res["accuracy_1pct_mean"] >= plain_res["accuracy_1pct_mean"])
@@ -794,6 +812,7 @@ def run_ours(args):
         t.numpy()[...] = a
         return t
 
+    b.set_tuning(*(choice_l if head_learned else choice))
     head_sched.apply(b)
     b.run(prune=True, graph=True, learned=head_learned)
     keep = [pinned(np.ascontiguousarray(im)) for im in vs.images[:n_maps]]
@@ -835,7 +854,8 @@ def run_ours(args):
                 f"(and cleaner) views, PatchMatch {ITERS} iterations, patch {PATCH}, "
                 f"min_patch_sd {MIN_SD}, cleaner 0.01 / 3 views, pruner 0.01; "
                 f"{sum(h * w for h, w in shapes[:n_maps]) / 1e6:.2f} Mpx per step")
-    hp_variant = choice[2] & 15
+    head_choice = choice_l if head_learned else choice
+    hp_variant = head_choice[2] & 15
     line = {
         "metric": METRIC if ring else (
             "1280px depthmaps/s (256-view aerial block, 6 views, 3 iters, cleaner + pruner)"
@@ -884,7 +904,7 @@ def run_ours(args):
     # persistent choice, one launch for all of PatchMatch, cleaner and pruner.
     n_groups = len({tuple(sh) for sh in shapes[:n_maps]})
     prop = (1 + 6 * n_groups + 1) if head_learned else 0
-    pm = 1 if (choice[2] & 16 and not head_sched.sample) else (
+    pm = 1 if (head_choice[2] & 16 and not head_sched.sample) else (
         1 + head_sched.half_passes + 1 + 1 + 3)
     line["gpu_launches"] = args.steps * (prop + pm)
     if ring and not args.no_mixed:
