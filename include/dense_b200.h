@@ -216,6 +216,11 @@ dn_status dn_batch_set_candidate_views(dn_batch* b, int mode);
  * half-pass update also tries the planes of the 8 pixels at (+-1, +-2) and
  * (+-2, +-1), which have the opposite red-black colour. */
 dn_status dn_batch_set_knight_moves(dn_batch* b, int on);
+/* One view per candidate (candidate view modes 1 and 2): with on = 1 (the
+ * default) the propagation candidates are scored two at a time with
+ * interleaved walks, with the same acceptances in the same order as one at
+ * a time (the results are identical); on = 0 scores them one at a time. */
+dn_status dn_batch_set_paired_candidates(dn_batch* b, int on);
 /* Active pixels (no reference counterpart): with on = 1, from the third
  * half-pass of a run on, a pixel is updated only if its own depth or one of
  * its 4 neighbours' depths moved at their last update -- by more than

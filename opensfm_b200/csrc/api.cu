@@ -205,6 +205,7 @@ struct Engine {
   float depth_range0 = 0.02f, normal_range0 = 0.5f;
   int sample_hp = 0;  // half-passes score one view per candidate (sample mode)
   int use_knight = 0;  // knight-move candidates in the half-passes
+  int paired = 1;      // sample mode: propagation candidates scored two at a time
   int active = 0;     // active-pixel half-passes
   float active_tol = 0.f;
   // Learned proposal (DN_RUN_LEARNED): network weights, the feature grid of
@@ -550,6 +551,7 @@ struct Engine {
     a.p.active = active;
     a.p.active_tol = active_tol;
     a.p.use_knight = use_knight;
+    a.p.paired = paired;
     return a;
   }
 
@@ -1596,6 +1598,13 @@ dn_status dn_batch_set_candidate_views(dn_batch* b, int mode) {
   DN_CHECK(mode >= 0 && mode <= 2,
            "candidate view mode must be 0 (all views), 1 (sample half-passes) or 2 (sample)");
   b->eng.sample_hp = mode;
+  b->eng.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_paired_candidates(dn_batch* b, int on) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(b, "NULL batch");
+  b->eng.paired = on ? 1 : 0;
   b->eng.invalidate();
   return DN_OK;
 }

@@ -269,11 +269,46 @@ def make_dataset(seeds: Sequence[int], W: int = 640, H: int = 480, chunk: int = 
 
 
 # -------------------------------------------------------------- training
+def save_checkpoint(net: ProposalNet, path: str, step: int, generator) -> None:
+    """Everything a training run needs to continue bit for bit where it
+    stopped: FP32 master weights and biases, both Adam moments, the Adam
+    step, the loop step and the state of the batch-sampling generator."""
+    torch = _torch()
+    d = net.state_dict()
+    for k, (m, v) in enumerate(zip(net.m, net.v)):
+        d[f"adam_m{k}"] = m.cpu().numpy()
+        d[f"adam_v{k}"] = v.cpu().numpy()
+    d["loop_step"] = np.array(step)
+    d["rng_state"] = generator.get_state().numpy()
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    np.savez(path, **d)
+
+
+def load_checkpoint(path: str) -> Tuple[ProposalNet, int, "object"]:
+    """(network with its Adam state, next loop step, generator) from
+    ``save_checkpoint``."""
+    torch = _torch()
+    z = np.load(path)
+    net = ProposalNet.load(path)
+    n = len(net.m)
+    net.m = [torch.from_numpy(z[f"adam_m{k}"]).cuda() for k in range(n)]
+    net.v = [torch.from_numpy(z[f"adam_v{k}"]).cuda() for k in range(n)]
+    g = torch.Generator(device="cpu")
+    g.set_state(torch.from_numpy(z["rng_state"]))
+    return net, int(z["loop_step"]), g
+
+
 def train(net: ProposalNet, feat, tgt, n_maps: int, H: int, W: int, steps: int = 1500,
-          batch: int = 8, lr: float = 2e-3, normal_weight: float = 0.1, seed: int = 0, log=None):
+          batch: int = 8, lr: float = 2e-3, normal_weight: float = 0.1, seed: int = 0, log=None,
+          start_step: int = 0, generator=None, stop_step: Optional[int] = None,
+          checkpoint: Optional[str] = None):
+    """Adam on the L1 loss over ``steps`` steps of a cosine learning-rate
+    schedule.  A run can stop early (``stop_step``; with ``checkpoint`` the
+    state is saved there) and continue from ``load_checkpoint``'s state
+    (``start_step``, ``generator``) with the same ``steps``."""
     torch = _torch()
     L = _lib.load()
-    g = torch.Generator(device="cpu").manual_seed(seed)
+    g = generator if generator is not None else torch.Generator(device="cpu").manual_seed(seed)
     per = H * W
     n_pix = batch * per
     loss_acc = torch.zeros(1, dtype=torch.float32, device="cuda")
@@ -283,7 +318,8 @@ def train(net: ProposalNet, feat, tgt, n_maps: int, H: int, W: int, steps: int =
     tv = tgt.view(n_maps, per * 4)
     history = []
     t0 = time.time()
-    for step in range(steps):
+    end = steps if stop_step is None else min(stop_step, steps)
+    for step in range(start_step, end):
         idx = torch.randint(0, n_maps, (batch,), generator=g).cuda()
         xb = fv.index_select(0, idx).reshape(-1).contiguous()
         tb = tv.index_select(0, idx).reshape(-1).contiguous()
@@ -300,6 +336,8 @@ def train(net: ProposalNet, feat, tgt, n_maps: int, H: int, W: int, steps: int =
             history.append((step, l))
             if log:
                 log(f"step {step} loss {l:.4f} lr {cur_lr:.2e} {time.time() - t0:.1f} s")
+    if checkpoint:
+        save_checkpoint(net, checkpoint, end, g)
     return history
 
 

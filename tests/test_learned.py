@@ -214,3 +214,29 @@ def test_trained_network_gains_over_random_initialisation():
               % (k, acc[f"learned-{k}hp"], ms[f"learned-{k}hp"], acc[f"plain-{k}hp"],
                  ms[f"plain-{k}hp"]))
         assert acc[f"learned-{k}hp"] > acc[f"plain-{k}hp"] + 0.05
+
+
+def test_training_checkpoint_resume(tmp_path):
+    """20 training steps in one go, and 10 steps + checkpoint + resume for
+    10 more, end at the same weights: the checkpoint holds the master
+    weights, both Adam moments, the Adam step and the batch sampler's state.
+    (The weight gradients are summed with atomics, in any order, so equal
+    means within float rounding.)"""
+    seeds = list(range(520, 528))
+    feat, tgt = learned.make_dataset(seeds, W=160, H=120, chunk=8, stride=1)
+    kw = dict(steps=20, batch=2, lr=3e-3)
+    a = learned.ProposalNet(seed=3, stride=1)
+    learned.train(a, feat, tgt, len(seeds), 120, 160, **kw)
+    b = learned.ProposalNet(seed=3, stride=1)
+    ck = str(tmp_path / "checkpoint.npz")
+    learned.train(b, feat, tgt, len(seeds), 120, 160, stop_step=10, checkpoint=ck, **kw)
+    c, start, g = learned.load_checkpoint(ck)
+    assert start == 10 and c.step == 10 and c.stride == 1
+    learned.train(c, feat, tgt, len(seeds), 120, 160, start_step=start, generator=g, **kw)
+    assert c.step == a.step == 20
+    for x, y in zip(a.w32 + a.b32, c.w32 + c.b32):
+        assert float((x - y).abs().max()) <= 1e-4 * max(float(x.abs().max()), 1e-3)
+    # A different sampler state would have drawn other batches.
+    d = learned.ProposalNet(seed=3, stride=1)
+    learned.train(d, feat, tgt, len(seeds), 120, 160, seed=1, **kw)
+    assert any(float((x - y).abs().max()) > 1e-3 for x, y in zip(a.w32, d.w32))
