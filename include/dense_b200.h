@@ -216,11 +216,6 @@ dn_status dn_batch_set_candidate_views(dn_batch* b, int mode);
  * half-pass update also tries the planes of the 8 pixels at (+-1, +-2) and
  * (+-2, +-1), which have the opposite red-black colour. */
 dn_status dn_batch_set_knight_moves(dn_batch* b, int on);
-/* One view per candidate (candidate view modes 1 and 2): with on = 1 (the
- * default) the propagation candidates are scored two at a time with
- * interleaved walks, with the same acceptances in the same order as one at
- * a time (the results are identical); on = 0 scores them one at a time. */
-dn_status dn_batch_set_paired_candidates(dn_batch* b, int on);
 /* Active pixels (no reference counterpart): with on = 1, from the third
  * half-pass of a run on, a pixel is updated only if its own depth or one of
  * its 4 neighbours' depths moved at their last update -- by more than
@@ -349,6 +344,18 @@ dn_status dn_nn_conv3x3_backward(const void* dy, const void* x, const void* w,
                                  const void* x_mask, int64_t n_pix, int H, int W, int cin,
                                  int cout, void* dx, float* dw, float* db, void* wt_scratch,
                                  void* stream);
+/* The same backward on the tcgen05 tensor cores (the training path; the
+ * warp-level mma.sync version above is kept as the comparison): dw and db
+ * from a split-K GEMM with FP32 accumulators in tensor memory, dx from the
+ * forward tcgen05 kernel on dy with flipped weights and the x_mask ReLU
+ * mask.  scratch: a device buffer of at least
+ * dn_nn_backward_scratch_bytes(n_pix, cout) bytes (16-byte aligned).
+ * Bounded waits report through dn_nn_synchronize. */
+int64_t dn_nn_backward_scratch_bytes(int64_t n_pix, int cout);
+dn_status dn_nn_conv3x3_backward_tc(const void* dy, const void* x, const void* w,
+                                    const void* x_mask, int64_t n_pix, int H, int W, int cin,
+                                    int cout, void* dx, float* dw, float* db, void* scratch,
+                                    int64_t scratch_bytes, void* stream);
 /* L1 loss of pred (f32 [n_pix][4]) against target ([n_pix][4], last = weight)
  * with the normal slopes weighted by normal_weight: adds the loss and the
  * weight total to loss_sum[0] / count[0] and writes dpred (BF16 [n_pix][4]). */

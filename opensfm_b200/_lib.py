@@ -85,7 +85,6 @@ _SIGNATURES = {
     "dn_batch_set_candidate_views": ([_vp, _i], _i),
     "dn_batch_set_active_pixels": ([_vp, _i, ctypes.c_float], _i),
     "dn_batch_set_knight_moves": ([_vp, _i], _i),
-    "dn_batch_set_paired_candidates": ([_vp, _i], _i),
     "dn_batch_set_proposal_net": ([_vp, ctypes.POINTER(ctypes.c_uint16), _f, _i, _i], _i),
     "dn_batch_pruned_count": ([_vp, ctypes.POINTER(ctypes.c_int64)], _i),
     "dn_batch_get_points": ([_vp, _i, _f, _f, _u8, _u8, ctypes.c_int64,
@@ -180,6 +179,9 @@ _SIGNATURES = {
     "dn_io_last_error": ([], ctypes.c_char_p),
     "dn_nn_conv3x3_backward": ([_vp, _vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _vp, _vp, _vp,
                                 _vp, _vp], _i),
+    "dn_nn_backward_scratch_bytes": ([ctypes.c_int64, _i], ctypes.c_int64),
+    "dn_nn_conv3x3_backward_tc": ([_vp, _vp, _vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _vp, _vp,
+                                   _vp, _vp, ctypes.c_int64, _vp], _i),
     "dn_nn_l1_loss": ([_vp, _vp, ctypes.c_int64, ctypes.c_float, _vp, _vp, _vp, _vp], _i),
     "dn_nn_adam": ([_vp, _vp, _vp, _vp, _i, _vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                     ctypes.c_float, ctypes.c_float, ctypes.c_float, _vp, _vp], _i),

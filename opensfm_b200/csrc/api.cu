@@ -205,7 +205,6 @@ struct Engine {
   float depth_range0 = 0.02f, normal_range0 = 0.5f;
   int sample_hp = 0;  // half-passes score one view per candidate (sample mode)
   int use_knight = 0;  // knight-move candidates in the half-passes
-  int paired = 1;      // sample mode: propagation candidates scored two at a time
   int active = 0;     // active-pixel half-passes
   float active_tol = 0.f;
   // Learned proposal (DN_RUN_LEARNED): network weights, the feature grid of
@@ -551,7 +550,6 @@ struct Engine {
     a.p.active = active;
     a.p.active_tol = active_tol;
     a.p.use_knight = use_knight;
-    a.p.paired = paired;
     return a;
   }
 
@@ -1601,13 +1599,6 @@ dn_status dn_batch_set_candidate_views(dn_batch* b, int mode) {
   b->eng.invalidate();
   return DN_OK;
 }
-dn_status dn_batch_set_paired_candidates(dn_batch* b, int on) {
-  const dn::DeviceRestore device_restore_;
-  DN_CHECK(b, "NULL batch");
-  b->eng.paired = on ? 1 : 0;
-  b->eng.invalidate();
-  return DN_OK;
-}
 dn_status dn_batch_set_knight_moves(dn_batch* b, int on) {
   const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
@@ -2001,6 +1992,38 @@ dn_status dn_nn_conv3x3_backward(const void* dy, const void* x, const void* w,
   c.db = db;
   DN_CUDA(dn::conv3x3_backward(c, static_cast<__nv_bfloat16*>(wt_scratch),
                                static_cast<cudaStream_t>(stream)));
+  return DN_OK;
+}
+int64_t dn_nn_backward_scratch_bytes(int64_t n_pix, int cout) {
+  // Flipped weights (32 x 288 BF16), then the gradient padded to 32 channels.
+  const int64_t w = (int64_t)32 * 288 * 2;
+  return cout == 32 ? w : w + n_pix * 32 * 2;
+}
+dn_status dn_nn_conv3x3_backward_tc(const void* dy, const void* x, const void* w,
+                                    const void* x_mask, int64_t n_pix, int H, int W, int cin,
+                                    int cout, void* dx, float* dw, float* db, void* scratch,
+                                    int64_t scratch_bytes, void* stream) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(dy && x && w && dw && db && scratch, "NULL argument");
+  DN_CHECK(nn_shape_ok(cin, cout), "supported shapes: cin 32, cout 32 or 4");
+  DN_CHECK(H > 0 && W > 0 && n_pix > 0 && n_pix % ((int64_t)H * W) == 0, "bad n_pix / H / W");
+  DN_CHECK(!dx || scratch_bytes >= dn_nn_backward_scratch_bytes(n_pix, cout),
+           "scratch smaller than dn_nn_backward_scratch_bytes");
+  dn::ConvArgs c{};
+  c.x = static_cast<const __nv_bfloat16*>(x);
+  c.w = static_cast<const __nv_bfloat16*>(w);
+  c.n_pix = n_pix;
+  c.H = H;
+  c.W = W;
+  c.cin = cin;
+  c.cout = cout;
+  c.dy = static_cast<const __nv_bfloat16*>(dy);
+  c.x_mask = static_cast<const __nv_bfloat16*>(x_mask);
+  c.dx = static_cast<__nv_bfloat16*>(dx);
+  c.dw = dw;
+  c.db = db;
+  __nv_bfloat16* wt = static_cast<__nv_bfloat16*>(scratch);
+  DN_CUDA(dn::conv3x3_backward_tc(c, wt, wt + 32 * 288, static_cast<cudaStream_t>(stream)));
   return DN_OK;
 }
 dn_status dn_nn_l1_loss(const float* pred, const float* target, int64_t n_pix,

@@ -87,9 +87,6 @@ struct RunParams {
   int use_near, use_far, n_refine;
   float depth_range0, normal_range0;
   int use_knight;  // the 8 knight-move pixels (+-1, +-2), (+-2, +-1) as candidates
-  // Sample mode: score the propagation candidates two at a time (the same
-  // acceptances, in the same order, as one at a time).
-  int paired;
   // Active pixels: from half-pass 2 on, a pixel is updated only if its own
   // depth or one of its 4 neighbours' depths moved at their last update
   // (MapDev::changed); otherwise its state is kept as it is.  A depth moves
@@ -718,66 +715,6 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
                         lo2(S3) + hi2(S3) + t3);
 }
 
-// Two candidates' walks at once (one view each, both inside the padded
-// table): the same per-sample arithmetic as coop_walk_fast, interleaved so
-// that the gathers of both walks are in flight together.  2 or 4 lanes per
-// pixel (two or more columns per lane).
-template <int L>
-__device__ inline float2 coop_walk_fast2(const CoopPatch<L>& cp, const ViewDev& va,
-                                         const Warp& wa, const ViewDev& vb, const Warp& wb) {
-  constexpr int C = CoopPatch<L>::C;
-  static_assert(C > 1, "one column per lane walks one view at a time");
-  constexpr int NP = C / 2;
-  const float dx0 = (float)(cp.lane - 3);
-  const float xla = fmaf(wa.ax, dx0, fmaf(wa.bx, -3.0f, wa.X0));
-  const float yla = fmaf(wa.ay, dx0, fmaf(wa.by, -3.0f, wa.Y0));
-  const float xlb = fmaf(wb.ax, dx0, fmaf(wb.bx, -3.0f, wb.X0));
-  const float ylb = fmaf(wb.ay, dx0, fmaf(wb.by, -3.0f, wb.Y0));
-  const u64 MMa = pk2(va.magic, va.magic), MMb = pk2(vb.magic, vb.magic);
-  const unsigned TPa = (unsigned)va.TP, TPb = (unsigned)vb.TP;
-  const uint2* __restrict__ q0a = va.quad0;
-  const uint2* __restrict__ q0b = vb.quad0;
-  const float nsha = -patch_shift<false>(va, wa), nshb = -patch_shift<false>(vb, wb);
-  u64 S1a = 0ull, S2a = 0ull, S3a = 0ull, S1b = 0ull, S2b = 0ull, S3b = 0ull;
-  u64 Xa[NP], Ya[NP], Xb[NP], Yb[NP];
-#pragma unroll
-  for (int m = 0; m < NP; ++m) {
-    const float c0 = coop_col<L>(cp.lane, 2 * m), c1 = coop_col<L>(cp.lane, 2 * m + 1);
-    Xa[m] = pk2(fmaf(wa.ax, c0, xla), fmaf(wa.ax, c1, xla));
-    Ya[m] = pk2(fmaf(wa.ay, c0, yla), fmaf(wa.ay, c1, yla));
-    Xb[m] = pk2(fmaf(wb.ax, c0, xlb), fmaf(wb.ax, c1, xlb));
-    Yb[m] = pk2(fmaf(wb.ay, c0, ylb), fmaf(wb.ay, c1, ylb));
-  }
-  const u64 BXa = pk2(wa.bx, wa.bx), BYa = pk2(wa.by, wa.by);
-  const u64 BXb = pk2(wb.bx, wb.bx), BYb = pk2(wb.by, wb.by);
-#pragma unroll
-  for (int r = 0; r < 7; ++r) {
-#pragma unroll
-    for (int m = 0; m < NP; ++m) {
-      const u64 YYa = sample_pair(Xa[m], Ya[m], MMa, TPa, q0a, nsha);
-      const u64 YYb = sample_pair(Xb[m], Yb[m], MMb, TPb, q0b, nshb);
-      const int k = r * NP + m;
-      const u64 WYa = mul2(cp.w2[k], YYa), WYb = mul2(cp.w2[k], YYb);
-      S1a = add2(S1a, WYa);
-      S2a = fma2(WYa, YYa, S2a);
-      S3a = fma2(cp.wx2[k], YYa, S3a);
-      S1b = add2(S1b, WYb);
-      S2b = fma2(WYb, YYb, S2b);
-      S3b = fma2(cp.wx2[k], YYb, S3b);
-      if (r < 6) {
-        Xa[m] = add2(Xa[m], BXa);
-        Ya[m] = add2(Ya[m], BYa);
-        Xb[m] = add2(Xb[m], BXb);
-        Yb[m] = add2(Yb[m], BYb);
-      }
-    }
-  }
-  return make_float2(coop_finish<L>(cp, lo2(S1a) + hi2(S1a), lo2(S2a) + hi2(S2a),
-                                    lo2(S3a) + hi2(S3a)),
-                     coop_finish<L>(cp, lo2(S1b) + hi2(S1b), lo2(S2b) + hi2(S2b),
-                                    lo2(S3b) + hi2(S3b)));
-}
-
 template <int L>
 __device__ inline Warp bcast_warp(const Warp& w, unsigned mask, int src) {
   Warp o;
@@ -850,13 +787,6 @@ struct Patch<HPZ, 1> {
                         unsigned& taps) const {
     return ncc_view<HPZ>(rp, vw, pr, h, j, i, taps);
   }
-  // Two candidates, each against one view (scored one after the other).
-  __device__ float2 view2(const ViewDev& va, const PairDev& pa, const Hyp& ha, const ViewDev& vb,
-                          const PairDev& pb, const Hyp& hb, float j, float i,
-                          unsigned& taps) const {
-    const float sa = ncc_view<HPZ>(rp, va, pa, ha, j, i, taps);
-    return make_float2(sa, ncc_view<HPZ>(rp, vb, pb, hb, j, i, taps));
-  }
   __device__ float max(const ViewDev* views, const PairDev* pairs, int n, const Hyp& h, float j,
                        float i, int& best_view, unsigned& taps) const {
     return ncc_max<HPZ>(rp, views, pairs, n, h, j, i, best_view, taps);
@@ -872,22 +802,6 @@ struct CoopIface {
   __device__ float view(const ViewDev& vw, const PairDev& pr, const Hyp& h, float j, float i,
                         unsigned& taps) const {
     return coop_ncc_view<L>(cp, vw, pr, h, j, i, taps);
-  }
-  // Two candidates, each against one view: interleaved walks when both
-  // patches lie inside the padded tables, otherwise one after the other.
-  __device__ float2 view2(const ViewDev& va, const PairDev& pa, const Hyp& ha, const ViewDev& vb,
-                          const PairDev& pb, const Hyp& hb, float j, float i,
-                          unsigned& taps) const {
-    const Warp wa = warp_setup<3>(va, pa, ha, j, i);
-    const Warp wb = warp_setup<3>(vb, pb, hb, j, i);
-    if constexpr (CoopPatch<L>::C > 1) {
-      if (wa.mode == kFast && wb.mode == kFast) {
-        if (cp.lane == 0) taps += 98;
-        return coop_walk_fast2<L>(cp, va, wa, vb, wb);
-      }
-    }
-    const float sa = coop_eval<L>(cp, va, wa, taps);
-    return make_float2(sa, coop_eval<L>(cp, vb, wb, taps));
   }
   __device__ float max(const ViewDev* views, const PairDev* pairs, int n, const Hyp& h, float j,
                        float i, int& best_view, unsigned& taps) const {

@@ -368,28 +368,11 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
     const int n_knight = p.use_knight ? 8 : 0;
     const int first_refine = 8 + n_knight;
     const int n_slots = first_refine + p.n_refine;
-    // Sample mode, paired: a propagation candidate waits here for a second
-    // one, then both are scored together and accepted in slot order.
-    bool has_pend = false;
-    float3 pend_v = make_float3(0.f, 0.f, 0.f);
-    int pend_view = 0;
-    auto accept = [&](float3 v, int nb, float s) {
-      if (s > cur) {
-        cur = s;
-        curn = nb;
-        cv = v;
-        cd = depth_of_plane(j, i, m.Kinv_d, v);
-      }
-    };
 #pragma unroll 1
     for (int slot = 0; slot < n_slots; ++slot) {
       float3 v = make_float3(0.f, 0.f, 0.f);
       int view = 0;
       bool valid = false;
-      if (SAMPLE && has_pend && slot >= first_refine) {
-        try_plane(pend_v, pend_view);
-        has_pend = false;
-      }
       if (slot < 4 && !p.use_near) continue;
       if (slot >= 4 && slot < 8 && !p.use_far) continue;
       if (slot >= 8 && slot < first_refine) {
@@ -453,40 +436,8 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
           normal_range *= 0.8f;
         }
       }
-      if (!valid) continue;
-      if (SAMPLE && p.paired && slot < first_refine) {
-        // The same decisions as try_plane one candidate at a time: a
-        // candidate with no usable view, or equal to the current plane, is
-        // not scored; a pair is scored against the state before it and
-        // accepted in order.
-        if (view < 1 || view > m.n_pairs) continue;
-        if (!has_pend) {
-          if (same_plane(v, cv)) continue;
-          pend_v = v;
-          pend_view = view;
-          has_pend = true;
-          continue;
-        }
-        if (same_plane(v, cv)) {
-          // Equal to the current plane now, but maybe not once the waiting
-          // candidate is accepted: one at a time.
-          try_plane(pend_v, pend_view);
-          has_pend = false;
-          try_plane(v, view);
-          continue;
-        }
-        const Hyp ha = make_hyp(m.Kinv, pend_v, fj, fi), hb = make_hyp(m.Kinv, v, fj, fi);
-        const PairDev& pa = mp[pend_view - 1];
-        const PairDev& pb = mp[view - 1];
-        const float2 sc = pt.view2(sv[pa.view], pa, ha, sv[pb.view], pb, hb, fj, fi, taps);
-        accept(pend_v, pend_view, sc.x);
-        if (!same_plane(v, cv)) accept(v, view, sc.y);
-        has_pend = false;
-        continue;
-      }
-      try_plane(v, view);
+      if (valid) try_plane(v, view);
     }
-    if (SAMPLE && has_pend) try_plane(pend_v, pend_view);
     if (SAMPLE && m.n_pairs >= 2) {
       // A random other matching view for the current plane.
       const uint4 r = philox4x32_10(make_uint4((uint32_t)pix, (uint32_t)tl.x, (uint32_t)p.pass, 6u),

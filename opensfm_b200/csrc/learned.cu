@@ -334,7 +334,8 @@ template <int NP>
 __global__ void __launch_bounds__(128, 4)
 conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ w,
                       const float* __restrict__ bias, int H, int W, int cout, int relu,
-                      __nv_bfloat16* __restrict__ y, float* __restrict__ y32, long long n_tiles) {
+                      __nv_bfloat16* __restrict__ y, float* __restrict__ y32, long long n_tiles,
+                      const __nv_bfloat16* __restrict__ mask) {
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* halo = smem;                    // 2 x [4 planes][kHR][kHC][16 B]
@@ -421,11 +422,18 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
         uint32_t o[16];
 #pragma unroll
         for (int c = 0; c < 16; ++c) {
-          float v0 = __uint_as_float(r[2 * c]) + bias[2 * c];
-          float v1 = __uint_as_float(r[2 * c + 1]) + bias[2 * c + 1];
+          float v0 = __uint_as_float(r[2 * c]) + (bias ? bias[2 * c] : 0.f);
+          float v1 = __uint_as_float(r[2 * c + 1]) + (bias ? bias[2 * c + 1] : 0.f);
           if (relu) {
             v0 = fmaxf(v0, 0.f);
             v1 = fmaxf(v1, 0.f);
+          }
+          if (mask) {
+            // The gradient of a ReLU input: zero where the activation is not
+            // positive (backward-data through the layer below's ReLU).
+            const __nv_bfloat162 mk = *reinterpret_cast<const __nv_bfloat162*>(mask + p * 32 + 2 * c);
+            if (!(__low2float(mk) > 0.f)) v0 = 0.f;
+            if (!(__high2float(mk) > 0.f)) v1 = 0.f;
           }
           o[c] = pack2(__float2bfloat16_rn(v0), __float2bfloat16_rn(v1));
         }
@@ -438,14 +446,14 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
         if (y32)
 #pragma unroll
           for (int c = 0; c < 32; ++c) {
-            const float v = __uint_as_float(r[c]) + bias[c];
+            const float v = __uint_as_float(r[c]) + (bias ? bias[c] : 0.f);
             y32[p * 32 + c] = relu ? fmaxf(v, 0.f) : v;
           }
       } else {
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           if (c >= cout) break;
-          float v = __uint_as_float(r[c]) + bias[c];
+          float v = __uint_as_float(r[c]) + (bias ? bias[c] : 0.f);
           if (relu) v = fmaxf(v, 0.f);
           if (y) y[p * cout + c] = __float2bfloat16_rn(v);
           if (y32) y32[p * cout + c] = v;
@@ -537,6 +545,225 @@ __global__ void transpose_weights_kernel(const __nv_bfloat16* __restrict__ w, in
   if (k >= n) return;
   const int ci = k / (9 * coutp), r = k - ci * 9 * coutp, tap = r / coutp, co = r - tap * coutp;
   wt[k] = co < cout ? w[(size_t)co * 9 * cin + tap * cin + ci] : __float2bfloat16(0.f);
+}
+
+// ------------------------------------------ conv backward-weight, tcgen05
+// dw[co][tap * 32 + ci] += sum_p g[p][co] x[p + off(tap)][ci] and
+// db[co] += sum_p g[p][co], off(tap) = (tap / 3 - 1, tap % 3 - 1), as a
+// split-K GEMM on the tensor cores.  A CTA walks tiles of 16 x 8 pixels
+// (K = 128 per tile) and keeps three 128 x N FP32 accumulators in tensor
+// memory, one per vertical offset dy = d - 1:
+//   D_d[m = (dxs, ci)][n = co] += sum_k A_d[m][k] B[n][k],
+//   A_d[(dxs, ci)][(r, c)] = x[y0 + r + d - 1][x0 + c + dxs - 1][ci] (dxs < 3),
+//   B[co][(r, c)] = g[y0 + r][x0 + c][co],
+// so D_d row (dxs, ci), column co is dw[co][(3 d + dxs) * 32 + ci].  Row
+// block dxs = 3 of A stays zero (M = 128 = 4 x 32).  Operands are staged in
+// shared memory in the canonical no-swizzle K-major layout (a core matrix is
+// 8 rows of 8 K-elements, 16 bytes a row, 128 contiguous bytes):
+//   A: halo row hr (18 rows) x [dxs 4][ci 32][8 px]: 8-row groups 128 B
+//      apart (SBO), the two K-halves of an MMA (tile rows 2c and 2c + 1)
+//      one halo row (2048 B) apart (LBO); A_d of K-chunk c starts at halo
+//      row 2c + d;
+//   B: tile row r (16) x [co N][8 px]: SBO 128 B, LBO N x 16 B.
+// x is NHWC BF16 with 32 channels, g NHWC BF16 with ldg channels per pixel
+// of which the first cout are used.  Two operand buffers: the loads of tile
+// t + 1 overlap the MMAs of tile t.  Each CTA adds its sums to dw and db
+// once, at the end, with atomics.  Waits are bounded (tc::kSpins); an
+// expired wait sets tc::g_error and the CTA stops.
+namespace tcw {
+constexpr int kTR = 16, kTC = 8, kHR = kTR + 2;
+constexpr int kARow = 4 * 32 * 16;    // one halo row of A: 2048 bytes
+constexpr int kABytes = kHR * kARow;  // 36864 bytes
+__host__ __device__ constexpr int b_row(int n) { return n * 16; }
+__host__ __device__ constexpr int buf_bytes(int n) { return kABytes + kTR * b_row(n); }
+constexpr size_t smem_bytes(int n) { return 2 * (size_t)buf_bytes(n) + 64; }
+}  // namespace tcw
+
+template <int N>
+__global__ void __launch_bounds__(128, 2)
+conv3x3_bwd_weight_tc_kernel(const __nv_bfloat16* __restrict__ g, int ldg, int cout,
+                             const __nv_bfloat16* __restrict__ x, int H, int W,
+                             long long n_tiles, float* __restrict__ dw, float* __restrict__ db) {
+  using namespace tc;
+  static_assert(N == 16 || N == 32, "N: output channels padded to 16 or 32");
+  static_assert(tcw::kTR == tc::kTR && tcw::kTC == tc::kTC, "the forward's tiling");
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + 2 * tcw::buf_bytes(N));
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int e = tid; e < 2 * tcw::buf_bytes(N) / 16; e += blockDim.x)
+    reinterpret_cast<uint4*>(smem)[e] = make_uint4(0u, 0u, 0u, 0u);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mbar + 1)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;\n" ::"r"(
+                     smem_u32(tslot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+  // db: the B loads of thread tid always carry channel tid % N (the block's
+  // 128 threads are a multiple of N), so each thread sums one channel.
+  float bsum = 0.f;
+
+  auto load_tile = [&](long long t, int b) {
+    unsigned char* A = smem + b * tcw::buf_bytes(N);
+    unsigned char* Bm = A + tcw::kABytes;
+    const TileXY tt = tile_xy(t, H, W);
+    for (int e = tid; e < tcw::kHR * 3 * 32; e += blockDim.x) {
+      const int ci = e & 31, q = e >> 5, dxs = q % 3, hr = q / 3;
+      const int y = tt.y0 - 1 + hr;
+      uint32_t pk[4];
+#pragma unroll
+      for (int c2 = 0; c2 < 4; ++c2) {
+        __nv_bfloat16 v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int xx = tt.x0 + 2 * c2 + h + dxs - 1;
+          const bool in = y >= 0 && y < H && xx >= 0 && xx < W;
+          v[h] = in ? x[((tt.img * H + y) * (long long)W + xx) * 32 + ci] : __float2bfloat16(0.f);
+        }
+        pk[c2] = pack2(v[0], v[1]);
+      }
+      *reinterpret_cast<uint4*>(A + hr * tcw::kARow + (dxs * 32 + ci) * 16) =
+          make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+    for (int e = tid; e < tcw::kTR * N; e += blockDim.x) {
+      const int co = e % N, r = e / N;
+      const int y = tt.y0 + r;
+      uint32_t pk[4];
+#pragma unroll
+      for (int c2 = 0; c2 < 4; ++c2) {
+        __nv_bfloat16 v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int xx = tt.x0 + 2 * c2 + h;
+          const bool in = co < cout && y < H && xx < W;
+          v[h] = in ? g[((tt.img * H + y) * (long long)W + xx) * ldg + co] : __float2bfloat16(0.f);
+          bsum += __bfloat162float(v[h]);
+        }
+        pk[c2] = pack2(v[0], v[1]);
+      }
+      *reinterpret_cast<uint4*>(Bm + r * tcw::b_row(N) + co * 16) =
+          make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+  };
+
+  constexpr uint32_t idesc = idesc_bf16(N);
+  uint32_t phase[2] = {0u, 0u};
+  bool pending[2] = {false, false};
+  bool ok = true, first = true;
+  int buf = 0;
+  long long t = blockIdx.x;
+  if (t < n_tiles) load_tile(t, 0);
+  for (; t < n_tiles && ok; t += gridDim.x) {
+    // The generic-proxy stores of this buffer become visible to the tensor
+    // core; then one thread issues the tile's 24 MMAs.
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t a_base = smem_u32(smem + buf * tcw::buf_bytes(N));
+      const uint32_t b_base = a_base + tcw::kABytes;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const uint64_t bd =
+            smem_desc(b_base + (uint32_t)(2 * c * tcw::b_row(N)), tcw::b_row(N), 128);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const uint64_t ad =
+              smem_desc(a_base + (uint32_t)((2 * c + d) * tcw::kARow), tcw::kARow, 128);
+          const uint32_t acc = (first && c == 0) ? 0u : 1u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
+                  tmem + (uint32_t)(d * N)),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+              : "memory");
+        }
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+              smem_u32(mbar + buf))
+          : "memory");
+    }
+    pending[buf] = true;
+    first = false;
+    const long long tn = t + gridDim.x;
+    const int nb = buf ^ 1;
+    if (tn < n_tiles) {
+      if (pending[nb]) {
+        // The MMAs that last read buffer nb must be done before it is reused.
+        bool done = mbar_wait(smem_u32(mbar + nb), phase[nb]);
+        if (!done) done = mbar_wait(smem_u32(mbar + nb), phase[nb]);
+        phase[nb] ^= 1u;
+        pending[nb] = false;
+        ok = __syncthreads_and(done) != 0;
+        if (!ok) break;
+      }
+      load_tile(tn, nb);
+    }
+    buf = nb;
+  }
+  for (int b = 0; b < 2; ++b) {
+    if (!pending[b]) continue;
+    bool done = mbar_wait(smem_u32(mbar + b), phase[b]);
+    if (!done) done = mbar_wait(smem_u32(mbar + b), phase[b]);
+    ok = ok && done;
+  }
+  ok = __syncthreads_and(ok) != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (ok && !first) {
+    if (warp < 3) {  // warp 3's TMEM lanes hold the zero row block
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        uint32_t r[N];
+        tmem_load<N>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * N), r);
+        const int tap = 3 * d + warp, ci = lane;
+#pragma unroll
+        for (int co = 0; co < N; ++co)
+          if (co < cout) atomicAdd(dw + (size_t)co * 288 + tap * 32 + ci, __uint_as_float(r[co]));
+      }
+    }
+    const int co = tid % N;
+    if (co < cout && bsum != 0.f) atomicAdd(db + co, bsum);
+  }
+  if (!ok && tid == 0) atomicExch(&g_error, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;\n" ::"r"(tmem) : "memory");
+}
+
+// Backward-data weights for the forward tcgen05 kernel: the gradient of a
+// layer's input is conv3x3(g, w') with w'[ci][tap * 32 + co] =
+// w[co][(8 - tap) * 32 + ci] (taps flipped, channels swapped) for co < cout,
+// zero for co >= cout (g padded to 32 channels).
+__global__ void flip_weights_kernel(const __nv_bfloat16* __restrict__ w, int cout,
+                                    __nv_bfloat16* __restrict__ wf) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 32 * 288) return;
+  const int ci = k / 288, r = k - ci * 288, tap = r / 32, co = r - tap * 32;
+  wf[k] = co < cout ? w[(size_t)co * 288 + (8 - tap) * 32 + ci] : __float2bfloat16(0.f);
+}
+
+// [n][cin] -> [n][32] with zeros after channel cin.
+__global__ void pad_channels_kernel(const __nv_bfloat16* __restrict__ src, int cin, long long n,
+                                    __nv_bfloat16* __restrict__ dst) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= n * 32) return;
+  const long long p = k >> 5;
+  const int c = (int)(k & 31);
+  dst[k] = c < cin ? src[p * cin + c] : __float2bfloat16(0.f);
 }
 
 // ----------------------------------------------------- conv backward-weight
@@ -816,7 +1043,7 @@ static cudaError_t conv_fwd_tc(const ConvArgs& c, cudaStream_t s) {
   const long long tiles = n_img * ((c.H + tc::kTR - 1) / tc::kTR) * ((c.W + tc::kTC - 1) / tc::kTC);
   const long long grid = std::min<long long>(tiles, (long long)std::max(per_sm, 1) * sms);
   kern<<<(unsigned)grid, 128, smem, s>>>(c.x, c.w, c.bias, c.H, c.W, c.cout, c.relu, c.y, c.y32,
-                                         tiles);
+                                         tiles, c.x_mask);
   return cudaGetLastError();
 }
 
@@ -845,6 +1072,55 @@ cudaError_t conv3x3_backward(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaS
   if (c.cin == 32 && c.cout == 32) return conv_bwd_t<32, 32>(c, wt_scratch, s);
   if (c.cin == 32 && c.cout == 4) return conv_bwd_t<32, 4>(c, wt_scratch, s);
   return cudaErrorInvalidValue;
+}
+
+template <int N>
+static cudaError_t conv_bwd_weight_tc(const ConvArgs& c, cudaStream_t s) {
+  auto kern = conv3x3_bwd_weight_tc_kernel<N>;
+  const size_t smem = tcw::smem_bytes(N);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long n_img = c.n_pix / ((long long)c.H * c.W);
+  const long long tiles = n_img * ((c.H + tc::kTR - 1) / tc::kTR) * ((c.W + tc::kTC - 1) / tc::kTC);
+  // Two CTAs per SM: each adds its sums to dw once, so fewer CTAs also
+  // means fewer atomics.
+  const long long grid = std::min<long long>(tiles, 2LL * sms);
+  if (grid <= 0) return cudaSuccess;
+  kern<<<(unsigned)grid, 128, smem, s>>>(c.dy, c.cout, c.cout, c.x, c.H, c.W, tiles, c.dw, c.db);
+  return cudaGetLastError();
+}
+
+cudaError_t conv3x3_backward_tc(const ConvArgs& c, __nv_bfloat16* wt_scratch,
+                                __nv_bfloat16* dy_pad, cudaStream_t s) {
+  if (c.cin != 32 || (c.cout != 32 && c.cout != 4)) return cudaErrorInvalidValue;
+  cudaError_t e = c.cout == 32 ? conv_bwd_weight_tc<32>(c, s) : conv_bwd_weight_tc<16>(c, s);
+  if (e != cudaSuccess || !c.dx) return e;
+  // Backward-data: the forward kernel on the gradient (32 channels) with the
+  // flipped weights, no bias, the ReLU mask of the layer's input.
+  flip_weights_kernel<<<(32 * 288 + 255) / 256, 256, 0, s>>>(c.w, c.cout, wt_scratch);
+  const __nv_bfloat16* g32 = c.dy;
+  if (c.cout != 32) {
+    pad_channels_kernel<<<(unsigned)((c.n_pix * 32 + 255) / 256), 256, 0, s>>>(c.dy, c.cout,
+                                                                               c.n_pix, dy_pad);
+    g32 = dy_pad;
+  }
+  ConvArgs f{};
+  f.x = g32;
+  f.w = wt_scratch;
+  f.bias = nullptr;
+  f.n_pix = c.n_pix;
+  f.H = c.H;
+  f.W = c.W;
+  f.cin = 32;
+  f.cout = 32;
+  f.relu = 0;
+  f.y = c.dx;
+  f.x_mask = c.x_mask;
+  return conv_fwd_tc<32>(f, s);
 }
 template <int L, int S>
 static cudaError_t sweep_l(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,

@@ -33,6 +33,12 @@ cudaError_t conv3x3_forward_mma_sync(const ConvArgs& c, cudaStream_t s);
 // (and clears it), 0 if not, -1 if the flag could not be read.
 int take_tc_error();
 cudaError_t conv3x3_backward(const ConvArgs& c, __nv_bfloat16* wt_scratch, cudaStream_t s);
+// The same backward on the tcgen05 tensor cores: weight and bias gradients
+// as a split-K GEMM with TMEM accumulators, the input gradient as the
+// forward kernel on the gradient with flipped weights and the ReLU mask.
+// wt_scratch: 32 x 288 BF16; dy_pad: n_pix x 32 BF16 when cout != 32.
+cudaError_t conv3x3_backward_tc(const ConvArgs& c, __nv_bfloat16* wt_scratch,
+                                __nv_bfloat16* dy_pad, cudaStream_t s);
 // Sweep features on the grid of every `stride`-th pixel (1 or 2); map k's
 // grid at feat + k map_stride, or at its MapDev::prop_off when map_stride < 0.
 cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map_stride,

@@ -135,12 +135,20 @@ class ProposalNet:
                 acts.append(y)
         return (out32, acts) if keep else out32
 
-    def backward(self, acts, dpred, n_pix: int, H: int, W: int):
-        """Gradients (FP32, summed over pixels) of every layer's weights and biases."""
+    def backward(self, acts, dpred, n_pix: int, H: int, W: int, tensor_cores: bool = True):
+        """Gradients (FP32, summed over pixels) of every layer's weights and
+        biases.  tensor_cores: the tcgen05 kernels (weight gradient as a
+        split-K GEMM in tensor memory, data gradient as the forward kernel on
+        flipped weights); False: the mma.sync kernels."""
         torch = _torch()
         L = _lib.load()
         dws = [torch.zeros_like(w) for w in self.w32]
         dbs = [torch.zeros_like(b) for b in self.b32]
+        if tensor_cores:
+            need = int(L.dn_nn_backward_scratch_bytes(n_pix, LAYERS[-1][1]))
+            scratch = getattr(self, "bwd_scratch", None)
+            if scratch is None or scratch.numel() < need:
+                scratch = self.bwd_scratch = torch.empty(need, dtype=torch.uint8, device="cuda")
         dy = dpred
         for k in range(len(LAYERS) - 1, -1, -1):
             cin, cout, relu = LAYERS[k]
@@ -148,10 +156,16 @@ class ProposalNet:
             need_dx = k > 0
             dx = torch.empty(n_pix * cin, dtype=torch.bfloat16, device="cuda") if need_dx else None
             # dx is masked by the ReLU of the layer below (its output x > 0).
-            _lib.check(L.dn_nn_conv3x3_backward(
-                _ptr(dy), _ptr(x), _ptr(self.w16[k]), _ptr(x) if need_dx else None, n_pix, H, W,
-                cin, cout, _ptr(dx) if need_dx else None, _ptr(dws[k]), _ptr(dbs[k]),
-                _ptr(self.wt_scratch), _stream()))
+            if tensor_cores:
+                _lib.check(L.dn_nn_conv3x3_backward_tc(
+                    _ptr(dy), _ptr(x), _ptr(self.w16[k]), _ptr(x) if need_dx else None, n_pix, H,
+                    W, cin, cout, _ptr(dx) if need_dx else None, _ptr(dws[k]), _ptr(dbs[k]),
+                    _ptr(scratch), scratch.numel(), _stream()))
+            else:
+                _lib.check(L.dn_nn_conv3x3_backward(
+                    _ptr(dy), _ptr(x), _ptr(self.w16[k]), _ptr(x) if need_dx else None, n_pix, H,
+                    W, cin, cout, _ptr(dx) if need_dx else None, _ptr(dws[k]), _ptr(dbs[k]),
+                    _ptr(self.wt_scratch), _stream()))
             dy = dx
         return dws, dbs
 

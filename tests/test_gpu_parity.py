@@ -931,32 +931,3 @@ def test_bounded_wait_expiry_reports_timeout():
     b.synchronize()
     assert (b.get_depth(0) > 0).any()
 
-
-@pytest.mark.parametrize("mode", [1, 2])
-def test_paired_candidates_match_one_at_a_time(scene, mode):
-    """One view per candidate: scoring the propagation candidates two at a
-    time (interleaved walks) gives the same maps as scoring them one at a
-    time -- the same acceptances in the same order."""
-    from opensfm_b200 import _lib
-
-    Ks, Rs, ts = cams(scene)
-    b = pydense.Batch()
-    for K, R, t, im in zip(Ks, Rs, ts, scene.images):
-        b.add_view(K, R, t, im)
-    n = len(scene.images)
-    for v in range(n):
-        b.add_depthmap(v, [o for o in range(n) if o != v][:4], *S.depth_range(scene.depths[v]))
-    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=3, seed=9)
-    b.set_candidate_views(mode)
-    b.set_schedule(half_passes=8)
-    b.set_active_pixels(True, 0.003)
-    out = []
-    for paired in (1, 0):
-        _lib.check(b._L.dn_batch_set_paired_candidates(b._h, paired))
-        b.run()
-        b.synchronize()
-        out.append([b.get(v) for v in range(n)])
-    for v in range(n):
-        for a, w in zip(out[0][v], out[1][v]):
-            assert np.array_equal(a, w)
-    assert (out[0][0][0] > 0).mean() > 0.3
