@@ -422,6 +422,10 @@ dn_status dn_gpu_cleaner_set_same_depth_threshold(dn_gpu_cleaner* c, float t);
 dn_status dn_gpu_cleaner_set_min_consistent_views(dn_gpu_cleaner* c, int n);
 dn_status dn_gpu_cleaner_set_carving_threshold(dn_gpu_cleaner* c, float t);
 dn_status dn_gpu_cleaner_set_max_carved_views(dn_gpu_cleaner* c, int n);
+/* The device the cleaner's views and kernels live on (default: the current
+ * device at create).  Keeps the settings above.  Only before the first
+ * add_view, or after dn_gpu_cleaner_clear; DN_INVALID_ARG otherwise. */
+dn_status dn_gpu_cleaner_set_device(dn_gpu_cleaner* c, int device);
 /* AddView (cleaner.cc:39-54): depth f32 [height][stride]; *id (may be NULL)
  * receives the view index. */
 dn_status dn_gpu_cleaner_add_view(dn_gpu_cleaner* c, const double K[9], const double R[9],

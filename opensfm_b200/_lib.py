@@ -113,6 +113,7 @@ _SIGNATURES = {
     "dn_gpu_cleaner_set_min_consistent_views": ([_vp, _i], _i),
     "dn_gpu_cleaner_set_carving_threshold": ([_vp, ctypes.c_float], _i),
     "dn_gpu_cleaner_set_max_carved_views": ([_vp, _i], _i),
+    "dn_gpu_cleaner_set_device": ([_vp, _i], _i),
     "dn_gpu_cleaner_add_view": ([_vp, _d, _d, _d, _f, _i, _i, _i, ctypes.POINTER(_i)], _i),
     "dn_gpu_cleaner_clean": ([_vp, _i, _i32, _i, _f], _i),
     "dn_gpu_cleaner_clear": ([_vp], _i),

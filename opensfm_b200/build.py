@@ -34,22 +34,31 @@ def _stale(target, deps):
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
+    """Compiles the sources whose object is older than the source or any
+    shared header (all of them in parallel), then links the library."""
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [
+    headers = [os.path.join(CSRC, h) for h in HEADERS] + [
         os.path.join(ROOT, "include", "dense_b200.h")]
-    if not force and not _stale(LIB, deps):
+    if not force and not _stale(LIB, srcs + headers):
         return LIB
-    objs = []
-    for s in srcs:
-        o = os.path.join(os.path.dirname(LIB), os.path.basename(s) + ".o")
+    objs = [os.path.join(os.path.dirname(LIB), os.path.basename(s) + ".o") for s in srcs]
+
+    def compile_one(so):
+        s, o = so
+        if not force and not _stale(o, [s] + headers):
+            return
         cmd = [NVCC, *ARCH, *FLAGS, *FILE_FLAGS.get(os.path.basename(s), []), "-c", s, "-o", o]
         if ptxas_v:
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)
-        objs.append(o)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        list(ex.map(compile_one, zip(srcs, objs)))
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
     subprocess.check_call(cmd)
     return LIB

@@ -1237,6 +1237,21 @@ dn_status dn_gpu_cleaner_set_max_carved_views(dn_gpu_cleaner* c, int n) {
   c->max_carved = std::max(0, n);  // cleaner.cc:35-37
   return DN_OK;
 }
+dn_status dn_gpu_cleaner_set_device(dn_gpu_cleaner* c, int device) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(c, "NULL cleaner");
+  DN_CHECK(device >= 0 && device < dn_device_count(), "device index out of range");
+  DN_CHECK(c->views.empty(), "set_device must come before the first add_view");
+  if (device == c->device) return DN_OK;
+  DN_CUDA(cudaSetDevice(c->device));
+  c->d_out.release();
+  if (c->stream) DN_CUDA(cudaStreamDestroy(c->stream));
+  c->stream = nullptr;
+  DN_CUDA(cudaSetDevice(device));
+  DN_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  c->device = device;
+  return DN_OK;
+}
 dn_status dn_gpu_cleaner_add_view(dn_gpu_cleaner* c, const double* K, const double* R,
                                   const double* t, const float* depth, int width, int height,
                                   int stride, int* id) {

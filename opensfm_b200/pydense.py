@@ -242,9 +242,7 @@ class GPUDepthmapCleaner(_Handle):
         one OpenCL device per cleaner)."""
         if self._shapes:
             raise ValueError("set_device must come before the first add_view")
-        check(self._L.dn_set_device(int(device)))
-        self.close()
-        super().__init__("dn_gpu_cleaner_create", "dn_gpu_cleaner_destroy")
+        check(self._L.dn_gpu_cleaner_set_device(self._h, int(device)))
 
     def add_view(self, K, R, t, depth) -> None:
         K = _mat(K, (3, 3), "K")

@@ -430,6 +430,7 @@ def test_gpu_cleaner_bit_identical_to_fp32_oracle(golden, scene, thr, min_views,
         c.set_min_consistent_views(min_views)
         c.set_carving_threshold(carving)
         c.set_max_carved_views(max_carved)
+        c.set_device(0)  # moves the cleaner and keeps the settings above
         for k in range(len(D)):
             c.add_view(K[k], R[k], t[k], D[k])
         for ref in range(len(D)):
