@@ -51,8 +51,14 @@ FLOPS_PER_TAP = 25  # affine warp 8 + bilinear 11 + NCC sums 6 (FMA = 2)
 # (half-passes, active-pixel threshold, knight moves), each after the
 # proposal network's initialisation with one view per candidate.
 PLAIN_HALF_PASSES, PLAIN_KNIGHTS = 2 * ITERS, False
-LEARNED_SCHEDULES = ((8, 0.003, False), (10, 0.003, False), (12, 0.003, False),
-                     (16, 0.003, False), (20, 0.003, False))
+# Learned schedules (half-passes, refinements per update, active-pixel
+# tolerance, candidate-view mode), in the order of their time on 12
+# held-out 640x480 scenes (seeds 900000-900011) among those that reached the
+# plain schedule's accuracy there: one view per candidate from the
+# initialisation on (mode 2), pixels whose neighbourhood moved by less than
+# 1 % left alone, 3 refinements.  The last two are the slower fallbacks.
+LEARNED_SCHEDULES = ((10, 3, 0.01, 2), (12, 3, 0.01, 2), (10, 4, 0.01, 2), (12, 4, 0.01, 2),
+                     (8, 6, 0.01, 2), (12, 6, 0.01, 1), (16, 6, 0.003, 1))
 
 
 # ---------------------------------------------------------------- workload
@@ -94,8 +100,9 @@ def schedules():
     from opensfm_b200.learned import Schedule
 
     plain = Schedule("plain", "plain", PLAIN_HALF_PASSES, {}, knights=PLAIN_KNIGHTS)
-    learned = [Schedule(f"learned-sample-{hp}hp-active{int(a * 1000)}", "learned", hp, {},
-                        sample=1, active=a, knights=kn) for hp, a, kn in LEARNED_SCHEDULES]
+    learned = [Schedule(f"learned-{hp}hp-refine{nr}-active{a:g}-views{mode}", "learned", hp,
+                        {} if nr == 6 else {"n_refine": nr}, sample=mode, active=a)
+               for hp, nr, a, mode in LEARNED_SCHEDULES]
     return plain, learned
 
 
@@ -733,7 +740,9 @@ def run_ours(args):
         acc = map_accuracy(b, vs, n_maps)
         ms = group.max(timed_runs(b, args.steps, learned, group))
         return {"schedule": sch.name, "half_passes": sch.half_passes,
-                "candidate_views": ["all", "one per candidate", "sample"][sch.sample],
+                "candidate_views": ["all", "one per candidate after a full initialisation",
+                                    "one per candidate (ComputePatchMatchSample)"][sch.sample],
+                "refinements": sch.kw.get("n_refine", 6),
                 "knight_moves": sch.knights, "active_pixels": sch.active,
                 "value": replica_throughput(world, n_maps, args.steps, ms),
                 "ms_per_step": ms / args.steps, "accuracy_1pct_median": acc[0],
@@ -902,10 +911,14 @@ def run_ours(args):
     # layers, plane install), then init + half-passes + post, one cleaner
     # launch and three pruner launches over all maps -- or, with the
     # persistent choice, one launch for all of PatchMatch, cleaner and pruner.
+    # An active half-pass from the third on is five launches: the per-tile
+    # counts, their scan per map, the pixel lists, the chunk offsets and the
+    # half-pass over the lists.
     n_groups = len({tuple(sh) for sh in shapes[:n_maps]})
     prop = (1 + 6 * n_groups + 1) if head_learned else 0
-    pm = 1 if (head_choice[2] & 16 and not head_sched.sample) else (
-        1 + head_sched.half_passes + 1 + 1 + 3)
+    hp = head_sched.half_passes
+    hp_launches = min(hp, 2) + 5 * max(hp - 2, 0) if head_sched.active else hp
+    pm = 1 if (head_choice[2] & 16 and not head_sched.sample) else (1 + hp_launches + 1 + 1 + 3)
     line["gpu_launches"] = args.steps * (prop + pm)
     if ring and not args.no_mixed:
         line["config"]["mixed_size_batches"] = {

@@ -222,6 +222,11 @@ dn_status dn_batch_set_knight_moves(dn_batch* b, int on);
  * min_change relative, or, with min_change = 0, any change of the plane;
  * the others keep their state. */
 dn_status dn_batch_set_active_pixels(dn_batch* b, int on, float min_change);
+/* How the active half-passes run (separate launches per stage; the
+ * persistent launch always takes the second way): on = 1 (default) lists
+ * the active pixels of each map and runs the half-pass over the lists; on =
+ * 0 runs every tile that holds an active pixel.  The maps are the same. */
+dn_status dn_batch_set_active_lists(dn_batch* b, int on);
 /* Initial planes (f32 [H][W][3], reference camera) for one depthmap. */
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes);
 /* Total kept pruner points over all maps of the last run (after sync). */

@@ -176,6 +176,7 @@ struct Map {
   bool has_init = false;
   DevBuf<float> prop_init;   // learned proposal planes [H][W][3]
   DevBuf<uint8_t> changed;   // active-pixel flags [H][W]
+  DevBuf<int> alist;         // active-pixel list of a half-pass [H W]
   // Pruner (DN_RUN_PRUNE): views (this map first), scratch, outputs.
   DevBuf<dn::PruneView> prune_views;
   DevBuf<uint8_t> prune_scratch, prune_colors, prune_labels;
@@ -207,6 +208,9 @@ struct Engine {
   int use_knight = 0;  // knight-move candidates in the half-passes
   int active = 0;     // active-pixel half-passes
   float active_tol = 0.f;
+  int active_lists = 1;  // active half-passes on compacted pixel lists
+  DevBuf<int> d_acount, d_chunk0;  // per map: listed pixels; chunk offsets
+  DevBuf<int> d_tile_count, d_tile_off;  // per half-pass tile: active pixels, list offset
   // Learned proposal (DN_RUN_LEARNED): network weights, the feature grid of
   // every map (maps of one grid size contiguous, one network launch per
   // size), activations and outputs.
@@ -399,6 +403,10 @@ struct Engine {
         prop_groups.push_back(g);
       }
     }
+    if (active) {
+      DN_CUDA(d_acount.alloc(maps.size()));
+      DN_CUDA(d_chunk0.alloc(maps.size() + 1));
+    }
     for (size_t mi = 0; mi < maps.size(); ++mi) {
       Map& m = *maps[mi];
       const View& r = *views[m.ref];
@@ -436,6 +444,9 @@ struct Engine {
       if (active) {
         DN_CUDA(m.changed.alloc(npx));
         d.changed = m.changed.p;
+        DN_CUDA(m.alist.alloc(npx));
+        d.alist = m.alist.p;
+        d.acount = d_acount.p + mi;
       }
       if (prop_on) {
         DN_CUDA(m.prop_init.alloc(3 * npx));
@@ -473,6 +484,8 @@ struct Engine {
       const int tx1 = (r.W + bx - 1) / bx, ty1 = (r.H + by - 1) / by;
       const int tx2 = (r.W + 2 * px - 1) / (2 * px);
       const int txi = (r.W + px - 1) / px;
+      hm[mi].hp_tile0 = (int)t2.size();  // the map's half-pass tiles are contiguous
+      hm[mi].hp_tiles = tx2 * ty1;
       for (int y = 0; y < ty1; ++y) {
         for (int x = 0; x < tx1; ++x) t1.push_back(make_int4((int)mi, x, y, 0));
         for (int x = 0; x < tx2; ++x) t2.push_back(make_int4((int)mi, x, y, 0));
@@ -485,6 +498,10 @@ struct Engine {
     DN_CUDA(d_tiles1.alloc(std::max<size_t>(t1.size(), 1)));
     DN_CUDA(d_tiles2.alloc(std::max<size_t>(t2.size(), 1)));
     DN_CUDA(d_tiles_init.alloc(std::max<size_t>(ti.size(), 1)));
+    if (active) {
+      DN_CUDA(d_tile_count.alloc(std::max<size_t>(t2.size(), 1)));
+      DN_CUDA(d_tile_off.alloc(std::max<size_t>(t2.size(), 1)));
+    }
     DN_CUDA(cudaMemcpyAsync(d_views.p, hv.data(), hv.size() * sizeof(dn::ViewDev),
                             cudaMemcpyHostToDevice, stream));
     if (!hp.empty())
@@ -683,7 +700,12 @@ struct Engine {
     for (int k = 0; k < hp; ++k) {
       a2.p.colour = k & 1;
       a2.p.pass = k;
-      DN_CUDA(dn::launch_stage(dn::Stage::kHalfPass, sample_half, a2, stream));
+      if (active && active_lists && k >= 2) {
+        DN_CUDA(dn::launch_halfpass_list(sample_half, a2, (int)maps.size(), d_chunk0.p,
+                                         d_tile_count.p, d_tile_off.p, stream));
+      } else {
+        DN_CUDA(dn::launch_stage(dn::Stage::kHalfPass, sample_half, a2, stream));
+      }
     }
     DN_TRY(mark(2, timing));
     a1.flag = 1;
@@ -1627,6 +1649,13 @@ dn_status dn_batch_set_active_pixels(dn_batch* b, int on, float min_change) {
   DN_CHECK(min_change >= 0.f && min_change < 1.f, "min_change must be in [0, 1)");
   b->eng.active = on ? 1 : 0;
   b->eng.active_tol = min_change;
+  b->eng.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_active_lists(dn_batch* b, int on) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(b, "NULL batch");
+  b->eng.active_lists = on ? 1 : 0;
   b->eng.invalidate();
   return DN_OK;
 }

@@ -67,6 +67,11 @@ struct MapDev {
   float* prop_init;                        // [H][W][3] learned proposal planes
   long long prop_off;                      // first point of the map in the proposal grid
   int prop_W, prop_H;                      // proposal grid (W, H divided by the stride)
+  // Active-pixel lists (list-mode half-passes): the pixels (y W + x) of
+  // the half-pass's colour that are updated, and their number.
+  int* alist;                              // [H W] capacity
+  int* acount;                             // one counter
+  int hp_tile0, hp_tiles;                  // the map's range in the half-pass tile list
 };
 
 struct RunParams {
@@ -191,13 +196,28 @@ struct RefPatch {
   float varx;
 };
 
-// Builds the reference patch terms for pixel (i, j) from a float tile in
-// shared memory (tile origin (ty0, tx0), row pitch `pitch`).
-template <int HPZ>
-__device__ inline void ref_patch_from_tile(RefPatch<HPZ>& rp, const float* tile, int pitch,
-                                           int ly, int lx) {
-  // ly, lx: tile coordinates of the centre pixel.
-  const float c = tile[ly * pitch + lx];
+// Where a reference patch is read: src(dy, dx) is the intensity at offset
+// (dy, dx) from the centre pixel.  TileSrc reads the block's float tile in
+// shared memory (centre at tile row ly, column lx); ImgSrc reads the view's
+// FP16 image in global memory (centre (i, j), inside the image).  Both give
+// the same values: the tile holds the image converted to float.
+struct TileSrc {
+  const float* tile;
+  int pitch, ly, lx;
+  __device__ float operator()(int dy, int dx) const { return tile[(ly + dy) * pitch + lx + dx]; }
+};
+struct ImgSrc {
+  const __half* img;
+  int W, i, j;
+  __device__ float operator()(int dy, int dx) const {
+    return __half2float(img[(size_t)(i + dy) * W + (j + dx)]);
+  }
+};
+
+// Builds the reference patch terms of a pixel from src.
+template <int HPZ, class Src>
+__device__ inline void ref_patch_build(RefPatch<HPZ>& rp, const Src& src) {
+  const float c = src(0, 0);
   const float dcf = 1.0f / 5000.0f;  // 1 / (2 * 50^2)
   const float dxf = 1.0f / 50.0f;    // 1 / (2 * 5^2)
   float sw = 0.f, swx = 0.f;
@@ -207,7 +227,7 @@ __device__ inline void ref_patch_from_tile(RefPatch<HPZ>& rp, const float* tile,
 #pragma unroll
     for (int dx = -HPZ; dx <= HPZ; ++dx) {
       const int t = (dy + HPZ) * (2 * HPZ + 1) + (dx + HPZ);
-      const float x = tile[(ly + dy) * pitch + lx + dx];
+      const float x = src(dy, dx);
       const float d = __fsub_rn(x, c);
       const float arg = __fsub_rn(__fmul_rn(__fmul_rn(-d, d), dcf),
                                   __fmul_rn((float)(dx * dx + dy * dy), dxf));
@@ -228,6 +248,12 @@ __device__ inline void ref_patch_from_tile(RefPatch<HPZ>& rp, const float* tile,
   }
   rp.inv_sw = inv_sw;
   rp.varx = sxx * inv_sw;
+}
+// From a float tile in shared memory (ly, lx: tile coordinates of the centre).
+template <int HPZ>
+__device__ inline void ref_patch_from_tile(RefPatch<HPZ>& rp, const float* tile, int pitch,
+                                           int ly, int lx) {
+  ref_patch_build<HPZ>(rp, TileSrc{tile, pitch, ly, lx});
 }
 
 // Per-hypothesis terms shared by every matching view: f = K_0^-T v and
@@ -274,7 +300,7 @@ __device__ inline Warp warp_setup(const ViewDev& vw, const PairDev& pr, const Hy
   const float H00 = fmaf(pr.e[0], h.f0, pr.G[0]), H01 = fmaf(pr.e[0], h.f1, pr.G[1]);
   const float H10 = fmaf(pr.e[1], h.f0, pr.G[3]), H11 = fmaf(pr.e[1], h.f1, pr.G[4]);
   const float H20 = fmaf(pr.e[2], h.f0, pr.G[6]), H21 = fmaf(pr.e[2], h.f1, pr.G[7]);
-  const float rw = 1.0f / w;
+  const float rw = __frcp_rn(w);  // 1 / w, correctly rounded, without the divide's slow path
   wp.X0 = u * rw;
   wp.Y0 = v * rw;
   wp.ax = (H00 - H20 * wp.X0) * rw;  // d x2 / d dx
@@ -507,14 +533,13 @@ __device__ inline float group_sum(float v, unsigned mask) {
   return v;
 }
 
-template <int L>
-__device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile, int pitch, int ly,
-                                            int lx, int lane, unsigned mask) {
+template <int L, class Src>
+__device__ inline void coop_patch_build(CoopPatch<L>& cp, const Src& src, int lane, unsigned mask) {
   constexpr int C = CoopPatch<L>::C;
   cp.lane = lane;
   cp.mask = mask;
   cp.src0 = (threadIdx.x & 31) - lane;
-  const float c = tile[ly * pitch + lx];
+  const float c = src(0, 0);
   const float dcf = 1.0f / 5000.0f;
   const float dxf = 1.0f / 50.0f;
   float sw = 0.f, swx = 0.f;
@@ -527,7 +552,7 @@ __device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile,
       const int dx = lane + L * q;
       const bool real = dx < 7;
       const int dxx = real ? dx : 6;
-      const float x = tile[(ly + r - 3) * pitch + lx + dxx - 3];
+      const float x = src(r - 3, dxx - 3);
       const float d = __fsub_rn(x, c);
       const int ddx = dxx - 3, ddy = r - 3;
       const float arg = __fsub_rn(__fmul_rn(__fmul_rn(-d, d), dcf),
@@ -564,6 +589,11 @@ __device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile,
   sxx = group_sum<L>(sxx, mask);
   cp.inv_sw = inv_sw;
   cp.varx = sxx * inv_sw;
+}
+template <int L>
+__device__ inline void coop_patch_from_tile(CoopPatch<L>& cp, const float* tile, int pitch, int ly,
+                                            int lx, int lane, unsigned mask) {
+  coop_patch_build<L>(cp, TileSrc{tile, pitch, ly, lx}, lane, mask);
 }
 
 template <int L>
@@ -783,6 +813,10 @@ struct Patch<HPZ, 1> {
   __device__ void build(const float* tile, int pitch, int ly, int lx, int, unsigned) {
     ref_patch_from_tile<HPZ>(rp, tile, pitch, ly, lx);
   }
+  template <class Src>
+  __device__ void build_src(const Src& src, int, unsigned) {
+    ref_patch_build<HPZ>(rp, src);
+  }
   __device__ float view(const ViewDev& vw, const PairDev& pr, const Hyp& h, float j, float i,
                         unsigned& taps) const {
     return ncc_view<HPZ>(rp, vw, pr, h, j, i, taps);
@@ -798,6 +832,10 @@ struct CoopIface {
   CoopPatch<L> cp;
   __device__ void build(const float* tile, int pitch, int ly, int lx, int lane, unsigned mask) {
     coop_patch_from_tile<L>(cp, tile, pitch, ly, lx, lane, mask);
+  }
+  template <class Src>
+  __device__ void build_src(const Src& src, int lane, unsigned mask) {
+    coop_patch_build<L>(cp, src, lane, mask);
   }
   __device__ float view(const ViewDev& vw, const PairDev& pr, const Hyp& h, float j, float i,
                         unsigned& taps) const {

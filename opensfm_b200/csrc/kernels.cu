@@ -289,6 +289,160 @@ score_planes_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__
 // A candidate whose plane equals the current plane bit for bit is skipped:
 // its score at this pixel is the current score.
 
+// One red-black PatchMatch update of pixel (i, j) of map m
+// (PatchMatchUpdatePixel, depthmap.cc:305-374, with the candidate schedule of
+// RunParams): st is the pixel's state, pt its reference patch, spv the map's
+// records in shared memory; map_index keys the random streams.
+template <int HPZ, bool SAMPLE, int L>
+__device__ inline void halfpass_update(const MapDev& m, const PairViewSm& spv, int map_index,
+                                       int i, int j, float4 st, const Patch<HPZ, L>& pt,
+                                       int lane, const RunParams& p, unsigned& taps) {
+  const int W = m.W, H = m.H;
+  const size_t pix = (size_t)i * W + j;
+  const float fj = (float)j, fi = (float)i;
+  float cur = m.score[pix];
+  int curn = m.nghbr[pix];
+  float3 cv = make_float3(st.x, st.y, st.z);
+  float cd = st.w;
+  const PairDev* mp = spv.p;
+  const ViewDev* sv = spv.v;
+
+  auto try_plane = [&](float3 v, int view) {
+    if (same_plane(v, cv)) return;
+    const Hyp h = make_hyp(m.Kinv, v, fj, fi);
+    float s;
+    int nb;
+    if (SAMPLE) {
+      nb = view;
+      if (nb < 1 || nb > m.n_pairs) return;
+      const PairDev& pr = mp[nb - 1];
+      s = pt.view(sv[pr.view], pr, h, fj, fi, taps);
+    } else {
+      s = patch_max<HPZ, L>(pt, sv, mp, m.n_pairs, h, fj, fi, nb, taps);
+    }
+    if (s > cur) {
+      cur = s;
+      curn = nb;
+      cv = v;
+      cd = depth_of_plane(j, i, m.Kinv_d, v);
+    }
+  };
+
+  // One evaluation site for all candidate slots keeps the kernel's code
+  // small and the warp's lanes at the same slot: 0-3 adjacent pixels,
+  // 4-7 far samples, then (use_knight) the 8 knight-move pixels, then the
+  // refinements.
+  int refn = curn;
+  float depth_range = p.depth_range0, normal_range = p.normal_range0;
+  const int n_knight = p.use_knight ? 8 : 0;
+  const int first_refine = 8 + n_knight;
+  const int n_slots = first_refine + p.n_refine;
+#pragma unroll 1
+  for (int slot = 0; slot < n_slots; ++slot) {
+    float3 v = make_float3(0.f, 0.f, 0.f);
+    int view = 0;
+    bool valid = false;
+    if (slot < 4 && !p.use_near) continue;
+    if (slot >= 4 && slot < 8 && !p.use_far) continue;
+    if (slot >= 8 && slot < first_refine) {
+      // (+-1, +-2) and (+-2, +-1): the opposite colour, so no race.
+      const int k = slot - 8;
+      const int a = (k & 1) ? 1 : -1, b = (k & 2) ? 2 : -2;
+      const int di = (k & 4) ? b : a, dj = (k & 4) ? a : b;
+      const int qi = i + di, qj = j + dj;
+      if (qi >= 0 && qi < H && qj >= 0 && qj < W) {
+        const long q = (long)qi * W + qj;
+        const float4 sq = m.state[q];
+        if (sq.w != 0.0f) {
+          v = make_float3(sq.x, sq.y, sq.z);
+          view = SAMPLE ? m.nghbr[q] : 0;
+          valid = true;
+        }
+      }
+    } else if (slot < 8) {
+      const int d = slot & 3;
+      const int di = (d == 0) ? -1 : (d == 2 ? 1 : 0);
+      const int dj = (d == 1) ? -1 : (d == 3 ? 1 : 0);
+      long q = -1;
+      if (slot < 4) {
+        q = (long)(i + di) * W + (j + dj);
+      } else {
+        // The samples inside the map are a prefix of the 11 distances: no
+        // early exit, so their loads need not wait on one another.  Compared
+        // in order (the first maximum wins).
+        const int room = di < 0 ? i : (di > 0 ? H - 1 - i : (dj < 0 ? j : W - 1 - j));
+        const int n_in = room < kFarStart ? 0 : min(kFarSamples, (room - kFarStart) / 2 + 1);
+        const long step = (long)di * W + dj;
+        const long q0 = (long)i * W + j + (long)kFarStart * step;
+        const float* wcol = reinterpret_cast<const float*>(m.state) + 3;
+        float bs = -3.0f;
+#pragma unroll
+        for (int k = 0; k < kFarSamples; ++k) {
+          if (k < n_in) {
+            const long qq = q0 + 2 * k * step;
+            const float sq = m.score[qq], dq = wcol[4 * qq];
+            if (sq > bs && dq != 0.0f) {
+              bs = sq;
+              q = qq;
+            }
+          }
+        }
+      }
+      if (q >= 0) {
+        const float4 sq = m.state[q];
+        if (sq.w != 0.0f) {
+          v = make_float3(sq.x, sq.y, sq.z);
+          view = SAMPLE ? m.nghbr[q] : 0;
+          valid = true;
+        }
+      }
+    } else {
+      if (slot == first_refine) refn = curn;
+      if (cv.z != 0.0f) {
+        const uint4 r =
+            philox4x32_10(make_uint4((uint32_t)pix, (uint32_t)map_index, (uint32_t)p.pass,
+                                     (uint32_t)(slot - first_refine)),
+                          p.seed_lo, p.seed_hi);
+        const float2 g0 = normal2(r.x, r.y), g1 = normal2(r.z, r.w);
+        const float depth = cd * expf(depth_range * g0.x);
+        const float3 n = make_float3(-cv.x / cv.z + normal_range * g0.y,
+                                     -cv.y / cv.z + normal_range * g1.x, -1.0f);
+        v = plane_from_depth_normal(fj, fi, m.Kinv_d, depth, n);
+        view = refn;
+        valid = true;
+        depth_range *= 0.3f;
+        normal_range *= 0.8f;
+      }
+    }
+    if (valid) try_plane(v, view);
+  }
+  if (SAMPLE && m.n_pairs >= 2) {
+    // A random other matching view for the current plane.
+    const uint4 r = philox4x32_10(
+        make_uint4((uint32_t)pix, (uint32_t)map_index, (uint32_t)p.pass, 6u), p.seed_lo, p.seed_hi);
+    int other = 1 + (int)(r.x % (uint32_t)(m.n_pairs - 1));
+    if (other >= curn) other += 1;
+    const Hyp h = make_hyp(m.Kinv, cv, fj, fi);
+    const PairDev& pr = mp[other - 1];
+    const float s = pt.view(sv[pr.view], pr, h, fj, fi, taps);
+    if (s > cur) {
+      cur = s;
+      curn = other;
+    }
+  }
+  if (lane == 0) {
+    m.state[pix] = make_float4(cv.x, cv.y, cv.z, cd);
+    m.score[pix] = cur;
+    m.nghbr[pix] = curn;
+    if (p.active) {
+      const bool moved = p.active_tol > 0.0f
+                             ? fabsf(cd - st.w) > p.active_tol * st.w
+                             : !same_plane(cv, make_float3(st.x, st.y, st.z));
+      m.changed[pix] = moved ? 1 : 0;
+    }
+  }
+}
+
 template <int HPZ, bool SAMPLE, int L>
 __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
                                      const ViewDev* __restrict__ views,
@@ -330,139 +484,7 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
   if (run) {
     Patch<HPZ, L> pt;
     pt.build(tile, pitch, threadIdx.y + HPZ, (j - x0) + HPZ, lane, mask);
-    const float fj = (float)j, fi = (float)i;
-    float cur = m.score[pix];
-    int curn = m.nghbr[pix];
-    float3 cv = make_float3(st.x, st.y, st.z);
-    float cd = st.w;
-    const PairDev* mp = spv.p;
-    const ViewDev* sv = spv.v;
-
-    auto try_plane = [&](float3 v, int view) {
-      if (same_plane(v, cv)) return;
-      const Hyp h = make_hyp(m.Kinv, v, fj, fi);
-      float s;
-      int nb;
-      if (SAMPLE) {
-        nb = view;
-        if (nb < 1 || nb > m.n_pairs) return;
-        const PairDev& pr = mp[nb - 1];
-        s = pt.view(sv[pr.view], pr, h, fj, fi, taps);
-      } else {
-        s = patch_max<HPZ, L>(pt, sv, mp, m.n_pairs, h, fj, fi, nb, taps);
-      }
-      if (s > cur) {
-        cur = s;
-        curn = nb;
-        cv = v;
-        cd = depth_of_plane(j, i, m.Kinv_d, v);
-      }
-    };
-
-    // One evaluation site for all candidate slots keeps the kernel's code
-    // small and the warp's lanes at the same slot: 0-3 adjacent pixels,
-    // 4-7 far samples, then (use_knight) the 8 knight-move pixels, then the
-    // refinements.
-    int refn = curn;
-    float depth_range = p.depth_range0, normal_range = p.normal_range0;
-    const int n_knight = p.use_knight ? 8 : 0;
-    const int first_refine = 8 + n_knight;
-    const int n_slots = first_refine + p.n_refine;
-#pragma unroll 1
-    for (int slot = 0; slot < n_slots; ++slot) {
-      float3 v = make_float3(0.f, 0.f, 0.f);
-      int view = 0;
-      bool valid = false;
-      if (slot < 4 && !p.use_near) continue;
-      if (slot >= 4 && slot < 8 && !p.use_far) continue;
-      if (slot >= 8 && slot < first_refine) {
-        // (+-1, +-2) and (+-2, +-1): the opposite colour, so no race.
-        const int k = slot - 8;
-        const int a = (k & 1) ? 1 : -1, b = (k & 2) ? 2 : -2;
-        const int di = (k & 4) ? b : a, dj = (k & 4) ? a : b;
-        const int qi = i + di, qj = j + dj;
-        if (qi >= 0 && qi < H && qj >= 0 && qj < W) {
-          const long q = (long)qi * W + qj;
-          const float4 sq = m.state[q];
-          if (sq.w != 0.0f) {
-            v = make_float3(sq.x, sq.y, sq.z);
-            view = SAMPLE ? m.nghbr[q] : 0;
-            valid = true;
-          }
-        }
-      } else if (slot < 8) {
-        const int d = slot & 3;
-        const int di = (d == 0) ? -1 : (d == 2 ? 1 : 0);
-        const int dj = (d == 1) ? -1 : (d == 3 ? 1 : 0);
-        long q = -1;
-        if (slot < 4) {
-          q = (long)(i + di) * W + (j + dj);
-        } else {
-          float bs = -3.0f;
-          for (int k = 0; k < kFarSamples; ++k) {
-            const int dist = kFarStart + 2 * k;
-            const int qi = i + di * dist, qj = j + dj * dist;
-            if (qi < 0 || qi >= H || qj < 0 || qj >= W) break;
-            const long qq = (long)qi * W + qj;
-            const float sq = m.score[qq];
-            if (sq > bs && m.state[qq].w != 0.0f) {
-              bs = sq;
-              q = qq;
-            }
-          }
-        }
-        if (q >= 0) {
-          const float4 sq = m.state[q];
-          if (sq.w != 0.0f) {
-            v = make_float3(sq.x, sq.y, sq.z);
-            view = SAMPLE ? m.nghbr[q] : 0;
-            valid = true;
-          }
-        }
-      } else {
-        if (slot == first_refine) refn = curn;
-        if (cv.z != 0.0f) {
-          const uint4 r = philox4x32_10(make_uint4((uint32_t)pix, (uint32_t)tl.x, (uint32_t)p.pass,
-                                                   (uint32_t)(slot - first_refine)),
-                                        p.seed_lo, p.seed_hi);
-          const float2 g0 = normal2(r.x, r.y), g1 = normal2(r.z, r.w);
-          const float depth = cd * expf(depth_range * g0.x);
-          const float3 n = make_float3(-cv.x / cv.z + normal_range * g0.y,
-                                       -cv.y / cv.z + normal_range * g1.x, -1.0f);
-          v = plane_from_depth_normal(fj, fi, m.Kinv_d, depth, n);
-          view = refn;
-          valid = true;
-          depth_range *= 0.3f;
-          normal_range *= 0.8f;
-        }
-      }
-      if (valid) try_plane(v, view);
-    }
-    if (SAMPLE && m.n_pairs >= 2) {
-      // A random other matching view for the current plane.
-      const uint4 r = philox4x32_10(make_uint4((uint32_t)pix, (uint32_t)tl.x, (uint32_t)p.pass, 6u),
-                                    p.seed_lo, p.seed_hi);
-      int other = 1 + (int)(r.x % (uint32_t)(m.n_pairs - 1));
-      if (other >= curn) other += 1;
-      const Hyp h = make_hyp(m.Kinv, cv, fj, fi);
-      const PairDev& pr = mp[other - 1];
-      const float s = pt.view(sv[pr.view], pr, h, fj, fi, taps);
-      if (s > cur) {
-        cur = s;
-        curn = other;
-      }
-    }
-    if (lane == 0) {
-      m.state[pix] = make_float4(cv.x, cv.y, cv.z, cd);
-      m.score[pix] = cur;
-      m.nghbr[pix] = curn;
-      if (p.active) {
-        const bool moved = p.active_tol > 0.0f
-                               ? fabsf(cd - st.w) > p.active_tol * st.w
-                               : !same_plane(cv, make_float3(st.x, st.y, st.z));
-        m.changed[pix] = moved ? 1 : 0;
-      }
-    }
+    halfpass_update<HPZ, SAMPLE, L>(m, spv, tl.x, i, j, st, pt, lane, p, taps);
   }
   // A skipped pixel's own flag is 0 already (it was part of the test).
   flush_taps(taps, p.taps);
@@ -474,6 +496,207 @@ halfpass_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ vie
                 const PairDev* __restrict__ pairs, const int4* __restrict__ tiles,
                 RunParams p) {
   halfpass_tile<HPZ, SAMPLE, L>(maps, views, pairs, tiles[blockIdx.x], p);
+}
+
+// ----------------------------------------------------------------------
+// Active-pixel lists.  From the third half-pass of an active-pixel run a
+// half-pass updates only the pixels of its colour whose own depth or a
+// 4-neighbour's depth moved at their last update.  Rather than running
+// every tile that holds one such pixel with its other lanes idle, list mode
+// compacts them per map in tile order (active_count_kernel,
+// active_scan_kernel, active_write_kernel), turns the counts into chunk
+// offsets (chunk_offsets_kernel) and runs a grid-stride half-pass over the
+// chunks (halfpass_list_kernel): a block takes a chunk of (bx / L) x by
+// listed pixels of one map at a time, one tile's or a few neighbouring
+// tiles' pixels, so its warps read overlapping patches as in a tile.  An update reads only pixels of the
+// other colour, writes only its own pixel, and draws from random streams
+// keyed by the pixel, so the order of a list changes nothing: the maps are
+// the tile launch's, bit for bit.
+
+// Whether the pixel of this thread's lane group in half-pass tile tl is
+// updated (lane 0 of a group answers; the other lanes say no): the pixel
+// halfpass_tile would take, inside the patch border, initialised, and its
+// own depth or a 4-neighbour's moved at their last update.
+template <int L>
+__device__ inline bool active_pixel(const MapDev& m, const int4 tl, const RunParams& p,
+                                    size_t& pix) {
+  const int W = m.W, H = m.H, hpz = p.hpz;
+  const int px = blockDim.x / L;
+  const int g = threadIdx.x / L, lane = threadIdx.x % L;
+  const int i = tl.z * blockDim.y + threadIdx.y;
+  const int j = tl.y * (2 * px) + 2 * g + ((i + p.colour) & 1);
+  pix = 0;
+  if (lane != 0 || i < hpz || i >= H - hpz || j < hpz || j >= W - hpz) return false;
+  pix = (size_t)i * W + j;
+  if (reinterpret_cast<const float*>(m.state)[4 * pix + 3] == 0.0f) return false;
+  const uint8_t* ch = m.changed;  // interior pixel: the 4 neighbours are inside the map
+  return (ch[pix] | ch[pix - W] | ch[pix + W] | ch[pix - 1] | ch[pix + 1]) != 0;
+}
+
+// The number of active pixels of every half-pass tile.
+template <int L>
+__global__ void __launch_bounds__(128)
+active_count_kernel(const MapDev* __restrict__ maps, const int4* __restrict__ tiles, RunParams p,
+                    int* __restrict__ tile_count) {
+  const int4 tl = tiles[blockIdx.x];
+  size_t pix;
+  const bool act = active_pixel<L>(maps[tl.x], tl, p, pix);
+  const int n = __syncthreads_count(act);
+  if (threadIdx.x == 0 && threadIdx.y == 0) tile_count[blockIdx.x] = n;
+}
+
+// One block of 1024 threads per map: tile_off[t] = the active pixels of the
+// map's half-pass tiles before tile t, *acount = the map's total.
+__global__ void __launch_bounds__(1024)
+active_scan_kernel(const MapDev* __restrict__ maps, const int* __restrict__ tile_count,
+                   int* __restrict__ tile_off) {
+  const MapDev& m = maps[blockIdx.x];
+  __shared__ int wsum[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int carry = 0;
+  for (int base = 0; base < m.hp_tiles; base += blockDim.x) {
+    const int k = base + (int)threadIdx.x;
+    const int c = k < m.hp_tiles ? tile_count[m.hp_tile0 + k] : 0;
+    int v = c;  // inclusive scan within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
+    }
+    if (lane == 31) wsum[w] = v;
+    __syncthreads();
+    if (w == 0) {
+      int s = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += t;
+      }
+      if (lane < nw) wsum[lane] = s;
+    }
+    __syncthreads();
+    const int before = (w ? wsum[w - 1] : 0) + v - c;
+    if (k < m.hp_tiles) tile_off[m.hp_tile0 + k] = carry + before;
+    carry += wsum[nw - 1];
+    __syncthreads();  // wsum is rewritten by the next round
+  }
+  if (threadIdx.x == 0) *m.acount = carry;
+}
+
+// The active pixels of every half-pass tile at the tile's offset, in the
+// tile's row order: the lists are in tile order, whatever the timing.
+template <int L>
+__global__ void __launch_bounds__(128)
+active_write_kernel(const MapDev* __restrict__ maps, const int4* __restrict__ tiles, RunParams p,
+                    const int* __restrict__ tile_off) {
+  const int4 tl = tiles[blockIdx.x];
+  const MapDev& m = maps[tl.x];
+  size_t pix;
+  const bool act = active_pixel<L>(m, tl, p, pix);
+  __shared__ int wcount[32];
+  const int lin = threadIdx.y * blockDim.x + threadIdx.x, wl = lin & 31, w = lin >> 5;
+  const unsigned ballot = __ballot_sync(0xffffffffu, act);
+  if (wl == 0) wcount[w] = __popc(ballot);
+  __syncthreads();
+  int before = 0;
+  for (int k = 0; k < w; ++k) before += wcount[k];
+  if (act) m.alist[tile_off[blockIdx.x] + before + __popc(ballot & ((1u << wl) - 1u))] = (int)pix;
+}
+
+// chunk0[k] = the chunks of `per` listed pixels of maps 0..k-1 (k = 0 ..
+// n_maps; chunk0[n_maps] is the total).  One warp.
+__global__ void chunk_offsets_kernel(const MapDev* __restrict__ maps, int n_maps, int per,
+                                     int* __restrict__ chunk0) {
+  int carry = 0;
+  for (int base = 0; base < n_maps; base += 32) {
+    const int k = base + (int)threadIdx.x;
+    const int c = k < n_maps ? (*maps[k].acount + per - 1) / per : 0;
+    int v = c;  // inclusive scan over the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, v, o);
+      if ((int)threadIdx.x >= o) v += t;
+    }
+    if (k < n_maps) chunk0[k] = carry + v - c;
+    carry += __shfl_sync(0xffffffffu, v, 31);
+  }
+  if (threadIdx.x == 0) chunk0[n_maps] = carry;
+}
+
+template <int HPZ, bool SAMPLE, int L>
+__global__ void __launch_bounds__(128, (kMinBlocksL<HPZ, L>))
+halfpass_list_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
+                     const PairDev* __restrict__ pairs, const int* __restrict__ chunk0,
+                     int n_maps, RunParams p) {
+  __shared__ PairViewSm spv;
+  const int px = blockDim.x / L, per = px * blockDim.y;
+  const int g = threadIdx.x / L, lane = threadIdx.x % L;
+  const unsigned mask = (L == 1) ? (1u << (threadIdx.x & 31))
+                                 : (((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1)));
+  const int total = chunk0[n_maps];
+  unsigned taps = 0;
+  for (int c = blockIdx.x; c < total; c += gridDim.x) {
+    // The map of chunk c: the last k with chunk0[k] <= c (maps without
+    // chunks share their start with the next map).
+    int lo = 0, hi = n_maps - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (chunk0[mid] <= c)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const MapDev& m = maps[lo];
+    __syncthreads();  // the previous chunk's readers of spv are done
+    stage_pairs(spv, m, views, pairs);
+    __syncthreads();
+    const int e = (c - chunk0[lo]) * per + (int)threadIdx.y * px + g;
+    if (e < *m.acount) {
+      const int pix = m.alist[e];
+      const int i = pix / m.W, j = pix - i * m.W;
+      Patch<HPZ, L> pt;
+      pt.build_src(ImgSrc{views[m.ref_view].img, m.W, i, j}, lane, mask);
+      halfpass_update<HPZ, SAMPLE, L>(m, spv, lo, i, j, m.state[pix], pt, lane, p, taps);
+    }
+  }
+  flush_taps(taps, p.taps);
+}
+
+template <int HPZ, int L>
+static cudaError_t launch_list_hpz(bool sample, const LaunchArgs& a, int n_maps,
+                                   int* chunk0, int* tile_count, int* tile_off, cudaStream_t s) {
+  const dim3 blk(a.bx, a.by);
+  const int per = (a.bx / L) * a.by;
+  active_count_kernel<L><<<a.n_tiles, blk, 0, s>>>(a.maps, a.tiles, a.p, tile_count);
+  active_scan_kernel<<<n_maps, 1024, 0, s>>>(a.maps, tile_count, tile_off);
+  active_write_kernel<L><<<a.n_tiles, blk, 0, s>>>(a.maps, a.tiles, a.p, tile_off);
+  chunk_offsets_kernel<<<1, 32, 0, s>>>(a.maps, n_maps, per, chunk0);
+  // A resident grid: every block walks chunks until the lists are done.
+  auto kern = sample ? halfpass_list_kernel<HPZ, true, L> : halfpass_list_kernel<HPZ, false, L>;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, a.bx * a.by, 0);
+  const int grid = std::max(1, std::min(a.n_tiles, std::max(per_sm, 1) * sms));
+  kern<<<grid, blk, 0, s>>>(a.maps, a.views, a.pairs, chunk0, n_maps, a.p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_halfpass_list(bool sample, const LaunchArgs& a, int n_maps, int* chunk0,
+                                 int* tile_count, int* tile_off, cudaStream_t s) {
+  if (a.n_tiles == 0 || n_maps == 0) return cudaSuccess;
+  switch (a.p.hpz) {
+    case 1: return launch_list_hpz<1, 1>(sample, a, n_maps, chunk0, tile_count, tile_off, s);
+    case 2: return launch_list_hpz<2, 1>(sample, a, n_maps, chunk0, tile_count, tile_off, s);
+    case 3:
+      if (a.p.variant == 2) return launch_list_hpz<3, 2>(sample, a, n_maps, chunk0, tile_count, tile_off, s);
+      if (a.p.variant == 4) return launch_list_hpz<3, 4>(sample, a, n_maps, chunk0, tile_count, tile_off, s);
+      if (a.p.variant == 8) return launch_list_hpz<3, 8>(sample, a, n_maps, chunk0, tile_count, tile_off, s);
+      return launch_list_hpz<3, 1>(sample, a, n_maps, chunk0, tile_count, tile_off, s);
+    case 4: return launch_list_hpz<4, 1>(sample, a, n_maps, chunk0, tile_count, tile_off, s);
+    case 5: return launch_list_hpz<5, 1>(sample, a, n_maps, chunk0, tile_count, tile_off, s);
+  }
+  return cudaErrorInvalidValue;
 }
 
 // ----------------------------------------------------------------------

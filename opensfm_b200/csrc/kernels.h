@@ -21,6 +21,13 @@ struct LaunchArgs {
 };
 
 cudaError_t launch_stage(Stage stage, bool sample, const LaunchArgs& a, cudaStream_t s);
+// An active-pixel half-pass in list mode (a.tiles: the half-pass tiles;
+// p.active, p.pass >= 2): lists the active pixels of the colour into
+// MapDev::alist in tile order (their number into MapDev::acount), chunk
+// offsets into chunk0 (n_maps + 1 ints), then the half-pass over the lists.
+// tile_count and tile_off: scratch of a.n_tiles ints each.
+cudaError_t launch_halfpass_list(bool sample, const LaunchArgs& a, int n_maps, int* chunk0,
+                                 int* tile_count, int* tile_off, cudaStream_t s);
 
 struct CleanView;
 struct CleanMap;

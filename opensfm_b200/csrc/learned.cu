@@ -296,7 +296,7 @@ __device__ __forceinline__ void tmem_load<16>(uint32_t taddr, uint32_t (&r)[16])
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-constexpr size_t smem_bytes(int np) { return 2 * (size_t)kHalo + (size_t)kKC * np * 16 + 16; }
+constexpr size_t smem_bytes(int np) { return 2 * (size_t)kHalo + (size_t)kKC * np * 16 + 32; }
 
 // Tile t of the batch: image, first row, first column.
 struct TileXY {
@@ -340,9 +340,10 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* halo = smem;                    // 2 x [4 planes][kHR][kHC][16 B]
   unsigned char* Bs = smem + 2 * kHalo;          // [kKC][NP][16 B]
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(Bs + (size_t)kKC * NP * 16);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(Bs + (size_t)kKC * NP * 16);  // 2 barriers
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
   const int tid = threadIdx.x, warp = tid >> 5;
+  constexpr uint32_t kCols = 2 * NP;  // two accumulators (32 or 64 columns)
 
   long long t = blockIdx.x;
   const uint32_t h_base = smem_u32(halo);
@@ -355,11 +356,12 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mbar + 1)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;\n" ::"r"(
-                     smem_u32(tslot))
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(tslot)), "n"(kCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
@@ -367,19 +369,16 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tslot;
-  const uint32_t b_base = smem_u32(Bs), mb = smem_u32(mbar);
+  const uint32_t b_base = smem_u32(Bs), mb0 = smem_u32(mbar);
   constexpr uint32_t idesc = idesc_bf16(NP);
-  uint32_t phase = 0;
-  int cur = 0;
-  bool ok = true;
-  for (; t < n_tiles; t += gridDim.x) {
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    const uint32_t a_base = h_base + (uint32_t)(cur * kHalo);
+  const long long G = gridDim.x;
+  // Tile k of this CTA (t = blockIdx.x + k G) uses halo buffer and
+  // accumulator k & 1.  The MMAs of tile k + 1 are issued before the
+  // epilogue of tile k, and the halo of tile k + 2 streams in meanwhile.
+  auto issue = [&](int buf) {
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t a_base = h_base + (uint32_t)(buf * kHalo);
 #pragma unroll
       for (int tap = 0; tap < 9; ++tap) {
 #pragma unroll
@@ -392,28 +391,53 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
           asm volatile(
               "{\n\t.reg .pred p;\n\t"
               "setp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
+                  tmem + (uint32_t)(buf * NP)),
               "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
               : "memory");
         }
       }
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-              mb)
+              mb0 + 8u * (uint32_t)buf)
           : "memory");
     }
-    // The next tile's halo streams in while the MMAs run and the epilogue
-    // stores; its buffer was last read by the MMAs of the previous tile.
-    const long long tn = t + gridDim.x;
-    if (tn < n_tiles) load_halo(h_base + (uint32_t)((cur ^ 1) * kHalo), x, tn, H, W);
-    bool done = mbar_wait(mb, phase);
-    if (!done) done = mbar_wait(mb, phase);  // a late completion
-    phase ^= 1u;
+  };
+  // The generic-proxy and cp.async writes of the halo become visible to
+  // the tensor core; the previous readers of the accumulator are done.
+  auto halo_ready = [&]() {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+  };
+  uint32_t phase[2] = {0u, 0u};
+  int pend = -1;  // accumulator whose MMAs are in flight and not yet waited for
+  int cur = 0;
+  bool ok = true;
+  if (t < n_tiles) {
+    halo_ready();
+    issue(0);
+    pend = 0;
+    if (t + G < n_tiles) load_halo(h_base + (uint32_t)kHalo, x, t + G, H, W);
+  }
+  for (; t < n_tiles; t += G) {
+    const long long tn = t + G;
+    if (tn < n_tiles) {
+      halo_ready();
+      issue(cur ^ 1);
+    }
+    bool done = mbar_wait(mb0 + 8u * (uint32_t)cur, phase[cur]);
+    if (!done) done = mbar_wait(mb0 + 8u * (uint32_t)cur, phase[cur]);  // a late completion
+    phase[cur] ^= 1u;
+    pend = tn < n_tiles ? (cur ^ 1) : -1;
     ok = __syncthreads_and(done) != 0;
     if (!ok) break;
+    // Tile k's halo buffer is free: the halo of tile k + 2 streams into it.
+    if (tn + G < n_tiles) load_halo(h_base + (uint32_t)(cur * kHalo), x, tn + G, H, W);
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     uint32_t r[NP];
-    tmem_load<NP>(tmem + ((uint32_t)(warp * 32) << 16), r);
+    tmem_load<NP>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cur * NP), r);
     const TileXY tt = tile_xy(t, H, W);
     const int py = tt.y0 + (tid >> 3), px = tt.x0 + (tid & 7);
     if (py < H && px < W) {
@@ -464,13 +488,19 @@ conv3x3_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* 
     __syncthreads();
     cur ^= 1;
   }
+  if (!ok && pend >= 0) {
+    // A wait ran out: wait (bounded) for the MMAs still in flight before the
+    // accumulators are freed.
+    mbar_wait(mb0 + 8u * (uint32_t)pend, phase[pend]);
+  }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   if (!ok && tid == 0) atomicExch(&g_error, 1);
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;\n" ::"r"(tmem) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(kCols)
+                 : "memory");
 }
 
 // ------------------------------------------------------- conv backward-data

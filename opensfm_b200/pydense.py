@@ -730,6 +730,11 @@ class Batch(_Handle):
         ``min_change`` relative; 0: any change of the plane)."""
         check(self._L.dn_batch_set_active_pixels(self._h, int(bool(on)), float(min_change)))
 
+    def set_active_lists(self, on: bool) -> None:
+        """Active half-passes over compacted lists of the active pixels (the
+        default) or over every tile that holds one; the maps are the same."""
+        check(self._L.dn_batch_set_active_lists(self._h, int(bool(on))))
+
     def set_proposal_net(self, weights: Optional[np.ndarray], biases: Optional[np.ndarray] = None,
                          n_planes: int = 8, stride: int = 2) -> None:
         """The network of learned runs (``run(learned=True)``): ``weights`` the

@@ -932,3 +932,34 @@ def test_bounded_wait_expiry_reports_timeout():
     b.synchronize()
     assert (b.get_depth(0) > 0).any()
 
+
+
+@pytest.mark.parametrize("mode,tuning", [(0, (32, 4, 2)), (1, (32, 4, 2)), (2, (32, 4, 4)),
+                                         (1, (32, 4, 1))])
+def test_active_lists_match_tile_launch(scene, mode, tuning):
+    """Active half-passes over compacted pixel lists give the same maps, bit
+    for bit, as running every tile that holds an active pixel: an update
+    reads only the other colour and its random streams are keyed by the
+    pixel, so the order of the list does not matter."""
+    Ks, Rs, ts = cams(scene)
+    b = pydense.Batch()
+    for K, R, t, im in zip(Ks, Rs, ts, scene.images):
+        b.add_view(K, R, t, im)
+    n = len(scene.images)
+    for v in range(n):
+        b.add_depthmap(v, [o for o in range(n) if o != v][:4], *S.depth_range(scene.depths[v]))
+    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=3, seed=9)
+    b.set_tuning(*tuning)
+    b.set_candidate_views(mode)
+    b.set_schedule(half_passes=8)
+    b.set_active_pixels(True, 0.003)
+    out = []
+    for lists in (True, False):
+        b.set_active_lists(lists)
+        b.run()
+        b.synchronize()
+        out.append([b.get(v) for v in range(n)])
+    for v in range(n):
+        for a, w in zip(out[0][v], out[1][v]):
+            assert np.array_equal(a, w)
+    assert (out[0][0][0] > 0).mean() > 0.3
