@@ -63,7 +63,7 @@ struct MapDev {
   float* clean;                            // [H][W] cleaned depth
   const float* init;                       // [H][W][3] optional initial planes
   uint8_t* keep;                           // [H][W] pruner flags (scratch)
-  uint8_t* changed;                        // [H][W] plane changed at the last update
+  uint8_t* changed;                        // [H][W] active-pixel flags (kMoved | kValid)
   float* prop_init;                        // [H][W][3] learned proposal planes
   long long prop_off;                      // first point of the map in the proposal grid
   int prop_W, prop_H;                      // proposal grid (W, H divided by the stride)
@@ -73,6 +73,11 @@ struct MapDev {
   int* acount;                             // one counter
   int hp_tile0, hp_tiles;                  // the map's range in the half-pass tile list
 };
+
+// Active-pixel flags (MapDev::changed): kValid is set by the initialisation
+// on every pixel it gives a plane (the pixels the half-passes update; it
+// never changes after), kMoved by an update whose depth moved.
+constexpr uint8_t kMoved = 1, kValid = 2;
 
 struct RunParams {
   int hpz;

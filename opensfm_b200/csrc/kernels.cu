@@ -170,6 +170,7 @@ __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev*
       m.state[pix] = st;
       m.score[pix] = sc;
       m.nghbr[pix] = nb;
+      if (p.active) m.changed[pix] = st.w != 0.0f ? kValid : 0;
     }
   }
   flush_taps(taps, p.taps);
@@ -438,7 +439,7 @@ __device__ inline void halfpass_update(const MapDev& m, const PairViewSm& spv, i
       const bool moved = p.active_tol > 0.0f
                              ? fabsf(cd - st.w) > p.active_tol * st.w
                              : !same_plane(cv, make_float3(st.x, st.y, st.z));
-      m.changed[pix] = moved ? 1 : 0;
+      m.changed[pix] = moved ? (kValid | kMoved) : kValid;
     }
   }
 }
@@ -472,7 +473,7 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
       // were written by the previous half-pass, the pixel's own by the one
       // before; this half-pass writes only pixels of its own colour.
       const uint8_t* ch = m.changed;
-      run = (ch[pix] | ch[pix - W] | ch[pix + W] | ch[pix - 1] | ch[pix + 1]) != 0;
+      run = ((ch[pix] | ch[pix - W] | ch[pix + W] | ch[pix - 1] | ch[pix + 1]) & kMoved) != 0;
     }
     // A tile without an active pixel leaves before staging (block-uniform:
     // every thread of the block takes the same branch).
@@ -528,9 +529,10 @@ __device__ inline bool active_pixel(const MapDev& m, const int4 tl, const RunPar
   pix = 0;
   if (lane != 0 || i < hpz || i >= H - hpz || j < hpz || j >= W - hpz) return false;
   pix = (size_t)i * W + j;
-  if (reinterpret_cast<const float*>(m.state)[4 * pix + 3] == 0.0f) return false;
   const uint8_t* ch = m.changed;  // interior pixel: the 4 neighbours are inside the map
-  return (ch[pix] | ch[pix - W] | ch[pix + W] | ch[pix - 1] | ch[pix + 1]) != 0;
+  const uint8_t own = ch[pix];
+  if (!(own & kValid)) return false;  // not initialised: the state has depth 0
+  return ((own | ch[pix - W] | ch[pix + W] | ch[pix - 1] | ch[pix + 1]) & kMoved) != 0;
 }
 
 // The number of active pixels of every half-pass tile.

@@ -74,7 +74,7 @@ sweep_features_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict
     const double a = 1.0 / m.min_depth, b = 1.0 / m.max_depth;
     unsigned taps = 0;
     const int nv = min(2, m.n_pairs);
-    for (int p = 0; p < n_planes && p < 8; ++p) {
+    for (int p = 0; p < n_planes && p < kMaxSweepPlanes; ++p) {
       const float depth = (float)(1.0 / (a + (b - a) * (p + 0.5) / n_planes));
       const float3 v = plane_from_depth_normal((float)j, (float)i, m.Kinv_d, depth,
                                                make_float3(0.f, 0.f, -1.f));
@@ -1177,6 +1177,7 @@ cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map
   if (a.n_tiles == 0) return cudaSuccess;
   if (stride == 1) return sweep_s<1>(a, feat, map_stride, n_planes, s);
   if (stride == 2) return sweep_s<2>(a, feat, map_stride, n_planes, s);
+  if (stride == 4) return sweep_s<4>(a, feat, map_stride, n_planes, s);
   return cudaErrorInvalidValue;
 }
 cudaError_t launch_l1_loss(const float* pred, const float* target, long long n_pix,
@@ -1213,6 +1214,8 @@ cudaError_t launch_proposal_to_planes(const float* out, const MapDev* maps, int 
     proposal_to_planes_kernel<1><<<grid, 256, 0, s>>>(out, maps);
   else if (stride == 2)
     proposal_to_planes_kernel<2><<<grid, 256, 0, s>>>(out, maps);
+  else if (stride == 4)
+    proposal_to_planes_kernel<4><<<grid, 256, 0, s>>>(out, maps);
   else
     return cudaErrorInvalidValue;
   return cudaGetLastError();

@@ -7,7 +7,10 @@
 
 namespace dn {
 
-constexpr int kFeatC = 32;  // network input channels (17 used, zero padded)
+constexpr int kFeatC = 32;  // network input channels (1 + 2 x planes used, zero padded)
+// Sweep planes: channel 0 is the intensity, 1 + 2 p + k the NCC of plane p
+// against matching view k (k < 2).
+constexpr int kMaxSweepPlanes = (kFeatC - 1) / 2;
 
 struct ConvArgs {
   const __nv_bfloat16* x;       // input activations [n_pix][cin]

@@ -56,9 +56,10 @@ def _stream():
 class ProposalNet:
     """FP32 master weights + Adam state on the device, BF16 copies for the kernels."""
 
-    def __init__(self, seed: int = 0, stride: int = 2):
+    def __init__(self, seed: int = 0, stride: int = 2, n_planes: int = 8):
         torch = _torch()
         self.stride = stride  # proposal grid the network was trained on
+        self.n_planes = n_planes  # sweep planes of its input features
         g = torch.Generator().manual_seed(seed)
         self.w32, self.b32, self.w16 = [], [], []
         for cin, cout, relu in LAYERS:
@@ -92,6 +93,7 @@ class ProposalNet:
             d[f"b{k}"] = b.cpu().numpy()
         d["step"] = np.array(self.step)
         d["stride"] = np.array(self.stride)
+        d["planes"] = np.array(self.n_planes)
         return d
 
     def save(self, path: str, **extra):
@@ -112,6 +114,7 @@ class ProposalNet:
         net.v = [torch.zeros_like(t) for t in net.w32 + net.b32]
         net.step = int(z["step"]) if "step" in z else 0
         net.stride = int(z["stride"]) if "stride" in z else 1
+        net.n_planes = int(z["planes"]) if "planes" in z else 8
         net.wt_scratch = torch.empty(32 * 9 * 32, dtype=torch.bfloat16, device="cuda")
         return net
 
@@ -263,19 +266,37 @@ def targets(b: pydense.Batch, n_maps: int, H: int, W: int, min_score: float = 0.
 
 
 def make_dataset(seeds: Sequence[int], W: int = 640, H: int = 480, chunk: int = 50,
-                 iterations: int = 3, stride: int = 2, log=None):
+                 iterations: int = 3, stride: int = 2, n_planes: int = 8,
+                 gt_filter: float = 0.0, log=None):
     """Features on the proposal grid and plain-PatchMatch targets at the same
-    grid points for every seed (device tensors)."""
+    grid points for every seed (device tensors).  gt_filter > 0 keeps only
+    the targets whose depth is within that relative error of the rendered
+    ground truth (the other grid points get weight 0)."""
     torch = _torch()
     feats, tgs = [], []
     t0 = time.time()
+    Hs, Ws = grid_shape(H, W, stride)
     for c0 in range(0, len(seeds), chunk):
         scenes = [make_scene(s, W, H) for s in seeds[c0:c0 + chunk]]
         b, maps = build_batch(scenes, iterations=iterations, seed=int(seeds[c0]) + 7)
         b.run()
         b.synchronize()
-        tgs.append(targets(b, len(maps), H, W, stride=stride))
-        feats.append(features(b, len(maps), H, W, stride=stride))
+        tg = targets(b, len(maps), H, W, stride=stride)
+        if gt_filter > 0:
+            # The target depth from its inverse-depth fraction, against the
+            # ground truth at the same pixel (grid point (ys, xs) = pixel
+            # (stride ys, stride xs)).
+            gt = torch.from_numpy(np.stack([sv.depths[sv.ref][::stride, ::stride]
+                                            for sv in scenes]).astype(np.float32)).cuda()
+            rng = np.array([depth_range_of(sv) for sv in scenes], np.float64)
+            a = torch.from_numpy(1.0 / rng[:, 1]).float().cuda().view(-1, 1, 1)
+            bb = torch.from_numpy(1.0 / rng[:, 0]).float().cuda().view(-1, 1, 1)
+            t4 = tg.view(len(maps), Hs, Ws, 4)
+            d = 1.0 / (a + (bb - a) * t4[..., 0])
+            keep = (t4[..., 3] > 0) & (gt > 0) & ((d - gt).abs() <= gt_filter * gt)
+            t4[..., 3] = keep.float()
+        tgs.append(tg)
+        feats.append(features(b, len(maps), H, W, n_planes=n_planes, stride=stride))
         b.close()
         if log:
             log(f"dataset {c0 + len(scenes)}/{len(seeds)} scenes, {time.time() - t0:.1f} s")
@@ -371,11 +392,13 @@ def propose(net: ProposalNet, b: pydense.Batch, maps: Sequence[int], H: int, W: 
     return out
 
 
-def install(net: ProposalNet, b: pydense.Batch, stride: int = 2, n_planes: int = 8) -> None:
+def install(net: ProposalNet, b: pydense.Batch, stride: Optional[int] = None,
+            n_planes: Optional[int] = None) -> None:
     """Hands the network to the batch: ``b.run(learned=True)`` then sweeps,
-    runs the network and installs the proposals on the batch stream."""
+    runs the network and installs the proposals on the batch stream (by
+    default on the grid and with the sweep planes it was trained with)."""
     w, bias = net.packed()
-    b.set_proposal_net(w, bias, n_planes=n_planes, stride=stride)
+    b.set_proposal_net(w, bias, n_planes=n_planes or net.n_planes, stride=stride or net.stride)
 
 
 def main(argv=None):
@@ -391,7 +414,10 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--size", default="640x480", help="training scene size WxH")
-    ap.add_argument("--stride", type=int, default=2, help="proposal grid stride (1 or 2)")
+    ap.add_argument("--stride", type=int, default=2, help="proposal grid stride (1, 2 or 4)")
+    ap.add_argument("--planes", type=int, default=8, help="sweep planes (1..15)")
+    ap.add_argument("--gt-filter", type=float, default=0.0,
+                    help="keep only targets within this relative depth error of the ground truth")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--evaluate", action="store_true",
@@ -409,16 +435,18 @@ def main(argv=None):
         return
     W, H = (int(x) for x in args.size.split("x"))
     seeds = list(range(100000, 100000 + args.scenes))
-    feat, tgt = make_dataset(seeds, W=W, H=H, stride=args.stride, log=log)
+    feat, tgt = make_dataset(seeds, W=W, H=H, stride=args.stride, n_planes=args.planes,
+                             gt_filter=args.gt_filter, log=log)
     valid = float((tgt.view(-1, 4)[:, 3] > 0).float().mean().item())
     log(f"target coverage {valid:.3f}")
     Hs, Ws = grid_shape(H, W, args.stride)
-    net = ProposalNet(seed=args.seed)
+    net = ProposalNet(seed=args.seed, stride=args.stride, n_planes=args.planes)
     hist = train(net, feat, tgt, len(seeds), Hs, Ws, steps=args.steps, batch=args.batch,
                  lr=args.lr, log=log)
     net.save(args.out, history=np.array(hist), scenes=np.array(args.scenes),
              seeds_start=np.array(seeds[0]), stride=np.array(args.stride),
-             train_W=np.array(W), train_H=np.array(H))
+             train_W=np.array(W), train_H=np.array(H), gt_filter=np.array(args.gt_filter),
+             steps=np.array(args.steps))
     log(f"saved {args.out}")
 
 
