@@ -410,13 +410,13 @@ def main(argv=None):
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--scenes", type=int, default=2000)
-    ap.add_argument("--steps", type=int, default=1500)
-    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--size", default="640x480", help="training scene size WxH")
-    ap.add_argument("--stride", type=int, default=2, help="proposal grid stride (1, 2 or 4)")
-    ap.add_argument("--planes", type=int, default=8, help="sweep planes (1..15)")
-    ap.add_argument("--gt-filter", type=float, default=0.0,
+    ap.add_argument("--stride", type=int, default=4, help="proposal grid stride (1, 2 or 4)")
+    ap.add_argument("--planes", type=int, default=15, help="sweep planes (1..15)")
+    ap.add_argument("--gt-filter", type=float, default=0.01,
                     help="keep only targets within this relative depth error of the ground truth")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--seed", type=int, default=0)
