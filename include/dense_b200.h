@@ -320,6 +320,13 @@ dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float
  * the network. */
 dn_status dn_batch_set_proposal_net(dn_batch* b, const uint16_t* weights, const float* biases,
                                     int n_planes, int stride);
+/* The larger side (pixels) of the images the network was trained on.  With
+ * ref_dim > 0 each map's proposal grid uses the network's stride scaled by
+ * the map's larger side over ref_dim, rounded down to 1, 2, 4 or 8, so that
+ * every map's grid has the training scale (a 320 x 240 map at stride 2
+ * when the network was trained at stride 4 on 640 x 480); ref_dim = 0 (the
+ * default): every map uses the stride. */
+dn_status dn_batch_set_proposal_scale(dn_batch* b, int ref_dim);
 /* Initial planes of one depthmap from the network output (device f32
  * [H][W][4]); the next dn_batch_run with DN_RUN_INIT starts from them. */
 dn_status dn_batch_init_from_output(dn_batch* b, int map_id, const float* out);

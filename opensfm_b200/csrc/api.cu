@@ -217,9 +217,26 @@ struct Engine {
   struct PropGroup {
     int W, H, n;
     long long off;  // first grid point
+    int S;          // grid stride of its maps
   };
   bool prop_on = false;
   int prop_stride = 2, prop_planes = 8;
+  int prop_ref_dim = 0;  // larger side of the training images (0: one stride for every map)
+  struct SweepRange {
+    int S, first, count;  // sweep tiles of the maps of grid stride S
+  };
+  std::vector<SweepRange> sweep_ranges;
+  // The proposal-grid stride of a map: the network's stride scaled by the
+  // map's larger side over the training images' (prop_ref_dim > 0), rounded
+  // down to 1, 2, 4 or 8, so that every map's grid has the scale the network
+  // was trained at; with prop_ref_dim = 0 the network's stride.
+  int map_prop_stride(const View& r) const {
+    if (prop_ref_dim <= 0) return prop_stride;
+    const double s = (double)prop_stride * std::max(r.W, r.H) / prop_ref_dim;
+    int k = 1;
+    while (k < 8 && 2.0 * k <= s) k *= 2;
+    return k;
+  }
   DevBuf<__nv_bfloat16> d_prop_w;
   DevBuf<float> d_prop_b;
   DevBuf<__nv_bfloat16> d_feat, d_act0, d_act1;
@@ -379,22 +396,26 @@ struct Engine {
     std::vector<dn::MapDev> hm(maps.size());
     std::vector<int4> t1, t2, ti, tp;
     const int lanes = (patch == 7) ? variant : 1;
-    // Proposal grid: maps grouped by grid size in order of first appearance,
-    // each group's maps contiguous.
+    // Proposal grid: every map at its own stride; maps grouped by grid size
+    // and stride in order of first appearance, each group's maps contiguous.
     std::vector<long long> prop_off(maps.size(), 0);
+    std::vector<int> prop_s(maps.size(), prop_stride);
     prop_groups.clear();
     prop_max_pixels = 0;
     long long prop_points = 0;
     if (prop_on) {
-      const int S = prop_stride;
+      for (size_t a = 0; a < maps.size(); ++a) prop_s[a] = map_prop_stride(*views[maps[a]->ref]);
       std::vector<int> done(maps.size(), 0);
       for (size_t a = 0; a < maps.size(); ++a) {
         if (done[a]) continue;
         const View& ra = *views[maps[a]->ref];
-        PropGroup g{(ra.W + S - 1) / S, (ra.H + S - 1) / S, 0, prop_points};
+        const int S = prop_s[a];
+        PropGroup g{(ra.W + S - 1) / S, (ra.H + S - 1) / S, 0, prop_points, S};
         for (size_t b2 = a; b2 < maps.size(); ++b2) {
           const View& rb = *views[maps[b2]->ref];
-          if (done[b2] || (rb.W + S - 1) / S != g.W || (rb.H + S - 1) / S != g.H) continue;
+          if (done[b2] || prop_s[b2] != S || (rb.W + S - 1) / S != g.W ||
+              (rb.H + S - 1) / S != g.H)
+            continue;
           done[b2] = 1;
           prop_off[b2] = prop_points;
           prop_points += (long long)g.W * g.H;
@@ -403,6 +424,7 @@ struct Engine {
         prop_groups.push_back(g);
       }
     }
+    std::vector<std::vector<int4>> tp_by_s(4);  // sweep tiles of strides 1, 2, 4, 8
     if (active) {
       DN_CUDA(d_acount.alloc(maps.size()));
       DN_CUDA(d_chunk0.alloc(maps.size() + 1));
@@ -452,14 +474,17 @@ struct Engine {
         DN_CUDA(m.prop_init.alloc(3 * npx));
         d.prop_init = m.prop_init.p;
         d.prop_off = prop_off[mi];
-        d.prop_W = (r.W + prop_stride - 1) / prop_stride;
-        d.prop_H = (r.H + prop_stride - 1) / prop_stride;
+        d.prop_S = prop_s[mi];
+        d.prop_W = (r.W + d.prop_S - 1) / d.prop_S;
+        d.prop_H = (r.H + d.prop_S - 1) / d.prop_S;
         prop_max_pixels = std::max(prop_max_pixels, r.W * r.H);
-        // Sweep tiles: (bx / lanes) x by grid points per block.
+        // Sweep tiles: (bx / lanes) x by grid points per block, one list per
+        // stride (the sweep kernel is compiled per stride).
         const int pxs = bx / lanes;
+        const int si = d.prop_S == 1 ? 0 : (d.prop_S == 2 ? 1 : (d.prop_S == 4 ? 2 : 3));
         for (int y = 0; y < (d.prop_H + by - 1) / by; ++y)
           for (int x = 0; x < (d.prop_W + pxs - 1) / pxs; ++x)
-            tp.push_back(make_int4((int)mi, x, y, 0));
+            tp_by_s[si].push_back(make_int4((int)mi, x, y, 0));
       }
       for (int o : m.nbrs) {
         const View& ov = *views[o];
@@ -516,7 +541,13 @@ struct Engine {
     DN_CUDA(cudaMemcpyAsync(d_tiles_init.p, ti.data(), ti.size() * sizeof(int4),
                             cudaMemcpyHostToDevice, stream));
     n_tiles_prop = 0;
+    sweep_ranges.clear();
     if (prop_on) {
+      for (int si = 0; si < 4; ++si) {
+        if (tp_by_s[si].empty()) continue;
+        sweep_ranges.push_back({1 << si, (int)tp.size(), (int)tp_by_s[si].size()});
+        tp.insert(tp.end(), tp_by_s[si].begin(), tp_by_s[si].end());
+      }
       DN_CUDA(d_tiles_prop.alloc(std::max<size_t>(tp.size(), 1)));
       DN_CUDA(cudaMemcpyAsync(d_tiles_prop.p, tp.data(), tp.size() * sizeof(int4),
                               cudaMemcpyHostToDevice, stream));
@@ -578,9 +609,11 @@ struct Engine {
     DN_CHECK(prop_on && d_prop_w.p, "DN_RUN_LEARNED needs dn_batch_set_proposal_net");
     DN_CHECK(patch == 7, "the learned initialisation uses the 7 x 7 patch");
     dn::LaunchArgs a = args(false);
-    a.tiles = d_tiles_prop.p;
-    a.n_tiles = n_tiles_prop;
-    DN_CUDA(dn::launch_sweep(a, d_feat.p, -1, prop_planes, prop_stride, stream));
+    for (const SweepRange& r : sweep_ranges) {
+      a.tiles = d_tiles_prop.p + r.first;
+      a.n_tiles = r.count;
+      DN_CUDA(dn::launch_sweep(a, d_feat.p, -1, prop_planes, r.S, stream));
+    }
     for (const PropGroup& g : prop_groups) {
       const long long n_pix = (long long)g.n * g.W * g.H;
       const __nv_bfloat16* x = d_feat.p + g.off * dn::kFeatC;
@@ -604,7 +637,7 @@ struct Engine {
       }
     }
     DN_CUDA(dn::launch_proposal_to_planes(d_prop_out.p, d_maps.p, (int)maps.size(),
-                                          prop_max_pixels, prop_stride, stream));
+                                          prop_max_pixels, stream));
     return DN_OK;
   }
 
@@ -1656,6 +1689,14 @@ dn_status dn_batch_set_active_lists(dn_batch* b, int on) {
   const dn::DeviceRestore device_restore_;
   DN_CHECK(b, "NULL batch");
   b->eng.active_lists = on ? 1 : 0;
+  b->eng.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_proposal_scale(dn_batch* b, int ref_dim) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(b, "NULL batch");
+  DN_CHECK(ref_dim >= 0, "ref_dim must be >= 0");
+  b->eng.prop_ref_dim = ref_dim;
   b->eng.invalidate();
   return DN_OK;
 }

@@ -167,6 +167,17 @@ __device__ inline long long to_int64_x86(double x) {
 }
 
 // Decision of one pixel; on keep, also the outputs (point, R^T n).
+// R1_normal = (float)R^T * n in float (cv::Matx33f * cv::Vec3f).
+__device__ inline void world_normal(const PruneView& rv, const float nrm[3], float out[3]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float s = 0.0f;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) s = __fadd_rn(s, __fmul_rn((float)rv.R[3 * b + a], nrm[b]));
+    out[a] = s;
+  }
+}
+
 __device__ inline bool prune_pixel(const PruneView* __restrict__ views, int n_views,
                                    const double* Kinv, int i, int j, float thr, float pt[3],
                                    float nrm_out[3]) {
@@ -199,15 +210,20 @@ __device__ inline bool prune_pixel(const PruneView* __restrict__ views, int n_vi
         return false;
     }
   }
-  // R1_normal = (float)R^T * n in float (cv::Matx33f * cv::Vec3f).
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float s = 0.0f;
-#pragma unroll
-    for (int b = 0; b < 3; ++b) s = __fadd_rn(s, __fmul_rn((float)rv.R[3 * b + a], nrm[b]));
-    nrm_out[a] = s;
-  }
+  world_normal(rv, nrm, nrm_out);
   return true;
+}
+
+// The point and world normal of a kept pixel, as prune_pixel computes them
+// (the same operations, without the checks against the other views).
+__device__ inline void prune_point(const PruneView* __restrict__ views, const double* Kinv, int i,
+                                   int j, float pt[3], float nrm_out[3]) {
+  const PruneView& rv = views[0];
+  const size_t pix = (size_t)i * rv.W + j;
+  float nrm[3];
+  normalize3f(rv.plane + (size_t)rv.plane_stride * pix, nrm);
+  backproject_f((double)j, (double)i, (double)rv.depth[pix], Kinv, rv.R, rv.t, pt);
+  world_normal(rv, nrm, nrm_out);
 }
 
 // Block-level steps of the pruner, for any block of B threads (a multiple
@@ -279,9 +295,11 @@ __device__ inline void scan_counts_block(const uint32_t* __restrict__ counts, in
   }
 }
 
+// The kept pixels' points, normals, colours and labels at their offsets
+// (the flags are final: the views and the threshold only name the pruner).
 template <int B>
-__device__ inline void prune_write_block(const PruneView* __restrict__ views, int n_views,
-                                         float thr, const uint8_t* __restrict__ keep,
+__device__ inline void prune_write_block(const PruneView* __restrict__ views, int /*n_views*/,
+                                         float /*thr*/, const uint8_t* __restrict__ keep,
                                          const uint32_t* __restrict__ offsets, PruneOut out,
                                          int block) {
   __shared__ double Kinv[9];
@@ -309,7 +327,7 @@ __device__ inline void prune_write_block(const PruneView* __restrict__ views, in
   const uint32_t pos = warp_base[warp] + __popc(ballot & ((1u << lane) - 1u));
   const int i = (int)(k / W), j = (int)(k - (long)i * W);
   float pt[3], nr[3];
-  prune_pixel(views, n_views, Kinv, i, j, thr, pt, nr);
+  prune_point(views, Kinv, i, j, pt, nr);
   const PruneView& rv = views[0];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {

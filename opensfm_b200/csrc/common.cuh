@@ -67,6 +67,7 @@ struct MapDev {
   float* prop_init;                        // [H][W][3] learned proposal planes
   long long prop_off;                      // first point of the map in the proposal grid
   int prop_W, prop_H;                      // proposal grid (W, H divided by the stride)
+  int prop_S;                              // the map's proposal-grid stride
   // Active-pixel lists (list-mode half-passes): the pixels (y W + x) of
   // the half-pass's colour that are updated, and their number.
   int* alist;                              // [H W] capacity

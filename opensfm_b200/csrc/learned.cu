@@ -955,13 +955,13 @@ __global__ void output_to_planes_kernel(const float* __restrict__ out, int W, in
 // (blockIdx.y = map): the network's (t, sx, sy) at full-resolution pixel
 // (i, j) are the bilinear interpolation of the grid values around
 // (i / S, j / S) (grid point (ys, xs) sits on pixel (S ys, S xs); clamped
-// at the grid's last row and column), then the same depth and plane as
+// at the grid's last row and column), S the map's grid stride
+// (MapDev::prop_S), then the same depth and plane as
 // output_to_planes_kernel.  Writes MapDev::prop_init.
-template <int S>
 __global__ void proposal_to_planes_kernel(const float* __restrict__ out,
                                           const MapDev* __restrict__ maps) {
   const MapDev& m = maps[blockIdx.y];
-  const int W = m.W, H = m.H;
+  const int W = m.W, H = m.H, S = m.prop_S;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= W * H) return;
   const int i = k / W, j = k - i * W;
@@ -975,7 +975,8 @@ __global__ void proposal_to_planes_kernel(const float* __restrict__ out,
   } else {
     const int y0 = min(i / S, Hs - 1), x0 = min(j / S, Ws - 1);
     const int y1 = min(y0 + 1, Hs - 1), x1 = min(x0 + 1, Ws - 1);
-    const float fy = (float)(i - S * y0) * (1.0f / S), fx = (float)(j - S * x0) * (1.0f / S);
+    const float inv = 1.0f / (float)S;  // exact: S is a power of two
+    const float fy = (float)(i - S * y0) * inv, fx = (float)(j - S * x0) * inv;
     const float* q00 = o + 4 * ((size_t)y0 * Ws + x0);
     const float* q01 = o + 4 * ((size_t)y0 * Ws + x1);
     const float* q10 = o + 4 * ((size_t)y1 * Ws + x0);
@@ -1071,7 +1072,11 @@ static cudaError_t conv_fwd_tc(const ConvArgs& c, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   const long long n_img = c.n_pix / ((long long)c.H * c.W);
   const long long tiles = n_img * ((c.H + tc::kTR - 1) / tc::kTR) * ((c.W + tc::kTC - 1) / tc::kTC);
-  const long long grid = std::min<long long>(tiles, (long long)std::max(per_sm, 1) * sms);
+  // The occupancy query has returned one CTA per SM on some calls, where 4
+  // fit (registers) and 5 (shared memory).  The CTAs do not wait on one
+  // another, so the grid follows the launch bound (4 per SM) at least: any
+  // that do not fit run when a slot frees.
+  const long long grid = std::min<long long>(tiles, (long long)std::max(per_sm, 4) * sms);
   kern<<<(unsigned)grid, 128, smem, s>>>(c.x, c.w, c.bias, c.H, c.W, c.cout, c.relu, c.y, c.y32,
                                          tiles, c.x_mask);
   return cudaGetLastError();
@@ -1178,6 +1183,7 @@ cudaError_t launch_sweep(const LaunchArgs& a, __nv_bfloat16* feat, long long map
   if (stride == 1) return sweep_s<1>(a, feat, map_stride, n_planes, s);
   if (stride == 2) return sweep_s<2>(a, feat, map_stride, n_planes, s);
   if (stride == 4) return sweep_s<4>(a, feat, map_stride, n_planes, s);
+  if (stride == 8) return sweep_s<8>(a, feat, map_stride, n_planes, s);
   return cudaErrorInvalidValue;
 }
 cudaError_t launch_l1_loss(const float* pred, const float* target, long long n_pix,
@@ -1207,17 +1213,10 @@ cudaError_t launch_planes_to_target(const float4* state, const float* score, int
   return cudaGetLastError();
 }
 cudaError_t launch_proposal_to_planes(const float* out, const MapDev* maps, int n_maps,
-                                      int max_pixels, int stride, cudaStream_t s) {
+                                      int max_pixels, cudaStream_t s) {
   if (n_maps == 0) return cudaSuccess;
   const dim3 grid((unsigned)((max_pixels + 255) / 256), (unsigned)n_maps);
-  if (stride == 1)
-    proposal_to_planes_kernel<1><<<grid, 256, 0, s>>>(out, maps);
-  else if (stride == 2)
-    proposal_to_planes_kernel<2><<<grid, 256, 0, s>>>(out, maps);
-  else if (stride == 4)
-    proposal_to_planes_kernel<4><<<grid, 256, 0, s>>>(out, maps);
-  else
-    return cudaErrorInvalidValue;
+  proposal_to_planes_kernel<<<grid, 256, 0, s>>>(out, maps);
   return cudaGetLastError();
 }
 

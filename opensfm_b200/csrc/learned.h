@@ -58,8 +58,8 @@ cudaError_t launch_planes_to_target(const float4* state, const float* score, int
                                     int stride, const MapDev* maps, int map, float min_score,
                                     float* target, cudaStream_t s);
 // Network outputs on every map's proposal grid (out + 4 prop_off) -> the
-// maps' MapDev::prop_init planes, upsampled by `stride` (1 or 2).
+// maps' MapDev::prop_init planes, upsampled by each map's MapDev::prop_S.
 cudaError_t launch_proposal_to_planes(const float* out, const MapDev* maps, int n_maps,
-                                      int max_pixels, int stride, cudaStream_t s);
+                                      int max_pixels, cudaStream_t s);
 
 }  // namespace dn

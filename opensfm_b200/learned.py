@@ -60,6 +60,7 @@ class ProposalNet:
         torch = _torch()
         self.stride = stride  # proposal grid the network was trained on
         self.n_planes = n_planes  # sweep planes of its input features
+        self.train_dim = 0  # larger side of its training images (0: not recorded)
         g = torch.Generator().manual_seed(seed)
         self.w32, self.b32, self.w16 = [], [], []
         for cin, cout, relu in LAYERS:
@@ -115,6 +116,7 @@ class ProposalNet:
         net.step = int(z["step"]) if "step" in z else 0
         net.stride = int(z["stride"]) if "stride" in z else 1
         net.n_planes = int(z["planes"]) if "planes" in z else 8
+        net.train_dim = (max(int(z["train_W"]), int(z["train_H"])) if "train_W" in z else 0)
         net.wt_scratch = torch.empty(32 * 9 * 32, dtype=torch.bfloat16, device="cuda")
         return net
 
@@ -396,9 +398,13 @@ def install(net: ProposalNet, b: pydense.Batch, stride: Optional[int] = None,
             n_planes: Optional[int] = None) -> None:
     """Hands the network to the batch: ``b.run(learned=True)`` then sweeps,
     runs the network and installs the proposals on the batch stream (by
-    default on the grid and with the sweep planes it was trained with)."""
+    default on the grid and with the sweep planes it was trained with).  Maps
+    of other sizes than the training images get the stride scaled to their
+    size (``Batch.set_proposal_scale``), so their grid has the training
+    scale."""
     w, bias = net.packed()
     b.set_proposal_net(w, bias, n_planes=n_planes or net.n_planes, stride=stride or net.stride)
+    b.set_proposal_scale(getattr(net, "train_dim", 0))
 
 
 def main(argv=None):

@@ -751,6 +751,12 @@ class Batch(_Handle):
             self._h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), ptr(b, _f), int(n_planes),
             int(stride)))
 
+    def set_proposal_scale(self, ref_dim: int) -> None:
+        """The larger side of the network's training images: each map's
+        proposal grid then uses the stride scaled by its own larger side over
+        ``ref_dim`` (rounded down to 1, 2, 4 or 8); 0: one stride for all."""
+        check(self._L.dn_batch_set_proposal_scale(self._h, int(ref_dim)))
+
     def set_init(self, map_id: int, planes: Optional[np.ndarray]) -> None:
         if planes is None:
             check(self._L.dn_batch_set_init(self._h, int(map_id), None))

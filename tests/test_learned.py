@@ -319,3 +319,36 @@ def test_headline_schedule_reaches_plain_accuracy_on_unseen_scenes():
           f"{q['ms']:.2f} ms, x{p['ms'] / q['ms']:.2f}")
     assert q["accuracy"] >= p["accuracy"]
     assert p["ms"] / q["ms"] >= 4.0
+
+
+def test_per_map_proposal_stride_matches_a_batch_of_that_size():
+    """With the training size recorded (Batch.set_proposal_scale), a 320 x 240
+    map batched with a 640 x 480 map gets the stride-2 grid that the network's
+    stride-4, 640 x 480 training scale asks for: its proposal (a learned run
+    without half-passes) equals the same map's alone at stride 2.  Without
+    the scale it shares the stride-4 grid, and differs."""
+    net = learned.ProposalNet.load()
+    assert net.stride == 4 and net.train_dim == 640
+    small = learned.make_scene(930000, 320, 240)
+    large = learned.make_scene(930001, 640, 480)
+    w, bias = net.packed()
+
+    def run(scenes, stride, scale):
+        b, maps = learned.build_batch(scenes, seed=5)
+        b.set_proposal_net(w, bias, n_planes=net.n_planes, stride=stride)
+        b.set_proposal_scale(scale)
+        b.set_schedule(half_passes=0)
+        b.run(learned=True)
+        b.synchronize()
+        out = [b.get_depth(m) for m in maps]
+        b.close()
+        return out
+
+    scaled = run([small, large], 4, 640)
+    alone = run([small], 2, 0)
+    assert np.array_equal(scaled[0], alone[0])
+    assert (scaled[0] > 0).mean() > 0.3
+    assert (scaled[1] > 0).mean() > 0.3
+    one_stride = run([small, large], 4, 0)
+    assert not np.array_equal(one_stride[0], scaled[0])
+    assert np.array_equal(one_stride[1], scaled[1])
