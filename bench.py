@@ -777,7 +777,7 @@ def run_ours(args):
     head, head_learned, clk = plain_res, False, clk_plain
     learned_res, tried = None, []
     choice_l = choice
-    if ring and len({tuple(sh) for sh in shapes[:n_maps]}) == 1:
+    if len({tuple(sh) for sh in shapes[:n_maps]}) == 1:  # one image size (ring24, aerial)
         LN.install(LN.ProposalNet.load(), b)
         # The cheapest learned schedule whose accuracy is no lower than plain's
         # (medians and means over the maps), from one graph replay each.

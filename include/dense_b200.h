@@ -227,6 +227,13 @@ dn_status dn_batch_set_active_pixels(dn_batch* b, int on, float min_change);
  * the active pixels of each map and runs the half-pass over the lists; on =
  * 0 runs every tile that holds an active pixel.  The maps are the same. */
 dn_status dn_batch_set_active_lists(dn_batch* b, int on);
+/* Settled start for active pixels: with min_score > 0 the initialisation
+ * marks as moved only the pixels whose initial score is below min_score,
+ * and the active rule applies from the first half-pass, so a pixel whose
+ * initial plane scores well is updated only once a neighbour moves.
+ * min_score = 0 (the default): every pixel starts as moved and the first
+ * two half-passes update every pixel. */
+dn_status dn_batch_set_active_seed(dn_batch* b, float min_score);
 /* Initial planes (f32 [H][W][3], reference camera) for one depthmap. */
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes);
 /* Total kept pruner points over all maps of the last run (after sync). */

@@ -209,6 +209,7 @@ struct Engine {
   int active = 0;     // active-pixel half-passes
   float active_tol = 0.f;
   int active_lists = 1;  // active half-passes on compacted pixel lists
+  float seed_score = 0.f;  // > 0: settled start below this initial score (see RunParams)
   DevBuf<int> d_acount, d_chunk0;  // per map: listed pixels; chunk offsets
   DevBuf<int> d_tile_count, d_tile_off;  // per half-pass tile: active pixels, list offset
   // Learned proposal (DN_RUN_LEARNED): network weights, the feature grid of
@@ -597,6 +598,8 @@ struct Engine {
     a.p.normal_range0 = normal_range0;
     a.p.active = active;
     a.p.active_tol = active_tol;
+    a.p.seed_score = seed_score > 0.f ? seed_score : 3.0f;  // NCC <= 1: every pixel moved
+    a.p.active_from = seed_score > 0.f ? 0 : 2;
     a.p.use_knight = use_knight;
     return a;
   }
@@ -733,7 +736,7 @@ struct Engine {
     for (int k = 0; k < hp; ++k) {
       a2.p.colour = k & 1;
       a2.p.pass = k;
-      if (active && active_lists && k >= 2) {
+      if (active && active_lists && k >= a2.p.active_from) {
         DN_CUDA(dn::launch_halfpass_list(sample_half, a2, (int)maps.size(), d_chunk0.p,
                                          d_tile_count.p, d_tile_off.p, stream));
       } else {
@@ -1682,6 +1685,14 @@ dn_status dn_batch_set_active_pixels(dn_batch* b, int on, float min_change) {
   DN_CHECK(min_change >= 0.f && min_change < 1.f, "min_change must be in [0, 1)");
   b->eng.active = on ? 1 : 0;
   b->eng.active_tol = min_change;
+  b->eng.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_active_seed(dn_batch* b, float min_score) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(b, "NULL batch");
+  DN_CHECK(min_score >= 0.f && min_score <= 1.f, "min_score must be in [0, 1]");
+  b->eng.seed_score = min_score;
   b->eng.invalidate();
   return DN_OK;
 }

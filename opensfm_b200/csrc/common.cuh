@@ -105,6 +105,12 @@ struct RunParams {
   // change of the plane counts).
   int active;
   float active_tol;
+  // Settled start (active pixels only): the initialisation marks a pixel
+  // as moved only if its initial score is below seed_score, and the active
+  // rule applies from half-pass active_from (2 by default: the first two
+  // update every pixel; 0 with a settled start).
+  float seed_score;
+  int active_from;
   int learned;  // initialise from MapDev::prop_init instead of MapDev::init
 };
 

@@ -170,7 +170,8 @@ __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev*
       m.state[pix] = st;
       m.score[pix] = sc;
       m.nghbr[pix] = nb;
-      if (p.active) m.changed[pix] = st.w != 0.0f ? kValid : 0;
+      if (p.active)
+        m.changed[pix] = st.w == 0.0f ? 0 : (sc < p.seed_score ? (kValid | kMoved) : kValid);
     }
   }
   flush_taps(taps, p.taps);
@@ -467,7 +468,7 @@ __device__ inline void halfpass_tile(const MapDev* __restrict__ maps,
   float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
   if (i >= HPZ && i < H - HPZ && j >= HPZ && j < W - HPZ) st = m.state[pix];
   bool run = st.w != 0.0f;
-  if (p.active && p.pass >= 2) {
+  if (p.active && p.pass >= p.active_from) {
     if (run) {
       // Interior pixel, so the 4 neighbours are inside the map.  Their flags
       // were written by the previous half-pass, the pixel's own by the one

@@ -471,11 +471,13 @@ class Schedule:
     sample: int = 0  # Batch.set_candidate_views mode
     active: float = 0.0  # > 0: active pixels, a depth moves by more than this
     knights: bool = False
+    seed: float = 0.0  # > 0: settled start below this initial score (Batch.set_active_seed)
 
     def apply(self, b: pydense.Batch) -> None:
         b.set_schedule(half_passes=self.half_passes, **self.kw)
         b.set_candidate_views(self.sample)
         b.set_active_pixels(self.active > 0, self.active)
+        b.set_active_seed(self.seed)
         b.set_knight_moves(self.knights)
 
 

@@ -730,6 +730,12 @@ class Batch(_Handle):
         ``min_change`` relative; 0: any change of the plane)."""
         check(self._L.dn_batch_set_active_pixels(self._h, int(bool(on)), float(min_change)))
 
+    def set_active_seed(self, min_score: float) -> None:
+        """Settled start: pixels whose initial score is at least ``min_score``
+        start as settled and the active rule applies from the first
+        half-pass; 0 (default): every pixel starts as moved."""
+        check(self._L.dn_batch_set_active_seed(self._h, float(min_score)))
+
     def set_active_lists(self, on: bool) -> None:
         """Active half-passes over compacted lists of the active pixels (the
         default) or over every tile that holds one; the maps are the same."""
