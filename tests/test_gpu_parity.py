@@ -934,13 +934,15 @@ def test_bounded_wait_expiry_reports_timeout():
 
 
 
-@pytest.mark.parametrize("mode,tuning", [(0, (32, 4, 2)), (1, (32, 4, 2)), (2, (32, 4, 4)),
-                                         (1, (32, 4, 1))])
-def test_active_lists_match_tile_launch(scene, mode, tuning):
+@pytest.mark.parametrize("mode,tuning,seed", [(0, (32, 4, 2), 0.0), (1, (32, 4, 2), 0.0),
+                                              (2, (32, 4, 4), 0.0), (1, (32, 4, 1), 0.0),
+                                              (2, (32, 4, 2), 0.8)])
+def test_active_lists_match_tile_launch(scene, mode, tuning, seed):
     """Active half-passes over compacted pixel lists give the same maps, bit
     for bit, as running every tile that holds an active pixel: an update
     reads only the other colour and its random streams are keyed by the
-    pixel, so the order of the list does not matter."""
+    pixel, so the order of the list does not matter.  Also with a settled
+    start (active from the first half-pass)."""
     Ks, Rs, ts = cams(scene)
     b = pydense.Batch()
     for K, R, t, im in zip(Ks, Rs, ts, scene.images):
@@ -953,6 +955,7 @@ def test_active_lists_match_tile_launch(scene, mode, tuning):
     b.set_candidate_views(mode)
     b.set_schedule(half_passes=8)
     b.set_active_pixels(True, 0.003)
+    b.set_active_seed(seed)
     out = []
     for lists in (True, False):
         b.set_active_lists(lists)
