@@ -234,6 +234,12 @@ dn_status dn_batch_set_active_lists(dn_batch* b, int on);
  * min_score = 0 (the default): every pixel starts as moved and the first
  * two half-passes update every pixel. */
 dn_status dn_batch_set_active_seed(dn_batch* b, float min_score);
+/* The random initialisation as the fallback of given planes (learned
+ * proposals or dn_batch_set_init): with on = 1 every pixel with a given
+ * plane also draws the reference's random plane (RandomInitialization,
+ * depthmap.cc:237-256) and keeps whichever scores higher on the same
+ * view(s), the given one on a tie.  Default 0: the given plane. */
+dn_status dn_batch_set_init_fallback(dn_batch* b, int on);
 /* Initial planes (f32 [H][W][3], reference camera) for one depthmap. */
 dn_status dn_batch_set_init(dn_batch* b, int map_id, const float* planes);
 /* Total kept pruner points over all maps of the last run (after sync). */

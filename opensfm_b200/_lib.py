@@ -86,6 +86,7 @@ _SIGNATURES = {
     "dn_batch_set_active_pixels": ([_vp, _i, ctypes.c_float], _i),
     "dn_batch_set_active_lists": ([_vp, _i], _i),
     "dn_batch_set_active_seed": ([_vp, ctypes.c_float], _i),
+    "dn_batch_set_init_fallback": ([_vp, _i], _i),
     "dn_batch_set_proposal_scale": ([_vp, _i], _i),
     "dn_batch_set_knight_moves": ([_vp, _i], _i),
     "dn_batch_set_proposal_net": ([_vp, ctypes.POINTER(ctypes.c_uint16), _f, _i, _i], _i),

@@ -210,6 +210,7 @@ struct Engine {
   float active_tol = 0.f;
   int active_lists = 1;  // active half-passes on compacted pixel lists
   float seed_score = 0.f;  // > 0: settled start below this initial score (see RunParams)
+  int init_fallback = 0;   // given / learned planes: random plane where it scores higher
   DevBuf<int> d_acount, d_chunk0;  // per map: listed pixels; chunk offsets
   DevBuf<int> d_tile_count, d_tile_off;  // per half-pass tile: active pixels, list offset
   // Learned proposal (DN_RUN_LEARNED): network weights, the feature grid of
@@ -599,6 +600,7 @@ struct Engine {
     a.p.active = active;
     a.p.active_tol = active_tol;
     a.p.seed_score = seed_score > 0.f ? seed_score : 3.0f;  // NCC <= 1: every pixel moved
+    a.p.init_fallback = init_fallback;
     a.p.active_from = seed_score > 0.f ? 0 : 2;
     a.p.use_knight = use_knight;
     return a;
@@ -1685,6 +1687,13 @@ dn_status dn_batch_set_active_pixels(dn_batch* b, int on, float min_change) {
   DN_CHECK(min_change >= 0.f && min_change < 1.f, "min_change must be in [0, 1)");
   b->eng.active = on ? 1 : 0;
   b->eng.active_tol = min_change;
+  b->eng.invalidate();
+  return DN_OK;
+}
+dn_status dn_batch_set_init_fallback(dn_batch* b, int on) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(b, "NULL batch");
+  b->eng.init_fallback = on ? 1 : 0;
   b->eng.invalidate();
   return DN_OK;
 }

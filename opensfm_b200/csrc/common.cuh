@@ -112,6 +112,7 @@ struct RunParams {
   float seed_score;
   int active_from;
   int learned;  // initialise from MapDev::prop_init instead of MapDev::init
+  int init_fallback;  // given planes: keep the random plane where it scores higher
 };
 
 // ------------------------------------------------------------------ RNG

@@ -148,21 +148,45 @@ __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev*
         given = v.z != 0.0f;
         if (given) depth = depth_of_plane(j, i, m.Kinv_d, v);
       }
-      if (!given) {
-        // UniformRand(log min, log max) then exp; normal (U(-1,1), U(-1,1), -1).
-        depth = expf(fmaf(m.log_max - m.log_min, u01(r.x), m.log_min));
+      // The reference's random plane: UniformRand(log min, log max) then
+      // exp; normal (U(-1,1), U(-1,1), -1).  Drawn for every pixel (the same
+      // draws), used where no plane is given or, with the fallback, where it
+      // scores better than the given one.
+      const bool draw = !given || p.init_fallback;
+      float3 vr = make_float3(0.f, 0.f, 0.f);
+      float dr = 0.f;
+      if (draw) {
+        dr = expf(fmaf(m.log_max - m.log_min, u01(r.x), m.log_min));
         const float3 n = make_float3(fmaf(2.f, u01(r.y), -1.f), fmaf(2.f, u01(r.z), -1.f), -1.f);
-        v = plane_from_depth_normal((float)j, (float)i, m.Kinv_d, depth, n);
+        vr = plane_from_depth_normal((float)j, (float)i, m.Kinv_d, dr, n);
+      }
+      if (!given) {
+        v = vr;
+        depth = dr;
       }
       Patch<HPZ, L> pt;
       pt.build(tile, pitch, ly, lx, lane, mask);
-      const Hyp h = make_hyp(m.Kinv, v, (float)j, (float)i);
-      if (SAMPLE) {
-        nb = 1 + (int)(r.w % (uint32_t)m.n_pairs);
-        const PairDev& pr = spv.p[nb - 1];
-        sc = pt.view(spv.v[pr.view], pr, h, (float)j, (float)i, taps);
-      } else {
-        sc = patch_max<HPZ, L>(pt, spv.v, spv.p, m.n_pairs, h, (float)j, (float)i, nb, taps);
+      auto score = [&](float3 w, int& view) {
+        const Hyp h = make_hyp(m.Kinv, w, (float)j, (float)i);
+        if (SAMPLE) {
+          view = 1 + (int)(r.w % (uint32_t)m.n_pairs);
+          const PairDev& pr = spv.p[view - 1];
+          return pt.view(spv.v[pr.view], pr, h, (float)j, (float)i, taps);
+        }
+        return patch_max<HPZ, L>(pt, spv.v, spv.p, m.n_pairs, h, (float)j, (float)i, view, taps);
+      };
+      sc = score(v, nb);
+      if (given && p.init_fallback) {
+        // The random initialisation as the fallback: the given plane is kept
+        // unless the random one scores higher on the same view(s).
+        int nb2 = 0;
+        const float sc2 = score(vr, nb2);
+        if (sc2 > sc) {
+          v = vr;
+          depth = dr;
+          sc = sc2;
+          nb = nb2;
+        }
       }
       st = make_float4(v.x, v.y, v.z, depth);
     }

@@ -472,12 +472,14 @@ class Schedule:
     active: float = 0.0  # > 0: active pixels, a depth moves by more than this
     knights: bool = False
     seed: float = 0.0  # > 0: settled start below this initial score (Batch.set_active_seed)
+    fallback: bool = False  # random plane where it scores higher (Batch.set_init_fallback)
 
     def apply(self, b: pydense.Batch) -> None:
         b.set_schedule(half_passes=self.half_passes, **self.kw)
         b.set_candidate_views(self.sample)
         b.set_active_pixels(self.active > 0, self.active)
         b.set_active_seed(self.seed)
+        b.set_init_fallback(self.fallback)
         b.set_knight_moves(self.knights)
 
 

@@ -730,6 +730,11 @@ class Batch(_Handle):
         ``min_change`` relative; 0: any change of the plane)."""
         check(self._L.dn_batch_set_active_pixels(self._h, int(bool(on)), float(min_change)))
 
+    def set_init_fallback(self, on: bool) -> None:
+        """Given planes (learned proposals) compete with the reference's random
+        initialisation per pixel: the higher score on the same view(s) wins."""
+        check(self._L.dn_batch_set_init_fallback(self._h, int(bool(on))))
+
     def set_active_seed(self, min_score: float) -> None:
         """Settled start: pixels whose initial score is at least ``min_score``
         start as settled and the active rule applies from the first

@@ -352,3 +352,30 @@ def test_per_map_proposal_stride_matches_a_batch_of_that_size():
     one_stride = run([small, large], 4, 0)
     assert not np.array_equal(one_stride[0], scaled[0])
     assert np.array_equal(one_stride[1], scaled[1])
+
+
+@pytest.mark.parametrize("mode", [0, 2])
+def test_random_initialisation_fallback_keeps_the_better_plane(mode):
+    """With the fallback on, the learned proposal competes with the
+    reference's random plane per pixel (same view(s)): after the
+    initialisation alone every pixel's score is at least its score with the
+    proposal alone, and pixels that switch score strictly higher."""
+    net = learned.ProposalNet.load()
+    scenes = [learned.make_scene(s, 640, 480) for s in (940000, 940001)]
+    out = {}
+    for fb in (False, True):
+        b, maps = learned.build_batch(scenes, seed=3)
+        learned.install(net, b)
+        learned.Schedule("init", "learned", 0, {}, sample=mode, fallback=fb).apply(b)
+        b.run(learned=True)
+        b.synchronize()
+        out[fb] = [b.get(m) for m in maps]
+        b.close()
+    switched = 0
+    for (d0, p0, s0, n0), (d1, p1, s1, n1) in zip(out[False], out[True]):
+        valid = p0[..., 2] != 0
+        assert (s1[valid] >= s0[valid]).all()
+        moved = valid & (p1 != p0).any(axis=-1)
+        assert (s1[moved] > s0[moved]).all()
+        switched += int(moved.sum())
+    assert switched > 0
