@@ -310,7 +310,7 @@ dn_status dn_fp32_peak(double* tflops, double* ms);
  * enqueues work and returns.
  * ---------------------------------------------------------------------- */
 /* Network input features (n_planes planes, 1..15) of every depthmap of the
- * batch on the grid of every `stride`-th pixel (1, 2 or 4; grid point (ys, xs) is pixel
+ * batch on the grid of every `stride`-th pixel (1, 2, 4 or 8; grid point (ys, xs) is pixel
  * (stride ys, stride xs), grid size ceil(W / stride) x ceil(H / stride)):
  * feat is a device BF16 buffer [n_maps][Hs][Ws][32] with map stride
  * `map_stride` elements (>= Hs * Ws * 32 of the largest map).  Runs on the
@@ -327,7 +327,7 @@ dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float
  * weights = BF16 bit patterns of the 6 layers' [cout][9 x 32] matrices one
  * after the other (cout 32 for layers 0-4, 4 for layer 5: 46,080 values),
  * biases = FP32 [32] x 5 then [4] (164 values).  Features are swept with
- * n_planes planes (1..15) on the grid of every `stride`-th pixel (1, 2 or 4),
+ * n_planes planes (1..15) on the grid of every `stride`-th pixel (1, 2, 4 or 8),
  * the network runs on that grid (maps of one grid size in one batch) and
  * its output is interpolated back to every pixel.  weights = NULL removes
  * the network. */

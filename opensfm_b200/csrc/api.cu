@@ -1735,7 +1735,7 @@ dn_status dn_batch_set_proposal_net(dn_batch* b, const uint16_t* weights, const 
   }
   DN_CHECK(biases, "biases must not be NULL");
   DN_CHECK(n_planes >= 1 && n_planes <= dn::kMaxSweepPlanes, "n_planes must be 1..15");
-  DN_CHECK(stride == 1 || stride == 2 || stride == 4, "stride must be 1, 2 or 4");
+  DN_CHECK(stride == 1 || stride == 2 || stride == 4 || stride == 8, "stride must be 1, 2, 4 or 8");
   // Layers 0-4: [32][288]; layer 5: [4][288] stored in a [32][288] slot
   // whose rows 4..31 stay zero (the kernel reads only cout rows).
   constexpr int kL = Engine::kPropLayers, kRow = 9 * 32;
@@ -1959,7 +1959,7 @@ dn_status dn_batch_sweep_features(dn_batch* b, void* feat, int64_t map_stride, i
   const dn::DeviceRestore device_restore_;
   DN_CHECK(b && feat, "NULL argument");
   DN_CHECK(n_planes >= 1 && n_planes <= dn::kMaxSweepPlanes, "n_planes must be 1..15");
-  DN_CHECK(stride == 1 || stride == 2 || stride == 4, "stride must be 1, 2 or 4");
+  DN_CHECK(stride == 1 || stride == 2 || stride == 4 || stride == 8, "stride must be 1, 2, 4 or 8");
   Engine& e = b->eng;
   DN_CUDA(cudaSetDevice(e.device));
   DN_CHECK(e.patch == 7, "the learned initialisation uses the 7 x 7 patch");
@@ -1994,7 +1994,7 @@ dn_status dn_batch_targets(dn_batch* b, float* target, int64_t map_stride, float
                            int stride) {
   const dn::DeviceRestore device_restore_;
   DN_CHECK(b && target, "NULL argument");
-  DN_CHECK(stride == 1 || stride == 2 || stride == 4, "stride must be 1, 2 or 4");
+  DN_CHECK(stride == 1 || stride == 2 || stride == 4 || stride == 8, "stride must be 1, 2, 4 or 8");
   Engine& e = b->eng;
   DN_CHECK(e.computed, "no PatchMatch result computed yet");
   DN_CUDA(cudaSetDevice(e.device));

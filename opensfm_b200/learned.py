@@ -199,10 +199,22 @@ class SceneViews:
 
 
 def make_scene(seed: int, W: int, H: int, kind: Optional[str] = None, n_match: int = 6) -> SceneViews:
-    """Box scene on a camera ring, or terrain under a nadir grid (by seed parity)."""
+    """Box scene on a camera ring, or terrain under a nadir grid (by seed
+    parity); kind "aerial": 300 x 300 m terrain with 40 buildings under a
+    nadir or 45-degree oblique grid (one of four headings) at 60 m."""
     rng = np.random.default_rng(seed)
     kind = kind or ("box" if seed % 2 == 0 else "terrain")
-    if kind == "box":
+    if kind == "aerial":
+        scene = S.terrain_scene(seed, size=300.0, amp=8.0, n_buildings=40)
+        tilt = 45.0 if rng.random() < 0.5 else 0.0
+        grid = S.nadir_cameras(300.0, 60.0, W, H, forward_overlap=0.7, side_overlap=0.6,
+                               oblique_deg=tilt, yaw_deg=90.0 * int(rng.integers(4)))
+        centres = np.stack([c.center for c in grid])
+        c0 = centres[int(rng.integers(len(grid)))]
+        order = np.argsort(np.linalg.norm(centres - c0, axis=1))[: n_match + 1]
+        cams = [grid[k] for k in order]
+        ref = 0
+    elif kind == "box":
         scene = S.box_scene(seed)
         n = n_match + 1
         cams = S.ring_cameras(n, W, H, step_deg=10.0, start_deg=float(rng.uniform(0, 360)))
@@ -269,7 +281,7 @@ def targets(b: pydense.Batch, n_maps: int, H: int, W: int, min_score: float = 0.
 
 def make_dataset(seeds: Sequence[int], W: int = 640, H: int = 480, chunk: int = 50,
                  iterations: int = 3, stride: int = 2, n_planes: int = 8,
-                 gt_filter: float = 0.0, log=None):
+                 gt_filter: float = 0.0, log=None, kind: Optional[str] = None):
     """Features on the proposal grid and plain-PatchMatch targets at the same
     grid points for every seed (device tensors).  gt_filter > 0 keeps only
     the targets whose depth is within that relative error of the rendered
@@ -279,7 +291,7 @@ def make_dataset(seeds: Sequence[int], W: int = 640, H: int = 480, chunk: int = 
     t0 = time.time()
     Hs, Ws = grid_shape(H, W, stride)
     for c0 in range(0, len(seeds), chunk):
-        scenes = [make_scene(s, W, H) for s in seeds[c0:c0 + chunk]]
+        scenes = [make_scene(s, W, H, kind=kind) for s in seeds[c0:c0 + chunk]]
         b, maps = build_batch(scenes, iterations=iterations, seed=int(seeds[c0]) + 7)
         b.run()
         b.synchronize()
@@ -343,20 +355,34 @@ def train(net: ProposalNet, feat, tgt, n_maps: int, H: int, W: int, steps: int =
     schedule.  A run can stop early (``stop_step``; with ``checkpoint`` the
     state is saved there) and continue from ``load_checkpoint``'s state
     (``start_step``, ``generator``) with the same ``steps``."""
+    return train_sets(net, [(feat, tgt, n_maps, H, W)], steps=steps, batch=batch, lr=lr,
+                      normal_weight=normal_weight, seed=seed, log=log, start_step=start_step,
+                      generator=generator, stop_step=stop_step, checkpoint=checkpoint)
+
+
+def train_sets(net: ProposalNet, sets, steps: int = 1500, batch: int = 8, lr: float = 2e-3,
+               normal_weight: float = 0.1, seed: int = 0, log=None, start_step: int = 0,
+               generator=None, stop_step: Optional[int] = None,
+               checkpoint: Optional[str] = None):
+    """``train`` over several datasets of different grid shapes, sets =
+    [(feat, tgt, n_maps, H, W), ...]: each step draws its dataset with
+    probability proportional to n_maps, then its batch from that dataset
+    (one dataset: the same draws as ``train``)."""
     torch = _torch()
     L = _lib.load()
     g = generator if generator is not None else torch.Generator(device="cpu").manual_seed(seed)
-    per = H * W
-    n_pix = batch * per
     loss_acc = torch.zeros(1, dtype=torch.float32, device="cuda")
     count = torch.zeros(1, dtype=torch.float32, device="cuda")
-    dpred = torch.empty(n_pix * 4, dtype=torch.bfloat16, device="cuda")
-    fv = feat.view(n_maps, per * FEAT_C)
-    tv = tgt.view(n_maps, per * 4)
+    views = [(f.view(n, H * W * FEAT_C), t.view(n, H * W * 4), n, H, W) for f, t, n, H, W in sets]
+    weights = torch.tensor([float(v[2]) for v in views])
     history = []
     t0 = time.time()
     end = steps if stop_step is None else min(stop_step, steps)
     for step in range(start_step, end):
+        k = 0 if len(views) == 1 else int(torch.multinomial(weights, 1, generator=g))
+        fv, tv, n_maps, H, W = views[k]
+        n_pix = batch * H * W
+        dpred = torch.empty(n_pix * 4, dtype=torch.bfloat16, device="cuda")
         idx = torch.randint(0, n_maps, (batch,), generator=g).cuda()
         xb = fv.index_select(0, idx).reshape(-1).contiguous()
         tb = tv.index_select(0, idx).reshape(-1).contiguous()
@@ -422,6 +448,12 @@ def main(argv=None):
     ap.add_argument("--size", default="640x480", help="training scene size WxH")
     ap.add_argument("--stride", type=int, default=4, help="proposal grid stride (1, 2 or 4)")
     ap.add_argument("--planes", type=int, default=15, help="sweep planes (1..15)")
+    ap.add_argument("--portrait", type=int, default=0,
+                    help="also train on this many portrait scenes (the size transposed; "
+                         "seeds 200000 and up)")
+    ap.add_argument("--aerial", type=int, default=0,
+                    help="also train on this many aerial scenes (terrain with buildings, nadir "
+                         "or oblique) at twice the size and stride (seeds 300000 and up)")
     ap.add_argument("--gt-filter", type=float, default=0.01,
                     help="keep only targets within this relative depth error of the ground truth")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
@@ -446,13 +478,28 @@ def main(argv=None):
     valid = float((tgt.view(-1, 4)[:, 3] > 0).float().mean().item())
     log(f"target coverage {valid:.3f}")
     Hs, Ws = grid_shape(H, W, args.stride)
+    torch = _torch()
+    n_main = len(seeds)
+    if args.aerial:
+        # Twice the size at twice the stride: the same grid as the main scenes.
+        fa, ta = make_dataset(list(range(300000, 300000 + args.aerial)), W=2 * W, H=2 * H,
+                              stride=2 * args.stride, n_planes=args.planes,
+                              gt_filter=args.gt_filter, log=log, kind="aerial", chunk=25)
+        feat, tgt = torch.cat([feat, fa]), torch.cat([tgt, ta])
+        n_main += args.aerial
+    sets = [(feat, tgt, n_main, Hs, Ws)]
+    if args.portrait:
+        fp, tp = make_dataset(list(range(200000, 200000 + args.portrait)), W=H, H=W,
+                              stride=args.stride, n_planes=args.planes,
+                              gt_filter=args.gt_filter, log=log)
+        sets.append((fp, tp, args.portrait, Ws, Hs))
     net = ProposalNet(seed=args.seed, stride=args.stride, n_planes=args.planes)
-    hist = train(net, feat, tgt, len(seeds), Hs, Ws, steps=args.steps, batch=args.batch,
-                 lr=args.lr, log=log)
+    hist = train_sets(net, sets, steps=args.steps, batch=args.batch, lr=args.lr, log=log)
     net.save(args.out, history=np.array(hist), scenes=np.array(args.scenes),
              seeds_start=np.array(seeds[0]), stride=np.array(args.stride),
              train_W=np.array(W), train_H=np.array(H), gt_filter=np.array(args.gt_filter),
-             steps=np.array(args.steps))
+             steps=np.array(args.steps), portrait=np.array(args.portrait),
+             aerial=np.array(args.aerial))
     log(f"saved {args.out}")
 
 
