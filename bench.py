@@ -62,19 +62,17 @@ TRAFFIC_SAMPLE_TILE, TRAFFIC_PLAIN_TILE = 318.8e6, 318.3e6
 # above plain's accuracy there.  Mode 2: one view per candidate from the
 # initialisation on; pixels whose neighbourhood moved by less than 1 % are
 # left alone.  In order:
-# - the settled-start schedules whose held-out accuracy beats plain's by at
-#   least as much as the 4-half-pass schedule without it (+0.007), fastest
-#   first (held-out 0.9029 / 5.78 ms, 0.9033 / 6.05, 0.9034 / 6.25 against
+# - the settled-start schedule, whose held-out accuracy beats plain's by at
+#   least as much as the same schedule without it (0.9031 / 5.93 ms against
 #   plain's 0.8959 / 47.5 ms);
-# - the schedules without it, fastest first (0.9032 / 6.50 ms, ...);
+# - the schedules without it, fastest first (0.9034 / 6.65, 0.9044 / 7.50,
+#   0.9041 / 7.88, 0.9038 / 8.18 ms);
 # - the schedules with the random-initialisation fallback, fastest first
-#   (0.9026 / 8.69 ms, ...), for views unlike the training scenes (oblique,
-#   portrait); the last scores every view per candidate (0.9030 / 23.2 ms).
-LEARNED_SCHEDULES = ((4, 2, 0.01, 2, 0.9, 0), (4, 3, 0.01, 2, 0.9, 0), (6, 2, 0.01, 2, 0.8, 0),
-                     (4, 2, 0.01, 2, 0.0, 0), (4, 3, 0.01, 2, 0.0, 0), (6, 2, 0.01, 2, 0.0, 0),
-                     (6, 3, 0.01, 2, 0.0, 0), (8, 3, 0.01, 2, 0.0, 0), (10, 3, 0.01, 2, 0.0, 0),
-                     (8, 3, 0.01, 2, 0.0, 1), (10, 3, 0.01, 2, 0.0, 1), (12, 3, 0.01, 2, 0.0, 1),
-                     (8, 6, 0.01, 2, 0.0, 1), (12, 6, 0.01, 2, 0.0, 1), (6, 6, 0.01, 0, 0.0, 1))
+#   (0.9024 / 8.73, 0.9023 / 9.05 ms), for views unlike the training scenes;
+#   the last scores every view per candidate.
+LEARNED_SCHEDULES = ((4, 2, 0.01, 2, 0.9, 0), (4, 2, 0.01, 2, 0.0, 0), (6, 3, 0.01, 2, 0.0, 0),
+                     (8, 3, 0.01, 2, 0.0, 0), (10, 3, 0.01, 2, 0.0, 0), (8, 3, 0.01, 2, 0.0, 1),
+                     (10, 3, 0.01, 2, 0.0, 1), (6, 6, 0.01, 0, 0.0, 1))
 
 
 # ---------------------------------------------------------------- workload

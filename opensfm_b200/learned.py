@@ -448,10 +448,10 @@ def main(argv=None):
     ap.add_argument("--size", default="640x480", help="training scene size WxH")
     ap.add_argument("--stride", type=int, default=4, help="proposal grid stride (1, 2 or 4)")
     ap.add_argument("--planes", type=int, default=15, help="sweep planes (1..15)")
-    ap.add_argument("--portrait", type=int, default=0,
+    ap.add_argument("--portrait", type=int, default=600,
                     help="also train on this many portrait scenes (the size transposed; "
                          "seeds 200000 and up)")
-    ap.add_argument("--aerial", type=int, default=0,
+    ap.add_argument("--aerial", type=int, default=400,
                     help="also train on this many aerial scenes (terrain with buildings, nadir "
                          "or oblique) at twice the size and stride (seeds 300000 and up)")
     ap.add_argument("--gt-filter", type=float, default=0.01,
