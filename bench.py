@@ -52,9 +52,12 @@ FLOPS_PER_TAP = 25  # affine warp 8 + bilinear 11 + NCC sums 6 (FMA = 2)
 # The plain GPU PatchMatch: the reference's random initialisation and
 # red-black half-passes with every matching view scored per candidate.
 PLAIN_HALF_PASSES, PLAIN_KNIGHTS = 2 * ITERS, False
-# DRAM bytes per tile half-pass on the ring workload, from ncu captures
-# (halfpass_kernel<3, true, 2> and <3, false, 2>, tuning 32,4,2).
-TRAFFIC_SAMPLE_TILE, TRAFFIC_PLAIN_TILE = 318.8e6, 318.3e6
+# DRAM bytes per half-pass on the ring workload, from ncu captures at tuning
+# 32,4,2: a tile half-pass over every pixel of a colour
+# (halfpass_kernel<3, true, 2> and <3, false, 2>), and the first list
+# half-pass of the learned schedule with a settled start
+# (halfpass_list_kernel<3, true, 2>).
+TRAFFIC_SAMPLE_TILE, TRAFFIC_PLAIN_TILE, TRAFFIC_SETTLED_LIST = 318.8e6, 318.3e6, 278.0e6
 # Learned schedules (half-passes, refinements per update, active-pixel
 # tolerance, candidate-view mode, settled-start score, random-initialisation
 # fallback), chosen on 12 held-out 640x480 scenes (seeds 900000-900011, none
@@ -931,12 +934,14 @@ def run_ours(args):
             # DRAM bytes (read + write) of one tile half-pass over every pixel
             # of a colour, from the ncu capture of this workload at tuning
             # 32,4,2 (not measured inside the bench).
-            "traffic": (TRAFFIC_SAMPLE_TILE if head_sched.sample else TRAFFIC_PLAIN_TILE)
+            "traffic": ((TRAFFIC_SETTLED_LIST if head_sched.seed > 0 else TRAFFIC_SAMPLE_TILE)
+                        if head_sched.sample else TRAFFIC_PLAIN_TILE)
             if ring and n_maps == len(vs.cameras) else None,
             "traffic_source": "ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of one "
-                              "tile half-pass over every pixel of a colour, 24 x 640x480, "
-                              "profiles/halfpass_sample_and_list_ring24_640x480.md; a "
-                              "list half-pass moves less (199 MB at half-pass 3)",
+                              "half-pass, 24 x 640x480: the first list half-pass with a settled "
+                              "start, else a tile half-pass over every pixel of a colour "
+                              "(profiles/halfpass_sample_and_list_ring24_640x480.md); later "
+                              "list half-passes move less",
             "peak_source": "measured FP32 FMA loop on this GPU (dn_fp32_peak); "
                            "MEASURED_PEAKS.json has no FP32 figure",
             "algorithmic": f"{FLOPS_PER_TAP} flops per NCC tap x {head['halfpass_taps']} taps "
