@@ -108,7 +108,9 @@ __device__ inline float patch_variance(const float* tile, int pitch, int ly, int
 // L lanes per pixel (L = 1, or 2 / 4 for the 7 x 7 patch): lane group g of
 // a warp row owns one pixel; every lane of a group computes the same values
 // and lane 0 writes them.
-template <int HPZ, bool SAMPLE, int L>
+// FB: the random-initialisation fallback of given planes (RunParams::
+// init_fallback), compiled in only where it is used.
+template <int HPZ, bool SAMPLE, int L, bool FB>
 __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
                                  const PairDev* __restrict__ pairs, const int4 tl,
                                  const RunParams& p) {
@@ -152,7 +154,7 @@ __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev*
       // exp; normal (U(-1,1), U(-1,1), -1).  Drawn for every pixel (the same
       // draws), used where no plane is given or, with the fallback, where it
       // scores better than the given one.
-      const bool draw = !given || p.init_fallback;
+      const bool draw = !given || FB;
       float3 vr = make_float3(0.f, 0.f, 0.f);
       float dr = 0.f;
       if (draw) {
@@ -176,7 +178,7 @@ __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev*
         return patch_max<HPZ, L>(pt, spv.v, spv.p, m.n_pairs, h, (float)j, (float)i, view, taps);
       };
       sc = score(v, nb);
-      if (given && p.init_fallback) {
+      if (FB && given) {
         // The random initialisation as the fallback: the given plane is kept
         // unless the random one scores higher on the same view(s).
         int nb2 = 0;
@@ -201,11 +203,11 @@ __device__ inline void init_tile(const MapDev* __restrict__ maps, const ViewDev*
   flush_taps(taps, p.taps);
 }
 
-template <int HPZ, bool SAMPLE, int L>
+template <int HPZ, bool SAMPLE, int L, bool FB>
 __global__ void __launch_bounds__(128, (kMinBlocksL<HPZ, L>))
 init_kernel(const MapDev* __restrict__ maps, const ViewDev* __restrict__ views,
             const PairDev* __restrict__ pairs, const int4* __restrict__ tiles, RunParams p) {
-  init_tile<HPZ, SAMPLE, L>(maps, views, pairs, tiles[blockIdx.x], p);
+  init_tile<HPZ, SAMPLE, L, FB>(maps, views, pairs, tiles[blockIdx.x], p);
 }
 
 // ----------------------------------------------------------------------
@@ -841,8 +843,12 @@ patchmatch_persistent_kernel(const MapDev* __restrict__ maps, const ViewDev* __r
                              const int4* __restrict__ tiles_post, int n_post, int n_half,
                              RunParams p, unsigned* sync, const PersistentTail tail) {
   const unsigned nb = gridDim.x;
-  for (int t = next_tile(sync + 2); t < n_init; t = next_tile(sync + 2))
-    init_tile<HPZ, false, L>(maps, views, pairs, tiles_init[t], p);
+  for (int t = next_tile(sync + 2); t < n_init; t = next_tile(sync + 2)) {
+    if (p.init_fallback)
+      init_tile<HPZ, false, L, true>(maps, views, pairs, tiles_init[t], p);
+    else
+      init_tile<HPZ, false, L, false>(maps, views, pairs, tiles_init[t], p);
+  }
   if (!grid_barrier(sync, nb, p.error)) return;
   RunParams q = p;
   for (int k = 0; k < n_half; ++k) {
@@ -961,10 +967,19 @@ static cudaError_t launch_hpz(Stage stage, bool sample, const LaunchArgs& a, cud
   switch (stage) {
     case Stage::kInit: {
       const size_t smem = sizeof(float) * (px + 2 * HPZ) * (a.by + 2 * HPZ);
-      if (sample)
-        init_kernel<HPZ, true, L><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+      const bool fb = a.p.init_fallback != 0;
+      if (sample && fb)
+        init_kernel<HPZ, true, L, true><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs,
+                                                                     a.tiles, a.p);
+      else if (sample)
+        init_kernel<HPZ, true, L, false><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs,
+                                                                      a.tiles, a.p);
+      else if (fb)
+        init_kernel<HPZ, false, L, true><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs,
+                                                                      a.tiles, a.p);
       else
-        init_kernel<HPZ, false, L><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs, a.tiles, a.p);
+        init_kernel<HPZ, false, L, false><<<a.n_tiles, blk, smem, s>>>(a.maps, a.views, a.pairs,
+                                                                       a.tiles, a.p);
       break;
     }
     case Stage::kBruteForce: {
