@@ -69,12 +69,15 @@ TRAFFIC_SAMPLE_TILE, TRAFFIC_PLAIN_TILE, TRAFFIC_SETTLED_LIST = 318.8e6, 318.3e6
 #   least as much as the same schedule without it (0.9031 / 5.93 ms against
 #   plain's 0.8959 / 47.5 ms);
 # - the schedules without it, fastest first (0.9034 / 6.65, 0.9044 / 7.50,
-#   0.9041 / 7.88, 0.9038 / 8.18 ms);
+#   0.9041 / 7.88, 0.9038 / 8.18, 0.9035 / 8.34, 0.9042 / 8.89 ms), the last
+#   a full initialisation on every view, then one view per candidate
+#   (mode 1; 0.9048 / 8.98 ms);
 # - the schedules with the random-initialisation fallback, fastest first
 #   (0.9024 / 8.73, 0.9023 / 9.05 ms), for views unlike the training scenes;
 #   the last scores every view per candidate.
 LEARNED_SCHEDULES = ((4, 2, 0.01, 2, 0.9, 0), (4, 2, 0.01, 2, 0.0, 0), (6, 3, 0.01, 2, 0.0, 0),
-                     (8, 3, 0.01, 2, 0.0, 0), (10, 3, 0.01, 2, 0.0, 0), (8, 3, 0.01, 2, 0.0, 1),
+                     (8, 3, 0.01, 2, 0.0, 0), (10, 3, 0.01, 2, 0.0, 0), (12, 3, 0.01, 2, 0.0, 0),
+                     (8, 6, 0.01, 2, 0.0, 0), (6, 6, 0.01, 1, 0.0, 0), (8, 3, 0.01, 2, 0.0, 1),
                      (10, 3, 0.01, 2, 0.0, 1), (6, 6, 0.01, 0, 0.0, 1))
 
 
