@@ -65,8 +65,8 @@ TRAFFIC_SAMPLE_TILE, TRAFFIC_PLAIN_TILE, TRAFFIC_SETTLED_LIST = 318.8e6, 318.3e6
 # above plain's accuracy there.  Mode 2: one view per candidate from the
 # initialisation on; pixels whose neighbourhood moved by less than 1 % are
 # left alone.  In order:
-# - the settled-start schedule, whose held-out accuracy beats plain's by at
-#   least as much as the same schedule without it (0.9031 / 5.93 ms against
+# - the settled-start schedule, whose held-out accuracy is within 0.0005 of
+#   the same schedule without it (0.9031 / 5.93 ms against 0.9034 / 6.65;
 #   plain's 0.8959 / 47.5 ms);
 # - the schedules without it, fastest first (0.9034 / 6.65, 0.9044 / 7.50,
 #   0.9041 / 7.88, 0.9038 / 8.18, 0.9035 / 8.34, 0.9042 / 8.89 ms), the last
