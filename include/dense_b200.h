@@ -257,6 +257,27 @@ dn_status dn_batch_last_taps(dn_batch* b, uint64_t* taps);
  * the batch stream; the host buffer must stay valid until the next
  * dn_batch_synchronize. */
 dn_status dn_batch_set_view_image(dn_batch* b, int view_id, const uint8_t* image, int stride);
+/* Pipelined batch I/O (no reference counterpart).  Both calls return at
+ * once, and every run gives the same results as with
+ * dn_batch_set_view_image / dn_batch_get_depths at the same points of the
+ * call sequence.  Their host copies run on two more streams of the batch
+ * (uploads, readbacks), so they overlap a run enqueued before (uploads) or
+ * after (readbacks); the views uploaded since the last run are prepared
+ * (FP16 image, coefficient table) together, in one launch, by the next
+ * call that reads views (dn_batch_run, dn_batch_sweep_features,
+ * dn_batch_set_view_image).  Host buffers must be pinned for the overlap
+ * (pageable ones work, with the copy done before the call returns) and stay
+ * valid, and unmodified for an upload, until dn_batch_synchronize; the timer
+ * events (dn_batch_timer_record) include these copies.
+ *
+ * upload_view_image: the pixels of view view_id for runs enqueued after
+ * the call.
+ * get_depths_async: the final (clean = 0) or cleaned (clean = 1) depth of n
+ * maps, as left by the runs enqueued before the call, into depths[k] (f32
+ * [H][W] of map map_ids[k]); complete after dn_batch_synchronize. */
+dn_status dn_batch_upload_view_image(dn_batch* b, int view_id, const uint8_t* image, int stride);
+dn_status dn_batch_get_depths_async(dn_batch* b, int n, const int* map_ids, float* const* depths,
+                                    int clean);
 /* Per-stage device times (ms) of the last run made with DN_RUN_TIMING:
  * out[0] init, out[1] all PatchMatch half-passes, out[2] post-process,
  * out[3] cleaner and pruner, out[4] whole run, out[5] the learned proposal

@@ -80,6 +80,7 @@ _SIGNATURES = {
     "dn_batch_synchronize": ([_vp], _i),
     "dn_batch_get_depthmap": ([_vp, _i, _f, _f, _f, _i32, _f], _i),
     "dn_batch_get_depths": ([_vp, _i, _i32, _vp, _i], _i),
+    "dn_batch_get_depths_async": ([_vp, _i, _i32, _vp, _i], _i),
     "dn_batch_set_init": ([_vp, _i, _f], _i),
     "dn_batch_set_schedule": ([_vp, _i, _i, _i, _i, ctypes.c_float, ctypes.c_float], _i),
     "dn_batch_set_candidate_views": ([_vp, _i], _i),
@@ -95,6 +96,7 @@ _SIGNATURES = {
                              ctypes.POINTER(ctypes.c_int64)], _i),
     "dn_batch_last_taps": ([_vp, ctypes.POINTER(ctypes.c_uint64)], _i),
     "dn_batch_set_view_image": ([_vp, _i, _u8, _i], _i),
+    "dn_batch_upload_view_image": ([_vp, _i, _u8, _i], _i),
     "dn_batch_last_timings": ([_vp, _f, _i, ctypes.POINTER(ctypes.c_uint64)], _i),
     "dn_batch_copy_depth_device": ([_vp, _i, _vp], _i),
     "dn_batch_timer_record": ([_vp, _i], _i),

@@ -7,6 +7,7 @@
 // opensfm/src/lib/dense/depthmap.h:57-153) are thin wrappers over it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -163,6 +164,9 @@ struct View {
   DevBuf<uint8_t> mask;
   DevBuf<uint2> quad;  // bilinear coefficient table, 4 x FP16 per entry
   DevBuf<uint8_t> gray;  // u8 copy (pruner colour when none is given)
+  // Pipelined replacement of the pixels (dn_batch_upload_view_image): the
+  // host copy lands here on the upload stream.
+  DevBuf<uint8_t> upload;
 };
 
 struct Map {
@@ -265,20 +269,77 @@ struct Engine {
   bool timed_learned = false;
   cudaEvent_t ev[kEvents] = {};
   bool timed = false;
+  // Pipelined host I/O: uploads run on `up` and readbacks on `down`, beside
+  // the work on the batch stream (two streams, so that the next step's
+  // uploads do not queue behind a readback that waits for the current run).
+  // - An upload copies the pixels into the view's upload buffer on `up` and
+  //   lists the view as pending.  The next work on the batch stream that
+  //   reads views (flush_uploads) waits for `up` (ev_uploaded), prepares
+  //   every pending view in one launch, and records ev_consumed, which later
+  //   uploads wait for before they overwrite an upload buffer.
+  // - A readback gathers the depths into one of two device staging buffers
+  //   on the batch stream (ev_staged), then copies them to the host on
+  //   `down` (ev_stage_done[k]: staging buffer k is free again).
+  cudaStream_t up = nullptr, down = nullptr;
+  std::vector<int> pending_uploads;
+  DevBuf<float> d_stage[2];
+  cudaEvent_t ev_uploaded = nullptr, ev_consumed = nullptr;
+  cudaEvent_t ev_staged = nullptr, ev_stage_done[2] = {}, ev_io_tail[2] = {};
+  int stage_next = 0;
 
   ~Engine() {
     if (graph) cudaGraphExecDestroy(graph);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {ev_uploaded, ev_consumed, ev_staged, ev_stage_done[0],
+                          ev_stage_done[1], ev_io_tail[0], ev_io_tail[1]})
+      if (e) cudaEventDestroy(e);
+    if (up) cudaStreamDestroy(up);
+    if (down) cudaStreamDestroy(down);
     if (stream) cudaStreamDestroy(stream);
   }
 
   dn_status init() {
     DN_CUDA(cudaGetDevice(&device));
     DN_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    DN_CUDA(cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking));
+    DN_CUDA(cudaStreamCreateWithFlags(&down, cudaStreamNonBlocking));
     DN_CUDA(d_taps.alloc(4));
     DN_CUDA(d_error.alloc(1));
     for (auto& e : ev) DN_CUDA(cudaEventCreate(&e));
+    for (cudaEvent_t* e : {&ev_uploaded, &ev_consumed, &ev_staged, &ev_stage_done[0],
+                           &ev_stage_done[1], &ev_io_tail[0], &ev_io_tail[1]})
+      DN_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return DN_OK;
+  }
+
+  // Prepares the views uploaded since the last flush, in stream order on the
+  // batch stream (see `up` above).
+  dn_status flush_uploads() {
+    if (pending_uploads.empty()) return DN_OK;
+    DN_CUDA(cudaSetDevice(device));
+    DN_CUDA(cudaEventRecord(ev_uploaded, up));
+    DN_CUDA(cudaStreamWaitEvent(stream, ev_uploaded, 0));
+    std::vector<dn::PrepareJob> jobs;
+    jobs.reserve(pending_uploads.size());
+    for (int v : pending_uploads) {
+      View& w = *views[v];
+      const dn::TableGeom tg = dn::table_geom(w.W, w.H);
+      jobs.push_back({w.upload.p, w.gray.p, w.img.p, w.quad.p, w.W, w.H, tg.TP, tg.TW, tg.TH,
+                      w.cbias});
+    }
+    pending_uploads.clear();
+    DN_CUDA(dn::launch_prepare_views(jobs.data(), (int)jobs.size(), stream));
+    DN_CUDA(cudaEventRecord(ev_consumed, stream));
+    return DN_OK;
+  }
+
+  // Makes the batch stream wait for everything enqueued on the I/O streams.
+  dn_status join_io() {
+    DN_CUDA(cudaEventRecord(ev_io_tail[0], up));
+    DN_CUDA(cudaEventRecord(ev_io_tail[1], down));
+    DN_CUDA(cudaStreamWaitEvent(stream, ev_io_tail[0], 0));
+    DN_CUDA(cudaStreamWaitEvent(stream, ev_io_tail[1], 0));
     return DN_OK;
   }
 
@@ -375,6 +436,7 @@ struct Engine {
 
   // Builds the per-pair homography factors (FP64) and the device tables.
   dn_status prepare() {
+    DN_TRY(flush_uploads());
     if (!dirty) return DN_OK;
     DN_CUDA(cudaSetDevice(device));
     std::vector<dn::ViewDev> hv(views.size());
@@ -889,10 +951,31 @@ struct Engine {
     if (stride <= 0) stride = w.W;
     DN_CHECK(stride >= w.W, "stride must be >= width");
     DN_CUDA(cudaSetDevice(device));
+    DN_TRY(flush_uploads());  // an earlier pipelined upload of the view must not win
     const dn::TableGeom tg = dn::table_geom(w.W, w.H);
     DN_CUDA(cudaMemcpy2DAsync(w.gray.p, w.W, image, stride, w.W, w.H, cudaMemcpyHostToDevice, stream));
     DN_CUDA(dn::launch_prepare_view(w.gray.p, w.W, w.H, w.W, w.img.p, w.quad.p, tg.TP, tg.TW, tg.TH,
                                     w.cbias, stream));
+    return DN_OK;
+  }
+
+  // The same replacement, pipelined: the host copy runs on the upload stream
+  // while earlier batch-stream work (a run) is still executing.  The view's
+  // FP16 image and coefficient table are rebuilt by the next work on the
+  // batch stream that reads views, for every uploaded view at once.
+  dn_status upload_view_image(int v, const uint8_t* image, int stride) {
+    DN_CHECK(v >= 0 && v < (int)views.size(), "view id out of range");
+    DN_CHECK(image, "image must not be NULL");
+    View& w = *views[v];
+    if (stride <= 0) stride = w.W;
+    DN_CHECK(stride >= w.W, "stride must be >= width");
+    DN_CUDA(cudaSetDevice(device));
+    DN_CUDA(w.upload.alloc((size_t)w.W * w.H));
+    // The last flush has read every upload buffer.
+    DN_CUDA(cudaStreamWaitEvent(up, ev_consumed, 0));
+    DN_CUDA(cudaMemcpy2DAsync(w.upload.p, w.W, image, stride, w.W, w.H, cudaMemcpyHostToDevice, up));
+    if (std::find(pending_uploads.begin(), pending_uploads.end(), v) == pending_uploads.end())
+      pending_uploads.push_back(v);
     return DN_OK;
   }
 
@@ -921,6 +1004,8 @@ struct Engine {
 
   dn_status finish() {
     DN_CUDA(cudaStreamSynchronize(stream));
+    DN_CUDA(cudaStreamSynchronize(up));
+    DN_CUDA(cudaStreamSynchronize(down));
     int err = 0;
     DN_CUDA(cudaMemcpy(&err, d_error.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return fail(DN_TIMEOUT, "a bounded device-side wait expired");
@@ -985,6 +1070,47 @@ struct Engine {
                               (size_t)r.W * r.H * sizeof(float), cudaMemcpyDeviceToHost, stream));
     }
     DN_CUDA(cudaStreamSynchronize(stream));
+    return DN_OK;
+  }
+
+  // The same readback, pipelined: the depths as the batch stream leaves them
+  // at this point are gathered into a staging buffer on the batch stream (one
+  // launch), then copied to the host on the readback stream, so a run enqueued
+  // next overlaps the host copies.  Two staging buffers alternate; a third
+  // readback in flight waits for the first one's host copies.
+  dn_status fetch_depths_async(int n, const int* ids, float* const* outs, int clean) {
+    DN_CHECK(n >= 0 && (n == 0 || (ids && outs)), "NULL argument");
+    DN_CHECK(computed, "no result computed yet");
+    DN_CUDA(cudaSetDevice(device));
+    std::vector<const float*> src(n);
+    std::vector<size_t> count(n), off(n);
+    size_t total = 0;
+    for (int k = 0; k < n; ++k) {
+      DN_CHECK(ids[k] >= 0 && ids[k] < (int)maps.size(), "depthmap id out of range");
+      DN_CHECK(outs[k], "NULL output buffer");
+      const Map& m = *maps[ids[k]];
+      DN_CHECK(!clean || m.clean.p, "the depthmap was not cleaned");
+      src[k] = clean ? m.clean.p : m.depth.p;
+      count[k] = (size_t)views[m.ref]->W * views[m.ref]->H;
+      off[k] = total;
+      total += (count[k] + 3) & ~(size_t)3;  // 16-byte aligned arrays
+    }
+    if (n == 0) return DN_OK;
+    const int s = stage_next;
+    stage_next ^= 1;
+    DevBuf<float>& st = d_stage[s];
+    if (st.n < total) {
+      DN_CUDA(cudaEventSynchronize(ev_stage_done[s]));
+      DN_CUDA(st.alloc(total));
+    }
+    DN_CUDA(cudaStreamWaitEvent(stream, ev_stage_done[s], 0));
+    DN_CUDA(dn::launch_gather_floats(src.data(), count.data(), off.data(), n, st.p, stream));
+    DN_CUDA(cudaEventRecord(ev_staged, stream));
+    DN_CUDA(cudaStreamWaitEvent(down, ev_staged, 0));
+    for (int k = 0; k < n; ++k)
+      DN_CUDA(cudaMemcpyAsync(outs[k], st.p + off[k], count[k] * sizeof(float),
+                              cudaMemcpyDeviceToHost, down));
+    DN_CUDA(cudaEventRecord(ev_stage_done[s], down));
     return DN_OK;
   }
 
@@ -1845,6 +1971,17 @@ dn_status dn_batch_get_depths(dn_batch* b, int n, const int* map_ids, float* con
   DN_CHECK(b, "NULL batch");
   return b->eng.fetch_depths(n, map_ids, depths, clean);
 }
+dn_status dn_batch_get_depths_async(dn_batch* b, int n, const int* map_ids, float* const* depths,
+                                    int clean) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(b, "NULL batch");
+  return b->eng.fetch_depths_async(n, map_ids, depths, clean);
+}
+dn_status dn_batch_upload_view_image(dn_batch* b, int view_id, const uint8_t* image, int stride) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(b, "NULL batch");
+  return b->eng.upload_view_image(view_id, image, stride);
+}
 dn_status dn_batch_pruned_count(dn_batch* b, int64_t* count) {
   const dn::DeviceRestore device_restore_;
   DN_CHECK(b && count, "NULL argument");
@@ -1929,6 +2066,9 @@ dn_status dn_batch_timer_record(dn_batch* b, int slot) {
   DN_CHECK(b, "NULL batch");
   DN_CHECK(slot == 0 || slot == 1, "timer slot must be 0 or 1");
   DN_CUDA(cudaSetDevice(b->eng.device));
+  // The timer covers the pipelined host copies too: the batch stream first
+  // waits for everything enqueued on the I/O streams.
+  DN_TRY(b->eng.join_io());
   DN_CUDA(cudaEventRecord(b->eng.ev[5 + slot], b->eng.stream));
   return DN_OK;
 }

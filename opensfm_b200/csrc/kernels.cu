@@ -5,6 +5,8 @@
 // Every kernel works on a batch: blockIdx.x indexes a tile list of
 // (map, tile_x, tile_y) built on the host, so one launch covers every
 // depthmap of a reconstruction whatever their sizes.
+#include <algorithm>
+
 #include "cleanprune.cuh"
 #include "common.cuh"
 #include "kernels.h"
@@ -51,6 +53,59 @@ __global__ void build_quad_kernel(const __half* __restrict__ img, int W, int H, 
   const __half2 lo = __floats2half2_rn(q.x, q.y), hi = __floats2half2_rn(q.z, q.w);
   quad[(size_t)ty * TP + tx] = make_uint2(*reinterpret_cast<const unsigned*>(&lo),
                                           *reinterpret_cast<const unsigned*>(&hi));
+}
+
+// Both steps above for a set of views in one launch, from the u8 pixels:
+// a pixel value v converted to FP16 and back is v exactly, so the entries
+// are build_quad_kernel's.  Thread (tx, ty) of job blockIdx.z writes table
+// entry (tx, ty) and, where (ix, iy) is a pixel, its FP16 and u8 copies
+// (the table's [-kPad, W-2+kPad] x [-kPad, H-2+kPad] covers every pixel).
+struct PrepareJobs {
+  PrepareJob job[kPrepareJobs];
+};
+
+__global__ void __launch_bounds__(256) prepare_views_kernel(const __grid_constant__ PrepareJobs p) {
+  const PrepareJob& j = p.job[blockIdx.z];
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x, ty = blockIdx.y;
+  if (tx >= j.TP || ty >= j.TH) return;
+  const int ix = tx - kPad, iy = ty - kPad;
+  const int W = j.W, H = j.H;
+  float4 q = make_float4(-j.cbias, 0.f, 0.f, 0.f);
+  if (tx < j.TW && ix >= 0 && ix < W && iy >= 0 && iy < H) {
+    const size_t o = (size_t)iy * W + ix;
+    const uint8_t u = j.src[o];
+    j.gray[o] = u;
+    j.img[o] = __ushort2half_rn(u);
+    if (ix <= W - 2 && iy <= H - 2) {
+      const float q00 = (float)u, q01 = (float)j.src[o + 1];
+      const float q10 = (float)j.src[o + W], q11 = (float)j.src[o + W + 1];
+      q = make_float4(q00 - j.cbias, q01 - q00, q10 - q00, q11 - q10 - q01 + q00);
+    }
+  }
+  const __half2 lo = __floats2half2_rn(q.x, q.y), hi = __floats2half2_rn(q.z, q.w);
+  j.quad[(size_t)ty * j.TP + tx] = make_uint2(*reinterpret_cast<const unsigned*>(&lo),
+                                              *reinterpret_cast<const unsigned*>(&hi));
+}
+
+struct GatherArrays {
+  const float* src[kGatherArrays];
+  size_t count[kGatherArrays];
+  size_t off[kGatherArrays];
+};
+
+// Array blockIdx.y: 16-byte moves for the bulk (source and destination
+// offsets are multiples of 4 floats: device allocations are 256-byte
+// aligned), then the tail.
+__global__ void __launch_bounds__(256) gather_floats_kernel(const __grid_constant__ GatherArrays g,
+                                                            float* __restrict__ dst) {
+  const float* __restrict__ s = g.src[blockIdx.y];
+  float* __restrict__ d = dst + g.off[blockIdx.y];
+  const size_t n = g.count[blockIdx.y], n4 = n / 4;
+  const size_t step = (size_t)gridDim.x * blockDim.x;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n4; k += step)
+    reinterpret_cast<float4*>(d)[k] = __ldg(reinterpret_cast<const float4*>(s) + k);
+  for (size_t k = 4 * n4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += step)
+    d[k] = s[k];
 }
 
 // ----------------------------------------------------------------------
@@ -1067,6 +1122,46 @@ cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, _
   build_quad_kernel<<<dim3((TP + 255) / 256, TH), 256, 0, s>>>(d_img, W, H, cbias, d_quad, TP, TW,
                                                                TH);
   return cudaGetLastError();
+}
+
+cudaError_t launch_prepare_views(const PrepareJob* jobs, int n, cudaStream_t s) {
+  for (int k0 = 0; k0 < n; k0 += kPrepareJobs) {
+    const int m = std::min(kPrepareJobs, n - k0);
+    PrepareJobs p{};
+    int TP = 0, TH = 0;
+    for (int k = 0; k < m; ++k) {
+      p.job[k] = jobs[k0 + k];
+      TP = std::max(TP, jobs[k0 + k].TP);
+      TH = std::max(TH, jobs[k0 + k].TH);
+    }
+    prepare_views_kernel<<<dim3((TP + 255) / 256, TH, m), 256, 0, s>>>(p);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_gather_floats(const float* const* src, const size_t* count, const size_t* off,
+                                 int n, float* dst, cudaStream_t s) {
+  for (int k0 = 0; k0 < n; k0 += kGatherArrays) {
+    const int m = std::min(kGatherArrays, n - k0);
+    GatherArrays g{};
+    size_t most = 0;
+    for (int k = 0; k < m; ++k) {
+      if (off[k0 + k] % 4) return cudaErrorInvalidValue;
+      g.src[k] = src[k0 + k];
+      g.count[k] = count[k0 + k];
+      g.off[k] = off[k0 + k];
+      most = std::max(most, count[k0 + k]);
+    }
+    // About 4 resident 256-thread blocks per SM over all arrays of the launch.
+    const int bx = (int)std::max<size_t>(1, std::min<size_t>((most / 4 + 255) / 256,
+                                                             (size_t)std::max(1, 592 / m)));
+    gather_floats_kernel<<<dim3(bx, m), 256, 0, s>>>(g, dst);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_postprocess_plain(const float* in, float* out, int W, int H, cudaStream_t s) {

@@ -78,6 +78,27 @@ cudaError_t launch_prepare_view(const uint8_t* d_u8, int W, int H, int stride, _
                                 uint2* d_quad, int TP, int TW, int TH, float cbias,
                                 cudaStream_t s);
 
+// Re-uploaded views prepared together: per job, the u8 pixels at `src`
+// (W x H, packed) become the view's u8 copy, FP16 image and coefficient
+// table (the same values as launch_prepare_view) in one pass.  Any n; one
+// launch per kPrepareJobs jobs (the jobs travel as kernel parameters).
+struct PrepareJob {
+  const uint8_t* src;
+  uint8_t* gray;
+  __half* img;
+  uint2* quad;
+  int W, H, TP, TW, TH;
+  float cbias;
+};
+constexpr int kPrepareJobs = 48;
+cudaError_t launch_prepare_views(const PrepareJob* jobs, int n, cudaStream_t s);
+
+// Packs n float arrays (src[k], count[k] floats) into dst, array k at
+// dst + off[k]; every off[k] a multiple of 4.  One launch per kGatherArrays.
+constexpr int kGatherArrays = 96;
+cudaError_t launch_gather_floats(const float* const* src, const size_t* count, const size_t* off,
+                                 int n, float* dst, cudaStream_t s);
+
 // Table geometry of a W x H view: used width TW = W - 1 + 2P, rows
 // TH = H - 1 + 2P, pitch TP = 1024 k - 1 >= TW (k a power of two) and the
 // floor constant M = 2^23 + 2^22 / k (see ViewDev).

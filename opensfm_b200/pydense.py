@@ -671,6 +671,7 @@ class Batch(_Handle):
         super().__init__("dn_batch_create", "dn_batch_destroy")
         self._shapes: List[tuple] = []
         self._map_shapes: List[tuple] = []
+        self._io_keep: list = []  # host buffers of pipelined copies in flight
 
     def add_view(self, K, R, t, image, mask=None) -> int:
         K = _mat(K, (3, 3), "K")
@@ -811,6 +812,17 @@ class Batch(_Handle):
             raise ValueError("image must keep the view's size")
         check(self._L.dn_batch_set_view_image(self._h, int(view_id), ptr(im, _u8), W))
 
+    def upload_view_image(self, view_id: int, image: np.ndarray) -> None:
+        """Pipelined re-upload of a view's pixels for the runs enqueued after
+        it: the host copy runs beside a run already enqueued.  ``image``
+        (pinned for the overlap) is kept referenced, and must stay unmodified,
+        until ``synchronize``."""
+        H, W = self._shapes[view_id]
+        if image.dtype != np.uint8 or not image.flags.c_contiguous or image.shape != (H, W):
+            raise ValueError("image must be a C-contiguous uint8 array of the view's size")
+        check(self._L.dn_batch_upload_view_image(self._h, int(view_id), ptr(image, _u8), W))
+        self._io_keep.append(image)
+
     def set_tuning(self, bx: int = 32, by: int = 4, variant: int = 2) -> None:
         check(self._L.dn_batch_set_tuning(self._h, int(bx), int(by), int(variant)))
 
@@ -832,6 +844,7 @@ class Batch(_Handle):
 
     def synchronize(self) -> None:
         check(self._L.dn_batch_synchronize(self._h))
+        self._io_keep = []
 
     def get(self, map_id: int, clean: bool = False) -> list:
         H, W = self._map_shapes[map_id]
@@ -873,6 +886,27 @@ class Batch(_Handle):
         ptr_arr = (ctypes.c_void_p * len(ids))(*[o.ctypes.data for o in outs])
         check(self._L.dn_batch_get_depths(self._h, len(ids), id_arr,
                                           ctypes.cast(ptr_arr, ctypes.c_void_p), int(bool(clean))))
+        return outs
+
+    def get_depths_async(self, map_ids, outs, clean: bool = False):
+        """Pipelined readback of the final (or cleaned) depths as the runs
+        enqueued before it leave them, into C-contiguous float32 (H, W) host
+        arrays ``outs`` (pinned for the overlap); complete after
+        ``synchronize``, which also releases the kept references."""
+        ids = [int(m) for m in map_ids]
+        if len(outs) != len(ids):
+            raise ValueError("one output per map")
+        for m, o in zip(ids, outs):
+            if not 0 <= m < len(self._map_shapes):
+                raise IndexError(f"depthmap id {m} out of range")
+            if o.dtype != np.float32 or not o.flags.c_contiguous or o.shape != self._map_shapes[m]:
+                raise ValueError("outputs must be C-contiguous float32 arrays of the map's shape")
+        id_arr = (ctypes.c_int32 * len(ids))(*ids)
+        ptr_arr = (ctypes.c_void_p * len(ids))(*[o.ctypes.data for o in outs])
+        check(self._L.dn_batch_get_depths_async(self._h, len(ids), id_arr,
+                                                ctypes.cast(ptr_arr, ctypes.c_void_p),
+                                                int(bool(clean))))
+        self._io_keep.append(list(outs))
         return outs
 
     def last_taps(self) -> int:

@@ -839,6 +839,113 @@ def test_batch_matches_single_estimator(scene):
         assert np.array_equal(a, w)
 
 
+def test_pipelined_io_matches_synchronous(scene):
+    """upload_view_image / get_depths_async keep the batch's stream order:
+    three pipelined steps over two image sets (A, B, A), with every upload
+    enqueued while the previous run may still execute and three readbacks
+    over the two staging buffers, give the synchronous results bit for bit."""
+    import torch
+
+    Ks, Rs, ts = cams(scene)
+    mn, mx = S.depth_range(scene.depths[0])
+    imgs_a = [np.ascontiguousarray(im) for im in scene.images]
+    imgs_b = [np.ascontiguousarray(255 - im) for im in scene.images]
+    b = pydense.Batch()
+    for K, R, t, im in zip(Ks, Rs, ts, imgs_a):
+        b.add_view(K, R, t, im)
+    maps = [b.add_depthmap(0, [1, 2, 3, 4], mn, mx), b.add_depthmap(2, [0, 1, 3, 4], mn, mx)]
+    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=3, seed=9)
+
+    want = {}
+    for key, imgs in (("b", imgs_b), ("a", imgs_a)):
+        for v, im in enumerate(imgs):
+            b.set_view_image(v, im)
+        b.run(graph=True)
+        b.synchronize()
+        want[key] = b.get_depths(maps)
+    assert not np.array_equal(want["a"][0], want["b"][0])
+
+    keep = []
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype))).pin_memory()
+        keep.append(t)
+        arr = t.numpy()
+        arr[...] = a
+        return arr
+
+    sets = {"a": [pinned(im) for im in imgs_a], "b": [pinned(im) for im in imgs_b]}
+    order = ["a", "b", "a"]
+    outs = [[pinned(np.zeros_like(w)) for w in want["a"]] for _ in order]
+    for step, key in enumerate(order):
+        for v, im in enumerate(sets[key]):
+            b.upload_view_image(v, im)
+        b.run(graph=True)
+        b.get_depths_async(maps, outs[step])
+    b.synchronize()
+    for step, key in enumerate(order):
+        for got, w in zip(outs[step], want[key]):
+            assert np.array_equal(got, w), (step, key)
+    with pytest.raises(ValueError):
+        b.get_depths_async(maps, outs[0][:1])
+    with pytest.raises(ValueError):
+        b.get_depths_async(maps, outs[0], clean=True)  # not cleaned
+    # A synchronous replacement after a pending upload wins.
+    for v, im in enumerate(sets["b"]):
+        b.upload_view_image(v, im)
+    for v, im in enumerate(imgs_a):
+        b.set_view_image(v, im)
+    b.run(graph=True)
+    b.synchronize()
+    for got, w in zip(b.get_depths(maps), want["a"]):
+        assert np.array_equal(got, w)
+
+
+def test_pipelined_upload_mixed_sizes(golden):
+    """Views of different sizes prepared by one batched launch give the same
+    PatchMatch, cleaned depths and pruner points as the per-view synchronous
+    preparation."""
+    g = golden("estimator_mixed_v4_p7.npz")
+    Ks, Rs, ts, ims, gts = _mixed(g)
+    n = len(ims)
+    assert len({im.shape for im in ims}) > 1
+    b = pydense.Batch()
+    for K, R, t, im in zip(Ks, Rs, ts, ims):
+        b.add_view(K, R, t, im)
+    for v in range(n):
+        mn, mx = S.depth_range(gts[v])
+        b.add_depthmap(v, [o for o in range(n) if o != v], mn, mx)
+    for v in range(n):
+        b.set_clean_views(v, [o for o in range(n) if o != v])
+    b.set_params(patch_size=7, min_patch_sd=1.0, iterations=2, same_depth_threshold=0.01,
+                 min_consistent_views=1, seed=5)
+    inv = [np.ascontiguousarray(255 - im) for im in ims]
+
+    def result():
+        return ([b.get(m, clean=True) for m in range(n)], b.pruned_count())
+
+    for v, im in enumerate(inv):
+        b.set_view_image(v, im)
+    b.run(prune=True)
+    b.synchronize()
+    want_inv = result()
+    for v, im in enumerate(ims):
+        b.set_view_image(v, im)
+    b.run(prune=True)
+    b.synchronize()
+    want = result()
+    for images, ref in ((inv, want_inv), (ims, want)):
+        for v, im in enumerate(images):
+            b.upload_view_image(v, np.ascontiguousarray(im))
+        b.run(prune=True)
+        b.synchronize()
+        got = result()
+        assert got[1] == ref[1]
+        for ga, wa in zip(got[0], ref[0]):
+            for x, y in zip(ga, wa):
+                assert np.array_equal(x, y)
+
+
 def test_batch_clean_and_prune_match_single_objects(scene):
     """Batched cleaner / pruner (one run for all maps) against the
     single-object DepthmapCleaner / DepthmapPruner on the same inputs."""
