@@ -761,6 +761,7 @@ def run_ours(args):
                   "source": "opensfm_b200.autotune"}
     choice = tuning["choice"]
     peak = pydense.fp32_peak()
+    walk_ceiling = pydense.walk_ceiling()  # G taps/s of the table walk alone
 
     def leg(sch, learned, choice):
         """Warm-up, one instrumented run (per-stage launches), accuracy, then
@@ -917,6 +918,7 @@ def run_ours(args):
                 f"min_patch_sd {MIN_SD}, cleaner 0.01 / 3 views, pruner 0.01; "
                 f"{sum(h * w for h, w in shapes[:n_maps]) / 1e6:.2f} Mpx per step")
     head_choice = choice_l if head_learned else choice
+    hp_gtaps = head["halfpass_taps"] / (head["stage_ms"]["halfpasses"] * 1e-3) / 1e9
     hp_variant = head_choice[2] & 15
     line = {
         "metric": METRIC if ring else (
@@ -959,6 +961,13 @@ def run_ours(args):
                               "list half-passes move less",
             "peak_source": "measured FP32 FMA loop on this GPU (dn_fp32_peak); "
                            "MEASURED_PEAKS.json has no FP32 figure",
+            "walk_ceiling": {
+                "gtaps_s": walk_ceiling,
+                "halfpass_gtaps_s": hp_gtaps,
+                "frac": hp_gtaps / walk_ceiling,
+                "source": "dn_walk_ceiling: 7x7 affine walks through the FP16 coefficient "
+                          "table with the production sampler and the three NCC sums alone, one "
+                          "thread per pixel of a 1024x768 view (measured on this GPU)"},
             "algorithmic": f"{FLOPS_PER_TAP} flops per NCC tap x {head['halfpass_taps']} taps "
                            f"in {head_sched.half_passes} half-passes "
                            f"({head['stage_ms']['halfpasses']:.2f} ms)",

@@ -319,6 +319,13 @@ dn_status dn_check_bounded_wait(int blocks, int64_t max_spins, float* ms);
 /* Measures the device's FP32 FMA throughput (TFLOP/s, FMA = 2 flops) with a
  * register-resident FMA loop on every SM; used as the scoring roofline. */
 dn_status dn_fp32_peak(double* tflops, double* ms);
+/* Measures the ceiling of the scoring walk (no reference counterpart): G
+ * taps/s of 7 x 7 affine walks through the FP16 coefficient table with the
+ * production sampler and the three weighted NCC sums, one thread per pixel
+ * of a 1024 x 768 view, and nothing else (no candidate generation, warp
+ * setup, lane groups or NCC finish); the half-pass's tap rate over it is the
+ * share of the walk's own ceiling it reaches. */
+dn_status dn_walk_ceiling(double* gtaps, double* ms);
 
 /* ------------------------------------------------------------------------
  * Learned initialisation (no reference counterpart: the reference draws the

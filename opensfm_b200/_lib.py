@@ -106,6 +106,7 @@ _SIGNATURES = {
     "dn_postprocess_depth": ([_f, _f, _i, _i], _i),
     "dn_check_bounded_wait": ([_i, ctypes.c_int64, _f], _i),
     "dn_fp32_peak": ([ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], _i),
+    "dn_walk_ceiling": ([ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], _i),
     "dn_batch_sweep_features": ([_vp, _vp, ctypes.c_int64, _i, _i], _i),
     "dn_batch_targets": ([_vp, _vp, ctypes.c_int64, ctypes.c_float, _i], _i),
     "dn_batch_init_from_output": ([_vp, _i, _vp], _i),

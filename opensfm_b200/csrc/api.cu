@@ -2344,5 +2344,12 @@ dn_status dn_fp32_peak(double* tflops, double* ms) {
   DN_CUDA(dn::fp32_peak(tflops, ms));
   return DN_OK;
 }
+dn_status dn_walk_ceiling(double* gtaps, double* ms) {
+  const dn::DeviceRestore device_restore_;
+  DN_CHECK(gtaps && ms, "NULL output");
+  DN_TRY(need_device());
+  DN_CUDA(dn::walk_ceiling(gtaps, ms));
+  return DN_OK;
+}
 
 }  // extern "C"

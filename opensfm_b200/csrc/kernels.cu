@@ -6,6 +6,7 @@
 // (map, tile_x, tile_y) built on the host, so one launch covers every
 // depthmap of a reconstruction whatever their sizes.
 #include <algorithm>
+#include <vector>
 
 #include "cleanprune.cuh"
 #include "common.cuh"
@@ -991,6 +992,80 @@ __global__ void fp32_peak_kernel(float* out, int iters, float a, float b) {
   if (s == 1234.5f) out[0] = s;  // keeps the loop alive
 }
 
+// Ceiling of the coefficient-table walk: one thread per pixel, adjacent
+// threads on adjacent pixels, `walks` affine 7 x 7 walks per thread through
+// the production sampler (patch shift, sample_pair) and weighted sums on
+// packed FP32 pairs (mul, add, two FMAs per pair), and nothing else: no
+// candidate generation, warp setup, lane groups or NCC finish.  A walk is
+// 49 taps: columns 0-5 as 3 pairs per row, column 6 as row pairs (0, 1),
+// (2, 3), (4, 5) and row 6 alone.  Walk w is shifted by 0.75 (w & 15) px
+// across and 0.11 (w & 3) px down, with a 2 % scale and shear; pixels keep
+// a 16 px margin (32 px on the right), so every tap lies inside the padded
+// table (the kFast walk).
+__global__ void __launch_bounds__(256) walk_ceiling_kernel(const ViewDev v, int walks,
+                                                           float* __restrict__ out) {
+  const int x = 16 + blockIdx.x * blockDim.x + threadIdx.x, y = 16 + blockIdx.y;
+  if (x >= v.W - 32 || y >= v.H - 16) return;
+  const float ax = 1.02f, bx = 0.015f, ay = -0.01f, by = 0.98f;
+  const u64 MM = pk2(v.magic, v.magic);
+  const unsigned TP = (unsigned)v.TP;
+  const uint2* __restrict__ q0 = v.quad0;
+  u64 Wt[4], Wx[4];  // per column pair (the 4th: column 6), as the lanes hold them
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    Wt[m] = pk2(1.0f - 0.05f * m, 0.97f - 0.05f * m);
+    Wx[m] = pk2(0.1f * (x & 7) - 0.3f + 0.02f * m, 0.2f - 0.1f * (y & 3) + 0.03f * m);
+  }
+  float acc = 0.f;
+#pragma unroll 1
+  for (int w = 0; w < walks; ++w) {
+    const float X0 = (float)x + 0.75f * (float)(w & 15) + 0.37f;
+    const float Y0 = (float)y + 0.11f * (float)(w & 3) + 0.29f;
+    const float xl = fmaf(ax, -3.0f, fmaf(bx, -3.0f, X0)), yl = fmaf(ay, -3.0f, fmaf(by, -3.0f, Y0));
+    const float tx = __fadd_rd(X0, v.magic), ty = __fadd_rd(Y0, v.magic);
+    const float nsh = -quad_entry(
+        q0, (int)(__float_as_uint(ty) * TP + __float_as_uint(tx))).x;
+    u64 X[3], Y[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      X[m] = pk2(fmaf(ax, (float)(2 * m), xl), fmaf(ax, (float)(2 * m + 1), xl));
+      Y[m] = pk2(fmaf(ay, (float)(2 * m), yl), fmaf(ay, (float)(2 * m + 1), yl));
+    }
+    const float x6 = fmaf(ax, 6.0f, xl), y6 = fmaf(ay, 6.0f, yl);
+    u64 X6 = pk2(x6, __fadd_rn(x6, bx)), Y6 = pk2(y6, __fadd_rn(y6, by));
+    const u64 BX = pk2(bx, bx), BY = pk2(by, by), BX2 = pk2(2.f * bx, 2.f * bx),
+              BY2 = pk2(2.f * by, 2.f * by);
+    u64 S1 = 0ull, S2 = 0ull, S3 = 0ull;
+#pragma unroll
+    for (int r = 0; r < 7; ++r) {
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const u64 YY = sample_pair(X[m], Y[m], MM, TP, q0, nsh);
+        const u64 WY = mul2(Wt[m], YY);
+        S1 = add2(S1, WY);
+        S2 = fma2(WY, YY, S2);
+        S3 = fma2(Wx[m], YY, S3);
+        X[m] = add2(X[m], BX);
+        Y[m] = add2(Y[m], BY);
+      }
+      if (r < 3) {
+        const u64 YY = sample_pair(X6, Y6, MM, TP, q0, nsh);
+        const u64 WY = mul2(Wt[3], YY);
+        S1 = add2(S1, WY);
+        S2 = fma2(WY, YY, S2);
+        S3 = fma2(Wx[3], YY, S3);
+        X6 = add2(X6, BX2);
+        Y6 = add2(Y6, BY2);
+      }
+    }
+    const float y66 = table_sample(v, lo2(X6), lo2(Y6)) + nsh;  // row 6, column 6
+    const float wy = lo2(Wt[3]) * y66;
+    acc += (lo2(S1) + hi2(S1) + wy) + (lo2(S2) + hi2(S2) + wy * y66) +
+           (lo2(S3) + hi2(S3) + lo2(Wx[3]) * y66);
+  }
+  out[(size_t)y * v.W + x] = acc;
+}
+
 // Interleaves the state into the reference's output layout.
 __global__ void pack_kernel(const MapDev* __restrict__ maps, int map, float* __restrict__ plane) {
   const MapDev& m = maps[map];
@@ -1194,6 +1269,58 @@ cudaError_t fp32_peak(double* tflops, double* ms) {
   const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
   *ms = t;
   *tflops = flops / (t * 1e-3) / 1e12;
+  return cudaGetLastError();
+}
+
+cudaError_t walk_ceiling(double* gtaps, double* ms) {
+  // A 1024 x 768 view with a hashed texture, its table built as for any view.
+  const int W = 1024, H = 768, walks = 64;
+  const TableGeom tg = table_geom(W, H);
+  std::vector<uint8_t> host((size_t)W * H);
+  for (size_t k = 0; k < host.size(); ++k) host[k] = (uint8_t)((k * 2654435761u) >> 24);
+  uint8_t* u8 = nullptr;
+  __half* img = nullptr;
+  uint2* quad = nullptr;
+  float* out = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float t = 0.f;
+  cudaError_t e = cudaMalloc(&u8, host.size());
+  if (e == cudaSuccess) e = cudaMalloc(&img, host.size() * sizeof(__half));
+  if (e == cudaSuccess) e = cudaMalloc(&quad, (size_t)tg.TP * tg.TH * sizeof(uint2));
+  if (e == cudaSuccess) e = cudaMalloc(&out, host.size() * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(u8, host.data(), host.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_prepare_view(u8, W, H, W, img, quad, tg.TP, tg.TW, tg.TH, 128.f, 0);
+  if (e == cudaSuccess) {
+    ViewDev v{};
+    v.img = img;
+    v.quad = quad;
+    v.quad0 = quad + (size_t)kPad * tg.TP + kPad;
+    v.W = W;
+    v.H = H;
+    v.TP = tg.TP;
+    v.TH = tg.TH;
+    v.cbias = 128.f;
+    v.magic = tg.magic;
+    const dim3 grid((W - 48 + 255) / 256, H - 32);
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    walk_ceiling_kernel<<<grid, 256>>>(v, 4, out);  // warm-up
+    cudaEventRecord(e0);
+    walk_ceiling_kernel<<<grid, 256>>>(v, walks, out);
+    cudaEventRecord(e1);
+    e = cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&t, e0, e1);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(u8);
+  cudaFree(img);
+  cudaFree(quad);
+  cudaFree(out);
+  if (e != cudaSuccess) return e;
+  const double taps = (double)(W - 48) * (H - 32) * walks * 49;
+  *ms = t;
+  *gtaps = taps / (t * 1e-3) / 1e9;
   return cudaGetLastError();
 }
 

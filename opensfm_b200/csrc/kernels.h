@@ -119,6 +119,9 @@ inline TableGeom table_geom(int W, int H) {
 cudaError_t launch_pack(const MapDev* maps, int map, float* plane, size_t n, cudaStream_t s);
 cudaError_t launch_postprocess_plain(const float* in, float* out, int W, int H, cudaStream_t s);
 cudaError_t fp32_peak(double* tflops, double* ms);
+// G taps/s of walk_ceiling_kernel (the table walk and its sums alone) on a
+// 1024 x 768 view, 64 walks per pixel.
+cudaError_t walk_ceiling(double* gtaps, double* ms);
 
 // Cleaner / pruner (cleanprune.cu).
 struct CleanView {

@@ -29,7 +29,7 @@ from ._lib import _d, _f, _i32, _u8, check, ptr
 
 __all__ = ["DepthmapEstimator", "DepthmapCleaner", "DepthmapPruner", "GPUDepthmapCleaner",
            "DepthmapFuser", "SVOFuser", "DepthmapClusterEstimator", "Batch", "postprocess_depth",
-           "sor_filter", "fp32_peak"]
+           "sor_filter", "fp32_peak", "walk_ceiling"]
 
 
 def postprocess_depth(depth: np.ndarray) -> np.ndarray:
@@ -48,6 +48,15 @@ def fp32_peak() -> float:
     ms = ctypes.c_double()
     check(_lib.load().dn_fp32_peak(ctypes.byref(tf), ctypes.byref(ms)))
     return float(tf.value)
+
+
+def walk_ceiling() -> float:
+    """Measured ceiling of the scoring walk on the current device, G taps/s:
+    affine 7 x 7 table walks with their NCC sums alone (dn_walk_ceiling)."""
+    gt = ctypes.c_double()
+    ms = ctypes.c_double()
+    check(_lib.load().dn_walk_ceiling(ctypes.byref(gt), ctypes.byref(ms)))
+    return float(gt.value)
 
 
 def _mat(a, shape, name):

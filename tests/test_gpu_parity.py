@@ -1073,3 +1073,14 @@ def test_active_lists_match_tile_launch(scene, mode, tuning, seed):
         for a, w in zip(out[0][v], out[1][v]):
             assert np.array_equal(a, w)
     assert (out[0][0][0] > 0).mean() > 0.3
+
+
+def test_roofline_probes():
+    """The two measured denominators of the scoring roofline: the FP32 FMA
+    peak, and the ceiling of the table walk with its sums alone.  The walk
+    at 25 flops per tap cannot beat the FMA peak, and the production
+    half-pass cannot beat the walk alone."""
+    peak = pydense.fp32_peak()
+    ceiling = pydense.walk_ceiling()
+    assert 10.0 < peak < 200.0  # TFLOP/s
+    assert 0.0 < ceiling and 25.0 * ceiling * 1e9 <= 1.05 * peak * 1e12
