@@ -459,18 +459,37 @@ __device__ inline void halfpass_update(const MapDev& m, const PairViewSm& spv, i
         const long step = (long)di * W + dj;
         const long q0 = (long)i * W + j + (long)kFarStart * step;
         const float* wcol = reinterpret_cast<const float*>(m.state) + 3;
+        // The lanes of the group share the scan: lane l takes distances
+        // l, l + L, ..., keeping its first maximum; the group then keeps the
+        // higher score, the lower distance index among equal ones.  That is
+        // the first maximum of the scan in order, as one lane would find it.
         float bs = -3.0f;
+        int bk = kFarSamples;  // none
 #pragma unroll
-        for (int k = 0; k < kFarSamples; ++k) {
+        for (int k0 = 0; k0 < kFarSamples; k0 += L) {
+          const int k = k0 + lane;
           if (k < n_in) {
             const long qq = q0 + 2 * k * step;
             const float sq = m.score[qq], dq = wcol[4 * qq];
             if (sq > bs && dq != 0.0f) {
               bs = sq;
-              q = qq;
+              bk = k;
             }
           }
         }
+        if (L > 1) {
+          const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
+#pragma unroll
+          for (int o = 1; o < L; o <<= 1) {
+            const float os = __shfl_xor_sync(gmask, bs, o);
+            const int ok = __shfl_xor_sync(gmask, bk, o);
+            if (os > bs || (os == bs && ok < bk)) {
+              bs = os;
+              bk = ok;
+            }
+          }
+        }
+        if (bk < kFarSamples) q = q0 + 2 * bk * step;
       }
       if (q >= 0) {
         const float4 sq = m.state[q];
