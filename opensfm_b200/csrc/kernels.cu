@@ -637,16 +637,32 @@ __device__ inline bool active_pixel(const MapDev& m, const int4 tl, const RunPar
   return ((own | ch[pix - W] | ch[pix + W] | ch[pix - 1] | ch[pix + 1]) & kMoved) != 0;
 }
 
-// The number of active pixels of every half-pass tile.
+// Half-pass tiles per block of the list-building kernels: a block's tiles
+// are read together, so their dependent loads (tile, map, flags) overlap.
+constexpr int kListTiles = 4;
+
+// The number of active pixels of every half-pass tile; block b takes tiles
+// kListTiles b ... kListTiles b + kListTiles - 1.
 template <int L>
 __global__ void __launch_bounds__(128)
-active_count_kernel(const MapDev* __restrict__ maps, const int4* __restrict__ tiles, RunParams p,
-                    int* __restrict__ tile_count) {
-  const int4 tl = tiles[blockIdx.x];
-  size_t pix;
-  const bool act = active_pixel<L>(maps[tl.x], tl, p, pix);
-  const int n = __syncthreads_count(act);
-  if (threadIdx.x == 0 && threadIdx.y == 0) tile_count[blockIdx.x] = n;
+active_count_kernel(const MapDev* __restrict__ maps, const int4* __restrict__ tiles, int n_tiles,
+                    RunParams p, int* __restrict__ tile_count) {
+  const int t0 = blockIdx.x * kListTiles;
+  bool act[kListTiles];
+#pragma unroll
+  for (int u = 0; u < kListTiles; ++u) {
+    act[u] = false;
+    if (t0 + u < n_tiles) {
+      const int4 tl = tiles[t0 + u];
+      size_t pix;
+      act[u] = active_pixel<L>(maps[tl.x], tl, p, pix);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kListTiles; ++u) {
+    const int n = __syncthreads_count(act[u]);
+    if (threadIdx.x == 0 && threadIdx.y == 0 && t0 + u < n_tiles) tile_count[t0 + u] = n;
+  }
 }
 
 // One block of 1024 threads per map: tile_off[t] = the active pixels of the
@@ -688,23 +704,41 @@ active_scan_kernel(const MapDev* __restrict__ maps, const int* __restrict__ tile
 }
 
 // The active pixels of every half-pass tile at the tile's offset, in the
-// tile's row order: the lists are in tile order, whatever the timing.
+// tile's row order: the lists are in tile order, whatever the timing.  Block
+// b takes tiles kListTiles b ... as active_count_kernel does.
 template <int L>
 __global__ void __launch_bounds__(128)
-active_write_kernel(const MapDev* __restrict__ maps, const int4* __restrict__ tiles, RunParams p,
-                    const int* __restrict__ tile_off) {
-  const int4 tl = tiles[blockIdx.x];
-  const MapDev& m = maps[tl.x];
-  size_t pix;
-  const bool act = active_pixel<L>(m, tl, p, pix);
-  __shared__ int wcount[32];
+active_write_kernel(const MapDev* __restrict__ maps, const int4* __restrict__ tiles, int n_tiles,
+                    RunParams p, const int* __restrict__ tile_off) {
+  const int t0 = blockIdx.x * kListTiles;
+  bool act[kListTiles];
+  size_t pix[kListTiles];
+#pragma unroll
+  for (int u = 0; u < kListTiles; ++u) {
+    act[u] = false;
+    pix[u] = 0;
+    if (t0 + u < n_tiles) {
+      const int4 tl = tiles[t0 + u];
+      act[u] = active_pixel<L>(maps[tl.x], tl, p, pix[u]);
+    }
+  }
+  __shared__ int wcount[kListTiles][32];
   const int lin = threadIdx.y * blockDim.x + threadIdx.x, wl = lin & 31, w = lin >> 5;
-  const unsigned ballot = __ballot_sync(0xffffffffu, act);
-  if (wl == 0) wcount[w] = __popc(ballot);
+  unsigned ballot[kListTiles];
+#pragma unroll
+  for (int u = 0; u < kListTiles; ++u) {
+    ballot[u] = __ballot_sync(0xffffffffu, act[u]);
+    if (wl == 0) wcount[u][w] = __popc(ballot[u]);
+  }
   __syncthreads();
-  int before = 0;
-  for (int k = 0; k < w; ++k) before += wcount[k];
-  if (act) m.alist[tile_off[blockIdx.x] + before + __popc(ballot & ((1u << wl) - 1u))] = (int)pix;
+#pragma unroll
+  for (int u = 0; u < kListTiles; ++u) {
+    if (!act[u]) continue;
+    const MapDev& m = maps[tiles[t0 + u].x];
+    int before = 0;
+    for (int k = 0; k < w; ++k) before += wcount[u][k];
+    m.alist[tile_off[t0 + u] + before + __popc(ballot[u] & ((1u << wl) - 1u))] = (int)pix[u];
+  }
 }
 
 // chunk0[k] = the chunks of `per` listed pixels of maps 0..k-1 (k = 0 ..
@@ -771,9 +805,10 @@ static cudaError_t launch_list_hpz(bool sample, const LaunchArgs& a, int n_maps,
                                    int* chunk0, int* tile_count, int* tile_off, cudaStream_t s) {
   const dim3 blk(a.bx, a.by);
   const int per = (a.bx / L) * a.by;
-  active_count_kernel<L><<<a.n_tiles, blk, 0, s>>>(a.maps, a.tiles, a.p, tile_count);
+  const int list_blocks = (a.n_tiles + kListTiles - 1) / kListTiles;
+  active_count_kernel<L><<<list_blocks, blk, 0, s>>>(a.maps, a.tiles, a.n_tiles, a.p, tile_count);
   active_scan_kernel<<<n_maps, 1024, 0, s>>>(a.maps, tile_count, tile_off);
-  active_write_kernel<L><<<a.n_tiles, blk, 0, s>>>(a.maps, a.tiles, a.p, tile_off);
+  active_write_kernel<L><<<list_blocks, blk, 0, s>>>(a.maps, a.tiles, a.n_tiles, a.p, tile_off);
   chunk_offsets_kernel<<<1, 32, 0, s>>>(a.maps, n_maps, per, chunk0);
   // A resident grid: every block walks chunks until the lists are done.
   auto kern = sample ? halfpass_list_kernel<HPZ, true, L> : halfpass_list_kernel<HPZ, false, L>;
