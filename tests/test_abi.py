@@ -53,6 +53,9 @@ def test_null_arguments_are_rejected_without_device():
     assert lib.dn_cleaner_clean(None, None) == _lib.DN_INVALID_ARG
     assert lib.dn_pruner_prune(None, None) == _lib.DN_INVALID_ARG
     assert lib.dn_batch_run(None, 0) == _lib.DN_INVALID_ARG
+    assert lib.dn_batch_upload_view_image(None, 0, None, 0) == _lib.DN_INVALID_ARG
+    assert lib.dn_batch_get_depths_async(None, 0, None, None, 0) == _lib.DN_INVALID_ARG
+    assert lib.dn_walk_ceiling(None, None) == _lib.DN_INVALID_ARG
 
 
 def test_pydense_argument_validation():
