@@ -516,17 +516,20 @@ __device__ __forceinline__ float h16lo_add(unsigned w, float c) {
 
 // ------------------------------------------------------------------------
 // Cooperative 7 x 7 patch: L lanes (2, 4 or 8, adjacent in the warp) share
-// one pixel.  The patch is padded to 8 columns; lane l owns columns l, l + L,
-// ... (8 / L columns x 7 rows), the padding column carries weight 0 and
-// samples column 6's position.  Each lane keeps 2 x 56 / L weights instead of
-// 98, so more warps fit on an SM, and lanes l and l + 1 read neighbouring
-// table entries (with 8 lanes a group reads a whole patch row at once).  The warp setup of a view is computed by one lane of the
+// one pixel, each lane holding the weights of its slots (coop_slot).  With 4
+// or 8 lanes the patch is padded to 8 columns: lane l owns columns l, l + L,
+// ... (8 / L columns x 7 rows), and the padding column carries weight 0 and
+// samples column 6's position; lanes l and l + 1 read neighbouring table
+// entries (with 8 lanes a group reads a whole patch row at once).  With 2
+// lanes the 49 taps split 25 / 24 without a padding column: each lane holds
+// 25 slots (24 on lane 1, plus one of weight 0) instead of 28, in 12 pairs
+// and one single.  The warp setup of a view is computed by one lane of the
 // group and broadcast; the three sums are combined with XOR shuffles, so
 // every lane of a group ends with the same score.
 template <int L>
 struct CoopPatch {
-  static constexpr int C = 8 / L;  // columns per lane
-  static constexpr int S = 7 * C;  // slots per lane
+  static constexpr int C = 8 / L;  // columns per lane (4 and 8 lanes)
+  static constexpr int S = L == 2 ? 25 : 7 * C;  // slots per lane
   static constexpr int P = S / 2;  // slot pairs per lane: slots 2k, 2k + 1
   static constexpr bool ODD = (S & 1) != 0;  // one column (L = 8): slot 6 alone
   u64 w2[P];                       // bilateral weights, packed in slot pairs
@@ -539,6 +542,46 @@ struct CoopPatch {
   int src0;       // warp lane of the group's lane 0
 };
 
+// Patch position (dx, dy in 0..6) of slot t of a lane; false for a padding
+// slot (weight 0, sampled at a real position).  2 lanes: slots 0-13 are rows
+// 0-6 of columns lane and lane + 2 (paired across the two columns), 14-19
+// rows 0-5 of column lane + 4 (paired across rows), 20-23 rows 0-3 (lane 0)
+// or 4-6 and a padding slot at row 6 (lane 1) of column 6, and 24 row 6 of
+// column lane + 4.  4 and 8 lanes: slot r C + q is row r of column
+// lane + L q, column 7 padding at column 6.
+template <int L>
+__device__ __forceinline__ bool coop_slot(int lane, int t, int& dx, int& dy) {
+  if constexpr (L == 2) {
+    if (t < 14) {
+      dx = lane + 2 * (t & 1);
+      dy = t >> 1;
+    } else if (t < 20) {
+      dx = lane + 4;
+      dy = t - 14;
+    } else if (t < 24) {
+      dx = 6;
+      dy = 4 * lane + (t - 20);
+      if (dy > 6) {
+        dy = 6;
+        return false;
+      }
+    } else {
+      dx = lane + 4;
+      dy = 6;
+    }
+    return true;
+  } else {
+    constexpr int C = 8 / L;
+    dx = lane + L * (t % C);
+    dy = t / C;
+    if (dx > 6) {
+      dx = 6;
+      return false;
+    }
+    return true;
+  }
+}
+
 template <int L>
 __device__ inline float group_sum(float v, unsigned mask) {
 #pragma unroll
@@ -548,7 +591,6 @@ __device__ inline float group_sum(float v, unsigned mask) {
 
 template <int L, class Src>
 __device__ inline void coop_patch_build(CoopPatch<L>& cp, const Src& src, int lane, unsigned mask) {
-  constexpr int C = CoopPatch<L>::C;
   cp.lane = lane;
   cp.mask = mask;
   cp.src0 = (threadIdx.x & 31) - lane;
@@ -558,24 +600,20 @@ __device__ inline void coop_patch_build(CoopPatch<L>& cp, const Src& src, int la
   float sw = 0.f, swx = 0.f;
   float ws[CoopPatch<L>::S], xs[CoopPatch<L>::S];
 #pragma unroll
-  for (int r = 0; r < 7; ++r)
-#pragma unroll
-    for (int q = 0; q < C; ++q) {
-      const int t = r * C + q;
-      const int dx = lane + L * q;
-      const bool real = dx < 7;
-      const int dxx = real ? dx : 6;
-      const float x = src(r - 3, dxx - 3);
-      const float d = __fsub_rn(x, c);
-      const int ddx = dxx - 3, ddy = r - 3;
-      const float arg = __fsub_rn(__fmul_rn(__fmul_rn(-d, d), dcf),
-                                  __fmul_rn((float)(ddx * ddx + ddy * ddy), dxf));
-      const float w = real ? expf(arg) : 0.0f;
-      ws[t] = w;
-      xs[t] = x;
-      sw += w;
-      swx = fmaf(w, x, swx);
-    }
+  for (int t = 0; t < CoopPatch<L>::S; ++t) {
+    int dx, dy;
+    const bool real = coop_slot<L>(lane, t, dx, dy);
+    const float x = src(dy - 3, dx - 3);
+    const float d = __fsub_rn(x, c);
+    const int ddx = dx - 3, ddy = dy - 3;
+    const float arg = __fsub_rn(__fmul_rn(__fmul_rn(-d, d), dcf),
+                                __fmul_rn((float)(ddx * ddx + ddy * ddy), dxf));
+    const float w = real ? expf(arg) : 0.0f;
+    ws[t] = w;
+    xs[t] = x;
+    sw += w;
+    swx = fmaf(w, x, swx);
+  }
   sw = group_sum<L>(sw, mask);
   swx = group_sum<L>(swx, mask);
   const float inv_sw = 1.0f / sw;
@@ -633,23 +671,20 @@ __device__ inline float coop_col(int lane, int q) {
 template <int L>
 __device__ inline float coop_walk_clamped(const CoopPatch<L>& cp, const ViewDev& vw,
                                           const Warp& wp) {
-  constexpr int C = CoopPatch<L>::C;
-  const float dx0 = (float)(cp.lane - 3);
-  const float xl = fmaf(wp.ax, dx0, fmaf(wp.bx, -3.0f, wp.X0));
-  const float yl = fmaf(wp.ay, dx0, fmaf(wp.by, -3.0f, wp.Y0));
-  const float sh = patch_shift<true>(vw, wp);
-  float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  if constexpr (L == 2) {
+    // The slots in order, each at X0 + ax (dx - 3) + bx (dy - 3).
+    const float sh = patch_shift<true>(vw, wp);
+    float s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
-  for (int r = 0; r < 7; ++r) {
-    const float xr = fmaf(wp.bx, (float)r, xl), yr = fmaf(wp.by, (float)r, yl);
-#pragma unroll
-    for (int q = 0; q < C; ++q) {
-      const float cq = coop_col<L>(cp.lane, q);
-      const float x = fmaf(wp.ax, cq, xr), yv = fmaf(wp.ay, cq, yr);
+    for (int t = 0; t < CoopPatch<L>::S; ++t) {
+      int dx, dy;
+      coop_slot<L>(cp.lane, t, dx, dy);
+      const float fx = (float)(dx - 3), fy = (float)(dy - 3);
+      const float x = fmaf(wp.ax, fx, fmaf(wp.bx, fy, wp.X0));
+      const float yv = fmaf(wp.ay, fx, fmaf(wp.by, fy, wp.Y0));
       const float y = table_sample_clamped(vw, x, yv) - sh;
-      const int t = r * C + q;
       float w, wx;
-      if (CoopPatch<L>::ODD && t == CoopPatch<L>::S - 1) {
+      if (t == CoopPatch<L>::S - 1) {
         w = cp.wt;
         wx = cp.wxt;
       } else {
@@ -662,8 +697,40 @@ __device__ inline float coop_walk_clamped(const CoopPatch<L>& cp, const ViewDev&
       s2 = fmaf(wy, y, s2);
       s3 = fmaf(wx, y, s3);
     }
+    return coop_finish<L>(cp, s1, s2, s3);
+  } else {
+    constexpr int C = CoopPatch<L>::C;
+    const float dx0 = (float)(cp.lane - 3);
+    const float xl = fmaf(wp.ax, dx0, fmaf(wp.bx, -3.0f, wp.X0));
+    const float yl = fmaf(wp.ay, dx0, fmaf(wp.by, -3.0f, wp.Y0));
+    const float sh = patch_shift<true>(vw, wp);
+    float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+    for (int r = 0; r < 7; ++r) {
+      const float xr = fmaf(wp.bx, (float)r, xl), yr = fmaf(wp.by, (float)r, yl);
+#pragma unroll
+      for (int q = 0; q < C; ++q) {
+        const float cq = coop_col<L>(cp.lane, q);
+        const float x = fmaf(wp.ax, cq, xr), yv = fmaf(wp.ay, cq, yr);
+        const float y = table_sample_clamped(vw, x, yv) - sh;
+        const int t = r * C + q;
+        float w, wx;
+        if (CoopPatch<L>::ODD && t == CoopPatch<L>::S - 1) {
+          w = cp.wt;
+          wx = cp.wxt;
+        } else {
+          const u64 wpair = cp.w2[t >> 1], wxpair = cp.wx2[t >> 1];
+          w = (t & 1) ? hi2(wpair) : lo2(wpair);
+          wx = (t & 1) ? hi2(wxpair) : lo2(wxpair);
+        }
+        const float wy = w * y;
+        s1 += wy;
+        s2 = fmaf(wy, y, s2);
+        s3 = fmaf(wx, y, s3);
+      }
+    }
+    return coop_finish<L>(cp, s1, s2, s3);
   }
-  return coop_finish<L>(cp, s1, s2, s3);
 }
 
 // Two table samples at the packed positions (X, Y), centred by nsh (minus
@@ -707,7 +774,66 @@ __device__ inline float coop_walk_fast(const CoopPatch<L>& cp, const ViewDev& vw
   const float nsh = -patch_shift<false>(vw, wp);
   u64 S1 = 0ull, S2 = 0ull, S3 = 0ull;  // (+0.0f, +0.0f) pairs
   float t1 = 0.f, t2 = 0.f, t3 = 0.f;   // the unpaired slot
-  if constexpr (C == 1) {
+  if constexpr (L == 2) {
+    // Columns lane and lane + 2, one row per step (slots 0-13).
+    const u64 BX = pk2(wp.bx, wp.bx), BY = pk2(wp.by, wp.by);
+    u64 X = pk2(xl, fmaf(wp.ax, 2.0f, xl)), Y = pk2(yl, fmaf(wp.ay, 2.0f, yl));
+#pragma unroll
+    for (int r = 0; r < 7; ++r) {
+      const u64 YY = sample_pair(X, Y, MM, TP, q0, nsh);
+      const u64 WY = mul2(cp.w2[r], YY);
+      S1 = add2(S1, WY);
+      S2 = fma2(WY, YY, S2);
+      S3 = fma2(cp.wx2[r], YY, S3);
+      if (r < 6) {
+        X = add2(X, BX);
+        Y = add2(Y, BY);
+      }
+    }
+    // Column lane + 4, two rows per step (slots 14-19); its row 6 is slot 24.
+    const float xb = fmaf(wp.ax, 4.0f, xl), yb = fmaf(wp.ay, 4.0f, yl);
+    const u64 BX2 = pk2(2.0f * wp.bx, 2.0f * wp.bx), BY2 = pk2(2.0f * wp.by, 2.0f * wp.by);
+    X = pk2(xb, __fadd_rn(xb, wp.bx));
+    Y = pk2(yb, __fadd_rn(yb, wp.by));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const u64 YY = sample_pair(X, Y, MM, TP, q0, nsh);
+      const u64 WY = mul2(cp.w2[7 + k], YY);
+      S1 = add2(S1, WY);
+      S2 = fma2(WY, YY, S2);
+      S3 = fma2(cp.wx2[7 + k], YY, S3);
+      if (k < 2) {
+        X = add2(X, BX2);
+        Y = add2(Y, BY2);
+      }
+    }
+    // Column 6 (slots 20-23): rows 0-3 on lane 0; rows 4-6 and row 6 again
+    // (weight 0) on lane 1.
+    const float lf = (float)cp.lane;
+    const float x6 = fmaf(wp.bx, 4.0f * lf, fmaf(wp.ax, 6.0f - lf, xl));
+    const float y6 = fmaf(wp.by, 4.0f * lf, fmaf(wp.ay, 6.0f - lf, yl));
+    const float last = cp.lane ? 2.0f : 3.0f;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      if (k == 0) {
+        X = pk2(x6, __fadd_rn(x6, wp.bx));
+        Y = pk2(y6, __fadd_rn(y6, wp.by));
+      } else {
+        X = pk2(fmaf(wp.bx, 2.0f, x6), fmaf(wp.bx, last, x6));
+        Y = pk2(fmaf(wp.by, 2.0f, y6), fmaf(wp.by, last, y6));
+      }
+      const u64 YY = sample_pair(X, Y, MM, TP, q0, nsh);
+      const u64 WY = mul2(cp.w2[10 + k], YY);
+      S1 = add2(S1, WY);
+      S2 = fma2(WY, YY, S2);
+      S3 = fma2(cp.wx2[10 + k], YY, S3);
+    }
+    const float y24 = table_sample(vw, fmaf(wp.bx, 6.0f, xb), fmaf(wp.by, 6.0f, yb)) + nsh;
+    const float wy = cp.wt * y24;
+    t1 = wy;
+    t2 = wy * y24;
+    t3 = cp.wxt * y24;
+  } else if constexpr (C == 1) {
     const float c0 = coop_col<L>(cp.lane, 0);
     const float xc = fmaf(wp.ax, c0, xl), yc = fmaf(wp.ay, c0, yl);
     u64 X = pk2(xc, __fadd_rn(xc, wp.bx)), Y = pk2(yc, __fadd_rn(yc, wp.by));
