@@ -550,7 +550,7 @@ struct CoopPatch {
 // column lane + 4.  4 and 8 lanes: slot r C + q is row r of column
 // lane + L q, column 7 padding at column 6.
 template <int L>
-__device__ __forceinline__ bool coop_slot(int lane, int t, int& dx, int& dy) {
+__host__ __device__ __forceinline__ bool coop_slot(int lane, int t, int& dx, int& dy) {
   if constexpr (L == 2) {
     if (t < 14) {
       dx = lane + 2 * (t & 1);
